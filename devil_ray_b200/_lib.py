@@ -1,0 +1,101 @@
+"""ctypes binding of the C-ABI in include/drb.h (libdrb.so, built in-tree).
+
+The library is loaded from the package directory only; there is no CPU
+fallback.  If the shared object is missing the import fails loudly.
+"""
+from __future__ import annotations
+
+import ctypes as C
+from pathlib import Path
+
+_PKG = Path(__file__).resolve().parent
+LIB_PATH = _PKG / "libdrb.so"
+
+DRB_OK = 0
+DRB_ERR_INVALID_ARG = 1
+DRB_ERR_OOM = 2
+DRB_ERR_CUDA = 3
+DRB_ERR_QUEUE_GIVEUP = 4
+DRB_ERR_UNSUPPORTED = 5
+
+GUESS_ZERO = 0
+GUESS_ELEM_CENTER = 1
+GUESS_SUBREF_CENTER = 2
+GUESS_GIVEN = 3
+
+
+class DrbMesh(C.Structure):
+    _fields_ = [("dim", C.c_int), ("order", C.c_int), ("ncomp", C.c_int),
+                ("n_elem", C.c_int), ("n_ctrl", C.c_int),
+                ("ctrl_idx", C.c_void_p), ("values", C.c_void_p), ("packed", C.c_void_p)]
+
+
+class DrbBvh(C.Structure):
+    _fields_ = [("n_inner", C.c_int), ("n_leaf", C.c_int),
+                ("inner_nodes", C.c_void_p), ("leaf_nodes", C.c_void_p),
+                ("aabb_ids", C.c_void_p), ("ref_boxes", C.c_void_p),
+                ("bounds", C.c_float * 6)]
+
+
+class DrbNewtonOpts(C.Structure):
+    _fields_ = [("tol", C.c_float), ("max_steps", C.c_int), ("guess_mode", C.c_int),
+                ("guess", C.c_void_p)]
+
+
+class DrbQueryStats(C.Structure):
+    _fields_ = [("iters", C.c_void_p), ("candidates", C.c_void_p)]
+
+
+class DrbError(RuntimeError):
+    def __init__(self, status: int, where: str, msg: str):
+        super().__init__(f"{where} failed with status {status}: {msg}")
+        self.status = status
+
+
+_lib = None
+
+# name -> (restype, argtypes)
+_SIGS = {
+    "drb_last_error": (C.c_char_p, []),
+    "drb_version": (C.c_int, []),
+    "drb_packed_stride": (C.c_int, [C.c_int, C.c_int, C.c_int]),
+    "drb_pack_elements": (C.c_int, [C.POINTER(DrbMesh), C.c_void_p, C.c_void_p]),
+    "drb_bvh_sizes": (C.c_int, [C.c_int, C.c_int, C.POINTER(C.c_int), C.POINTER(C.c_int)]),
+    "drb_elem_subboxes": (C.c_int, [C.POINTER(DrbMesh), C.c_void_p, C.c_void_p, C.c_void_p,
+                                    C.c_void_p, C.c_void_p]),
+    "drb_morton_codes": (C.c_int, [C.c_void_p, C.c_int, C.c_void_p, C.c_void_p, C.c_void_p]),
+    "drb_radix_sort_pairs": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p,
+                                       C.c_int, C.c_int, C.c_void_p]),
+    "drb_lbvh_build": (C.c_int, [C.POINTER(DrbMesh), C.POINTER(DrbBvh), C.c_void_p, C.c_void_p]),
+    "drb_locate": (C.c_int, [C.POINTER(DrbMesh), C.POINTER(DrbBvh), C.c_void_p, C.c_int,
+                             C.POINTER(DrbNewtonOpts), C.c_void_p, C.c_void_p, DrbQueryStats,
+                             C.c_void_p]),
+}
+
+
+def declared_symbols():
+    """Names of every entry point declared in include/drb.h."""
+    import re
+    hdr = (_PKG.parent / "include" / "drb.h").read_text()
+    return sorted(set(re.findall(r"^\s*(?:const\s+)?\w+\s*\*?\s*(drb_\w+)\s*\(", hdr, re.M)))
+
+
+def lib():
+    """Load libdrb.so (raises if it has not been built)."""
+    global _lib
+    if _lib is None:
+        if not LIB_PATH.exists():
+            raise ImportError(f"{LIB_PATH} is missing: run __graft_entry__.build() "
+                              "(no CPU fallback exists)")
+        L = C.CDLL(str(LIB_PATH))
+        for name, (res, args) in _SIGS.items():
+            fn = getattr(L, name)
+            fn.restype = res
+            fn.argtypes = args
+        _lib = L
+    return _lib
+
+
+def check(status: int, where: str):
+    if status != DRB_OK:
+        raise DrbError(status, where, lib().drb_last_error().decode(errors="replace"))

@@ -1,0 +1,198 @@
+"""Host-side mirror of the reference's data model for this path, over the
+C-ABI (libdrb.so), with torch tensors as device-memory plumbing.
+
+Names follow Devil Ray (src/dray):
+  GridFunction        data_model/grid_function.hpp:19-50
+  UnstructuredMesh    data_model/unstructured_mesh.hpp (get_bvh, locate, bounds)
+  UnstructuredField   data_model/unstructured_field.hpp
+  BVH                 bvh.hpp:16-37
+  Location            location.hpp:16-20 (cell id, reference point)
+
+All compute goes through libdrb.so; there is no CPU fallback.
+"""
+from __future__ import annotations
+
+import ctypes as C
+from dataclasses import dataclass
+
+import numpy as np
+import torch
+
+from . import _lib as L
+
+
+def _ptr(t: torch.Tensor | None):
+    if t is None:
+        return None
+    return C.c_void_p(t.data_ptr())
+
+
+def _stream(stream=None):
+    s = stream if stream is not None else torch.cuda.current_stream()
+    return C.c_void_p(s.cuda_stream)
+
+
+def _dev(a, dtype, device):
+    if isinstance(a, torch.Tensor):
+        return a.to(device=device, dtype=dtype).contiguous()
+    return torch.as_tensor(np.ascontiguousarray(a), dtype=dtype, device=device).contiguous()
+
+
+@dataclass
+class GridFunction:
+    """ctrl_idx int32[n_elem*nd] + values float[n_ctrl, ncomp] on the device."""
+    ctrl_idx: torch.Tensor
+    values: torch.Tensor
+    el_dofs: int
+
+    @property
+    def num_elem(self) -> int:
+        return self.ctrl_idx.numel() // self.el_dofs
+
+
+class BVH:
+    """Device BVH in the reference layout (4 x float4 per inner node)."""
+
+    def __init__(self, dim: int, n_elem: int, device):
+        ni, nl = C.c_int(), C.c_int()
+        L.check(L.lib().drb_bvh_sizes(dim, n_elem, C.byref(ni), C.byref(nl)), "drb_bvh_sizes")
+        self.n_inner, self.n_leaf = ni.value, nl.value
+        self.inner_nodes = torch.empty((self.n_inner, 16), dtype=torch.float32, device=device)
+        self.leaf_nodes = torch.empty(self.n_leaf, dtype=torch.int32, device=device)
+        self.aabb_ids = torch.empty(self.n_leaf, dtype=torch.int32, device=device)
+        self.ref_boxes = torch.empty((self.n_leaf, 2 * dim), dtype=torch.float32, device=device)
+        self.bounds = np.zeros(6, np.float32)
+        self.sorted_codes = None
+
+    def desc(self) -> L.DrbBvh:
+        d = L.DrbBvh()
+        d.n_inner, d.n_leaf = self.n_inner, self.n_leaf
+        d.inner_nodes = self.inner_nodes.data_ptr()
+        d.leaf_nodes = self.leaf_nodes.data_ptr()
+        d.aabb_ids = self.aabb_ids.data_ptr()
+        d.ref_boxes = self.ref_boxes.data_ptr()
+        for q in range(6):
+            d.bounds[q] = float(self.bounds[q])
+        return d
+
+
+class UnstructuredMesh:
+    """Tensor Bernstein hex (dim 3) or quad (dim 2) mesh of order 1..3."""
+
+    def __init__(self, ctrl_idx, xyz, order: int, dim: int = 3, device="cuda", pack: bool = True):
+        self.dim = dim
+        self.order = int(order)
+        nd = (self.order + 1) ** dim
+        self.dof_data = GridFunction(_dev(ctrl_idx, torch.int32, device),
+                                     _dev(xyz, torch.float32, device).reshape(-1, 3), nd)
+        self.device = torch.device(device)
+        self.packed = None
+        self._bvh = None
+        if pack:
+            self.pack()
+
+    @property
+    def n_elem(self) -> int:
+        return self.dof_data.num_elem
+
+    def cells(self) -> int:
+        return self.n_elem
+
+    def desc(self, packed: bool = True) -> L.DrbMesh:
+        m = L.DrbMesh()
+        m.dim, m.order, m.ncomp = self.dim, self.order, 3
+        m.n_elem = self.n_elem
+        m.n_ctrl = self.dof_data.values.shape[0]
+        m.ctrl_idx = self.dof_data.ctrl_idx.data_ptr()
+        m.values = self.dof_data.values.data_ptr()
+        m.packed = self.packed.data_ptr() if (packed and self.packed is not None) else None
+        return m
+
+    def pack(self, stream=None):
+        stride = L.lib().drb_packed_stride(self.dim, self.order, 3)
+        self.packed = torch.empty((max(self.n_elem, 1), stride), dtype=torch.float32,
+                                  device=self.device)
+        d = self.desc(packed=False)
+        L.check(L.lib().drb_pack_elements(C.byref(d), _ptr(self.packed), _stream(stream)),
+                "drb_pack_elements")
+
+    def get_bvh(self, stream=None, keep_codes: bool = False) -> BVH:
+        """Lazily build the LBVH (UnstructuredMesh::get_bvh,
+        data_model/unstructured_mesh.cpp:23-31)."""
+        if self._bvh is None:
+            self._bvh = self.build_bvh(stream, keep_codes)
+        return self._bvh
+
+    def build_bvh(self, stream=None, keep_codes: bool = False) -> BVH:
+        b = BVH(self.dim, self.n_elem, self.device)
+        codes = None
+        if keep_codes:
+            codes = torch.empty(b.n_leaf, dtype=torch.int32, device=self.device)
+        d = self.desc()
+        bd = b.desc()
+        L.check(L.lib().drb_lbvh_build(C.byref(d), C.byref(bd), _ptr(codes), _stream(stream)),
+                "drb_lbvh_build")
+        b.bounds = np.array(list(bd.bounds), np.float32)
+        b.sorted_codes = codes
+        return b
+
+    def bounds(self):
+        return self.get_bvh().bounds
+
+    def locate(self, points, tol: float = 1e-4, max_steps: int = 20,
+               guess_mode: int = L.GUESS_ELEM_CENTER, guess=None, stats: bool = False,
+               stream=None, packed: bool = True):
+        """Mesh::locate: returns (cell int32[n], ref float[n,3]) and, with
+        stats=True, (iterations, candidates) per point."""
+        pts = _dev(points, torch.float32, self.device).reshape(-1, 3)
+        n = pts.shape[0]
+        cell = torch.empty(n, dtype=torch.int32, device=self.device)
+        ref = torch.empty((n, 3), dtype=torch.float32, device=self.device)
+        it = cand = None
+        if stats:
+            it = torch.empty(n, dtype=torch.int32, device=self.device)
+            cand = torch.empty(n, dtype=torch.int32, device=self.device)
+        g = None if guess is None else _dev(guess, torch.float32, self.device).reshape(-1, 3)
+        opts = L.DrbNewtonOpts(tol, max_steps, guess_mode, None if g is None else g.data_ptr())
+        st = L.DrbQueryStats(None if it is None else it.data_ptr(),
+                             None if cand is None else cand.data_ptr())
+        b = self.get_bvh(stream)
+        d = self.desc(packed)
+        bd = b.desc()
+        L.check(L.lib().drb_locate(C.byref(d), C.byref(bd), _ptr(pts), n, C.byref(opts),
+                                   _ptr(cell), _ptr(ref), st, _stream(stream)), "drb_locate")
+        if stats:
+            return cell, ref, it, cand
+        return cell, ref
+
+
+def elem_subboxes(mesh: UnstructuredMesh, stream=None):
+    """Per-element sub-boxes (aabbs6, prim_ids, ref_boxes, bounds6) on device."""
+    nb = 33 if mesh.dim == 3 else 17
+    n = mesh.n_elem * nb
+    dev = mesh.device
+    aabbs = torch.empty((n, 6), dtype=torch.float32, device=dev)
+    prim = torch.empty(n, dtype=torch.int32, device=dev)
+    refb = torch.empty((n, 2 * mesh.dim), dtype=torch.float32, device=dev)
+    bounds = torch.empty(6, dtype=torch.float32, device=dev)
+    d = mesh.desc()
+    L.check(L.lib().drb_elem_subboxes(C.byref(d), _ptr(aabbs), _ptr(prim), _ptr(refb),
+                                      _ptr(bounds), _stream(stream)), "drb_elem_subboxes")
+    return aabbs, prim, refb, bounds
+
+
+def morton_codes(aabbs6: torch.Tensor, bounds6: torch.Tensor, stream=None):
+    n = aabbs6.shape[0]
+    codes = torch.empty(n, dtype=torch.int32, device=aabbs6.device)
+    L.check(L.lib().drb_morton_codes(_ptr(aabbs6), n, _ptr(bounds6), _ptr(codes),
+                                     _stream(stream)), "drb_morton_codes")
+    return codes
+
+
+def radix_sort_pairs(keys: torch.Tensor, vals: torch.Tensor, bits: int = 32, stream=None):
+    n = keys.numel()
+    ko = torch.empty_like(keys)
+    vo = torch.empty_like(vals)
+    L.check(L.lib().drb_radix_sort_pairs(_ptr(keys), _ptr(vals), _ptr(ko), _ptr(vo), n, bits,
+                                         _stream(stream)), "drb_radix_sort_pairs")
+    return ko, vo

@@ -1,0 +1,45 @@
+// Error reporting and small shared helpers of the C-ABI (include/drb.h).
+#include "drb_internal.h"
+
+#include <cstdio>
+#include <cstring>
+#include <string>
+
+namespace drb
+{
+namespace
+{
+thread_local std::string g_last_error;
+}
+
+void set_last_error (const char *msg) { g_last_error = msg ? msg : ""; }
+
+int check_launch (const char *what)
+{
+  const cudaError_t e = cudaGetLastError ();
+  if (e == cudaSuccess) return DRB_OK;
+  char buf[512];
+  std::snprintf (buf, sizeof (buf), "%s: %s", what, cudaGetErrorString (e));
+  set_last_error (buf);
+  return status_from (e);
+}
+
+int sm_count ()
+{
+  static int cached = 0;
+  if (cached == 0)
+  {
+    int dev = 0;
+    cudaGetDevice (&dev);
+    int v = 0;
+    cudaDeviceGetAttribute (&v, cudaDevAttrMultiProcessorCount, dev);
+    cached = v > 0 ? v : 148;
+  }
+  return cached;
+}
+
+} // namespace drb
+
+extern "C" const char *drb_last_error (void) { return drb::g_last_error.c_str (); }
+
+extern "C" int drb_version (void) { return 1; }

@@ -1,0 +1,56 @@
+// Internal host-side declarations shared by the CUDA translation units of
+// libdrb.  Not part of the public C-ABI (include/drb.h is).
+#pragma once
+
+#include "../../include/drb.h"
+#include <cuda_runtime.h>
+#include <cstddef>
+
+namespace drb
+{
+
+// Stream-ordered scratch allocation; all scratch is freed before a public
+// entry point returns (stream-ordered, so no synchronisation is implied).
+struct Scratch
+{
+  cudaStream_t stream;
+  void *ptrs[32];
+  int n = 0;
+  cudaError_t err = cudaSuccess;
+  explicit Scratch (cudaStream_t s) : stream (s) {}
+  template <typename T> T *alloc (size_t count)
+  {
+    if (err != cudaSuccess || n >= 32) return nullptr;
+    void *p = nullptr;
+    err = cudaMallocAsync (&p, count * sizeof (T) + 16, stream);
+    if (err != cudaSuccess) return nullptr;
+    ptrs[n++] = p;
+    return static_cast<T *> (p);
+  }
+  ~Scratch ()
+  {
+    for (int i = 0; i < n; ++i) cudaFreeAsync (ptrs[i], stream);
+  }
+};
+
+inline int status_from (cudaError_t e)
+{
+  if (e == cudaSuccess) return DRB_OK;
+  if (e == cudaErrorMemoryAllocation) return DRB_ERR_OOM;
+  return DRB_ERR_CUDA;
+}
+
+void set_last_error (const char *msg);
+int check_launch (const char *what);
+
+// radix sort of (key, value) pairs on the low `bits` bits of the keys
+int radix_sort_pairs (const unsigned *keys_in, const int *vals_in, unsigned *keys_out,
+                      int *vals_out, int n, int bits, cudaStream_t stream);
+// exclusive prefix sum of n int32 values (in may equal out); total -> *d_total if non-null
+int exclusive_scan_i32 (const int *in, int *out, int n, int *d_total, cudaStream_t stream);
+
+inline int div_up (long long a, long long b) { return (int)((a + b - 1) / b); }
+
+int sm_count ();
+
+} // namespace drb

@@ -1,0 +1,123 @@
+// Newton inversion of tensor Bernstein elements and BVH point queries.
+//
+//   hex_newton   InvertibleElement_impl::eval_inverse_local with
+//                IterativeMethod::solve (data_model/element.hpp:435-486,
+//                newton_solver.hpp:33-74): clamp x to [0,1], eval_d, LUP-solve
+//                J dx = target - X(x), x += dx; converged when the inf-norm of
+//                the change from the previous (unclamped) iterate is < tol;
+//                accept only if converged and is_inside(x, tol)
+//                (pos_tensor_element.tcc:49-61).  tol and max_steps are
+//                parameters (the reference fixes 1e-4 and 20).
+//   Element access goes through a functor cp(i, k) so the same solver runs on
+//   register-resident control points (orders 1-2) or L1-resident packed rows.
+#pragma once
+
+#include "bernstein.cuh"
+#include "drb_common.cuh"
+
+namespace drb
+{
+
+DRB_D bool is_inside_ref (const float (&x)[3], float eps)
+{
+  float mn = 2.f, mx = -1.f;
+#pragma unroll
+  for (int d = 0; d < 3; ++d)
+  {
+    mn = fminf (x[d], mn);
+    mx = fmaxf (x[d], mx);
+  }
+  return (mn >= 0.f - eps) && (mx <= 1.f + eps);
+}
+
+// Vec::Normlinf (vec.hpp:229-238): fmaxf-based, so a NaN component is skipped.
+DRB_D float norm_linf3 (float a, float b, float c)
+{
+  float m = fmaxf (-a, a);
+  m = fmaxf (m, fmaxf (-b, b));
+  m = fmaxf (m, fmaxf (-c, c));
+  return m;
+}
+
+template <int P, class CP>
+DRB_D bool hex_newton (const CP &cp, const float (&target)[3], float (&x)[3], float tol,
+                       int max_steps, int &steps)
+{
+  float prev[3] = { x[0], x[1], x[2] };
+  bool converged = false;
+  steps = 0;
+  while (steps < max_steps && !converged)
+  {
+#pragma unroll
+    for (int d = 0; d < 3; ++d) x[d] = fminf (1.f, fmaxf (x[d], 0.f));
+    float X[3], Ju[3], Jv[3], Jw[3];
+    hex_eval_d<P, 3> (cp, x[0], x[1], x[2], X, Ju, Jv, Jw);
+    float dy[3], J[3][3], dx[3];
+#pragma unroll
+    for (int r = 0; r < 3; ++r)
+    {
+      dy[r] = target[r] - X[r];
+      J[r][0] = Ju[r];
+      J[r][1] = Jv[r];
+      J[r][2] = Jw[r];
+    }
+    LU3 lu;
+    lu.factor (J);
+    lu.solve (dy, dx);
+#pragma unroll
+    for (int d = 0; d < 3; ++d) x[d] += dx[d];
+    ++steps;
+    const float res = norm_linf3 (x[0] - prev[0], x[1] - prev[1], x[2] - prev[2]);
+    converged = res < tol;
+#pragma unroll
+    for (int d = 0; d < 3; ++d) prev[d] = x[d];
+  }
+  return converged && is_inside_ref (x, tol);
+}
+
+// Control points of one element read through the packed element-major copy.
+struct PackedCP
+{
+  const float *__restrict__ p;
+  DRB_D float operator() (int i, int k) const { return __ldg (p + 3 * i + k); }
+};
+
+// Control points of one element read through the reference's double
+// indirection val[ctrl_idx[e*nd+i]] (data_model/dof_access.hpp:23-54).
+struct IndirectCP
+{
+  const int *__restrict__ idx;
+  const float *__restrict__ val;
+  int ncomp;
+  DRB_D float operator() (int i, int k) const
+  {
+    return __ldg (val + (size_t)ncomp * __ldg (idx + i) + k);
+  }
+};
+
+// Register-resident copy of an element (orders 1-2: 24 or 81 floats).
+template <int N> struct RegCP
+{
+  float v[N];
+  DRB_D float operator() (int i, int k) const { return v[3 * i + k]; }
+};
+
+template <int P> DRB_D void load_reg_cp (RegCP<3 * (P + 1) * (P + 1) * (P + 1)> &r, const float *p)
+{
+  constexpr int N = 3 * (P + 1) * (P + 1) * (P + 1);
+  // packed rows start on a float4 boundary (drb_packed_stride)
+  const float4 *p4 = reinterpret_cast<const float4 *> (p);
+#pragma unroll
+  for (int q = 0; q < N / 4; ++q)
+  {
+    const float4 t = __ldg (p4 + q);
+    r.v[4 * q] = t.x;
+    r.v[4 * q + 1] = t.y;
+    r.v[4 * q + 2] = t.z;
+    r.v[4 * q + 3] = t.w;
+  }
+#pragma unroll
+  for (int q = (N / 4) * 4; q < N; ++q) r.v[q] = __ldg (p + q);
+}
+
+} // namespace drb

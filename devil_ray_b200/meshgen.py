@@ -1,0 +1,191 @@
+"""Seeded synthetic Bernstein hex meshes and query sets for the benchmark
+workloads.
+
+Lattice convention (the reference's synthetic generators,
+synthetic/affine_radial.cpp:124-139,193-240): a mesh of n^3 elements of
+order p shares one lattice of (p*n+1)^3 control points, point (I,J,K) at
+flat index (K*(p*n+1)+J)*(p*n+1)+I; element (ei,ej,ek) has id
+(ek*n+ej)*n+ei and its dof (a,b,c) (u fastest) is lattice point
+(p*ei+a, p*ej+b, p*ek+c).  The same ctrl_idx serves the geometry and the
+scalar field.
+
+Workloads (sizes and distributions; all randomness from numpy PCG64 with a
+recorded seed):
+  volume_8     8^3 hex P2, interior points displaced by
+               0.05*sin(2pi x)sin(2pi y)sin(2pi z) on every axis,
+               f = sin(3x)cos(2y)+z^2 at the displaced control point
+  surface_32   32^3 hex P3, same warp with amplitude 0.08 plus uniform +-0.01
+               jitter per interior control point
+  locate_64    64^3 hex P2 whose geometry is exactly trilinear per element:
+               the vertex lattice is displaced by uniform offsets up to
+               `distortion` x h (boundary vertices keep their normal
+               coordinate) and the P2 control points interpolate the
+               element corners
+  volume_128   128^3 hex P3, warp 0.05, f = sum of 8 seeded Gaussians
+               (sigma 0.1)
+"""
+from __future__ import annotations
+
+from dataclasses import dataclass, field
+
+import numpy as np
+
+TWO_PI = 2.0 * np.pi
+
+
+@dataclass
+class HexMeshData:
+    order: int
+    n: int                      # elements per axis
+    ctrl_idx: np.ndarray        # int32 [n_elem * (p+1)^3]
+    xyz: np.ndarray             # float32 [n_ctrl, 3]
+    field: np.ndarray           # float32 [n_ctrl]
+    meta: dict = field(default_factory=dict)
+
+    @property
+    def n_elem(self) -> int:
+        return self.n ** 3
+
+    @property
+    def n_ctrl(self) -> int:
+        return self.xyz.shape[0]
+
+    @property
+    def nd(self) -> int:
+        return (self.order + 1) ** 3
+
+
+def lattice_ctrl_idx(n: int, p: int) -> np.ndarray:
+    """ctrl_idx of an n^3 order-p hex lattice mesh (element-major, u fastest)."""
+    m = p * n + 1
+    e = np.arange(n, dtype=np.int64)
+    a = np.arange(p + 1, dtype=np.int64)
+    # element (ek, ej, ei), dof (c, b, a) -> lattice (p*ek+c, p*ej+b, p*ei+a)
+    K = (p * e[:, None, None, None, None, None] + a[None, None, None, :, None, None])
+    J = (p * e[None, :, None, None, None, None] + a[None, None, None, None, :, None])
+    I = (p * e[None, None, :, None, None, None] + a[None, None, None, None, None, :])
+    idx = (K * m + J) * m + I
+    return idx.reshape(-1).astype(np.int32)
+
+
+def lattice_points(n: int, p: int) -> np.ndarray:
+    """Undisplaced lattice coordinates in [0,1]^3, float64 [m^3, 3]."""
+    m = p * n + 1
+    t = np.linspace(0.0, 1.0, m)
+    Z, Y, X = np.meshgrid(t, t, t, indexing="ij")
+    return np.stack([X.ravel(), Y.ravel(), Z.ravel()], axis=1)
+
+
+def interior_mask(n: int, p: int) -> np.ndarray:
+    m = p * n + 1
+    i = np.arange(m)
+    inner = (i > 0) & (i < m - 1)
+    Z, Y, X = np.meshgrid(inner, inner, inner, indexing="ij")
+    return (X & Y & Z).ravel()
+
+
+def field_sincos(xyz: np.ndarray) -> np.ndarray:
+    x, y, z = xyz[:, 0], xyz[:, 1], xyz[:, 2]
+    return np.sin(3.0 * x) * np.cos(2.0 * y) + z * z
+
+
+def field_gaussians(xyz: np.ndarray, seed: int, count: int = 8, sigma: float = 0.1):
+    rng = np.random.default_rng(seed)
+    centres = rng.uniform(0.15, 0.85, size=(count, 3))
+    amps = rng.uniform(0.5, 1.0, size=count)
+    f = np.zeros(xyz.shape[0], dtype=np.float64)
+    for c, a in zip(centres, amps):
+        d2 = ((xyz - c) ** 2).sum(axis=1)
+        f += a * np.exp(-d2 / (2.0 * sigma * sigma))
+    return f, centres, amps
+
+
+def warped_mesh(n: int, p: int, amp: float, jitter: float = 0.0, seed: int = 0,
+                gaussian_field_seed: int | None = None) -> HexMeshData:
+    base = lattice_points(n, p)
+    inner = interior_mask(n, p)
+    s = np.sin(TWO_PI * base[:, 0]) * np.sin(TWO_PI * base[:, 1]) * np.sin(TWO_PI * base[:, 2])
+    disp = amp * s
+    xyz = base.copy()
+    xyz[inner] += disp[inner, None]
+    if jitter > 0.0:
+        rng = np.random.default_rng(seed)
+        j = rng.uniform(-jitter, jitter, size=(int(inner.sum()), 3))
+        xyz[inner] += j
+    meta = {"warp_amplitude": amp, "jitter": jitter, "seed": seed}
+    if gaussian_field_seed is None:
+        f = field_sincos(xyz)
+        meta["field"] = "sin(3x)cos(2y)+z^2"
+    else:
+        f, c, a = field_gaussians(xyz, gaussian_field_seed)
+        meta["field"] = "8 gaussians sigma 0.1"
+        meta["field_seed"] = gaussian_field_seed
+    return HexMeshData(order=p, n=n, ctrl_idx=lattice_ctrl_idx(n, p),
+                       xyz=xyz.astype(np.float32), field=f.astype(np.float32), meta=meta)
+
+
+def trilinear_distorted_mesh(n: int, p: int, distortion: float, seed: int) -> HexMeshData:
+    """Order-p mesh whose elements are trilinear maps of a randomly displaced
+    vertex lattice (offsets uniform in [-distortion*h, distortion*h] per axis,
+    boundary vertices keep the coordinate normal to their boundary plane)."""
+    h = 1.0 / n
+    t = np.linspace(0.0, 1.0, n + 1)
+    Z, Y, X = np.meshgrid(t, t, t, indexing="ij")
+    verts = np.stack([X, Y, Z], axis=-1)           # [k, j, i, 3]
+    rng = np.random.default_rng(seed)
+    off = rng.uniform(-distortion * h, distortion * h, size=verts.shape)
+    idx = np.arange(n + 1)
+    on_b = (idx == 0) | (idx == n)
+    off[..., 0] *= ~on_b[None, None, :]
+    off[..., 1] *= ~on_b[None, :, None]
+    off[..., 2] *= ~on_b[:, None, None]
+    verts = verts + off
+    m = p * n + 1
+    L = np.arange(m)
+    e = np.minimum(L // p, n - 1)
+    u = (L - p * e) / p                             # 0, 1/p, ..., 1
+    ek, ej, ei = np.meshgrid(e, e, e, indexing="ij")
+    w, v, uu = np.meshgrid(u, u, u, indexing="ij")
+    xyz = np.zeros((m, m, m, 3))
+    for c in range(2):
+        for b in range(2):
+            for a in range(2):
+                wt = ((uu if a else 1 - uu) * (v if b else 1 - v) * (w if c else 1 - w))
+                xyz += wt[..., None] * verts[ek + c, ej + b, ei + a]
+    xyz = xyz.reshape(-1, 3)
+    f = field_sincos(xyz)
+    meta = {"distortion": distortion, "seed": seed, "field": "sin(3x)cos(2y)+z^2"}
+    return HexMeshData(order=p, n=n, ctrl_idx=lattice_ctrl_idx(n, p),
+                       xyz=xyz.astype(np.float32), field=f.astype(np.float32), meta=meta)
+
+
+# outside fraction of uniform queries: the meshes fill [0,1]^3, so queries are
+# drawn from a cube padded so that about 8% of its volume lies outside
+OUTSIDE_FRACTION = 0.08
+QUERY_PAD = ((1.0 / (1.0 - OUTSIDE_FRACTION)) ** (1.0 / 3.0) - 1.0) / 2.0
+
+
+def uniform_queries(count: int, seed: int, pad: float = QUERY_PAD) -> np.ndarray:
+    rng = np.random.default_rng(seed)
+    return rng.uniform(-pad, 1.0 + pad, size=(count, 3)).astype(np.float32)
+
+
+def workload_mesh(name: str) -> HexMeshData:
+    if name == "volume_8":
+        return warped_mesh(8, 2, 0.05)
+    if name == "surface_32":
+        return warped_mesh(32, 3, 0.08, jitter=0.01, seed=1)
+    if name == "locate_64":
+        return trilinear_distorted_mesh(64, 2, 0.15, seed=2)
+    if name == "locate_64_d25":
+        return trilinear_distorted_mesh(64, 2, 0.25, seed=3)
+    if name == "volume_128":
+        return warped_mesh(128, 3, 0.05, gaussian_field_seed=4)
+    raise KeyError(name)
+
+
+# Camera and transfer function of the volume/surface workloads
+CAMERA = {"pos": (2.5, 2.5, 2.5), "look_at": (0.5, 0.5, 0.5), "up": (0.0, 1.0, 0.0),
+          "fov": 30.0}
+TF_RGB = [(0.0, 0.23, 0.30, 0.75), (1.0, 0.71, 0.02, 0.15)]   # (pos, r, g, b)
+TF_ALPHA = [(0.0, 0.05), (1.0, 0.9)]                            # (pos, alpha)

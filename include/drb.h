@@ -1,0 +1,150 @@
+/*
+ * drb.h - C-ABI of the B200-native (sm_100a) ray-element hot path.
+ *
+ * Plain C types, device pointers and sizes; no C++ or torch types.  Every
+ * entry point takes a cudaStream_t (as void*, NULL = legacy default stream),
+ * enqueues its work on it and returns a drb_status.  Buffers named "device"
+ * must be device-accessible; "host" buffers are read or written on the host
+ * after the stream has been synchronised by the call where noted.
+ *
+ * Each entry point names the reference interface (Devil Ray, src/dray/...)
+ * whose behaviour it replaces.
+ */
+#ifndef DRB_H
+#define DRB_H
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* Status codes.  The reference throws dray::DRayError (error.hpp:41-49) on
+ * host-side misuse and only prints device errors (error_check.hpp:17-28);
+ * here every failure is returned, with a message in drb_last_error(). */
+enum drb_status
+{
+  DRB_OK = 0,
+  DRB_ERR_INVALID_ARG = 1,
+  DRB_ERR_OOM = 2,
+  DRB_ERR_CUDA = 3,
+  DRB_ERR_QUEUE_GIVEUP = 4, /* a bounded device-side wait ran out */
+  DRB_ERR_UNSUPPORTED = 5
+};
+
+/* Initial guess for the per-candidate Newton solve of point location. */
+enum drb_guess_mode
+{
+  /* (0,0,0): the reference as compiled with zero-initialised locals; its
+   * DeviceMesh::locate passes use_init_guess=true with an uninitialised
+   * guess (data_model/device_mesh.hpp:327-334). */
+  DRB_GUESS_ZERO = 0,
+  /* element centre (0.5,0.5,0.5): the plain GPU path. */
+  DRB_GUESS_ELEM_CENTER = 1,
+  /* centre of the candidate leaf's reference sub-box, the reference's
+   * intended guess (device_mesh.hpp:161-162). */
+  DRB_GUESS_SUBREF_CENTER = 2,
+  /* caller-provided guess per point for its first candidate element (e.g.
+   * the learned guess), element centre for later candidates and as the
+   * fallback when the guessed solve does not converge. */
+  DRB_GUESS_GIVEN = 3
+};
+
+/* A tensor-product Bernstein mesh or field: GridFunction<ncomp> of the
+ * reference (data_model/grid_function.hpp:19-30).  dim 3 = hex, dim 2 = quad. */
+typedef struct drb_mesh
+{
+  int dim;               /* 3 hex, 2 quad */
+  int order;             /* polynomial order 1..3 */
+  int ncomp;             /* 3 geometry, 1 scalar field */
+  int n_elem;
+  int n_ctrl;
+  const int *ctrl_idx;   /* device int32[n_elem * (order+1)^dim] */
+  const float *values;   /* device float[n_ctrl * ncomp] */
+  const float *packed;   /* optional device float[n_elem * drb_packed_stride()]:
+                            element-major copy made by drb_pack_elements(), or NULL */
+} drb_mesh;
+
+/* Linear BVH in the reference's layout (bvh.hpp:16-37, device_bvh.hpp:15-28). */
+typedef struct drb_bvh
+{
+  int n_inner;           /* n_leaf - 1 */
+  int n_leaf;
+  float *inner_nodes;    /* device float[16 * n_inner]: 4 x float4 per node */
+  int *leaf_nodes;       /* device int32[n_leaf]: element id per sorted leaf */
+  int *aabb_ids;         /* device int32[n_leaf]: sub-box id per sorted leaf */
+  float *ref_boxes;      /* device float[n_leaf * 2 * dim]: reference sub-box per sub-box id */
+  float bounds[6];       /* host: xmin,xmax,ymin,ymax,zmin,zmax (filled by the build) */
+} drb_bvh;
+
+/* Newton options.  The reference hard-codes tol 1e-4 and 20 steps for
+ * volume elements (data_model/element.hpp:474-475), 1e-4 and 10 steps for
+ * ray-face solves (face_intersection.hpp:153-154). */
+typedef struct drb_newton_opts
+{
+  float tol;             /* reference-space step tolerance, also is_inside eps */
+  int max_steps;
+  int guess_mode;        /* enum drb_guess_mode */
+  const float *guess;    /* device float[3*n] for DRB_GUESS_GIVEN, else NULL */
+} drb_newton_opts;
+
+/* Per-query statistics (utils/appstats.hpp:18-63 counts the same things). */
+typedef struct drb_query_stats
+{
+  int *iters;            /* device int32[n]: Newton iterations summed over candidates, or NULL */
+  int *candidates;       /* device int32[n]: leaves whose box held the query, or NULL */
+} drb_query_stats;
+
+const char *drb_last_error (void);
+int drb_version (void);
+
+/* Floats per element in a packed element-major copy (padded to float4). */
+int drb_packed_stride (int dim, int order, int ncomp);
+
+/* Gather the element control points into an element-major array
+ * (replaces the double indirection val[ctrl_idx[e*nd+i]] of SharedDofPtr,
+ * data_model/dof_access.hpp:23-54). */
+int drb_pack_elements (const drb_mesh *mesh, float *packed, void *stream);
+
+/* Sizes of the BVH over a mesh's sub-boxes: 33 per hex, 17 per quad
+ * (construct_bvh, data_model/mesh_utils.cpp:527-531). */
+int drb_bvh_sizes (int dim, int n_elem, int *n_inner, int *n_leaf);
+
+/* Per-element sub-box split (the forall of detail::construct_bvh,
+ * data_model/mesh_utils.cpp:557-670): 32 (hex) / 16 (quad) de Casteljau
+ * splits of the largest box, convex-hull AABBs scaled by 1.000001.
+ * Outputs per sub-box (element-major, e*(splits+1)+i): aabbs6 device
+ * float[6*n], prim_ids device int32[n], ref_boxes device float[2*dim*n];
+ * bounds6 device float[6] receives the reduction of linear_bvh_builder.cpp:19-58. */
+int drb_elem_subboxes (const drb_mesh *mesh, float *aabbs6, int *prim_ids, float *ref_boxes,
+                       float *bounds6, void *stream);
+
+/* 30-bit Morton codes of AABB centroids (get_mcodes + morton_3d,
+ * linear_bvh_builder.cpp:60-90, morton_codes.hpp:39-53). */
+int drb_morton_codes (const float *aabbs6, int n, const float *bounds6, unsigned *codes,
+                      void *stream);
+
+/* Stable LSD radix sort of (key, value) pairs on the low `bits` key bits
+ * (replaces the host std::sort of sort_mcodes, linear_bvh_builder.cpp:120-135). */
+int drb_radix_sort_pairs (const unsigned *keys_in, const int *vals_in, unsigned *keys_out,
+                          int *vals_out, int n, int bits, void *stream);
+
+/* Full BVH over a mesh: detail::construct_bvh + LinearBVHBuilder::construct
+ * (mesh_utils.cpp:514-677, linear_bvh_builder.cpp:399-518).  bvh arrays are
+ * caller-allocated with drb_bvh_sizes(); sorted_codes (device uint32[n_leaf])
+ * optionally receives the sorted Morton codes.  Synchronises the stream to
+ * fill bvh->bounds. */
+int drb_lbvh_build (const drb_mesh *mesh, drb_bvh *bvh, unsigned *sorted_codes, void *stream);
+
+/* Point location: Mesh::locate (data_model/unstructured_mesh.cpp:124-148,
+ * DeviceMesh::locate device_mesh.hpp:248-354).  One thread per point, BVH
+ * traversal left child first, first leaf whose Newton solve converges and is
+ * inside wins.  pts device float[3n]; cell device int32[n] (-1 = not found);
+ * ref device float[3n] (-1 for misses). */
+int drb_locate (const drb_mesh *mesh, const drb_bvh *bvh, const float *pts, int n,
+                const drb_newton_opts *opts, int *cell, float *ref, drb_query_stats stats,
+                void *stream);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* DRB_H */

@@ -1,0 +1,551 @@
+// Test oracle: a thin extern "C" driver over the reference's own C++ classes
+// (Devil Ray, compiled from its sources against the host-only shims in
+// oracle/shims).  It is test infrastructure: tests, smoke() and the bench's
+// CPU-baseline leg call it to obtain the reference's results; the product
+// never links it.
+//
+// Every entry point drives the reference through its public API:
+//   UnstructuredMesh<E>(GridFunction<3>, order)        data_model/unstructured_mesh.cpp:34
+//   UnstructuredMesh::get_bvh / get_ref_aabbs           data_model/unstructured_mesh.cpp:23, .hpp:109
+//   UnstructuredMesh::locate                            data_model/unstructured_mesh.cpp:124
+//   get_mcodes / reduce (LBVH internals, non-static)    linear_bvh_builder.cpp:19,60
+//   Camera::create_rays                                 rendering/camera.cpp:219
+//   Volume::integrate + the host compositing loop of
+//   Volume::save                                        rendering/volume.cpp:324,369
+//   MeshBoundary::execute                               filters/mesh_boundary.cpp:339
+//   Surface::nearest_hit / fragments / shade            rendering/surface.cpp:497, traceable.cpp
+//   Framebuffer::clear / composite_background           rendering/framebuffer.cpp:126,146
+#include <dray/aabb.hpp>
+#include <dray/array.hpp>
+#include <dray/bvh.hpp>
+#include <dray/color_map.hpp>
+#include <dray/color_table.hpp>
+#include <dray/data_model/collection.hpp>
+#include <dray/data_model/element.hpp>
+#include <dray/data_model/dof_access.hpp>
+#include <dray/data_model/data_set.hpp>
+#include <dray/data_model/grid_function.hpp>
+#include <dray/data_model/unstructured_field.hpp>
+#include <dray/data_model/unstructured_mesh.hpp>
+#include <dray/filters/mesh_boundary.hpp>
+#include <dray/location.hpp>
+#include <dray/ray.hpp>
+#include <dray/ray_hit.hpp>
+#include <dray/rendering/camera.hpp>
+#include <dray/rendering/colors.hpp>
+#include <dray/rendering/fragment.hpp>
+#include <dray/rendering/framebuffer.hpp>
+#include <dray/rendering/point_light.hpp>
+#include <dray/rendering/surface.hpp>
+#include <dray/rendering/volume.hpp>
+#include <dray/rendering/volume_partial.hpp>
+
+#include <cstring>
+#include <exception>
+#include <memory>
+#include <string>
+#include <vector>
+#ifdef _OPENMP
+#include <omp.h>
+#endif
+
+namespace dray
+{
+// Free functions of linear_bvh_builder.cpp (external linkage there).
+AABB<> reduce (const Array<AABB<>> &aabbs);
+Array<uint32> get_mcodes (Array<AABB<>> &aabbs, const AABB<> &bounds);
+} // namespace dray
+
+using namespace dray;
+
+namespace
+{
+struct RefMesh
+{
+  int order = 0;
+  std::shared_ptr<Mesh> mesh;
+  Collection collection;
+  bool has_field = false;
+};
+
+GridFunction<3> make_gf3 (int n_el, int nd, const int *idx, int n_ctrl, const float *xyz)
+{
+  GridFunction<3> gf;
+  gf.resize (n_el, nd, n_ctrl);
+  std::memcpy (gf.m_ctrl_idx.get_host_ptr (), idx, sizeof (int) * (size_t)n_el * nd);
+  std::memcpy ((void *)gf.m_values.get_host_ptr (), xyz, sizeof (float) * 3 * (size_t)n_ctrl);
+  return gf;
+}
+
+GridFunction<1> make_gf1 (int n_el, int nd, const int *idx, int n_ctrl, const float *vals)
+{
+  GridFunction<1> gf;
+  gf.resize (n_el, nd, n_ctrl);
+  std::memcpy (gf.m_ctrl_idx.get_host_ptr (), idx, sizeof (int) * (size_t)n_el * nd);
+  std::memcpy ((void *)gf.m_values.get_host_ptr (), vals, sizeof (float) * (size_t)n_ctrl);
+  return gf;
+}
+
+std::shared_ptr<Mesh> make_hex_mesh (int order, const GridFunction<3> &gf)
+{
+  if (order == 1) return std::make_shared<HexMesh_P1> (gf, 1);
+  if (order == 2) return std::make_shared<HexMesh_P2> (gf, 2);
+  return std::make_shared<HexMesh> (gf, order);
+}
+
+std::shared_ptr<Field> make_hex_field (int order, const GridFunction<1> &gf, const char *name)
+{
+  if (order == 1)
+    return std::make_shared<UnstructuredField<HexScalar_P1>> (gf, 1, name);
+  if (order == 2)
+    return std::make_shared<UnstructuredField<HexScalar_P2>> (gf, 2, name);
+  return std::make_shared<UnstructuredField<HexScalar>> (gf, order, name);
+}
+
+template <typename MeshT> BVH bvh_of (Mesh *m)
+{
+  return dynamic_cast<MeshT *> (m)->get_bvh ();
+}
+
+BVH get_bvh_any (Mesh *m)
+{
+  if (auto *p = dynamic_cast<HexMesh_P1 *> (m)) return p->get_bvh ();
+  if (auto *p = dynamic_cast<HexMesh_P2 *> (m)) return p->get_bvh ();
+  if (auto *p = dynamic_cast<HexMesh *> (m)) return p->get_bvh ();
+  if (auto *p = dynamic_cast<QuadMesh_P1 *> (m)) return p->get_bvh ();
+  if (auto *p = dynamic_cast<QuadMesh_P2 *> (m)) return p->get_bvh ();
+  if (auto *p = dynamic_cast<QuadMesh *> (m)) return p->get_bvh ();
+  throw std::runtime_error ("unsupported mesh type");
+}
+
+// Reference boxes are SubRef<dim,Tensor>: two corners of dim floats.
+int copy_ref_boxes (Mesh *m, float *out)
+{
+  if (auto *p = dynamic_cast<HexMesh_P1 *> (m))
+  { auto a = p->get_ref_aabbs (); std::memcpy (out, (const void *)a.get_host_ptr_const (), a.size () * 24); return 3; }
+  if (auto *p = dynamic_cast<HexMesh_P2 *> (m))
+  { auto a = p->get_ref_aabbs (); std::memcpy (out, (const void *)a.get_host_ptr_const (), a.size () * 24); return 3; }
+  if (auto *p = dynamic_cast<HexMesh *> (m))
+  { auto a = p->get_ref_aabbs (); std::memcpy (out, (const void *)a.get_host_ptr_const (), a.size () * 24); return 3; }
+  if (auto *p = dynamic_cast<QuadMesh_P1 *> (m))
+  { auto a = p->get_ref_aabbs (); std::memcpy (out, (const void *)a.get_host_ptr_const (), a.size () * 16); return 2; }
+  if (auto *p = dynamic_cast<QuadMesh_P2 *> (m))
+  { auto a = p->get_ref_aabbs (); std::memcpy (out, (const void *)a.get_host_ptr_const (), a.size () * 16); return 2; }
+  if (auto *p = dynamic_cast<QuadMesh *> (m))
+  { auto a = p->get_ref_aabbs (); std::memcpy (out, (const void *)a.get_host_ptr_const (), a.size () * 16); return 2; }
+  return 0;
+}
+
+thread_local std::string g_err;
+
+ColorTable make_table (int n_rgb, const float *rgb_pts, int n_alpha, const float *alpha_pts)
+{
+  // rgb_pts: n_rgb x (pos, r, g, b); alpha_pts: n_alpha x (pos, a)
+  ColorTable t;
+  t.set_smooth (true);
+  for (int i = 0; i < n_rgb; ++i)
+    t.add_point (rgb_pts[4 * i], make_vec3f (rgb_pts[4 * i + 1], rgb_pts[4 * i + 2], rgb_pts[4 * i + 3]));
+  for (int i = 0; i < n_alpha; ++i) t.add_alpha (alpha_pts[2 * i], alpha_pts[2 * i + 1]);
+  return t;
+}
+
+void setup_camera (Camera &cam, int w, int h, const float *cam9, float fov)
+{
+  cam.set_width (w);
+  cam.set_height (h);
+  cam.set_pos (make_vec3f (cam9[0], cam9[1], cam9[2]));
+  cam.set_look_at (make_vec3f (cam9[3], cam9[4], cam9[5]));
+  cam.set_up (make_vec3f (cam9[6], cam9[7], cam9[8]));
+  cam.set_fov (fov);
+}
+
+Array<PointLight> make_lights (int n, const float *l13)
+{
+  // l13: n x (pos3, amb3, diff3, spec3, spec_pow)
+  Array<PointLight> lights;
+  lights.resize (n);
+  PointLight *lp = lights.get_host_ptr ();
+  for (int i = 0; i < n; ++i)
+  {
+    const float *s = l13 + 13 * i;
+    lp[i].m_pos = make_vec3f (s[0], s[1], s[2]);
+    lp[i].m_amb = make_vec3f (s[3], s[4], s[5]);
+    lp[i].m_diff = make_vec3f (s[6], s[7], s[8]);
+    lp[i].m_spec = make_vec3f (s[9], s[10], s[11]);
+    lp[i].m_spec_pow = s[12];
+  }
+  return lights;
+}
+} // namespace
+
+extern "C" {
+
+const char *ref_last_error () { return g_err.c_str (); }
+
+int ref_num_threads ()
+{
+#ifdef _OPENMP
+  return omp_get_max_threads ();
+#else
+  return 1;
+#endif
+}
+
+void ref_set_num_threads (int n)
+{
+#ifdef _OPENMP
+  if (n > 0) omp_set_num_threads (n);
+#else
+  (void)n;
+#endif
+}
+
+// Create a hex mesh of polynomial order `order` (element type chosen as the
+// reference's dispatcher does: fixed-order P1/P2 specialisations, General
+// otherwise) plus an optional scalar field named "f" on the same layout.
+void *ref_hex_create (int order, int n_el, const int *ctrl_idx, int n_ctrl, const float *xyz,
+                      const int *field_idx, int n_field_ctrl, const float *field_vals)
+{
+  try
+  {
+    const int nd = (order + 1) * (order + 1) * (order + 1);
+    RefMesh *r = new RefMesh ();
+    r->order = order;
+    r->mesh = make_hex_mesh (order, make_gf3 (n_el, nd, ctrl_idx, n_ctrl, xyz));
+    DataSet ds (r->mesh);
+    if (field_vals != nullptr)
+    {
+      ds.add_field (make_hex_field (order, make_gf1 (n_el, nd, field_idx, n_field_ctrl, field_vals), "f"));
+      r->has_field = true;
+    }
+    r->collection.add_domain (ds);
+    return r;
+  }
+  catch (const std::exception &e)
+  {
+    g_err = e.what ();
+    return nullptr;
+  }
+}
+
+void ref_free (void *h) { delete static_cast<RefMesh *> (h); }
+
+// Builds (if needed) the mesh BVH and reports its sizes.
+int ref_bvh_sizes (void *h, int *n_inner, int *n_leaf)
+{
+  try
+  {
+    RefMesh *r = static_cast<RefMesh *> (h);
+    BVH b = get_bvh_any (r->mesh.get ());
+    *n_inner = (int)b.m_inner_nodes.size () / 4;
+    *n_leaf = (int)b.m_leaf_nodes.size ();
+    return 0;
+  }
+  catch (const std::exception &e)
+  {
+    g_err = e.what ();
+    return -1;
+  }
+}
+
+// Copies the BVH: inner nodes (16 floats each), leaf prim ids, aabb ids
+// (sort permutation), bounds (xmin,xmax,ymin,ymax,zmin,zmax) and the
+// per-sub-box reference boxes (2*dim floats each, original sub-box order).
+int ref_bvh_copy (void *h, float *inner, int *leaf_nodes, int *aabb_ids, float *bounds6,
+                  float *ref_boxes)
+{
+  try
+  {
+    RefMesh *r = static_cast<RefMesh *> (h);
+    BVH b = get_bvh_any (r->mesh.get ());
+    std::memcpy (inner, (const void *)b.m_inner_nodes.get_host_ptr_const (),
+                 sizeof (float) * 4 * b.m_inner_nodes.size ());
+    std::memcpy (leaf_nodes, b.m_leaf_nodes.get_host_ptr_const (), sizeof (int) * b.m_leaf_nodes.size ());
+    std::memcpy (aabb_ids, b.m_aabb_ids.get_host_ptr_const (), sizeof (int) * b.m_aabb_ids.size ());
+    for (int d = 0; d < 3; ++d)
+    {
+      bounds6[2 * d] = b.m_bounds.m_ranges[d].min ();
+      bounds6[2 * d + 1] = b.m_bounds.m_ranges[d].max ();
+    }
+    if (ref_boxes) copy_ref_boxes (r->mesh.get (), ref_boxes);
+    return 0;
+  }
+  catch (const std::exception &e)
+  {
+    g_err = e.what ();
+    return -1;
+  }
+}
+
+// Reference Morton codes and scene bounds for a list of AABBs given as
+// (xmin,xmax,ymin,ymax,zmin,zmax) records.
+void ref_morton (int n, const float *aabbs6, unsigned *codes, float *bounds6)
+{
+  Array<AABB<>> boxes;
+  boxes.resize (n);
+  std::memcpy ((void *)boxes.get_host_ptr (), aabbs6, sizeof (float) * 6 * (size_t)n);
+  AABB<> bounds = reduce (boxes);
+  Array<uint32> m = get_mcodes (boxes, bounds);
+  std::memcpy (codes, m.get_host_ptr_const (), sizeof (unsigned) * (size_t)n);
+  for (int d = 0; d < 3; ++d)
+  {
+    bounds6[2 * d] = bounds.m_ranges[d].min ();
+    bounds6[2 * d + 1] = bounds.m_ranges[d].max ();
+  }
+}
+
+// Mesh::locate: cell id (-1 = not found) and reference coordinates.
+int ref_locate (void *h, int n, const float *pts, int *cell, float *ref3)
+{
+  try
+  {
+    RefMesh *r = static_cast<RefMesh *> (h);
+    Array<Vec<Float, 3>> p;
+    p.resize (n);
+    std::memcpy ((void *)p.get_host_ptr (), pts, sizeof (float) * 3 * (size_t)n);
+    Array<Location> loc = r->mesh->locate (p);
+    const Location *lp = loc.get_host_ptr_const ();
+    for (int i = 0; i < n; ++i)
+    {
+      cell[i] = lp[i].m_cell_id;
+      ref3[3 * i] = lp[i].m_ref_pt[0];
+      ref3[3 * i + 1] = lp[i].m_ref_pt[1];
+      ref3[3 * i + 2] = lp[i].m_ref_pt[2];
+    }
+    return 0;
+  }
+  catch (const std::exception &e)
+  {
+    g_err = e.what ();
+    return -1;
+  }
+}
+
+// Camera::create_rays: rays as (dir3, near, orig3, far, pixel_id) = 9 words.
+int ref_camera_rays (int w, int h, const float *cam9, float fov, float *rays9)
+{
+  try
+  {
+    Camera cam;
+    setup_camera (cam, w, h, cam9, fov);
+    Array<Ray> rays;
+    cam.create_rays (rays);
+    std::memcpy (rays9, (const void *)rays.get_host_ptr_const (), sizeof (Ray) * (size_t)rays.size ());
+    return rays.size ();
+  }
+  catch (const std::exception &e)
+  {
+    g_err = e.what ();
+    return -1;
+  }
+}
+
+// Volume::integrate over camera rays, then the host compositing of
+// Volume::save and Framebuffer::composite_background (white background).
+// Outputs the partial count and, when rgba/partials are non-null, the
+// composited image (w*h*4 floats) and the raw partials (6 words each:
+// pixel, depth, r, g, b, a).
+int ref_volume (void *h, int w, int hgt, const float *cam9, float fov, int samples,
+                int use_lighting, int tf_samples, int n_rgb, const float *rgb_pts, int n_alpha,
+                const float *alpha_pts, int n_lights, const float *lights13, float *rgba,
+                float *partials6, int max_partials)
+{
+  try
+  {
+    RefMesh *r = static_cast<RefMesh *> (h);
+    Camera cam;
+    setup_camera (cam, w, hgt, cam9, fov);
+    Array<Ray> rays;
+    cam.create_rays (rays);
+    Volume vol (r->collection);
+    vol.field ("f");
+    vol.samples (samples);
+    vol.use_lighting (use_lighting != 0);
+    ColorMap &cmap = vol.color_map ();
+    cmap.samples (tf_samples);
+    cmap.color_table (make_table (n_rgb, rgb_pts, n_alpha, alpha_pts));
+    Array<PointLight> lights = make_lights (n_lights, lights13);
+    Array<VolumePartial> partials = vol.integrate (rays, lights);
+
+    const int size = partials.size ();
+    const VolumePartial *pp = partials.get_host_ptr_const ();
+    if (partials6)
+    {
+      for (int i = 0; i < size && i < max_partials; ++i)
+      {
+        partials6[6 * i] = (float)pp[i].m_pixel_id;
+        partials6[6 * i + 1] = pp[i].m_depth;
+        for (int c = 0; c < 4; ++c) partials6[6 * i + 2 + c] = pp[i].m_color[c];
+      }
+    }
+    if (rgba)
+    {
+      Framebuffer fb (w, hgt);
+      fb.clear ();
+      Vec<float32, 4> *color_ptr = fb.colors ().get_host_ptr ();
+      if (size > 0)
+      {
+        Vec<float32, 4> color = pp[0].m_color;
+        int32 current_pixel = -1;
+        for (int i = 0; i < size; ++i)
+        {
+          VolumePartial p = pp[i];
+          if (current_pixel != p.m_pixel_id)
+          {
+            if (current_pixel != -1) color_ptr[current_pixel] = color;
+            color = p.m_color;
+            current_pixel = p.m_pixel_id;
+          }
+          else
+          {
+            pre_mult_alpha_blend_host (color, p.m_color);
+          }
+          if (i == size - 1) color_ptr[current_pixel] = color;
+        }
+      }
+      fb.composite_background ();
+      std::memcpy (rgba, (const void *)fb.colors ().get_host_ptr_const (), sizeof (float) * 4 * (size_t)w * hgt);
+    }
+    return size;
+  }
+  catch (const std::exception &e)
+  {
+    g_err = e.what ();
+    return -1;
+  }
+}
+
+// MeshBoundary::execute: number of boundary faces and their (element,
+// face-id) pairs are not exposed by the reference, so this returns the
+// boundary quad mesh's control-index array (n_faces * (p+1)^2 ints).
+int ref_boundary (void *h, int *face_ctrl_idx, int max_faces)
+{
+  try
+  {
+    RefMesh *r = static_cast<RefMesh *> (h);
+    MeshBoundary mb;
+    Collection out = mb.execute (r->collection);
+    DataSet ds = out.domain (0);
+    Mesh *m = ds.mesh ();
+    GridFunction<3> gf;
+    if (auto *p = dynamic_cast<QuadMesh_P1 *> (m)) gf = p->get_dof_data ();
+    else if (auto *p = dynamic_cast<QuadMesh_P2 *> (m)) gf = p->get_dof_data ();
+    else if (auto *p = dynamic_cast<QuadMesh *> (m)) gf = p->get_dof_data ();
+    else throw std::runtime_error ("boundary: unexpected mesh type");
+    const int nf = gf.get_num_elem ();
+    if (face_ctrl_idx && nf <= max_faces)
+      std::memcpy (face_ctrl_idx, gf.m_ctrl_idx.get_host_ptr_const (), sizeof (int) * (size_t)gf.m_ctrl_idx.size ());
+    return nf;
+  }
+  catch (const std::exception &e)
+  {
+    g_err = e.what ();
+    return -1;
+  }
+}
+
+// Surface render of the mesh boundary: MeshBoundary -> Surface::nearest_hit
+// -> fragments -> shade (lit) into a cleared framebuffer.  Outputs hits
+// (idx, dist, ref u, ref v per ray) and the framebuffer (w*h*4 floats +
+// w*h depths) before background compositing.
+int ref_surface (void *h, int w, int hgt, const float *cam9, float fov, int tf_samples,
+                 int n_rgb, const float *rgb_pts, int n_alpha, const float *alpha_pts,
+                 int n_lights, const float *lights13, int *hit_idx, float *hit_dist,
+                 float *hit_ref2, float *rgba, float *depth)
+{
+  try
+  {
+    RefMesh *r = static_cast<RefMesh *> (h);
+    MeshBoundary mb;
+    Collection faces = mb.execute (r->collection);
+    Camera cam;
+    setup_camera (cam, w, hgt, cam9, fov);
+    Array<Ray> rays;
+    cam.create_rays (rays);
+    Surface surf (faces);
+    surf.field ("f");
+    ColorMap &cmap = surf.color_map ();
+    cmap.samples (tf_samples);
+    cmap.color_table (make_table (n_rgb, rgb_pts, n_alpha, alpha_pts));
+    Array<RayHit> hits = surf.nearest_hit (rays);
+    Array<Fragment> frags = surf.fragments (hits);
+    Framebuffer fb (w, hgt);
+    fb.clear ();
+    if (n_lights > 0)
+    {
+      Array<PointLight> lights = make_lights (n_lights, lights13);
+      surf.shade (rays, hits, frags, lights, fb);
+    }
+    else
+    {
+      surf.shade (rays, hits, frags, fb);
+    }
+    const RayHit *hp = hits.get_host_ptr_const ();
+    const int n = hits.size ();
+    for (int i = 0; i < n; ++i)
+    {
+      if (hit_idx) hit_idx[i] = hp[i].m_hit_idx;
+      if (hit_dist) hit_dist[i] = hp[i].m_dist;
+      if (hit_ref2)
+      {
+        hit_ref2[2 * i] = hp[i].m_ref_pt[0];
+        hit_ref2[2 * i + 1] = hp[i].m_ref_pt[1];
+      }
+    }
+    if (rgba)
+      std::memcpy (rgba, (const void *)fb.colors ().get_host_ptr_const (), sizeof (float) * 4 * (size_t)w * hgt);
+    if (depth)
+      std::memcpy (depth, fb.depths ().get_host_ptr_const (), sizeof (float) * (size_t)w * hgt);
+    return n;
+  }
+  catch (const std::exception &e)
+  {
+    g_err = e.what ();
+    return -1;
+  }
+}
+
+// Element<3,1,Tensor,P>::eval_d of one scalar hex element with control
+// values `vals` ((p+1)^3, u fastest) at n reference points; fixed != 0 uses
+// the fixed-order specialisation (orders 1 and 2), else Order::General.
+// This is how the reference's own t_dray_external_evals test drives it.
+int ref_eval_hex_scalar (int p, int fixed, const float *vals, int n, const float *ref3,
+                         float *out_val, float *out_d3)
+{
+  try
+  {
+    const int nd = (p + 1) * (p + 1) * (p + 1);
+    std::vector<int32> ids (nd);
+    std::vector<Vec<Float, 1>> data (nd);
+    for (int i = 0; i < nd; ++i)
+    {
+      ids[i] = i;
+      data[i][0] = vals[i];
+    }
+    ReadDofPtr<Vec<Float, 1>> rdp;
+    rdp.m_offset_ptr = ids.data ();
+    rdp.m_dof_ptr = data.data ();
+    for (int q = 0; q < n; ++q)
+    {
+      Vec<Float, 3> r = { { ref3[3 * q], ref3[3 * q + 1], ref3[3 * q + 2] } };
+      Vec<Vec<Float, 1>, 3> d;
+      Vec<Float, 1> v;
+      if (fixed && p == 1)
+        v = Element<3, 1, ElemType::Tensor, Order::Linear>::create (0, rdp, p).eval_d (r, d);
+      else if (fixed && p == 2)
+        v = Element<3, 1, ElemType::Tensor, Order::Quadratic>::create (0, rdp, p).eval_d (r, d);
+      else
+        v = Element<3, 1, ElemType::Tensor, Order::General>::create (0, rdp, p).eval_d (r, d);
+      out_val[q] = v[0];
+      for (int k = 0; k < 3; ++k) out_d3[3 * q + k] = d[k][0];
+    }
+    return 0;
+  }
+  catch (const std::exception &e)
+  {
+    g_err = e.what ();
+    return -1;
+  }
+}
+
+} // extern "C"

@@ -1,0 +1,180 @@
+"""Test oracle: ctypes wrapper over oracle/_ref/libdray_ref.so, the
+reference's own C++ sources built by oracle/Makefile (see ref_api.cpp).
+
+Test infrastructure only: imported by tests/, __graft_entry__.smoke() and the
+bench's CPU-baseline leg, never by the product.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+from pathlib import Path
+
+import numpy as np
+
+HERE = Path(__file__).resolve().parent
+REF_LIB = HERE / "_ref" / "libdray_ref.so"
+
+_lib = None
+
+
+def available() -> bool:
+    return REF_LIB.exists()
+
+
+def lib():
+    global _lib
+    if _lib is None:
+        if not REF_LIB.exists():
+            raise FileNotFoundError(f"{REF_LIB} not built (make -C oracle ref)")
+        L = C.CDLL(str(REF_LIB))
+        vp, ip, fp = C.c_void_p, C.POINTER(C.c_int), C.POINTER(C.c_float)
+        L.ref_last_error.restype = C.c_char_p
+        L.ref_num_threads.restype = C.c_int
+        L.ref_set_num_threads.argtypes = [C.c_int]
+        L.ref_hex_create.restype = vp
+        L.ref_hex_create.argtypes = [C.c_int, C.c_int, vp, C.c_int, vp, vp, C.c_int, vp]
+        L.ref_free.argtypes = [vp]
+        L.ref_bvh_sizes.argtypes = [vp, ip, ip]
+        L.ref_bvh_copy.argtypes = [vp, vp, vp, vp, vp, vp]
+        L.ref_morton.argtypes = [C.c_int, vp, vp, vp]
+        L.ref_locate.argtypes = [vp, C.c_int, vp, vp, vp]
+        L.ref_camera_rays.argtypes = [C.c_int, C.c_int, vp, C.c_float, vp]
+        L.ref_volume.argtypes = [vp, C.c_int, C.c_int, vp, C.c_float, C.c_int, C.c_int, C.c_int,
+                                 C.c_int, vp, C.c_int, vp, C.c_int, vp, vp, vp, C.c_int]
+        L.ref_boundary.argtypes = [vp, vp, C.c_int]
+        L.ref_surface.argtypes = [vp, C.c_int, C.c_int, vp, C.c_float, C.c_int, C.c_int, vp,
+                                  C.c_int, vp, C.c_int, vp, vp, vp, vp, vp, vp]
+        L.ref_eval_hex_scalar.argtypes = [C.c_int, C.c_int, vp, C.c_int, vp, vp, vp]
+        _lib = L
+    return _lib
+
+
+def _p(a: np.ndarray):
+    return a.ctypes.data_as(C.c_void_p)
+
+
+def set_threads(n: int):
+    lib().ref_set_num_threads(int(n))
+
+
+def num_threads() -> int:
+    return lib().ref_num_threads()
+
+
+class RefHexMesh:
+    """The reference's UnstructuredMesh<Hex> (+ scalar field "f")."""
+
+    def __init__(self, order, ctrl_idx, xyz, field=None):
+        self.order = int(order)
+        self.ctrl_idx = np.ascontiguousarray(ctrl_idx, dtype=np.int32)
+        self.xyz = np.ascontiguousarray(xyz, dtype=np.float32).reshape(-1, 3)
+        self.field = None if field is None else np.ascontiguousarray(field, dtype=np.float32)
+        nd = (self.order + 1) ** 3
+        self.n_elem = self.ctrl_idx.size // nd
+        fptr = None if self.field is None else _p(self.field)
+        self.h = lib().ref_hex_create(self.order, self.n_elem, _p(self.ctrl_idx), self.xyz.shape[0],
+                                      _p(self.xyz), _p(self.ctrl_idx),
+                                      0 if self.field is None else self.field.size, fptr)
+        if not self.h:
+            raise RuntimeError(lib().ref_last_error().decode())
+
+    def __del__(self):
+        if getattr(self, "h", None):
+            lib().ref_free(self.h)
+            self.h = None
+
+    def bvh(self):
+        ni, nl = C.c_int(), C.c_int()
+        if lib().ref_bvh_sizes(self.h, C.byref(ni), C.byref(nl)) != 0:
+            raise RuntimeError(lib().ref_last_error().decode())
+        inner = np.zeros((ni.value, 16), np.float32)
+        leaf = np.zeros(nl.value, np.int32)
+        ids = np.zeros(nl.value, np.int32)
+        bounds = np.zeros(6, np.float32)
+        refb = np.zeros((nl.value, 6), np.float32)
+        if lib().ref_bvh_copy(self.h, _p(inner), _p(leaf), _p(ids), _p(bounds), _p(refb)) != 0:
+            raise RuntimeError(lib().ref_last_error().decode())
+        return {"inner": inner, "leaf_nodes": leaf, "aabb_ids": ids, "bounds": bounds,
+                "ref_boxes": refb}
+
+    def locate(self, pts):
+        pts = np.ascontiguousarray(pts, dtype=np.float32).reshape(-1, 3)
+        n = pts.shape[0]
+        cell = np.zeros(n, np.int32)
+        ref = np.zeros((n, 3), np.float32)
+        if lib().ref_locate(self.h, n, _p(pts), _p(cell), _p(ref)) != 0:
+            raise RuntimeError(lib().ref_last_error().decode())
+        return cell, ref
+
+    def volume(self, w, h, cam9, fov, samples, use_lighting, tf_samples, rgb_pts, alpha_pts,
+               lights13, want_partials=False):
+        rgb = np.ascontiguousarray(rgb_pts, np.float32).reshape(-1)
+        alp = np.ascontiguousarray(alpha_pts, np.float32).reshape(-1)
+        lights = np.ascontiguousarray(lights13, np.float32).reshape(-1)
+        cam = np.ascontiguousarray(cam9, np.float32)
+        img = np.zeros((h, w, 4), np.float32)
+        maxp = 5 * w * h if want_partials else 0
+        parts = np.zeros((max(maxp, 1), 6), np.float32)
+        n = lib().ref_volume(self.h, w, h, _p(cam), fov, samples, int(use_lighting), tf_samples,
+                             rgb.size // 4, _p(rgb), alp.size // 2, _p(alp), lights.size // 13,
+                             _p(lights), _p(img), _p(parts) if want_partials else None, maxp)
+        if n < 0:
+            raise RuntimeError(lib().ref_last_error().decode())
+        return img, (parts[:n] if want_partials else None)
+
+    def boundary_ctrl_idx(self):
+        p = self.order
+        maxf = 6 * self.n_elem
+        out = np.zeros(maxf * (p + 1) ** 2, np.int32)
+        nf = lib().ref_boundary(self.h, _p(out), maxf)
+        if nf < 0:
+            raise RuntimeError(lib().ref_last_error().decode())
+        return out[: nf * (p + 1) ** 2].reshape(nf, (p + 1) ** 2)
+
+    def surface(self, w, h, cam9, fov, tf_samples, rgb_pts, alpha_pts, lights13):
+        rgb = np.ascontiguousarray(rgb_pts, np.float32).reshape(-1)
+        alp = np.ascontiguousarray(alpha_pts, np.float32).reshape(-1)
+        lights = np.ascontiguousarray(lights13, np.float32).reshape(-1)
+        cam = np.ascontiguousarray(cam9, np.float32)
+        n = w * h
+        hit = np.zeros(n, np.int32)
+        dist = np.zeros(n, np.float32)
+        ref2 = np.zeros((n, 2), np.float32)
+        img = np.zeros((h, w, 4), np.float32)
+        depth = np.zeros((h, w), np.float32)
+        r = lib().ref_surface(self.h, w, h, _p(cam), fov, tf_samples, rgb.size // 4, _p(rgb),
+                              alp.size // 2, _p(alp), lights.size // 13, _p(lights), _p(hit),
+                              _p(dist), _p(ref2), _p(img), _p(depth))
+        if r < 0:
+            raise RuntimeError(lib().ref_last_error().decode())
+        return {"hit_idx": hit, "dist": dist, "ref": ref2, "rgba": img, "depth": depth}
+
+
+def morton(aabbs6):
+    a = np.ascontiguousarray(aabbs6, np.float32).reshape(-1, 6)
+    codes = np.zeros(a.shape[0], np.uint32)
+    bounds = np.zeros(6, np.float32)
+    lib().ref_morton(a.shape[0], _p(a), _p(codes), _p(bounds))
+    return codes, bounds
+
+
+def camera_rays(w, h, cam9, fov):
+    cam = np.ascontiguousarray(cam9, np.float32)
+    rays = np.zeros((w * h, 9), np.float32)
+    n = lib().ref_camera_rays(w, h, _p(cam), fov, _p(rays))
+    if n < 0:
+        raise RuntimeError(lib().ref_last_error().decode())
+    return rays
+
+
+def eval_hex_scalar(p, vals, refs, fixed=False):
+    """The reference's Element<3,1,Tensor,P>::eval_d of one scalar element."""
+    vals = np.ascontiguousarray(vals, np.float32)
+    refs = np.ascontiguousarray(refs, np.float32).reshape(-1, 3)
+    n = refs.shape[0]
+    v = np.zeros(n, np.float32)
+    d = np.zeros((n, 3), np.float32)
+    if lib().ref_eval_hex_scalar(p, int(fixed), _p(vals), n, _p(refs), _p(v), _p(d)) != 0:
+        raise RuntimeError(lib().ref_last_error().decode())
+    return v, d

@@ -1,0 +1,78 @@
+"""Helpers to read BVHs in the reference layout (bvh.hpp:16-37) for parity
+checks: node children, leaf boxes by sub-box id, tie runs of Morton codes."""
+from __future__ import annotations
+
+import numpy as np
+
+
+def node_children(inner: np.ndarray):
+    """(left, right) child ids of every inner node, as the int bits of
+    floats 12 and 13: inner child = 4*node, leaf = -(i+1)."""
+    kids = np.ascontiguousarray(inner[:, 12:14]).view(np.int32)
+    return kids[:, 0].copy(), kids[:, 1].copy()
+
+
+def node_boxes(inner: np.ndarray):
+    """Left and right child boxes of every node as (xmin,xmax,ymin,ymax,zmin,zmax)."""
+    lb = inner[:, [0, 3, 1, 4, 2, 5]]
+    rb = inner[:, [6, 9, 7, 10, 8, 11]]
+    return lb, rb
+
+
+def leaf_boxes(inner: np.ndarray, n_leaf: int) -> np.ndarray:
+    """AABB of every sorted leaf, recovered from its parent's node record."""
+    l, r = node_children(inner)
+    lb, rb = node_boxes(inner)
+    out = np.full((n_leaf, 6), np.nan, np.float32)
+    m = l < 0
+    out[-l[m] - 1] = lb[m]
+    m = r < 0
+    out[-r[m] - 1] = rb[m]
+    return out
+
+
+def subbox_aabbs(inner: np.ndarray, aabb_ids: np.ndarray) -> np.ndarray:
+    """Per-sub-box AABBs in the original (element-major) order."""
+    n_leaf = aabb_ids.shape[0]
+    lbx = leaf_boxes(inner, n_leaf)
+    out = np.empty_like(lbx)
+    out[aabb_ids] = lbx
+    return out
+
+
+def tie_runs(sorted_codes: np.ndarray):
+    """(start, end) of every run of >=2 equal codes in a sorted array."""
+    c = np.asarray(sorted_codes)
+    if c.size == 0:
+        return []
+    change = np.flatnonzero(np.diff(c) != 0) + 1
+    starts = np.concatenate([[0], change])
+    ends = np.concatenate([change, [c.size]])
+    return [(int(s), int(e)) for s, e in zip(starts, ends) if e - s > 1]
+
+
+def node_leaf_ranges(inner: np.ndarray):
+    """[first, last] sorted-leaf range covered by each inner node."""
+    l, r = node_children(inner)
+    n_inner = inner.shape[0]
+    lo = np.full(n_inner, -1, np.int64)
+    hi = np.full(n_inner, -1, np.int64)
+    # iterative post-order from the root
+    order = []
+    stack = [0]
+    while stack:
+        n = stack.pop()
+        order.append(n)
+        for c in (l[n], r[n]):
+            if c >= 0:
+                stack.append(c // 4)
+    for n in reversed(order):
+        ranges = []
+        for c in (l[n], r[n]):
+            if c < 0:
+                ranges.append((-c - 1, -c - 1))
+            else:
+                ranges.append((lo[c // 4], hi[c // 4]))
+        lo[n] = min(a for a, _ in ranges)
+        hi[n] = max(b for _, b in ranges)
+    return lo, hi

@@ -1,0 +1,49 @@
+"""C-ABI boundary checks that need no GPU: the library loads, exports every
+symbol declared in include/drb.h, and the pure host-side queries work."""
+import ctypes as C
+
+import numpy as np
+import pytest
+
+
+def test_library_exports_declared_symbols():
+    from devil_ray_b200 import _lib as L
+    lib = L.lib()
+    names = L.declared_symbols()
+    assert len(names) >= 8
+    missing = [n for n in names if not hasattr(lib, n)]
+    assert not missing, f"libdrb.so lacks {missing}"
+
+
+def test_host_queries():
+    from devil_ray_b200 import _lib as L
+    lib = L.lib()
+    assert lib.drb_version() >= 1
+    assert lib.drb_packed_stride(3, 2, 3) == 84
+    assert lib.drb_packed_stride(3, 3, 3) == 192
+    assert lib.drb_packed_stride(3, 1, 1) == 8
+    assert lib.drb_packed_stride(2, 3, 3) == 48
+    assert lib.drb_packed_stride(4, 3, 3) == -1
+    ni, nl = C.c_int(), C.c_int()
+    assert lib.drb_bvh_sizes(3, 262144, C.byref(ni), C.byref(nl)) == 0
+    assert nl.value == 262144 * 33 and ni.value == nl.value - 1
+    assert lib.drb_bvh_sizes(2, 6144, C.byref(ni), C.byref(nl)) == 0
+    assert nl.value == 6144 * 17
+    assert lib.drb_bvh_sizes(3, 0, C.byref(ni), C.byref(nl)) == 0
+    assert nl.value == 2 and ni.value == 1
+    assert lib.drb_bvh_sizes(3, 2 ** 27, C.byref(ni), C.byref(nl)) == L.DRB_ERR_INVALID_ARG
+    assert b"too many" in lib.drb_last_error()
+
+
+def test_invalid_arguments_rejected_without_gpu():
+    from devil_ray_b200 import _lib as L
+    lib = L.lib()
+    m = L.DrbMesh()
+    m.dim, m.order, m.ncomp, m.n_elem = 3, 7, 3, 1
+    assert lib.drb_pack_elements(C.byref(m), None, None) == L.DRB_ERR_UNSUPPORTED
+    assert lib.drb_radix_sort_pairs(None, None, None, None, -1, 30, None) == L.DRB_ERR_INVALID_ARG
+    opts = L.DrbNewtonOpts(1e-4, 20, L.GUESS_GIVEN, None)
+    m.order = 2
+    b = L.DrbBvh()
+    assert lib.drb_locate(C.byref(m), C.byref(b), None, 4, C.byref(opts), None, None,
+                          L.DrbQueryStats(), None) == L.DRB_ERR_INVALID_ARG

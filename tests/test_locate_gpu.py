@@ -1,0 +1,119 @@
+"""Point-location parity on the GPU (drb_locate through the C-ABI) against
+the reference's Mesh::locate (oracle/_ref) and the restated oracle.
+
+Bar (from the north star): located element ids identical except for points
+on shared faces/edges (counted and checked to be within the is_inside band
+of both elements); reference coordinates within 1e-5; the FP64 Newton error
+of every GPU result is stated and bounded.
+"""
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+
+
+def _setup(cuda, name, npts, seed):
+    from devil_ray_b200 import api, meshgen
+    if name == "volume_8":
+        m = meshgen.workload_mesh("volume_8")
+    elif name == "trilinear_12":
+        m = meshgen.trilinear_distorted_mesh(12, 2, 0.15, seed=11)
+    elif name == "trilinear_12_d25":
+        m = meshgen.trilinear_distorted_mesh(12, 2, 0.25, seed=12)
+    elif name == "p3_10":
+        m = meshgen.warped_mesh(10, 3, 0.08, jitter=0.01, seed=5)
+    elif name == "p1_9":
+        m = meshgen.warped_mesh(9, 1, 0.05)
+    q = meshgen.uniform_queries(npts, seed)
+    g = api.UnstructuredMesh(m.ctrl_idx, m.xyz, m.order, device=cuda)
+    return m, q, g
+
+
+def _shared_face_ok(m, cell_a, ref_a, cell_b, ref_b, band=2e-3):
+    """Both answers lie on the boundary band of their elements (a point on a
+    face or edge shared by the two elements)."""
+    def on_boundary(r):
+        return np.any((r < band) | (r > 1.0 - band), axis=-1)
+    ok = np.ones(cell_a.shape, bool)
+    both = (cell_a >= 0) & (cell_b >= 0)
+    ok[both] = on_boundary(ref_a[both]) & on_boundary(ref_b[both])
+    one = (cell_a >= 0) ^ (cell_b >= 0)
+    ra = np.where((cell_a >= 0)[:, None], ref_a, ref_b)
+    ok[one] = on_boundary(ra[one])
+    return ok
+
+
+@pytest.mark.parametrize("name", ["volume_8", "trilinear_12", "p3_10", "p1_9"])
+def test_locate_matches_reference(cuda, ref, name):
+    import torch
+    from devil_ray_b200 import _lib as L
+    m, q, g = _setup(cuda, name, 40000, 7)
+    r = ref.RefHexMesh(m.order, m.ctrl_idx, m.xyz, m.field)
+    rc, rr = r.locate(q)
+    # reference settings: tol 1e-4, 20 steps, zero-initialised guess
+    cell, rf = g.locate(q, tol=1e-4, max_steps=20, guess_mode=L.GUESS_ZERO)
+    torch.cuda.synchronize()
+    cell = cell.cpu().numpy()
+    rf = rf.cpu().numpy()
+    same = cell == rc
+    diff = ~same
+    assert _shared_face_ok(m, cell[diff], rf[diff], rc[diff], rr[diff]).all(), \
+        f"{name}: {diff.sum()} mismatches not on shared faces"
+    assert diff.mean() < 2e-3, f"{name}: {diff.sum()} cell mismatches"
+    hit = same & (cell >= 0)
+    err = np.abs(rf[hit] - rr[hit]).max()
+    assert err < 1e-5, f"{name}: max ref diff {err}"
+    print(f"{name}: located {np.mean(cell >= 0):.4f}, cell mismatches {diff.sum()} "
+          f"(shared faces), max |ref - ref_ref| {err:.2e}")
+
+
+@pytest.mark.parametrize("name", ["volume_8", "trilinear_12_d25"])
+@pytest.mark.parametrize("guess", ["center", "subref"])
+def test_locate_tol_1e5_vs_restated_and_fp64(cuda, name, guess):
+    import torch
+    from devil_ray_b200 import _lib as L
+    from oracle import restate
+    if not restate.available():
+        pytest.skip("restated oracle not built")
+    m, q, g = _setup(cuda, name, 30000, 9)
+    mode = L.GUESS_ELEM_CENTER if guess == "center" else L.GUESS_SUBREF_CENTER
+    cell, rf, it, ca = g.locate(q, tol=1e-5, max_steps=20, guess_mode=mode, stats=True)
+    torch.cuda.synchronize()
+    b = g.get_bvh()
+    bvh = {"inner": b.inner_nodes.cpu().numpy(), "leaf_nodes": b.leaf_nodes.cpu().numpy(),
+           "aabb_ids": b.aabb_ids.cpu().numpy(), "ref_boxes": b.ref_boxes.cpu().numpy()}
+    oc, orf, oit, oca = restate.locate(m.order, m.ctrl_idx, m.xyz, bvh, q, 1e-5, 20, mode)
+    cell = cell.cpu().numpy()
+    rf = rf.cpu().numpy()
+    same = cell == oc
+    assert (~same).mean() < 2e-3
+    assert _shared_face_ok(m, cell[~same], rf[~same], oc[~same], orf[~same]).all()
+    hit = same & (cell >= 0)
+    assert np.abs(rf[hit] - orf[hit]).max() < 1e-5
+    # same traversal -> same candidate counts except where the result differs
+    assert np.array_equal(ca.cpu().numpy()[same], oca[same])
+    # FP64 error of the GPU solution
+    f64, ok = restate.newton_fp64(m.order, m.ctrl_idx, m.xyz, cell, q)
+    e = np.abs(f64[(cell >= 0) & ok] - rf[(cell >= 0) & ok]).max()
+    assert e < 1e-5, f"FP64 error {e}"
+    print(f"{name}/{guess}: mean iters {it.float().mean().item():.3f}, FP64 max err {e:.2e}")
+
+
+def test_locate_edge_cases(cuda):
+    import torch
+    from devil_ray_b200 import _lib as L
+    m, q, g = _setup(cuda, "volume_8", 10, 1)
+    # empty query
+    c, r = g.locate(np.zeros((0, 3), np.float32))
+    assert c.numel() == 0
+    # far outside, NaN and the exact corners / centre
+    pts = np.array([[5, 5, 5], [-1, 0.5, 0.5], [np.nan, 0.5, 0.5], [0, 0, 0], [1, 1, 1],
+                    [0.5, 0.5, 0.5]], np.float32)
+    c, r = g.locate(pts, guess_mode=L.GUESS_ZERO)
+    c = c.cpu().numpy()
+    assert c[0] == -1 and c[1] == -1 and c[2] == -1
+    assert c[3] >= 0 and c[4] >= 0 and c[5] >= 0
+    with pytest.raises(L.DrbError):
+        g.locate(pts, tol=-1.0)
+    with pytest.raises(L.DrbError):
+        g.locate(pts, guess_mode=L.GUESS_GIVEN)
