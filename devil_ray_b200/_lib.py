@@ -43,7 +43,31 @@ class DrbNewtonOpts(C.Structure):
 
 
 class DrbQueryStats(C.Structure):
-    _fields_ = [("iters", C.c_void_p), ("candidates", C.c_void_p)]
+    _fields_ = [("iters", C.c_void_p), ("candidates", C.c_void_p), ("nodes", C.c_void_p)]
+
+
+class DrbLocateConfig(C.Structure):
+    _fields_ = [("block", C.c_int), ("blocks_per_sm", C.c_int), ("chunk", C.c_int),
+                ("sort_queries", C.c_int)]
+
+    def as_dict(self):
+        return {k: getattr(self, k) for k, _ in self._fields_}
+
+
+class DrbCamera(C.Structure):
+    _fields_ = [("width", C.c_int), ("height", C.c_int), ("pos", C.c_float * 3),
+                ("look_at", C.c_float * 3), ("up", C.c_float * 3), ("fov_y", C.c_float),
+                ("zoom", C.c_float)]
+
+
+class DrbRayStats(C.Structure):
+    _fields_ = [("samples", C.c_void_p), ("iters", C.c_void_p), ("candidates", C.c_void_p)]
+
+
+class DrbVolumeOpts(C.Structure):
+    _fields_ = [("samples", C.c_int), ("use_lighting", C.c_int), ("tol", C.c_float),
+                ("max_steps", C.c_int), ("guess_mode", C.c_int), ("coherent", C.c_int),
+                ("bounds", C.c_float * 6)]
 
 
 class DrbError(RuntimeError):
@@ -58,6 +82,37 @@ _lib = None
 _SIGS = {
     "drb_last_error": (C.c_char_p, []),
     "drb_version": (C.c_int, []),
+    "drb_camera_rays": (C.c_int, [C.POINTER(DrbCamera), C.c_void_p, C.c_void_p]),
+    "drb_default_light": (C.c_int, [C.POINTER(DrbCamera), C.c_void_p]),
+    "drb_cull_rays": (C.c_int, [C.c_void_p, C.c_int, C.c_void_p, C.c_void_p,
+                                C.POINTER(C.c_int), C.c_void_p]),
+    "drb_field_range": (C.c_int, [C.POINTER(DrbMesh), C.c_void_p, C.c_void_p]),
+    "drb_color_table_sample": (C.c_int, [C.c_int, C.c_void_p, C.c_int, C.c_void_p, C.c_int,
+                                         C.c_int, C.c_float, C.c_float, C.c_void_p]),
+    "drb_volume_integrate": (C.c_int, [C.POINTER(DrbMesh), C.POINTER(DrbMesh), C.POINTER(DrbBvh),
+                                       C.c_void_p, C.c_int, C.POINTER(DrbVolumeOpts), C.c_void_p,
+                                       C.c_int, C.c_void_p, C.c_void_p, C.c_int, C.c_void_p,
+                                       C.POINTER(C.c_int), DrbRayStats, C.c_void_p]),
+    "drb_volume_render": (C.c_int, [C.POINTER(DrbMesh), C.POINTER(DrbMesh), C.POINTER(DrbBvh),
+                                    C.c_void_p, C.c_int, C.POINTER(DrbVolumeOpts), C.c_void_p,
+                                    C.c_int, C.c_void_p, C.c_void_p, C.c_int, C.c_void_p,
+                                    C.c_void_p, DrbRayStats, C.c_void_p]),
+    "drb_composite_partials": (C.c_int, [C.c_void_p, C.c_int, C.c_void_p, C.c_void_p]),
+    "drb_framebuffer_clear": (C.c_int, [C.c_void_p, C.c_void_p, C.c_int, C.c_void_p, C.c_void_p]),
+    "drb_framebuffer_composite_background": (C.c_int, [C.c_void_p, C.c_int, C.c_void_p,
+                                                       C.c_void_p]),
+    "drb_kernel_launches": (C.c_ulonglong, []),
+    "drb_locate_batched": (C.c_int, [C.POINTER(DrbMesh), C.POINTER(DrbBvh), C.c_void_p, C.c_int,
+                                     C.POINTER(DrbNewtonOpts), C.c_void_p, C.c_void_p,
+                                     C.c_void_p, DrbQueryStats, C.c_void_p]),
+    "drb_query_order": (C.c_int, [C.POINTER(DrbBvh), C.c_void_p, C.c_int, C.c_void_p,
+                                  C.c_void_p]),
+    "drb_locate_ordered": (C.c_int, [C.POINTER(DrbMesh), C.POINTER(DrbBvh), C.c_void_p, C.c_int,
+                                     C.c_void_p, C.POINTER(DrbNewtonOpts), C.c_void_p,
+                                     C.c_void_p, C.c_void_p, DrbQueryStats, C.c_void_p]),
+    "drb_locate_tune": (C.c_int, [C.POINTER(DrbMesh), C.POINTER(DrbBvh), C.c_void_p, C.c_int,
+                                  C.POINTER(DrbNewtonOpts), C.c_void_p, C.POINTER(C.c_float),
+                                  C.c_void_p]),
     "drb_packed_stride": (C.c_int, [C.c_int, C.c_int, C.c_int]),
     "drb_pack_elements": (C.c_int, [C.POINTER(DrbMesh), C.c_void_p, C.c_void_p]),
     "drb_bvh_sizes": (C.c_int, [C.c_int, C.c_int, C.POINTER(C.c_int), C.POINTER(C.c_int)]),

@@ -148,21 +148,90 @@ class UnstructuredMesh:
         n = pts.shape[0]
         cell = torch.empty(n, dtype=torch.int32, device=self.device)
         ref = torch.empty((n, 3), dtype=torch.float32, device=self.device)
-        it = cand = None
+        it = cand = nodes = None
         if stats:
             it = torch.empty(n, dtype=torch.int32, device=self.device)
             cand = torch.empty(n, dtype=torch.int32, device=self.device)
+            nodes = torch.empty(n, dtype=torch.int32, device=self.device)
         g = None if guess is None else _dev(guess, torch.float32, self.device).reshape(-1, 3)
         opts = L.DrbNewtonOpts(tol, max_steps, guess_mode, None if g is None else g.data_ptr())
         st = L.DrbQueryStats(None if it is None else it.data_ptr(),
-                             None if cand is None else cand.data_ptr())
+                             None if cand is None else cand.data_ptr(),
+                             None if nodes is None else nodes.data_ptr())
         b = self.get_bvh(stream)
         d = self.desc(packed)
         bd = b.desc()
         L.check(L.lib().drb_locate(C.byref(d), C.byref(bd), _ptr(pts), n, C.byref(opts),
                                    _ptr(cell), _ptr(ref), st, _stream(stream)), "drb_locate")
         if stats:
-            return cell, ref, it, cand
+            return cell, ref, it, cand, nodes
+        return cell, ref
+
+
+def _locate_outputs(n, device, stats):
+    cell = torch.empty(n, dtype=torch.int32, device=device)
+    ref = torch.empty((n, 3), dtype=torch.float32, device=device)
+    st = [torch.empty(n, dtype=torch.int32, device=device) for _ in range(3)] if stats else None
+    qs = L.DrbQueryStats(*(None if st is None else t.data_ptr() for t in (st or [None] * 3)))
+    return cell, ref, st, qs
+
+
+class BatchedLocator:
+    """Persistent, batched Mesh::locate (drb_locate_batched): Morton-ordered
+    queries, a global work queue, autotuned launch shape."""
+
+    def __init__(self, mesh: UnstructuredMesh, tol: float = 1e-5, max_steps: int = 20,
+                 guess_mode: int = L.GUESS_ELEM_CENTER, config: L.DrbLocateConfig | None = None):
+        self.mesh = mesh
+        self.tol, self.max_steps, self.guess_mode = tol, max_steps, guess_mode
+        self.config = config
+
+    def tune(self, sample_points, stream=None):
+        pts = _dev(sample_points, torch.float32, self.mesh.device).reshape(-1, 3)
+        best = L.DrbLocateConfig()
+        ms = C.c_float()
+        opts = L.DrbNewtonOpts(self.tol, self.max_steps, self.guess_mode, None)
+        d = self.mesh.desc()
+        bd = self.mesh.get_bvh(stream).desc()
+        L.check(L.lib().drb_locate_tune(C.byref(d), C.byref(bd), _ptr(pts), pts.shape[0],
+                                        C.byref(opts), C.byref(best), C.byref(ms),
+                                        _stream(stream)), "drb_locate_tune")
+        self.config = best
+        return best, ms.value
+
+    def order(self, points, stream=None):
+        pts = _dev(points, torch.float32, self.mesh.device).reshape(-1, 3)
+        o = torch.empty(pts.shape[0], dtype=torch.int32, device=self.mesh.device)
+        bd = self.mesh.get_bvh(stream).desc()
+        L.check(L.lib().drb_query_order(C.byref(bd), _ptr(pts), pts.shape[0], _ptr(o),
+                                        _stream(stream)), "drb_query_order")
+        return o
+
+    def locate(self, points, order=None, guess=None, stats=False, out=None, stream=None):
+        pts = _dev(points, torch.float32, self.mesh.device).reshape(-1, 3)
+        n = pts.shape[0]
+        if out is None:
+            cell, ref, st, qs = _locate_outputs(n, self.mesh.device, stats)
+        else:
+            cell, ref = out
+            st, qs = None, L.DrbQueryStats()
+        mode = self.guess_mode if guess is None else L.GUESS_GIVEN
+        opts = L.DrbNewtonOpts(self.tol, self.max_steps, mode,
+                               None if guess is None else guess.data_ptr())
+        cfg = None if self.config is None else C.byref(self.config)
+        d = self.mesh.desc()
+        bd = self.mesh.get_bvh(stream).desc()
+        if order is None:
+            L.check(L.lib().drb_locate_batched(C.byref(d), C.byref(bd), _ptr(pts), n,
+                                               C.byref(opts), cfg, _ptr(cell), _ptr(ref), qs,
+                                               _stream(stream)), "drb_locate_batched")
+        else:
+            L.check(L.lib().drb_locate_ordered(C.byref(d), C.byref(bd), _ptr(pts), n,
+                                               _ptr(order), C.byref(opts), cfg, _ptr(cell),
+                                               _ptr(ref), qs, _stream(stream)),
+                    "drb_locate_ordered")
+        if stats:
+            return cell, ref, st[0], st[1], st[2]
         return cell, ref
 
 

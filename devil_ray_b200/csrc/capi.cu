@@ -1,6 +1,7 @@
 // Error reporting and small shared helpers of the C-ABI (include/drb.h).
 #include "drb_internal.h"
 
+#include <atomic>
 #include <cstdio>
 #include <cstring>
 #include <string>
@@ -14,8 +15,14 @@ thread_local std::string g_last_error;
 
 void set_last_error (const char *msg) { g_last_error = msg ? msg : ""; }
 
+namespace
+{
+std::atomic<unsigned long long> g_launches{ 0 };
+}
+
 int check_launch (const char *what)
 {
+  ++g_launches;
   const cudaError_t e = cudaGetLastError ();
   if (e == cudaSuccess) return DRB_OK;
   char buf[512];
@@ -43,3 +50,5 @@ int sm_count ()
 extern "C" const char *drb_last_error (void) { return drb::g_last_error.c_str (); }
 
 extern "C" int drb_version (void) { return 1; }
+
+extern "C" unsigned long long drb_kernel_launches (void) { return drb::g_launches.load (); }

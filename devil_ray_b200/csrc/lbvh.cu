@@ -647,6 +647,7 @@ extern "C" int drb_elem_subboxes (const drb_mesh *mesh, float *aabbs6, int *prim
   unsigned *bord = scr.alloc<unsigned> (6);
   if (!bord) return status_from (scr.err);
   bounds_init_kernel<<<1, 32, 0, s>>> (bord);
+  if ((st = check_launch ("bounds_init_kernel"))) return st;
   st = dispatch_subbox (mesh, aabbs6, prim_ids, ref_boxes, bord, s);
   if (st) return st;
   bounds_finish_kernel<<<1, 32, 0, s>>> (bord, bounds6);
@@ -726,9 +727,11 @@ extern "C" int drb_lbvh_build (const drb_mesh *mesh, drb_bvh *bvh, unsigned *sor
   if (scr.err != cudaSuccess) return status_from (scr.err);
 
   bounds_init_kernel<<<1, 32, 0, s>>> (bord);
+  if ((st = check_launch ("bounds_init_kernel"))) return st;
   st = dispatch_subbox (mesh, aabbs, prim, bvh->ref_boxes, bord, s);
   if (st) return st;
   bounds_finish_kernel<<<1, 32, 0, s>>> (bord, bounds6);
+  if ((st = check_launch ("bounds_finish_kernel"))) return st;
   morton_kernel<<<div_up (n, 256), 256, 0, s>>> (aabbs, n, bounds6, codes, iota);
   if ((st = check_launch ("morton_kernel"))) return st;
   st = radix_sort_pairs (codes, iota, codes_sorted, bvh->aabb_ids, n, 30, s);

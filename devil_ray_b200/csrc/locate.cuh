@@ -1,0 +1,169 @@
+// Device pieces shared by the point-location kernels (plain, persistent)
+// and the volume renderer: node tests, the per-candidate guess and the
+// per-element Newton dispatch.
+#pragma once
+
+#include "drb_common.cuh"
+#include "newton.cuh"
+#include "../../include/drb.h"
+
+namespace drb
+{
+
+// Point-in-box tests of both children of an inner node (device_mesh.hpp:262-318).
+DRB_D void node_point_test (const float4 *__restrict__ nodes, int node, const float (&p)[3],
+                            bool &in_left, bool &in_right)
+{
+  const float4 a = __ldg (nodes + node + 0);
+  const float4 b = __ldg (nodes + node + 1);
+  const float4 c = __ldg (nodes + node + 2);
+  in_left = !(p[0] < a.x || p[1] < a.y || p[2] < a.z || p[0] > a.w || p[1] > b.x || p[2] > b.y);
+  in_right = !(p[0] < b.z || p[1] < b.w || p[2] < c.x || p[0] > c.y || p[1] > c.z || p[2] > c.w);
+}
+
+struct LocateParams
+{
+  const float4 *nodes;
+  const int *leaf_nodes;
+  const int *aabb_ids;
+  const float *ref_boxes;
+  const float *packed;
+  const int *ctrl_idx;
+  const float *xyz;
+  int stride;
+  float tol;
+  int max_steps;
+  int guess_mode;
+  const float *guess;
+};
+
+// Newton solve of one point in one element, choosing register-resident or
+// L1-read control points by order.
+template <int P>
+DRB_D bool solve_in_element (const LocateParams &lp, int el, const float (&pt)[3], float (&x)[3],
+                             int &steps)
+{
+  constexpr int ND = (P + 1) * (P + 1) * (P + 1);
+  if (lp.packed)
+  {
+    const float *row = lp.packed + (size_t)el * lp.stride;
+    if (P <= 2)
+    {
+      RegCP<3 * ND> r;
+      load_reg_cp<P> (r, row);
+      return hex_newton<P> (r, pt, x, lp.tol, lp.max_steps, steps);
+    }
+    PackedCP cp{ row };
+    return hex_newton<P> (cp, pt, x, lp.tol, lp.max_steps, steps);
+  }
+  IndirectCP cp{ lp.ctrl_idx + (size_t)el * ND, lp.xyz, 3 };
+  return hex_newton<P> (cp, pt, x, lp.tol, lp.max_steps, steps);
+}
+
+// Initial guess of a candidate leaf's Newton solve (drb_guess_mode).
+DRB_D void candidate_guess (const LocateParams &lp, int leaf, long long qi, bool first,
+                            float (&x)[3], bool &given)
+{
+  given = false;
+  if (lp.guess_mode == DRB_GUESS_ZERO)
+  {
+    x[0] = x[1] = x[2] = 0.f;
+  }
+  else if (lp.guess_mode == DRB_GUESS_SUBREF_CENTER)
+  {
+    const float *rb = lp.ref_boxes + 6 * (size_t)__ldg (lp.aabb_ids + leaf);
+#pragma unroll
+    for (int d = 0; d < 3; ++d) x[d] = (rb[d] + rb[3 + d]) * 0.5f;
+  }
+  else if (lp.guess_mode == DRB_GUESS_GIVEN && first)
+  {
+#pragma unroll
+    for (int d = 0; d < 3; ++d) x[d] = lp.guess[3 * (size_t)qi + d];
+    given = true;
+  }
+  else
+  {
+    x[0] = x[1] = x[2] = 0.5f;
+  }
+}
+
+// Newton in one candidate element with the guess-mode fallback: a given
+// guess that does not converge is retried from the element centre.
+template <int P>
+DRB_D bool solve_candidate (const LocateParams &lp, int leaf, int el, long long qi, bool first,
+                            const float (&pt)[3], float (&x)[3], int &iters)
+{
+  bool given;
+  candidate_guess (lp, leaf, qi, first, x, given);
+  int steps = 0;
+  bool found = solve_in_element<P> (lp, el, pt, x, steps);
+  iters += steps;
+  if (!found && given)
+  {
+    x[0] = x[1] = x[2] = 0.5f;
+    found = solve_in_element<P> (lp, el, pt, x, steps);
+    iters += steps;
+  }
+  return found;
+}
+
+// Full point location of one query (DeviceMesh::locate, device_mesh.hpp:248-354):
+// traversal left child first, first converged+inside candidate wins.
+template <int P>
+DRB_D int locate_point (const LocateParams &lp, int qi, const float (&pt)[3], float (&out_ref)[3],
+                        int &iters, int &cands, int &nodes)
+{
+  int todo[kStackDepth];
+  int current = 0;
+  int sp = 0;
+  todo[sp] = kBarrier;
+  bool first_candidate = true;
+  while (current != kBarrier)
+  {
+    if (current > -1)
+    {
+      bool in_l, in_r;
+      ++nodes;
+      node_point_test (lp.nodes, current, pt, in_l, in_r);
+      if (!in_l && !in_r)
+      {
+        current = todo[sp];
+        --sp;
+      }
+      else
+      {
+        const float4 ch = __ldg (lp.nodes + current + 3);
+        const int l = __float_as_int (ch.x);
+        const int r = __float_as_int (ch.y);
+        current = in_l ? l : r;
+        if (in_l && in_r)
+        {
+          // depth is bounded by the tree height; 64 covers 2^63 leaves of a
+          // balanced tree and the reference uses the same fixed stack
+          if (sp < kStackDepth - 1) todo[++sp] = r;
+        }
+      }
+    }
+    else
+    {
+      const int leaf = -current - 1;
+      const int el = __ldg (lp.leaf_nodes + leaf);
+      ++cands;
+      float x[3];
+      const bool found = solve_candidate<P> (lp, leaf, el, qi, first_candidate, pt, x, iters);
+      first_candidate = false;
+      if (found)
+      {
+        out_ref[0] = x[0];
+        out_ref[1] = x[1];
+        out_ref[2] = x[2];
+        return el;
+      }
+      current = todo[sp];
+      --sp;
+    }
+  }
+  return -1;
+}
+
+} // namespace drb

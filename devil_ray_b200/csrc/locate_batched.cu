@@ -1,0 +1,440 @@
+// Persistent, batched point location.
+//
+// The reference launches one thread per point in input order
+// (data_model/unstructured_mesh.cpp:137-148): warps mix points from
+// unrelated parts of the mesh, and every lane waits for the slowest lane's
+// traversal and Newton iterations.  This path instead
+//   1. sorts the queries along a 30-bit Morton curve over the BVH bounds
+//      (query_codes_kernel + the radix sort), so a warp's lanes follow
+//      nearly the same BVH path and hit the same few elements (L1/L2 reuse);
+//   2. runs a persistent kernel, grid sized to the resident capacity of the
+//      148 SMs, whose warps pop chunks of sorted queries from a global atomic
+//      queue;
+//   3. inside a warp, lanes that finish a query are refilled immediately from
+//      the warp's chunk by ballot ranking (warp-ballot compaction), and
+//      traversal and Newton are separated into phases so the Newton solves of
+//      a warp run converged (traverse until every busy lane holds a
+//      candidate leaf or has finished, then solve together).
+// Results are identical to the plain kernel's: every query follows the same
+// traversal order and per-candidate solves.  The queue holds no waits (only
+// atomicAdd pops), so nothing in the kernel can spin.
+#include "drb_common.cuh"
+#include "drb_internal.h"
+#include "locate.cuh"
+
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+
+namespace drb
+{
+namespace
+{
+
+__global__ void query_codes_kernel (const float *__restrict__ pts, int n, float x0, float y0,
+                                    float z0, float sx, float sy, float sz,
+                                    unsigned *__restrict__ codes, int *__restrict__ iota)
+{
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const float lo[3] = { x0, y0, z0 };
+  const float sc[3] = { sx, sy, sz };
+  unsigned e[3];
+#pragma unroll
+  for (int k = 0; k < 3; ++k)
+  {
+    float t = (pts[3 * (size_t)i + k] - lo[k]) * sc[k];
+    t = fminf (fmaxf (t * 1024.f, 0.f), 1023.f);
+    unsigned x = (t == t) ? (unsigned)t : 0u; // NaN queries sort first
+    x = (x | (x << 16)) & 0x030000FFu;
+    x = (x | (x << 8)) & 0x0300F00Fu;
+    x = (x | (x << 4)) & 0x030C30C3u;
+    x = (x | (x << 2)) & 0x09249249u;
+    e[k] = x;
+  }
+  codes[i] = (e[2] << 2) | (e[1] << 1) | e[0];
+  iota[i] = i;
+}
+
+template <int P>
+__global__ void locate_persistent_kernel (LocateParams lp, const float *__restrict__ pts,
+                                          const int *__restrict__ order, int n, int chunk,
+                                          int *__restrict__ queue_head, int *__restrict__ cell,
+                                          float *__restrict__ ref, int *__restrict__ it_out,
+                                          int *__restrict__ ca_out, int *__restrict__ nd_out)
+{
+  const unsigned FULL = 0xffffffffu;
+  const int lane = threadIdx.x & 31;
+  const unsigned lt = (1u << lane) - 1u;
+  int pool_next = 0, pool_end = 0; // warp-uniform
+  bool exhausted = false;          // warp-uniform
+  int qi = -1;
+  float pt[3] = { 0.f, 0.f, 0.f };
+  int todo[kStackDepth];
+  int sp = 0, cur = kBarrier;
+  int iters = 0, cands = 0, nodes = 0;
+  bool first = true;
+
+  while (true)
+  {
+    // ---- refill idle lanes from the warp's chunk (ballot ranking) ----
+    unsigned need = __ballot_sync (FULL, qi < 0);
+    while (need != 0u && !exhausted)
+    {
+      if (pool_next >= pool_end)
+      {
+        int base = 0;
+        if (lane == 0) base = atomicAdd (queue_head, chunk);
+        base = __shfl_sync (FULL, base, 0);
+        if (base >= n)
+        {
+          exhausted = true;
+          break;
+        }
+        pool_next = base;
+        pool_end = min (base + chunk, n);
+      }
+      const int avail = pool_end - pool_next;
+      const int rank = __popc (need & lt);
+      if (qi < 0 && rank < avail)
+      {
+        const int pos = pool_next + rank;
+        qi = order ? __ldg (order + pos) : pos;
+        pt[0] = __ldg (pts + 3 * (size_t)qi);
+        pt[1] = __ldg (pts + 3 * (size_t)qi + 1);
+        pt[2] = __ldg (pts + 3 * (size_t)qi + 2);
+        sp = 0;
+        todo[0] = kBarrier;
+        cur = 0;
+        iters = cands = nodes = 0;
+        first = true;
+      }
+      pool_next += min (__popc (need), avail);
+      need = __ballot_sync (FULL, qi < 0);
+    }
+    if (__ballot_sync (FULL, qi >= 0) == 0u) break;
+
+    // ---- traversal phase: advance to the next candidate leaf ----
+    int leaf = -1;
+    if (qi >= 0)
+    {
+      while (cur != kBarrier)
+      {
+        if (cur > -1)
+        {
+          bool in_l, in_r;
+          ++nodes;
+          node_point_test (lp.nodes, cur, pt, in_l, in_r);
+          if (!in_l && !in_r)
+          {
+            cur = todo[sp];
+            --sp;
+          }
+          else
+          {
+            const float4 ch = __ldg (lp.nodes + cur + 3);
+            const int l = __float_as_int (ch.x);
+            const int r = __float_as_int (ch.y);
+            cur = in_l ? l : r;
+            if (in_l && in_r && sp < kStackDepth - 1) todo[++sp] = r;
+          }
+        }
+        else
+        {
+          leaf = -cur - 1;
+          break;
+        }
+      }
+    }
+
+    // ---- candidate phase: converged Newton solves ----
+    if (qi >= 0)
+    {
+      bool done = false;
+      int found_el = -1;
+      float x[3] = { -1.f, -1.f, -1.f };
+      if (leaf >= 0)
+      {
+        const int el = __ldg (lp.leaf_nodes + leaf);
+        ++cands;
+        const bool found = solve_candidate<P> (lp, leaf, el, qi, first, pt, x, iters);
+        first = false;
+        if (found)
+        {
+          found_el = el;
+          done = true;
+        }
+        else
+        {
+          cur = todo[sp];
+          --sp;
+        }
+      }
+      else
+      {
+        done = true; // traversal exhausted: not found
+      }
+      if (done)
+      {
+        cell[qi] = found_el;
+        if (found_el < 0) x[0] = x[1] = x[2] = -1.f;
+        ref[3 * (size_t)qi] = x[0];
+        ref[3 * (size_t)qi + 1] = x[1];
+        ref[3 * (size_t)qi + 2] = x[2];
+        if (it_out) it_out[qi] = iters;
+        if (ca_out) ca_out[qi] = cands;
+        if (nd_out) nd_out[qi] = nodes;
+        qi = -1;
+      }
+    }
+  }
+}
+
+template <int P> const void *persistent_fn ()
+{
+  return (const void *)locate_persistent_kernel<P>;
+}
+
+int launch_persistent (int order, dim3 grid, int block, cudaStream_t s, const LocateParams &lp,
+                       const float *pts, const int *ord, int n, int chunk, int *head, int *cell,
+                       float *ref, drb_query_stats st)
+{
+  if (order == 1)
+    locate_persistent_kernel<1><<<grid, block, 0, s>>> (lp, pts, ord, n, chunk, head, cell, ref, st.iters, st.candidates, st.nodes);
+  else if (order == 2)
+    locate_persistent_kernel<2><<<grid, block, 0, s>>> (lp, pts, ord, n, chunk, head, cell, ref, st.iters, st.candidates, st.nodes);
+  else
+    locate_persistent_kernel<3><<<grid, block, 0, s>>> (lp, pts, ord, n, chunk, head, cell, ref, st.iters, st.candidates, st.nodes);
+  return check_launch ("locate_persistent_kernel");
+}
+
+int resident_blocks (int order, int block)
+{
+  int nb = 0;
+  const void *fn = order == 1 ? persistent_fn<1> () : (order == 2 ? persistent_fn<2> () : persistent_fn<3> ());
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor (&nb, fn, block, 0);
+  return nb > 0 ? nb : 1;
+}
+
+LocateParams make_params (const drb_mesh *mesh, const drb_bvh *bvh, const drb_newton_opts *opts)
+{
+  LocateParams lp;
+  lp.nodes = (const float4 *)bvh->inner_nodes;
+  lp.leaf_nodes = bvh->leaf_nodes;
+  lp.aabb_ids = bvh->aabb_ids;
+  lp.ref_boxes = bvh->ref_boxes;
+  lp.packed = mesh->packed;
+  lp.ctrl_idx = mesh->ctrl_idx;
+  lp.xyz = mesh->values;
+  lp.stride = packed_stride ((mesh->order + 1) * (mesh->order + 1) * (mesh->order + 1), 3);
+  lp.tol = opts->tol;
+  lp.max_steps = opts->max_steps;
+  lp.guess_mode = opts->guess_mode;
+  lp.guess = opts->guess;
+  return lp;
+}
+
+int check_args (const drb_mesh *mesh, const drb_bvh *bvh, const float *pts, int n,
+                const drb_newton_opts *opts, const int *cell, const float *ref)
+{
+  if (!mesh || !bvh || !opts || n < 0 || (n > 0 && (!pts || !cell || !ref)))
+  {
+    set_last_error ("locate_batched: bad arguments");
+    return DRB_ERR_INVALID_ARG;
+  }
+  if (mesh->dim != 3 || mesh->ncomp != 3 || mesh->order < 1 || mesh->order > 3)
+  {
+    set_last_error ("locate_batched: needs a hex geometry mesh of order 1..3");
+    return DRB_ERR_UNSUPPORTED;
+  }
+  if (opts->guess_mode == DRB_GUESS_GIVEN && !opts->guess)
+  {
+    set_last_error ("locate_batched: DRB_GUESS_GIVEN needs a guess array");
+    return DRB_ERR_INVALID_ARG;
+  }
+  if (opts->max_steps < 0 || !(opts->tol > 0.f))
+  {
+    set_last_error ("locate_batched: tol must be > 0 and max_steps >= 0");
+    return DRB_ERR_INVALID_ARG;
+  }
+  return DRB_OK;
+}
+
+drb_locate_config default_config (int order)
+{
+  drb_locate_config c;
+  c.block = 128;
+  c.blocks_per_sm = 0; // 0 = all resident blocks
+  c.chunk = 64;
+  c.sort_queries = 1;
+  (void)order;
+  return c;
+}
+
+} // namespace
+
+// Morton order of the queries over the BVH bounds (device int32 order[n]).
+int query_morton_order (const drb_bvh *bvh, const float *pts, int n, int *order, cudaStream_t s)
+{
+  Scratch scr (s);
+  unsigned *codes = scr.alloc<unsigned> (n);
+  unsigned *codes_sorted = scr.alloc<unsigned> (n);
+  int *iota = scr.alloc<int> (n);
+  if (scr.err != cudaSuccess) return status_from (scr.err);
+  const float *b = bvh->bounds;
+  float sc[3];
+  for (int k = 0; k < 3; ++k)
+  {
+    const float ext = b[2 * k + 1] - b[2 * k];
+    sc[k] = (ext > 0.f && std::isfinite (ext)) ? 1.f / ext : 0.f;
+  }
+  const float lo[3] = { std::isfinite (b[0]) ? b[0] : 0.f, std::isfinite (b[2]) ? b[2] : 0.f,
+                        std::isfinite (b[4]) ? b[4] : 0.f };
+  query_codes_kernel<<<div_up (n, 256), 256, 0, s>>> (pts, n, lo[0], lo[1], lo[2], sc[0], sc[1],
+                                                       sc[2], codes, iota);
+  int st = check_launch ("query_codes_kernel");
+  if (st) return st;
+  return radix_sort_pairs (codes, iota, codes_sorted, order, n, 30, s);
+}
+
+int locate_batched_impl (const drb_mesh *mesh, const drb_bvh *bvh, const float *pts, int n,
+                         const drb_newton_opts *opts, const drb_locate_config *cfg_in,
+                         const int *order_in, int *cell, float *ref, drb_query_stats stats,
+                         cudaStream_t s)
+{
+  int st = check_args (mesh, bvh, pts, n, opts, cell, ref);
+  if (st) return st;
+  if (n == 0) return DRB_OK;
+  drb_locate_config cfg = cfg_in ? *cfg_in : default_config (mesh->order);
+  if (cfg.block < 32 || cfg.block > 1024 || (cfg.block % 32) || cfg.chunk < 1)
+  {
+    set_last_error ("locate_batched: block must be a multiple of 32 in [32,1024], chunk >= 1");
+    return DRB_ERR_INVALID_ARG;
+  }
+  Scratch scr (s);
+  int *head = scr.alloc<int> (1);
+  const int *ord = order_in;
+  if (!ord && cfg.sort_queries)
+  {
+    int *o = scr.alloc<int> (n);
+    if (!o) return status_from (scr.err);
+    st = query_morton_order (bvh, pts, n, o, s);
+    if (st) return st;
+    ord = o;
+  }
+  if (scr.err != cudaSuccess) return status_from (scr.err);
+  cudaMemsetAsync (head, 0, sizeof (int), s);
+  const int per_sm = resident_blocks (mesh->order, cfg.block);
+  const int bps = (cfg.blocks_per_sm > 0) ? min (cfg.blocks_per_sm, per_sm) : per_sm;
+  const long long warps_needed = ((long long)n + 31) / 32;
+  long long blocks = (long long)bps * sm_count ();
+  const long long blocks_needed = (warps_needed * 32 + cfg.block - 1) / cfg.block;
+  if (blocks > blocks_needed) blocks = blocks_needed;
+  if (blocks < 1) blocks = 1;
+  const LocateParams lp = make_params (mesh, bvh, opts);
+  return launch_persistent (mesh->order, dim3 ((unsigned)blocks), cfg.block, s, lp, pts, ord, n,
+                            cfg.chunk, head, cell, ref, stats);
+}
+
+} // namespace drb
+
+using namespace drb;
+
+extern "C" int drb_locate_batched (const drb_mesh *mesh, const drb_bvh *bvh, const float *pts,
+                                   int n, const drb_newton_opts *opts,
+                                   const drb_locate_config *cfg, int *cell, float *ref,
+                                   drb_query_stats stats, void *stream)
+{
+  return locate_batched_impl (mesh, bvh, pts, n, opts, cfg, nullptr, cell, ref, stats,
+                              (cudaStream_t)stream);
+}
+
+extern "C" int drb_query_order (const drb_bvh *bvh, const float *pts, int n, int *order,
+                                void *stream)
+{
+  if (!bvh || n < 0 || (n > 0 && (!pts || !order)))
+  {
+    set_last_error ("query_order: bad arguments");
+    return DRB_ERR_INVALID_ARG;
+  }
+  if (n == 0) return DRB_OK;
+  return query_morton_order (bvh, pts, n, order, (cudaStream_t)stream);
+}
+
+extern "C" int drb_locate_ordered (const drb_mesh *mesh, const drb_bvh *bvh, const float *pts,
+                                   int n, const int *order, const drb_newton_opts *opts,
+                                   const drb_locate_config *cfg, int *cell, float *ref,
+                                   drb_query_stats stats, void *stream)
+{
+  if (!order && n > 0)
+  {
+    set_last_error ("locate_ordered: order is NULL");
+    return DRB_ERR_INVALID_ARG;
+  }
+  return locate_batched_impl (mesh, bvh, pts, n, opts, cfg, order, cell, ref, stats,
+                              (cudaStream_t)stream);
+}
+
+// Autotuner: times every (block, blocks/SM, chunk) candidate on the given
+// sample with CUDA events and returns the fastest.  The sample is located
+// in Morton order once; each candidate runs twice and the second run counts.
+extern "C" int drb_locate_tune (const drb_mesh *mesh, const drb_bvh *bvh, const float *pts, int n,
+                                const drb_newton_opts *opts, drb_locate_config *best,
+                                float *best_ms, void *stream)
+{
+  int st = check_args (mesh, bvh, pts, n, opts, (const int *)1, (const float *)1);
+  if (st) return st;
+  if (!best || n <= 0)
+  {
+    set_last_error ("locate_tune: best is NULL or the sample is empty");
+    return DRB_ERR_INVALID_ARG;
+  }
+  cudaStream_t s = (cudaStream_t)stream;
+  Scratch scr (s);
+  int *ord = scr.alloc<int> (n);
+  int *cell = scr.alloc<int> (n);
+  float *ref = scr.alloc<float> ((size_t)3 * n);
+  if (scr.err != cudaSuccess) return status_from (scr.err);
+  st = query_morton_order (bvh, pts, n, ord, s);
+  if (st) return st;
+  const int blocks[] = { 64, 128, 256 };
+  const int per_sm[] = { 0, 4, 2 };
+  const int chunks[] = { 32, 64, 128, 256 };
+  cudaEvent_t e0, e1;
+  cudaEventCreate (&e0);
+  cudaEventCreate (&e1);
+  float best_t = 1e30f;
+  drb_locate_config bc = default_config (mesh->order);
+  for (int b : blocks)
+    for (int ps : per_sm)
+      for (int c : chunks)
+      {
+        drb_locate_config cfg;
+        cfg.block = b;
+        cfg.blocks_per_sm = ps;
+        cfg.chunk = c;
+        cfg.sort_queries = 1;
+        float t = 0.f;
+        for (int rep = 0; rep < 2 && st == DRB_OK; ++rep)
+        {
+          cudaEventRecord (e0, s);
+          st = locate_batched_impl (mesh, bvh, pts, n, opts, &cfg, ord, cell, ref,
+                                    drb_query_stats{ nullptr, nullptr, nullptr }, s);
+          cudaEventRecord (e1, s);
+          cudaEventSynchronize (e1);
+          cudaEventElapsedTime (&t, e0, e1);
+        }
+        if (st) break;
+        if (t < best_t)
+        {
+          best_t = t;
+          bc = cfg;
+        }
+      }
+  cudaEventDestroy (e0);
+  cudaEventDestroy (e1);
+  if (st) return st;
+  *best = bc;
+  if (best_ms) *best_ms = best_t;
+  return DRB_OK;
+}

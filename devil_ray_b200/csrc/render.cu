@@ -1,0 +1,1005 @@
+// Camera rays, ray culling, transfer functions, volume integration and
+// compositing (the reference's rendering/ layer on the hot path).
+//
+//   camera_rays_kernel      Camera::gen_perspective (rendering/camera.cpp:402-483);
+//                           host part of the set-up (set_fov, basis, deltas)
+//                           in host float arithmetic, per-ray part with
+//                           explicitly rounded ops: rays are bit-exact
+//   cull_kernel + scan      mark_active / index_flags / gather / calc_ray_start
+//                           (ray.cpp:102-241), stable compaction
+//   volume_kernel           integrate_partials (rendering/volume.cpp:71-228):
+//                           fixed-step march, locate per sample, <=5 segments,
+//                           alpha cut 0.95, Blinn-Phong from the field gradient
+//                           (rendering/volume_shader.hpp:40-167), front-to-back
+//                           blend (rendering/colors.hpp:15-23).  Persistent
+//                           warps pop rays from a global queue.  Optional
+//                           coherent mode: a sample first tries the previous
+//                           sample's element from the previous reference point,
+//                           and falls back to the full BVH locate.
+//   composite kernels       Volume::save / Framebuffer::composite_background
+//                           (volume.cpp:369-416, framebuffer.cpp:126-162)
+#include "bernstein.cuh"
+#include "drb_common.cuh"
+#include "drb_internal.h"
+#include "locate.cuh"
+
+#include <cmath>
+#include <cstring>
+#include <vector>
+
+namespace drb
+{
+
+// ---------------------------------------------------------------- camera --
+
+struct HostVec3
+{
+  float v[3];
+};
+
+static float h_mag (const float *a)
+{
+  float s = 0.f;
+  for (int i = 0; i < 3; ++i) s += a[i] * a[i];
+  return sqrtf (s);
+}
+static void h_normalize (float *a)
+{
+  const float m = h_mag (a);
+  for (int i = 0; i < 3; ++i) a[i] /= m;
+}
+static void h_cross (const float *a, const float *b, float *r)
+{
+  r[0] = a[1] * b[2] - a[2] * b[1];
+  r[1] = a[2] * b[0] - a[0] * b[2];
+  r[2] = a[0] * b[1] - a[1] * b[0];
+}
+
+struct CamSetup
+{
+  float nlook[3], dx[3], dy[3], pos[3];
+  int w, h;
+};
+
+// Camera::set_fov + create_rays_imp + the host part of gen_perspective.
+static int camera_setup (const drb_camera *cam, CamSetup &cs)
+{
+  if (!cam || cam->width <= 0 || cam->height <= 0)
+  {
+    set_last_error ("camera: width and height must be > 0");
+    return DRB_ERR_INVALID_ARG;
+  }
+  if (!(cam->fov_y > 0.f) || cam->fov_y > 180.f)
+  {
+    set_last_error ("camera: field of view must be in (0, 180]");
+    return DRB_ERR_INVALID_ARG;
+  }
+  const float pi_f = (float)3.14159265358979323846264338327950288;
+  // set_fov (camera.cpp:132-163)
+  const float fov_y = cam->fov_y;
+  const float fov_y_rad = (fov_y * pi_f) / 180.0f;
+  const float vertical = tanf (0.5f * fov_y_rad);
+  const float aspect = float (cam->width) / float (cam->height);
+  const float horizontal = aspect * vertical;
+  const float fov_x_rad = 2.0f * atanf (horizontal);
+  const float fov_x = 180.0f * (fov_x_rad / pi_f);
+  // set_up normalises the up vector (camera.cpp:172-176)
+  float up[3] = { cam->up[0], cam->up[1], cam->up[2] };
+  h_normalize (up);
+  float look[3];
+  for (int i = 0; i < 3; ++i) look[i] = cam->look_at[i] - cam->pos[i];
+  // gen_perspective (camera.cpp:402-455)
+  const float thx = tanf ((fov_x * pi_f / 180.f) * .5f);
+  const float thy = tanf ((fov_y * pi_f / 180.f) * .5f);
+  float ruf[3], ru[3], rvf[3], rv[3];
+  h_cross (look, up, ruf);
+  for (int i = 0; i < 3; ++i) ru[i] = ruf[i];
+  h_normalize (ru);
+  h_cross (ruf, look, rvf);
+  for (int i = 0; i < 3; ++i) rv[i] = rvf[i];
+  h_normalize (rv);
+  const float sx = 2 * thx / (float)cam->width;
+  const float sy = 2 * thy / (float)cam->height;
+  const float zoom = cam->zoom > 0.f ? cam->zoom : 1.f;
+  for (int i = 0; i < 3; ++i)
+  {
+    cs.dx[i] = ru[i] * sx;
+    cs.dy[i] = rv[i] * sy;
+    if (cam->zoom > 0.f)
+    {
+      cs.dx[i] = cs.dx[i] / zoom;
+      cs.dy[i] = cs.dy[i] / zoom;
+    }
+    cs.nlook[i] = look[i];
+    cs.pos[i] = cam->pos[i];
+  }
+  h_normalize (cs.nlook);
+  cs.w = cam->width;
+  cs.h = cam->height;
+  return DRB_OK;
+}
+
+__global__ void camera_rays_kernel (CamSetup cs, Ray *__restrict__ rays)
+{
+  const long long idx = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (idx >= (long long)cs.w * cs.h) return;
+  const int i = (int)(idx % cs.w);
+  const int j = (int)(idx / cs.w);
+  // (2 i - w) / 2 and (2 j - w) / 2: the reference uses the width for both
+  // (camera.cpp:469-470)
+  const float si = __fdiv_rn (__fsub_rn (__fmul_rn (2.f, (float)i), (float)cs.w), 2.0f);
+  const float sj = __fdiv_rn (__fsub_rn (__fmul_rn (2.f, (float)j), (float)cs.w), 2.0f);
+  float d[3];
+#pragma unroll
+  for (int k = 0; k < 3; ++k)
+  {
+    d[k] = __fadd_rn (__fadd_rn (cs.nlook[k], __fmul_rn (cs.dx[k], si)), __fmul_rn (cs.dy[k], sj));
+    if (d[k] == 0.f) d[k] = __fadd_rn (d[k], 0.0000001f);
+  }
+  const float m2 = __fadd_rn (__fadd_rn (__fmul_rn (d[0], d[0]), __fmul_rn (d[1], d[1])),
+                              __fmul_rn (d[2], d[2]));
+  const float mag = __fsqrt_rn (m2);
+  Ray r;
+  r.dir = make3 (__fdiv_rn (d[0], mag), __fdiv_rn (d[1], mag), __fdiv_rn (d[2], mag));
+  r.near_t = 0.f;
+  r.orig = make3 (cs.pos[0], cs.pos[1], cs.pos[2]);
+  r.far_t = INFINITY;
+  r.pixel_id = j * cs.w + i;
+  rays[idx] = r;
+}
+
+// ------------------------------------------------------------ ray culling --
+
+struct CullBox
+{
+  float mn[3], mx[3];
+};
+
+// slab test of ray.cpp:132-176 / 190-235, explicit rounding
+DRB_D bool slab (const Ray &r, const CullBox &b, float &tmin, float &tmax)
+{
+  const float inv[3] = { rcp_safe (r.dir.x), rcp_safe (r.dir.y), rcp_safe (r.dir.z) };
+  const float o[3] = { r.orig.x, r.orig.y, r.orig.z };
+  float lo[3], hi[3];
+#pragma unroll
+  for (int k = 0; k < 3; ++k)
+  {
+    const float od = __fmul_rn (o[k], inv[k]);
+    lo[k] = __fsub_rn (__fmul_rn (b.mn[k], inv[k]), od);
+    hi[k] = __fsub_rn (__fmul_rn (b.mx[k], inv[k]), od);
+  }
+  float min_dist = fmaxf (fmaxf (fmaxf (fminf (lo[1], hi[1]), fminf (lo[0], hi[0])), fminf (lo[2], hi[2])), r.near_t);
+  float max_dist = fminf (fminf (fmaxf (lo[1], hi[1]), fmaxf (lo[0], hi[0])), fmaxf (lo[2], hi[2]));
+  max_dist = fminf (max_dist, r.far_t);
+  tmin = min_dist;
+  tmax = max_dist;
+  return max_dist > min_dist;
+}
+
+__global__ void cull_flags_kernel (const Ray *__restrict__ rays, int n, CullBox b, int *__restrict__ flags)
+{
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  float t0, t1;
+  flags[i] = slab (rays[i], b, t0, t1) ? 1 : 0;
+}
+
+__global__ void cull_gather_kernel (const Ray *__restrict__ rays, int n, CullBox b,
+                                    const int *__restrict__ flags, const int *__restrict__ offs,
+                                    Ray *__restrict__ out)
+{
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n || !flags[i]) return;
+  Ray r = rays[i];
+  float t0, t1;
+  slab (r, b, t0, t1);
+  r.near_t = t0;
+  r.far_t = t1;
+  out[offs[i]] = r;
+}
+
+static CullBox cull_box (const float *bounds6)
+{
+  // AABB::scale(1.001f) about the centre (ray.cpp:120-121, range.hpp:162-172)
+  CullBox b;
+  const float s = 1.001f;
+  for (int k = 0; k < 3; ++k)
+  {
+    float mn = bounds6[2 * k], mx = bounds6[2 * k + 1];
+    if (!(mn > mx))
+    {
+      const float c = 0.5f * (mn + mx);
+      const float delta = s * 0.5f * (mx - mn);
+      mn = fminf (mn, c - delta);
+      mx = fmaxf (mx, c + delta);
+    }
+    b.mn[k] = mn;
+    b.mx[k] = mx;
+  }
+  return b;
+}
+
+// ---------------------------------------------------------- field range --
+
+__global__ void range_kernel (const float *__restrict__ v, long long n, unsigned *__restrict__ ord)
+{
+  float mn = INFINITY, mx = -INFINITY;
+  for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n;
+       i += (long long)gridDim.x * blockDim.x)
+  {
+    mn = fminf (mn, v[i]);
+    mx = fmaxf (mx, v[i]);
+  }
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1)
+  {
+    mn = fminf (mn, __shfl_xor_sync (0xffffffffu, mn, o));
+    mx = fmaxf (mx, __shfl_xor_sync (0xffffffffu, mx, o));
+  }
+  if ((threadIdx.x & 31) == 0 && mn <= mx)
+  {
+    atomicMin (ord, float_to_ordered (mn));
+    atomicMax (ord + 1, float_to_ordered (mx));
+  }
+}
+
+__global__ void range_init_kernel (unsigned *ord)
+{
+  ord[0] = float_to_ordered (INFINITY);
+  ord[1] = float_to_ordered (-INFINITY);
+}
+
+__global__ void range_finish_kernel (const unsigned *ord, float *out)
+{
+  out[0] = ordered_to_float (ord[0]);
+  out[1] = ordered_to_float (ord[1]);
+}
+
+// ------------------------------------------------------------- volume --
+
+struct VolumeParams
+{
+  LocateParams lp;            // geometry + BVH + Newton options
+  const float *field_packed;  // packed scalar rows (stride fstride) or NULL
+  const int *field_idx;
+  const float *field_vals;
+  int fstride;
+  const float4 *tf;           // transfer function (opacity corrected)
+  int tf_size;
+  float fmin, fmax, inv_range;
+  const PointLight *lights;
+  int n_lights;
+  int use_lighting;
+  int coherent;
+  float sample_dist;
+};
+
+template <int P> struct FieldCP
+{
+  const float *__restrict__ row;
+  DRB_D float operator() (int i, int) const { return __ldg (row + i); }
+};
+template <int P> struct FieldIndCP
+{
+  const int *__restrict__ idx;
+  const float *__restrict__ val;
+  DRB_D float operator() (int i, int) const { return __ldg (val + __ldg (idx + i)); }
+};
+
+// DeviceColorMap::color (device_color_map.hpp:61-78), linear scale
+DRB_D float4 colormap (const VolumeParams &vp, float s)
+{
+  s = clampf (s, vp.fmin, vp.fmax);
+  const float normalized = (s - vp.fmin) * vp.inv_range;
+  int idx = (int)(normalized * float (vp.tf_size - 1));
+  idx = min (max (idx, 0), vp.tf_size - 1);
+  return __ldg (vp.tf + idx);
+}
+
+template <int P>
+DRB_D void field_eval_d (const VolumeParams &vp, int el, const float (&r)[3], float &f, float (&g)[3])
+{
+  constexpr int ND = (P + 1) * (P + 1) * (P + 1);
+  float X[1], Ju[1], Jv[1], Jw[1];
+  if (vp.field_packed)
+  {
+    FieldCP<P> cp{ vp.field_packed + (size_t)el * vp.fstride };
+    hex_eval_d<P, 1> (cp, r[0], r[1], r[2], X, Ju, Jv, Jw);
+  }
+  else
+  {
+    FieldIndCP<P> cp{ vp.field_idx + (size_t)el * ND, vp.field_vals };
+    hex_eval_d<P, 1> (cp, r[0], r[1], r[2], X, Ju, Jv, Jw);
+  }
+  f = X[0];
+  g[0] = Ju[0];
+  g[1] = Jv[0];
+  g[2] = Jw[0];
+}
+
+// VolumeShader::color / shaded_color (volume_shader.hpp:40-167)
+template <int P>
+DRB_D float4 shade_sample (const VolumeParams &vp, int el, const float (&r)[3], const Ray &ray)
+{
+  float f, gref[3];
+  field_eval_d<P> (vp, el, r, f, gref);
+  const float4 c = colormap (vp, f);
+  if (!vp.use_lighting) return c;
+  float4 acc = make_float4 (0.f, 0.f, 0.f, 0.f);
+  if (!(c.w > 0.01f)) return acc;
+  // world position and Jacobian of the geometry
+  constexpr int ND = (P + 1) * (P + 1) * (P + 1);
+  float X[3], Ju[3], Jv[3], Jw[3];
+  if (vp.lp.packed)
+  {
+    PackedCP cp{ vp.lp.packed + (size_t)el * vp.lp.stride };
+    hex_eval_d<P, 3> (cp, r[0], r[1], r[2], X, Ju, Jv, Jw);
+  }
+  else
+  {
+    IndirectCP cp{ vp.lp.ctrl_idx + (size_t)el * ND, vp.lp.xyz, 3 };
+    hex_eval_d<P, 3> (cp, r[0], r[1], r[2], X, Ju, Jv, Jw);
+  }
+  float J[3][3];
+#pragma unroll
+  for (int k = 0; k < 3; ++k)
+  {
+    J[k][0] = Ju[k];
+    J[k][1] = Jv[k];
+    J[k][2] = Jw[k];
+  }
+  // matrix_inverse via LUP (matrix.hpp:430-456); gradient = gref * J^-1
+  LU3 lu;
+  lu.factor (J);
+  float inv[3][3];
+#pragma unroll
+  for (int c = 0; c < 3; ++c)
+  {
+    float e[3] = { 0.f, 0.f, 0.f };
+    e[c] = 1.f;
+    float col[3];
+    lu.solve (e, col);
+#pragma unroll
+    for (int rr = 0; rr < 3; ++rr) inv[rr][c] = col[rr];
+  }
+  Vec3 g;
+  g.x = gref[0] * inv[0][0] + gref[1] * inv[1][0] + gref[2] * inv[2][0];
+  g.y = gref[0] * inv[0][1] + gref[1] * inv[1][1] + gref[2] * inv[2][1];
+  g.z = gref[0] * inv[0][2] + gref[1] * inv[1][2] + gref[2] * inv[2][2];
+  {
+    const float m = sqrtf (dot (g, g));
+    g = make3 (g.x / m, g.y / m, g.z / m);
+  }
+  const Vec3 view = make3 (-ray.dir.x, -ray.dir.y, -ray.dir.z);
+  const Vec3 wp = make3 (X[0], X[1], X[2]);
+  for (int l = 0; l < vp.n_lights; ++l)
+  {
+    const PointLight L = vp.lights[l];
+    Vec3 ld = make3 (L.pos[0] - wp.x, L.pos[1] - wp.y, L.pos[2] - wp.z);
+    {
+      const float m = sqrtf (dot (ld, ld));
+      ld = make3 (ld.x / m, ld.y / m, ld.z / m);
+    }
+    if (dot (ld, g) < 0.f) g = make3 (-g.x, -g.y, -g.z);
+    const float diffuse = clampf (dot (ld, g), 0.f, 1.f);
+    float sc[4] = { L.amb[0] * c.x, L.amb[1] * c.y, L.amb[2] * c.z, c.w };
+    const float cc[3] = { c.x, c.y, c.z };
+#pragma unroll
+    for (int k = 0; k < 3; ++k) sc[k] += diffuse * L.diff[k] * cc[k];
+    Vec3 hv = 0.5f * (view + ld);
+    {
+      const float m = sqrtf (dot (hv, hv));
+      hv = make3 (hv.x / m, hv.y / m, hv.z / m);
+    }
+    if (dot (g, hv) < 0.f) g = make3 (-g.x, -g.y, -g.z);
+    const float doth = clampf (dot (g, hv), 0.f, 1.f);
+    const float intensity = powf (doth, L.spec_pow);
+#pragma unroll
+    for (int k = 0; k < 3; ++k) sc[k] += intensity * L.spec[k] * cc[k];
+    acc.x = clampf (acc.x + sc[0], 0.f, 1.f);
+    acc.y = clampf (acc.y + sc[1], 0.f, 1.f);
+    acc.z = clampf (acc.z + sc[2], 0.f, 1.f);
+    acc.w = acc.w + sc[3];
+  }
+  return acc;
+}
+
+DRB_D void blend (float4 &front, const float4 &back)
+{
+  const float alpha = back.w * (1.f - front.w);
+  front.x = front.x + back.x * alpha;
+  front.y = front.y + back.y * alpha;
+  front.z = front.z + back.z * alpha;
+  front.w = alpha + front.w;
+}
+
+// Locate one sample: coherent first try in the previous element, then the
+// full BVH locate (same acceptance rule either way).
+template <int P>
+DRB_D int locate_sample (const VolumeParams &vp, const float (&pt)[3], int prev_el,
+                         const float (&prev_ref)[3], float (&ref)[3], int &iters, int &cands,
+                         int &nodes)
+{
+  if (vp.coherent && prev_el >= 0)
+  {
+    float x[3] = { prev_ref[0], prev_ref[1], prev_ref[2] };
+    int steps = 0;
+    ++cands;
+    const bool found = solve_in_element<P> (vp.lp, prev_el, pt, x, steps);
+    iters += steps;
+    if (found)
+    {
+      ref[0] = x[0];
+      ref[1] = x[1];
+      ref[2] = x[2];
+      return prev_el;
+    }
+  }
+  return locate_point<P> (vp.lp, 0, pt, ref, iters, cands, nodes);
+}
+
+template <int P>
+__global__ void __launch_bounds__ (128)
+volume_kernel (VolumeParams vp, const Ray *__restrict__ rays, int n_rays, int *__restrict__ queue,
+               VolumePartial *__restrict__ partials, float4 *__restrict__ fb_color,
+               float *__restrict__ fb_depth, int *__restrict__ ray_samples,
+               int *__restrict__ ray_iters, int *__restrict__ ray_cands)
+{
+  constexpr int kMaxSegments = 5; // volume.cpp:110
+  const unsigned FULL = 0xffffffffu;
+  const int lane = threadIdx.x & 31;
+  while (true)
+  {
+    int base = 0;
+    if (lane == 0) base = atomicAdd (queue, 32);
+    base = __shfl_sync (FULL, base, 0);
+    if (base >= n_rays) break;
+    const int i = base + lane;
+    if (i >= n_rays) continue;
+    const Ray ray = rays[i];
+    float distance = ray.near_t + vp.sample_dist;
+    int segment = 0;
+    float4 pixel = make_float4 (0.f, 0.f, 0.f, 0.f);
+    float first_depth = INFINITY;
+    int n_samples = 0, iters = 0, cands = 0, nodes = 0;
+    int prev_el = -1;
+    float prev_ref[3] = { 0.5f, 0.5f, 0.5f };
+    for (int s = 0; s < kMaxSegments; ++s)
+    {
+      bool found = false;
+      int el = -1;
+      float ref[3];
+      while (distance < ray.far_t && !found)
+      {
+        const float pt[3] = { ray.orig.x + distance * ray.dir.x, ray.orig.y + distance * ray.dir.y,
+                              ray.orig.z + distance * ray.dir.z };
+        el = locate_sample<P> (vp, pt, prev_el, prev_ref, ref, iters, cands, nodes);
+        if (el != -1) found = true;
+        else distance += vp.sample_dist;
+        prev_el = el;
+      }
+      if (distance >= ray.far_t) break;
+      VolumePartial part;
+      part.pixel_id = ray.pixel_id;
+      part.depth = distance;
+      float4 color = make_float4 (0.f, 0.f, 0.f, 0.f);
+      do
+      {
+        ++n_samples;
+        const float4 sc = shade_sample<P> (vp, el, ref, ray);
+        blend (color, sc);
+        prev_el = el;
+        prev_ref[0] = ref[0];
+        prev_ref[1] = ref[1];
+        prev_ref[2] = ref[2];
+        distance += vp.sample_dist;
+        const float pt[3] = { ray.orig.x + distance * ray.dir.x, ray.orig.y + distance * ray.dir.y,
+                              ray.orig.z + distance * ray.dir.z };
+        el = locate_sample<P> (vp, pt, prev_el, prev_ref, ref, iters, cands, nodes);
+        found = el != -1;
+        if (!found) prev_el = -1;
+      } while (distance < ray.far_t && found && color.w < 0.95f);
+      part.color[0] = color.x;
+      part.color[1] = color.y;
+      part.color[2] = color.z;
+      part.color[3] = color.w;
+      if (partials) partials[(size_t)kMaxSegments * i + segment] = part;
+      // fused Volume::save compositing: partials of one ray arrive in depth
+      // order, the first one sets the pixel, later ones blend behind it
+      if (segment == 0)
+      {
+        pixel = color;
+        first_depth = part.depth;
+      }
+      else
+      {
+        const float a = 1.f - pixel.w;
+        pixel.x = pixel.x + color.x * a;
+        pixel.y = pixel.y + color.y * a;
+        pixel.z = pixel.z + color.z * a;
+        pixel.w = pixel.w + color.w * a;
+      }
+      ++segment;
+      if (distance >= ray.far_t || color.w > 0.95f) break;
+    }
+    if (fb_color && segment > 0)
+    {
+      fb_color[ray.pixel_id] = pixel;
+      if (fb_depth) fb_depth[ray.pixel_id] = first_depth;
+    }
+    if (ray_samples) ray_samples[i] = n_samples;
+    if (ray_iters) ray_iters[i] = iters;
+    if (ray_cands) ray_cands[i] = cands;
+  }
+}
+
+__global__ void init_partials_kernel (VolumePartial *p, long long n)
+{
+  const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  VolumePartial v;
+  v.pixel_id = -1;
+  v.depth = INFINITY;
+  v.color[0] = v.color[1] = v.color[2] = v.color[3] = 0.f;
+  p[i] = v;
+}
+
+__global__ void partial_flags_kernel (const VolumePartial *p, int n, int *flags)
+{
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < n) flags[i] = (p[i].depth == INFINITY) ? 0 : 1;
+}
+
+__global__ void partial_gather_kernel (const VolumePartial *p, int n, const int *flags,
+                                       const int *offs, VolumePartial *out)
+{
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < n && flags[i]) out[offs[i]] = p[i];
+}
+
+// Volume::save compositing over partials sorted by pixel then depth
+__global__ void composite_partials_kernel (const VolumePartial *p, int n, float4 *fb)
+{
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const int pix = p[i].pixel_id;
+  if (i > 0 && p[i - 1].pixel_id == pix) return; // not the first of its run
+  float4 c = make_float4 (p[i].color[0], p[i].color[1], p[i].color[2], p[i].color[3]);
+  for (int k = i + 1; k < n && p[k].pixel_id == pix; ++k)
+  {
+    const float a = 1.f - c.w;
+    c.x = c.x + p[k].color[0] * a;
+    c.y = c.y + p[k].color[1] * a;
+    c.z = c.z + p[k].color[2] * a;
+    c.w = c.w + p[k].color[3] * a;
+  }
+  fb[pix] = c;
+}
+
+__global__ void fb_clear_kernel (float4 *c, float *d, int n, float4 v)
+{
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  c[i] = v;
+  if (d) d[i] = INFINITY;
+}
+
+__global__ void fb_background_kernel (float4 *c, int n, float4 bg)
+{
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  float4 v = c[i];
+  if (v.w < 1.f)
+  {
+    // blend_pre_alpha (colors.hpp:25-33)
+    const float a = 1.f - v.w;
+    v.x = v.x + bg.x * a;
+    v.y = v.y + bg.y * a;
+    v.z = v.z + bg.z * a;
+    v.w = v.w + bg.w * a;
+    c[i] = v;
+  }
+}
+
+template <int P>
+int launch_volume (const VolumeParams &vp, const Ray *rays, int n, int *queue,
+                   VolumePartial *partials, float4 *fb, float *depth, const drb_ray_stats &st,
+                   cudaStream_t s)
+{
+  int nb = 0;
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor (&nb, volume_kernel<P>, 128, 0);
+  if (nb < 1) nb = 1;
+  long long blocks = (long long)nb * sm_count ();
+  const long long need = ((long long)n + 127) / 128;
+  if (blocks > need) blocks = need;
+  if (blocks < 1) blocks = 1;
+  volume_kernel<P><<<(unsigned)blocks, 128, 0, s>>> (vp, rays, n, queue, partials, fb, depth,
+                                                     st.samples, st.iters, st.candidates);
+  return check_launch ("volume_kernel");
+}
+
+} // namespace drb
+
+using namespace drb;
+
+// ------------------------------------------------------------- C-ABI --
+
+extern "C" int drb_camera_rays (const drb_camera *cam, void *rays, void *stream)
+{
+  CamSetup cs;
+  int st = camera_setup (cam, cs);
+  if (st) return st;
+  if (!rays)
+  {
+    set_last_error ("camera_rays: rays is NULL");
+    return DRB_ERR_INVALID_ARG;
+  }
+  const long long n = (long long)cs.w * cs.h;
+  camera_rays_kernel<<<div_up (n, 256), 256, 0, (cudaStream_t)stream>>> (cs, (Ray *)rays);
+  return check_launch ("camera_rays_kernel");
+}
+
+// detail::default_light (rendering/renderer.cpp:141-159): a point light
+// above the camera; host float arithmetic.  light13 = pos3, amb3, diff3,
+// spec3, spec_pow with the PointLight defaults (rendering/point_light.hpp).
+extern "C" int drb_default_light (const drb_camera *cam, float *light13)
+{
+  if (!cam || !light13)
+  {
+    set_last_error ("default_light: bad arguments");
+    return DRB_ERR_INVALID_ARG;
+  }
+  float up[3] = { cam->up[0], cam->up[1], cam->up[2] };
+  h_normalize (up); // Camera::set_up
+  h_normalize (up); // default_light normalises again
+  float look[3];
+  for (int i = 0; i < 3; ++i) look[i] = cam->look_at[i] - cam->pos[i];
+  const float mag = h_mag (look);
+  float right[3], mup[3];
+  h_cross (look, up, right);
+  h_normalize (right);
+  h_cross (right, look, mup);
+  h_normalize (mup);
+  for (int i = 0; i < 3; ++i) light13[i] = cam->pos[i] + .1f * mag * mup[i];
+  const float amb = 0.4f, diff = 0.75f, spec = 0.8f;
+  for (int i = 0; i < 3; ++i)
+  {
+    light13[3 + i] = amb;
+    light13[6 + i] = diff;
+    light13[9 + i] = spec;
+  }
+  light13[12] = 15.f;
+  return DRB_OK;
+}
+
+extern "C" int drb_cull_rays (const void *rays, int n, const float *bounds6, void *active_rays,
+                              int *n_active, void *stream)
+{
+  if (n < 0 || (n > 0 && (!rays || !bounds6 || !active_rays || !n_active)))
+  {
+    set_last_error ("cull_rays: bad arguments");
+    return DRB_ERR_INVALID_ARG;
+  }
+  if (n == 0)
+  {
+    *n_active = 0;
+    return DRB_OK;
+  }
+  cudaStream_t s = (cudaStream_t)stream;
+  const CullBox b = cull_box (bounds6);
+  Scratch scr (s);
+  int *flags = scr.alloc<int> (n);
+  int *offs = scr.alloc<int> (n);
+  int *total = scr.alloc<int> (1);
+  if (scr.err != cudaSuccess) return status_from (scr.err);
+  cull_flags_kernel<<<div_up (n, 256), 256, 0, s>>> ((const Ray *)rays, n, b, flags);
+  int st = check_launch ("cull_flags_kernel");
+  if (st) return st;
+  st = exclusive_scan_i32 (flags, offs, n, total, s);
+  if (st) return st;
+  cull_gather_kernel<<<div_up (n, 256), 256, 0, s>>> ((const Ray *)rays, n, b, flags, offs, (Ray *)active_rays);
+  st = check_launch ("cull_gather_kernel");
+  if (st) return st;
+  int h = 0;
+  cudaError_t e = cudaMemcpyAsync (&h, total, sizeof (int), cudaMemcpyDeviceToHost, s);
+  if (e == cudaSuccess) e = cudaStreamSynchronize (s);
+  if (e != cudaSuccess) return status_from (e);
+  *n_active = h;
+  return DRB_OK;
+}
+
+extern "C" int drb_field_range (const drb_mesh *field, float *range2, void *stream)
+{
+  if (!field || !range2 || field->ncomp != 1 || field->n_ctrl < 0 || (field->n_ctrl > 0 && !field->values))
+  {
+    set_last_error ("field_range: needs a scalar field");
+    return DRB_ERR_INVALID_ARG;
+  }
+  cudaStream_t s = (cudaStream_t)stream;
+  Scratch scr (s);
+  unsigned *ord = scr.alloc<unsigned> (2);
+  if (!ord) return status_from (scr.err);
+  range_init_kernel<<<1, 1, 0, s>>> (ord);
+  int st = check_launch ("range_init_kernel");
+  if (st) return st;
+  if (field->n_ctrl > 0)
+  {
+    const int blocks = min (div_up (field->n_ctrl, 256), sm_count () * 8);
+    range_kernel<<<blocks, 256, 0, s>>> (field->values, field->n_ctrl, ord);
+    if ((st = check_launch ("range_kernel"))) return st;
+  }
+  range_finish_kernel<<<1, 1, 0, s>>> (ord, range2);
+  return check_launch ("range_finish_kernel");
+}
+
+// ColorTable::sample with correct_opacity (color_table.cpp:152-323): host.
+extern "C" int drb_color_table_sample (int n_rgb, const float *rgb_pts, int n_alpha,
+                                       const float *alpha_pts, int smooth, int n_samples,
+                                       float alpha_scale, float opacity_factor, float *rgba)
+{
+  if (n_samples < 1 || !rgba || n_rgb < 0 || n_alpha < 0 || (n_rgb > 0 && !rgb_pts) ||
+      (n_alpha > 0 && !alpha_pts))
+  {
+    set_last_error ("color_table_sample: bad arguments");
+    return DRB_ERR_INVALID_ARG;
+  }
+  std::vector<float> apos (n_alpha), aval (n_alpha);
+  for (int i = 0; i < n_alpha; ++i)
+  {
+    apos[i] = alpha_pts[2 * i];
+    aval[i] = alpha_pts[2 * i + 1];
+    if (opacity_factor > 0.f) aval[i] = 1.f - powf ((1.f - aval[i]), opacity_factor);
+  }
+  for (int i = 0; i < n_samples; ++i)
+  {
+    const float scalar = n_samples > 1 ? static_cast<float> (i) / static_cast<float> (n_samples - 1) : 0.f;
+    float c[4] = { 0.5f, 0.5f, 0.5f, 1.f };
+    // map_rgb
+    if (n_rgb > 0)
+    {
+      if (n_rgb == 1 || scalar <= rgb_pts[0])
+      {
+        for (int k = 0; k < 3; ++k) c[k] = rgb_pts[1 + k];
+        c[3] = 1.f;
+      }
+      else if (scalar >= rgb_pts[4 * (n_rgb - 1)])
+      {
+        for (int k = 0; k < 3; ++k) c[k] = rgb_pts[4 * (n_rgb - 1) + 1 + k];
+        c[3] = 1.f;
+      }
+      else
+      {
+        int second;
+        for (second = 1; second < n_rgb - 1; ++second)
+          if (scalar < rgb_pts[4 * second]) break;
+        const int first = second - 1;
+        const float seg = rgb_pts[4 * second] - rgb_pts[4 * first];
+        const float alpha = (seg == 0.f) ? .5f : (scalar - rgb_pts[4 * first]) / seg;
+        for (int k = 0; k < 3; ++k)
+        {
+          const float a = rgb_pts[4 * first + 1 + k], b = rgb_pts[4 * second + 1 + k];
+          c[k] = smooth ? (a * (1.0f - alpha) + b * alpha) : (alpha < .5 ? a : b);
+        }
+        c[3] = smooth ? (1.f * (1.0f - alpha) + 1.f * alpha) : 1.f;
+      }
+    }
+    // map_alpha
+    float av = 1.f;
+    if (n_alpha > 0)
+    {
+      if (n_alpha == 1 || scalar <= apos[0]) av = aval[0];
+      else if (scalar >= apos[n_alpha - 1]) av = aval[n_alpha - 1];
+      else
+      {
+        int second;
+        for (second = 1; second < n_alpha - 1; ++second)
+          if (scalar < apos[second]) break;
+        const int first = second - 1;
+        const float seg = apos[second] - apos[first];
+        const float alpha = (seg == 0.f) ? .5f : (scalar - apos[first]) / seg;
+        av = smooth ? (aval[first] * (1.f - alpha) + aval[second] * alpha)
+                    : (alpha < .5 ? aval[first] : aval[second]);
+      }
+    }
+    c[3] = av * alpha_scale;
+    for (int k = 0; k < 4; ++k) rgba[4 * i + k] = c[k];
+  }
+  return DRB_OK;
+}
+
+static int volume_common (const drb_mesh *mesh, const drb_mesh *field, const drb_bvh *bvh,
+                          const void *active_rays, int n_rays, const drb_volume_opts *o,
+                          const float *tf, int tf_size, const float *range2,
+                          const void *lights, int n_lights, VolumeParams &vp)
+{
+  if (!mesh || !field || !bvh || !o || n_rays < 0 || (n_rays > 0 && !active_rays) || !tf ||
+      tf_size < 1 || !range2 || n_lights < 0 || (n_lights > 0 && !lights))
+  {
+    set_last_error ("volume: bad arguments");
+    return DRB_ERR_INVALID_ARG;
+  }
+  if (mesh->dim != 3 || mesh->ncomp != 3 || field->dim != 3 || field->ncomp != 1 ||
+      mesh->order != field->order || mesh->n_elem != field->n_elem || mesh->order < 1 ||
+      mesh->order > 3)
+  {
+    set_last_error ("volume: needs a hex mesh and a scalar hex field of the same order 1..3");
+    return DRB_ERR_UNSUPPORTED;
+  }
+  if (o->samples < 1 || !(o->tol > 0.f) || o->max_steps < 0)
+  {
+    set_last_error ("volume: samples >= 1, tol > 0, max_steps >= 0 required");
+    return DRB_ERR_INVALID_ARG;
+  }
+  drb_newton_opts no;
+  no.tol = o->tol;
+  no.max_steps = o->max_steps;
+  no.guess_mode = o->guess_mode == DRB_GUESS_GIVEN ? DRB_GUESS_ELEM_CENTER : o->guess_mode;
+  no.guess = nullptr;
+  LocateParams &lp = vp.lp;
+  lp.nodes = (const float4 *)bvh->inner_nodes;
+  lp.leaf_nodes = bvh->leaf_nodes;
+  lp.aabb_ids = bvh->aabb_ids;
+  lp.ref_boxes = bvh->ref_boxes;
+  lp.packed = mesh->packed;
+  lp.ctrl_idx = mesh->ctrl_idx;
+  lp.xyz = mesh->values;
+  const int nd = (mesh->order + 1) * (mesh->order + 1) * (mesh->order + 1);
+  lp.stride = packed_stride (nd, 3);
+  lp.tol = no.tol;
+  lp.max_steps = no.max_steps;
+  lp.guess_mode = no.guess_mode;
+  lp.guess = nullptr;
+  vp.field_packed = field->packed;
+  vp.field_idx = field->ctrl_idx;
+  vp.field_vals = field->values;
+  vp.fstride = packed_stride (nd, 1);
+  vp.tf = (const float4 *)tf;
+  vp.tf_size = tf_size;
+  // DeviceColorMap: range of the field's control values, rcp_safe(length)
+  vp.fmin = range2[0];
+  vp.fmax = range2[1];
+  {
+    float len = vp.fmax - vp.fmin;
+    float g = (fabsf (len) < 1e-8f) ? (std::signbit (len) ? -1e-8f : 1e-8f) : len;
+    vp.inv_range = 1.0f / g;
+  }
+  vp.lights = (const PointLight *)lights;
+  vp.n_lights = n_lights;
+  vp.use_lighting = o->use_lighting;
+  vp.coherent = o->coherent;
+  // sample distance: |bounds diagonal| / samples (volume.cpp:89-91)
+  const float *b = o->bounds;
+  float dd[3] = { b[1] - b[0], b[3] - b[2], b[5] - b[4] };
+  const float mag = h_mag (dd);
+  vp.sample_dist = mag / float (o->samples);
+  return DRB_OK;
+}
+
+extern "C" int drb_volume_integrate (const drb_mesh *mesh, const drb_mesh *field,
+                                     const drb_bvh *bvh, const void *active_rays, int n_rays,
+                                     const drb_volume_opts *opts, const float *tf, int tf_size,
+                                     const float *range2, const void *lights, int n_lights,
+                                     void *partials, int *n_partials, drb_ray_stats stats,
+                                     void *stream)
+{
+  VolumeParams vp;
+  int st = volume_common (mesh, field, bvh, active_rays, n_rays, opts, tf, tf_size, range2,
+                          lights, n_lights, vp);
+  if (st) return st;
+  if (!partials || !n_partials)
+  {
+    set_last_error ("volume_integrate: partials and n_partials are required");
+    return DRB_ERR_INVALID_ARG;
+  }
+  if (n_rays == 0)
+  {
+    *n_partials = 0;
+    return DRB_OK;
+  }
+  cudaStream_t s = (cudaStream_t)stream;
+  const long long np = 5ll * n_rays;
+  if (np >= (1ll << 31))
+  {
+    set_last_error ("volume_integrate: too many rays for int32 partial indices");
+    return DRB_ERR_INVALID_ARG;
+  }
+  Scratch scr (s);
+  VolumePartial *raw = scr.alloc<VolumePartial> (np);
+  int *flags = scr.alloc<int> (np);
+  int *offs = scr.alloc<int> (np);
+  int *total = scr.alloc<int> (1);
+  int *queue = scr.alloc<int> (1);
+  if (scr.err != cudaSuccess) return status_from (scr.err);
+  init_partials_kernel<<<div_up (np, 256), 256, 0, s>>> (raw, np);
+  if ((st = check_launch ("init_partials_kernel"))) return st;
+  cudaMemsetAsync (queue, 0, sizeof (int), s);
+  const Ray *rays = (const Ray *)active_rays;
+  if (mesh->order == 1) st = launch_volume<1> (vp, rays, n_rays, queue, raw, nullptr, nullptr, stats, s);
+  else if (mesh->order == 2) st = launch_volume<2> (vp, rays, n_rays, queue, raw, nullptr, nullptr, stats, s);
+  else st = launch_volume<3> (vp, rays, n_rays, queue, raw, nullptr, nullptr, stats, s);
+  if (st) return st;
+  // compact_partials (volume.cpp:42-67)
+  partial_flags_kernel<<<div_up (np, 256), 256, 0, s>>> (raw, (int)np, flags);
+  if ((st = check_launch ("partial_flags_kernel"))) return st;
+  if ((st = exclusive_scan_i32 (flags, offs, (int)np, total, s))) return st;
+  partial_gather_kernel<<<div_up (np, 256), 256, 0, s>>> (raw, (int)np, flags, offs, (VolumePartial *)partials);
+  if ((st = check_launch ("partial_gather_kernel"))) return st;
+  int h = 0;
+  cudaError_t e = cudaMemcpyAsync (&h, total, sizeof (int), cudaMemcpyDeviceToHost, s);
+  if (e == cudaSuccess) e = cudaStreamSynchronize (s);
+  if (e != cudaSuccess) return status_from (e);
+  *n_partials = h;
+  return DRB_OK;
+}
+
+extern "C" int drb_volume_render (const drb_mesh *mesh, const drb_mesh *field, const drb_bvh *bvh,
+                                  const void *active_rays, int n_rays,
+                                  const drb_volume_opts *opts, const float *tf, int tf_size,
+                                  const float *range2, const void *lights, int n_lights,
+                                  float *fb_rgba, float *fb_depth, drb_ray_stats stats,
+                                  void *stream)
+{
+  VolumeParams vp;
+  int st = volume_common (mesh, field, bvh, active_rays, n_rays, opts, tf, tf_size, range2,
+                          lights, n_lights, vp);
+  if (st) return st;
+  if (!fb_rgba)
+  {
+    set_last_error ("volume_render: fb_rgba is required");
+    return DRB_ERR_INVALID_ARG;
+  }
+  if (n_rays == 0) return DRB_OK;
+  cudaStream_t s = (cudaStream_t)stream;
+  Scratch scr (s);
+  int *queue = scr.alloc<int> (1);
+  if (!queue) return status_from (scr.err);
+  cudaMemsetAsync (queue, 0, sizeof (int), s);
+  const Ray *rays = (const Ray *)active_rays;
+  float4 *fb = (float4 *)fb_rgba;
+  if (mesh->order == 1) st = launch_volume<1> (vp, rays, n_rays, queue, nullptr, fb, fb_depth, stats, s);
+  else if (mesh->order == 2) st = launch_volume<2> (vp, rays, n_rays, queue, nullptr, fb, fb_depth, stats, s);
+  else st = launch_volume<3> (vp, rays, n_rays, queue, nullptr, fb, fb_depth, stats, s);
+  return st;
+}
+
+extern "C" int drb_composite_partials (const void *partials, int n, float *fb_rgba, void *stream)
+{
+  if (n < 0 || (n > 0 && (!partials || !fb_rgba)))
+  {
+    set_last_error ("composite_partials: bad arguments");
+    return DRB_ERR_INVALID_ARG;
+  }
+  if (n == 0) return DRB_OK;
+  composite_partials_kernel<<<div_up (n, 256), 256, 0, (cudaStream_t)stream>>> (
+  (const VolumePartial *)partials, n, (float4 *)fb_rgba);
+  return check_launch ("composite_partials_kernel");
+}
+
+extern "C" int drb_framebuffer_clear (float *rgba, float *depth, int n_pixels, const float *color4,
+                                      void *stream)
+{
+  if (n_pixels < 0 || (n_pixels > 0 && !rgba))
+  {
+    set_last_error ("framebuffer_clear: bad arguments");
+    return DRB_ERR_INVALID_ARG;
+  }
+  if (n_pixels == 0) return DRB_OK;
+  const float4 c = color4 ? make_float4 (color4[0], color4[1], color4[2], color4[3])
+                          : make_float4 (0.f, 0.f, 0.f, 0.f);
+  fb_clear_kernel<<<div_up (n_pixels, 256), 256, 0, (cudaStream_t)stream>>> ((float4 *)rgba, depth, n_pixels, c);
+  return check_launch ("fb_clear_kernel");
+}
+
+extern "C" int drb_framebuffer_composite_background (float *rgba, int n_pixels,
+                                                     const float *bg4, void *stream)
+{
+  if (n_pixels < 0 || (n_pixels > 0 && !rgba))
+  {
+    set_last_error ("framebuffer_composite_background: bad arguments");
+    return DRB_ERR_INVALID_ARG;
+  }
+  if (n_pixels == 0) return DRB_OK;
+  const float4 c = bg4 ? make_float4 (bg4[0], bg4[1], bg4[2], bg4[3]) : make_float4 (1.f, 1.f, 1.f, 1.f);
+  fb_background_kernel<<<div_up (n_pixels, 256), 256, 0, (cudaStream_t)stream>>> ((float4 *)rgba, n_pixels, c);
+  return check_launch ("fb_background_kernel");
+}

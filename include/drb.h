@@ -91,10 +91,13 @@ typedef struct drb_query_stats
 {
   int *iters;            /* device int32[n]: Newton iterations summed over candidates, or NULL */
   int *candidates;       /* device int32[n]: leaves whose box held the query, or NULL */
+  int *nodes;            /* device int32[n]: inner BVH nodes visited, or NULL */
 } drb_query_stats;
 
 const char *drb_last_error (void);
 int drb_version (void);
+/* Number of kernels this library has launched in the process (all threads). */
+unsigned long long drb_kernel_launches (void);
 
 /* Floats per element in a packed element-major copy (padded to float4). */
 int drb_packed_stride (int dim, int order, int ncomp);
@@ -142,6 +145,139 @@ int drb_lbvh_build (const drb_mesh *mesh, drb_bvh *bvh, unsigned *sorted_codes, 
 int drb_locate (const drb_mesh *mesh, const drb_bvh *bvh, const float *pts, int n,
                 const drb_newton_opts *opts, int *cell, float *ref, drb_query_stats stats,
                 void *stream);
+
+/* Launch shape of the persistent point-location kernel (chosen by
+ * drb_locate_tune; no counterpart in the reference, which launches one
+ * thread per point in 128-thread blocks, policies.hpp:17-21). */
+typedef struct drb_locate_config
+{
+  int block;             /* threads per block, multiple of 32 */
+  int blocks_per_sm;     /* resident blocks per SM, 0 = as many as fit */
+  int chunk;             /* queries a warp pops from the global queue at once */
+  int sort_queries;      /* 1 = process the queries in Morton order */
+} drb_locate_config;
+
+/* Batched point location, same results as drb_locate (same traversal order
+ * and per-candidate solves per point): queries Morton-sorted, persistent
+ * warps popping chunks from a global atomic queue, idle lanes refilled by
+ * ballot ranking, Newton solves of a warp run converged.  cfg NULL = default.
+ * Replaces UnstructuredMesh::locate (data_model/unstructured_mesh.cpp:124-148). */
+int drb_locate_batched (const drb_mesh *mesh, const drb_bvh *bvh, const float *pts, int n,
+                        const drb_newton_opts *opts, const drb_locate_config *cfg, int *cell,
+                        float *ref, drb_query_stats stats, void *stream);
+
+/* Morton order of query points over the BVH bounds: device int32 order[n]
+ * (a permutation of 0..n-1).  No reference counterpart (it never reorders). */
+int drb_query_order (const drb_bvh *bvh, const float *pts, int n, int *order, void *stream);
+
+/* drb_locate_batched with a caller-supplied processing order (e.g. from
+ * drb_query_order, reused across calls on the same queries). */
+int drb_locate_ordered (const drb_mesh *mesh, const drb_bvh *bvh, const float *pts, int n,
+                        const int *order, const drb_newton_opts *opts,
+                        const drb_locate_config *cfg, int *cell, float *ref,
+                        drb_query_stats stats, void *stream);
+
+/* Autotuner of the persistent kernel: times every candidate launch shape on
+ * a query sample (CUDA events, synchronous) and returns the fastest in
+ * *best and its time in *best_ms (may be NULL).  No reference counterpart. */
+int drb_locate_tune (const drb_mesh *mesh, const drb_bvh *bvh, const float *pts, int n,
+                     const drb_newton_opts *opts, drb_locate_config *best, float *best_ms,
+                     void *stream);
+
+/* ------------------------------------------------------------ rendering */
+
+/* Ray records are dray::Ray (ray.hpp:20-27): dir[3], near, orig[3], far,
+ * int32 pixel_id = 36 bytes.  Partials are dray::VolumePartial
+ * (rendering/volume_partial.hpp): int32 pixel, depth, rgba = 24 bytes.
+ * Point lights are dray::PointLight (rendering/point_light.hpp): pos, amb,
+ * diff, spec (3 floats each), spec_pow = 52 bytes. */
+
+/* Camera state of dray::Camera (rendering/camera.hpp:18-118). */
+typedef struct drb_camera
+{
+  int width, height;
+  float pos[3];
+  float look_at[3];
+  float up[3];
+  float fov_y;            /* degrees; fov_x follows from the aspect (camera.cpp:132-163) */
+  float zoom;             /* 1 = none */
+} drb_camera;
+
+/* Per-ray counters of the renderers (device int32[n] each, or NULL). */
+typedef struct drb_ray_stats
+{
+  int *samples;           /* volume: samples that located (Newton-resolved) */
+  int *iters;             /* Newton iterations */
+  int *candidates;        /* candidate elements tried */
+} drb_ray_stats;
+
+/* Volume::integrate options (rendering/volume.hpp:19-59). */
+typedef struct drb_volume_opts
+{
+  int samples;            /* Volume::samples: steps over the bounds diagonal */
+  int use_lighting;       /* Blinn-Phong from the field gradient */
+  float tol;              /* Newton tolerance (reference: 1e-4) */
+  int max_steps;          /* Newton steps (reference: 20) */
+  int guess_mode;         /* drb_guess_mode for full locates */
+  int coherent;           /* 1: try the previous sample's element first */
+  float bounds[6];        /* Collection::bounds of the data (sample distance) */
+} drb_volume_opts;
+
+/* Camera::create_rays / gen_perspective (rendering/camera.cpp:219-483):
+ * width*height rays, pixel id j*width+i.  rays: device dray::Ray[w*h]. */
+int drb_camera_rays (const drb_camera *cam, void *rays, void *stream);
+
+/* detail::default_light (rendering/renderer.cpp:141-159) on the host:
+ * light13 = pos[3], amb[3], diff[3], spec[3], spec_pow (PointLight defaults). */
+int drb_default_light (const drb_camera *cam, float *light13);
+
+/* remove_missed_rays (ray.cpp:102-115): keep rays hitting bounds6 scaled by
+ * 1.001, in order, with near/far set by calc_ray_start (ray.cpp:183-241).
+ * Synchronises the stream to return *n_active. */
+int drb_cull_rays (const void *rays, int n, const float *bounds6, void *active_rays,
+                   int *n_active, void *stream);
+
+/* Range of a scalar field's control values (get_range,
+ * data_model/unstructured_field.cpp:35-80): range2 device float[2]. */
+int drb_field_range (const drb_mesh *field, float *range2, void *stream);
+
+/* ColorTable::sample after correct_opacity(opacity_factor)
+ * (color_table.cpp:152-323); host arrays, no GPU.  rgb_pts n x (pos,r,g,b),
+ * alpha_pts n x (pos,a); opacity_factor <= 0 skips the correction. */
+int drb_color_table_sample (int n_rgb, const float *rgb_pts, int n_alpha, const float *alpha_pts,
+                            int smooth, int n_samples, float alpha_scale, float opacity_factor,
+                            float *rgba);
+
+/* Volume::integrate (rendering/volume.cpp:71-228, 324-348) over culled
+ * rays: partials compacted in ray then depth order (device
+ * dray::VolumePartial[5*n_rays] capacity); *n_partials returned after a
+ * stream synchronise.  tf: device float4[tf_size] (opacity corrected);
+ * range2: host float[2] scalar range; lights: device PointLight[n_lights]. */
+int drb_volume_integrate (const drb_mesh *mesh, const drb_mesh *field, const drb_bvh *bvh,
+                          const void *active_rays, int n_rays, const drb_volume_opts *opts,
+                          const float *tf, int tf_size, const float *range2, const void *lights,
+                          int n_lights, void *partials, int *n_partials, drb_ray_stats stats,
+                          void *stream);
+
+/* Volume::integrate fused with the compositing of Volume::save
+ * (volume.cpp:369-416): writes the composited colour of every pixel with a
+ * partial into fb_rgba (device float4[w*h], cleared by the caller) and the
+ * first partial's depth into fb_depth (may be NULL).  No partial buffer. */
+int drb_volume_render (const drb_mesh *mesh, const drb_mesh *field, const drb_bvh *bvh,
+                       const void *active_rays, int n_rays, const drb_volume_opts *opts,
+                       const float *tf, int tf_size, const float *range2, const void *lights,
+                       int n_lights, float *fb_rgba, float *fb_depth, drb_ray_stats stats,
+                       void *stream);
+
+/* Volume::save compositing of partials sorted by pixel then depth. */
+int drb_composite_partials (const void *partials, int n, float *fb_rgba, void *stream);
+
+/* Framebuffer::clear / composite_background (rendering/framebuffer.cpp:126-162).
+ * color4/bg4 are host float[4]; NULL = (0,0,0,0) / white. */
+int drb_framebuffer_clear (float *rgba, float *depth, int n_pixels, const float *color4,
+                           void *stream);
+int drb_framebuffer_composite_background (float *rgba, int n_pixels, const float *bg4,
+                                          void *stream);
 
 #ifdef __cplusplus
 }

@@ -77,7 +77,7 @@ def test_locate_tol_1e5_vs_restated_and_fp64(cuda, name, guess):
         pytest.skip("restated oracle not built")
     m, q, g = _setup(cuda, name, 30000, 9)
     mode = L.GUESS_ELEM_CENTER if guess == "center" else L.GUESS_SUBREF_CENTER
-    cell, rf, it, ca = g.locate(q, tol=1e-5, max_steps=20, guess_mode=mode, stats=True)
+    cell, rf, it, ca, nd = g.locate(q, tol=1e-5, max_steps=20, guess_mode=mode, stats=True)
     torch.cuda.synchronize()
     b = g.get_bvh()
     bvh = {"inner": b.inner_nodes.cpu().numpy(), "leaf_nodes": b.leaf_nodes.cpu().numpy(),
