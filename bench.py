@@ -48,13 +48,16 @@ METRIC = "located pts/s (Newton-resolved, tol 1e-5)"
 def parse():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--steps", type=int, default=50)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--queries", type=int, default=N_QUERIES)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--cpu-sample", type=int, default=0,
                     help="reference CPU sample size (0 = sized for ~15 s)")
+    ap.add_argument("--profile", action="store_true",
+                    help="profiling run: fixed launch shape, only the timed steps "
+                         "(no tuning, plain/e2e/statistics/CPU legs)")
     return ap.parse_args()
 
 
@@ -226,7 +229,11 @@ def main():
     pts = torch.as_tensor(queries, device=dev)
     n = pts.shape[0]
     loc = api.BatchedLocator(mesh, tol=TOL, max_steps=MAX_STEPS, guess_mode=L.GUESS_ELEM_CENTER)
-    best_cfg, tune_ms = loc.tune(pts[: min(n, 1 << 21)])
+    if args.profile:
+        best_cfg = L.DrbLocateConfig(128, 4, 64, 1)
+        loc.config, tune_ms = best_cfg, 0.0
+    else:
+        best_cfg, tune_ms = loc.tune(pts[: min(n, 1 << 21)])
     cell = torch.empty(n, dtype=torch.int32, device=dev)
     ref = torch.empty((n, 3), dtype=torch.float32, device=dev)
 
@@ -266,6 +273,14 @@ def main():
     clk = clocks.stop()
     ms_step = total_ms / args.steps
     located = int((cell >= 0).sum().item())
+    if args.profile:
+        if rank == 0:
+            print(json.dumps({"profile": True, "ms_per_step": ms_step, "queries": n,
+                              "located": located, "launches_per_step": launches / args.steps}))
+        if pg:
+            pg.barrier()
+            pg.destroy_process_group()
+        return 0
     # statistics of the same queries (untimed): iterations, candidates, nodes
     _, _, it, ca, nd = loc.locate(pts, stats=True)
     mean_it = float(it.float().mean())

@@ -82,6 +82,16 @@ _lib = None
 _SIGS = {
     "drb_last_error": (C.c_char_p, []),
     "drb_version": (C.c_int, []),
+    "drb_mesh_boundary": (C.c_int, [C.POINTER(DrbMesh), C.c_void_p, C.c_void_p, C.c_void_p,
+                                    C.c_void_p, C.POINTER(C.c_int), C.c_void_p]),
+    "drb_surface_intersect": (C.c_int, [C.POINTER(DrbMesh), C.POINTER(DrbBvh), C.c_void_p,
+                                        C.c_int, C.c_float, C.c_int, C.c_void_p, DrbRayStats,
+                                        C.c_void_p]),
+    "drb_surface_shade": (C.c_int, [C.POINTER(DrbMesh), C.POINTER(DrbMesh), C.c_void_p,
+                                    C.c_void_p, C.c_int, C.c_void_p, C.c_int, C.c_void_p,
+                                    C.c_void_p, C.c_int, C.c_int, C.c_void_p, C.c_void_p,
+                                    C.c_void_p, C.c_void_p]),
+    "drb_ray_max": (C.c_int, [C.c_void_p, C.c_void_p, C.c_int, C.c_void_p]),
     "drb_camera_rays": (C.c_int, [C.POINTER(DrbCamera), C.c_void_p, C.c_void_p]),
     "drb_default_light": (C.c_int, [C.POINTER(DrbCamera), C.c_void_p]),
     "drb_cull_rays": (C.c_int, [C.c_void_p, C.c_int, C.c_void_p, C.c_void_p,

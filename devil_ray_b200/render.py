@@ -298,3 +298,107 @@ class Volume:
                 "drb_composite_partials")
         fb.composite_background(stream)
         return fb
+
+
+class MeshBoundary:
+    """MeshBoundary::execute for one hex mesh (+ scalar field): boundary quad
+    mesh and face field sharing the volume's value arrays."""
+
+    def execute(self, mesh: UnstructuredMesh, field: UnstructuredField | None = None,
+                stream=None):
+        d = mesh.desc()
+        nf = C.c_int()
+        L.check(L.lib().drb_mesh_boundary(C.byref(d), None, None, None, None, C.byref(nf),
+                                          _stream(stream)), "drb_mesh_boundary")
+        p = mesh.order
+        n = nf.value
+        dev = mesh.device
+        fidx = torch.empty((max(n, 1), (p + 1) ** 2), dtype=torch.int32, device=dev)
+        ffidx = torch.empty_like(fidx) if field is not None else None
+        elface = torch.empty((max(n, 1), 2), dtype=torch.int32, device=dev)
+        L.check(L.lib().drb_mesh_boundary(C.byref(d),
+                                          None if field is None else _ptr(field.ctrl_idx),
+                                          _ptr(fidx), _ptr(ffidx), _ptr(elface), C.byref(nf),
+                                          _stream(stream)), "drb_mesh_boundary")
+        faces = UnstructuredMesh(fidx[:n].reshape(-1), mesh.dof_data.values, p, dim=2, device=dev)
+        face_field = None
+        if field is not None:
+            face_field = QuadField(ffidx[:n].reshape(-1), field.values, p, name=field.name,
+                                   device=dev)
+        self.elid_faceid = elface[:n]
+        return faces, face_field
+
+
+class QuadField(UnstructuredField):
+    """Scalar field on quad faces (UnstructuredField<QuadScalar>)."""
+
+    def __init__(self, ctrl_idx, values, order: int, name: str = "f", device="cuda"):
+        self.order = int(order)
+        self.name = name
+        self.device = torch.device(device)
+        self.ctrl_idx = _dev(ctrl_idx, torch.int32, device)
+        self.values = _dev(values, torch.float32, device).reshape(-1)
+        nd = (self.order + 1) ** 2
+        self.n_elem = self.ctrl_idx.numel() // nd
+        stride = L.lib().drb_packed_stride(2, self.order, 1)
+        self.packed = torch.empty((max(self.n_elem, 1), stride), dtype=torch.float32,
+                                  device=self.device)
+        d = self.desc(packed=False)
+        L.check(L.lib().drb_pack_elements(C.byref(d), _ptr(self.packed), _stream(None)),
+                "drb_pack_elements")
+        self._range = None
+
+    def desc(self, packed=True) -> L.DrbMesh:
+        m = super().desc(packed)
+        m.dim = 2
+        return m
+
+
+class Surface:
+    """Surface of a quad mesh (Surface / Traceable)."""
+
+    def __init__(self, faces: UnstructuredMesh, field: UnstructuredField):
+        self.faces, self.field_ = faces, field
+        self.cmap = ColorMap()
+        self.tol, self.max_steps = 1e-4, 10   # face_intersection.hpp:153-154
+
+    def color_map(self) -> ColorMap:
+        return self.cmap
+
+    def nearest_hit(self, rays: torch.Tensor, stats=False, stream=None):
+        n = rays.shape[0]
+        hits = torch.empty((n, 5), dtype=torch.float32, device=self.faces.device)
+        st = [torch.zeros(max(n, 1), dtype=torch.int32, device=self.faces.device)
+              for _ in range(2)] if stats else None
+        rs = L.DrbRayStats(None, *(t.data_ptr() for t in st)) if stats else L.DrbRayStats()
+        L.check(L.lib().drb_surface_intersect(C.byref(self.faces.desc()),
+                                              C.byref(self.faces.get_bvh().desc()), _ptr(rays),
+                                              n, self.tol, self.max_steps, _ptr(hits), rs,
+                                              _stream(stream)), "drb_surface_intersect")
+        return (hits, st) if stats else hits
+
+    def _tf(self):
+        return torch.as_tensor(self.cmap.table.sample(self.cmap.n_samples), device=self.faces.device)
+
+    def shade(self, rays, hits, lights, fb: Framebuffer, use_lighting=True, stream=None):
+        n = rays.shape[0]
+        frags = torch.empty((n, 4), dtype=torch.float32, device=self.faces.device)
+        tf = self._tf()
+        rng = np.array(self.cmap.range or self.field_.range(), np.float32)
+        lt = lights_tensor(lights, self.faces.device)
+        L.check(L.lib().drb_surface_shade(C.byref(self.faces.desc()), C.byref(self.field_.desc()),
+                                          _ptr(rays), _ptr(hits), n, _ptr(tf), tf.shape[0],
+                                          rng.ctypes.data_as(C.c_void_p), _ptr(lt), len(lights),
+                                          int(use_lighting), _ptr(frags), _ptr(fb.colors),
+                                          _ptr(fb.depths), _stream(stream)), "drb_surface_shade")
+        return frags
+
+    def render(self, camera: Camera, lights=None, use_lighting=True, stream=None):
+        if lights is None:
+            lights = [PointLight.default(camera)]
+        rays = camera.create_rays(self.faces.device, stream)
+        fb = Framebuffer(camera.width, camera.height, self.faces.device)
+        fb.clear(stream=stream)
+        hits = self.nearest_hit(rays, stream=stream)
+        self.shade(rays, hits, lights, fb, use_lighting, stream)
+        return fb, hits

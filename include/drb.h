@@ -279,6 +279,36 @@ int drb_framebuffer_clear (float *rgba, float *depth, int n_pixels, const float 
 int drb_framebuffer_composite_background (float *rgba, int n_pixels, const float *bg4,
                                           void *stream);
 
+/* MeshBoundary::execute (filters/mesh_boundary.cpp:339-361, 205-236) for a
+ * hex mesh: the boundary quads in the reference's order (sorted face corner
+ * tuples), each as (p+1)^2 indices into the unchanged value arrays.
+ * field_ctrl_idx (optional) is the scalar field's ctrl_idx, mapped to
+ * face_field_idx the same way; elid_faceid (optional) receives (element,
+ * face id 0..5) pairs.  Outputs need capacity 6*n_elem faces; *n_faces is
+ * returned after a stream synchronise (call once with NULL outputs to size). */
+int drb_mesh_boundary (const drb_mesh *hex, const int *field_ctrl_idx, int *face_ctrl_idx,
+                       int *face_field_idx, int *elid_faceid, int *n_faces, void *stream);
+
+/* Surface::nearest_hit (rendering/surface.cpp:304-437, 497-520) over a quad
+ * mesh and its BVH: ordered traversal, ray-face Newton per candidate
+ * (face_intersection.hpp:96-173; reference tol 1e-4, 10 steps).  hits:
+ * device dray::RayHit[n] (int32 idx, dist, ref[3] = 20 bytes). */
+int drb_surface_intersect (const drb_mesh *faces, const drb_bvh *bvh, const void *rays, int n,
+                           float tol, int max_steps, void *hits, drb_ray_stats stats,
+                           void *stream);
+
+/* Traceable::fragments + Traceable::shade (rendering/traceable.cpp:49-147,
+ * 242-387) for quad faces, fused: fragments (optional device float[4n]:
+ * scalar, normal) and, for hits, the shaded colour and depth into the
+ * framebuffer (device float4/float [w*h], indexed by the ray's pixel id). */
+int drb_surface_shade (const drb_mesh *faces, const drb_mesh *face_field, const void *rays,
+                       const void *hits, int n, const float *tf, int tf_size,
+                       const float *range2, const void *lights, int n_lights, int use_lighting,
+                       float *fragments, float *fb_rgba, float *fb_depth, void *stream);
+
+/* ray_max (ray.cpp:243-259): far = hit distance for rays that hit. */
+int drb_ray_max (void *rays, const void *hits, int n, void *stream);
+
 #ifdef __cplusplus
 }
 #endif
