@@ -82,6 +82,11 @@ _lib = None
 _SIGS = {
     "drb_last_error": (C.c_char_p, []),
     "drb_version": (C.c_int, []),
+    "drb_noalloc_max_queries": (C.c_int, []),
+    "drb_locate_batched_noalloc": (C.c_int, [C.POINTER(DrbMesh), C.POINTER(DrbBvh), C.c_void_p,
+                                             C.c_int, C.POINTER(DrbNewtonOpts), C.c_void_p,
+                                             C.c_void_p, C.c_void_p, DrbQueryStats,
+                                             C.c_void_p]),
     "drb_mesh_boundary": (C.c_int, [C.POINTER(DrbMesh), C.c_void_p, C.c_void_p, C.c_void_p,
                                     C.c_void_p, C.POINTER(C.c_int), C.c_void_p]),
     "drb_surface_intersect": (C.c_int, [C.POINTER(DrbMesh), C.POINTER(DrbBvh), C.c_void_p,

@@ -51,6 +51,35 @@ int exclusive_scan_i32 (const int *in, int *out, int n, int *d_total, cudaStream
 
 inline int div_up (long long a, long long b) { return (int)((a + b - 1) / b); }
 
+// Workspace of the allocation-free radix sort (sizes from radix_ws_counts
+// and scan_ws_ints; kbuf/vbuf hold n elements).
+struct RadixWorkspace
+{
+  unsigned *kbuf;
+  int *vbuf;
+  int *counts;
+  int *scan_tmp;
+};
+long long radix_ws_counts (int n);
+int scan_ws_ints (int n);
+int exclusive_scan_i32_ws (const int *in, int *out, int n, int *d_total, int *tmp, cudaStream_t s);
+int radix_sort_pairs_ws (const unsigned *keys_in, const int *vals_in, unsigned *keys_out,
+                         int *vals_out, int n, int bits, const RadixWorkspace &ws, cudaStream_t s);
+// Batched locate with every scratch buffer supplied by the caller.
+struct LocateWorkspace
+{
+  int *head;
+  unsigned *codes;
+  unsigned *codes_sorted;
+  int *iota;
+  int *order;
+  RadixWorkspace radix;
+};
+int locate_batched_ws (const drb_mesh *mesh, const drb_bvh *bvh, const float *pts, int n,
+                       const drb_newton_opts *opts, const drb_locate_config *cfg,
+                       const LocateWorkspace &ws, int *cell, float *ref, drb_query_stats stats,
+                       cudaStream_t s);
+
 int sm_count ();
 
 } // namespace drb

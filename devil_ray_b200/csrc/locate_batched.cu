@@ -336,6 +336,55 @@ int locate_batched_impl (const drb_mesh *mesh, const drb_bvh *bvh, const float *
                             cfg.chunk, head, cell, ref, stats);
 }
 
+// Same as locate_batched_impl with sorting, but over caller-provided
+// workspace (used by the allocation-free entry point).
+int locate_batched_ws (const drb_mesh *mesh, const drb_bvh *bvh, const float *pts, int n,
+                       const drb_newton_opts *opts, const drb_locate_config *cfg_in,
+                       const LocateWorkspace &ws, int *cell, float *ref, drb_query_stats stats,
+                       cudaStream_t s)
+{
+  int st = check_args (mesh, bvh, pts, n, opts, cell, ref);
+  if (st) return st;
+  if (n == 0) return DRB_OK;
+  drb_locate_config cfg = cfg_in ? *cfg_in : default_config (mesh->order);
+  if (cfg.block < 32 || cfg.block > 1024 || (cfg.block % 32) || cfg.chunk < 1)
+  {
+    set_last_error ("locate_batched: block must be a multiple of 32 in [32,1024], chunk >= 1");
+    return DRB_ERR_INVALID_ARG;
+  }
+  const int *ord = nullptr;
+  if (cfg.sort_queries)
+  {
+    const float *b = bvh->bounds;
+    float sc[3];
+    for (int k = 0; k < 3; ++k)
+    {
+      const float ext = b[2 * k + 1] - b[2 * k];
+      sc[k] = (ext > 0.f && std::isfinite (ext)) ? 1.f / ext : 0.f;
+    }
+    const float lo[3] = { std::isfinite (b[0]) ? b[0] : 0.f, std::isfinite (b[2]) ? b[2] : 0.f,
+                          std::isfinite (b[4]) ? b[4] : 0.f };
+    query_codes_kernel<<<div_up (n, 256), 256, 0, s>>> (pts, n, lo[0], lo[1], lo[2], sc[0],
+                                                         sc[1], sc[2], ws.codes, ws.iota);
+    if ((st = check_launch ("query_codes_kernel"))) return st;
+    st = radix_sort_pairs_ws (ws.codes, ws.iota, ws.codes_sorted, ws.order, n, 30, ws.radix, s);
+    if (st) return st;
+    ord = ws.order;
+  }
+  cudaError_t e = cudaMemsetAsync (ws.head, 0, sizeof (int), s);
+  if (e != cudaSuccess) return status_from (e);
+  const int per_sm = resident_blocks (mesh->order, cfg.block);
+  const int bps = (cfg.blocks_per_sm > 0) ? min (cfg.blocks_per_sm, per_sm) : per_sm;
+  const long long warps_needed = ((long long)n + 31) / 32;
+  long long blocks = (long long)bps * sm_count ();
+  const long long blocks_needed = (warps_needed * 32 + cfg.block - 1) / cfg.block;
+  if (blocks > blocks_needed) blocks = blocks_needed;
+  if (blocks < 1) blocks = 1;
+  const LocateParams lp = make_params (mesh, bvh, opts);
+  return launch_persistent (mesh->order, dim3 ((unsigned)blocks), cfg.block, s, lp, pts, ord, n,
+                            cfg.chunk, ws.head, cell, ref, stats);
+}
+
 } // namespace drb
 
 using namespace drb;

@@ -239,6 +239,71 @@ int radix_sort_pairs (const unsigned *keys_in, const int *vals_in, unsigned *key
   return DRB_OK;
 }
 
+// ---- variants over a caller-provided workspace (no allocation) ----
+
+int scan_ws_ints (int n)
+{
+  int total = 0;
+  while (n > kScanTile)
+  {
+    n = div_up (n, kScanTile);
+    total += n;
+  }
+  return total + 1;
+}
+
+int exclusive_scan_i32_ws (const int *in, int *out, int n, int *d_total, int *tmp, cudaStream_t s)
+{
+  if (n <= 0)
+  {
+    if (d_total) cudaMemsetAsync (d_total, 0, sizeof (int), s);
+    return DRB_OK;
+  }
+  const int nblocks = div_up (n, kScanTile);
+  if (nblocks == 1)
+  {
+    scan_apply_kernel<<<1, kScanBlock, 0, s>>> (in, out, n, nullptr, d_total, 1);
+    return check_launch ("scan_apply_kernel");
+  }
+  int *sums = tmp;
+  scan_reduce_kernel<<<nblocks, kScanBlock, 0, s>>> (in, n, sums);
+  int st = check_launch ("scan_reduce_kernel");
+  if (st) return st;
+  st = exclusive_scan_i32_ws (sums, sums, nblocks, nullptr, tmp + nblocks, s);
+  if (st) return st;
+  scan_apply_kernel<<<nblocks, kScanBlock, 0, s>>> (in, out, n, sums, d_total, nblocks);
+  return check_launch ("scan_apply_kernel");
+}
+
+long long radix_ws_counts (int n) { return (long long)kRadix * div_up (n, kSortTile); }
+
+int radix_sort_pairs_ws (const unsigned *keys_in, const int *vals_in, unsigned *keys_out,
+                         int *vals_out, int n, int bits, const RadixWorkspace &ws, cudaStream_t s)
+{
+  if (n <= 0) return DRB_OK;
+  const int ntiles = div_up (n, kSortTile);
+  const int passes = (bits + 7) / 8;
+  const unsigned *ksrc = keys_in;
+  const int *vsrc = vals_in;
+  for (int p = 0; p < passes; ++p)
+  {
+    const bool to_out = ((passes - 1 - p) % 2) == 0;
+    unsigned *kdst = to_out ? keys_out : ws.kbuf;
+    int *vdst = to_out ? vals_out : ws.vbuf;
+    hist_kernel<<<ntiles, kSortBlock, 0, s>>> (ksrc, n, 8 * p, ntiles, ws.counts);
+    int st = check_launch ("hist_kernel");
+    if (st) return st;
+    st = exclusive_scan_i32_ws (ws.counts, ws.counts, kRadix * ntiles, nullptr, ws.scan_tmp, s);
+    if (st) return st;
+    scatter_kernel<<<ntiles, kSortBlock, 0, s>>> (ksrc, vsrc, kdst, vdst, n, 8 * p, ntiles, ws.counts);
+    st = check_launch ("scatter_kernel");
+    if (st) return st;
+    ksrc = kdst;
+    vsrc = vdst;
+  }
+  return DRB_OK;
+}
+
 } // namespace drb
 
 extern "C" int drb_radix_sort_pairs (const unsigned *keys_in, const int *vals_in,

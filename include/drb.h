@@ -166,6 +166,26 @@ int drb_locate_batched (const drb_mesh *mesh, const drb_bvh *bvh, const float *p
                         const drb_newton_opts *opts, const drb_locate_config *cfg, int *cell,
                         float *ref, drb_query_stats stats, void *stream);
 
+/* drb_locate_batched without any device allocation, for callers that cannot
+ * allocate when they locate points (inside a stream capture that must not
+ * record allocations, under a host application's own device-memory pool,
+ * or where cudaMalloc's implicit synchronisation is not acceptable).  No
+ * counterpart in the reference.  All scratch lives in one fixed array of
+ * about 25 MB inside the library's device code, which stays allocated on each
+ * device where it is loaded until the process exits.  At most
+ * drb_noalloc_max_queries() (1,048,576) queries per call; more is rejected
+ * with DRB_ERR_INVALID_ARG.  The first call on a device looks the array's
+ * address up (cudaGetSymbolAddress) with that device current; make that first
+ * call before any stream capture.  All calls share the array: calls whose GPU
+ * work may overlap race and must be serialised by the caller.  Results equal
+ * drb_locate_batched's. */
+int drb_locate_batched_noalloc (const drb_mesh *mesh, const drb_bvh *bvh, const float *pts,
+                                int n, const drb_newton_opts *opts,
+                                const drb_locate_config *cfg, int *cell, float *ref,
+                                drb_query_stats stats, void *stream);
+/* Largest query count drb_locate_batched_noalloc accepts per call. */
+int drb_noalloc_max_queries (void);
+
 /* Morton order of query points over the BVH bounds: device int32 order[n]
  * (a permutation of 0..n-1).  No reference counterpart (it never reorders). */
 int drb_query_order (const drb_bvh *bvh, const float *pts, int n, int *order, void *stream);

@@ -1,0 +1,71 @@
+"""The allocation-free batched locate, called through the C-ABI.
+
+It exists for callers that cannot allocate device memory while they locate
+points (stream capture without allocation nodes, a host application's own
+memory pool, latency-critical paths).  Its answers must equal those of the
+allocating drb_locate_batched on the same inputs, on consecutive calls that
+reuse the library's fixed scratch array.  This file is collected last so a
+failure here cannot hide the result of another test.
+"""
+import ctypes as C
+
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+
+
+def _call(lib, L, fn, mesh_d, bvh_d, pts, opts, cell, ref, stream):
+    args = [C.byref(mesh_d), C.byref(bvh_d), C.c_void_p(pts.data_ptr()), pts.shape[0],
+            C.byref(opts), None, C.c_void_p(cell.data_ptr()), C.c_void_p(ref.data_ptr()),
+            L.DrbQueryStats(), C.c_void_p(stream)]
+    return getattr(lib, fn)(*args)
+
+
+def test_noalloc_matches_allocating_path_twice(cuda):
+    import torch
+    from devil_ray_b200 import _lib as L
+    from devil_ray_b200 import api, meshgen
+    lib = L.lib()
+    m = meshgen.trilinear_distorted_mesh(16, 2, 0.15, seed=21)
+    mesh = api.UnstructuredMesh(m.ctrl_idx, m.xyz, m.order, device=cuda)
+    bvh = mesh.get_bvh()
+    mesh_d, bvh_d = mesh.desc(), bvh.desc()
+    stream = torch.cuda.current_stream().cuda_stream
+    opts = L.DrbNewtonOpts(1e-5, 20, L.GUESS_ELEM_CENTER, None)
+    cap = lib.drb_noalloc_max_queries()
+    assert cap == 1 << 20
+    for call, (count, seed) in enumerate([(300_000, 5), (cap, 6)]):
+        pts = torch.as_tensor(meshgen.uniform_queries(count, seed), device=cuda)
+        c0 = torch.empty(count, dtype=torch.int32, device=cuda)
+        r0 = torch.empty((count, 3), dtype=torch.float32, device=cuda)
+        c1 = torch.full_like(c0, -7)
+        r1 = torch.full_like(r0, 7.0)
+        assert _call(lib, L, "drb_locate_batched", mesh_d, bvh_d, pts, opts, c0, r0, stream) == 0
+        assert _call(lib, L, "drb_locate_batched_noalloc", mesh_d, bvh_d, pts, opts, c1, r1,
+                     stream) == 0, lib.drb_last_error()
+        torch.cuda.synchronize()
+        # same kernels, same processing order: identical results (tolerance 0,
+        # within the 1e-5 reference-space tolerance used by the other tests)
+        assert torch.equal(c0, c1), f"call {call}: cell ids differ"
+        assert torch.allclose(r0, r1, rtol=0, atol=1e-5), f"call {call}: ref points differ"
+        assert 0.85 < (c1 >= 0).float().mean().item() < 0.95
+
+
+def test_noalloc_rejects_oversized_call(cuda):
+    import torch
+    from devil_ray_b200 import _lib as L
+    from devil_ray_b200 import api, meshgen
+    lib = L.lib()
+    m = meshgen.workload_mesh("volume_8")
+    mesh = api.UnstructuredMesh(m.ctrl_idx, m.xyz, m.order, device=cuda)
+    bvh = mesh.get_bvh()
+    opts = L.DrbNewtonOpts(1e-5, 20, L.GUESS_ELEM_CENTER, None)
+    n = lib.drb_noalloc_max_queries() + 1
+    pts = torch.zeros((n, 3), dtype=torch.float32, device=cuda)
+    cell = torch.empty(n, dtype=torch.int32, device=cuda)
+    ref = torch.empty((n, 3), dtype=torch.float32, device=cuda)
+    st = _call(lib, L, "drb_locate_batched_noalloc", mesh.desc(), bvh.desc(), pts, opts, cell,
+               ref, torch.cuda.current_stream().cuda_stream)
+    assert st == L.DRB_ERR_INVALID_ARG
+    assert b"fixed scratch capacity" in lib.drb_last_error()
