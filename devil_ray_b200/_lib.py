@@ -34,7 +34,7 @@ class DrbBvh(C.Structure):
     _fields_ = [("n_inner", C.c_int), ("n_leaf", C.c_int),
                 ("inner_nodes", C.c_void_p), ("leaf_nodes", C.c_void_p),
                 ("aabb_ids", C.c_void_p), ("ref_boxes", C.c_void_p),
-                ("bounds", C.c_float * 6)]
+                ("bounds", C.c_float * 6), ("cull", C.c_int)]
 
 
 class DrbNewtonOpts(C.Structure):
@@ -67,7 +67,7 @@ class DrbRayStats(C.Structure):
 class DrbVolumeOpts(C.Structure):
     _fields_ = [("samples", C.c_int), ("use_lighting", C.c_int), ("tol", C.c_float),
                 ("max_steps", C.c_int), ("guess_mode", C.c_int), ("coherent", C.c_int),
-                ("bounds", C.c_float * 6)]
+                ("bounds", C.c_float * 6), ("cull", C.c_int)]
 
 
 class DrbError(RuntimeError):

@@ -1,0 +1,821 @@
+// Learned initial guess for the Newton inversion: a small MLP
+// (84 -> 128 -> 128 -> 3, GELU) mapping an order-2 hex element's 27 control
+// points plus a physical point to a reference-space guess.  No counterpart
+// in the reference; it feeds DRB_GUESS_GIVEN, with plain Newton from the
+// element centre as the fallback whenever the guessed solve fails.
+//
+// Tensor-core kernels (tcgen05 / UMMA, BF16 operands, FP32 accumulation in
+// tensor memory):
+//   gemm_kernel       D = A * B^T for A [M x K], B [N x K] (both K-major
+//                     bf16), one 128-row tile per CTA, K in chunks of 64,
+//                     optional split-K; fused epilogues: +bias & GELU
+//                     (storing the pre-activation), x GELU'(Z), fp32 store or
+//                     fp32 atomic accumulation (weight gradients)
+//   mlp_guess_kernel  fused inference: per tile of 128 (point, element)
+//                     pairs, features are built in shared memory, two UMMA
+//                     GEMMs run with the weights resident in shared memory,
+//                     the 128 -> 3 head runs on the CUDA cores
+// Every mbarrier wait is bounded; on timeout the kernel records an error
+// flag, frees its tensor memory and returns.
+#include <cuda_bf16.h>
+
+#include "bernstein.cuh"
+#include "drb_common.cuh"
+#include "drb_internal.h"
+#include "umma.cuh"
+
+namespace drb
+{
+namespace mlp
+{
+
+constexpr int kIn = 84;      // 27 control points x 3 + point x 3
+constexpr int kInPad = 96;   // K padded to a multiple of 16
+constexpr int kHid = 128;
+constexpr int kOut = 3;
+// parameter offsets in the fp32 master vector
+constexpr int kW1 = 0;
+constexpr int kB1 = kW1 + kHid * kIn;
+constexpr int kW2 = kB1 + kHid;
+constexpr int kB2 = kW2 + kHid * kHid;
+constexpr int kW3 = kB2 + kHid;
+constexpr int kB3 = kW3 + kOut * kHid;
+constexpr int kParams = kB3 + kOut;
+// bf16 operand copies: W1 [128 x 96], W2 [128 x 128], W2^T [128 x 128]
+constexpr int kBW1 = 0;
+constexpr int kBW2 = kBW1 + kHid * kInPad;
+constexpr int kBW2T = kBW2 + kHid * kHid;
+constexpr int kBf16 = kBW2T + kHid * kHid;
+
+constexpr uint32_t kWaitTries = 1u << 22;
+
+// GELU, tanh form: 0.5 x (1 + tanh(sqrt(2/pi) (x + 0.044715 x^3)))
+DRB_D float gelu (float x)
+{
+  const float u = 0.7978845608028654f * (x + 0.044715f * x * x * x);
+  return 0.5f * x * (1.f + tanhf (u));
+}
+DRB_D float gelu_grad (float x)
+{
+  const float u = 0.7978845608028654f * (x + 0.044715f * x * x * x);
+  const float t = tanhf (u);
+  const float du = 0.7978845608028654f * (1.f + 3.f * 0.044715f * x * x);
+  return 0.5f * (1.f + t) + 0.5f * x * (1.f - t * t) * du;
+}
+
+// Features of one (element, point) pair: control points and point relative
+// to the centre of the element's control-point box, scaled by its largest
+// half-extent.  27 x 3 control coordinates, then the point, then zeros.
+DRB_D void pair_features (const float *__restrict__ row, const float (&pt)[3], float (&f)[kInPad])
+{
+  float mn[3] = { INFINITY, INFINITY, INFINITY }, mx[3] = { -INFINITY, -INFINITY, -INFINITY };
+#pragma unroll
+  for (int i = 0; i < 27; ++i)
+#pragma unroll
+    for (int k = 0; k < 3; ++k)
+    {
+      const float v = __ldg (row + 3 * i + k);
+      f[3 * i + k] = v;
+      mn[k] = fminf (mn[k], v);
+      mx[k] = fmaxf (mx[k], v);
+    }
+  float c[3], h = 0.f;
+#pragma unroll
+  for (int k = 0; k < 3; ++k)
+  {
+    c[k] = 0.5f * (mn[k] + mx[k]);
+    h = fmaxf (h, 0.5f * (mx[k] - mn[k]));
+  }
+  const float inv = h > 0.f ? 1.f / h : 0.f;
+#pragma unroll
+  for (int i = 0; i < 27; ++i)
+#pragma unroll
+    for (int k = 0; k < 3; ++k) f[3 * i + k] = (f[3 * i + k] - c[k]) * inv;
+#pragma unroll
+  for (int k = 0; k < 3; ++k) f[81 + k] = (pt[k] - c[k]) * inv;
+#pragma unroll
+  for (int q = kIn; q < kInPad; ++q) f[q] = 0.f;
+}
+
+// Store one row of K bf16 values into an interleaved K-major tile.
+template <int K>
+DRB_D void store_row_bf16 (unsigned char *tile, int r, const float *v)
+{
+#pragma unroll
+  for (int k8 = 0; k8 < K / 8; ++k8)
+  {
+    __align__ (16) __nv_bfloat16 b[8];
+#pragma unroll
+    for (int j = 0; j < 8; ++j) b[j] = __float2bfloat16_rn (v[8 * k8 + j]);
+    *reinterpret_cast<uint4 *> (tile + umma::tile_offset (r, 8 * k8, K)) =
+    *reinterpret_cast<const uint4 *> (b);
+  }
+}
+
+// ------------------------------------------------------------ prepare --
+
+__global__ void prepare_kernel (const float *__restrict__ p, __nv_bfloat16 *__restrict__ wb)
+{
+  const int t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t < kHid * kInPad)
+  {
+    const int r = t / kInPad, k = t - r * kInPad;
+    wb[kBW1 + t] = __float2bfloat16_rn (k < kIn ? p[kW1 + r * kIn + k] : 0.f);
+  }
+  if (t < kHid * kHid)
+  {
+    const int r = t / kHid, k = t - r * kHid;
+    wb[kBW2 + t] = __float2bfloat16_rn (p[kW2 + t]);
+    wb[kBW2T + t] = __float2bfloat16_rn (p[kW2 + k * kHid + r]);
+  }
+}
+
+// ----------------------------------------------------------- features --
+
+__global__ void features_kernel (const float *__restrict__ packed, int stride,
+                                 const int *__restrict__ elem, const float *__restrict__ pts, int n,
+                                 int n_pad, __nv_bfloat16 *__restrict__ X)
+{
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n_pad) return;
+  float f[kInPad];
+  const int e = i < n ? elem[i] : -1;
+  if (e >= 0)
+  {
+    const float pt[3] = { pts[3 * (size_t)i], pts[3 * (size_t)i + 1], pts[3 * (size_t)i + 2] };
+    pair_features (packed + (size_t)e * stride, pt, f);
+  }
+  else
+  {
+#pragma unroll
+    for (int q = 0; q < kInPad; ++q) f[q] = 0.f;
+  }
+#pragma unroll
+  for (int q = 0; q < kInPad; q += 8)
+  {
+    __align__ (16) __nv_bfloat16 b[8];
+#pragma unroll
+    for (int j = 0; j < 8; ++j) b[j] = __float2bfloat16_rn (f[q + j]);
+    *reinterpret_cast<uint4 *> (X + (size_t)i * kInPad + q) = *reinterpret_cast<const uint4 *> (b);
+  }
+}
+
+// --------------------------------------------------------------- GEMM --
+
+enum Epilogue
+{
+  EPI_STORE = 0,     // C[r, c] = D (+ bias[c])                 fp32
+  EPI_BIAS_GELU = 1, // Z[r, c] = D + bias[c], H = bf16(gelu(Z))
+  EPI_GELU_GRAD = 2, // H[r, c] = bf16(D * gelu'(Z[r, c]))
+  EPI_ATOMIC = 3     // atomicAdd(C[r * ldc + c], D) for c < ncols
+};
+
+struct GemmArgs
+{
+  const __nv_bfloat16 *A; // [M x K]
+  const __nv_bfloat16 *B; // [N x K]
+  int M, N, K;
+  int k_split;             // K elements per split (multiple of 64)
+  const float *bias;
+  float *C;                // fp32 output / pre-activation Z
+  __nv_bfloat16 *H;        // bf16 output
+  const float *Zin;        // pre-activation for EPI_GELU_GRAD
+  int ldc, ncols;          // for EPI_ATOMIC
+  int *err;
+};
+
+constexpr int kKC = 64;       // K per chunk
+constexpr int kGemmN = 128;   // max N handled (TMEM columns)
+
+template <int EPI>
+__global__ void __launch_bounds__ (128) gemm_kernel (GemmArgs g)
+{
+  extern __shared__ __align__ (1024) unsigned char smem[];
+  unsigned char *sA = smem;                       // 128 x 64 bf16 = 16 KB
+  unsigned char *sB = smem + 128 * kKC * 2;       // N x 64 bf16 <= 16 KB
+  __shared__ __align__ (8) uint64_t mbar;
+  __shared__ uint32_t tmem_base;
+  const int tid = threadIdx.x;
+  const int warp = tid >> 5;
+  const int m0 = blockIdx.x * 128;
+  const int kbeg = blockIdx.y * g.k_split;
+  const int kend = min (g.K, kbeg + g.k_split);
+  if (warp == 0) umma::tmem_alloc (&tmem_base, kGemmN);
+  if (tid == 0) umma::mbar_init (&mbar, 1);
+  umma::fence_before_sync ();
+  __syncthreads ();
+  umma::fence_after_sync ();
+  const uint32_t tbase = tmem_base;
+  const uint32_t idesc = umma::idesc_bf16_f32 (128, g.N);
+  uint32_t phase = 0;
+  bool ok = true;
+  int chunks = 0;
+  for (int k0 = kbeg; k0 < kend; k0 += kKC)
+  {
+    // cooperative 16-byte loads into the interleaved layout
+    for (int v = tid; v < 128 * (kKC / 8); v += 128)
+    {
+      const int r = v / (kKC / 8), j = v - r * (kKC / 8);
+      const int k = k0 + 8 * j;
+      uint4 val = make_uint4 (0, 0, 0, 0);
+      if (m0 + r < g.M && k < kend)
+        val = *reinterpret_cast<const uint4 *> (g.A + (size_t)(m0 + r) * g.K + k);
+      *reinterpret_cast<uint4 *> (sA + umma::tile_offset (r, 8 * j, kKC)) = val;
+    }
+    for (int v = tid; v < g.N * (kKC / 8); v += 128)
+    {
+      const int r = v / (kKC / 8), j = v - r * (kKC / 8);
+      const int k = k0 + 8 * j;
+      uint4 val = make_uint4 (0, 0, 0, 0);
+      if (k < kend) val = *reinterpret_cast<const uint4 *> (g.B + (size_t)r * g.K + k);
+      *reinterpret_cast<uint4 *> (sB + umma::tile_offset (r, 8 * j, kKC)) = val;
+    }
+    umma::fence_async_smem ();
+    __syncthreads ();
+    if (tid == 0)
+    {
+      umma::fence_after_sync ();
+      const uint32_t a0 = umma::smem_addr (sA), b0 = umma::smem_addr (sB);
+#pragma unroll
+      for (int kk = 0; kk < kKC / 16; ++kk)
+      {
+        const uint64_t ad = umma::desc_kmajor (a0 + kk * 256, 128, (kKC / 8) * 128);
+        const uint64_t bd = umma::desc_kmajor (b0 + kk * 256, 128, (kKC / 8) * 128);
+        umma::mma_bf16 (tbase, ad, bd, idesc, (chunks > 0 || kk > 0) ? 1u : 0u);
+      }
+      umma::mma_commit (&mbar);
+    }
+    ok = umma::mbar_wait (&mbar, phase, kWaitTries) && ok;
+    phase ^= 1u;
+    ++chunks;
+    umma::fence_after_sync ();
+    __syncthreads ();
+    if (!__syncthreads_and (ok)) break;
+  }
+  ok = __syncthreads_and (ok) != 0; // CTA-uniform before the warp-collective loads
+  if (!ok && tid == 0 && g.err) atomicExch (g.err, 1);
+  // epilogue: thread t owns accumulator row t (TMEM lane t)
+  const int r = m0 + tid;
+  if (ok && chunks > 0)
+  {
+    for (int c0 = 0; c0 < g.N; c0 += 32)
+    {
+      float d[32];
+      umma::tmem_ld32 (tbase + ((uint32_t)(warp * 32) << 16) + c0, d);
+      if (r >= g.M) continue;
+#pragma unroll
+      for (int j = 0; j < 32; ++j)
+      {
+        const int c = c0 + j;
+        if (c >= g.N) break;
+        if (EPI == EPI_STORE)
+          g.C[(size_t)r * g.N + c] = d[j] + (g.bias ? g.bias[c] : 0.f);
+        else if (EPI == EPI_BIAS_GELU)
+        {
+          const float z = d[j] + g.bias[c];
+          g.C[(size_t)r * g.N + c] = z;
+          g.H[(size_t)r * g.N + c] = __float2bfloat16_rn (gelu (z));
+        }
+        else if (EPI == EPI_GELU_GRAD)
+          g.H[(size_t)r * g.N + c] = __float2bfloat16_rn (d[j] * gelu_grad (g.Zin[(size_t)r * g.N + c]));
+        else if (c < g.ncols)
+          atomicAdd (g.C + (size_t)r * g.ldc + c, d[j]);
+      }
+    }
+  }
+  umma::fence_before_sync ();
+  __syncthreads ();
+  if (warp == 0) umma::tmem_dealloc (tbase, kGemmN);
+}
+
+// ------------------------------------------------------- head / losses --
+
+// y = W3 gelu(Z2) + b3; masked MSE; dY; grads of W3, b3; dZ2 = (W3^T dY) x
+// gelu'(Z2) as bf16; db2 partial sums.  One thread per row.
+__global__ void __launch_bounds__ (128)
+head_kernel (const float *__restrict__ p, const float *__restrict__ Z2, const float *__restrict__ target,
+             const float *__restrict__ weight, int n, int n_pad, float inv_count, float *__restrict__ y_out,
+             float *__restrict__ grad, __nv_bfloat16 *__restrict__ dZ2, float *__restrict__ loss)
+{
+  __shared__ float s_w3[kOut * kHid];
+  __shared__ float s_gw3[kOut * kHid];
+  __shared__ float s_db2[kHid];
+  __shared__ float s_gb3[kOut];
+  __shared__ float s_loss;
+  for (int q = threadIdx.x; q < kOut * kHid; q += blockDim.x)
+  {
+    s_w3[q] = p[kW3 + q];
+    s_gw3[q] = 0.f;
+  }
+  for (int q = threadIdx.x; q < kHid; q += blockDim.x) s_db2[q] = 0.f;
+  if (threadIdx.x < kOut) s_gb3[threadIdx.x] = 0.f;
+  if (threadIdx.x == 0) s_loss = 0.f;
+  __syncthreads ();
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < n_pad)
+  {
+    float h[kHid];
+    const float *z = Z2 + (size_t)i * kHid;
+#pragma unroll 8
+    for (int c = 0; c < kHid; ++c) h[c] = gelu (z[c]);
+    float y[kOut], dy[kOut];
+#pragma unroll
+    for (int o = 0; o < kOut; ++o)
+    {
+      float s = p[kB3 + o];
+#pragma unroll 8
+      for (int c = 0; c < kHid; ++c) s += s_w3[o * kHid + c] * h[c];
+      y[o] = s;
+    }
+    const float w = (i < n && weight) ? weight[i] : (i < n ? 1.f : 0.f);
+    float l = 0.f;
+#pragma unroll
+    for (int o = 0; o < kOut; ++o)
+    {
+      const float e = (i < n && target) ? (y[o] - target[3 * (size_t)i + o]) : 0.f;
+      l += w * e * e;
+      dy[o] = 2.f * w * e * inv_count;
+      if (y_out && i < n) y_out[3 * (size_t)i + o] = y[o];
+    }
+    if (grad)
+    {
+      atomicAdd (&s_loss, l * inv_count);
+#pragma unroll
+      for (int o = 0; o < kOut; ++o)
+      {
+        atomicAdd (&s_gb3[o], dy[o]);
+        for (int c = 0; c < kHid; ++c) atomicAdd (&s_gw3[o * kHid + c], dy[o] * h[c]);
+      }
+      for (int c = 0; c < kHid; ++c)
+      {
+        float dh = 0.f;
+#pragma unroll
+        for (int o = 0; o < kOut; ++o) dh += s_w3[o * kHid + c] * dy[o];
+        const float dz = dh * gelu_grad (z[c]);
+        dZ2[(size_t)i * kHid + c] = __float2bfloat16_rn (dz);
+        atomicAdd (&s_db2[c], dz);
+      }
+    }
+  }
+  __syncthreads ();
+  if (grad)
+  {
+    for (int q = threadIdx.x; q < kOut * kHid; q += blockDim.x) atomicAdd (grad + kW3 + q, s_gw3[q]);
+    for (int q = threadIdx.x; q < kHid; q += blockDim.x) atomicAdd (grad + kB2 + q, s_db2[q]);
+    if (threadIdx.x < kOut) atomicAdd (grad + kB3 + threadIdx.x, s_gb3[threadIdx.x]);
+    if (threadIdx.x == 0 && loss) atomicAdd (loss, s_loss);
+  }
+}
+
+// column sums of a bf16 [rows x 128] matrix into grad[off + c]
+__global__ void colsum_kernel (const __nv_bfloat16 *__restrict__ M, int rows, float *__restrict__ out)
+{
+  __shared__ float s[kHid];
+  if (threadIdx.x < kHid) s[threadIdx.x] = 0.f;
+  __syncthreads ();
+  const int c = threadIdx.x & (kHid - 1);
+  float acc = 0.f;
+  for (int r = blockIdx.x * (blockDim.x / kHid) + threadIdx.x / kHid; r < rows;
+       r += gridDim.x * (blockDim.x / kHid))
+    acc += __bfloat162float (M[(size_t)r * kHid + c]);
+  atomicAdd (&s[c], acc);
+  __syncthreads ();
+  if (threadIdx.x < kHid) atomicAdd (out + threadIdx.x, s[threadIdx.x]);
+}
+
+// bf16 transpose [rows x cols] -> [cols x rows]
+__global__ void transpose_kernel (const __nv_bfloat16 *__restrict__ in, int rows, int cols,
+                                  __nv_bfloat16 *__restrict__ out)
+{
+  __shared__ __nv_bfloat16 t[32][33];
+  const int bx = blockIdx.x * 32, by = blockIdx.y * 32;
+  for (int j = threadIdx.y; j < 32; j += blockDim.y)
+  {
+    const int r = by + j, c = bx + threadIdx.x;
+    t[j][threadIdx.x] = (r < rows && c < cols) ? in[(size_t)r * cols + c] : __float2bfloat16_rn (0.f);
+  }
+  __syncthreads ();
+  for (int j = threadIdx.y; j < 32; j += blockDim.y)
+  {
+    const int c = bx + j, r = by + threadIdx.x;
+    if (c < cols && r < rows) out[(size_t)c * rows + r] = t[threadIdx.x][j];
+  }
+}
+
+__global__ void adam_kernel (float *__restrict__ p, const float *__restrict__ g, float *__restrict__ m,
+                             float *__restrict__ v, int n, float lr, float b1, float b2, float eps,
+                             float c1, float c2)
+{
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const float gi = g[i];
+  const float mi = b1 * m[i] + (1.f - b1) * gi;
+  const float vi = b2 * v[i] + (1.f - b2) * gi * gi;
+  m[i] = mi;
+  v[i] = vi;
+  p[i] -= lr * (mi * c1) / (sqrtf (vi * c2) + eps);
+}
+
+// ------------------------------------------------------ fused inference --
+
+struct GuessArgs
+{
+  const float *params;
+  const __nv_bfloat16 *wb;
+  const float *packed;
+  int stride;
+  const int *elem;
+  const float *pts;
+  int n;
+  float *guess;
+  int *err;
+};
+
+constexpr size_t kGuessSmem = (size_t)kHid * kInPad * 2 * 2 + (size_t)kHid * kHid * 2 * 2 + 1024;
+
+__global__ void __launch_bounds__ (128) mlp_guess_kernel (GuessArgs a)
+{
+  extern __shared__ __align__ (1024) unsigned char smem[];
+  unsigned char *sW1 = smem;                                 // 128 x 96
+  unsigned char *sW2 = sW1 + kHid * kInPad * 2;              // 128 x 128
+  unsigned char *sA1 = sW2 + kHid * kHid * 2;                // 128 x 96
+  unsigned char *sA2 = sA1 + kHid * kInPad * 2;              // 128 x 128
+  __shared__ float s_b1[kHid], s_b2[kHid], s_w3[kOut * kHid], s_b3[kOut];
+  __shared__ __align__ (8) uint64_t mbar;
+  __shared__ uint32_t tmem_base;
+  const int tid = threadIdx.x;
+  const int warp = tid >> 5;
+  // weights into the interleaved layout (once per CTA)
+  for (int v = tid; v < kHid * (kInPad / 8); v += 128)
+  {
+    const int r = v / (kInPad / 8), j = v - r * (kInPad / 8);
+    *reinterpret_cast<uint4 *> (sW1 + umma::tile_offset (r, 8 * j, kInPad)) =
+    *reinterpret_cast<const uint4 *> (a.wb + kBW1 + (size_t)r * kInPad + 8 * j);
+  }
+  for (int v = tid; v < kHid * (kHid / 8); v += 128)
+  {
+    const int r = v / (kHid / 8), j = v - r * (kHid / 8);
+    *reinterpret_cast<uint4 *> (sW2 + umma::tile_offset (r, 8 * j, kHid)) =
+    *reinterpret_cast<const uint4 *> (a.wb + kBW2 + (size_t)r * kHid + 8 * j);
+  }
+  for (int q = tid; q < kHid; q += 128)
+  {
+    s_b1[q] = a.params[kB1 + q];
+    s_b2[q] = a.params[kB2 + q];
+  }
+  for (int q = tid; q < kOut * kHid; q += 128) s_w3[q] = a.params[kW3 + q];
+  if (tid < kOut) s_b3[tid] = a.params[kB3 + tid];
+  if (warp == 0) umma::tmem_alloc (&tmem_base, 2 * kHid);
+  if (tid == 0) umma::mbar_init (&mbar, 1);
+  umma::fence_before_sync ();
+  __syncthreads ();
+  umma::fence_after_sync ();
+  const uint32_t t1 = tmem_base;          // D1: columns [0, 128)
+  const uint32_t t2 = tmem_base + kHid;   // D2: columns [128, 256)
+  const uint32_t lane_off = (uint32_t)(warp * 32) << 16;
+  const uint32_t idesc = umma::idesc_bf16_f32 (128, kHid);
+  uint32_t phase = 0;
+  bool ok = true;
+  const int tiles = (a.n + 127) / 128;
+  for (int tile = blockIdx.x; tile < tiles && ok; tile += gridDim.x)
+  {
+    const int i = tile * 128 + tid;
+    const int e = (i < a.n) ? a.elem[i] : -1;
+    {
+      float f[kInPad];
+      if (e >= 0)
+      {
+        const float pt[3] = { a.pts[3 * (size_t)i], a.pts[3 * (size_t)i + 1], a.pts[3 * (size_t)i + 2] };
+        pair_features (a.packed + (size_t)e * a.stride, pt, f);
+      }
+      else
+      {
+#pragma unroll
+        for (int q = 0; q < kInPad; ++q) f[q] = 0.f;
+      }
+      store_row_bf16<kInPad> (sA1, tid, f);
+    }
+    umma::fence_async_smem ();
+    __syncthreads ();
+    if (tid == 0)
+    {
+      umma::fence_after_sync ();
+      const uint32_t a0 = umma::smem_addr (sA1), b0 = umma::smem_addr (sW1);
+#pragma unroll
+      for (int kk = 0; kk < kInPad / 16; ++kk)
+        umma::mma_bf16 (t1, umma::desc_kmajor (a0 + kk * 256, 128, (kInPad / 8) * 128),
+                        umma::desc_kmajor (b0 + kk * 256, 128, (kInPad / 8) * 128), idesc,
+                        kk > 0 ? 1u : 0u);
+      umma::mma_commit (&mbar);
+    }
+    ok = umma::mbar_wait (&mbar, phase, kWaitTries);
+    phase ^= 1u;
+    umma::fence_after_sync ();
+    if (!__syncthreads_and (ok)) break;
+    // layer 1 epilogue -> A2 (bf16 GELU activations)
+    for (int c0 = 0; c0 < kHid; c0 += 32)
+    {
+      float d[32];
+      umma::tmem_ld32 (t1 + lane_off + c0, d);
+#pragma unroll
+      for (int j = 0; j < 32; ++j) d[j] = gelu (d[j] + s_b1[c0 + j]);
+#pragma unroll
+      for (int k8 = 0; k8 < 4; ++k8)
+      {
+        __align__ (16) __nv_bfloat16 b[8];
+#pragma unroll
+        for (int j = 0; j < 8; ++j) b[j] = __float2bfloat16_rn (d[8 * k8 + j]);
+        *reinterpret_cast<uint4 *> (sA2 + umma::tile_offset (tid, c0 + 8 * k8, kHid)) =
+        *reinterpret_cast<const uint4 *> (b);
+      }
+    }
+    umma::fence_async_smem ();
+    umma::fence_before_sync ();
+    __syncthreads ();
+    if (tid == 0)
+    {
+      umma::fence_after_sync ();
+      const uint32_t a0 = umma::smem_addr (sA2), b0 = umma::smem_addr (sW2);
+#pragma unroll
+      for (int kk = 0; kk < kHid / 16; ++kk)
+        umma::mma_bf16 (t2, umma::desc_kmajor (a0 + kk * 256, 128, (kHid / 8) * 128),
+                        umma::desc_kmajor (b0 + kk * 256, 128, (kHid / 8) * 128), idesc,
+                        kk > 0 ? 1u : 0u);
+      umma::mma_commit (&mbar);
+    }
+    ok = umma::mbar_wait (&mbar, phase, kWaitTries);
+    phase ^= 1u;
+    umma::fence_after_sync ();
+    if (!__syncthreads_and (ok)) break;
+    // layer 2 epilogue + 128 -> 3 head on the CUDA cores
+    float y[kOut] = { s_b3[0], s_b3[1], s_b3[2] };
+    for (int c0 = 0; c0 < kHid; c0 += 32)
+    {
+      float d[32];
+      umma::tmem_ld32 (t2 + lane_off + c0, d);
+#pragma unroll
+      for (int j = 0; j < 32; ++j)
+      {
+        const float h = gelu (d[j] + s_b2[c0 + j]);
+#pragma unroll
+        for (int o = 0; o < kOut; ++o) y[o] = fmaf (s_w3[o * kHid + c0 + j], h, y[o]);
+      }
+    }
+    if (i < a.n)
+    {
+#pragma unroll
+      for (int o = 0; o < kOut; ++o)
+        a.guess[3 * (size_t)i + o] = (e >= 0) ? fminf (1.f, fmaxf (0.f, y[o])) : 0.5f;
+    }
+    umma::fence_before_sync ();
+    __syncthreads ();
+  }
+  if (!ok && tid == 0 && a.err) atomicExch (a.err, 1);
+  umma::fence_before_sync ();
+  __syncthreads ();
+  if (warp == 0) umma::tmem_dealloc (tmem_base, 2 * kHid);
+}
+
+template <int EPI> int launch_gemm (const GemmArgs &g, cudaStream_t s)
+{
+  const size_t smem = (size_t)128 * kKC * 2 + (size_t)kGemmN * kKC * 2;
+  // at most 4 CTAs per SM so that their TMEM (128 columns each) always fits
+  const size_t smem_req = smem < 48 * 1024 ? 48 * 1024 : smem;
+  cudaFuncSetAttribute (gemm_kernel<EPI>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_req);
+  dim3 grid ((unsigned)div_up (g.M, 128), (unsigned)div_up (g.K, g.k_split));
+  gemm_kernel<EPI><<<grid, 128, smem_req, s>>> (g);
+  return check_launch ("gemm_kernel");
+}
+
+} // namespace mlp
+} // namespace drb
+
+using namespace drb;
+using namespace drb::mlp;
+
+extern "C" int drb_mlp_param_count (void) { return kParams; }
+extern "C" int drb_mlp_bf16_count (void) { return kBf16; }
+
+extern "C" int drb_mlp_prepare (const float *params, void *wbf16, void *stream)
+{
+  if (!params || !wbf16)
+  {
+    set_last_error ("mlp_prepare: bad arguments");
+    return DRB_ERR_INVALID_ARG;
+  }
+  prepare_kernel<<<div_up (kHid * kHid, 256), 256, 0, (cudaStream_t)stream>>> (
+  params, (__nv_bfloat16 *)wbf16);
+  return check_launch ("prepare_kernel");
+}
+
+extern "C" int drb_mlp_features (const drb_mesh *mesh, const int *elem, const float *pts, int n,
+                                 int n_pad, void *X, void *stream)
+{
+  if (!mesh || !mesh->packed || mesh->dim != 3 || mesh->order != 2 || mesh->ncomp != 3 ||
+      n < 0 || n_pad < n || (n_pad > 0 && !X) || (n > 0 && (!elem || !pts)))
+  {
+    set_last_error ("mlp_features: needs a packed order-2 hex mesh and n <= n_pad");
+    return DRB_ERR_INVALID_ARG;
+  }
+  if (n_pad == 0) return DRB_OK;
+  features_kernel<<<div_up (n_pad, 128), 128, 0, (cudaStream_t)stream>>> (
+  mesh->packed, packed_stride (27, 3), elem, pts, n, n_pad, (__nv_bfloat16 *)X);
+  return check_launch ("features_kernel");
+}
+
+// Workspace of one training step over n_pad rows (multiple of 128):
+// Z1, Z2 fp32 [n_pad x 128]; H1, H2, dZ2, dZ1 bf16 [n_pad x 128];
+// transposes dZ2T, H1T, dZ1T bf16 [128 x n_pad], XT bf16 [96 x n_pad].
+extern "C" long long drb_mlp_workspace_bytes (int n_pad)
+{
+  const long long r = n_pad;
+  return r * kHid * 4 * 2 + r * kHid * 2 * 4 + r * kHid * 2 * 3 + r * kInPad * 2 + 4096;
+}
+
+extern "C" int drb_mlp_forward (const float *params, const void *wbf16, const void *X, int n,
+                                int n_pad, float *y, void *workspace, int *err, void *stream)
+{
+  if (!params || !wbf16 || !X || !y || !workspace || n < 0 || n_pad < n || (n_pad % 128))
+  {
+    set_last_error ("mlp_forward: bad arguments (n_pad must be a multiple of 128 and >= n)");
+    return DRB_ERR_INVALID_ARG;
+  }
+  if (n_pad == 0) return DRB_OK;
+  cudaStream_t s = (cudaStream_t)stream;
+  unsigned char *w = (unsigned char *)workspace;
+  float *Z1 = (float *)w;
+  float *Z2 = Z1 + (size_t)n_pad * kHid;
+  __nv_bfloat16 *H1 = (__nv_bfloat16 *)(Z2 + (size_t)n_pad * kHid);
+  __nv_bfloat16 *H2 = H1 + (size_t)n_pad * kHid;
+  const __nv_bfloat16 *wb = (const __nv_bfloat16 *)wbf16;
+  GemmArgs g{};
+  g.A = (const __nv_bfloat16 *)X;
+  g.B = wb + kBW1;
+  g.M = n_pad;
+  g.N = kHid;
+  g.K = kInPad;
+  g.k_split = kInPad;
+  g.bias = params + kB1;
+  g.C = Z1;
+  g.H = H1;
+  g.err = err;
+  int st = launch_gemm<EPI_BIAS_GELU> (g, s);
+  if (st) return st;
+  g.A = H1;
+  g.B = wb + kBW2;
+  g.K = kHid;
+  g.k_split = kHid;
+  g.bias = params + kB2;
+  g.C = Z2;
+  g.H = H2;
+  if ((st = launch_gemm<EPI_BIAS_GELU> (g, s))) return st;
+  head_kernel<<<div_up (n_pad, 128), 128, 0, s>>> (params, Z2, nullptr, nullptr, n, n_pad, 0.f, y,
+                                                   nullptr, nullptr, nullptr);
+  return check_launch ("head_kernel");
+}
+
+extern "C" int drb_mlp_train_step (const float *params, const void *wbf16, const void *X,
+                                   const float *target, const float *weight, int n, int n_pad,
+                                   float *grad, float *loss, void *workspace, int *err,
+                                   void *stream)
+{
+  if (!params || !wbf16 || !X || !target || !grad || !workspace || n < 1 || n_pad < n ||
+      (n_pad % 128))
+  {
+    set_last_error ("mlp_train_step: bad arguments (n_pad must be a multiple of 128 and >= n)");
+    return DRB_ERR_INVALID_ARG;
+  }
+  cudaStream_t s = (cudaStream_t)stream;
+  unsigned char *w = (unsigned char *)workspace;
+  const size_t R = (size_t)n_pad;
+  float *Z1 = (float *)w;
+  float *Z2 = Z1 + R * kHid;
+  __nv_bfloat16 *H1 = (__nv_bfloat16 *)(Z2 + R * kHid);
+  __nv_bfloat16 *H2 = H1 + R * kHid;
+  __nv_bfloat16 *dZ2 = H2 + R * kHid;
+  __nv_bfloat16 *dZ1 = dZ2 + R * kHid;
+  __nv_bfloat16 *dZ2T = dZ1 + R * kHid;
+  __nv_bfloat16 *H1T = dZ2T + R * kHid;
+  __nv_bfloat16 *dZ1T = H1T + R * kHid;
+  __nv_bfloat16 *XT = dZ1T + R * kHid;
+  const __nv_bfloat16 *wb = (const __nv_bfloat16 *)wbf16;
+  cudaMemsetAsync (grad, 0, sizeof (float) * kParams, s);
+  if (loss) cudaMemsetAsync (loss, 0, sizeof (float), s);
+  // forward
+  GemmArgs g{};
+  g.A = (const __nv_bfloat16 *)X;
+  g.B = wb + kBW1;
+  g.M = n_pad;
+  g.N = kHid;
+  g.K = kInPad;
+  g.k_split = kInPad;
+  g.bias = params + kB1;
+  g.C = Z1;
+  g.H = H1;
+  g.err = err;
+  int st = launch_gemm<EPI_BIAS_GELU> (g, s);
+  if (st) return st;
+  g.A = H1;
+  g.B = wb + kBW2;
+  g.K = kHid;
+  g.k_split = kHid;
+  g.bias = params + kB2;
+  g.C = Z2;
+  g.H = H2;
+  if ((st = launch_gemm<EPI_BIAS_GELU> (g, s))) return st;
+  // head, loss, dW3, db3, dZ2, db2
+  head_kernel<<<div_up (n_pad, 128), 128, 0, s>>> (params, Z2, target, weight, n, n_pad,
+                                                   1.f / (float)n, nullptr, grad, dZ2, loss);
+  if ((st = check_launch ("head_kernel"))) return st;
+  // dZ1 = (dZ2 W2) x gelu'(Z1): B operand is W2^T
+  GemmArgs b{};
+  b.A = dZ2;
+  b.B = wb + kBW2T;
+  b.M = n_pad;
+  b.N = kHid;
+  b.K = kHid;
+  b.k_split = kHid;
+  b.Zin = Z1;
+  b.H = dZ1;
+  b.err = err;
+  if ((st = launch_gemm<EPI_GELU_GRAD> (b, s))) return st;
+  colsum_kernel<<<min (div_up (n_pad, 2), 1024), 256, 0, s>>> (dZ1, n_pad, grad + kB1);
+  if ((st = check_launch ("colsum_kernel"))) return st;
+  // transposes for the weight gradients (K = batch)
+  dim3 tb (32, 8);
+  transpose_kernel<<<dim3 (kHid / 32, div_up (n_pad, 32)), tb, 0, s>>> (dZ2, n_pad, kHid, dZ2T);
+  transpose_kernel<<<dim3 (kHid / 32, div_up (n_pad, 32)), tb, 0, s>>> (H1, n_pad, kHid, H1T);
+  transpose_kernel<<<dim3 (kHid / 32, div_up (n_pad, 32)), tb, 0, s>>> (dZ1, n_pad, kHid, dZ1T);
+  transpose_kernel<<<dim3 (kInPad / 32, div_up (n_pad, 32)), tb, 0, s>>> ((const __nv_bfloat16 *)X, n_pad, kInPad, XT);
+  if ((st = check_launch ("transpose_kernel"))) return st;
+  const int ksplit = n_pad <= 1024 ? ((n_pad + kKC - 1) / kKC) * kKC : 1024;
+  // dW2 = dZ2^T H1
+  GemmArgs d2{};
+  d2.A = dZ2T;
+  d2.B = H1T;
+  d2.M = kHid;
+  d2.N = kHid;
+  d2.K = n_pad;
+  d2.k_split = ksplit;
+  d2.C = grad + kW2;
+  d2.ldc = kHid;
+  d2.ncols = kHid;
+  d2.err = err;
+  if ((st = launch_gemm<EPI_ATOMIC> (d2, s))) return st;
+  // dW1 = dZ1^T X (first 84 of 96 columns)
+  GemmArgs d1{};
+  d1.A = dZ1T;
+  d1.B = XT;
+  d1.M = kHid;
+  d1.N = kInPad;
+  d1.K = n_pad;
+  d1.k_split = ksplit;
+  d1.C = grad + kW1;
+  d1.ldc = kIn;
+  d1.ncols = kIn;
+  d1.err = err;
+  return launch_gemm<EPI_ATOMIC> (d1, s);
+}
+
+extern "C" int drb_mlp_adam (float *params, const float *grad, float *m, float *v, float lr,
+                             float beta1, float beta2, float eps, int step, void *stream)
+{
+  if (!params || !grad || !m || !v || step < 1)
+  {
+    set_last_error ("mlp_adam: bad arguments");
+    return DRB_ERR_INVALID_ARG;
+  }
+  const float c1 = 1.f / (1.f - powf (beta1, (float)step));
+  const float c2 = 1.f / (1.f - powf (beta2, (float)step));
+  adam_kernel<<<div_up (kParams, 256), 256, 0, (cudaStream_t)stream>>> (params, grad, m, v, kParams, lr,
+                                                                        beta1, beta2, eps, c1, c2);
+  return check_launch ("adam_kernel");
+}
+
+extern "C" int drb_mlp_guess (const float *params, const void *wbf16, const drb_mesh *mesh,
+                              const int *elem, const float *pts, int n, float *guess, int *err,
+                              void *stream)
+{
+  if (!params || !wbf16 || !mesh || !mesh->packed || mesh->dim != 3 || mesh->order != 2 ||
+      mesh->ncomp != 3 || n < 0 || (n > 0 && (!elem || !pts || !guess)))
+  {
+    set_last_error ("mlp_guess: needs a packed order-2 hex mesh");
+    return DRB_ERR_INVALID_ARG;
+  }
+  if (n == 0) return DRB_OK;
+  GuessArgs a;
+  a.params = params;
+  a.wb = (const __nv_bfloat16 *)wbf16;
+  a.packed = mesh->packed;
+  a.stride = packed_stride (27, 3);
+  a.elem = elem;
+  a.pts = pts;
+  a.n = n;
+  a.guess = guess;
+  a.err = err;
+  cudaFuncSetAttribute (mlp_guess_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kGuessSmem);
+  const int tiles = div_up (n, 128);
+  const int grid = min (tiles, sm_count ());
+  mlp_guess_kernel<<<grid, 128, kGuessSmem, (cudaStream_t)stream>>> (a);
+  return check_launch ("mlp_guess_kernel");
+}

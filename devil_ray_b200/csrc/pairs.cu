@@ -1,0 +1,137 @@
+// Per-(element, point) kernels used to generate and judge the learned guess:
+//   map_points_kernel    physical point X_e(r) of reference points r
+//                        (Element::eval, pos_tensor_element.tcc:99-232)
+//   newton_pairs_kernel  Newton inversion of each point in a given element
+//                        (eval_inverse_local, data_model/element.hpp:435-486)
+//                        from the element centre or a given guess; the
+//                        labels of the training set are these solutions.
+#include "drb_common.cuh"
+#include "drb_internal.h"
+#include "newton.cuh"
+
+namespace drb
+{
+namespace
+{
+
+template <int P>
+__global__ void map_points_kernel (const float *__restrict__ packed, int stride,
+                                   const int *__restrict__ elem, const float *__restrict__ ref,
+                                   int n, float *__restrict__ pts)
+{
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const int e = elem[i];
+  float X[3] = { NAN, NAN, NAN };
+  if (e >= 0)
+  {
+    PackedCP cp{ packed + (size_t)e * stride };
+    hex_eval<P, 3> (cp, ref[3 * (size_t)i], ref[3 * (size_t)i + 1], ref[3 * (size_t)i + 2], X);
+  }
+  pts[3 * (size_t)i] = X[0];
+  pts[3 * (size_t)i + 1] = X[1];
+  pts[3 * (size_t)i + 2] = X[2];
+}
+
+template <int P>
+__global__ void newton_pairs_kernel (const float *__restrict__ packed, int stride,
+                                     const int *__restrict__ elem, const float *__restrict__ pts,
+                                     int n, float tol, int max_steps,
+                                     const float *__restrict__ guess, float *__restrict__ ref,
+                                     int *__restrict__ found, int *__restrict__ iters)
+{
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const int e = elem[i];
+  float x[3] = { 0.5f, 0.5f, 0.5f };
+  if (guess)
+  {
+    x[0] = guess[3 * (size_t)i];
+    x[1] = guess[3 * (size_t)i + 1];
+    x[2] = guess[3 * (size_t)i + 2];
+  }
+  int steps = 0;
+  bool ok = false;
+  if (e >= 0)
+  {
+    const float pt[3] = { pts[3 * (size_t)i], pts[3 * (size_t)i + 1], pts[3 * (size_t)i + 2] };
+    const float *row = packed + (size_t)e * stride;
+    if (P <= 2)
+    {
+      RegCP<3 * (P + 1) * (P + 1) * (P + 1)> r;
+      load_reg_cp<P> (r, row);
+      ok = hex_newton<P> (r, pt, x, tol, max_steps, steps);
+    }
+    else
+    {
+      PackedCP cp{ row };
+      ok = hex_newton<P> (cp, pt, x, tol, max_steps, steps);
+    }
+  }
+  ref[3 * (size_t)i] = x[0];
+  ref[3 * (size_t)i + 1] = x[1];
+  ref[3 * (size_t)i + 2] = x[2];
+  if (found) found[i] = ok ? 1 : 0;
+  if (iters) iters[i] = steps;
+}
+
+int check_pairs (const drb_mesh *m, int n)
+{
+  if (!m || !m->packed || m->dim != 3 || m->ncomp != 3 || m->order < 1 || m->order > 3 || n < 0)
+  {
+    set_last_error ("pairs: needs a packed hex geometry mesh of order 1..3");
+    return DRB_ERR_INVALID_ARG;
+  }
+  return DRB_OK;
+}
+
+} // namespace
+} // namespace drb
+
+using namespace drb;
+
+extern "C" int drb_map_points (const drb_mesh *mesh, const int *elem, const float *ref, int n,
+                               float *pts, void *stream)
+{
+  int st = check_pairs (mesh, n);
+  if (st) return st;
+  if (n == 0) return DRB_OK;
+  if (!elem || !ref || !pts)
+  {
+    set_last_error ("map_points: NULL array");
+    return DRB_ERR_INVALID_ARG;
+  }
+  const int nd = (mesh->order + 1) * (mesh->order + 1) * (mesh->order + 1);
+  const int stride = packed_stride (nd, 3);
+  cudaStream_t s = (cudaStream_t)stream;
+  const int b = div_up (n, 256);
+  if (mesh->order == 1) map_points_kernel<1><<<b, 256, 0, s>>> (mesh->packed, stride, elem, ref, n, pts);
+  else if (mesh->order == 2) map_points_kernel<2><<<b, 256, 0, s>>> (mesh->packed, stride, elem, ref, n, pts);
+  else map_points_kernel<3><<<b, 256, 0, s>>> (mesh->packed, stride, elem, ref, n, pts);
+  return check_launch ("map_points_kernel");
+}
+
+extern "C" int drb_newton_pairs (const drb_mesh *mesh, const int *elem, const float *pts, int n,
+                                 float tol, int max_steps, const float *guess, float *ref,
+                                 int *found, int *iters, void *stream)
+{
+  int st = check_pairs (mesh, n);
+  if (st) return st;
+  if (n == 0) return DRB_OK;
+  if (!elem || !pts || !ref || !(tol > 0.f) || max_steps < 0)
+  {
+    set_last_error ("newton_pairs: bad arguments");
+    return DRB_ERR_INVALID_ARG;
+  }
+  const int nd = (mesh->order + 1) * (mesh->order + 1) * (mesh->order + 1);
+  const int stride = packed_stride (nd, 3);
+  cudaStream_t s = (cudaStream_t)stream;
+  const int b = div_up (n, 128);
+  if (mesh->order == 1)
+    newton_pairs_kernel<1><<<b, 128, 0, s>>> (mesh->packed, stride, elem, pts, n, tol, max_steps, guess, ref, found, iters);
+  else if (mesh->order == 2)
+    newton_pairs_kernel<2><<<b, 128, 0, s>>> (mesh->packed, stride, elem, pts, n, tol, max_steps, guess, ref, found, iters);
+  else
+    newton_pairs_kernel<3><<<b, 128, 0, s>>> (mesh->packed, stride, elem, pts, n, tol, max_steps, guess, ref, found, iters);
+  return check_launch ("newton_pairs_kernel");
+}

@@ -272,6 +272,8 @@ struct VolumeParams
   int use_lighting;
   int coherent;
   float sample_dist;
+  int cull;
+  CullBox box;
 };
 
 template <int P> struct FieldCP
@@ -456,7 +458,21 @@ volume_kernel (VolumeParams vp, const Ray *__restrict__ rays, int n_rays, int *_
     if (base >= n_rays) break;
     const int i = base + lane;
     if (i >= n_rays) continue;
-    const Ray ray = rays[i];
+    Ray ray = rays[i];
+    if (vp.cull)
+    {
+      // mark_active + calc_ray_start (ray.cpp:117-241) on the raw ray
+      float t0, t1;
+      if (!slab (ray, vp.box, t0, t1))
+      {
+        if (ray_samples) ray_samples[i] = 0;
+        if (ray_iters) ray_iters[i] = 0;
+        if (ray_cands) ray_cands[i] = 0;
+        continue;
+      }
+      ray.near_t = t0;
+      ray.far_t = t1;
+    }
     float distance = ray.near_t + vp.sample_dist;
     int segment = 0;
     float4 pixel = make_float4 (0.f, 0.f, 0.f, 0.f);
@@ -867,6 +883,8 @@ static int volume_common (const drb_mesh *mesh, const drb_mesh *field, const drb
   vp.n_lights = n_lights;
   vp.use_lighting = o->use_lighting;
   vp.coherent = o->coherent;
+  vp.cull = o->cull;
+  vp.box = cull_box (bvh->bounds);
   // sample distance: |bounds diagonal| / samples (volume.cpp:89-91)
   const float *b = o->bounds;
   float dd[3] = { b[1] - b[0], b[3] - b[2], b[5] - b[4] };

@@ -241,6 +241,9 @@ typedef struct drb_volume_opts
   int guess_mode;         /* drb_guess_mode for full locates */
   int coherent;           /* 1: try the previous sample's element first */
   float bounds[6];        /* Collection::bounds of the data (sample distance) */
+  int cull;               /* 1: rays are raw camera rays; the march applies the
+                             slab test of remove_missed_rays itself (no
+                             compaction, no host synchronisation) */
 } drb_volume_opts;
 
 /* Camera::create_rays / gen_perspective (rendering/camera.cpp:219-483):
@@ -328,6 +331,56 @@ int drb_surface_shade (const drb_mesh *faces, const drb_mesh *face_field, const 
 
 /* ray_max (ray.cpp:243-259): far = hit distance for rays that hit. */
 int drb_ray_max (void *rays, const void *hits, int n, void *stream);
+
+/* -------------------------------------------- learned initial guess --
+ * No counterpart in the reference.  A small MLP (27 control points x 3 +
+ * point x 3 = 84 inputs -> 128 -> 128 -> 3, GELU) predicts the reference
+ * coordinates of a point in an order-2 hex candidate element.  Parameters:
+ * one fp32 vector of drb_mlp_param_count() floats (W1 [128 x 84], b1,
+ * W2 [128 x 128], b2, W3 [3 x 128], b3); bf16 tensor-core operands:
+ * drb_mlp_bf16_count() values written by drb_mlp_prepare.  Tensor-core
+ * kernels report a bounded-wait timeout through *err (device int32). */
+int drb_mlp_param_count (void);
+int drb_mlp_bf16_count (void);
+long long drb_mlp_workspace_bytes (int n_pad);
+int drb_mlp_prepare (const float *params, void *wbf16, void *stream);
+/* features of (element, point) pairs: X device bf16 [n_pad x 96] */
+int drb_mlp_features (const drb_mesh *mesh, const int *elem, const float *pts, int n, int n_pad,
+                      void *X, void *stream);
+/* forward: y device float[3n]; n_pad multiple of 128 */
+int drb_mlp_forward (const float *params, const void *wbf16, const void *X, int n, int n_pad,
+                     float *y, void *workspace, int *err, void *stream);
+/* one training step: masked MSE against target (device float[3n], weight
+ * optional device float[n]); grad (device float[param_count]) and *loss */
+int drb_mlp_train_step (const float *params, const void *wbf16, const void *X,
+                        const float *target, const float *weight, int n, int n_pad, float *grad,
+                        float *loss, void *workspace, int *err, void *stream);
+int drb_mlp_adam (float *params, const float *grad, float *m, float *v, float lr, float beta1,
+                  float beta2, float eps, int step, void *stream);
+/* fused tensor-core inference: guess device float[3n] for the pairs */
+int drb_mlp_guess (const float *params, const void *wbf16, const drb_mesh *mesh,
+                   const int *elem, const float *pts, int n, float *guess, int *err,
+                   void *stream);
+
+/* Physical points X_e(r) (Element::eval, pos_tensor_element.tcc:99-232). */
+int drb_map_points (const drb_mesh *mesh, const int *elem, const float *ref, int n, float *pts,
+                    void *stream);
+/* Newton in a given element per point (eval_inverse_local,
+ * data_model/element.hpp:435-486): guess NULL = element centre. */
+int drb_newton_pairs (const drb_mesh *mesh, const int *elem, const float *pts, int n, float tol,
+                      int max_steps, const float *guess, float *ref, int *found, int *iters,
+                      void *stream);
+/* First candidate leaf (and element) of each query in the traversal order of
+ * DeviceMesh::locate (device_mesh.hpp:248-318); -1 when there is none. */
+int drb_first_candidates (const drb_bvh *bvh, const float *pts, int n, const int *order,
+                          int *first_leaf, int *first_elem, void *stream);
+/* Persistent locate that starts at each query's first candidate (guess from
+ * opts, element-centre fallback) and resumes the traversal only when that
+ * fails; results equal drb_locate with the same options. */
+int drb_locate_hinted (const drb_mesh *mesh, const drb_bvh *bvh, const float *pts, int n,
+                       const int *order, const int *first_leaf, const drb_newton_opts *opts,
+                       const drb_locate_config *cfg, int *cell, float *ref,
+                       drb_query_stats stats, void *stream);
 
 #ifdef __cplusplus
 }
