@@ -55,6 +55,10 @@ def parse():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--cpu-sample", type=int, default=0,
                     help="reference CPU sample size (0 = sized for ~15 s)")
+    ap.add_argument("--no-learned", action="store_true", help="skip the learned-guess path")
+    ap.add_argument("--no-volume", action="store_true", help="skip the volume workload")
+    ap.add_argument("--train-samples", type=int, default=1 << 22)
+    ap.add_argument("--orbits", type=int, default=16)
     ap.add_argument("--profile", action="store_true",
                     help="profiling run: fixed launch shape, only the timed steps "
                          "(no tuning, plain/e2e/statistics/CPU legs)")
@@ -191,6 +195,131 @@ def cpu_baseline(mesh_data, queries, bvh_np):
                       f"{t:.1f} s; reference BVH build {build_s:.1f} s not timed"}
 
 
+def orbit_cameras(count, width, seed=5):
+    """Orbits about the mesh centre at the distance of the (2.5,2.5,2.5)
+    camera: azimuth k * 22.5 degrees plus a seeded elevation jitter."""
+    from devil_ray_b200.render import Camera
+    rng = np.random.default_rng(seed)
+    c = np.array([0.5, 0.5, 0.5])
+    r = float(np.linalg.norm(np.array([2.0, 2.0, 2.0])))
+    base_el = float(np.arcsin(1.0 / np.sqrt(3.0)))
+    cams = []
+    for k in range(count):
+        az = np.deg2rad(45.0 + 22.5 * k)
+        el = base_el + rng.uniform(-0.15, 0.15)
+        pos = c + r * np.array([np.cos(el) * np.cos(az), np.sin(el), np.cos(el) * np.sin(az)])
+        cams.append(Camera(width, width, tuple(float(x) for x in pos), (0.5, 0.5, 0.5),
+                           (0.0, 1.0, 0.0), 30.0))
+    return cams
+
+
+def volume_bench(dev, args, timed):
+    """128^3 order-3 volume (SURVEY config 4): 2048^2 rays, 1000 samples,
+    1024-entry transfer function, `orbits` seeded cameras replayed from one
+    CUDA graph; Newton-resolved samples/s of the coherent march and of the
+    plain march (a full BVH locate per sample, one frame)."""
+    import torch
+    from devil_ray_b200 import _lib as L
+    from devil_ray_b200 import api, meshgen
+    from devil_ray_b200.render import (ColorTable, Framebuffer, PointLight, UnstructuredField,
+                                       Volume)
+    t0 = time.perf_counter()
+    m = meshgen.workload_mesh("volume_128")
+    gen_s = time.perf_counter() - t0
+    mesh = api.UnstructuredMesh(m.ctrl_idx, m.xyz, m.order, device=dev)
+    field = UnstructuredField(m.ctrl_idx, m.field, m.order, device=dev)
+    del m
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    mesh.get_bvh()
+    e1.record()
+    torch.cuda.synchronize()
+    bvh_ms = e0.elapsed_time(e1)
+    vol = Volume(mesh, field)
+    vol.samples(1000)
+    vol.use_lighting(True)
+    t = ColorTable()
+    for p in meshgen.TF_RGB:
+        t.add_point(p[0], p[1:])
+    for p in meshgen.TF_ALPHA:
+        t.add_alpha(*p)
+    vol.color_map().color_table(t)
+    vol.tol, vol.max_steps = 1e-5, 20
+    W = 2048
+    cams = orbit_cameras(args.orbits, W)
+    lights = [PointLight.default(c) for c in cams]
+    fbs = [Framebuffer(W, W, dev) for _ in cams]
+    n = W * W
+    rays = torch.empty((n, 9), dtype=torch.float32, device=dev)
+    samp = [torch.zeros(n, dtype=torch.int32, device=dev) for _ in cams]
+    its = [torch.zeros(n, dtype=torch.int32, device=dev) for _ in cams]
+    import ctypes as C
+    from devil_ray_b200.api import _ptr, _stream
+    from devil_ray_b200.render import lights_tensor
+
+    def frame(k, coherent, stream=None):
+        cam = cams[k]
+        L.check(L.lib().drb_camera_rays(C.byref(cam.desc()), _ptr(rays), _stream(stream)), "rays")
+        fbs[k].clear(stream=stream)
+        vol.coherent = coherent
+        o = vol._opts()
+        o.cull = 1
+        tf = vol._tf()
+        rng = vol._range()
+        lt = lights_by_cam[k]
+        rs = L.DrbRayStats(samp[k].data_ptr(), its[k].data_ptr(), None)
+        L.check(L.lib().drb_volume_render(
+            C.byref(mesh.desc()), C.byref(field.desc()), C.byref(mesh.get_bvh().desc()),
+            _ptr(rays), n, C.byref(o), _ptr(tf), tf.shape[0], rng.ctypes.data_as(C.c_void_p),
+            _ptr(lt), 1, _ptr(fbs[k].colors), _ptr(fbs[k].depths), rs, _stream(stream)),
+            "drb_volume_render")
+        fbs[k].composite_background(stream)
+
+    lights_by_cam = [lights_tensor([l], dev) for l in lights]
+    vol._tf()
+    vol._range()
+    # warm up, then capture every orbit into one graph
+    frame(0, True)
+    torch.cuda.synchronize()
+    g = torch.cuda.CUDAGraph()
+    s = torch.cuda.Stream()
+    s.wait_stream(torch.cuda.current_stream())
+    with torch.cuda.stream(s):
+        frame(0, True, s)
+    torch.cuda.current_stream().wait_stream(s)
+    torch.cuda.synchronize()
+    with torch.cuda.graph(g):
+        for k in range(len(cams)):
+            frame(k, True)
+    g.replay()
+    torch.cuda.synchronize()
+    launches0 = L.lib().drb_kernel_launches()
+    ms = timed(lambda: g.replay(), 1)
+    samples = int(sum(int(x.sum().item()) for x in samp))
+    iters = int(sum(int(x.sum().item()) for x in its))
+    coherent_sps = samples / (ms * 1e-3)
+    # plain march on the first orbit (a full BVH locate for every sample)
+    frame(0, False)
+    torch.cuda.synchronize()
+    ms_plain = timed(lambda: frame(0, False), 1)
+    samples_plain = int(samp[0].sum().item())
+    img = fbs[0].image()
+    return {
+        "workload": "volume_128: 128^3 hex order 3 (2.1M elements, 69.2M sub-box leaves), "
+                    "warp 0.05, 8 Gaussian blobs; 2048^2 rays, 1000 samples, 1024-entry TF, "
+                    f"{len(cams)} orbits in one CUDA graph, tol 1e-5",
+        "metric": "Newton-resolved samples/s",
+        "coherent": {"value": coherent_sps, "ms_total": ms, "frames": len(cams),
+                     "samples": samples, "mean_iters_per_sample": iters / max(samples, 1)},
+        "plain": {"value": samples_plain / (ms_plain * 1e-3), "ms_per_frame": ms_plain,
+                  "samples": samples_plain,
+                  "note": "full BVH locate from the element centre for every sample"},
+        "speedup_coherent_vs_plain": coherent_sps / max(samples_plain / (ms_plain * 1e-3), 1e-9),
+        "bvh_build_ms": bvh_ms, "mesh_generation_s": gen_s,
+        "mean_pixel_alpha": float(img[..., 3].mean()),
+    }
+
+
 def main():
     args = parse()
     rank, world, local = dist_info()
@@ -213,12 +342,8 @@ def main():
     m = meshgen.workload_mesh(WORKLOAD)
     queries = meshgen.uniform_queries(args.queries, 1000 + rank)
     mesh = api.UnstructuredMesh(m.ctrl_idx, m.xyz, m.order, device=dev)
-    torch.cuda.synchronize()
-    t0 = time.perf_counter()
     bvh = mesh.get_bvh()
-    torch.cuda.synchronize()
-    bvh_build_ms = 1e3 * (time.perf_counter() - t0)
-    # BVH build timed again warm (first call includes lazy module loading)
+    # BVH build timed warm (the first call includes lazy module loading)
     ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     ev0.record()
     mesh.build_bvh()
@@ -230,23 +355,12 @@ def main():
     n = pts.shape[0]
     loc = api.BatchedLocator(mesh, tol=TOL, max_steps=MAX_STEPS, guess_mode=L.GUESS_ELEM_CENTER)
     if args.profile:
-        best_cfg = L.DrbLocateConfig(128, 4, 64, 1)
+        best_cfg = L.DrbLocateConfig(128, 4, 64, 1, 0)
         loc.config, tune_ms = best_cfg, 0.0
     else:
         best_cfg, tune_ms = loc.tune(pts[: min(n, 1 << 21)])
     cell = torch.empty(n, dtype=torch.int32, device=dev)
     ref = torch.empty((n, 3), dtype=torch.float32, device=dev)
-
-    def step():
-        loc.locate(pts, out=(cell, ref))
-
-    # plain path (the reference's launch pattern on the GPU) for comparison
-    def plain_step():
-        mesh.locate(pts, tol=TOL, max_steps=MAX_STEPS, guess_mode=L.GUESS_ELEM_CENTER)
-
-    for _ in range(max(args.warmup, 3)):
-        step()
-    torch.cuda.synchronize()
 
     def timed(fn, k):
         if pg:
@@ -265,42 +379,107 @@ def main():
             ms = float(t.item())
         return ms
 
-    clocks = ClockSampler(local)
-    clocks.start()
-    launches0 = L.lib().drb_kernel_launches()
-    total_ms = timed(step, args.steps)
-    launches = L.lib().drb_kernel_launches() - launches0
-    clk = clocks.stop()
-    ms_step = total_ms / args.steps
-    located = int((cell >= 0).sum().item())
+    def batched_step():
+        loc.locate(pts, out=(cell, ref))
+
+    def plain_step():
+        mesh.locate(pts, tol=TOL, max_steps=MAX_STEPS, guess_mode=L.GUESS_ELEM_CENTER)
+
+    for _ in range(max(args.warmup, 3)):
+        batched_step()
+    torch.cuda.synchronize()
     if args.profile:
+        launches0 = L.lib().drb_kernel_launches()
+        ms_step = timed(batched_step, args.steps) / args.steps
+        launches = L.lib().drb_kernel_launches() - launches0
         if rank == 0:
             print(json.dumps({"profile": True, "ms_per_step": ms_step, "queries": n,
-                              "located": located, "launches_per_step": launches / args.steps}))
+                              "located": int((cell >= 0).sum().item()),
+                              "launches_per_step": launches / args.steps}))
         if pg:
             pg.barrier()
             pg.destroy_process_group()
         return 0
-    # statistics of the same queries (untimed): iterations, candidates, nodes
+
+    # batched path (element-centre guess)
+    batched_ms = timed(batched_step, args.steps) / args.steps
+    located = int((cell >= 0).sum().item())
+    batched_value = world * located / (batched_ms * 1e-3)
     _, _, it, ca, nd = loc.locate(pts, stats=True)
-    mean_it = float(it.float().mean())
-    mean_ca = float(ca.float().mean())
-    mean_nd = float(nd.float().mean())
+    mean_it, mean_ca, mean_nd = (float(it.float().mean()), float(ca.float().mean()),
+                                 float(nd.float().mean()))
     hist = torch.bincount(it.long().clamp(max=40), minlength=41).cpu().numpy().tolist()
-    # plain path
+    # plain path: the reference's launch pattern on the GPU
     for _ in range(2):
         plain_step()
-    plain_ms = timed(plain_step, max(2, args.steps // 2)) / max(2, args.steps // 2)
-
-    # persistent kernel alone (roofline): time it separately on a fixed order
+    k_plain = max(2, args.steps // 5)
+    plain_ms = timed(plain_step, k_plain) / k_plain
+    plain_value = world * located / (plain_ms * 1e-3)
+    # persistent kernel alone (roofline), queries already ordered
     order = loc.order(pts)
     kern_ms = timed(lambda: loc.locate(pts, order=order, out=(cell, ref)), args.steps) / args.steps
 
+    head_name, head_locate = "batched (element-centre guess)", loc.locate
+    learned = None
+    if not args.no_learned and m.order == 2:
+        from devil_ray_b200 import learned as LG
+        t0 = time.perf_counter()
+        model = LG.GuessMLP(dev, seed=1)
+        losses = LG.train(model, mesh, samples=args.train_samples, batch=16384, epochs=3,
+                          lr=3e-3)
+        torch.cuda.synchronize()
+        train_s = time.perf_counter() - t0
+        model.check_err()
+        ll = LG.LearnedLocator(mesh, model, TOL, MAX_STEPS, config=best_cfg)
+        cell_l = torch.empty_like(cell)
+        ref_l = torch.empty_like(ref)
+        for _ in range(3):
+            ll.locate(pts, out=(cell_l, ref_l))
+        ms_l = timed(lambda: ll.locate(pts, out=(cell_l, ref_l)), args.steps) / args.steps
+        located_l = int((cell_l >= 0).sum().item())
+        _, _, it_l, ca_l, nd_l = ll.locate(pts, stats=True)
+        agree = float((cell_l == cell).float().mean().item())
+        hist_l = torch.bincount(it_l.long().clamp(max=40), minlength=41).cpu().numpy().tolist()
+        # fallback rate of the guessed first-candidate solves (held-out pairs)
+        he, hp, hl, hw = LG.training_set(mesh, 1 << 20, seed=12345)
+        gss = model.guess(mesh, he, hp)
+        _, fg, ig = LG.newton_pairs(mesh, he, hp, TOL, MAX_STEPS, gss)
+        _, fc, ic = LG.newton_pairs(mesh, he, hp, TOL, MAX_STEPS)
+        ok = fc
+        learned_value = world * located_l / (ms_l * 1e-3)
+        learned = {"value": learned_value, "ms_per_step": ms_l, "located": located_l,
+                   "cell_agreement_with_centre_guess": agree,
+                   "mean_newton_iters": float(it_l.float().mean()),
+                   "mean_newton_iters_centre": mean_it,
+                   "iteration_histogram": hist_l,
+                   "held_out_pairs": {"fallback_rate": float(1.0 - fg[ok].float().mean()),
+                                      "mean_iters_guess": float(ig[ok].float().mean()),
+                                      "mean_iters_centre": float(ic[ok].float().mean())},
+                   "train": {"samples": args.train_samples, "epochs": 3, "batch": 16384,
+                             "seconds": train_s, "first_loss": losses[0],
+                             "final_loss": losses[-1]},
+                   "speedup_vs_plain": learned_value / plain_value}
+        if learned_value > batched_value:
+            head_name, head_locate = "learned guess + batched", ll.locate
+
+    # headline: the faster path, timed again with clock sampling
+    def head_step():
+        head_locate(pts, out=(cell, ref))
+
+    for _ in range(2):
+        head_step()
+    clocks = ClockSampler(local)
+    clocks.start()
+    launches0 = L.lib().drb_kernel_launches()
+    ms_step = timed(head_step, args.steps) / args.steps
+    launches = L.lib().drb_kernel_launches() - launches0
+    clk = clocks.stop()
+    located = int((cell >= 0).sum().item())
     value = world * located / (ms_step * 1e-3)
 
-    # algorithmic bytes per query (SURVEY 8d formula): point 12 B + Location
-    # 16 B + per candidate one element's control points (nd x 12 B packed)
-    # and reference box 24 B + 64 B per inner node visited
+    # algorithmic bytes per query: point 12 B + Location 16 B +
+    # per candidate one element's control points (27 x 12 B packed) and its
+    # reference box (24 B) + 64 B per inner node visited
     nd_dofs = (m.order + 1) ** 3
     bytes_q = 12 + 16 + mean_ca * (nd_dofs * 12 + 24) + 64 * mean_nd
     achieved_gbs = n * bytes_q / (kern_ms * 1e-3) / 1e9
@@ -310,9 +489,10 @@ def main():
     except Exception:
         pass
     peak = peaks.get("hbm_gbs", 6650.0)
+    peak_src = "measured" if "hbm_gbs" in peaks else "fallback"
 
     # end to end through the public API: pinned host queries -> device ->
-    # batched locate -> Location records back to pinned host memory
+    # locate -> cell ids and reference points back to pinned host memory
     host_pts = torch.from_numpy(queries).pin_memory()
     host_cell = torch.empty(n, dtype=torch.int32).pin_memory()
     host_ref = torch.empty((n, 3), dtype=torch.float32).pin_memory()
@@ -320,7 +500,7 @@ def main():
 
     def e2e_step():
         dpts.copy_(host_pts, non_blocking=True)
-        loc.locate(dpts, out=(cell, ref))
+        head_locate(dpts, out=(cell, ref))
         host_cell.copy_(cell, non_blocking=True)
         host_ref.copy_(ref, non_blocking=True)
 
@@ -328,6 +508,13 @@ def main():
     e2e_ms = timed(e2e_step, args.steps) / args.steps
     e2e_located = int((host_cell >= 0).sum())
     e2e_value = world * e2e_located / (e2e_ms * 1e-3)
+
+    vol = None
+    if not args.no_volume:
+        try:
+            vol = volume_bench(dev, args, timed)
+        except Exception as exc:
+            vol = {"error": repr(exc)}
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
@@ -345,12 +532,12 @@ def main():
             "config": {"workload": "locate_64: 64^3 hex order 2, trilinear distortion 15%, "
                                    "16M uniform queries (8% outside), tol 1e-5, 20 steps",
                        "queries_per_gpu": n, "elements": m.n_elem, "bvh_leaves": bvh.n_leaf,
-                       "guess": "element centre", "launch_config": best_cfg.as_dict(),
+                       "path": head_name, "launch_config": best_cfg.as_dict(),
                        "l2": "inputs larger than L2 (201 MB queries, 553 MB BVH nodes)",
                        "parallelism": f"replicas x{world}, queries sharded, no collective"},
             "roofline": {"bound": "hbm", "achieved": achieved_gbs, "peak": peak, "unit": "GB/s",
                          "frac": achieved_gbs / peak, "traffic": None,
-                         "kernel": "locate_persistent_kernel",
+                         "peak_source": peak_src, "kernel": "locate_persistent_kernel",
                          "bytes_per_query": bytes_q, "kernel_ms": kern_ms},
             "e2e": {"value": e2e_value, "unit": "points/s",
                     "h2d_bytes_per_step": int(n * 12), "d2h_bytes_per_step": int(n * 16),
@@ -360,8 +547,13 @@ def main():
             "stats": {"located_fraction": located / n, "mean_newton_iters": mean_it,
                       "mean_candidates": mean_ca, "mean_nodes_visited": mean_nd,
                       "iteration_histogram": hist},
-            "plain": {"ms_per_step": plain_ms, "value": world * located / (plain_ms * 1e-3),
-                      "note": "one thread per query in input order (reference launch pattern)"},
+            "plain": {"ms_per_step": plain_ms, "value": plain_value,
+                      "note": "one thread per query in input order (reference launch pattern), "
+                              "element-centre guess"},
+            "batched": {"value": batched_value, "ms_per_step": batched_ms,
+                        "note": "Morton-ordered persistent kernel, element-centre guess"},
+            "learned": learned,
+            "volume": vol,
             "bvh_build_ms": bvh_build_ms, "tune_ms": tune_ms,
             "cpu_baseline": cpu,
         }

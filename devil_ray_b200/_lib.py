@@ -48,7 +48,7 @@ class DrbQueryStats(C.Structure):
 
 class DrbLocateConfig(C.Structure):
     _fields_ = [("block", C.c_int), ("blocks_per_sm", C.c_int), ("chunk", C.c_int),
-                ("sort_queries", C.c_int)]
+                ("sort_queries", C.c_int), ("reg_elements", C.c_int)]
 
     def as_dict(self):
         return {k: getattr(self, k) for k, _ in self._fields_}

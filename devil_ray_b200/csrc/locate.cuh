@@ -21,6 +21,21 @@ DRB_D void node_point_test (const float4 *__restrict__ nodes, int node, const fl
   in_right = !(p[0] < b.z || p[1] < b.w || p[2] < c.x || p[0] > c.y || p[1] > c.z || p[2] > c.w);
 }
 
+// The whole 64-byte node record in one go: boxes and child ids are issued
+// together, so a visit costs one dependent round trip instead of two.
+DRB_D void node_point_test_kids (const float4 *__restrict__ nodes, int node, const float (&p)[3],
+                                 bool &in_left, bool &in_right, int &l, int &r)
+{
+  const float4 a = __ldg (nodes + node + 0);
+  const float4 b = __ldg (nodes + node + 1);
+  const float4 c = __ldg (nodes + node + 2);
+  const float4 d = __ldg (nodes + node + 3);
+  in_left = !(p[0] < a.x || p[1] < a.y || p[2] < a.z || p[0] > a.w || p[1] > b.x || p[2] > b.y);
+  in_right = !(p[0] < b.z || p[1] < b.w || p[2] < c.x || p[0] > c.y || p[1] > c.z || p[2] > c.w);
+  l = __float_as_int (d.x);
+  r = __float_as_int (d.y);
+}
+
 struct LocateParams
 {
   const float4 *nodes;
@@ -39,7 +54,7 @@ struct LocateParams
 
 // Newton solve of one point in one element, choosing register-resident or
 // L1-read control points by order.
-template <int P>
+template <int P, bool REG = (P <= 2)>
 DRB_D bool solve_in_element (const LocateParams &lp, int el, const float (&pt)[3], float (&x)[3],
                              int &steps)
 {
@@ -47,7 +62,7 @@ DRB_D bool solve_in_element (const LocateParams &lp, int el, const float (&pt)[3
   if (lp.packed)
   {
     const float *row = lp.packed + (size_t)el * lp.stride;
-    if (P <= 2)
+    if (REG && P <= 2)
     {
       RegCP<3 * ND> r;
       load_reg_cp<P> (r, row);
@@ -89,19 +104,19 @@ DRB_D void candidate_guess (const LocateParams &lp, int leaf, long long qi, bool
 
 // Newton in one candidate element with the guess-mode fallback: a given
 // guess that does not converge is retried from the element centre.
-template <int P>
+template <int P, bool REG = (P <= 2)>
 DRB_D bool solve_candidate (const LocateParams &lp, int leaf, int el, long long qi, bool first,
                             const float (&pt)[3], float (&x)[3], int &iters)
 {
   bool given;
   candidate_guess (lp, leaf, qi, first, x, given);
   int steps = 0;
-  bool found = solve_in_element<P> (lp, el, pt, x, steps);
+  bool found = solve_in_element<P, REG> (lp, el, pt, x, steps);
   iters += steps;
   if (!found && given)
   {
     x[0] = x[1] = x[2] = 0.5f;
-    found = solve_in_element<P> (lp, el, pt, x, steps);
+    found = solve_in_element<P, REG> (lp, el, pt, x, steps);
     iters += steps;
   }
   return found;

@@ -56,7 +56,7 @@ __global__ void query_codes_kernel (const float *__restrict__ pts, int n, float 
   iota[i] = i;
 }
 
-template <int P>
+template <int P, bool REG>
 __global__ void locate_persistent_kernel (LocateParams lp, const float *__restrict__ pts,
                                           const int *__restrict__ order, int n, int chunk,
                                           int *__restrict__ queue_head, int *__restrict__ cell,
@@ -123,8 +123,9 @@ __global__ void locate_persistent_kernel (LocateParams lp, const float *__restri
         if (cur > -1)
         {
           bool in_l, in_r;
+          int l, r;
           ++nodes;
-          node_point_test (lp.nodes, cur, pt, in_l, in_r);
+          node_point_test_kids (lp.nodes, cur, pt, in_l, in_r, l, r);
           if (!in_l && !in_r)
           {
             cur = todo[sp];
@@ -132,9 +133,6 @@ __global__ void locate_persistent_kernel (LocateParams lp, const float *__restri
           }
           else
           {
-            const float4 ch = __ldg (lp.nodes + cur + 3);
-            const int l = __float_as_int (ch.x);
-            const int r = __float_as_int (ch.y);
             cur = in_l ? l : r;
             if (in_l && in_r && sp < kStackDepth - 1) todo[++sp] = r;
           }
@@ -157,7 +155,7 @@ __global__ void locate_persistent_kernel (LocateParams lp, const float *__restri
       {
         const int el = __ldg (lp.leaf_nodes + leaf);
         ++cands;
-        const bool found = solve_candidate<P> (lp, leaf, el, qi, first, pt, x, iters);
+        const bool found = solve_candidate<P, REG> (lp, leaf, el, qi, first, pt, x, iters);
         first = false;
         if (found)
         {
@@ -190,29 +188,29 @@ __global__ void locate_persistent_kernel (LocateParams lp, const float *__restri
   }
 }
 
-template <int P> const void *persistent_fn ()
+const void *persistent_fn (int order, bool reg)
 {
-  return (const void *)locate_persistent_kernel<P>;
+  if (order == 1) return reg ? (const void *)locate_persistent_kernel<1, true> : (const void *)locate_persistent_kernel<1, false>;
+  if (order == 2) return reg ? (const void *)locate_persistent_kernel<2, true> : (const void *)locate_persistent_kernel<2, false>;
+  return (const void *)locate_persistent_kernel<3, false>;
 }
 
-int launch_persistent (int order, dim3 grid, int block, cudaStream_t s, const LocateParams &lp,
-                       const float *pts, const int *ord, int n, int chunk, int *head, int *cell,
-                       float *ref, drb_query_stats st)
+int launch_persistent (int order, bool reg, dim3 grid, int block, cudaStream_t s,
+                       const LocateParams &lp, const float *pts, const int *ord, int n, int chunk,
+                       int *head, int *cell, float *ref, drb_query_stats st)
 {
-  if (order == 1)
-    locate_persistent_kernel<1><<<grid, block, 0, s>>> (lp, pts, ord, n, chunk, head, cell, ref, st.iters, st.candidates, st.nodes);
-  else if (order == 2)
-    locate_persistent_kernel<2><<<grid, block, 0, s>>> (lp, pts, ord, n, chunk, head, cell, ref, st.iters, st.candidates, st.nodes);
-  else
-    locate_persistent_kernel<3><<<grid, block, 0, s>>> (lp, pts, ord, n, chunk, head, cell, ref, st.iters, st.candidates, st.nodes);
+#define DRB_LP(P, R) locate_persistent_kernel<P, R><<<grid, block, 0, s>>> (lp, pts, ord, n, chunk, head, cell, ref, st.iters, st.candidates, st.nodes)
+  if (order == 1) { if (reg) DRB_LP (1, true); else DRB_LP (1, false); }
+  else if (order == 2) { if (reg) DRB_LP (2, true); else DRB_LP (2, false); }
+  else DRB_LP (3, false);
+#undef DRB_LP
   return check_launch ("locate_persistent_kernel");
 }
 
-int resident_blocks (int order, int block)
+int resident_blocks (int order, bool reg, int block)
 {
   int nb = 0;
-  const void *fn = order == 1 ? persistent_fn<1> () : (order == 2 ? persistent_fn<2> () : persistent_fn<3> ());
-  cudaOccupancyMaxActiveBlocksPerMultiprocessor (&nb, fn, block, 0);
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor (&nb, persistent_fn (order, reg), block, 0);
   return nb > 0 ? nb : 1;
 }
 
@@ -267,6 +265,7 @@ drb_locate_config default_config (int order)
   c.blocks_per_sm = 0; // 0 = all resident blocks
   c.chunk = 64;
   c.sort_queries = 1;
+  c.reg_elements = 0;
   (void)order;
   return c;
 }
@@ -324,7 +323,8 @@ int locate_batched_impl (const drb_mesh *mesh, const drb_bvh *bvh, const float *
   }
   if (scr.err != cudaSuccess) return status_from (scr.err);
   cudaMemsetAsync (head, 0, sizeof (int), s);
-  const int per_sm = resident_blocks (mesh->order, cfg.block);
+  const bool reg = cfg.reg_elements != 0;
+  const int per_sm = resident_blocks (mesh->order, reg, cfg.block);
   const int bps = (cfg.blocks_per_sm > 0) ? min (cfg.blocks_per_sm, per_sm) : per_sm;
   const long long warps_needed = ((long long)n + 31) / 32;
   long long blocks = (long long)bps * sm_count ();
@@ -332,7 +332,7 @@ int locate_batched_impl (const drb_mesh *mesh, const drb_bvh *bvh, const float *
   if (blocks > blocks_needed) blocks = blocks_needed;
   if (blocks < 1) blocks = 1;
   const LocateParams lp = make_params (mesh, bvh, opts);
-  return launch_persistent (mesh->order, dim3 ((unsigned)blocks), cfg.block, s, lp, pts, ord, n,
+  return launch_persistent (mesh->order, reg, dim3 ((unsigned)blocks), cfg.block, s, lp, pts, ord, n,
                             cfg.chunk, head, cell, ref, stats);
 }
 
@@ -373,7 +373,8 @@ int locate_batched_ws (const drb_mesh *mesh, const drb_bvh *bvh, const float *pt
   }
   cudaError_t e = cudaMemsetAsync (ws.head, 0, sizeof (int), s);
   if (e != cudaSuccess) return status_from (e);
-  const int per_sm = resident_blocks (mesh->order, cfg.block);
+  const bool reg = cfg.reg_elements != 0;
+  const int per_sm = resident_blocks (mesh->order, reg, cfg.block);
   const int bps = (cfg.blocks_per_sm > 0) ? min (cfg.blocks_per_sm, per_sm) : per_sm;
   const long long warps_needed = ((long long)n + 31) / 32;
   long long blocks = (long long)bps * sm_count ();
@@ -381,7 +382,7 @@ int locate_batched_ws (const drb_mesh *mesh, const drb_bvh *bvh, const float *pt
   if (blocks > blocks_needed) blocks = blocks_needed;
   if (blocks < 1) blocks = 1;
   const LocateParams lp = make_params (mesh, bvh, opts);
-  return launch_persistent (mesh->order, dim3 ((unsigned)blocks), cfg.block, s, lp, pts, ord, n,
+  return launch_persistent (mesh->order, reg, dim3 ((unsigned)blocks), cfg.block, s, lp, pts, ord, n,
                             cfg.chunk, ws.head, cell, ref, stats);
 }
 
@@ -454,6 +455,7 @@ extern "C" int drb_locate_tune (const drb_mesh *mesh, const drb_bvh *bvh, const 
   cudaEventCreate (&e1);
   float best_t = 1e30f;
   drb_locate_config bc = default_config (mesh->order);
+  for (int rg = 0; rg < (mesh->order <= 2 ? 2 : 1); ++rg)
   for (int b : blocks)
     for (int ps : per_sm)
       for (int c : chunks)
@@ -463,6 +465,7 @@ extern "C" int drb_locate_tune (const drb_mesh *mesh, const drb_bvh *bvh, const 
         cfg.blocks_per_sm = ps;
         cfg.chunk = c;
         cfg.sort_queries = 1;
+        cfg.reg_elements = rg;
         float t = 0.f;
         for (int rep = 0; rep < 2 && st == DRB_OK; ++rep)
         {

@@ -28,8 +28,9 @@ DRB_D int traverse_to_leaf (const float4 *__restrict__ nodes, const float (&pt)[
     if (cur > -1)
     {
       bool in_l, in_r;
+      int l, r;
       ++nodes_visited;
-      node_point_test (nodes, cur, pt, in_l, in_r);
+      node_point_test_kids (nodes, cur, pt, in_l, in_r, l, r);
       if (!in_l && !in_r)
       {
         cur = todo[sp];
@@ -37,9 +38,6 @@ DRB_D int traverse_to_leaf (const float4 *__restrict__ nodes, const float (&pt)[
       }
       else
       {
-        const float4 ch = __ldg (nodes + cur + 3);
-        const int l = __float_as_int (ch.x);
-        const int r = __float_as_int (ch.y);
         cur = in_l ? l : r;
         if (in_l && in_r && sp < kStackDepth - 1) todo[++sp] = r;
       }
@@ -76,7 +74,7 @@ __global__ void first_candidate_kernel (const float4 *__restrict__ nodes, const 
   if (first_elem) first_elem[qi] = leaf >= 0 ? __ldg (leaf_nodes + leaf) : -1;
 }
 
-template <int P>
+template <int P, bool REG>
 __global__ void locate_hinted_kernel (LocateParams lp, const float *__restrict__ pts,
                                       const int *__restrict__ order, const int *__restrict__ hint,
                                       int n, int chunk, int *__restrict__ queue_head,
@@ -162,7 +160,7 @@ __global__ void locate_hinted_kernel (LocateParams lp, const float *__restrict__
       {
         const int el = __ldg (lp.leaf_nodes + leaf);
         ++cands;
-        const bool found = solve_candidate<P> (lp, leaf, el, qi, first, pt, x, iters);
+        const bool found = solve_candidate<P, REG> (lp, leaf, el, qi, first, pt, x, iters);
         first = false;
         if (found)
         {
@@ -243,6 +241,7 @@ extern "C" int drb_locate_hinted (const drb_mesh *mesh, const drb_bvh *bvh, cons
     cfg.blocks_per_sm = 0;
     cfg.chunk = 64;
     cfg.sort_queries = 1;
+    cfg.reg_elements = 0;
   }
   if (cfg.block < 32 || cfg.block > 1024 || (cfg.block % 32) || cfg.chunk < 1)
   {
@@ -268,9 +267,10 @@ extern "C" int drb_locate_hinted (const drb_mesh *mesh, const drb_bvh *bvh, cons
   lp.guess_mode = opts->guess_mode;
   lp.guess = opts->guess;
   int nb = 0;
-  const void *fn = mesh->order == 1 ? (const void *)locate_hinted_kernel<1>
-                                    : (mesh->order == 2 ? (const void *)locate_hinted_kernel<2>
-                                                        : (const void *)locate_hinted_kernel<3>);
+  const bool reg = cfg.reg_elements != 0 && mesh->order <= 2;
+  const void *fn = mesh->order == 1 ? (reg ? (const void *)locate_hinted_kernel<1, true> : (const void *)locate_hinted_kernel<1, false>)
+                   : mesh->order == 2 ? (reg ? (const void *)locate_hinted_kernel<2, true> : (const void *)locate_hinted_kernel<2, false>)
+                                      : (const void *)locate_hinted_kernel<3, false>;
   cudaOccupancyMaxActiveBlocksPerMultiprocessor (&nb, fn, cfg.block, 0);
   if (nb < 1) nb = 1;
   const int bps = cfg.blocks_per_sm > 0 ? min (cfg.blocks_per_sm, nb) : nb;
@@ -278,14 +278,14 @@ extern "C" int drb_locate_hinted (const drb_mesh *mesh, const drb_bvh *bvh, cons
   const long long need = ((long long)n + cfg.block - 1) / cfg.block;
   if (blocks > need) blocks = need;
   if (blocks < 1) blocks = 1;
-#define DRB_HINT(P)                                                                              \
-  locate_hinted_kernel<P><<<(unsigned)blocks, cfg.block, 0, s>>> (lp, pts, order, first_leaf, n, \
-                                                                  cfg.chunk, head, cell, ref,    \
-                                                                  stats.iters, stats.candidates, \
-                                                                  stats.nodes)
-  if (mesh->order == 1) DRB_HINT (1);
-  else if (mesh->order == 2) DRB_HINT (2);
-  else DRB_HINT (3);
+#define DRB_HINT(P, R)                                                                              \
+  locate_hinted_kernel<P, R><<<(unsigned)blocks, cfg.block, 0, s>>> (lp, pts, order, first_leaf, n, \
+                                                                     cfg.chunk, head, cell, ref,    \
+                                                                     stats.iters, stats.candidates, \
+                                                                     stats.nodes)
+  if (mesh->order == 1) { if (reg) DRB_HINT (1, true); else DRB_HINT (1, false); }
+  else if (mesh->order == 2) { if (reg) DRB_HINT (2, true); else DRB_HINT (2, false); }
+  else DRB_HINT (3, false);
 #undef DRB_HINT
   return check_launch ("locate_hinted_kernel");
 }

@@ -155,6 +155,9 @@ typedef struct drb_locate_config
   int blocks_per_sm;     /* resident blocks per SM, 0 = as many as fit */
   int chunk;             /* queries a warp pops from the global queue at once */
   int sort_queries;      /* 1 = process the queries in Morton order */
+  int reg_elements;      /* 1 = keep an order <= 2 candidate's control points in
+                            registers for its whole Newton solve (fewer loads,
+                            more registers); 0 = read them through L1 */
 } drb_locate_config;
 
 /* Batched point location, same results as drb_locate (same traversal order
