@@ -1,0 +1,691 @@
+// Implementation of the C++ host interface (include/dray/dray_b200.hpp)
+// over the C-ABI of include/drb.h.  Every compute step is a libdrb call on
+// the legacy default stream; host synchronisation happens only where the
+// reference's API returns host-visible results.
+#include "dray/dray_b200.hpp"
+
+#include <algorithm>
+#include <cstring>
+
+#include "drb.h"
+
+namespace dray
+{
+
+namespace
+{
+void drb_check (int st, const char *what)
+{
+  if (st != DRB_OK)
+  {
+    std::ostringstream os;
+    os << what << " failed (status " << st << "): " << drb_last_error ();
+    throw DRayError (os.str ());
+  }
+}
+
+template <typename T> struct DevBuf
+{
+  T *p = nullptr;
+  size_t n = 0;
+  void alloc (size_t count)
+  {
+    release ();
+    n = count;
+    if (count) cuda_check (cudaMalloc ((void **)&p, sizeof (T) * count), "cudaMalloc");
+  }
+  void release ()
+  {
+    if (p) cudaFree (p);
+    p = nullptr;
+    n = 0;
+  }
+  ~DevBuf () { release (); }
+};
+
+int32 nd_of (int32 dim, int32 order)
+{
+  int32 nd = 1;
+  for (int d = 0; d < dim; ++d) nd *= order + 1;
+  return nd;
+}
+} // namespace
+
+// Device copies, packed element rows and (for meshes) the lazily built BVH.
+struct DeviceGeometry
+{
+  drb_mesh mesh{};
+  DevBuf<float> packed;
+  bool has_bvh = false;
+  drb_bvh bvh{};
+  DevBuf<float> inner, refb;
+  DevBuf<int32> leaf, ids;
+};
+
+// ------------------------------------------------------------ meshes --
+
+TensorMesh::TensorMesh (const GridFunction<3> &dof, int32 order, int32 dim)
+: m_dof_data (dof), m_poly_order (order), m_dim (dim), m_dev (std::make_shared<DeviceGeometry> ())
+{
+  if (order < 1 || order > 3) DRAY_ERROR ("polynomial order " << order << " is outside 1..3");
+  if (dof.m_el_dofs != nd_of (dim, order))
+    DRAY_ERROR ("GridFunction has " << dof.m_el_dofs << " dofs per element, order " << order
+                                    << " needs " << nd_of (dim, order));
+}
+
+TensorMesh::~TensorMesh () {}
+
+const drb_mesh *TensorMesh::device_mesh ()
+{
+  DeviceGeometry &g = *m_dev;
+  if (!g.mesh.ctrl_idx || g.mesh.n_elem != cells ())
+  {
+    g.mesh.dim = m_dim;
+    g.mesh.order = m_poly_order;
+    g.mesh.ncomp = 3;
+    g.mesh.n_elem = cells ();
+    g.mesh.n_ctrl = (int)m_dof_data.m_values.size ();
+    g.mesh.ctrl_idx = m_dof_data.m_ctrl_idx.get_device_ptr_const ();
+    g.mesh.values = (const float *)m_dof_data.m_values.get_device_ptr_const ();
+    const int stride = drb_packed_stride (m_dim, m_poly_order, 3);
+    g.packed.alloc ((size_t)std::max (cells (), 1) * stride);
+    g.mesh.packed = nullptr;
+    drb_check (drb_pack_elements (&g.mesh, g.packed.p, nullptr), "drb_pack_elements");
+    g.mesh.packed = g.packed.p;
+  }
+  return &g.mesh;
+}
+
+const drb_bvh *TensorMesh::device_bvh ()
+{
+  DeviceGeometry &g = *m_dev;
+  device_mesh ();
+  if (!g.has_bvh)
+  {
+    int ni = 0, nl = 0;
+    drb_check (drb_bvh_sizes (m_dim, cells (), &ni, &nl), "drb_bvh_sizes");
+    g.inner.alloc ((size_t)16 * ni);
+    g.leaf.alloc (nl);
+    g.ids.alloc (nl);
+    g.refb.alloc ((size_t)2 * m_dim * nl);
+    g.bvh.n_inner = ni;
+    g.bvh.n_leaf = nl;
+    g.bvh.inner_nodes = g.inner.p;
+    g.bvh.leaf_nodes = g.leaf.p;
+    g.bvh.aabb_ids = g.ids.p;
+    g.bvh.ref_boxes = g.refb.p;
+    drb_check (drb_lbvh_build (&g.mesh, &g.bvh, nullptr, nullptr), "drb_lbvh_build");
+    g.has_bvh = true;
+  }
+  return &g.bvh;
+}
+
+AABB<3> TensorMesh::bounds ()
+{
+  const drb_bvh *b = device_bvh ();
+  AABB<3> r;
+  for (int d = 0; d < 3; ++d)
+  {
+    if (b->bounds[2 * d] <= b->bounds[2 * d + 1])
+    {
+      r.m_ranges[d].include (b->bounds[2 * d]);
+      r.m_ranges[d].include (b->bounds[2 * d + 1]);
+    }
+  }
+  return r;
+}
+
+Array<Location> TensorMesh::locate (Array<Vec<Float, 3>> &wpoints)
+{
+  if (m_dim != 3) DRAY_ERROR ("locate needs a volume (hex) mesh");
+  const int n = (int)wpoints.size ();
+  Array<Location> out;
+  out.resize (n);
+  if (n == 0) return out;
+  const drb_bvh *b = device_bvh ();
+  DevBuf<int32> cell;
+  DevBuf<float> ref;
+  cell.alloc (n);
+  ref.alloc ((size_t)3 * n);
+  drb_newton_opts opts{ m_locate.tol, m_locate.max_steps, m_locate.guess_mode, nullptr };
+  drb_check (drb_locate_batched (device_mesh (), b, (const float *)wpoints.get_device_ptr_const (), n,
+                                 &opts, nullptr, cell.p, ref.p, drb_query_stats{}, nullptr),
+             "drb_locate_batched");
+  std::vector<int32> hc (n);
+  std::vector<float> hr ((size_t)3 * n);
+  cuda_check (cudaMemcpy (hc.data (), cell.p, sizeof (int32) * n, cudaMemcpyDeviceToHost), "copy");
+  cuda_check (cudaMemcpy (hr.data (), ref.p, sizeof (float) * 3 * n, cudaMemcpyDeviceToHost), "copy");
+  Location *lp = out.get_host_ptr ();
+  for (int i = 0; i < n; ++i)
+  {
+    lp[i].m_cell_id = hc[i];
+    for (int k = 0; k < 3; ++k) lp[i].m_ref_pt[k] = hr[3 * (size_t)i + k];
+  }
+  return out;
+}
+
+// ------------------------------------------------------------ fields --
+
+TensorField::TensorField (const GridFunction<1> &dof, int32 order, int32 dim, const std::string &name)
+: m_dof_data (dof), m_poly_order (order), m_dim (dim), m_dev (std::make_shared<DeviceGeometry> ())
+{
+  m_name = name;
+  if (order < 1 || order > 3) DRAY_ERROR ("polynomial order " << order << " is outside 1..3");
+}
+
+TensorField::~TensorField () {}
+
+const drb_mesh *TensorField::device_field ()
+{
+  DeviceGeometry &g = *m_dev;
+  if (!g.mesh.ctrl_idx)
+  {
+    g.mesh.dim = m_dim;
+    g.mesh.order = m_poly_order;
+    g.mesh.ncomp = 1;
+    g.mesh.n_elem = m_dof_data.get_num_elem ();
+    g.mesh.n_ctrl = (int)m_dof_data.m_values.size ();
+    g.mesh.ctrl_idx = m_dof_data.m_ctrl_idx.get_device_ptr_const ();
+    g.mesh.values = (const float *)m_dof_data.m_values.get_device_ptr_const ();
+    const int stride = drb_packed_stride (m_dim, m_poly_order, 1);
+    g.packed.alloc ((size_t)std::max (g.mesh.n_elem, 1) * stride);
+    drb_check (drb_pack_elements (&g.mesh, g.packed.p, nullptr), "drb_pack_elements");
+    g.mesh.packed = g.packed.p;
+  }
+  return &g.mesh;
+}
+
+std::vector<Range> TensorField::range () const
+{
+  if (m_range.empty ())
+  {
+    float r[2];
+    DevBuf<float> d;
+    d.alloc (2);
+    drb_check (drb_field_range (const_cast<TensorField *> (this)->device_field (), d.p, nullptr),
+               "drb_field_range");
+    cuda_check (cudaMemcpy (r, d.p, sizeof (r), cudaMemcpyDeviceToHost), "copy");
+    Range rr;
+    if (r[0] <= r[1])
+    {
+      rr.include (r[0]);
+      rr.include (r[1]);
+    }
+    m_range.push_back (rr);
+  }
+  return m_range;
+}
+
+void TensorField::eval (const Array<Location> locs, Array<Float> &values)
+{
+  if (m_dim != 3) DRAY_ERROR ("field eval at locations needs a hex field");
+  const int n = (int)locs.size ();
+  values.resize (n);
+  if (n == 0) return;
+  // split Location records into cell ids and reference points on the device
+  std::vector<int32> cell (n);
+  std::vector<float> ref ((size_t)3 * n);
+  const Location *lp = locs.get_host_ptr_const ();
+  for (int i = 0; i < n; ++i)
+  {
+    cell[i] = lp[i].m_cell_id;
+    for (int k = 0; k < 3; ++k) ref[3 * (size_t)i + k] = lp[i].m_ref_pt[k];
+  }
+  Array<int32> dcell (cell.data (), n);
+  Array<float> dref (ref.data (), (size_t)3 * n);
+  drb_check (drb_field_eval (device_field (), dcell.get_device_ptr_const (),
+                             dref.get_device_ptr_const (), n, 0.f, values.get_device_ptr (), nullptr),
+             "drb_field_eval");
+}
+
+// --------------------------------------------------------- collection --
+
+bool DataSet::has_field (const std::string &n) const
+{
+  for (auto &f : m_fields)
+    if (f->name () == n) return true;
+  return false;
+}
+
+Field *DataSet::field (const std::string &n) { return field_shared (n).get (); }
+
+std::shared_ptr<Field> DataSet::field_shared (const std::string &n)
+{
+  for (auto &f : m_fields)
+    if (f->name () == n) return f;
+  DRAY_ERROR ("No field named '" << n << "'");
+}
+
+AABB<3> Collection::bounds ()
+{
+  AABB<3> r;
+  for (auto &d : m_domains)
+  {
+    AABB<3> b = d.mesh ()->bounds ();
+    for (int k = 0; k < 3; ++k)
+      if (!b.m_ranges[k].is_empty ())
+      {
+        r.m_ranges[k].include (b.m_ranges[k].min ());
+        r.m_ranges[k].include (b.m_ranges[k].max ());
+      }
+  }
+  return r;
+}
+
+Range Collection::range (const std::string &field_name)
+{
+  Range r;
+  for (auto &d : m_domains)
+    if (d.has_field (field_name))
+    {
+      Range fr = d.field (field_name)->range ()[0];
+      if (!fr.is_empty ())
+      {
+        r.include (fr.min ());
+        r.include (fr.max ());
+      }
+    }
+  return r;
+}
+
+// ------------------------------------------------------------ colours --
+
+std::vector<float32> ColorTable::sample (int32 n, float32 alpha_scale, float32 opacity_factor) const
+{
+  std::vector<float32> out ((size_t)4 * n);
+  std::vector<float32> rgb, al;
+  for (auto &v : m_rgb)
+    for (int k = 0; k < 4; ++k) rgb.push_back (v[k]);
+  for (auto &v : m_alpha)
+    for (int k = 0; k < 2; ++k) al.push_back (v[k]);
+  drb_check (drb_color_table_sample ((int)m_rgb.size (), rgb.empty () ? nullptr : rgb.data (),
+                                     (int)m_alpha.size (), al.empty () ? nullptr : al.data (),
+                                     m_smooth ? 1 : 0, n, alpha_scale, opacity_factor, out.data ()),
+             "drb_color_table_sample");
+  return out;
+}
+
+// ------------------------------------------------------------- camera --
+
+void Camera::set_width (const int32 &w)
+{
+  if (w <= 0) DRAY_ERROR ("Camera width must be greater than zero.");
+  m_width = w;
+}
+void Camera::set_height (const int32 &h)
+{
+  if (h <= 0) DRAY_ERROR ("Camera height must be greater than zero.");
+  m_height = h;
+}
+void Camera::set_fov (const float32 &d)
+{
+  if (d <= 0) DRAY_ERROR ("Camera feild of view must be greater than zero.");
+  if (d > 180) DRAY_ERROR ("Camera feild of view must be less than 180.");
+  m_fov_y = d;
+}
+void Camera::set_zoom (const float32 z)
+{
+  if (z <= 0) DRAY_ERROR ("Zoom must be greater than 0");
+  m_zoom = z;
+}
+
+static drb_camera to_drb (const Camera &c)
+{
+  drb_camera d{};
+  d.width = c.get_width ();
+  d.height = c.get_height ();
+  for (int k = 0; k < 3; ++k)
+  {
+    d.pos[k] = c.get_pos ()[k];
+    d.look_at[k] = c.get_look_at ()[k];
+    d.up[k] = c.get_up ()[k];
+  }
+  d.fov_y = c.get_fov ();
+  d.zoom = 1.f;
+  return d;
+}
+
+void Camera::create_rays (Array<Ray> &rays)
+{
+  rays.resize ((size_t)m_width * m_height);
+  drb_camera d = to_drb (*this);
+  d.zoom = m_zoom;
+  drb_check (drb_camera_rays (&d, rays.get_device_ptr (), nullptr), "drb_camera_rays");
+}
+
+PointLight default_light (Camera &camera)
+{
+  drb_camera d = to_drb (camera);
+  float l[13];
+  drb_check (drb_default_light (&d, l), "drb_default_light");
+  PointLight p;
+  for (int k = 0; k < 3; ++k)
+  {
+    p.m_pos[k] = l[k];
+    p.m_amb[k] = l[3 + k];
+    p.m_diff[k] = l[6 + k];
+    p.m_spec[k] = l[9 + k];
+  }
+  p.m_spec_pow = l[12];
+  return p;
+}
+
+// -------------------------------------------------------- framebuffer --
+
+Framebuffer::Framebuffer (int32 w, int32 h) : m_width (w), m_height (h)
+{
+  m_colors.resize ((size_t)w * h);
+  m_depths.resize ((size_t)w * h);
+  clear ();
+}
+
+void Framebuffer::clear () { clear (make_vec4f (0.f, 0.f, 0.f, 0.f)); }
+
+void Framebuffer::clear (const Vec4f &c)
+{
+  float col[4] = { c[0], c[1], c[2], c[3] };
+  drb_check (drb_framebuffer_clear ((float *)m_colors.get_device_ptr (), m_depths.get_device_ptr (),
+                                    m_width * m_height, col, nullptr),
+             "drb_framebuffer_clear");
+}
+
+void Framebuffer::composite_background ()
+{
+  float bg[4] = { m_bg_color[0], m_bg_color[1], m_bg_color[2], m_bg_color[3] };
+  drb_check (drb_framebuffer_composite_background ((float *)m_colors.get_device_ptr (),
+                                                   m_width * m_height, bg, nullptr),
+             "drb_framebuffer_composite_background");
+}
+
+// ------------------------------------------------------------- volume --
+
+Volume::Volume (Collection &c) : m_collection (c)
+{
+  // Volume() adds two alpha points to its default table (volume.cpp:274-282)
+  ColorTable t = m_color_map.color_table ();
+  t.add_alpha (0.1f, 0.f);
+  t.add_alpha (1.0f, 0.7f);
+  m_color_map.color_table (t);
+}
+
+static TensorMesh *as_tensor_mesh (Mesh *m)
+{
+  TensorMesh *t = dynamic_cast<TensorMesh *> (m);
+  if (!t) DRAY_ERROR ("mesh type is not a tensor mesh of this path");
+  return t;
+}
+static TensorField *as_tensor_field (Field *f)
+{
+  TensorField *t = dynamic_cast<TensorField *> (f);
+  if (!t) DRAY_ERROR ("field type is not a scalar tensor field of this path");
+  return t;
+}
+
+Array<VolumePartial> Volume::integrate (Array<Ray> &rays, Array<PointLight> &lights)
+{
+  if (m_field == "") DRAY_ERROR ("Field never set");
+  DataSet ds = m_collection.domain (0);
+  TensorMesh *mesh = as_tensor_mesh (ds.mesh ());
+  TensorField *field = as_tensor_field (ds.field (m_field));
+  Range r = m_color_map.range_set () ? m_color_map.scalar_range () : m_collection.range (m_field);
+  const AABB<3> bounds = m_collection.bounds ();
+  const drb_bvh *bvh = mesh->device_bvh ();
+  // remove_missed_rays against the mesh bounds
+  const int n = (int)rays.size ();
+  Array<Ray> active;
+  active.resize (n);
+  int n_active = 0;
+  drb_check (drb_cull_rays (rays.get_device_ptr_const (), n, bvh->bounds, active.get_device_ptr (),
+                            &n_active, nullptr),
+             "drb_cull_rays");
+  // opacity-corrected table sampled at the default 1024 entries (volume.cpp:81-87)
+  std::vector<float32> tf = m_color_map.color_table ().sample (1024, 1.f, 10.f / m_samples);
+  Array<Vec4f> tfa ((const Vec4f *)tf.data (), 1024);
+  drb_volume_opts o{};
+  o.samples = m_samples;
+  o.use_lighting = m_use_lighting ? 1 : 0;
+  o.tol = m_locate.tol;
+  o.max_steps = m_locate.max_steps;
+  o.guess_mode = m_locate.guess_mode;
+  o.coherent = m_coherent ? 1 : 0;
+  for (int d = 0; d < 3; ++d)
+  {
+    o.bounds[2 * d] = bounds.m_ranges[d].min ();
+    o.bounds[2 * d + 1] = bounds.m_ranges[d].max ();
+  }
+  o.cull = 0;
+  float range2[2] = { r.min (), r.max () };
+  Array<VolumePartial> out;
+  out.resize ((size_t)5 * std::max (n_active, 1));
+  int np = 0;
+  drb_check (drb_volume_integrate (mesh->device_mesh (), field->device_field (), bvh,
+                                   active.get_device_ptr_const (), n_active, &o,
+                                   (const float *)tfa.get_device_ptr_const (), 1024, range2,
+                                   lights.get_device_ptr_const (), (int)lights.size (),
+                                   out.get_device_ptr (), &np, drb_ray_stats{}, nullptr),
+             "drb_volume_integrate");
+  Array<VolumePartial> res;
+  res.resize (np);
+  if (np)
+    cuda_check (cudaMemcpy (res.get_device_ptr (), out.get_device_ptr_const (),
+                            sizeof (VolumePartial) * np, cudaMemcpyDeviceToDevice),
+                "copy");
+  return res;
+}
+
+Framebuffer Volume::composite (Array<VolumePartial> partials, int32 w, int32 h)
+{
+  Framebuffer fb (w, h);
+  Array<Vec<float32, 4>> c = fb.colors ();
+  drb_check (drb_composite_partials (partials.get_device_ptr_const (), (int)partials.size (),
+                                     (float *)c.get_device_ptr (), nullptr),
+             "drb_composite_partials");
+  fb.composite_background ();
+  return fb;
+}
+
+// ------------------------------------------------------------ surfaces --
+
+Array<RayHit> Surface::nearest_hit (Array<Ray> &rays)
+{
+  DataSet ds = m_collection.domain (0);
+  TensorMesh *faces = as_tensor_mesh (ds.mesh ());
+  if (faces->dims () != 2) DRAY_ERROR ("Surface needs a quad (boundary) mesh");
+  Array<RayHit> hits;
+  hits.resize (rays.size ());
+  // face_intersection.hpp:153-154: tol 1e-4, 10 steps
+  drb_check (drb_surface_intersect (faces->device_mesh (), faces->device_bvh (),
+                                    rays.get_device_ptr_const (), (int)rays.size (), 1e-4f, 10,
+                                    hits.get_device_ptr (), drb_ray_stats{}, nullptr),
+             "drb_surface_intersect");
+  return hits;
+}
+
+void Traceable::shade_impl (const Array<Ray> *rays, const Array<RayHit> &hits,
+                            const Array<PointLight> *lights, Framebuffer *fb, Array<Fragment> *frags)
+{
+  DataSet ds = m_collection.domain (0);
+  TensorMesh *faces = as_tensor_mesh (ds.mesh ());
+  TensorField *field = as_tensor_field (ds.field (m_field_name));
+  Range r = m_color_map.range_set () ? m_color_map.scalar_range () : m_collection.range (m_field_name);
+  std::vector<float32> tf = m_color_map.color_table ().sample (m_color_map.samples ());
+  Array<Vec4f> tfa ((const Vec4f *)tf.data (), m_color_map.samples ());
+  float range2[2] = { r.min (), r.max () };
+  Array<Fragment> local;
+  Array<Fragment> &fr = frags ? *frags : local;
+  fr.resize (hits.size ());
+  Array<Vec<float32, 4>> colors;
+  Array<float32> depths;
+  if (fb)
+  {
+    colors = fb->colors ();
+    depths = fb->depths ();
+  }
+  drb_check (drb_surface_shade (faces->device_mesh (), field->device_field (),
+                                rays ? rays->get_device_ptr_const () : nullptr,
+                                hits.get_device_ptr_const (), (int)hits.size (),
+                                (const float *)tfa.get_device_ptr_const (), m_color_map.samples (),
+                                range2, lights ? lights->get_device_ptr_const () : nullptr,
+                                lights ? (int)lights->size () : 0, lights ? 1 : 0,
+                                (float *)fr.get_device_ptr (),
+                                fb ? (float *)colors.get_device_ptr () : nullptr,
+                                fb ? depths.get_device_ptr () : nullptr, nullptr),
+             "drb_surface_shade");
+}
+
+Array<Fragment> Traceable::fragments (Array<RayHit> &hits)
+{
+  // get_fragments (traceable.cpp:49-147): field value and surface normal
+  Array<Fragment> frags;
+  shade_impl (nullptr, hits, nullptr, nullptr, &frags);
+  return frags;
+}
+
+void Traceable::shade (const Array<Ray> &rays, const Array<RayHit> &hits, const Array<Fragment> &,
+                       const Array<PointLight> &lights, Framebuffer &fb)
+{
+  shade_impl (&rays, hits, &lights, &fb, nullptr);
+}
+
+void Traceable::shade (const Array<Ray> &rays, const Array<RayHit> &hits, const Array<Fragment> &,
+                       Framebuffer &fb)
+{
+  shade_impl (&rays, hits, nullptr, &fb, nullptr);
+}
+
+// ------------------------------------------------------------ filters --
+
+Collection MeshBoundary::execute (Collection &collection)
+{
+  Collection res;
+  for (int32 i = 0; i < collection.local_size (); ++i)
+  {
+    DataSet ds = collection.domain (i);
+    TensorMesh *hex = dynamic_cast<TensorMesh *> (ds.mesh ());
+    if (!hex || hex->dims () != 3)
+    {
+      res.add_domain (ds);
+      continue;
+    }
+    const drb_mesh *dm = hex->device_mesh ();
+    int nf = 0;
+    drb_check (drb_mesh_boundary (dm, nullptr, nullptr, nullptr, nullptr, &nf, nullptr),
+               "drb_mesh_boundary");
+    const int p = hex->order ();
+    const int fd = (p + 1) * (p + 1);
+    GridFunction<3> fg;
+    GridFunction<3> vol = hex->get_dof_data ();
+    fg.m_values = vol.m_values; // the quads index the volume's value array
+    fg.m_el_dofs = fd;
+    fg.m_size_el = nf;
+    fg.m_size_ctrl = vol.m_size_ctrl;
+    fg.m_ctrl_idx.resize ((size_t)nf * fd);
+    std::vector<std::shared_ptr<Field>> fields;
+    std::vector<GridFunction<1>> fgs;
+    // one pass per scalar field (the dof mapping is identical for all)
+    DataSet out;
+    int32 *fi = fg.m_ctrl_idx.get_device_ptr ();
+    drb_check (drb_mesh_boundary (dm, nullptr, fi, nullptr, nullptr, &nf, nullptr), "drb_mesh_boundary");
+    std::shared_ptr<Mesh> qm;
+    if (p == 1) qm = std::make_shared<QuadMesh_P1> (fg, 1);
+    else if (p == 2) qm = std::make_shared<QuadMesh_P2> (fg, 2);
+    else qm = std::make_shared<QuadMesh> (fg, p);
+    out.add_mesh (qm);
+    for (int32 k = 0; k < ds.number_of_fields (); ++k)
+    {
+      TensorField *f = dynamic_cast<TensorField *> (ds.field (k));
+      if (!f || f->order () != p) continue;
+      GridFunction<1> vf = f->get_dof_data ();
+      GridFunction<1> ff;
+      ff.m_values = vf.m_values;
+      ff.m_el_dofs = fd;
+      ff.m_size_el = nf;
+      ff.m_size_ctrl = vf.m_size_ctrl;
+      ff.m_ctrl_idx.resize ((size_t)nf * fd);
+      drb_check (drb_mesh_boundary (dm, vf.m_ctrl_idx.get_device_ptr_const (),
+                                    fg.m_ctrl_idx.get_device_ptr (), ff.m_ctrl_idx.get_device_ptr (),
+                                    nullptr, &nf, nullptr),
+                 "drb_mesh_boundary");
+      std::shared_ptr<Field> qf;
+      if (p == 1) qf = std::make_shared<UnstructuredField<QuadScalar_P1>> (ff, 1, f->name ());
+      else if (p == 2) qf = std::make_shared<UnstructuredField<QuadScalar_P2>> (ff, 2, f->name ());
+      else qf = std::make_shared<UnstructuredField<QuadScalar>> (ff, p, f->name ());
+      out.add_field (qf);
+    }
+    res.add_domain (out);
+  }
+  return res;
+}
+
+PointLocation::Result PointLocation::execute (Collection &collection, Array<Vec<Float, 3>> &points)
+{
+  // queries/point_location.cpp:178-287, single domain per rank
+  Result r;
+  r.m_points = points;
+  r.m_vars = m_vars;
+  r.m_empty_val = m_empty_val;
+  const int n = (int)points.size ();
+  for (size_t v = 0; v < m_vars.size (); ++v)
+  {
+    Array<Float> a;
+    a.resize (n);
+    Float *ap = a.get_host_ptr ();
+    for (int i = 0; i < n; ++i) ap[i] = m_empty_val;
+    r.m_values.push_back (a);
+  }
+  for (int32 d = 0; d < collection.local_size (); ++d)
+  {
+    DataSet ds = collection.domain (d);
+    Array<Location> locs = ds.mesh ()->locate (points);
+    const Location *lp = locs.get_host_ptr_const ();
+    for (size_t v = 0; v < m_vars.size (); ++v)
+    {
+      if (!ds.has_field (m_vars[v])) continue;
+      Array<Float> vals;
+      ds.field (m_vars[v])->eval (locs, vals);
+      const Float *vp = vals.get_host_ptr_const ();
+      Float *out = r.m_values[v].get_host_ptr ();
+      for (int i = 0; i < n; ++i)
+        if (lp[i].m_cell_id != -1) out[i] = vp[i];
+    }
+  }
+  return r;
+}
+
+// ------------------------------------------------------------ renderer --
+
+Framebuffer Renderer::render (Camera &camera)
+{
+  // Renderer::render (rendering/renderer.cpp:229-363), single domain:
+  // surfaces shade and shorten the rays, then the volume composites in
+  // front of them (partials_to_framebuffer with blending)
+  Array<Ray> rays;
+  camera.create_rays (rays);
+  Framebuffer fb (camera.get_width (), camera.get_height ());
+  std::vector<PointLight> lv = m_lights;
+  if (lv.empty ()) lv.push_back (default_light (camera));
+  Array<PointLight> lights (lv.data (), lv.size ());
+  for (auto &t : m_traceables)
+  {
+    Array<RayHit> hits = t->nearest_hit (rays);
+    Array<Fragment> frags;
+    if (m_use_lighting) t->shade (rays, hits, frags, lights, fb);
+    else t->shade (rays, hits, frags, fb);
+    drb_check (drb_ray_max (rays.get_device_ptr (), hits.get_device_ptr_const (), (int)rays.size (),
+                            nullptr),
+               "drb_ray_max");
+  }
+  if (m_volume)
+  {
+    Array<VolumePartial> parts = m_volume->integrate (rays, lights);
+    Array<Vec<float32, 4>> c = fb.colors ();
+    Array<float32> d = fb.depths ();
+    drb_check (drb_partials_to_framebuffer (parts.get_device_ptr_const (), (int)parts.size (),
+                                            (float *)c.get_device_ptr (), d.get_device_ptr (),
+                                            m_traceables.empty () ? 0 : 1, nullptr),
+               "drb_partials_to_framebuffer");
+  }
+  return fb;
+}
+
+} // namespace dray

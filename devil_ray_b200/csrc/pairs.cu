@@ -75,6 +75,31 @@ __global__ void newton_pairs_kernel (const float *__restrict__ packed, int strid
   if (iters) iters[i] = steps;
 }
 
+// UnstructuredField::eval at located points (unstructured_field.cpp:214-245):
+// value of the scalar field at (cell, ref); cell -1 -> empty value.
+template <int P>
+__global__ void field_eval_kernel (const float *__restrict__ packed, int stride,
+                                   const int *__restrict__ cell, const float *__restrict__ ref,
+                                   int n, float empty, float *__restrict__ out)
+{
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const int e = cell[i];
+  float v = empty;
+  if (e >= 0)
+  {
+    struct F
+    {
+      const float *p;
+      DRB_D float operator() (int q, int) const { return __ldg (p + q); }
+    } cp{ packed + (size_t)e * stride };
+    float X[1];
+    hex_eval<P, 1> (cp, ref[3 * (size_t)i], ref[3 * (size_t)i + 1], ref[3 * (size_t)i + 2], X);
+    v = X[0];
+  }
+  out[i] = v;
+}
+
 int check_pairs (const drb_mesh *m, int n)
 {
   if (!m || !m->packed || m->dim != 3 || m->ncomp != 3 || m->order < 1 || m->order > 3 || n < 0)
@@ -134,4 +159,24 @@ extern "C" int drb_newton_pairs (const drb_mesh *mesh, const int *elem, const fl
   else
     newton_pairs_kernel<3><<<b, 128, 0, s>>> (mesh->packed, stride, elem, pts, n, tol, max_steps, guess, ref, found, iters);
   return check_launch ("newton_pairs_kernel");
+}
+
+extern "C" int drb_field_eval (const drb_mesh *field, const int *cell, const float *ref, int n,
+                               float empty_value, float *values, void *stream)
+{
+  if (!field || !field->packed || field->dim != 3 || field->ncomp != 1 || field->order < 1 ||
+      field->order > 3 || n < 0 || (n > 0 && (!cell || !ref || !values)))
+  {
+    set_last_error ("field_eval: needs a packed scalar hex field of order 1..3");
+    return DRB_ERR_INVALID_ARG;
+  }
+  if (n == 0) return DRB_OK;
+  const int nd = (field->order + 1) * (field->order + 1) * (field->order + 1);
+  const int stride = packed_stride (nd, 1);
+  cudaStream_t s = (cudaStream_t)stream;
+  const int b = div_up (n, 256);
+  if (field->order == 1) field_eval_kernel<1><<<b, 256, 0, s>>> (field->packed, stride, cell, ref, n, empty_value, values);
+  else if (field->order == 2) field_eval_kernel<2><<<b, 256, 0, s>>> (field->packed, stride, cell, ref, n, empty_value, values);
+  else field_eval_kernel<3><<<b, 256, 0, s>>> (field->packed, stride, cell, ref, n, empty_value, values);
+  return check_launch ("field_eval_kernel");
 }

@@ -592,6 +592,35 @@ __global__ void composite_partials_kernel (const VolumePartial *p, int n, float4
   fb[pix] = c;
 }
 
+// partials_to_framebuffer (rendering/renderer.cpp:98-139) after the
+// per-pixel composite of partials sorted by pixel then depth; with blend the
+// volume is composited in front of what the framebuffer holds (surfaces).
+__global__ void partials_to_fb_kernel (const VolumePartial *p, int n, float4 *fb, float *depth,
+                                       int blend_over)
+{
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const int pix = p[i].pixel_id;
+  if (i > 0 && p[i - 1].pixel_id == pix) return;
+  float4 c = make_float4 (p[i].color[0], p[i].color[1], p[i].color[2], p[i].color[3]);
+  for (int k = i + 1; k < n && p[k].pixel_id == pix; ++k)
+  {
+    const float a = 1.f - c.w;
+    c.x = c.x + p[k].color[0] * a;
+    c.y = c.y + p[k].color[1] * a;
+    c.z = c.z + p[k].color[2] * a;
+    c.w = c.w + p[k].color[3] * a;
+  }
+  if (blend_over)
+  {
+    const float4 f = fb[pix];
+    const float op = 1.f - c.w;
+    c = make_float4 (c.x + op * f.x, c.y + op * f.y, c.z + op * f.z, c.w + op * f.w);
+  }
+  fb[pix] = c;
+  if (depth) depth[pix] = p[i].depth;
+}
+
 __global__ void fb_clear_kernel (float4 *c, float *d, int n, float4 v)
 {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
@@ -1020,4 +1049,18 @@ extern "C" int drb_framebuffer_composite_background (float *rgba, int n_pixels,
   const float4 c = bg4 ? make_float4 (bg4[0], bg4[1], bg4[2], bg4[3]) : make_float4 (1.f, 1.f, 1.f, 1.f);
   fb_background_kernel<<<div_up (n_pixels, 256), 256, 0, (cudaStream_t)stream>>> ((float4 *)rgba, n_pixels, c);
   return check_launch ("fb_background_kernel");
+}
+
+extern "C" int drb_partials_to_framebuffer (const void *partials, int n, float *fb_rgba,
+                                            float *fb_depth, int blend_over, void *stream)
+{
+  if (n < 0 || (n > 0 && (!partials || !fb_rgba)))
+  {
+    set_last_error ("partials_to_framebuffer: bad arguments");
+    return DRB_ERR_INVALID_ARG;
+  }
+  if (n == 0) return DRB_OK;
+  partials_to_fb_kernel<<<div_up (n, 256), 256, 0, (cudaStream_t)stream>>> (
+  (const VolumePartial *)partials, n, (float4 *)fb_rgba, fb_depth, blend_over);
+  return check_launch ("partials_to_fb_kernel");
 }

@@ -522,7 +522,7 @@ extern "C" int drb_surface_shade (const drb_mesh *faces, const drb_mesh *face_fi
                                   int n_lights, int use_lighting, float *fragments,
                                   float *fb_rgba, float *fb_depth, void *stream)
 {
-  if (!faces || !face_field || n < 0 || (n > 0 && (!rays || !hits)) || !tf || tf_size < 1 ||
+  if (!faces || !face_field || n < 0 || (n > 0 && (!hits || (fb_rgba && !rays))) || !tf || tf_size < 1 ||
       !range2 || n_lights < 0 || (n_lights > 0 && !lights))
   {
     set_last_error ("surface_shade: bad arguments");

@@ -298,6 +298,12 @@ int drb_volume_render (const drb_mesh *mesh, const drb_mesh *field, const drb_bv
 /* Volume::save compositing of partials sorted by pixel then depth. */
 int drb_composite_partials (const void *partials, int n, float *fb_rgba, void *stream);
 
+/* Renderer's partials_to_framebuffer (rendering/renderer.cpp:98-139) after
+ * compositing each pixel's partials (sorted by pixel then depth); blend_over
+ * puts the volume in front of the framebuffer's current (surface) colour. */
+int drb_partials_to_framebuffer (const void *partials, int n, float *fb_rgba, float *fb_depth,
+                                 int blend_over, void *stream);
+
 /* Framebuffer::clear / composite_background (rendering/framebuffer.cpp:126-162).
  * color4/bg4 are host float[4]; NULL = (0,0,0,0) / white. */
 int drb_framebuffer_clear (float *rgba, float *depth, int n_pixels, const float *color4,
@@ -326,7 +332,8 @@ int drb_surface_intersect (const drb_mesh *faces, const drb_bvh *bvh, const void
 /* Traceable::fragments + Traceable::shade (rendering/traceable.cpp:49-147,
  * 242-387) for quad faces, fused: fragments (optional device float[4n]:
  * scalar, normal) and, for hits, the shaded colour and depth into the
- * framebuffer (device float4/float [w*h], indexed by the ray's pixel id). */
+ * framebuffer (device float4/float [w*h], indexed by the ray's pixel id).
+ * With fb_rgba NULL only the fragments are computed and rays may be NULL. */
 int drb_surface_shade (const drb_mesh *faces, const drb_mesh *face_field, const void *rays,
                        const void *hits, int n, const float *tf, int tf_size,
                        const float *range2, const void *lights, int n_lights, int use_lighting,
@@ -364,6 +371,11 @@ int drb_mlp_adam (float *params, const float *grad, float *m, float *v, float lr
 int drb_mlp_guess (const float *params, const void *wbf16, const drb_mesh *mesh,
                    const int *elem, const float *pts, int n, float *guess, int *err,
                    void *stream);
+
+/* UnstructuredField::eval at located points (data_model/unstructured_field.cpp:
+ * 214-245): values[i] = f(cell[i], ref[i]), empty_value where cell is -1. */
+int drb_field_eval (const drb_mesh *field, const int *cell, const float *ref, int n,
+                    float empty_value, float *values, void *stream);
 
 /* Physical points X_e(r) (Element::eval, pos_tensor_element.tcc:99-232). */
 int drb_map_points (const drb_mesh *mesh, const int *elem, const float *ref, int n, float *pts,
