@@ -213,6 +213,22 @@ def orbit_cameras(count, width, seed=5):
     return cams
 
 
+# FP32 pipe peak of a B200: 148 SMs x 128 FP32 lanes x 2 FLOP (FMA) x 1.965 GHz
+FP32_PEAK_TFLOPS = 148 * 128 * 2 * 1.965e9 / 1e12
+
+
+def newton_step_flops(p):
+    """FLOPs of one Newton step of the sum-factorised kernels (add, mul and
+    compare count 1, FMA 2): three 1-D Bernstein bases with derivatives,
+    eval_d of 3 components (2 FMA per control point and component in the
+    u-sums, 3 per (v, w) pair, 4 per w), the residual, the 3x3 LUP solve and
+    the clamp/update/convergence test."""
+    n = p + 1
+    basis = 3 * (4 + 5 * p)
+    eval_d = 2 * (2 * 3 * n ** 3 + 3 * 3 * n ** 2 + 4 * 3 * n)
+    return basis + eval_d + 3 + 40 + 18
+
+
 def volume_bench(dev, args, timed):
     """128^3 order-3 volume (SURVEY config 4): 2048^2 rays, 1000 samples,
     1024-entry transfer function, `orbits` seeded cameras replayed from one
@@ -477,12 +493,16 @@ def main():
     located = int((cell >= 0).sum().item())
     value = world * located / (ms_step * 1e-3)
 
-    # algorithmic bytes per query: point 12 B + Location 16 B +
-    # per candidate one element's control points (27 x 12 B packed) and its
-    # reference box (24 B) + 64 B per inner node visited
+    # algorithmic bytes per located point: point 12 B + Location 16 B + one
+    # element's control-point indices and coordinates nd x (4 + 12) B + its
+    # reference box 24 B + 64 B per inner node visited
     nd_dofs = (m.order + 1) ** 3
-    bytes_q = 12 + 16 + mean_ca * (nd_dofs * 12 + 24) + 64 * mean_nd
+    bytes_q = 12 + 16 + nd_dofs * 16 + 24 + 64 * mean_nd
     achieved_gbs = n * bytes_q / (kern_ms * 1e-3) / 1e9
+    # FP32 work of the same launch: Newton steps, inside tests (6 compares
+    # per candidate) and node tests (12 compares per inner node)
+    flops_q = mean_it * newton_step_flops(m.order) + 6 * mean_ca + 12 * mean_nd
+    achieved_tflops = n * flops_q / (kern_ms * 1e-3) / 1e12
     peaks = {}
     try:
         peaks = json.loads((ROOT / "MEASURED_PEAKS.json").read_text())
@@ -538,7 +558,11 @@ def main():
             "roofline": {"bound": "hbm", "achieved": achieved_gbs, "peak": peak, "unit": "GB/s",
                          "frac": achieved_gbs / peak, "traffic": None,
                          "peak_source": peak_src, "kernel": "locate_persistent_kernel",
-                         "bytes_per_query": bytes_q, "kernel_ms": kern_ms},
+                         "bytes_per_query": bytes_q, "kernel_ms": kern_ms,
+                         "fp32": {"flops_per_query": flops_q, "achieved_tflops": achieved_tflops,
+                                  "peak_tflops": FP32_PEAK_TFLOPS,
+                                  "frac": achieved_tflops / FP32_PEAK_TFLOPS,
+                                  "peak_source": "nominal: 148 SMs x 128 lanes x 2 x 1.965 GHz"}},
             "e2e": {"value": e2e_value, "unit": "points/s",
                     "h2d_bytes_per_step": int(n * 12), "d2h_bytes_per_step": int(n * 16),
                     "ms_per_step": e2e_ms},

@@ -68,8 +68,21 @@ template <> struct Basis1D<3>
 
 template <int P> constexpr int hex_dofs () { return (P + 1) * (P + 1) * (P + 1); }
 template <int P> constexpr int quad_dofs () { return (P + 1) * (P + 1); }
-// Packed per-element stride (floats), padded to a float4 multiple.
-DRB_HD constexpr int packed_stride (int nd, int ncomp) { return ((nd * ncomp + 3) / 4) * 4; }
+// Packed element rows (drb_pack_elements), one per element, padded to a
+// multiple of 4 floats so every row starts on a 16-byte boundary.
+//   geometry (ncomp 3): control points relative to the element's first
+//     control point O (P_i - O, rounded once in FP32), then O itself at
+//     float offset 3 nd.  Newton then works on X(r) - O and pt - O, whose
+//     magnitudes are the element size instead of the domain size, so its
+//     rounding noise in reference space no longer grows with the element
+//     count (with absolute coordinates a 128^3 mesh in [0,1]^3 sits at
+//     about 2e-5, above a 1e-5 tolerance).
+//   scalar fields (ncomp 1): the values.
+DRB_HD constexpr int packed_stride (int nd, int ncomp)
+{
+  return ncomp == 3 ? ((3 * nd + 3 + 3) / 4) * 4 : ((nd * ncomp + 3) / 4) * 4;
+}
+DRB_HD constexpr int packed_origin (int nd) { return 3 * nd; }
 
 // Hex element: value X and the three columns dX/du, dX/dv, dX/dw.
 // `cp(i, k)` returns component k of control point i.

@@ -525,6 +525,12 @@ __global__ void pack_kernel (const int *__restrict__ ctrl_idx, const float *__re
     const int i = r / NC;
     const int k = r - NC * i;
     v = __ldg (vals + (size_t)NC * __ldg (ctrl_idx + (size_t)e * nd + i) + k);
+    // geometry rows: relative to the first control point (packed_stride)
+    if (NC == 3) v = __fsub_rn (v, __ldg (vals + (size_t)NC * __ldg (ctrl_idx + (size_t)e * nd) + k));
+  }
+  else if (NC == 3 && r < nd * NC + 3)
+  {
+    v = __ldg (vals + (size_t)NC * __ldg (ctrl_idx + (size_t)e * nd) + (r - nd * NC));
   }
   packed[t] = v;
 }

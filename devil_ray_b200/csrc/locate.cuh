@@ -61,15 +61,18 @@ DRB_D bool solve_in_element (const LocateParams &lp, int el, const float (&pt)[3
   constexpr int ND = (P + 1) * (P + 1) * (P + 1);
   if (lp.packed)
   {
+    // packed rows are relative to the element's first control point
     const float *row = lp.packed + (size_t)el * lp.stride;
+    float t[3];
+    local_target<ND> (row, pt, t);
     if (REG && P <= 2)
     {
       RegCP<3 * ND> r;
       load_reg_cp<P> (r, row);
-      return hex_newton<P> (r, pt, x, lp.tol, lp.max_steps, steps);
+      return hex_newton<P> (r, t, x, lp.tol, lp.max_steps, steps);
     }
     PackedCP cp{ row };
-    return hex_newton<P> (cp, pt, x, lp.tol, lp.max_steps, steps);
+    return hex_newton<P> (cp, t, x, lp.tol, lp.max_steps, steps);
   }
   IndirectCP cp{ lp.ctrl_idx + (size_t)el * ND, lp.xyz, 3 };
   return hex_newton<P> (cp, pt, x, lp.tol, lp.max_steps, steps);

@@ -49,16 +49,26 @@ constexpr int kBf16 = kBW2T + kHid * kHid;
 
 constexpr uint32_t kWaitTries = 1u << 22;
 
+// tanh on the special-function unit (PTX tanh.approx.f32, relative error
+// about 2^-11): one instruction instead of a libm-style evaluation, and
+// well below the bf16 rounding the activations go through.
+DRB_D float tanh_sfu (float x)
+{
+  float y;
+  asm ("tanh.approx.f32 %0, %1;" : "=f"(y) : "f"(x));
+  return y;
+}
+
 // GELU, tanh form: 0.5 x (1 + tanh(sqrt(2/pi) (x + 0.044715 x^3)))
 DRB_D float gelu (float x)
 {
   const float u = 0.7978845608028654f * (x + 0.044715f * x * x * x);
-  return 0.5f * x * (1.f + tanhf (u));
+  return 0.5f * x * (1.f + tanh_sfu (u));
 }
 DRB_D float gelu_grad (float x)
 {
   const float u = 0.7978845608028654f * (x + 0.044715f * x * x * x);
-  const float t = tanhf (u);
+  const float t = tanh_sfu (u);
   const float du = 0.7978845608028654f * (1.f + 3.f * 0.044715f * x * x);
   return 0.5f * (1.f + t) + 0.5f * x * (1.f - t * t) * du;
 }
@@ -66,50 +76,85 @@ DRB_D float gelu_grad (float x)
 // Features of one (element, point) pair: control points and point relative
 // to the centre of the element's control-point box, scaled by its largest
 // half-extent.  27 x 3 control coordinates, then the point, then zeros.
-DRB_D void pair_features (const float *__restrict__ row, const float (&pt)[3], float (&f)[kInPad])
+// The packed row holds 84 floats (81 coordinates relative to the first
+// control point O, then O), 16-byte aligned, so it is read as float4.
+constexpr int kRowF4 = 21;
+static_assert (packed_stride (27, 3) == 4 * kRowF4 && packed_origin (27) == 81,
+               "order-2 geometry rows: 81 relative coordinates, then the origin");
+
+// Centre and inverse largest half-extent of the control-point box.
+DRB_D void pair_frame (const float *__restrict__ row, float (&c)[3], float &inv)
 {
+  const float4 *r4 = reinterpret_cast<const float4 *> (row);
   float mn[3] = { INFINITY, INFINITY, INFINITY }, mx[3] = { -INFINITY, -INFINITY, -INFINITY };
 #pragma unroll
-  for (int i = 0; i < 27; ++i)
+  for (int j = 0; j < kRowF4; ++j)
+  {
+    const float4 v4 = __ldg (r4 + j);
+    const float v[4] = { v4.x, v4.y, v4.z, v4.w };
 #pragma unroll
-    for (int k = 0; k < 3; ++k)
+    for (int t = 0; t < 4; ++t)
     {
-      const float v = __ldg (row + 3 * i + k);
-      f[3 * i + k] = v;
-      mn[k] = fminf (mn[k], v);
-      mx[k] = fmaxf (mx[k], v);
+      const int q = 4 * j + t;
+      if (q < 81)
+      {
+        mn[q % 3] = fminf (mn[q % 3], v[t]);
+        mx[q % 3] = fmaxf (mx[q % 3], v[t]);
+      }
     }
-  float c[3], h = 0.f;
+  }
+  float h = 0.f;
 #pragma unroll
   for (int k = 0; k < 3; ++k)
   {
     c[k] = 0.5f * (mn[k] + mx[k]);
     h = fmaxf (h, 0.5f * (mx[k] - mn[k]));
   }
-  const float inv = h > 0.f ? 1.f / h : 0.f;
-#pragma unroll
-  for (int i = 0; i < 27; ++i)
-#pragma unroll
-    for (int k = 0; k < 3; ++k) f[3 * i + k] = (f[3 * i + k] - c[k]) * inv;
-#pragma unroll
-  for (int k = 0; k < 3; ++k) f[81 + k] = (pt[k] - c[k]) * inv;
-#pragma unroll
-  for (int q = kIn; q < kInPad; ++q) f[q] = 0.f;
+  inv = h > 0.f ? 1.f / h : 0.f;
 }
 
-// Store one row of K bf16 values into an interleaved K-major tile.
-template <int K>
-DRB_D void store_row_bf16 (unsigned char *tile, int r, const float *v)
+// Features [8 k8, 8 k8 + 8) of one pair as eight packed bf16 (k8 < 12).
+DRB_D uint4 pair_features8 (const float *__restrict__ row, const float (&pt)[3], const float (&c)[3],
+                            float inv, int k8)
 {
-#pragma unroll
-  for (int k8 = 0; k8 < K / 8; ++k8)
+  float v[8];
+  if (k8 < 10)
   {
-    __align__ (16) __nv_bfloat16 b[8];
-#pragma unroll
-    for (int j = 0; j < 8; ++j) b[j] = __float2bfloat16_rn (v[8 * k8 + j]);
-    *reinterpret_cast<uint4 *> (tile + umma::tile_offset (r, 8 * k8, K)) =
-    *reinterpret_cast<const uint4 *> (b);
+    const float4 a = __ldg (reinterpret_cast<const float4 *> (row) + 2 * k8);
+    const float4 b = __ldg (reinterpret_cast<const float4 *> (row) + 2 * k8 + 1);
+    v[0] = a.x; v[1] = a.y; v[2] = a.z; v[3] = a.w;
+    v[4] = b.x; v[5] = b.y; v[6] = b.z; v[7] = b.w;
   }
+  else if (k8 == 10)
+  {
+    // floats 80..83: the last coordinate, then the row's origin O; the
+    // point enters in the row's frame, pt - O
+    const float4 a = __ldg (reinterpret_cast<const float4 *> (row) + 20);
+    v[0] = a.x;
+    v[1] = __fsub_rn (pt[0], a.y);
+    v[2] = __fsub_rn (pt[1], a.z);
+    v[3] = __fsub_rn (pt[2], a.w);
+    v[4] = v[5] = v[6] = v[7] = 0.f;
+  }
+  else
+  {
+#pragma unroll
+    for (int t = 0; t < 8; ++t) v[t] = 0.f;
+  }
+#pragma unroll
+  for (int t = 0; t < 8; ++t)
+  {
+    const int q = 8 * k8 + t;
+    if (q < 84) v[t] = (v[t] - c[q % 3]) * inv;
+  }
+  uint4 out;
+  __nv_bfloat162 p0 = __floats2bfloat162_rn (v[0], v[1]), p1 = __floats2bfloat162_rn (v[2], v[3]);
+  __nv_bfloat162 p2 = __floats2bfloat162_rn (v[4], v[5]), p3 = __floats2bfloat162_rn (v[6], v[7]);
+  out.x = *reinterpret_cast<uint32_t *> (&p0);
+  out.y = *reinterpret_cast<uint32_t *> (&p1);
+  out.z = *reinterpret_cast<uint32_t *> (&p2);
+  out.w = *reinterpret_cast<uint32_t *> (&p3);
+  return out;
 }
 
 // ------------------------------------------------------------ prepare --
@@ -138,26 +183,20 @@ __global__ void features_kernel (const float *__restrict__ packed, int stride,
 {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= n_pad) return;
-  float f[kInPad];
   const int e = i < n ? elem[i] : -1;
-  if (e >= 0)
-  {
-    const float pt[3] = { pts[3 * (size_t)i], pts[3 * (size_t)i + 1], pts[3 * (size_t)i + 2] };
-    pair_features (packed + (size_t)e * stride, pt, f);
-  }
-  else
+  uint4 *dst = reinterpret_cast<uint4 *> (X + (size_t)i * kInPad);
+  if (e < 0)
   {
 #pragma unroll
-    for (int q = 0; q < kInPad; ++q) f[q] = 0.f;
+    for (int k8 = 0; k8 < kInPad / 8; ++k8) dst[k8] = make_uint4 (0u, 0u, 0u, 0u);
+    return;
   }
+  const float *row = packed + (size_t)e * stride;
+  const float pt[3] = { pts[3 * (size_t)i], pts[3 * (size_t)i + 1], pts[3 * (size_t)i + 2] };
+  float c[3], inv;
+  pair_frame (row, c, inv);
 #pragma unroll
-  for (int q = 0; q < kInPad; q += 8)
-  {
-    __align__ (16) __nv_bfloat16 b[8];
-#pragma unroll
-    for (int j = 0; j < 8; ++j) b[j] = __float2bfloat16_rn (f[q + j]);
-    *reinterpret_cast<uint4 *> (X + (size_t)i * kInPad + q) = *reinterpret_cast<const uint4 *> (b);
-  }
+  for (int k8 = 0; k8 < kInPad / 8; ++k8) dst[k8] = pair_features8 (row, pt, c, inv, k8);
 }
 
 // --------------------------------------------------------------- GEMM --
@@ -291,80 +330,94 @@ __global__ void __launch_bounds__ (128) gemm_kernel (GemmArgs g)
 // ------------------------------------------------------- head / losses --
 
 // y = W3 gelu(Z2) + b3; masked MSE; dY; grads of W3, b3; dZ2 = (W3^T dY) x
-// gelu'(Z2) as bf16; db2 partial sums.  One thread per row.
+// gelu'(Z2) as bf16; db2.  One block of 128 threads per 128 rows, in two
+// coalesced phases: a warp per row for the head and dY (Z2 rows read as
+// float4, the 3 dot products reduced by shuffles), then a thread per column
+// over the block's rows for dZ2 and the weight-gradient column sums, so the
+// block adds one partial per parameter to the global gradient.
 __global__ void __launch_bounds__ (128)
 head_kernel (const float *__restrict__ p, const float *__restrict__ Z2, const float *__restrict__ target,
              const float *__restrict__ weight, int n, int n_pad, float inv_count, float *__restrict__ y_out,
              float *__restrict__ grad, __nv_bfloat16 *__restrict__ dZ2, float *__restrict__ loss)
 {
   __shared__ float s_w3[kOut * kHid];
-  __shared__ float s_gw3[kOut * kHid];
-  __shared__ float s_db2[kHid];
-  __shared__ float s_gb3[kOut];
+  __shared__ float s_dy[128][kOut];
   __shared__ float s_loss;
-  for (int q = threadIdx.x; q < kOut * kHid; q += blockDim.x)
-  {
-    s_w3[q] = p[kW3 + q];
-    s_gw3[q] = 0.f;
-  }
-  for (int q = threadIdx.x; q < kHid; q += blockDim.x) s_db2[q] = 0.f;
-  if (threadIdx.x < kOut) s_gb3[threadIdx.x] = 0.f;
-  if (threadIdx.x == 0) s_loss = 0.f;
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  for (int q = tid; q < kOut * kHid; q += blockDim.x) s_w3[q] = p[kW3 + q];
+  if (tid == 0) s_loss = 0.f;
   __syncthreads ();
-  const int i = blockIdx.x * blockDim.x + threadIdx.x;
-  if (i < n_pad)
+  const int r0 = blockIdx.x * 128;
+  const int rows = min (128, n_pad - r0);
+  const float b3[kOut] = { p[kB3], p[kB3 + 1], p[kB3 + 2] };
+  // phase 1: head and dY, a warp per row, lane l holds columns [4 l, 4 l + 4)
+  for (int rr = warp; rr < rows; rr += 4)
   {
-    float h[kHid];
-    const float *z = Z2 + (size_t)i * kHid;
-#pragma unroll 8
-    for (int c = 0; c < kHid; ++c) h[c] = gelu (z[c]);
-    float y[kOut], dy[kOut];
+    const int i = r0 + rr;
+    const float4 z4 = *reinterpret_cast<const float4 *> (Z2 + (size_t)i * kHid + 4 * lane);
+    const float z[4] = { z4.x, z4.y, z4.z, z4.w };
+    float y[kOut] = { 0.f, 0.f, 0.f };
+#pragma unroll
+    for (int t = 0; t < 4; ++t)
+    {
+      const float h = gelu (z[t]);
+#pragma unroll
+      for (int o = 0; o < kOut; ++o) y[o] = fmaf (s_w3[o * kHid + 4 * lane + t], h, y[o]);
+    }
 #pragma unroll
     for (int o = 0; o < kOut; ++o)
-    {
-      float s = p[kB3 + o];
-#pragma unroll 8
-      for (int c = 0; c < kHid; ++c) s += s_w3[o * kHid + c] * h[c];
-      y[o] = s;
-    }
-    const float w = (i < n && weight) ? weight[i] : (i < n ? 1.f : 0.f);
-    float l = 0.f;
 #pragma unroll
-    for (int o = 0; o < kOut; ++o)
+      for (int off = 16; off > 0; off >>= 1) y[o] += __shfl_xor_sync (0xffffffffu, y[o], off);
+    if (lane == 0)
     {
-      const float e = (i < n && target) ? (y[o] - target[3 * (size_t)i + o]) : 0.f;
-      l += w * e * e;
-      dy[o] = 2.f * w * e * inv_count;
-      if (y_out && i < n) y_out[3 * (size_t)i + o] = y[o];
-    }
-    if (grad)
-    {
-      atomicAdd (&s_loss, l * inv_count);
+      const float w = (i < n && weight) ? weight[i] : (i < n ? 1.f : 0.f);
+      float l = 0.f;
 #pragma unroll
       for (int o = 0; o < kOut; ++o)
       {
-        atomicAdd (&s_gb3[o], dy[o]);
-        for (int c = 0; c < kHid; ++c) atomicAdd (&s_gw3[o * kHid + c], dy[o] * h[c]);
+        const float yo = y[o] + b3[o];
+        const float e = (i < n && target) ? (yo - target[3 * (size_t)i + o]) : 0.f;
+        l += w * e * e;
+        s_dy[rr][o] = 2.f * w * e * inv_count;
+        if (y_out && i < n) y_out[3 * (size_t)i + o] = yo;
       }
-      for (int c = 0; c < kHid; ++c)
-      {
-        float dh = 0.f;
-#pragma unroll
-        for (int o = 0; o < kOut; ++o) dh += s_w3[o * kHid + c] * dy[o];
-        const float dz = dh * gelu_grad (z[c]);
-        dZ2[(size_t)i * kHid + c] = __float2bfloat16_rn (dz);
-        atomicAdd (&s_db2[c], dz);
-      }
+      if (grad) atomicAdd (&s_loss, l * inv_count);
     }
   }
+  if (!grad) return;
   __syncthreads ();
-  if (grad)
+  // phase 2: thread c owns column c of the block's rows
+  const int c = tid;
+  float gw3[kOut] = { 0.f, 0.f, 0.f };
+  float db2 = 0.f;
+  const float w3c[kOut] = { s_w3[c], s_w3[kHid + c], s_w3[2 * kHid + c] };
+  for (int rr = 0; rr < rows; ++rr)
   {
-    for (int q = threadIdx.x; q < kOut * kHid; q += blockDim.x) atomicAdd (grad + kW3 + q, s_gw3[q]);
-    for (int q = threadIdx.x; q < kHid; q += blockDim.x) atomicAdd (grad + kB2 + q, s_db2[q]);
-    if (threadIdx.x < kOut) atomicAdd (grad + kB3 + threadIdx.x, s_gb3[threadIdx.x]);
-    if (threadIdx.x == 0 && loss) atomicAdd (loss, s_loss);
+    const size_t at = (size_t)(r0 + rr) * kHid + c;
+    const float z = Z2[at];
+    const float h = gelu (z);
+    float dh = 0.f;
+#pragma unroll
+    for (int o = 0; o < kOut; ++o)
+    {
+      const float dy = s_dy[rr][o];
+      gw3[o] = fmaf (dy, h, gw3[o]);
+      dh = fmaf (w3c[o], dy, dh);
+    }
+    const float dz = dh * gelu_grad (z);
+    dZ2[at] = __float2bfloat16_rn (dz);
+    db2 += dz;
   }
+#pragma unroll
+  for (int o = 0; o < kOut; ++o) atomicAdd (grad + kW3 + o * kHid + c, gw3[o]);
+  atomicAdd (grad + kB2 + c, db2);
+  if (tid < kOut)
+  {
+    float gb = 0.f;
+    for (int rr = 0; rr < rows; ++rr) gb += s_dy[rr][tid];
+    atomicAdd (grad + kB3 + tid, gb);
+  }
+  if (tid == 0 && loss) atomicAdd (loss, s_loss);
 }
 
 // column sums of a bf16 [rows x 128] matrix into grad[off + c]
@@ -426,133 +479,176 @@ struct GuessArgs
   int stride;
   const int *elem;
   const float *pts;
+  const int *order;
   int n;
   float *guess;
   int *err;
 };
 
-constexpr size_t kGuessSmem = (size_t)kHid * kInPad * 2 * 2 + (size_t)kHid * kHid * 2 * 2 + 1024;
+// Fused inference keeps four 128-row tiles in flight per CTA, one per
+// warpgroup, with the bf16 weights resident once per CTA.  Each warpgroup
+// owns one activation tile (the 96-wide layer-1 input, then the 128-wide
+// layer-2 input in the same bytes) and 128 TMEM columns (D1, then D2 in the
+// same columns), and synchronises only with itself (named barrier 1 + g),
+// so one group's gathers and epilogues overlap the others' MMAs.
+constexpr int kGuessGroups = 4;
+constexpr int kGuessThreads = 128 * kGuessGroups;
+constexpr size_t kGuessW1 = (size_t)kHid * kInPad * 2;
+constexpr size_t kGuessW2 = (size_t)kHid * kHid * 2;
+constexpr size_t kGuessAct = (size_t)128 * kHid * 2;
+constexpr size_t kGuessSmem = kGuessW1 + kGuessW2 + kGuessGroups * kGuessAct;
 
-__global__ void __launch_bounds__ (128) mlp_guess_kernel (GuessArgs a)
+DRB_D void group_sync (int g)
+{
+  asm volatile ("bar.sync %0, %1;" ::"r"(1 + g), "r"(128) : "memory");
+}
+// AND of a predicate over the 128 threads of warpgroup g.
+DRB_D bool group_and (int g, bool v)
+{
+  uint32_t r;
+  asm volatile ("{\n\t.reg .pred p, q;\n\tsetp.ne.u32 q, %1, 0;\n\t"
+                "bar.red.and.pred p, %2, 128, q;\n\tselp.u32 %0, 1, 0, p;\n\t}\n"
+                : "=r"(r)
+                : "r"((uint32_t)v), "r"(1 + g)
+                : "memory");
+  return r != 0;
+}
+
+__global__ void __launch_bounds__ (kGuessThreads, 1) mlp_guess_kernel (GuessArgs a)
 {
   extern __shared__ __align__ (1024) unsigned char smem[];
-  unsigned char *sW1 = smem;                                 // 128 x 96
-  unsigned char *sW2 = sW1 + kHid * kInPad * 2;              // 128 x 128
-  unsigned char *sA1 = sW2 + kHid * kHid * 2;                // 128 x 96
-  unsigned char *sA2 = sA1 + kHid * kInPad * 2;              // 128 x 128
+  unsigned char *sW1 = smem;                     // 128 x 96
+  unsigned char *sW2 = sW1 + kGuessW1;           // 128 x 128
   __shared__ float s_b1[kHid], s_b2[kHid], s_w3[kOut * kHid], s_b3[kOut];
-  __shared__ __align__ (8) uint64_t mbar;
+  __shared__ __align__ (8) uint64_t mbar[kGuessGroups];
   __shared__ uint32_t tmem_base;
   const int tid = threadIdx.x;
   const int warp = tid >> 5;
-  // weights into the interleaved layout (once per CTA)
-  for (int v = tid; v < kHid * (kInPad / 8); v += 128)
+  const int g = warp >> 2;              // warpgroup = tile slot
+  const int row = tid & 127;            // row of the tile = TMEM lane
+  unsigned char *sAct = sW2 + kGuessW2 + (size_t)g * kGuessAct;
+  for (int v = tid; v < kHid * (kInPad / 8); v += kGuessThreads)
   {
     const int r = v / (kInPad / 8), j = v - r * (kInPad / 8);
     *reinterpret_cast<uint4 *> (sW1 + umma::tile_offset (r, 8 * j, kInPad)) =
     *reinterpret_cast<const uint4 *> (a.wb + kBW1 + (size_t)r * kInPad + 8 * j);
   }
-  for (int v = tid; v < kHid * (kHid / 8); v += 128)
+  for (int v = tid; v < kHid * (kHid / 8); v += kGuessThreads)
   {
     const int r = v / (kHid / 8), j = v - r * (kHid / 8);
     *reinterpret_cast<uint4 *> (sW2 + umma::tile_offset (r, 8 * j, kHid)) =
     *reinterpret_cast<const uint4 *> (a.wb + kBW2 + (size_t)r * kHid + 8 * j);
   }
-  for (int q = tid; q < kHid; q += 128)
+  for (int q = tid; q < kHid; q += kGuessThreads)
   {
     s_b1[q] = a.params[kB1 + q];
     s_b2[q] = a.params[kB2 + q];
   }
-  for (int q = tid; q < kOut * kHid; q += 128) s_w3[q] = a.params[kW3 + q];
+  for (int q = tid; q < kOut * kHid; q += kGuessThreads) s_w3[q] = a.params[kW3 + q];
   if (tid < kOut) s_b3[tid] = a.params[kB3 + tid];
-  if (warp == 0) umma::tmem_alloc (&tmem_base, 2 * kHid);
-  if (tid == 0) umma::mbar_init (&mbar, 1);
+  if (warp == 0) umma::tmem_alloc (&tmem_base, kGuessGroups * kHid);
+  if (tid < kGuessGroups) umma::mbar_init (&mbar[tid], 1);
   umma::fence_before_sync ();
   __syncthreads ();
   umma::fence_after_sync ();
-  const uint32_t t1 = tmem_base;          // D1: columns [0, 128)
-  const uint32_t t2 = tmem_base + kHid;   // D2: columns [128, 256)
-  const uint32_t lane_off = (uint32_t)(warp * 32) << 16;
+  // warp w reads TMEM lanes [32 (w % 4), +32); its group's columns start at 128 g
+  const uint32_t tacc = tmem_base + (uint32_t)(g * kHid) + ((uint32_t)((warp & 3) * 32) << 16);
+  const uint32_t tmma = tmem_base + (uint32_t)(g * kHid);
   const uint32_t idesc = umma::idesc_bf16_f32 (128, kHid);
   uint32_t phase = 0;
   bool ok = true;
   const int tiles = (a.n + 127) / 128;
-  for (int tile = blockIdx.x; tile < tiles && ok; tile += gridDim.x)
+  for (int tile = blockIdx.x * kGuessGroups + g; tile < tiles; tile += gridDim.x * kGuessGroups)
   {
-    const int i = tile * 128 + tid;
-    const int e = (i < a.n) ? a.elem[i] : -1;
+    const int i = tile * 128 + row;
+    const int q = i < a.n ? (a.order ? __ldg (a.order + i) : i) : -1;
+    const int e = q >= 0 ? __ldg (a.elem + q) : -1;
+    float pt[3] = { 0.f, 0.f, 0.f };
+    // layer-1 input row: features in the 96-wide interleaved layout
+    if (e >= 0)
     {
-      float f[kInPad];
-      if (e >= 0)
-      {
-        const float pt[3] = { a.pts[3 * (size_t)i], a.pts[3 * (size_t)i + 1], a.pts[3 * (size_t)i + 2] };
-        pair_features (a.packed + (size_t)e * a.stride, pt, f);
-      }
-      else
-      {
+      pt[0] = __ldg (a.pts + 3 * (size_t)q);
+      pt[1] = __ldg (a.pts + 3 * (size_t)q + 1);
+      pt[2] = __ldg (a.pts + 3 * (size_t)q + 2);
+      const float *er = a.packed + (size_t)e * a.stride;
+      float c[3], inv;
+      pair_frame (er, c, inv);
 #pragma unroll
-        for (int q = 0; q < kInPad; ++q) f[q] = 0.f;
-      }
-      store_row_bf16<kInPad> (sA1, tid, f);
+      for (int k8 = 0; k8 < kInPad / 8; ++k8)
+        *reinterpret_cast<uint4 *> (sAct + umma::tile_offset (row, 8 * k8, kInPad)) =
+        pair_features8 (er, pt, c, inv, k8);
+    }
+    else
+    {
+#pragma unroll
+      for (int k8 = 0; k8 < kInPad / 8; ++k8)
+        *reinterpret_cast<uint4 *> (sAct + umma::tile_offset (row, 8 * k8, kInPad)) =
+        make_uint4 (0u, 0u, 0u, 0u);
     }
     umma::fence_async_smem ();
-    __syncthreads ();
-    if (tid == 0)
+    group_sync (g);
+    if (row == 0)
     {
       umma::fence_after_sync ();
-      const uint32_t a0 = umma::smem_addr (sA1), b0 = umma::smem_addr (sW1);
+      const uint32_t a0 = umma::smem_addr (sAct), b0 = umma::smem_addr (sW1);
 #pragma unroll
       for (int kk = 0; kk < kInPad / 16; ++kk)
-        umma::mma_bf16 (t1, umma::desc_kmajor (a0 + kk * 256, 128, (kInPad / 8) * 128),
+        umma::mma_bf16 (tmma, umma::desc_kmajor (a0 + kk * 256, 128, (kInPad / 8) * 128),
                         umma::desc_kmajor (b0 + kk * 256, 128, (kInPad / 8) * 128), idesc,
                         kk > 0 ? 1u : 0u);
-      umma::mma_commit (&mbar);
+      umma::mma_commit (&mbar[g]);
     }
-    ok = umma::mbar_wait (&mbar, phase, kWaitTries);
+    ok = group_and (g, umma::mbar_wait (&mbar[g], phase, kWaitTries));
     phase ^= 1u;
     umma::fence_after_sync ();
-    if (!__syncthreads_and (ok)) break;
-    // layer 1 epilogue -> A2 (bf16 GELU activations)
+    if (!ok) break;
+    // layer-1 epilogue: GELU(D1 + b1) as bf16 -> layer-2 input (same bytes)
+#pragma unroll 1
     for (int c0 = 0; c0 < kHid; c0 += 32)
     {
       float d[32];
-      umma::tmem_ld32 (t1 + lane_off + c0, d);
-#pragma unroll
-      for (int j = 0; j < 32; ++j) d[j] = gelu (d[j] + s_b1[c0 + j]);
+      umma::tmem_ld32 (tacc + c0, d);
 #pragma unroll
       for (int k8 = 0; k8 < 4; ++k8)
       {
-        __align__ (16) __nv_bfloat16 b[8];
+        uint4 o;
+        uint32_t *ow = reinterpret_cast<uint32_t *> (&o);
 #pragma unroll
-        for (int j = 0; j < 8; ++j) b[j] = __float2bfloat16_rn (d[8 * k8 + j]);
-        *reinterpret_cast<uint4 *> (sA2 + umma::tile_offset (tid, c0 + 8 * k8, kHid)) =
-        *reinterpret_cast<const uint4 *> (b);
+        for (int j = 0; j < 4; ++j)
+        {
+          const int cc = 8 * k8 + 2 * j;
+          __nv_bfloat162 h2 = __floats2bfloat162_rn (gelu (d[cc] + s_b1[c0 + cc]),
+                                                     gelu (d[cc + 1] + s_b1[c0 + cc + 1]));
+          ow[j] = *reinterpret_cast<uint32_t *> (&h2);
+        }
+        *reinterpret_cast<uint4 *> (sAct + umma::tile_offset (row, c0 + 8 * k8, kHid)) = o;
       }
     }
     umma::fence_async_smem ();
     umma::fence_before_sync ();
-    __syncthreads ();
-    if (tid == 0)
+    group_sync (g);
+    if (row == 0)
     {
       umma::fence_after_sync ();
-      const uint32_t a0 = umma::smem_addr (sA2), b0 = umma::smem_addr (sW2);
+      const uint32_t a0 = umma::smem_addr (sAct), b0 = umma::smem_addr (sW2);
 #pragma unroll
       for (int kk = 0; kk < kHid / 16; ++kk)
-        umma::mma_bf16 (t2, umma::desc_kmajor (a0 + kk * 256, 128, (kHid / 8) * 128),
+        umma::mma_bf16 (tmma, umma::desc_kmajor (a0 + kk * 256, 128, (kHid / 8) * 128),
                         umma::desc_kmajor (b0 + kk * 256, 128, (kHid / 8) * 128), idesc,
                         kk > 0 ? 1u : 0u);
-      umma::mma_commit (&mbar);
+      umma::mma_commit (&mbar[g]);
     }
-    ok = umma::mbar_wait (&mbar, phase, kWaitTries);
+    ok = group_and (g, umma::mbar_wait (&mbar[g], phase, kWaitTries));
     phase ^= 1u;
     umma::fence_after_sync ();
-    if (!__syncthreads_and (ok)) break;
-    // layer 2 epilogue + 128 -> 3 head on the CUDA cores
+    if (!ok) break;
+    // layer-2 epilogue + 128 -> 3 head on the CUDA cores
     float y[kOut] = { s_b3[0], s_b3[1], s_b3[2] };
+#pragma unroll 1
     for (int c0 = 0; c0 < kHid; c0 += 32)
     {
       float d[32];
-      umma::tmem_ld32 (t2 + lane_off + c0, d);
+      umma::tmem_ld32 (tacc + c0, d);
 #pragma unroll
       for (int j = 0; j < 32; ++j)
       {
@@ -561,19 +657,20 @@ __global__ void __launch_bounds__ (128) mlp_guess_kernel (GuessArgs a)
         for (int o = 0; o < kOut; ++o) y[o] = fmaf (s_w3[o * kHid + c0 + j], h, y[o]);
       }
     }
-    if (i < a.n)
+    if (q >= 0)
     {
 #pragma unroll
       for (int o = 0; o < kOut; ++o)
-        a.guess[3 * (size_t)i + o] = (e >= 0) ? fminf (1.f, fmaxf (0.f, y[o])) : 0.5f;
+        a.guess[3 * (size_t)q + o] = (e >= 0) ? fminf (1.f, fmaxf (0.f, y[o])) : 0.5f;
     }
+    // D2 and the activation tile are reused by the next tile of this group
     umma::fence_before_sync ();
-    __syncthreads ();
+    group_sync (g);
   }
-  if (!ok && tid == 0 && a.err) atomicExch (a.err, 1);
+  if (!ok && row == 0 && a.err) atomicExch (a.err, 1);
   umma::fence_before_sync ();
   __syncthreads ();
-  if (warp == 0) umma::tmem_dealloc (tmem_base, 2 * kHid);
+  if (warp == 0) umma::tmem_dealloc (tmem_base, kGuessGroups * kHid);
 }
 
 template <int EPI> int launch_gemm (const GemmArgs &g, cudaStream_t s)
@@ -793,8 +890,8 @@ extern "C" int drb_mlp_adam (float *params, const float *grad, float *m, float *
 }
 
 extern "C" int drb_mlp_guess (const float *params, const void *wbf16, const drb_mesh *mesh,
-                              const int *elem, const float *pts, int n, float *guess, int *err,
-                              void *stream)
+                              const int *elem, const float *pts, const int *order, int n,
+                              float *guess, int *err, void *stream)
 {
   if (!params || !wbf16 || !mesh || !mesh->packed || mesh->dim != 3 || mesh->order != 2 ||
       mesh->ncomp != 3 || n < 0 || (n > 0 && (!elem || !pts || !guess)))
@@ -810,12 +907,13 @@ extern "C" int drb_mlp_guess (const float *params, const void *wbf16, const drb_
   a.stride = packed_stride (27, 3);
   a.elem = elem;
   a.pts = pts;
+  a.order = order;
   a.n = n;
   a.guess = guess;
   a.err = err;
   cudaFuncSetAttribute (mlp_guess_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kGuessSmem);
   const int tiles = div_up (n, 128);
-  const int grid = min (tiles, sm_count ());
-  mlp_guess_kernel<<<grid, 128, kGuessSmem, (cudaStream_t)stream>>> (a);
+  const int grid = min (div_up (tiles, kGuessGroups), sm_count ());
+  mlp_guess_kernel<<<grid, kGuessThreads, kGuessSmem, (cudaStream_t)stream>>> (a);
   return check_launch ("mlp_guess_kernel");
 }

@@ -82,6 +82,21 @@ struct PackedCP
   DRB_D float operator() (int i, int k) const { return __ldg (p + 3 * i + k); }
 };
 
+// pt - O for a packed geometry row with ND control points (O stored at
+// packed_origin(ND)); t is the Newton target in the row's frame.
+template <int ND> DRB_D void local_target (const float *__restrict__ row, const float (&pt)[3], float (&t)[3])
+{
+#pragma unroll
+  for (int d = 0; d < 3; ++d) t[d] = __fsub_rn (pt[d], __ldg (row + packed_origin (ND) + d));
+}
+
+// X + O: a position evaluated from a packed geometry row, in world space.
+template <int ND> DRB_D void to_world (const float *__restrict__ row, float (&X)[3])
+{
+#pragma unroll
+  for (int d = 0; d < 3; ++d) X[d] = __fadd_rn (X[d], __ldg (row + packed_origin (ND) + d));
+}
+
 // Control points of one element read through the reference's double
 // indirection val[ctrl_idx[e*nd+i]] (data_model/dof_access.hpp:23-54).
 struct IndirectCP

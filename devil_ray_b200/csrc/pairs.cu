@@ -25,8 +25,10 @@ __global__ void map_points_kernel (const float *__restrict__ packed, int stride,
   float X[3] = { NAN, NAN, NAN };
   if (e >= 0)
   {
-    PackedCP cp{ packed + (size_t)e * stride };
+    const float *row = packed + (size_t)e * stride;
+    PackedCP cp{ row };
     hex_eval<P, 3> (cp, ref[3 * (size_t)i], ref[3 * (size_t)i + 1], ref[3 * (size_t)i + 2], X);
+    to_world<(P + 1) * (P + 1) * (P + 1)> (row, X);
   }
   pts[3 * (size_t)i] = X[0];
   pts[3 * (size_t)i + 1] = X[1];
@@ -54,8 +56,10 @@ __global__ void newton_pairs_kernel (const float *__restrict__ packed, int strid
   bool ok = false;
   if (e >= 0)
   {
-    const float pt[3] = { pts[3 * (size_t)i], pts[3 * (size_t)i + 1], pts[3 * (size_t)i + 2] };
+    const float pw[3] = { pts[3 * (size_t)i], pts[3 * (size_t)i + 1], pts[3 * (size_t)i + 2] };
     const float *row = packed + (size_t)e * stride;
+    float pt[3];
+    local_target<(P + 1) * (P + 1) * (P + 1)> (row, pw, pt);
     if (P <= 2)
     {
       RegCP<3 * (P + 1) * (P + 1) * (P + 1)> r;

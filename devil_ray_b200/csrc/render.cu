@@ -334,8 +334,10 @@ DRB_D float4 shade_sample (const VolumeParams &vp, int el, const float (&r)[3], 
   float X[3], Ju[3], Jv[3], Jw[3];
   if (vp.lp.packed)
   {
-    PackedCP cp{ vp.lp.packed + (size_t)el * vp.lp.stride };
+    const float *row = vp.lp.packed + (size_t)el * vp.lp.stride;
+    PackedCP cp{ row };
     hex_eval_d<P, 3> (cp, r[0], r[1], r[2], X, Ju, Jv, Jw);
+    to_world<ND> (row, X);
   }
   else
   {

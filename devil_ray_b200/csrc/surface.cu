@@ -279,8 +279,14 @@ surface_kernel (SurfParams sp, const Ray *__restrict__ rays, int n, RayHit *__re
       bool inside;
       if (sp.packed)
       {
-        QuadPackedCP cp{ sp.packed + (size_t)el * sp.stride };
-        inside = face_newton<P> (cp, ray, x, t, sp.tol, sp.max_steps, steps);
+        // packed rows are relative to the face's first control point
+        const float *row = sp.packed + (size_t)el * sp.stride;
+        Ray lr = ray;
+        lr.orig.x = __fsub_rn (ray.orig.x, __ldg (row + packed_origin (ND)));
+        lr.orig.y = __fsub_rn (ray.orig.y, __ldg (row + packed_origin (ND) + 1));
+        lr.orig.z = __fsub_rn (ray.orig.z, __ldg (row + packed_origin (ND) + 2));
+        QuadPackedCP cp{ row };
+        inside = face_newton<P> (cp, lr, x, t, sp.tol, sp.max_steps, steps);
       }
       else
       {

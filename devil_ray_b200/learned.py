@@ -51,7 +51,7 @@ def _lib():
             "drb_mlp_forward": (ci, [vp, vp, vp, ci, ci, vp, vp, vp, vp]),
             "drb_mlp_train_step": (ci, [vp, vp, vp, vp, vp, ci, ci, vp, vp, vp, vp, vp]),
             "drb_mlp_adam": (ci, [vp, vp, vp, vp, cf, cf, cf, cf, ci, vp]),
-            "drb_mlp_guess": (ci, [vp, vp, C.POINTER(L.DrbMesh), vp, vp, ci, vp, vp, vp]),
+            "drb_mlp_guess": (ci, [vp, vp, C.POINTER(L.DrbMesh), vp, vp, vp, ci, vp, vp, vp]),
             "drb_map_points": (ci, [C.POINTER(L.DrbMesh), vp, vp, ci, vp, vp]),
             "drb_newton_pairs": (ci, [C.POINTER(L.DrbMesh), vp, vp, ci, cf, ci, vp, vp, vp, vp,
                                       vp]),
@@ -162,12 +162,12 @@ class GuessMLP:
                                     b1, b2, eps, self.step_count, _stream(stream)), "drb_mlp_adam")
         self.prepare(stream)
 
-    def guess(self, mesh, elem, pts, stream=None):
+    def guess(self, mesh, elem, pts, order=None, stream=None):
         n = elem.numel()
         out = torch.empty((max(n, 1), 3), dtype=torch.float32, device=self.device)
         L.check(_lib().drb_mlp_guess(_ptr(self.params), _ptr(self.wbf16), C.byref(mesh.desc()),
-                                     _ptr(elem), _ptr(pts), n, _ptr(out), _ptr(self.err),
-                                     _stream(stream)), "drb_mlp_guess")
+                                     _ptr(elem), _ptr(pts), _ptr(order), n, _ptr(out),
+                                     _ptr(self.err), _stream(stream)), "drb_mlp_guess")
         return out[:n]
 
     # -- checkpoint of weights and optimiser state --
@@ -245,7 +245,7 @@ class LearnedLocator:
         L.check(_lib().drb_first_candidates(C.byref(bvh.desc()), _ptr(pts), n, _ptr(order),
                                             _ptr(first_leaf), _ptr(first_elem), _stream(stream)),
                 "drb_first_candidates")
-        guess = self.model.guess(self.mesh, first_elem, pts, stream)
+        guess = self.model.guess(self.mesh, first_elem, pts, order, stream)
         if out is None:
             cell = torch.empty(n, dtype=torch.int32, device=dev)
             ref = torch.empty((n, 3), dtype=torch.float32, device=dev)

@@ -99,12 +99,17 @@ int drb_version (void);
 /* Number of kernels this library has launched in the process (all threads). */
 unsigned long long drb_kernel_launches (void);
 
-/* Floats per element in a packed element-major copy (padded to float4). */
+/* Floats per element in a packed element-major copy, padded to a multiple
+ * of 4 so each row is 16-byte aligned: geometry (ncomp 3) 3 nd + 3 (the
+ * origin), scalar fields nd. */
 int drb_packed_stride (int dim, int order, int ncomp);
 
 /* Gather the element control points into an element-major array
  * (replaces the double indirection val[ctrl_idx[e*nd+i]] of SharedDofPtr,
- * data_model/dof_access.hpp:23-54). */
+ * data_model/dof_access.hpp:23-54).  Geometry rows hold P_i - P_0 (FP32)
+ * followed by P_0, the element's first control point: the Newton solves
+ * run in that local frame, where FP32 rounding is relative to the element
+ * size rather than to the domain.  Scalar rows hold the values. */
 int drb_pack_elements (const drb_mesh *mesh, float *packed, void *stream);
 
 /* Sizes of the BVH over a mesh's sub-boxes: 33 per hex, 17 per quad
@@ -367,10 +372,13 @@ int drb_mlp_train_step (const float *params, const void *wbf16, const void *X,
                         float *loss, void *workspace, int *err, void *stream);
 int drb_mlp_adam (float *params, const float *grad, float *m, float *v, float lr, float beta1,
                   float beta2, float eps, int step, void *stream);
-/* fused tensor-core inference: guess device float[3n] for the pairs */
+/* fused tensor-core inference: guess device float[3n] for the pairs
+ * (elem[q], pts[q]); rows are visited in the order order[0..n) when given
+ * (the Morton order of drb_query_order keeps a tile's elements together in
+ * L1), else 0..n-1.  Results do not depend on the order. */
 int drb_mlp_guess (const float *params, const void *wbf16, const drb_mesh *mesh,
-                   const int *elem, const float *pts, int n, float *guess, int *err,
-                   void *stream);
+                   const int *elem, const float *pts, const int *order, int n, float *guess,
+                   int *err, void *stream);
 
 /* UnstructuredField::eval at located points (data_model/unstructured_field.cpp:
  * 214-245): values[i] = f(cell[i], ref[i]), empty_value where cell is -1. */

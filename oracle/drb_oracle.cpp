@@ -115,11 +115,19 @@ template <typename T> T maxabs3 (T a, T b, T c)
   return m;
 }
 
+// Control points of one element.  With an origin o (local frame), the value
+// is the FP32 difference P_i - o, as the packed element rows of the CUDA
+// path hold them (origin = the element's first control point).
 struct ElemCP
 {
   const int *idx;
   const float *xyz;
-  double operator() (int i, int k) const { return xyz[3 * (size_t)idx[i] + k]; }
+  const float *o = nullptr;
+  double operator() (int i, int k) const
+  {
+    const float v = xyz[3 * (size_t)idx[i] + k];
+    return o ? (double)(float)(v - o[k]) : (double)v;
+  }
 };
 
 // eval_inverse_local + IterativeMethod::solve (data_model/element.hpp:435-486,
@@ -166,8 +174,8 @@ bool newton (int p, const ElemCP &cp, const T *target, T *x, T tol, int max_step
 template <typename T>
 int locate_one (int p, const int *ctrl_idx, const float *xyz, const float *nodes, const int *leaf_nodes,
                 const int *aabb_ids, const float *ref_boxes, const float *pt, float tol,
-                int max_steps, int guess_mode, const float *guess, float *out_ref, int &iters,
-                int &cands)
+                int max_steps, int guess_mode, const float *guess, int local_frame, float *out_ref,
+                int &iters, int &cands)
 {
   // DeviceMesh::locate (device_mesh.hpp:248-354)
   const int nd = (p + 1) * (p + 1) * (p + 1);
@@ -218,7 +226,13 @@ int locate_one (int p, const int *ctrl_idx, const float *xyz, const float *nodes
       else x[0] = x[1] = x[2] = T (0.5);
       first = false;
       ElemCP cp{ ctrl_idx + (size_t)el * nd, xyz };
-      const T tgt[3] = { pt[0], pt[1], pt[2] };
+      T tgt[3] = { pt[0], pt[1], pt[2] };
+      if (local_frame)
+      {
+        // the target relative to the first control point, in FP32
+        cp.o = xyz + 3 * (size_t)ctrl_idx[(size_t)el * nd];
+        for (int d = 0; d < 3; ++d) tgt[d] = T ((float)(pt[d] - cp.o[d]));
+      }
       int steps = 0;
       bool found = newton<T> (p, cp, tgt, x, T (tol), max_steps, steps);
       iters += steps;
@@ -257,7 +271,7 @@ extern "C" void orc_locate (int p, int n_elem, const int *ctrl_idx, const float 
                             const float *inner_nodes, const int *leaf_nodes, const int *aabb_ids,
                             const float *ref_boxes, int n, const float *pts, float tol,
                             int max_steps, int guess_mode, const float *guess, int use_double,
-                            int *cell, float *ref, int *iters, int *cands)
+                            int local_frame, int *cell, float *ref, int *iters, int *cands)
 {
   (void)n_elem;
   (void)n_inner;
@@ -269,9 +283,9 @@ extern "C" void orc_locate (int p, int n_elem, const int *ctrl_idx, const float 
     const float *g = guess ? guess + 3 * (size_t)i : nullptr;
     int c = use_double
             ? locate_one<double> (p, ctrl_idx, xyz, inner_nodes, leaf_nodes, aabb_ids, ref_boxes,
-                                  pts + 3 * (size_t)i, tol, max_steps, guess_mode, g, r, it, ca)
+                                  pts + 3 * (size_t)i, tol, max_steps, guess_mode, g, local_frame, r, it, ca)
             : locate_one<float> (p, ctrl_idx, xyz, inner_nodes, leaf_nodes, aabb_ids, ref_boxes,
-                                 pts + 3 * (size_t)i, tol, max_steps, guess_mode, g, r, it, ca);
+                                 pts + 3 * (size_t)i, tol, max_steps, guess_mode, g, local_frame, r, it, ca);
     cell[i] = c;
     if (c < 0) r[0] = r[1] = r[2] = -1.f;
     for (int d = 0; d < 3; ++d) ref[3 * (size_t)i + d] = r[d];

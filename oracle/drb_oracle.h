@@ -22,12 +22,15 @@ void orc_hex_eval_d (int p, int ncomp, const double *cp, int n, const double *re
 
 /* Point location over a given BVH in the reference layout, with the
  * reference's traversal order.  use_double selects the FP64 Newton.
- * guess_mode as drb_guess_mode; guess (n*3) for mode 3.  OpenMP over points. */
+ * guess_mode as drb_guess_mode; guess (n*3) for mode 3.  local_frame != 0
+ * evaluates each candidate relative to its first control point in FP32, as
+ * the CUDA path's packed rows do (the reference uses absolute coordinates).
+ * OpenMP over points. */
 void orc_locate (int p, int n_elem, const int *ctrl_idx, const float *xyz, int n_inner,
                  const float *inner_nodes, const int *leaf_nodes, const int *aabb_ids,
                  const float *ref_boxes, int n, const float *pts, float tol, int max_steps,
-                 int guess_mode, const float *guess, int use_double, int *cell, float *ref,
-                 int *iters, int *cands);
+                 int guess_mode, const float *guess, int use_double, int local_frame,
+                 int *cell, float *ref, int *iters, int *cands);
 
 /* FP64 Newton solve of each (point, element) pair from the element centre
  * to tol 1e-13, up to 60 steps; ref_out = the FP64 solution (n*3), ok[i] = 1

@@ -29,7 +29,8 @@ def lib():
         vp = C.c_void_p
         L.orc_hex_eval_d.argtypes = [C.c_int, C.c_int, vp, C.c_int, vp, vp, vp]
         L.orc_locate.argtypes = [C.c_int, C.c_int, vp, vp, C.c_int, vp, vp, vp, vp, C.c_int, vp,
-                                 C.c_float, C.c_int, C.c_int, vp, C.c_int, vp, vp, vp, vp]
+                                 C.c_float, C.c_int, C.c_int, vp, C.c_int, C.c_int, vp, vp, vp,
+                                 vp]
         L.orc_newton_fp64.argtypes = [C.c_int, vp, vp, C.c_int, vp, vp, vp, vp]
         _lib = L
     return _lib
@@ -52,7 +53,7 @@ def hex_eval_d(p: int, cp: np.ndarray, ref: np.ndarray):
 
 
 def locate(p, ctrl_idx, xyz, bvh, pts, tol=1e-4, max_steps=20, guess_mode=0, guess=None,
-           use_double=False):
+           use_double=False, local_frame=False):
     """Restated DeviceMesh::locate over a BVH given as numpy arrays
     (inner [n_inner,16], leaf_nodes, aabb_ids, ref_boxes [n_leaf,6])."""
     ctrl_idx = np.ascontiguousarray(ctrl_idx, np.int32)
@@ -71,7 +72,7 @@ def locate(p, ctrl_idx, xyz, bvh, pts, tol=1e-4, max_steps=20, guess_mode=0, gue
     nd = (p + 1) ** 3
     lib().orc_locate(p, ctrl_idx.size // nd, _p(ctrl_idx), _p(xyz), inner.shape[0], _p(inner),
                      _p(leaf), _p(ids), _p(refb), n, _p(pts), tol, max_steps, guess_mode, _p(g),
-                     int(use_double), _p(cell), _p(ref), _p(it), _p(ca))
+                     int(use_double), int(local_frame), _p(cell), _p(ref), _p(it), _p(ca))
     return cell, ref, it, ca
 
 

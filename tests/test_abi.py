@@ -19,10 +19,13 @@ def test_host_queries():
     from devil_ray_b200 import _lib as L
     lib = L.lib()
     assert lib.drb_version() >= 1
+    # geometry rows: 3 nd relative coordinates + the 3-float origin, padded to 4
     assert lib.drb_packed_stride(3, 2, 3) == 84
-    assert lib.drb_packed_stride(3, 3, 3) == 192
+    assert lib.drb_packed_stride(3, 3, 3) == 196
+    assert lib.drb_packed_stride(3, 1, 3) == 28
     assert lib.drb_packed_stride(3, 1, 1) == 8
-    assert lib.drb_packed_stride(2, 3, 3) == 48
+    assert lib.drb_packed_stride(2, 3, 3) == 52
+    assert lib.drb_packed_stride(2, 1, 3) == 16
     assert lib.drb_packed_stride(4, 3, 3) == -1
     ni, nl = C.c_int(), C.c_int()
     assert lib.drb_bvh_sizes(3, 262144, C.byref(ni), C.byref(nl)) == 0

@@ -134,6 +134,13 @@ def test_fused_guess_matches_forward(setup):
     torch.cuda.synchronize()
     model.check_err()
     assert torch.allclose(gss, y, atol=2e-3), (gss - y).abs().max()
+    # visiting the rows in another order (as the Morton order does) changes nothing
+    perm = torch.randperm(elem.numel(), generator=torch.Generator().manual_seed(9)).to(
+        device=elem.device, dtype=torch.int32)
+    gp = model.guess(mesh, elem, pts, order=perm)
+    torch.cuda.synchronize()
+    model.check_err()
+    assert torch.equal(gp, gss)
 
 
 def test_hinted_locate_equals_plain_given_guess(cuda, setup):

@@ -103,3 +103,27 @@ def test_meshgen_shapes_and_outside_fraction():
     q = meshgen.uniform_queries(200000, 1)
     outside = np.any((q < 0) | (q > 1), axis=1).mean()
     assert abs(outside - 0.08) < 0.005
+
+
+def test_local_frame_newton_reaches_tolerance_on_fine_mesh(ref):
+    """FP32 Newton in absolute coordinates stalls near tol 1e-5 once elements
+    are small (rounding of X(r) ~ 1e-7 absolute, times 1/h in reference
+    space); evaluated relative to each element's first control point, as the
+    packed rows of the CUDA path are, it converges for every interior point."""
+    from devil_ray_b200 import meshgen
+    from oracle import restate
+    if not restate.available():
+        pytest.skip("restated oracle not built")
+    m = meshgen.warped_mesh(40, 3, 0.05, gaussian_field_seed=4)
+    b = ref.RefHexMesh(m.order, m.ctrl_idx, m.xyz, m.field).bvh()
+    q = np.random.default_rng(3).uniform(0.001, 0.999, size=(40000, 3)).astype(np.float32)
+    ca, ra, ia, _ = restate.locate(m.order, m.ctrl_idx, m.xyz, b, q, 1e-5, 20, 1)
+    cl, rl, il, _ = restate.locate(m.order, m.ctrl_idx, m.xyz, b, q, 1e-5, 20, 1,
+                                   local_frame=True)
+    assert (cl >= 0).all()
+    assert (ca < 0).sum() > 0          # the absolute form misses some
+    assert il.mean() < ia.mean()
+    both = (ca >= 0) & (ca == cl)
+    assert np.abs(ra[both] - rl[both]).max() < 1e-4
+    f64, ok = restate.newton_fp64(m.order, m.ctrl_idx, m.xyz, cl, q)
+    assert np.abs(f64[ok] - rl[ok]).max() < 1e-5
