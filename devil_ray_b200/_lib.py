@@ -34,7 +34,8 @@ class DrbBvh(C.Structure):
     _fields_ = [("n_inner", C.c_int), ("n_leaf", C.c_int),
                 ("inner_nodes", C.c_void_p), ("leaf_nodes", C.c_void_p),
                 ("aabb_ids", C.c_void_p), ("ref_boxes", C.c_void_p),
-                ("bounds", C.c_float * 6), ("cull", C.c_int)]
+                ("bounds", C.c_float * 6), ("wide_nodes", C.c_void_p), ("n_wide", C.c_int),
+                ("wide_depth", C.c_int)]
 
 
 class DrbNewtonOpts(C.Structure):
@@ -137,6 +138,7 @@ _SIGS = {
     "drb_radix_sort_pairs": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p,
                                        C.c_int, C.c_int, C.c_void_p]),
     "drb_lbvh_build": (C.c_int, [C.POINTER(DrbMesh), C.POINTER(DrbBvh), C.c_void_p, C.c_void_p]),
+    "drb_bvh_widen": (C.c_int, [C.POINTER(DrbBvh), C.c_void_p, C.c_int, C.c_void_p]),
     "drb_locate": (C.c_int, [C.POINTER(DrbMesh), C.POINTER(DrbBvh), C.c_void_p, C.c_int,
                              C.POINTER(DrbNewtonOpts), C.c_void_p, C.c_void_p, DrbQueryStats,
                              C.c_void_p]),

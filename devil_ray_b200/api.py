@@ -63,6 +63,10 @@ class BVH:
         self.ref_boxes = torch.empty((self.n_leaf, 2 * dim), dtype=torch.float32, device=device)
         self.bounds = np.zeros(6, np.float32)
         self.sorted_codes = None
+        # optional 4-wide traversal tree (drb_bvh_widen)
+        self.wide_nodes = None
+        self.n_wide = 0
+        self.wide_depth = 0
 
     def desc(self) -> L.DrbBvh:
         d = L.DrbBvh()
@@ -73,7 +77,29 @@ class BVH:
         d.ref_boxes = self.ref_boxes.data_ptr()
         for q in range(6):
             d.bounds[q] = float(self.bounds[q])
+        if self.wide_nodes is not None:
+            d.wide_nodes = self.wide_nodes.data_ptr()
+            d.n_wide, d.wide_depth = self.n_wide, self.wide_depth
         return d
+
+    def widen(self, stream=None):
+        """Build the 4-wide traversal tree of this BVH (same candidates in
+        the same order; one 128-byte node per two binary levels)."""
+        d = self.desc()
+        L.check(L.lib().drb_bvh_widen(C.byref(d), None, 0, _stream(stream)), "drb_bvh_widen")
+        self.wide_nodes = torch.empty((max(d.n_wide, 1), 32), dtype=torch.float32,
+                                      device=self.inner_nodes.device)
+        L.check(L.lib().drb_bvh_widen(C.byref(d), _ptr(self.wide_nodes), d.n_wide,
+                                      _stream(stream)), "drb_bvh_widen")
+        self.n_wide, self.wide_depth = d.n_wide, d.wide_depth
+        return self
+
+    def binary_only(self) -> "BVH":
+        """A view of the same BVH without the wide tree (the binary traversal)."""
+        b = BVH.__new__(BVH)
+        b.__dict__.update(self.__dict__)
+        b.wide_nodes, b.n_wide, b.wide_depth = None, 0, 0
+        return b
 
 
 class UnstructuredMesh:
@@ -118,9 +144,12 @@ class UnstructuredMesh:
 
     def get_bvh(self, stream=None, keep_codes: bool = False) -> BVH:
         """Lazily build the LBVH (UnstructuredMesh::get_bvh,
-        data_model/unstructured_mesh.cpp:23-31)."""
+        data_model/unstructured_mesh.cpp:23-31), and for hex meshes its
+        4-wide traversal tree."""
         if self._bvh is None:
             self._bvh = self.build_bvh(stream, keep_codes)
+            if self.dim == 3:
+                self._bvh.widen(stream)
         return self._bvh
 
     def build_bvh(self, stream=None, keep_codes: bool = False) -> BVH:
@@ -181,10 +210,15 @@ class BatchedLocator:
     queries, a global work queue, autotuned launch shape."""
 
     def __init__(self, mesh: UnstructuredMesh, tol: float = 1e-5, max_steps: int = 20,
-                 guess_mode: int = L.GUESS_ELEM_CENTER, config: L.DrbLocateConfig | None = None):
+                 guess_mode: int = L.GUESS_ELEM_CENTER, config: L.DrbLocateConfig | None = None,
+                 bvh: BVH | None = None):
         self.mesh = mesh
         self.tol, self.max_steps, self.guess_mode = tol, max_steps, guess_mode
         self.config = config
+        self.bvh = bvh  # None: the mesh's own BVH (with its wide tree)
+
+    def _bvh(self, stream=None) -> BVH:
+        return self.bvh if self.bvh is not None else self.mesh.get_bvh(stream)
 
     def tune(self, sample_points, stream=None):
         pts = _dev(sample_points, torch.float32, self.mesh.device).reshape(-1, 3)
@@ -192,7 +226,7 @@ class BatchedLocator:
         ms = C.c_float()
         opts = L.DrbNewtonOpts(self.tol, self.max_steps, self.guess_mode, None)
         d = self.mesh.desc()
-        bd = self.mesh.get_bvh(stream).desc()
+        bd = self._bvh(stream).desc()
         L.check(L.lib().drb_locate_tune(C.byref(d), C.byref(bd), _ptr(pts), pts.shape[0],
                                         C.byref(opts), C.byref(best), C.byref(ms),
                                         _stream(stream)), "drb_locate_tune")
@@ -202,7 +236,7 @@ class BatchedLocator:
     def order(self, points, stream=None):
         pts = _dev(points, torch.float32, self.mesh.device).reshape(-1, 3)
         o = torch.empty(pts.shape[0], dtype=torch.int32, device=self.mesh.device)
-        bd = self.mesh.get_bvh(stream).desc()
+        bd = self._bvh(stream).desc()
         L.check(L.lib().drb_query_order(C.byref(bd), _ptr(pts), pts.shape[0], _ptr(o),
                                         _stream(stream)), "drb_query_order")
         return o
@@ -220,7 +254,7 @@ class BatchedLocator:
                                None if guess is None else guess.data_ptr())
         cfg = None if self.config is None else C.byref(self.config)
         d = self.mesh.desc()
-        bd = self.mesh.get_bvh(stream).desc()
+        bd = self._bvh(stream).desc()
         if order is None:
             L.check(L.lib().drb_locate_batched(C.byref(d), C.byref(bd), _ptr(pts), n,
                                                C.byref(opts), cfg, _ptr(cell), _ptr(ref), qs,

@@ -58,7 +58,7 @@ struct DeviceGeometry
   DevBuf<float> packed;
   bool has_bvh = false;
   drb_bvh bvh{};
-  DevBuf<float> inner, refb;
+  DevBuf<float> inner, refb, wide;
   DevBuf<int32> leaf, ids;
 };
 
@@ -115,6 +115,13 @@ const drb_bvh *TensorMesh::device_bvh ()
     g.bvh.aabb_ids = g.ids.p;
     g.bvh.ref_boxes = g.refb.p;
     drb_check (drb_lbvh_build (&g.mesh, &g.bvh, nullptr, nullptr), "drb_lbvh_build");
+    if (m_dim == 3)
+    {
+      // 4-wide traversal tree for the batched locate and the volume march
+      drb_check (drb_bvh_widen (&g.bvh, nullptr, 0, nullptr), "drb_bvh_widen");
+      g.wide.alloc ((size_t)32 * g.bvh.n_wide);
+      drb_check (drb_bvh_widen (&g.bvh, g.wide.p, g.bvh.n_wide, nullptr), "drb_bvh_widen");
+    }
     g.has_bvh = true;
   }
   return &g.bvh;

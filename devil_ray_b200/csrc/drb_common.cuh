@@ -24,6 +24,10 @@ namespace drb
 constexpr int kWarp = 32;
 constexpr int kStackDepth = 64;          // device_mesh.hpp:255 (int32 todo[64])
 constexpr int kBarrier = -2000000000;     // device_mesh.hpp:259
+// 4-wide traversal (drb_bvh_widen): stack bound 3 per wide level, checked
+// against the tree depth when the wide tree is built; empty child slot code
+constexpr int kWideStack = 96;
+constexpr int kWideEmpty = (int)0x80000000;
 constexpr float kEpsilon = 1e-4f;         // math.hpp:25 DRAY_EPSILON_32
 
 struct Vec3

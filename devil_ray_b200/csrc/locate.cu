@@ -68,6 +68,7 @@ extern "C" int drb_locate (const drb_mesh *mesh, const drb_bvh *bvh, const float
   if (n == 0) return DRB_OK;
   LocateParams lp;
   lp.nodes = (const float4 *)bvh->inner_nodes;
+  lp.wide = nullptr; // the reference's binary traversal
   lp.leaf_nodes = bvh->leaf_nodes;
   lp.aabb_ids = bvh->aabb_ids;
   lp.ref_boxes = bvh->ref_boxes;

@@ -36,9 +36,93 @@ DRB_D void node_point_test_kids (const float4 *__restrict__ nodes, int node, con
   r = __float_as_int (d.y);
 }
 
+// The four child boxes of a wide node (drb_bvh_widen) against a point, with
+// the binary node test's comparisons: bit c set when child c holds p.
+DRB_D unsigned wide_node_test (const float4 *__restrict__ wide, int w, const float (&p)[3],
+                               int4 &kids)
+{
+  const float4 *q = wide + 8 * (size_t)w;
+  const float4 lx = __ldg (q), ly = __ldg (q + 1), lz = __ldg (q + 2);
+  const float4 hx = __ldg (q + 3), hy = __ldg (q + 4), hz = __ldg (q + 5);
+  const float4 kk = __ldg (q + 6);
+  kids = make_int4 (__float_as_int (kk.x), __float_as_int (kk.y), __float_as_int (kk.z),
+                    __float_as_int (kk.w));
+  unsigned m = 0u;
+  m |= !(p[0] < lx.x || p[1] < ly.x || p[2] < lz.x || p[0] > hx.x || p[1] > hy.x || p[2] > hz.x) ? 1u : 0u;
+  m |= !(p[0] < lx.y || p[1] < ly.y || p[2] < lz.y || p[0] > hx.y || p[1] > hy.y || p[2] > hz.y) ? 2u : 0u;
+  m |= !(p[0] < lx.z || p[1] < ly.z || p[2] < lz.z || p[0] > hx.z || p[1] > hy.z || p[2] > hz.z) ? 4u : 0u;
+  m |= !(p[0] < lx.w || p[1] < ly.w || p[2] < lz.w || p[0] > hx.w || p[1] > hy.w || p[2] > hz.w) ? 8u : 0u;
+  return m;
+}
+
+template <bool WIDE> struct TraversalStack
+{
+  static constexpr int kDepth = WIDE ? kWideStack : kStackDepth;
+};
+
+// Advance a traversal to its next candidate leaf (left-first DFS, as
+// device_mesh.hpp:262-318): returns the leaf, or -1 when the tree is
+// exhausted.  After a candidate the caller resumes with cur = todo[sp--].
+// WIDE walks the 4-wide tree (lowest hit child first, the other hits
+// pushed highest first), else the binary nodes.
+template <bool WIDE>
+DRB_D int next_leaf (const float4 *__restrict__ nodes, const float4 *__restrict__ wide,
+                     const float (&pt)[3], int (&todo)[TraversalStack<WIDE>::kDepth], int &sp,
+                     int &cur, int &visited)
+{
+  constexpr int D = TraversalStack<WIDE>::kDepth;
+  while (cur != kBarrier)
+  {
+    if (cur > -1)
+    {
+      ++visited;
+      if (WIDE)
+      {
+        int4 k;
+        const unsigned m = wide_node_test (wide, cur, pt, k);
+        if (m == 0u)
+        {
+          cur = todo[sp];
+          --sp;
+        }
+        else
+        {
+          const int f = __ffs (m) - 1;
+          if ((m & 8u) && f != 3 && sp < D - 1) todo[++sp] = k.w;
+          if ((m & 4u) && f != 2 && sp < D - 1) todo[++sp] = k.z;
+          if ((m & 2u) && f != 1 && sp < D - 1) todo[++sp] = k.y;
+          cur = f == 0 ? k.x : f == 1 ? k.y : f == 2 ? k.z : k.w;
+        }
+      }
+      else
+      {
+        bool in_l, in_r;
+        int l, r;
+        node_point_test_kids (nodes, cur, pt, in_l, in_r, l, r);
+        if (!in_l && !in_r)
+        {
+          cur = todo[sp];
+          --sp;
+        }
+        else
+        {
+          cur = in_l ? l : r;
+          if (in_l && in_r && sp < D - 1) todo[++sp] = r;
+        }
+      }
+    }
+    else
+    {
+      return -cur - 1;
+    }
+  }
+  return -1;
+}
+
 struct LocateParams
 {
   const float4 *nodes;
+  const float4 *wide = nullptr; // 4-wide tree or NULL
   const int *leaf_nodes;
   const int *aabb_ids;
   const float *ref_boxes;
@@ -56,7 +140,7 @@ struct LocateParams
 // L1-read control points by order.
 template <int P, bool REG = (P <= 2)>
 DRB_D bool solve_in_element (const LocateParams &lp, int el, const float (&pt)[3], float (&x)[3],
-                             int &steps)
+                             int &steps, LU3 &lu)
 {
   constexpr int ND = (P + 1) * (P + 1) * (P + 1);
   if (lp.packed)
@@ -69,13 +153,21 @@ DRB_D bool solve_in_element (const LocateParams &lp, int el, const float (&pt)[3
     {
       RegCP<3 * ND> r;
       load_reg_cp<P> (r, row);
-      return hex_newton<P> (r, t, x, lp.tol, lp.max_steps, steps);
+      return hex_newton<P> (r, t, x, lp.tol, lp.max_steps, steps, lu);
     }
     PackedCP cp{ row };
-    return hex_newton<P> (cp, t, x, lp.tol, lp.max_steps, steps);
+    return hex_newton<P> (cp, t, x, lp.tol, lp.max_steps, steps, lu);
   }
   IndirectCP cp{ lp.ctrl_idx + (size_t)el * ND, lp.xyz, 3 };
-  return hex_newton<P> (cp, pt, x, lp.tol, lp.max_steps, steps);
+  return hex_newton<P> (cp, pt, x, lp.tol, lp.max_steps, steps, lu);
+}
+
+template <int P, bool REG = (P <= 2)>
+DRB_D bool solve_in_element (const LocateParams &lp, int el, const float (&pt)[3], float (&x)[3],
+                             int &steps)
+{
+  LU3 lu;
+  return solve_in_element<P, REG> (lp, el, pt, x, steps, lu);
 }
 
 // Initial guess of a candidate leaf's Newton solve (drb_guess_mode).
@@ -109,79 +201,71 @@ DRB_D void candidate_guess (const LocateParams &lp, int leaf, long long qi, bool
 // guess that does not converge is retried from the element centre.
 template <int P, bool REG = (P <= 2)>
 DRB_D bool solve_candidate (const LocateParams &lp, int leaf, int el, long long qi, bool first,
-                            const float (&pt)[3], float (&x)[3], int &iters)
+                            const float (&pt)[3], float (&x)[3], int &iters, LU3 &lu)
 {
   bool given;
   candidate_guess (lp, leaf, qi, first, x, given);
   int steps = 0;
-  bool found = solve_in_element<P, REG> (lp, el, pt, x, steps);
+  bool found = solve_in_element<P, REG> (lp, el, pt, x, steps, lu);
   iters += steps;
   if (!found && given)
   {
     x[0] = x[1] = x[2] = 0.5f;
-    found = solve_in_element<P, REG> (lp, el, pt, x, steps);
+    found = solve_in_element<P, REG> (lp, el, pt, x, steps, lu);
     iters += steps;
   }
   return found;
 }
 
+template <int P, bool REG = (P <= 2)>
+DRB_D bool solve_candidate (const LocateParams &lp, int leaf, int el, long long qi, bool first,
+                            const float (&pt)[3], float (&x)[3], int &iters)
+{
+  LU3 lu;
+  return solve_candidate<P, REG> (lp, leaf, el, qi, first, pt, x, iters, lu);
+}
+
 // Full point location of one query (DeviceMesh::locate, device_mesh.hpp:248-354):
 // traversal left child first, first converged+inside candidate wins.
-template <int P>
+template <int P, bool WIDE = false>
 DRB_D int locate_point (const LocateParams &lp, int qi, const float (&pt)[3], float (&out_ref)[3],
-                        int &iters, int &cands, int &nodes)
+                        int &iters, int &cands, int &nodes, LU3 &lu)
 {
-  int todo[kStackDepth];
+  // depth is bounded by the tree height; the binary stack of 64 covers 2^63
+  // leaves of a balanced tree and the reference uses the same fixed stack
+  int todo[TraversalStack<WIDE>::kDepth];
   int current = 0;
   int sp = 0;
   todo[sp] = kBarrier;
   bool first_candidate = true;
-  while (current != kBarrier)
+  while (true)
   {
-    if (current > -1)
+    const int leaf = next_leaf<WIDE> (lp.nodes, lp.wide, pt, todo, sp, current, nodes);
+    if (leaf < 0) break;
+    const int el = __ldg (lp.leaf_nodes + leaf);
+    ++cands;
+    float x[3];
+    const bool found = solve_candidate<P> (lp, leaf, el, qi, first_candidate, pt, x, iters, lu);
+    first_candidate = false;
+    if (found)
     {
-      bool in_l, in_r;
-      ++nodes;
-      node_point_test (lp.nodes, current, pt, in_l, in_r);
-      if (!in_l && !in_r)
-      {
-        current = todo[sp];
-        --sp;
-      }
-      else
-      {
-        const float4 ch = __ldg (lp.nodes + current + 3);
-        const int l = __float_as_int (ch.x);
-        const int r = __float_as_int (ch.y);
-        current = in_l ? l : r;
-        if (in_l && in_r)
-        {
-          // depth is bounded by the tree height; 64 covers 2^63 leaves of a
-          // balanced tree and the reference uses the same fixed stack
-          if (sp < kStackDepth - 1) todo[++sp] = r;
-        }
-      }
+      out_ref[0] = x[0];
+      out_ref[1] = x[1];
+      out_ref[2] = x[2];
+      return el;
     }
-    else
-    {
-      const int leaf = -current - 1;
-      const int el = __ldg (lp.leaf_nodes + leaf);
-      ++cands;
-      float x[3];
-      const bool found = solve_candidate<P> (lp, leaf, el, qi, first_candidate, pt, x, iters);
-      first_candidate = false;
-      if (found)
-      {
-        out_ref[0] = x[0];
-        out_ref[1] = x[1];
-        out_ref[2] = x[2];
-        return el;
-      }
-      current = todo[sp];
-      --sp;
-    }
+    current = todo[sp];
+    --sp;
   }
   return -1;
+}
+
+template <int P, bool WIDE = false>
+DRB_D int locate_point (const LocateParams &lp, int qi, const float (&pt)[3], float (&out_ref)[3],
+                        int &iters, int &cands, int &nodes)
+{
+  LU3 lu;
+  return locate_point<P, WIDE> (lp, qi, pt, out_ref, iters, cands, nodes, lu);
 }
 
 } // namespace drb

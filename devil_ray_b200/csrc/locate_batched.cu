@@ -56,7 +56,7 @@ __global__ void query_codes_kernel (const float *__restrict__ pts, int n, float 
   iota[i] = i;
 }
 
-template <int P, bool REG>
+template <int P, bool REG, bool WIDE>
 __global__ void locate_persistent_kernel (LocateParams lp, const float *__restrict__ pts,
                                           const int *__restrict__ order, int n, int chunk,
                                           int *__restrict__ queue_head, int *__restrict__ cell,
@@ -70,7 +70,7 @@ __global__ void locate_persistent_kernel (LocateParams lp, const float *__restri
   bool exhausted = false;          // warp-uniform
   int qi = -1;
   float pt[3] = { 0.f, 0.f, 0.f };
-  int todo[kStackDepth];
+  int todo[TraversalStack<WIDE>::kDepth];
   int sp = 0, cur = kBarrier;
   int iters = 0, cands = 0, nodes = 0;
   bool first = true;
@@ -116,34 +116,7 @@ __global__ void locate_persistent_kernel (LocateParams lp, const float *__restri
 
     // ---- traversal phase: advance to the next candidate leaf ----
     int leaf = -1;
-    if (qi >= 0)
-    {
-      while (cur != kBarrier)
-      {
-        if (cur > -1)
-        {
-          bool in_l, in_r;
-          int l, r;
-          ++nodes;
-          node_point_test_kids (lp.nodes, cur, pt, in_l, in_r, l, r);
-          if (!in_l && !in_r)
-          {
-            cur = todo[sp];
-            --sp;
-          }
-          else
-          {
-            cur = in_l ? l : r;
-            if (in_l && in_r && sp < kStackDepth - 1) todo[++sp] = r;
-          }
-        }
-        else
-        {
-          leaf = -cur - 1;
-          break;
-        }
-      }
-    }
+    if (qi >= 0) leaf = next_leaf<WIDE> (lp.nodes, lp.wide, pt, todo, sp, cur, nodes);
 
     // ---- candidate phase: converged Newton solves ----
     if (qi >= 0)
@@ -188,29 +161,43 @@ __global__ void locate_persistent_kernel (LocateParams lp, const float *__restri
   }
 }
 
-const void *persistent_fn (int order, bool reg)
+template <bool W> const void *persistent_fn_w (int order, bool reg)
 {
-  if (order == 1) return reg ? (const void *)locate_persistent_kernel<1, true> : (const void *)locate_persistent_kernel<1, false>;
-  if (order == 2) return reg ? (const void *)locate_persistent_kernel<2, true> : (const void *)locate_persistent_kernel<2, false>;
-  return (const void *)locate_persistent_kernel<3, false>;
+  if (order == 1) return reg ? (const void *)locate_persistent_kernel<1, true, W> : (const void *)locate_persistent_kernel<1, false, W>;
+  if (order == 2) return reg ? (const void *)locate_persistent_kernel<2, true, W> : (const void *)locate_persistent_kernel<2, false, W>;
+  return (const void *)locate_persistent_kernel<3, false, W>;
+}
+
+const void *persistent_fn (int order, bool reg, bool wide)
+{
+  return wide ? persistent_fn_w<true> (order, reg) : persistent_fn_w<false> (order, reg);
 }
 
 int launch_persistent (int order, bool reg, dim3 grid, int block, cudaStream_t s,
                        const LocateParams &lp, const float *pts, const int *ord, int n, int chunk,
                        int *head, int *cell, float *ref, drb_query_stats st)
 {
-#define DRB_LP(P, R) locate_persistent_kernel<P, R><<<grid, block, 0, s>>> (lp, pts, ord, n, chunk, head, cell, ref, st.iters, st.candidates, st.nodes)
-  if (order == 1) { if (reg) DRB_LP (1, true); else DRB_LP (1, false); }
-  else if (order == 2) { if (reg) DRB_LP (2, true); else DRB_LP (2, false); }
-  else DRB_LP (3, false);
+#define DRB_LP(P, R, W) locate_persistent_kernel<P, R, W><<<grid, block, 0, s>>> (lp, pts, ord, n, chunk, head, cell, ref, st.iters, st.candidates, st.nodes)
+  if (lp.wide)
+  {
+    if (order == 1) { if (reg) DRB_LP (1, true, true); else DRB_LP (1, false, true); }
+    else if (order == 2) { if (reg) DRB_LP (2, true, true); else DRB_LP (2, false, true); }
+    else DRB_LP (3, false, true);
+  }
+  else
+  {
+    if (order == 1) { if (reg) DRB_LP (1, true, false); else DRB_LP (1, false, false); }
+    else if (order == 2) { if (reg) DRB_LP (2, true, false); else DRB_LP (2, false, false); }
+    else DRB_LP (3, false, false);
+  }
 #undef DRB_LP
   return check_launch ("locate_persistent_kernel");
 }
 
-int resident_blocks (int order, bool reg, int block)
+int resident_blocks (int order, bool reg, bool wide, int block)
 {
   int nb = 0;
-  cudaOccupancyMaxActiveBlocksPerMultiprocessor (&nb, persistent_fn (order, reg), block, 0);
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor (&nb, persistent_fn (order, reg, wide), block, 0);
   return nb > 0 ? nb : 1;
 }
 
@@ -218,6 +205,7 @@ LocateParams make_params (const drb_mesh *mesh, const drb_bvh *bvh, const drb_ne
 {
   LocateParams lp;
   lp.nodes = (const float4 *)bvh->inner_nodes;
+  lp.wide = (const float4 *)bvh->wide_nodes;
   lp.leaf_nodes = bvh->leaf_nodes;
   lp.aabb_ids = bvh->aabb_ids;
   lp.ref_boxes = bvh->ref_boxes;
@@ -324,7 +312,7 @@ int locate_batched_impl (const drb_mesh *mesh, const drb_bvh *bvh, const float *
   if (scr.err != cudaSuccess) return status_from (scr.err);
   cudaMemsetAsync (head, 0, sizeof (int), s);
   const bool reg = cfg.reg_elements != 0;
-  const int per_sm = resident_blocks (mesh->order, reg, cfg.block);
+  const int per_sm = resident_blocks (mesh->order, reg, bvh->wide_nodes != nullptr, cfg.block);
   const int bps = (cfg.blocks_per_sm > 0) ? min (cfg.blocks_per_sm, per_sm) : per_sm;
   const long long warps_needed = ((long long)n + 31) / 32;
   long long blocks = (long long)bps * sm_count ();
@@ -374,7 +362,7 @@ int locate_batched_ws (const drb_mesh *mesh, const drb_bvh *bvh, const float *pt
   cudaError_t e = cudaMemsetAsync (ws.head, 0, sizeof (int), s);
   if (e != cudaSuccess) return status_from (e);
   const bool reg = cfg.reg_elements != 0;
-  const int per_sm = resident_blocks (mesh->order, reg, cfg.block);
+  const int per_sm = resident_blocks (mesh->order, reg, bvh->wide_nodes != nullptr, cfg.block);
   const int bps = (cfg.blocks_per_sm > 0) ? min (cfg.blocks_per_sm, per_sm) : per_sm;
   const long long warps_needed = ((long long)n + 31) / 32;
   long long blocks = (long long)bps * sm_count ();

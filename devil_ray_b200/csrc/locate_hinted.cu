@@ -20,45 +20,9 @@ namespace drb
 namespace
 {
 
-DRB_D int traverse_to_leaf (const float4 *__restrict__ nodes, const float (&pt)[3], int (&todo)[kStackDepth],
-                            int &sp, int &cur, int skip_leaf, int &nodes_visited)
-{
-  while (cur != kBarrier)
-  {
-    if (cur > -1)
-    {
-      bool in_l, in_r;
-      int l, r;
-      ++nodes_visited;
-      node_point_test_kids (nodes, cur, pt, in_l, in_r, l, r);
-      if (!in_l && !in_r)
-      {
-        cur = todo[sp];
-        --sp;
-      }
-      else
-      {
-        cur = in_l ? l : r;
-        if (in_l && in_r && sp < kStackDepth - 1) todo[++sp] = r;
-      }
-    }
-    else
-    {
-      const int leaf = -cur - 1;
-      if (leaf == skip_leaf)
-      {
-        skip_leaf = -1;
-        cur = todo[sp];
-        --sp;
-        continue;
-      }
-      return leaf;
-    }
-  }
-  return -1;
-}
-
-__global__ void first_candidate_kernel (const float4 *__restrict__ nodes, const int *__restrict__ leaf_nodes,
+template <bool WIDE>
+__global__ void first_candidate_kernel (const float4 *__restrict__ nodes, const float4 *__restrict__ wide,
+                                        const int *__restrict__ leaf_nodes,
                                         const float *__restrict__ pts, const int *__restrict__ order,
                                         int n, int *__restrict__ first_leaf, int *__restrict__ first_elem)
 {
@@ -66,15 +30,15 @@ __global__ void first_candidate_kernel (const float4 *__restrict__ nodes, const 
   if (pos >= n) return;
   const int qi = order ? order[pos] : pos;
   const float pt[3] = { pts[3 * (size_t)qi], pts[3 * (size_t)qi + 1], pts[3 * (size_t)qi + 2] };
-  int todo[kStackDepth];
+  int todo[TraversalStack<WIDE>::kDepth];
   int sp = 0, cur = 0, visited = 0;
   todo[0] = kBarrier;
-  const int leaf = traverse_to_leaf (nodes, pt, todo, sp, cur, -1, visited);
+  const int leaf = next_leaf<WIDE> (nodes, wide, pt, todo, sp, cur, visited);
   first_leaf[qi] = leaf;
   if (first_elem) first_elem[qi] = leaf >= 0 ? __ldg (leaf_nodes + leaf) : -1;
 }
 
-template <int P, bool REG>
+template <int P, bool REG, bool WIDE>
 __global__ void locate_hinted_kernel (LocateParams lp, const float *__restrict__ pts,
                                       const int *__restrict__ order, const int *__restrict__ hint,
                                       int n, int chunk, int *__restrict__ queue_head,
@@ -89,7 +53,7 @@ __global__ void locate_hinted_kernel (LocateParams lp, const float *__restrict__
   bool exhausted = false;
   int qi = -1;
   float pt[3] = { 0.f, 0.f, 0.f };
-  int todo[kStackDepth];
+  int todo[TraversalStack<WIDE>::kDepth];
   int sp = 0, cur = kBarrier, skip = -1;
   int iters = 0, cands = 0, nodes = 0;
   int pending = -1; // leaf to solve next (the hinted first candidate)
@@ -147,7 +111,13 @@ __global__ void locate_hinted_kernel (LocateParams lp, const float *__restrict__
       else
       {
         // the first leaf met from the root is the hinted one: skip it once
-        leaf = traverse_to_leaf (lp.nodes, pt, todo, sp, cur, skip, nodes);
+        leaf = next_leaf<WIDE> (lp.nodes, lp.wide, pt, todo, sp, cur, nodes);
+        if (leaf >= 0 && leaf == skip)
+        {
+          cur = todo[sp];
+          --sp;
+          leaf = next_leaf<WIDE> (lp.nodes, lp.wide, pt, todo, sp, cur, nodes);
+        }
         skip = -1;
       }
     }
@@ -207,8 +177,14 @@ extern "C" int drb_first_candidates (const drb_bvh *bvh, const float *pts, int n
     return DRB_ERR_INVALID_ARG;
   }
   if (n == 0) return DRB_OK;
-  first_candidate_kernel<<<div_up (n, 128), 128, 0, (cudaStream_t)stream>>> (
-  (const float4 *)bvh->inner_nodes, bvh->leaf_nodes, pts, order, n, first_leaf, first_elem);
+  if (bvh->wide_nodes)
+    first_candidate_kernel<true><<<div_up (n, 128), 128, 0, (cudaStream_t)stream>>> (
+    (const float4 *)bvh->inner_nodes, (const float4 *)bvh->wide_nodes, bvh->leaf_nodes, pts, order,
+    n, first_leaf, first_elem);
+  else
+    first_candidate_kernel<false><<<div_up (n, 128), 128, 0, (cudaStream_t)stream>>> (
+    (const float4 *)bvh->inner_nodes, nullptr, bvh->leaf_nodes, pts, order, n, first_leaf,
+    first_elem);
   return check_launch ("first_candidate_kernel");
 }
 
@@ -255,6 +231,7 @@ extern "C" int drb_locate_hinted (const drb_mesh *mesh, const drb_bvh *bvh, cons
   cudaMemsetAsync (head, 0, sizeof (int), s);
   LocateParams lp;
   lp.nodes = (const float4 *)bvh->inner_nodes;
+  lp.wide = (const float4 *)bvh->wide_nodes;
   lp.leaf_nodes = bvh->leaf_nodes;
   lp.aabb_ids = bvh->aabb_ids;
   lp.ref_boxes = bvh->ref_boxes;
@@ -268,9 +245,12 @@ extern "C" int drb_locate_hinted (const drb_mesh *mesh, const drb_bvh *bvh, cons
   lp.guess = opts->guess;
   int nb = 0;
   const bool reg = cfg.reg_elements != 0 && mesh->order <= 2;
-  const void *fn = mesh->order == 1 ? (reg ? (const void *)locate_hinted_kernel<1, true> : (const void *)locate_hinted_kernel<1, false>)
-                   : mesh->order == 2 ? (reg ? (const void *)locate_hinted_kernel<2, true> : (const void *)locate_hinted_kernel<2, false>)
-                                      : (const void *)locate_hinted_kernel<3, false>;
+  const bool wide = lp.wide != nullptr;
+#define DRB_HFN(W) (mesh->order == 1 ? (reg ? (const void *)locate_hinted_kernel<1, true, W> : (const void *)locate_hinted_kernel<1, false, W>) \
+                   : mesh->order == 2 ? (reg ? (const void *)locate_hinted_kernel<2, true, W> : (const void *)locate_hinted_kernel<2, false, W>) \
+                                      : (const void *)locate_hinted_kernel<3, false, W>)
+  const void *fn = wide ? DRB_HFN (true) : DRB_HFN (false);
+#undef DRB_HFN
   cudaOccupancyMaxActiveBlocksPerMultiprocessor (&nb, fn, cfg.block, 0);
   if (nb < 1) nb = 1;
   const int bps = cfg.blocks_per_sm > 0 ? min (cfg.blocks_per_sm, nb) : nb;
@@ -278,14 +258,23 @@ extern "C" int drb_locate_hinted (const drb_mesh *mesh, const drb_bvh *bvh, cons
   const long long need = ((long long)n + cfg.block - 1) / cfg.block;
   if (blocks > need) blocks = need;
   if (blocks < 1) blocks = 1;
-#define DRB_HINT(P, R)                                                                              \
-  locate_hinted_kernel<P, R><<<(unsigned)blocks, cfg.block, 0, s>>> (lp, pts, order, first_leaf, n, \
-                                                                     cfg.chunk, head, cell, ref,    \
-                                                                     stats.iters, stats.candidates, \
-                                                                     stats.nodes)
-  if (mesh->order == 1) { if (reg) DRB_HINT (1, true); else DRB_HINT (1, false); }
-  else if (mesh->order == 2) { if (reg) DRB_HINT (2, true); else DRB_HINT (2, false); }
-  else DRB_HINT (3, false);
+#define DRB_HINT(P, R, W)                                                                              \
+  locate_hinted_kernel<P, R, W><<<(unsigned)blocks, cfg.block, 0, s>>> (lp, pts, order, first_leaf, n, \
+                                                                        cfg.chunk, head, cell, ref,    \
+                                                                        stats.iters, stats.candidates, \
+                                                                        stats.nodes)
+  if (wide)
+  {
+    if (mesh->order == 1) { if (reg) DRB_HINT (1, true, true); else DRB_HINT (1, false, true); }
+    else if (mesh->order == 2) { if (reg) DRB_HINT (2, true, true); else DRB_HINT (2, false, true); }
+    else DRB_HINT (3, false, true);
+  }
+  else
+  {
+    if (mesh->order == 1) { if (reg) DRB_HINT (1, true, false); else DRB_HINT (1, false, false); }
+    else if (mesh->order == 2) { if (reg) DRB_HINT (2, true, false); else DRB_HINT (2, false, false); }
+    else DRB_HINT (3, false, false);
+  }
 #undef DRB_HINT
   return check_launch ("locate_hinted_kernel");
 }

@@ -39,9 +39,13 @@ DRB_D float norm_linf3 (float a, float b, float c)
   return m;
 }
 
+// lu receives the factorised Jacobian of the last step, taken within tol
+// (in reference space) of the returned x when the solve converged: the
+// volume renderer reuses it for the world-space gradient and for the next
+// sample's predictor instead of evaluating the geometry again.
 template <int P, class CP>
 DRB_D bool hex_newton (const CP &cp, const float (&target)[3], float (&x)[3], float tol,
-                       int max_steps, int &steps)
+                       int max_steps, int &steps, LU3 &lu)
 {
   float prev[3] = { x[0], x[1], x[2] };
   bool converged = false;
@@ -61,7 +65,6 @@ DRB_D bool hex_newton (const CP &cp, const float (&target)[3], float (&x)[3], fl
       J[r][1] = Jv[r];
       J[r][2] = Jw[r];
     }
-    LU3 lu;
     lu.factor (J);
     lu.solve (dy, dx);
 #pragma unroll
@@ -73,6 +76,14 @@ DRB_D bool hex_newton (const CP &cp, const float (&target)[3], float (&x)[3], fl
     for (int d = 0; d < 3; ++d) prev[d] = x[d];
   }
   return converged && is_inside_ref (x, tol);
+}
+
+template <int P, class CP>
+DRB_D bool hex_newton (const CP &cp, const float (&target)[3], float (&x)[3], float tol,
+                       int max_steps, int &steps)
+{
+  LU3 lu;
+  return hex_newton<P> (cp, target, x, tol, max_steps, steps, lu);
 }
 
 // Control points of one element read through the packed element-major copy.

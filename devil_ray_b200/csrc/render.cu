@@ -319,9 +319,13 @@ DRB_D void field_eval_d (const VolumeParams &vp, int el, const float (&r)[3], fl
   g[2] = Jw[0];
 }
 
-// VolumeShader::color / shaded_color (volume_shader.hpp:40-167)
+// VolumeShader::color / shaded_color (volume_shader.hpp:40-167).  The
+// geometry Jacobian is not evaluated again: lu is the factorised Jacobian of
+// the located sample's last Newton step, taken within tol of ref, and the
+// world position is the sample point itself (the solve's target).
 template <int P>
-DRB_D float4 shade_sample (const VolumeParams &vp, int el, const float (&r)[3], const Ray &ray)
+DRB_D float4 shade_sample (const VolumeParams &vp, int el, const float (&r)[3], const Ray &ray,
+                           const LU3 &lu, const float (&wpos)[3])
 {
   float f, gref[3];
   field_eval_d<P> (vp, el, r, f, gref);
@@ -329,32 +333,7 @@ DRB_D float4 shade_sample (const VolumeParams &vp, int el, const float (&r)[3], 
   if (!vp.use_lighting) return c;
   float4 acc = make_float4 (0.f, 0.f, 0.f, 0.f);
   if (!(c.w > 0.01f)) return acc;
-  // world position and Jacobian of the geometry
-  constexpr int ND = (P + 1) * (P + 1) * (P + 1);
-  float X[3], Ju[3], Jv[3], Jw[3];
-  if (vp.lp.packed)
-  {
-    const float *row = vp.lp.packed + (size_t)el * vp.lp.stride;
-    PackedCP cp{ row };
-    hex_eval_d<P, 3> (cp, r[0], r[1], r[2], X, Ju, Jv, Jw);
-    to_world<ND> (row, X);
-  }
-  else
-  {
-    IndirectCP cp{ vp.lp.ctrl_idx + (size_t)el * ND, vp.lp.xyz, 3 };
-    hex_eval_d<P, 3> (cp, r[0], r[1], r[2], X, Ju, Jv, Jw);
-  }
-  float J[3][3];
-#pragma unroll
-  for (int k = 0; k < 3; ++k)
-  {
-    J[k][0] = Ju[k];
-    J[k][1] = Jv[k];
-    J[k][2] = Jw[k];
-  }
   // matrix_inverse via LUP (matrix.hpp:430-456); gradient = gref * J^-1
-  LU3 lu;
-  lu.factor (J);
   float inv[3][3];
 #pragma unroll
   for (int c = 0; c < 3; ++c)
@@ -375,7 +354,7 @@ DRB_D float4 shade_sample (const VolumeParams &vp, int el, const float (&r)[3], 
     g = make3 (g.x / m, g.y / m, g.z / m);
   }
   const Vec3 view = make3 (-ray.dir.x, -ray.dir.y, -ray.dir.z);
-  const Vec3 wp = make3 (X[0], X[1], X[2]);
+  const Vec3 wp = make3 (wpos[0], wpos[1], wpos[2]);
   for (int l = 0; l < vp.n_lights; ++l)
   {
     const PointLight L = vp.lights[l];
@@ -417,32 +396,44 @@ DRB_D void blend (float4 &front, const float4 &back)
   front.w = alpha + front.w;
 }
 
-// Locate one sample: coherent first try in the previous element, then the
-// full BVH locate (same acceptance rule either way).
-template <int P>
-DRB_D int locate_sample (const VolumeParams &vp, const float (&pt)[3], int prev_el,
-                         const float (&prev_ref)[3], float (&ref)[3], int &iters, int &cands,
-                         int &nodes)
+// A predicted reference point this far outside [0,1]^3 means the sample
+// has left the previous element: go straight to the BVH.
+constexpr float kCoherentMargin = 0.1f;
+
+// Locate one sample.  Coherent mode first tries the previous sample's
+// element, starting from a predictor step r_prev + J^-1 (pt - pt_prev) with
+// the previous solve's Jacobian (lu), so that the solve usually converges in
+// two steps; then, or in plain mode, the full BVH locate (same acceptance
+// rule either way).  On success lu holds the located solve's Jacobian.
+template <int P, bool WIDE>
+DRB_D int locate_sample (const VolumeParams &vp, const float (&pt)[3], const float (&step)[3],
+                         int prev_el, const float (&prev_ref)[3], LU3 &lu, float (&ref)[3],
+                         int &iters, int &cands, int &nodes)
 {
   if (vp.coherent && prev_el >= 0)
   {
-    float x[3] = { prev_ref[0], prev_ref[1], prev_ref[2] };
-    int steps = 0;
-    ++cands;
-    const bool found = solve_in_element<P> (vp.lp, prev_el, pt, x, steps);
-    iters += steps;
-    if (found)
+    float dr[3];
+    lu.solve (step, dr);
+    float x[3] = { prev_ref[0] + dr[0], prev_ref[1] + dr[1], prev_ref[2] + dr[2] };
+    if (is_inside_ref (x, kCoherentMargin))
     {
-      ref[0] = x[0];
-      ref[1] = x[1];
-      ref[2] = x[2];
-      return prev_el;
+      int steps = 0;
+      ++cands;
+      const bool found = solve_in_element<P> (vp.lp, prev_el, pt, x, steps, lu);
+      iters += steps;
+      if (found)
+      {
+        ref[0] = x[0];
+        ref[1] = x[1];
+        ref[2] = x[2];
+        return prev_el;
+      }
     }
   }
-  return locate_point<P> (vp.lp, 0, pt, ref, iters, cands, nodes);
+  return locate_point<P, WIDE> (vp.lp, 0, pt, ref, iters, cands, nodes, lu);
 }
 
-template <int P>
+template <int P, bool WIDE>
 __global__ void __launch_bounds__ (128)
 volume_kernel (VolumeParams vp, const Ray *__restrict__ rays, int n_rays, int *__restrict__ queue,
                VolumePartial *__restrict__ partials, float4 *__restrict__ fb_color,
@@ -482,16 +473,22 @@ volume_kernel (VolumeParams vp, const Ray *__restrict__ rays, int n_rays, int *_
     int n_samples = 0, iters = 0, cands = 0, nodes = 0;
     int prev_el = -1;
     float prev_ref[3] = { 0.5f, 0.5f, 0.5f };
+    LU3 lu;
+    // displacement between consecutive samples, for the coherent predictor
+    const float step[3] = { ray.dir.x * vp.sample_dist, ray.dir.y * vp.sample_dist,
+                            ray.dir.z * vp.sample_dist };
     for (int s = 0; s < kMaxSegments; ++s)
     {
       bool found = false;
       int el = -1;
       float ref[3];
+      float pt[3];
       while (distance < ray.far_t && !found)
       {
-        const float pt[3] = { ray.orig.x + distance * ray.dir.x, ray.orig.y + distance * ray.dir.y,
-                              ray.orig.z + distance * ray.dir.z };
-        el = locate_sample<P> (vp, pt, prev_el, prev_ref, ref, iters, cands, nodes);
+        pt[0] = ray.orig.x + distance * ray.dir.x;
+        pt[1] = ray.orig.y + distance * ray.dir.y;
+        pt[2] = ray.orig.z + distance * ray.dir.z;
+        el = locate_sample<P, WIDE> (vp, pt, step, prev_el, prev_ref, lu, ref, iters, cands, nodes);
         if (el != -1) found = true;
         else distance += vp.sample_dist;
         prev_el = el;
@@ -504,16 +501,17 @@ volume_kernel (VolumeParams vp, const Ray *__restrict__ rays, int n_rays, int *_
       do
       {
         ++n_samples;
-        const float4 sc = shade_sample<P> (vp, el, ref, ray);
+        const float4 sc = shade_sample<P> (vp, el, ref, ray, lu, pt);
         blend (color, sc);
         prev_el = el;
         prev_ref[0] = ref[0];
         prev_ref[1] = ref[1];
         prev_ref[2] = ref[2];
         distance += vp.sample_dist;
-        const float pt[3] = { ray.orig.x + distance * ray.dir.x, ray.orig.y + distance * ray.dir.y,
-                              ray.orig.z + distance * ray.dir.z };
-        el = locate_sample<P> (vp, pt, prev_el, prev_ref, ref, iters, cands, nodes);
+        pt[0] = ray.orig.x + distance * ray.dir.x;
+        pt[1] = ray.orig.y + distance * ray.dir.y;
+        pt[2] = ray.orig.z + distance * ray.dir.z;
+        el = locate_sample<P, WIDE> (vp, pt, step, prev_el, prev_ref, lu, ref, iters, cands, nodes);
         found = el != -1;
         if (!found) prev_el = -1;
       } while (distance < ray.far_t && found && color.w < 0.95f);
@@ -648,21 +646,31 @@ __global__ void fb_background_kernel (float4 *c, int n, float4 bg)
   }
 }
 
-template <int P>
-int launch_volume (const VolumeParams &vp, const Ray *rays, int n, int *queue,
-                   VolumePartial *partials, float4 *fb, float *depth, const drb_ray_stats &st,
-                   cudaStream_t s)
+template <int P, bool WIDE>
+int launch_volume_w (const VolumeParams &vp, const Ray *rays, int n, int *queue,
+                     VolumePartial *partials, float4 *fb, float *depth, const drb_ray_stats &st,
+                     cudaStream_t s)
 {
   int nb = 0;
-  cudaOccupancyMaxActiveBlocksPerMultiprocessor (&nb, volume_kernel<P>, 128, 0);
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor (&nb, volume_kernel<P, WIDE>, 128, 0);
   if (nb < 1) nb = 1;
   long long blocks = (long long)nb * sm_count ();
   const long long need = ((long long)n + 127) / 128;
   if (blocks > need) blocks = need;
   if (blocks < 1) blocks = 1;
-  volume_kernel<P><<<(unsigned)blocks, 128, 0, s>>> (vp, rays, n, queue, partials, fb, depth,
-                                                     st.samples, st.iters, st.candidates);
+  volume_kernel<P, WIDE><<<(unsigned)blocks, 128, 0, s>>> (vp, rays, n, queue, partials, fb, depth,
+                                                           st.samples, st.iters, st.candidates);
   return check_launch ("volume_kernel");
+}
+
+// full locates of the march walk the 4-wide tree when the BVH has one
+template <int P>
+int launch_volume (const VolumeParams &vp, const Ray *rays, int n, int *queue,
+                   VolumePartial *partials, float4 *fb, float *depth, const drb_ray_stats &st,
+                   cudaStream_t s)
+{
+  if (vp.lp.wide) return launch_volume_w<P, true> (vp, rays, n, queue, partials, fb, depth, st, s);
+  return launch_volume_w<P, false> (vp, rays, n, queue, partials, fb, depth, st, s);
 }
 
 } // namespace drb
@@ -884,6 +892,7 @@ static int volume_common (const drb_mesh *mesh, const drb_mesh *field, const drb
   no.guess = nullptr;
   LocateParams &lp = vp.lp;
   lp.nodes = (const float4 *)bvh->inner_nodes;
+  lp.wide = (const float4 *)bvh->wide_nodes;
   lp.leaf_nodes = bvh->leaf_nodes;
   lp.aabb_ids = bvh->aabb_ids;
   lp.ref_boxes = bvh->ref_boxes;

@@ -73,7 +73,24 @@ typedef struct drb_bvh
   int *aabb_ids;         /* device int32[n_leaf]: sub-box id per sorted leaf */
   float *ref_boxes;      /* device float[n_leaf * 2 * dim]: reference sub-box per sub-box id */
   float bounds[6];       /* host: xmin,xmax,ymin,ymax,zmin,zmax (filled by the build) */
+  /* Optional 4-wide collapse of the same tree for the batched kernels
+   * (drb_bvh_widen); NULL: they traverse the binary nodes. */
+  float *wide_nodes;     /* device float[32 * n_wide]: 8 x float4 per node */
+  int n_wide;
+  int wide_depth;        /* wide levels (root = 1) */
 } drb_bvh;
+
+/* 4-wide traversal tree of a built BVH (no reference counterpart: the
+ * reference traverses the binary nodes, device_mesh.hpp:262-318).  Every
+ * binary inner node at even depth becomes a 128-byte node holding its up to
+ * four grandchildren (children where those are leaves) in left-to-right
+ * order: child boxes as SoA float4 lo x/y/z, hi x/y/z (copied bit for bit),
+ * child codes (wide index >= 0, leaf -(leaf+1), empty INT_MIN), count.
+ * Locate over it tries the same candidates in the same order as over the
+ * binary tree.  With wide_nodes NULL it only fills bvh->n_wide and
+ * bvh->wide_depth; otherwise it writes up to capacity nodes and sets
+ * bvh->wide_nodes.  Synchronises the stream (reads the node count). */
+int drb_bvh_widen (drb_bvh *bvh, float *wide_nodes, int capacity, void *stream);
 
 /* Newton options.  The reference hard-codes tol 1e-4 and 20 steps for
  * volume elements (data_model/element.hpp:474-475), 1e-4 and 10 steps for

@@ -76,3 +76,43 @@ def node_leaf_ranges(inner: np.ndarray):
         lo[n] = min(a for a, _ in ranges)
         hi[n] = max(b for _, b in ranges)
     return lo, hi
+
+
+def widen(inner: np.ndarray):
+    """Reference collapse of a binary BVH into the 4-wide tree the CUDA path
+    builds: every inner node at even depth keeps its grandchildren (or its
+    children where those are leaves) left to right.  Returns (boxes
+    [n_wide, 4, 6] as xmin,xmax,ymin,ymax,zmin,zmax, codes [n_wide, 4]) with
+    wide nodes numbered in binary-node order, empty slots code INT_MIN."""
+    l, r = node_children(inner)
+    lb, rb = node_boxes(inner)
+    n = inner.shape[0]
+    depth = np.full(n, -1, np.int64)
+    depth[0] = 0
+    stack = [0]
+    while stack:
+        i = stack.pop()
+        for c in (l[i], r[i]):
+            if c >= 0:
+                depth[c // 4] = depth[i] + 1
+                stack.append(c // 4)
+    wide = np.where(depth % 2 == 0)[0]
+    wid = np.full(n, -1, np.int64)
+    wid[wide] = np.arange(wide.size)
+    boxes = np.zeros((wide.size, 4, 6), np.float32)
+    boxes[:, :, [0, 2, 4]] = np.inf
+    boxes[:, :, [1, 3, 5]] = -np.inf
+    codes = np.full((wide.size, 4), np.iinfo(np.int32).min, np.int64)
+    for w, i in enumerate(wide):
+        k = 0
+        for c, b in ((l[i], lb[i]), (r[i], rb[i])):
+            if c < 0:
+                boxes[w, k], codes[w, k] = b, c
+                k += 1
+            else:
+                j = c // 4
+                for g, gb in ((l[j], lb[j]), (r[j], rb[j])):
+                    boxes[w, k] = gb
+                    codes[w, k] = g if g < 0 else wid[g // 4]
+                    k += 1
+    return boxes, codes.astype(np.int32)

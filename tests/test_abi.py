@@ -50,3 +50,10 @@ def test_invalid_arguments_rejected_without_gpu():
     b = L.DrbBvh()
     assert lib.drb_locate(C.byref(m), C.byref(b), None, 4, C.byref(opts), None, None,
                           L.DrbQueryStats(), None) == L.DRB_ERR_INVALID_ARG
+
+
+def test_widen_rejects_missing_bvh():
+    from devil_ray_b200 import _lib as L
+    lib = L.lib()
+    assert lib.drb_bvh_widen(None, None, 0, None) == L.DRB_ERR_INVALID_ARG
+    assert b"built BVH" in lib.drb_last_error()

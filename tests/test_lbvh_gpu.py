@@ -41,6 +41,7 @@ def built(request, cuda, ref):
     rb = r.bvh()
     g = api.UnstructuredMesh(m.ctrl_idx, m.xyz, m.order, device=cuda)
     b = g.build_bvh(keep_codes=True)
+    b.widen()
     sub = api.elem_subboxes(g)
     torch.cuda.synchronize()
     gb = {"inner": b.inner_nodes.cpu().numpy(), "leaf_nodes": b.leaf_nodes.cpu().numpy(),
@@ -48,7 +49,8 @@ def built(request, cuda, ref):
           "ref_boxes": b.ref_boxes.cpu().numpy(),
           "codes": b.sorted_codes.cpu().numpy().view(np.uint32),
           "sub_aabbs": sub[0].cpu().numpy(), "sub_prim": sub[1].cpu().numpy(),
-          "sub_bounds": sub[3].cpu().numpy()}
+          "sub_bounds": sub[3].cpu().numpy(), "wide": b.wide_nodes.cpu().numpy(),
+          "n_wide": b.n_wide, "wide_depth": b.wide_depth}
     return request.param, m, r, rb, gb
 
 
@@ -149,3 +151,23 @@ def test_empty_mesh_special_case(cuda):
     l, r = node_children(b.inner_nodes.cpu().numpy())
     assert l[0] == -1 and r[0] == -2
     assert np.all(np.isinf(b.bounds))
+
+
+def test_wide_tree_is_the_exact_collapse(built):
+    """The 4-wide traversal tree equals the collapse of the binary tree:
+    grandchild boxes copied bit for bit, left-to-right child codes, empty
+    slots as inverted boxes."""
+    from tests.bvh_util import widen
+    name, m, r, rb, gb = built
+    boxes, codes = widen(gb["inner"])
+    assert gb["n_wide"] == boxes.shape[0]
+    w = gb["wide"][: gb["n_wide"]]
+    lo = w[:, 0:12].reshape(-1, 3, 4)   # [node, axis, child]
+    hi = w[:, 12:24].reshape(-1, 3, 4)
+    for a in range(3):
+        assert np.array_equal(lo[:, a, :].view(np.int32), boxes[:, :, 2 * a].view(np.int32)), name
+        assert np.array_equal(hi[:, a, :].view(np.int32), boxes[:, :, 2 * a + 1].view(np.int32)), name
+    assert np.array_equal(w[:, 24:28].view(np.int32), codes)
+    assert np.array_equal(w[:, 28].view(np.int32), (codes != np.iinfo(np.int32).min).sum(1))
+    print(f"{name}: {gb['n_wide']} wide nodes for {gb['inner'].shape[0]} binary, "
+          f"wide depth {gb['wide_depth']}")

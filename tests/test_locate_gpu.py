@@ -156,3 +156,25 @@ def test_local_frame_locates_fine_order3_mesh(cuda):
     ac, *_ = restate.locate(m.order, m.ctrl_idx, m.xyz, bvh, q, 1e-5, 20, L.GUESS_ELEM_CENTER)
     print(f"48^3 P3: mean iters {it.float().mean().item():.3f}, FP64 max err {e:.2e}; "
           f"absolute-coordinate FP32 Newton misses {(ac < 0).sum()} of {len(q)}")
+
+
+@pytest.mark.parametrize("name", ["volume_8", "p3_10", "p1_9"])
+def test_wide_traversal_equals_binary(cuda, name):
+    """The batched kernel over the 4-wide tree returns exactly what it
+    returns over the binary tree: cells, reference points (bit for bit),
+    Newton iterations and candidate counts; only node visits differ."""
+    import torch
+    from devil_ray_b200 import api
+    m, q, g = _setup(cuda, name, 50000, 13)
+    b = g.get_bvh()
+    assert b.wide_nodes is not None
+    wide = api.BatchedLocator(g, tol=1e-5, max_steps=20, bvh=b)
+    binary = api.BatchedLocator(g, tol=1e-5, max_steps=20, bvh=b.binary_only())
+    c0, r0, i0, a0, n0 = binary.locate(q, stats=True)
+    c1, r1, i1, a1, n1 = wide.locate(q, stats=True)
+    torch.cuda.synchronize()
+    assert torch.equal(c0, c1)
+    assert torch.equal(r0.view(torch.int32), r1.view(torch.int32))
+    assert torch.equal(i0, i1) and torch.equal(a0, a1)
+    print(f"{name}: nodes visited binary {n0.float().mean().item():.2f}, "
+          f"wide {n1.float().mean().item():.2f}")

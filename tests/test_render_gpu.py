@@ -95,3 +95,36 @@ def test_volume_order3(cuda, ref):
     bad = np.any(d > 1.0 / 255.0, axis=-1)
     print(f"p3: max diff {d.max():.2e}, pixels > 1/255: {bad.sum()} of {bad.size}")
     assert bad.mean() < 0.005
+
+
+def test_volume_wide_traversal_identical(cuda):
+    """The march's full locates over the 4-wide tree give the same image,
+    bit for bit, as over the binary tree (plain and coherent)."""
+    import torch
+    from devil_ray_b200 import api, meshgen
+    from devil_ray_b200.render import Camera, ColorTable, PointLight, UnstructuredField, Volume
+    m = meshgen.warped_mesh(6, 3, 0.05, gaussian_field_seed=4)
+    g = api.UnstructuredMesh(m.ctrl_idx, m.xyz, m.order, device=cuda)
+    gb = api.UnstructuredMesh(m.ctrl_idx, m.xyz, m.order, device=cuda)
+    gb._bvh = g.get_bvh().binary_only()
+    assert g.get_bvh().wide_nodes is not None and gb.get_bvh().wide_nodes is None
+    field = UnstructuredField(m.ctrl_idx, m.field, m.order, device=cuda)
+    cam = Camera(96, 96, CAM["pos"], CAM["look_at"], CAM["up"], CAM["fov"])
+    light = PointLight.default(cam)
+    imgs = []
+    for coherent in (False, True):
+        for mesh in (g, gb):
+            vol = Volume(mesh, field)
+            vol.samples(300)
+            t = ColorTable()
+            for p in meshgen.TF_RGB:
+                t.add_point(p[0], p[1:])
+            for p in meshgen.TF_ALPHA:
+                t.add_alpha(*p)
+            vol.color_map().color_table(t)
+            vol.coherent = coherent
+            fb = vol.render(cam, [light])
+            torch.cuda.synchronize()
+            imgs.append(fb.image())
+    assert np.array_equal(imgs[0].view(np.int32), imgs[1].view(np.int32))
+    assert np.array_equal(imgs[2].view(np.int32), imgs[3].view(np.int32))
