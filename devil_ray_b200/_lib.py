@@ -126,6 +126,9 @@ _SIGS = {
     "drb_locate_ordered": (C.c_int, [C.POINTER(DrbMesh), C.POINTER(DrbBvh), C.c_void_p, C.c_int,
                                      C.c_void_p, C.POINTER(DrbNewtonOpts), C.c_void_p,
                                      C.c_void_p, C.c_void_p, DrbQueryStats, C.c_void_p]),
+    "drb_locate_host": (C.c_int, [C.POINTER(DrbMesh), C.POINTER(DrbBvh), C.c_void_p, C.c_int,
+                                  C.POINTER(DrbNewtonOpts), C.c_void_p, C.c_int, C.c_void_p,
+                                  C.c_void_p, C.c_void_p]),
     "drb_locate_tune": (C.c_int, [C.POINTER(DrbMesh), C.POINTER(DrbBvh), C.c_void_p, C.c_int,
                                   C.POINTER(DrbNewtonOpts), C.c_void_p, C.POINTER(C.c_float),
                                   C.c_void_p]),

@@ -269,6 +269,24 @@ class BatchedLocator:
         return cell, ref
 
 
+    def locate_host(self, host_points, out, chunk: int = 0, stream=None):
+        """Locate points held in (page-locked) host memory, writing cell ids
+        and reference points into the host tensors out = (cell, ref); the
+        copies of consecutive chunks overlap the locate (drb_locate_host)."""
+        assert host_points.device.type == "cpu" and host_points.dtype == torch.float32
+        cell, ref = out
+        assert cell.device.type == "cpu" and ref.device.type == "cpu"
+        n = host_points.shape[0]
+        opts = L.DrbNewtonOpts(self.tol, self.max_steps, self.guess_mode, None)
+        cfg = None if self.config is None else C.byref(self.config)
+        d = self.mesh.desc()
+        bd = self._bvh(stream).desc()
+        L.check(L.lib().drb_locate_host(C.byref(d), C.byref(bd), _ptr(host_points), n,
+                                        C.byref(opts), cfg, chunk, _ptr(cell), _ptr(ref),
+                                        _stream(stream)), "drb_locate_host")
+        return cell, ref
+
+
 def elem_subboxes(mesh: UnstructuredMesh, stream=None):
     """Per-element sub-boxes (aabbs6, prim_ids, ref_boxes, bounds6) on device."""
     nb = 33 if mesh.dim == 3 else 17

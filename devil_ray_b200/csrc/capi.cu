@@ -31,6 +31,27 @@ int check_launch (const char *what)
   return status_from (e);
 }
 
+// The scratch of every entry point comes from the device's default
+// stream-ordered pool.  With the pool's default release threshold (0) the
+// memory goes back to the driver at every synchronisation, and the next
+// call maps it again; calls that synchronise (drb_locate_host, the build)
+// would pay that each time.  Keep it reserved instead, once per device.
+void keep_pool_reserved ()
+{
+  static std::atomic<unsigned long long> done{ 0 };
+  int dev = 0;
+  if (cudaGetDevice (&dev) != cudaSuccess || dev < 0 || dev >= 64) return;
+  const unsigned long long bit = 1ull << dev;
+  if (done.load (std::memory_order_relaxed) & bit) return;
+  cudaMemPool_t pool;
+  if (cudaDeviceGetDefaultMemPool (&pool, dev) == cudaSuccess)
+  {
+    unsigned long long threshold = ~0ull;
+    cudaMemPoolSetAttribute (pool, cudaMemPoolAttrReleaseThreshold, &threshold);
+  }
+  done.fetch_or (bit);
+}
+
 int sm_count ()
 {
   static int cached = 0;

@@ -9,6 +9,9 @@
 namespace drb
 {
 
+// Keep the device's default memory pool reserved across synchronisations.
+void keep_pool_reserved ();
+
 // Stream-ordered scratch allocation; all scratch is freed before a public
 // entry point returns (stream-ordered, so no synchronisation is implied).
 struct Scratch
@@ -17,7 +20,7 @@ struct Scratch
   void *ptrs[32];
   int n = 0;
   cudaError_t err = cudaSuccess;
-  explicit Scratch (cudaStream_t s) : stream (s) {}
+  explicit Scratch (cudaStream_t s) : stream (s) { keep_pool_reserved (); }
   template <typename T> T *alloc (size_t count)
   {
     if (err != cudaSuccess || n >= 32) return nullptr;

@@ -222,6 +222,19 @@ int drb_locate_ordered (const drb_mesh *mesh, const drb_bvh *bvh, const float *p
                         const drb_locate_config *cfg, int *cell, float *ref,
                         drb_query_stats stats, void *stream);
 
+/* UnstructuredMesh::locate (unstructured_mesh.cpp:124-148) on points that
+ * live in host memory: host_pts float[3n] in, host_cell int32[n] and
+ * host_ref float[3n] out.  The batch is cut into chunks (chunk <= 0: 2M
+ * points) that cycle through three internal streams, so the copies in, the
+ * batched locate (drb_locate_batched, Morton order per chunk) and the
+ * copies out of consecutive chunks overlap.  Results equal
+ * drb_locate_batched's.  Host buffers should be page-locked for the copies
+ * to overlap.  Work already queued on stream runs first; the call returns
+ * when the results are in host memory. */
+int drb_locate_host (const drb_mesh *mesh, const drb_bvh *bvh, const float *host_pts, int n,
+                     const drb_newton_opts *opts, const drb_locate_config *cfg, int chunk,
+                     int *host_cell, float *host_ref, void *stream);
+
 /* Autotuner of the persistent kernel: times every candidate launch shape on
  * a query sample (CUDA events, synchronous) and returns the fastest in
  * *best and its time in *best_ms (may be NULL).  No reference counterpart. */

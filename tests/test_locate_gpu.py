@@ -178,3 +178,22 @@ def test_wide_traversal_equals_binary(cuda, name):
     assert torch.equal(i0, i1) and torch.equal(a0, a1)
     print(f"{name}: nodes visited binary {n0.float().mean().item():.2f}, "
           f"wide {n1.float().mean().item():.2f}")
+
+
+def test_locate_host_equals_device_batched(cuda):
+    """drb_locate_host (chunked, copies overlapped on three streams) gives
+    the batched locate's results, for chunk sizes that do and do not divide
+    the batch."""
+    import torch
+    from devil_ray_b200 import api
+    m, q, g = _setup(cuda, "volume_8", 100000, 17)
+    loc = api.BatchedLocator(g, tol=1e-5, max_steps=20)
+    c0, r0 = loc.locate(q)
+    torch.cuda.synchronize()
+    hq = torch.from_numpy(np.ascontiguousarray(q, np.float32)).pin_memory()
+    for chunk in (0, 30000, 1 << 20):
+        hc = torch.empty(q.shape[0], dtype=torch.int32).pin_memory()
+        hr = torch.empty((q.shape[0], 3), dtype=torch.float32).pin_memory()
+        loc.locate_host(hq, out=(hc, hr), chunk=chunk)
+        assert torch.equal(hc, c0.cpu())
+        assert torch.equal(hr.view(torch.int32), r0.cpu().view(torch.int32))
