@@ -170,6 +170,31 @@ DRB_D bool solve_in_element (const LocateParams &lp, int el, const float (&pt)[3
   return solve_in_element<P, REG> (lp, el, pt, x, steps, lu);
 }
 
+// Element rows staged in shared memory by the warp (locate_persistent_kernel
+// with shared rows): a packed geometry row (relative coordinates, then the
+// origin) at a lane-group slot; reads are plain shared-memory loads.
+struct SmemCP
+{
+  // volatile: read on every use, so the row stays in shared memory instead
+  // of being hoisted into 81+ registers across the Newton steps
+  const volatile float *p;
+  DRB_D float operator() (int i, int k) const { return p[3 * i + k]; }
+};
+
+// Newton solve of one point in the element whose packed row is in shared
+// memory (same arithmetic as the packed path of solve_in_element).
+template <int P>
+DRB_D bool solve_in_smem_row (const LocateParams &lp, const float *row, const float (&pt)[3],
+                              float (&x)[3], int &steps)
+{
+  constexpr int ND = (P + 1) * (P + 1) * (P + 1);
+  float t[3];
+#pragma unroll
+  for (int d = 0; d < 3; ++d) t[d] = __fsub_rn (pt[d], row[packed_origin (ND) + d]);
+  SmemCP cp{ row };
+  return hex_newton<P> (cp, t, x, lp.tol, lp.max_steps, steps);
+}
+
 // Initial guess of a candidate leaf's Newton solve (drb_guess_mode).
 DRB_D void candidate_guess (const LocateParams &lp, int leaf, long long qi, bool first,
                             float (&x)[3], bool &given)
@@ -223,6 +248,25 @@ DRB_D bool solve_candidate (const LocateParams &lp, int leaf, int el, long long 
 {
   LU3 lu;
   return solve_candidate<P, REG> (lp, leaf, el, qi, first, pt, x, iters, lu);
+}
+
+// solve_candidate on a shared-memory row (same guess and fallback rule).
+template <int P>
+DRB_D bool solve_candidate_smem (const LocateParams &lp, int leaf, const float *row, long long qi,
+                                 bool first, const float (&pt)[3], float (&x)[3], int &iters)
+{
+  bool given;
+  candidate_guess (lp, leaf, qi, first, x, given);
+  int steps = 0;
+  bool found = solve_in_smem_row<P> (lp, row, pt, x, steps);
+  iters += steps;
+  if (!found && given)
+  {
+    x[0] = x[1] = x[2] = 0.5f;
+    found = solve_in_smem_row<P> (lp, row, pt, x, steps);
+    iters += steps;
+  }
+  return found;
 }
 
 // Full point location of one query (DeviceMesh::locate, device_mesh.hpp:248-354):

@@ -56,7 +56,26 @@ __global__ void query_codes_kernel (const float *__restrict__ pts, int n, float 
   iota[i] = i;
 }
 
-template <int P, bool REG, bool WIDE>
+// Element-row modes of the candidate solves (drb_locate_config.reg_elements)
+enum RowMode
+{
+  kRowsL1 = 0,     // control points read through L1 on every Newton step
+  kRowsReg = 1,    // the row copied into registers (orders 1-2)
+  kRowsShared = 2  // the distinct rows of a warp's candidates staged in shared memory
+};
+
+// Shared-memory row stride (floats): the packed row plus one, odd, so 32
+// lanes reading the same column of different rows hit 32 different banks.
+template <int P> constexpr int smem_row_stride ()
+{
+  return packed_stride ((P + 1) * (P + 1) * (P + 1), 3) + 1;
+}
+template <int P> constexpr size_t smem_rows_bytes_per_warp ()
+{
+  return sizeof (float) * 32 * (size_t)smem_row_stride<P> ();
+}
+
+template <int P, int MODE, bool WIDE>
 __global__ void locate_persistent_kernel (LocateParams lp, const float *__restrict__ pts,
                                           const int *__restrict__ order, int n, int chunk,
                                           int *__restrict__ queue_head, int *__restrict__ cell,
@@ -66,6 +85,8 @@ __global__ void locate_persistent_kernel (LocateParams lp, const float *__restri
   const unsigned FULL = 0xffffffffu;
   const int lane = threadIdx.x & 31;
   const unsigned lt = (1u << lane) - 1u;
+  extern __shared__ float s_rows[]; // kRowsShared: 32 row slots per warp
+  float *warp_rows = s_rows + (size_t)(threadIdx.x >> 5) * 32 * smem_row_stride<P> ();
   int pool_next = 0, pool_end = 0; // warp-uniform
   bool exhausted = false;          // warp-uniform
   int qi = -1;
@@ -119,6 +140,42 @@ __global__ void locate_persistent_kernel (LocateParams lp, const float *__restri
     if (qi >= 0) leaf = next_leaf<WIDE> (lp.nodes, lp.wide, pt, todo, sp, cur, nodes);
 
     // ---- candidate phase: converged Newton solves ----
+    int el = -1;
+    if (qi >= 0 && leaf >= 0) el = __ldg (lp.leaf_nodes + leaf);
+    const float *my_row = nullptr;
+    if (MODE == kRowsShared)
+    {
+      // lanes with the same element share one slot; the warp loads each
+      // distinct row once with float4 reads and stores it at odd stride
+      constexpr int S = smem_row_stride<P> ();
+      constexpr int F4 = (S - 1) / 4;
+      const bool has = el >= 0;
+      const unsigned same = __match_any_sync (FULL, has ? el : -1 - lane);
+      const int leader = __ffs (same) - 1;
+      const unsigned leaders = __ballot_sync (FULL, has && leader == lane);
+      const int slot = __popc (leaders & ((1u << leader) - 1u));
+      __syncwarp ();
+      unsigned todo_rows = leaders;
+      int r = 0;
+      while (todo_rows)
+      {
+        const int src = __ffs (todo_rows) - 1;
+        todo_rows &= todo_rows - 1u;
+        const int e = __shfl_sync (FULL, el, src);
+        for (int q = lane; q < F4; q += 32)
+        {
+          const float4 v = __ldg (reinterpret_cast<const float4 *> (lp.packed + (size_t)e * lp.stride) + q);
+          float *d = warp_rows + r * S + 4 * q;
+          d[0] = v.x;
+          d[1] = v.y;
+          d[2] = v.z;
+          d[3] = v.w;
+        }
+        ++r;
+      }
+      __syncwarp ();
+      if (has) my_row = warp_rows + slot * S;
+    }
     if (qi >= 0)
     {
       bool done = false;
@@ -126,9 +183,10 @@ __global__ void locate_persistent_kernel (LocateParams lp, const float *__restri
       float x[3] = { -1.f, -1.f, -1.f };
       if (leaf >= 0)
       {
-        const int el = __ldg (lp.leaf_nodes + leaf);
         ++cands;
-        const bool found = solve_candidate<P, REG> (lp, leaf, el, qi, first, pt, x, iters);
+        const bool found = (MODE == kRowsShared)
+                           ? solve_candidate_smem<P> (lp, leaf, my_row, qi, first, pt, x, iters)
+                           : solve_candidate<P, MODE == kRowsReg> (lp, leaf, el, qi, first, pt, x, iters);
         first = false;
         if (found)
         {
@@ -161,43 +219,72 @@ __global__ void locate_persistent_kernel (LocateParams lp, const float *__restri
   }
 }
 
-template <bool W> const void *persistent_fn_w (int order, bool reg)
+template <int P, bool W> const void *persistent_fn_pw (int mode)
 {
-  if (order == 1) return reg ? (const void *)locate_persistent_kernel<1, true, W> : (const void *)locate_persistent_kernel<1, false, W>;
-  if (order == 2) return reg ? (const void *)locate_persistent_kernel<2, true, W> : (const void *)locate_persistent_kernel<2, false, W>;
-  return (const void *)locate_persistent_kernel<3, false, W>;
+  if (mode == kRowsShared) return (const void *)locate_persistent_kernel<P, kRowsShared, W>;
+  if (mode == kRowsReg && P <= 2) return (const void *)locate_persistent_kernel<P, kRowsReg, W>;
+  return (const void *)locate_persistent_kernel<P, kRowsL1, W>;
 }
 
-const void *persistent_fn (int order, bool reg, bool wide)
+const void *persistent_fn (int order, int mode, bool wide)
 {
-  return wide ? persistent_fn_w<true> (order, reg) : persistent_fn_w<false> (order, reg);
+  if (order == 1) return wide ? persistent_fn_pw<1, true> (mode) : persistent_fn_pw<1, false> (mode);
+  if (order == 2) return wide ? persistent_fn_pw<2, true> (mode) : persistent_fn_pw<2, false> (mode);
+  return wide ? persistent_fn_pw<3, true> (mode) : persistent_fn_pw<3, false> (mode);
 }
 
-int launch_persistent (int order, bool reg, dim3 grid, int block, cudaStream_t s,
+// Row mode actually used: registers only for orders 1-2, shared rows only
+// with a packed element copy.
+int effective_mode (const drb_mesh *mesh, int requested)
+{
+  if (requested == kRowsReg && mesh->order <= 2) return kRowsReg;
+  if (requested == kRowsShared && mesh->packed) return kRowsShared;
+  return kRowsL1;
+}
+
+size_t dynamic_smem (int order, int mode, int block)
+{
+  if (mode != kRowsShared) return 0;
+  const size_t per_warp = order == 1 ? smem_rows_bytes_per_warp<1> ()
+                          : order == 2 ? smem_rows_bytes_per_warp<2> () : smem_rows_bytes_per_warp<3> ();
+  return per_warp * (size_t)(block / 32);
+}
+
+template <int P, bool W>
+void launch_pw (int mode, dim3 grid, int block, size_t smem, cudaStream_t s, const LocateParams &lp,
+                const float *pts, const int *ord, int n, int chunk, int *head, int *cell, float *ref,
+                drb_query_stats st)
+{
+#define DRB_LP(M) locate_persistent_kernel<P, M, W><<<grid, block, smem, s>>> (lp, pts, ord, n, chunk, head, cell, ref, st.iters, st.candidates, st.nodes)
+  if (mode == kRowsShared) DRB_LP (kRowsShared);
+  else if (mode == kRowsReg && P <= 2) DRB_LP (P <= 2 ? kRowsReg : kRowsL1);
+  else DRB_LP (kRowsL1);
+#undef DRB_LP
+}
+
+int launch_persistent (int order, int mode, dim3 grid, int block, cudaStream_t s,
                        const LocateParams &lp, const float *pts, const int *ord, int n, int chunk,
                        int *head, int *cell, float *ref, drb_query_stats st)
 {
-#define DRB_LP(P, R, W) locate_persistent_kernel<P, R, W><<<grid, block, 0, s>>> (lp, pts, ord, n, chunk, head, cell, ref, st.iters, st.candidates, st.nodes)
-  if (lp.wide)
-  {
-    if (order == 1) { if (reg) DRB_LP (1, true, true); else DRB_LP (1, false, true); }
-    else if (order == 2) { if (reg) DRB_LP (2, true, true); else DRB_LP (2, false, true); }
-    else DRB_LP (3, false, true);
-  }
-  else
-  {
-    if (order == 1) { if (reg) DRB_LP (1, true, false); else DRB_LP (1, false, false); }
-    else if (order == 2) { if (reg) DRB_LP (2, true, false); else DRB_LP (2, false, false); }
-    else DRB_LP (3, false, false);
-  }
-#undef DRB_LP
+  const size_t smem = dynamic_smem (order, mode, block);
+  const bool wide = lp.wide != nullptr;
+  if (smem > 48 * 1024)
+    cudaFuncSetAttribute (persistent_fn (order, mode, wide), cudaFuncAttributeMaxDynamicSharedMemorySize,
+                          (int)smem);
+  if (order == 1) { if (wide) launch_pw<1, true> (mode, grid, block, smem, s, lp, pts, ord, n, chunk, head, cell, ref, st); else launch_pw<1, false> (mode, grid, block, smem, s, lp, pts, ord, n, chunk, head, cell, ref, st); }
+  else if (order == 2) { if (wide) launch_pw<2, true> (mode, grid, block, smem, s, lp, pts, ord, n, chunk, head, cell, ref, st); else launch_pw<2, false> (mode, grid, block, smem, s, lp, pts, ord, n, chunk, head, cell, ref, st); }
+  else { if (wide) launch_pw<3, true> (mode, grid, block, smem, s, lp, pts, ord, n, chunk, head, cell, ref, st); else launch_pw<3, false> (mode, grid, block, smem, s, lp, pts, ord, n, chunk, head, cell, ref, st); }
   return check_launch ("locate_persistent_kernel");
 }
 
-int resident_blocks (int order, bool reg, bool wide, int block)
+int resident_blocks (int order, int mode, bool wide, int block)
 {
+  const size_t smem = dynamic_smem (order, mode, block);
+  const void *fn = persistent_fn (order, mode, wide);
+  if (smem > 48 * 1024)
+    cudaFuncSetAttribute (fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
   int nb = 0;
-  cudaOccupancyMaxActiveBlocksPerMultiprocessor (&nb, persistent_fn (order, reg, wide), block, 0);
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor (&nb, fn, block, smem);
   return nb > 0 ? nb : 1;
 }
 
@@ -311,8 +398,8 @@ int locate_batched_impl (const drb_mesh *mesh, const drb_bvh *bvh, const float *
   }
   if (scr.err != cudaSuccess) return status_from (scr.err);
   cudaMemsetAsync (head, 0, sizeof (int), s);
-  const bool reg = cfg.reg_elements != 0;
-  const int per_sm = resident_blocks (mesh->order, reg, bvh->wide_nodes != nullptr, cfg.block);
+  const int mode = effective_mode (mesh, cfg.reg_elements);
+  const int per_sm = resident_blocks (mesh->order, mode, bvh->wide_nodes != nullptr, cfg.block);
   const int bps = (cfg.blocks_per_sm > 0) ? min (cfg.blocks_per_sm, per_sm) : per_sm;
   const long long warps_needed = ((long long)n + 31) / 32;
   long long blocks = (long long)bps * sm_count ();
@@ -320,7 +407,7 @@ int locate_batched_impl (const drb_mesh *mesh, const drb_bvh *bvh, const float *
   if (blocks > blocks_needed) blocks = blocks_needed;
   if (blocks < 1) blocks = 1;
   const LocateParams lp = make_params (mesh, bvh, opts);
-  return launch_persistent (mesh->order, reg, dim3 ((unsigned)blocks), cfg.block, s, lp, pts, ord, n,
+  return launch_persistent (mesh->order, mode, dim3 ((unsigned)blocks), cfg.block, s, lp, pts, ord, n,
                             cfg.chunk, head, cell, ref, stats);
 }
 
@@ -361,8 +448,8 @@ int locate_batched_ws (const drb_mesh *mesh, const drb_bvh *bvh, const float *pt
   }
   cudaError_t e = cudaMemsetAsync (ws.head, 0, sizeof (int), s);
   if (e != cudaSuccess) return status_from (e);
-  const bool reg = cfg.reg_elements != 0;
-  const int per_sm = resident_blocks (mesh->order, reg, bvh->wide_nodes != nullptr, cfg.block);
+  const int mode = effective_mode (mesh, cfg.reg_elements);
+  const int per_sm = resident_blocks (mesh->order, mode, bvh->wide_nodes != nullptr, cfg.block);
   const int bps = (cfg.blocks_per_sm > 0) ? min (cfg.blocks_per_sm, per_sm) : per_sm;
   const long long warps_needed = ((long long)n + 31) / 32;
   long long blocks = (long long)bps * sm_count ();
@@ -370,7 +457,7 @@ int locate_batched_ws (const drb_mesh *mesh, const drb_bvh *bvh, const float *pt
   if (blocks > blocks_needed) blocks = blocks_needed;
   if (blocks < 1) blocks = 1;
   const LocateParams lp = make_params (mesh, bvh, opts);
-  return launch_persistent (mesh->order, reg, dim3 ((unsigned)blocks), cfg.block, s, lp, pts, ord, n,
+  return launch_persistent (mesh->order, mode, dim3 ((unsigned)blocks), cfg.block, s, lp, pts, ord, n,
                             cfg.chunk, ws.head, cell, ref, stats);
 }
 
@@ -443,7 +530,9 @@ extern "C" int drb_locate_tune (const drb_mesh *mesh, const drb_bvh *bvh, const 
   cudaEventCreate (&e1);
   float best_t = 1e30f;
   drb_locate_config bc = default_config (mesh->order);
-  for (int rg = 0; rg < (mesh->order <= 2 ? 2 : 1); ++rg)
+  const int modes[] = { kRowsL1, kRowsReg, kRowsShared };
+  for (int rg : modes)
+  if (effective_mode (mesh, rg) == rg)
   for (int b : blocks)
     for (int ps : per_sm)
       for (int c : chunks)

@@ -177,9 +177,12 @@ typedef struct drb_locate_config
   int blocks_per_sm;     /* resident blocks per SM, 0 = as many as fit */
   int chunk;             /* queries a warp pops from the global queue at once */
   int sort_queries;      /* 1 = process the queries in Morton order */
-  int reg_elements;      /* 1 = keep an order <= 2 candidate's control points in
-                            registers for its whole Newton solve (fewer loads,
-                            more registers); 0 = read them through L1 */
+  int reg_elements;      /* where a candidate's control points are read from
+                            during its Newton solve: 0 = through L1 on every
+                            step; 1 = registers (orders <= 2; fewer loads,
+                            more registers); 2 = shared memory: the warp
+                            stages each distinct element row of its lanes'
+                            candidates once (packed meshes; falls back to 0) */
 } drb_locate_config;
 
 /* Batched point location, same results as drb_locate (same traversal order

@@ -197,3 +197,26 @@ def test_locate_host_equals_device_batched(cuda):
         loc.locate_host(hq, out=(hc, hr), chunk=chunk)
         assert torch.equal(hc, c0.cpu())
         assert torch.equal(hr.view(torch.int32), r0.cpu().view(torch.int32))
+
+
+@pytest.mark.parametrize("name", ["volume_8", "p3_10", "p1_9"])
+def test_row_modes_identical(cuda, name):
+    """The three places a candidate's control points can be read from during
+    its Newton solve (L1 on every step, registers, warp-shared rows in shared
+    memory) give bit-identical results and statistics."""
+    import torch
+    from devil_ray_b200 import _lib as L
+    from devil_ray_b200 import api
+    m, q, g = _setup(cuda, name, 50000, 19)
+    out = []
+    for mode in (0, 1, 2):
+        for block in (64, 128):
+            loc = api.BatchedLocator(g, tol=1e-5, max_steps=20,
+                                     config=L.DrbLocateConfig(block, 0, 32, 1, mode))
+            out.append(loc.locate(q, stats=True))
+    torch.cuda.synchronize()
+    c0, r0, i0, a0, n0 = out[0]
+    for c, r, i, a, nd in out[1:]:
+        assert torch.equal(c, c0)
+        assert torch.equal(r.view(torch.int32), r0.view(torch.int32))
+        assert torch.equal(i, i0) and torch.equal(a, a0) and torch.equal(nd, n0)
