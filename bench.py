@@ -213,6 +213,13 @@ def orbit_cameras(count, width, seed=5):
     return cams
 
 
+# DRAM bytes (read + write) of one locate_persistent_kernel launch on this
+# workload (16M queries, 4-wide tree), from an ncu capture of the same launch
+# (profiles/locate_persistent_kernel__locate_64_16M_queries.md): 4.019 GB
+# read + 1.197 GB written.  Used for roofline.traffic, scaled by the query
+# count when --queries differs.
+LOCATE_TRAFFIC_16M = 4.018994e9 + 1.197257e9
+
 # FP32 pipe peak of a B200: 148 SMs x 128 FP32 lanes x 2 FLOP (FMA) x 1.965 GHz
 FP32_PEAK_TFLOPS = 148 * 128 * 2 * 1.965e9 / 1e12
 
@@ -561,7 +568,10 @@ def main():
                        "l2": "inputs larger than L2 (201 MB queries, 553 MB BVH nodes)",
                        "parallelism": f"replicas x{world}, queries sharded, no collective"},
             "roofline": {"bound": "hbm", "achieved": achieved_gbs, "peak": peak, "unit": "GB/s",
-                         "frac": achieved_gbs / peak, "traffic": None,
+                         "frac": achieved_gbs / peak,
+                         "traffic": LOCATE_TRAFFIC_16M * n / float(1 << 24),
+                         "traffic_source": "ncu capture of the same kernel on 16M queries, "
+                                           "scaled by queries",
                          "peak_source": peak_src, "kernel": "locate_persistent_kernel",
                          "bytes_per_query": bytes_q, "kernel_ms": kern_ms,
                          "fp32": {"flops_per_query": flops_q, "achieved_tflops": achieved_tflops,
