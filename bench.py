@@ -59,6 +59,9 @@ def parse():
     ap.add_argument("--no-volume", action="store_true", help="skip the volume workload")
     ap.add_argument("--train-samples", type=int, default=1 << 22)
     ap.add_argument("--orbits", type=int, default=16)
+    ap.add_argument("--profile-volume", type=int, default=0, metavar="N",
+                    help="profiling run of the volume march alone: one coherent 1024^2 frame "
+                         "of the order-3 warped mesh at N^3 elements, timed --steps times")
     ap.add_argument("--profile", action="store_true",
                     help="profiling run: fixed launch shape, only the timed steps "
                          "(no tuning, plain/e2e/statistics/CPU legs)")
@@ -343,6 +346,47 @@ def volume_bench(dev, args, timed):
     }
 
 
+def profile_volume(dev, args):
+    """One coherent 1024^2 frame of the volume workload's mesh family at
+    N^3 elements (order 3, warp 0.05, Gaussian field), 1000 samples."""
+    import torch
+    from devil_ray_b200 import api, meshgen
+    from devil_ray_b200.render import Camera, ColorTable, PointLight, UnstructuredField, Volume
+    m = meshgen.warped_mesh(args.profile_volume, 3, 0.05, gaussian_field_seed=4)
+    mesh = api.UnstructuredMesh(m.ctrl_idx, m.xyz, m.order, device=dev)
+    field = UnstructuredField(m.ctrl_idx, m.field, m.order, device=dev)
+    vol = Volume(mesh, field)
+    vol.samples(1000)
+    vol.use_lighting(True)
+    t = ColorTable()
+    for p in meshgen.TF_RGB:
+        t.add_point(p[0], p[1:])
+    for p in meshgen.TF_ALPHA:
+        t.add_alpha(*p)
+    vol.color_map().color_table(t)
+    vol.tol, vol.max_steps = 1e-5, 20
+    vol.coherent = True
+    c = meshgen.CAMERA
+    cam = Camera(1024, 1024, c["pos"], c["look_at"], c["up"], c["fov"])
+    fb, st = vol.render(cam, stats=True)
+    torch.cuda.synchronize()
+    samples = int(st[0].long().sum())
+    for _ in range(max(args.warmup, 1)):
+        vol.render(cam, fb=fb)
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    for _ in range(args.steps):
+        vol.render(cam, fb=fb)
+    e1.record()
+    torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1) / args.steps
+    print(json.dumps({"profile_volume": args.profile_volume, "ms_per_frame": ms,
+                      "samples": samples, "samples_per_s": samples / (ms * 1e-3),
+                      "mean_iters_per_sample": float(st[1].long().sum()) / max(samples, 1)}))
+    return 0
+
+
 def main():
     args = parse()
     rank, world, local = dist_info()
@@ -355,6 +399,8 @@ def main():
 
     dev = torch.device("cuda", local)
     torch.cuda.set_device(dev)
+    if args.profile_volume:
+        return profile_volume(dev, args)
     pg = None
     if world > 1:
         import torch.distributed as dist
