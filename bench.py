@@ -474,6 +474,12 @@ def main():
     batched_ms = timed(batched_step, args.steps) / args.steps
     located = int((cell >= 0).sum().item())
     batched_value = world * located / (batched_ms * 1e-3)
+    # binary-tree node visits of the same queries (the reference's traversal),
+    # for the algorithmic bytes; the timed path walks the 4-wide tree
+    _, _, _, _, nd_bin = api.BatchedLocator(mesh, TOL, MAX_STEPS, L.GUESS_ELEM_CENTER,
+                                            bvh=bvh.binary_only()).locate(pts, stats=True)
+    mean_nd_binary = float(nd_bin.float().mean())
+    del nd_bin
     _, _, it, ca, nd = loc.locate(pts, stats=True)
     mean_it, mean_ca, mean_nd = (float(it.float().mean()), float(ca.float().mean()),
                                  float(nd.float().mean()))
@@ -548,13 +554,14 @@ def main():
 
     # algorithmic bytes per located point: point 12 B + Location 16 B + one
     # element's control-point indices and coordinates nd x (4 + 12) B + its
-    # reference box 24 B + 64 B per inner node visited
+    # reference box 24 B + 64 B per binary inner node the reference's
+    # traversal visits
     nd_dofs = (m.order + 1) ** 3
-    bytes_q = 12 + 16 + nd_dofs * 16 + 24 + 64 * mean_nd
+    bytes_q = 12 + 16 + nd_dofs * 16 + 24 + 64 * mean_nd_binary
     achieved_gbs = n * bytes_q / (kern_ms * 1e-3) / 1e9
     # FP32 work of the same launch: Newton steps, inside tests (6 compares
-    # per candidate) and node tests (12 compares per inner node)
-    flops_q = mean_it * newton_step_flops(m.order) + 6 * mean_ca + 12 * mean_nd
+    # per candidate) and box tests (24 compares per 4-wide node visited)
+    flops_q = mean_it * newton_step_flops(m.order) + 6 * mean_ca + 24 * mean_nd
     achieved_tflops = n * flops_q / (kern_ms * 1e-3) / 1e12
     peaks = {}
     try:
@@ -634,6 +641,7 @@ def main():
             "clocks": clk,
             "stats": {"located_fraction": located / n, "mean_newton_iters": mean_it,
                       "mean_candidates": mean_ca, "mean_nodes_visited": mean_nd,
+                      "mean_binary_nodes_visited": mean_nd_binary,
                       "iteration_histogram": hist},
             "plain": {"ms_per_step": plain_ms, "value": plain_value,
                       "note": "one thread per query in input order (reference launch pattern), "
