@@ -198,6 +198,69 @@ def cpu_baseline(mesh_data, queries, bvh_np):
                       f"{t:.1f} s; reference BVH build {build_s:.1f} s not timed"}
 
 
+def volume_c0(dev, with_cpu):
+    """The CPU-runnable volume config (8^3 order-2 mesh, warp 0.05, 256^2
+    rays from (2.5,2.5,2.5), 500 samples, lit): Newton-resolved samples/s of
+    the GPU march (plain and coherent) and of the reference's OpenMP
+    Volume::integrate + Volume::save on the host cores."""
+    import torch
+    from devil_ray_b200 import api, meshgen
+    from devil_ray_b200.render import Camera, ColorTable, PointLight, UnstructuredField, Volume
+    m = meshgen.workload_mesh("volume_8")
+    c = meshgen.CAMERA
+    cam = Camera(256, 256, c["pos"], c["look_at"], c["up"], c["fov"])
+    light = PointLight.default(cam)
+    mesh = api.UnstructuredMesh(m.ctrl_idx, m.xyz, m.order, device=dev)
+    field = UnstructuredField(m.ctrl_idx, m.field, m.order, device=dev)
+    out = {"workload": "volume_8: 8^3 hex order 2, warp 0.05, 256^2 rays, 500 samples, "
+                       "256-entry TF, lit"}
+    for coherent in (False, True):
+        vol = Volume(mesh, field)
+        vol.samples(500)
+        vol.use_lighting(True)
+        t = ColorTable()
+        for p in meshgen.TF_RGB:
+            t.add_point(p[0], p[1:])
+        for p in meshgen.TF_ALPHA:
+            t.add_alpha(*p)
+        vol.color_map().color_table(t)
+        vol.color_map().samples(256)
+        vol.coherent = coherent
+        fb, st = vol.render(cam, [light], stats=True)
+        torch.cuda.synchronize()
+        samples = int(st[0].long().sum())
+        for _ in range(3):
+            vol.render(cam, [light], fb=fb)
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        reps = 20
+        torch.cuda.synchronize()
+        e0.record()
+        for _ in range(reps):
+            vol.render(cam, [light], fb=fb)
+        e1.record()
+        torch.cuda.synchronize()
+        ms = e0.elapsed_time(e1) / reps
+        out["coherent" if coherent else "plain"] = {"value": samples / (ms * 1e-3),
+                                                    "ms_per_frame": ms, "samples": samples}
+    if with_cpu:
+        from oracle import refpy
+        if refpy.available():
+            r = refpy.RefHexMesh(m.order, m.ctrl_idx, m.xyz, m.field)
+            cam9 = np.array([*c["pos"], *c["look_at"], *c["up"]], np.float32)
+            args = (256, 256, cam9, c["fov"], 500, True, 256, np.array(meshgen.TF_RGB, np.float32),
+                    np.array(meshgen.TF_ALPHA, np.float32), light.as13()[None])
+            r.volume(*args)  # builds the reference BVH
+            t0 = time.perf_counter()
+            r.volume(*args)
+            cpu_s = time.perf_counter() - t0
+            n = out["plain"]["samples"]
+            out["cpu_reference"] = {"value": n / cpu_s, "unit": "samples/s", "seconds": cpu_s,
+                                    "cores": refpy.num_threads(), "kind": "reference",
+                                    "sample": "the whole frame; samples counted by the GPU "
+                                              "march (same located samples)"}
+    return out
+
+
 def orbit_cameras(count, width, seed=5):
     """Orbits about the mesh centre at the distance of the (2.5,2.5,2.5)
     camera: azimuth k * 22.5 degrees plus a seeded elevation jitter."""
@@ -601,6 +664,13 @@ def main():
         except Exception as exc:
             vol = {"error": repr(exc)}
 
+    vol_c0 = None
+    if not args.no_volume:
+        try:
+            vol_c0 = volume_c0(dev, rank == 0 and world == 1 and not args.no_cpu_baseline)
+        except Exception as exc:
+            vol_c0 = {"error": repr(exc)}
+
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         try:
@@ -650,6 +720,7 @@ def main():
                         "note": "Morton-ordered persistent kernel, element-centre guess"},
             "learned": learned,
             "volume": vol,
+            "volume_c0": vol_c0,
             "bvh_build_ms": bvh_build_ms, "tune_ms": tune_ms,
             "cpu_baseline": cpu,
         }

@@ -403,36 +403,137 @@ constexpr float kCoherentMargin = 0.1f;
 // Locate one sample.  Coherent mode first tries the previous sample's
 // element, starting from a predictor step r_prev + J^-1 (pt - pt_prev) with
 // the previous solve's Jacobian (lu), so that the solve usually converges in
-// two steps; then, or in plain mode, the full BVH locate (same acceptance
-// rule either way).  On success lu holds the located solve's Jacobian.
+// two steps; then, or in plain mode, the BVH candidates in the reference's
+// order (same acceptance rule either way).  All candidates go through one
+// Newton call site, which keeps the kernel's code small.  On success lu
+// holds the located solve's Jacobian.
 template <int P, bool WIDE>
 DRB_D int locate_sample (const VolumeParams &vp, const float (&pt)[3], const float (&step)[3],
                          int prev_el, const float (&prev_ref)[3], LU3 &lu, float (&ref)[3],
                          int &iters, int &cands, int &nodes)
 {
+  int todo[TraversalStack<WIDE>::kDepth];
+  int sp = 0, cur = 0;
+  todo[0] = kBarrier;
+  int el = -1, leaf = -1;
+  float x[3];
   if (vp.coherent && prev_el >= 0)
   {
     float dr[3];
     lu.solve (step, dr);
-    float x[3] = { prev_ref[0] + dr[0], prev_ref[1] + dr[1], prev_ref[2] + dr[2] };
-    if (is_inside_ref (x, kCoherentMargin))
+    x[0] = prev_ref[0] + dr[0];
+    x[1] = prev_ref[1] + dr[1];
+    x[2] = prev_ref[2] + dr[2];
+    if (is_inside_ref (x, kCoherentMargin)) el = prev_el;
+  }
+  while (true)
+  {
+    if (el < 0)
     {
-      int steps = 0;
-      ++cands;
-      const bool found = solve_in_element<P> (vp.lp, prev_el, pt, x, steps, lu);
-      iters += steps;
-      if (found)
-      {
-        ref[0] = x[0];
-        ref[1] = x[1];
-        ref[2] = x[2];
-        return prev_el;
-      }
+      leaf = next_leaf<WIDE> (vp.lp.nodes, vp.lp.wide, pt, todo, sp, cur, nodes);
+      if (leaf < 0) return -1;
+      el = __ldg (vp.lp.leaf_nodes + leaf);
+      bool given;
+      candidate_guess (vp.lp, leaf, 0, false, x, given);
+    }
+    int steps = 0;
+    ++cands;
+    // order 2 and 3 rows are read through L1: keeping 81+ values in
+    // registers would halve the resident warps of this kernel
+    const bool found = solve_in_element<P, (P == 1)> (vp.lp, el, pt, x, steps, lu);
+    iters += steps;
+    if (found)
+    {
+      ref[0] = x[0];
+      ref[1] = x[1];
+      ref[2] = x[2];
+      return el;
+    }
+    el = -1;
+    if (leaf >= 0)
+    {
+      cur = todo[sp];
+      --sp;
     }
   }
-  return locate_point<P, WIDE> (vp.lp, 0, pt, ref, iters, cands, nodes, lu);
 }
 
+// One ray's march (integrate_partials, volume.cpp:71-228) as a state that
+// advances one sample at a time, so a lane whose ray ends takes the next
+// ray at once instead of idling until the warp's longest ray ends.
+struct RayMarch
+{
+  Ray ray;
+  int i;              // ray index, -1: lane idle
+  float distance;     // position of the next sample
+  int segment;        // partials written so far (at most 5)
+  bool in_seg;        // inside a run of located samples
+  float seg_depth;
+  float4 color;       // the current segment's blend
+  float4 pixel;       // partials composited front to back (Volume::save)
+  float first_depth;
+  int prev_el;
+  float prev_ref[3];
+  int n_samples, iters, cands, nodes;
+};
+
+// End of a run of located samples: write the partial and composite it
+// behind the earlier ones (Volume::save order).
+DRB_D void end_segment (RayMarch &s, VolumePartial *__restrict__ partials)
+{
+  constexpr int kMaxSegments = 5;
+  if (partials)
+  {
+    VolumePartial part;
+    part.pixel_id = s.ray.pixel_id;
+    part.depth = s.seg_depth;
+    part.color[0] = s.color.x;
+    part.color[1] = s.color.y;
+    part.color[2] = s.color.z;
+    part.color[3] = s.color.w;
+    partials[(size_t)kMaxSegments * s.i + s.segment] = part;
+  }
+  if (s.segment == 0)
+  {
+    s.pixel = s.color;
+    s.first_depth = s.seg_depth;
+  }
+  else
+  {
+    const float a = 1.f - s.pixel.w;
+    s.pixel.x = s.pixel.x + s.color.x * a;
+    s.pixel.y = s.pixel.y + s.color.y * a;
+    s.pixel.z = s.pixel.z + s.color.z * a;
+    s.pixel.w = s.pixel.w + s.color.w * a;
+  }
+  ++s.segment;
+  s.in_seg = false;
+}
+
+DRB_D void finish_ray (RayMarch &s, float4 *__restrict__ fb_color, float *__restrict__ fb_depth,
+                       int *__restrict__ ray_samples, int *__restrict__ ray_iters,
+                       int *__restrict__ ray_cands)
+{
+  if (fb_color && s.segment > 0)
+  {
+    fb_color[s.ray.pixel_id] = s.pixel;
+    if (fb_depth) fb_depth[s.ray.pixel_id] = s.first_depth;
+  }
+  if (ray_samples) ray_samples[s.i] = s.n_samples;
+  if (ray_iters) ray_iters[s.i] = s.iters;
+  if (ray_cands) ray_cands[s.i] = s.cands;
+  s.i = -1;
+}
+
+// Persistent march: warps pop chunks of rays from a global queue and keep
+// every lane on a ray (ballot refill, as the batched locate does with
+// queries).  Each loop iteration advances every busy lane by one sample:
+// locate (coherent or full), shade, blend, and the segment and ray
+// termination rules of integrate_partials: a segment ends at the first
+// sample not located, at the ray's far distance or when its alpha reaches
+// 0.95; the ray ends after 5 segments, at far, or when alpha exceeds 0.95.
+// Partials go to slot 5 i + segment of ray i and the framebuffer pixel gets
+// their front-to-back composite, so the processing order changes nothing.
 template <int P, bool WIDE>
 __global__ void __launch_bounds__ (128)
 volume_kernel (VolumeParams vp, const Ray *__restrict__ rays, int n_rays, int *__restrict__ queue,
@@ -441,111 +542,115 @@ volume_kernel (VolumeParams vp, const Ray *__restrict__ rays, int n_rays, int *_
                int *__restrict__ ray_iters, int *__restrict__ ray_cands)
 {
   constexpr int kMaxSegments = 5; // volume.cpp:110
+  constexpr int kChunk = 32;
   const unsigned FULL = 0xffffffffu;
   const int lane = threadIdx.x & 31;
+  const unsigned lt = (1u << lane) - 1u;
+  int pool_next = 0, pool_end = 0; // warp-uniform
+  bool exhausted = false;          // warp-uniform
+  RayMarch s;
+  s.i = -1;
+  LU3 lu;
+  float step[3] = { 0.f, 0.f, 0.f };
   while (true)
   {
-    int base = 0;
-    if (lane == 0) base = atomicAdd (queue, 32);
-    base = __shfl_sync (FULL, base, 0);
-    if (base >= n_rays) break;
-    const int i = base + lane;
-    if (i >= n_rays) continue;
-    Ray ray = rays[i];
-    if (vp.cull)
+    // ---- give idle lanes the next rays of the warp's chunk ----
+    unsigned need = __ballot_sync (FULL, s.i < 0);
+    while (need != 0u && !exhausted)
     {
-      // mark_active + calc_ray_start (ray.cpp:117-241) on the raw ray
-      float t0, t1;
-      if (!slab (ray, vp.box, t0, t1))
+      if (pool_next >= pool_end)
       {
-        if (ray_samples) ray_samples[i] = 0;
-        if (ray_iters) ray_iters[i] = 0;
-        if (ray_cands) ray_cands[i] = 0;
-        continue;
+        int base = 0;
+        if (lane == 0) base = atomicAdd (queue, kChunk);
+        base = __shfl_sync (FULL, base, 0);
+        if (base >= n_rays)
+        {
+          exhausted = true;
+          break;
+        }
+        pool_next = base;
+        pool_end = min (base + kChunk, n_rays);
       }
-      ray.near_t = t0;
-      ray.far_t = t1;
+      const int avail = pool_end - pool_next;
+      const int rank = __popc (need & lt);
+      if (s.i < 0 && rank < avail)
+      {
+        s.i = pool_next + rank;
+        s.ray = rays[s.i];
+        bool live = true;
+        if (vp.cull)
+        {
+          // mark_active + calc_ray_start (ray.cpp:117-241) on the raw ray
+          float t0, t1;
+          live = slab (s.ray, vp.box, t0, t1);
+          s.ray.near_t = t0;
+          s.ray.far_t = t1;
+        }
+        s.distance = s.ray.near_t + vp.sample_dist;
+        s.segment = 0;
+        s.in_seg = false;
+        s.color = make_float4 (0.f, 0.f, 0.f, 0.f);
+        s.pixel = make_float4 (0.f, 0.f, 0.f, 0.f);
+        s.first_depth = INFINITY;
+        s.seg_depth = 0.f;
+        s.prev_el = -1;
+        s.prev_ref[0] = s.prev_ref[1] = s.prev_ref[2] = 0.5f;
+        s.n_samples = s.iters = s.cands = s.nodes = 0;
+        step[0] = s.ray.dir.x * vp.sample_dist;
+        step[1] = s.ray.dir.y * vp.sample_dist;
+        step[2] = s.ray.dir.z * vp.sample_dist;
+        if (!live || !(s.distance < s.ray.far_t))
+          finish_ray (s, fb_color, fb_depth, ray_samples, ray_iters, ray_cands);
+      }
+      pool_next += min (__popc (need), avail);
+      need = __ballot_sync (FULL, s.i < 0);
     }
-    float distance = ray.near_t + vp.sample_dist;
-    int segment = 0;
-    float4 pixel = make_float4 (0.f, 0.f, 0.f, 0.f);
-    float first_depth = INFINITY;
-    int n_samples = 0, iters = 0, cands = 0, nodes = 0;
-    int prev_el = -1;
-    float prev_ref[3] = { 0.5f, 0.5f, 0.5f };
-    LU3 lu;
-    // displacement between consecutive samples, for the coherent predictor
-    const float step[3] = { ray.dir.x * vp.sample_dist, ray.dir.y * vp.sample_dist,
-                            ray.dir.z * vp.sample_dist };
-    for (int s = 0; s < kMaxSegments; ++s)
+    if (__ballot_sync (FULL, s.i >= 0) == 0u) break;
+    if (s.i < 0) continue;
+
+    // ---- one sample of this lane's ray ----
+    const float pt[3] = { s.ray.orig.x + s.distance * s.ray.dir.x,
+                          s.ray.orig.y + s.distance * s.ray.dir.y,
+                          s.ray.orig.z + s.distance * s.ray.dir.z };
+    float ref[3];
+    const int el = locate_sample<P, WIDE> (vp, pt, step, s.prev_el, s.prev_ref, lu, ref, s.iters,
+                                           s.cands, s.nodes);
+    bool done = false;
+    if (el >= 0)
     {
-      bool found = false;
-      int el = -1;
-      float ref[3];
-      float pt[3];
-      while (distance < ray.far_t && !found)
+      if (!s.in_seg)
       {
-        pt[0] = ray.orig.x + distance * ray.dir.x;
-        pt[1] = ray.orig.y + distance * ray.dir.y;
-        pt[2] = ray.orig.z + distance * ray.dir.z;
-        el = locate_sample<P, WIDE> (vp, pt, step, prev_el, prev_ref, lu, ref, iters, cands, nodes);
-        if (el != -1) found = true;
-        else distance += vp.sample_dist;
-        prev_el = el;
+        s.in_seg = true;
+        s.seg_depth = s.distance;
+        s.color = make_float4 (0.f, 0.f, 0.f, 0.f);
       }
-      if (distance >= ray.far_t) break;
-      VolumePartial part;
-      part.pixel_id = ray.pixel_id;
-      part.depth = distance;
-      float4 color = make_float4 (0.f, 0.f, 0.f, 0.f);
-      do
+      ++s.n_samples;
+      const float4 sc = shade_sample<P> (vp, el, ref, s.ray, lu, pt);
+      blend (s.color, sc);
+      s.prev_el = el;
+      s.prev_ref[0] = ref[0];
+      s.prev_ref[1] = ref[1];
+      s.prev_ref[2] = ref[2];
+      s.distance += vp.sample_dist;
+      if (!(s.distance < s.ray.far_t) || !(s.color.w < 0.95f))
       {
-        ++n_samples;
-        const float4 sc = shade_sample<P> (vp, el, ref, ray, lu, pt);
-        blend (color, sc);
-        prev_el = el;
-        prev_ref[0] = ref[0];
-        prev_ref[1] = ref[1];
-        prev_ref[2] = ref[2];
-        distance += vp.sample_dist;
-        pt[0] = ray.orig.x + distance * ray.dir.x;
-        pt[1] = ray.orig.y + distance * ray.dir.y;
-        pt[2] = ray.orig.z + distance * ray.dir.z;
-        el = locate_sample<P, WIDE> (vp, pt, step, prev_el, prev_ref, lu, ref, iters, cands, nodes);
-        found = el != -1;
-        if (!found) prev_el = -1;
-      } while (distance < ray.far_t && found && color.w < 0.95f);
-      part.color[0] = color.x;
-      part.color[1] = color.y;
-      part.color[2] = color.z;
-      part.color[3] = color.w;
-      if (partials) partials[(size_t)kMaxSegments * i + segment] = part;
-      // fused Volume::save compositing: partials of one ray arrive in depth
-      // order, the first one sets the pixel, later ones blend behind it
-      if (segment == 0)
-      {
-        pixel = color;
-        first_depth = part.depth;
+        const float alpha = s.color.w;
+        end_segment (s, partials);
+        done = !(s.distance < s.ray.far_t) || alpha > 0.95f || s.segment == kMaxSegments;
       }
-      else
-      {
-        const float a = 1.f - pixel.w;
-        pixel.x = pixel.x + color.x * a;
-        pixel.y = pixel.y + color.y * a;
-        pixel.z = pixel.z + color.z * a;
-        pixel.w = pixel.w + color.w * a;
-      }
-      ++segment;
-      if (distance >= ray.far_t || color.w > 0.95f) break;
     }
-    if (fb_color && segment > 0)
+    else
     {
-      fb_color[ray.pixel_id] = pixel;
-      if (fb_depth) fb_depth[ray.pixel_id] = first_depth;
+      s.prev_el = -1;
+      if (s.in_seg)
+      {
+        end_segment (s, partials);
+        done = s.segment == kMaxSegments;
+      }
+      s.distance += vp.sample_dist;
+      if (!(s.distance < s.ray.far_t)) done = true;
     }
-    if (ray_samples) ray_samples[i] = n_samples;
-    if (ray_iters) ray_iters[i] = iters;
-    if (ray_cands) ray_cands[i] = cands;
+    if (done) finish_ray (s, fb_color, fb_depth, ray_samples, ray_iters, ray_cands);
   }
 }
 
