@@ -27,7 +27,8 @@ GUESS_GIVEN = 3
 class DrbMesh(C.Structure):
     _fields_ = [("dim", C.c_int), ("order", C.c_int), ("ncomp", C.c_int),
                 ("n_elem", C.c_int), ("n_ctrl", C.c_int),
-                ("ctrl_idx", C.c_void_p), ("values", C.c_void_p), ("packed", C.c_void_p)]
+                ("ctrl_idx", C.c_void_p), ("values", C.c_void_p), ("packed", C.c_void_p),
+                ("face_neighbors", C.c_void_p)]
 
 
 class DrbBvh(C.Structure):
@@ -141,6 +142,7 @@ _SIGS = {
     "drb_radix_sort_pairs": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p,
                                        C.c_int, C.c_int, C.c_void_p]),
     "drb_lbvh_build": (C.c_int, [C.POINTER(DrbMesh), C.POINTER(DrbBvh), C.c_void_p, C.c_void_p]),
+    "drb_mesh_face_neighbors": (C.c_int, [C.POINTER(DrbMesh), C.c_void_p, C.c_void_p]),
     "drb_bvh_widen": (C.c_int, [C.POINTER(DrbBvh), C.c_void_p, C.c_int, C.c_void_p]),
     "drb_locate": (C.c_int, [C.POINTER(DrbMesh), C.POINTER(DrbBvh), C.c_void_p, C.c_int,
                              C.POINTER(DrbNewtonOpts), C.c_void_p, C.c_void_p, DrbQueryStats,

@@ -113,6 +113,7 @@ class UnstructuredMesh:
                                      _dev(xyz, torch.float32, device).reshape(-1, 3), nd)
         self.device = torch.device(device)
         self.packed = None
+        self._neighbors = None
         self._bvh = None
         if pack:
             self.pack()
@@ -132,7 +133,21 @@ class UnstructuredMesh:
         m.ctrl_idx = self.dof_data.ctrl_idx.data_ptr()
         m.values = self.dof_data.values.data_ptr()
         m.packed = self.packed.data_ptr() if (packed and self.packed is not None) else None
+        nb = getattr(self, "_neighbors", None)
+        m.face_neighbors = nb.data_ptr() if nb is not None else None
         return m
+
+    def face_neighbors(self, stream=None):
+        """Element across each of the six faces of every element (-1 on the
+        boundary), built once (drb_mesh_face_neighbors); the volume march
+        follows rays across faces with it."""
+        if getattr(self, "_neighbors", None) is None:
+            nb = torch.empty((max(self.n_elem, 1), 6), dtype=torch.int32, device=self.device)
+            d = self.desc()
+            L.check(L.lib().drb_mesh_face_neighbors(C.byref(d), _ptr(nb), _stream(stream)),
+                    "drb_mesh_face_neighbors")
+            self._neighbors = nb
+        return self._neighbors
 
     def pack(self, stream=None):
         stride = L.lib().drb_packed_stride(self.dim, self.order, 3)

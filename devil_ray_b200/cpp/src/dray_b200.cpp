@@ -59,7 +59,7 @@ struct DeviceGeometry
   bool has_bvh = false;
   drb_bvh bvh{};
   DevBuf<float> inner, refb, wide;
-  DevBuf<int32> leaf, ids;
+  DevBuf<int32> leaf, ids, nbr;
 };
 
 // ------------------------------------------------------------ meshes --
@@ -121,6 +121,10 @@ const drb_bvh *TensorMesh::device_bvh ()
       drb_check (drb_bvh_widen (&g.bvh, nullptr, 0, nullptr), "drb_bvh_widen");
       g.wide.alloc ((size_t)32 * g.bvh.n_wide);
       drb_check (drb_bvh_widen (&g.bvh, g.wide.p, g.bvh.n_wide, nullptr), "drb_bvh_widen");
+      // face neighbours: the volume march steps across faces with them
+      g.nbr.alloc ((size_t)6 * cells ());
+      drb_check (drb_mesh_face_neighbors (&g.mesh, g.nbr.p, nullptr), "drb_mesh_face_neighbors");
+      g.mesh.face_neighbors = g.nbr.p;
     }
     g.has_bvh = true;
   }

@@ -274,6 +274,7 @@ struct VolumeParams
   float sample_dist;
   int cull;
   CullBox box;
+  const int *nbr;             // face neighbours (6 per element) or NULL
 };
 
 template <int P> struct FieldCP
@@ -407,6 +408,48 @@ constexpr float kCoherentMargin = 0.1f;
 // order (same acceptance rule either way).  All candidates go through one
 // Newton call site, which keeps the kernel's code small.  On success lu
 // holds the located solve's Jacobian.
+// Face by which a reference point outside [0,1]^3 leaves the element (the
+// axis with the largest excursion; faces u0, u1, v0, v1, w0, w1), -1 inside.
+DRB_D int exit_face (const float (&x)[3])
+{
+  int f = -1;
+  float worst = 0.f;
+#pragma unroll
+  for (int d = 0; d < 3; ++d)
+  {
+    if (-x[d] > worst)
+    {
+      worst = -x[d];
+      f = 2 * d;
+    }
+    if (x[d] - 1.f > worst)
+    {
+      worst = x[d] - 1.f;
+      f = 2 * d + 1;
+    }
+  }
+  return f;
+}
+
+// The element across face f, and the guess carried over into its frame
+// (the structured-lattice case: the same axes, shifted by one).
+DRB_D int step_across (const VolumeParams &vp, int el, int f, float (&x)[3])
+{
+  if (f < 0 || !vp.nbr) return -1;
+  const int nb = __ldg (vp.nbr + 6 * (size_t)el + f);
+  if (nb >= 0) x[f >> 1] += (f & 1) ? -1.f : 1.f;
+  return nb;
+}
+
+// Locate one sample.  Coherent mode first tries the previous sample's
+// element, starting from a predictor step r_prev + J^-1 (pt - pt_prev) with
+// the previous solve's Jacobian (lu), so that the solve usually converges in
+// two steps.  When the prediction (or that solve) leaves the element, the
+// element across the exit face is tried once (face-neighbour table).  Then,
+// or in plain mode, the BVH candidates in the reference's order; the same
+// acceptance rule throughout.  All candidates go through one Newton call
+// site, which keeps the kernel's code small.  On success lu holds the
+// located solve's Jacobian.
 template <int P, bool WIDE>
 DRB_D int locate_sample (const VolumeParams &vp, const float (&pt)[3], const float (&step)[3],
                          int prev_el, const float (&prev_ref)[3], LU3 &lu, float (&ref)[3],
@@ -416,6 +459,7 @@ DRB_D int locate_sample (const VolumeParams &vp, const float (&pt)[3], const flo
   int sp = 0, cur = 0;
   todo[0] = kBarrier;
   int el = -1, leaf = -1;
+  bool crossed = false; // the one face step of this sample is used
   float x[3];
   if (vp.coherent && prev_el >= 0)
   {
@@ -424,7 +468,15 @@ DRB_D int locate_sample (const VolumeParams &vp, const float (&pt)[3], const flo
     x[0] = prev_ref[0] + dr[0];
     x[1] = prev_ref[1] + dr[1];
     x[2] = prev_ref[2] + dr[2];
-    if (is_inside_ref (x, kCoherentMargin)) el = prev_el;
+    if (is_inside_ref (x, kCoherentMargin))
+    {
+      el = prev_el;
+    }
+    else
+    {
+      el = step_across (vp, prev_el, exit_face (x), x);
+      crossed = true;
+    }
   }
   while (true)
   {
@@ -448,6 +500,13 @@ DRB_D int locate_sample (const VolumeParams &vp, const float (&pt)[3], const flo
       ref[1] = x[1];
       ref[2] = x[2];
       return el;
+    }
+    if (leaf < 0 && !crossed)
+    {
+      // the previous element's solve ended outside it: step across
+      crossed = true;
+      el = step_across (vp, el, exit_face (x), x);
+      if (el >= 0) continue;
     }
     el = -1;
     if (leaf >= 0)
@@ -1014,6 +1073,7 @@ static int volume_common (const drb_mesh *mesh, const drb_mesh *field, const drb
   vp.field_idx = field->ctrl_idx;
   vp.field_vals = field->values;
   vp.fstride = packed_stride (nd, 1);
+  vp.nbr = mesh->face_neighbors;
   vp.tf = (const float4 *)tf;
   vp.tf_size = tf_size;
   // DeviceColorMap: range of the field's control values, rcp_safe(length)

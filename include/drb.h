@@ -61,7 +61,18 @@ typedef struct drb_mesh
   const float *values;   /* device float[n_ctrl * ncomp] */
   const float *packed;   /* optional device float[n_elem * drb_packed_stride()]:
                             element-major copy made by drb_pack_elements(), or NULL */
+  const int *face_neighbors; /* optional device int32[6 * n_elem] of a hex geometry
+                            mesh (drb_mesh_face_neighbors), or NULL */
 } drb_mesh;
+
+/* Face neighbours of a hex mesh (no reference counterpart; faces are
+ * matched by their four corner control points, as MeshBoundary matches
+ * them, mesh_utils.cpp:98-398): neighbors[6 e + f] is the element across
+ * face f of element e (f = u0, u1, v0, v1, w0, w1), -1 on the boundary.
+ * The volume march uses it (through drb_mesh.face_neighbors) to step into
+ * the next element across the face a ray leaves by before searching the
+ * BVH. */
+int drb_mesh_face_neighbors (const drb_mesh *mesh, int *neighbors, void *stream);
 
 /* Linear BVH in the reference's layout (bvh.hpp:16-37, device_bvh.hpp:15-28). */
 typedef struct drb_bvh

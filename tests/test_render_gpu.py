@@ -128,3 +128,37 @@ def test_volume_wide_traversal_identical(cuda):
             imgs.append(fb.image())
     assert np.array_equal(imgs[0].view(np.int32), imgs[1].view(np.int32))
     assert np.array_equal(imgs[2].view(np.int32), imgs[3].view(np.int32))
+
+
+def test_face_neighbors(cuda):
+    """Face-neighbour table: 6 n^2 boundary faces on an n^3 mesh, and every
+    neighbour across face f shares that face's four corners as its own
+    opposite face (the lattice keeps the axes)."""
+    import torch
+    from devil_ray_b200 import api, meshgen
+    n, p = 5, 3
+    m = meshgen.warped_mesh(n, p, 0.05)
+    g = api.UnstructuredMesh(m.ctrl_idx, m.xyz, m.order, device=cuda)
+    nb = g.face_neighbors().cpu().numpy()
+    torch.cuda.synchronize()
+    assert nb.shape == (n ** 3, 6)
+    assert (nb < 0).sum() == 6 * n * n
+    conn = np.asarray(m.ctrl_idx).reshape(-1, (p + 1) ** 3)
+    n1 = p + 1
+
+    def corners(e, f):
+        axis, side = f // 2, (f % 2) * p
+        out = []
+        for s in (0, p):
+            for r in (0, p):
+                abc = [0, 0, 0]
+                abc[axis], abc[(axis + 1) % 3], abc[(axis + 2) % 3] = side, s, r
+                out.append(conn[e, (abc[2] * n1 + abc[1]) * n1 + abc[0]])
+        return sorted(out)
+
+    for e in range(n ** 3):
+        for f in range(6):
+            o = nb[e, f]
+            if o >= 0:
+                assert o != e and nb[o, f ^ 1] == e
+                assert corners(e, f) == corners(o, f ^ 1)
