@@ -10,7 +10,9 @@ element: plain Newton from the element centre remains the fallback whenever
 the guessed solve does not converge.
 
 Pipeline per batch of queries (LearnedLocator.locate):
-  drb_query_order       Morton order of the queries
+  drb_query_order       Morton order of the queries (the points are then
+                        gathered into that order, and the results scattered
+                        back at the end)
   drb_first_candidates  first candidate leaf of every query (traversal only)
   drb_mlp_guess         fused tensor-core inference on (query, element) pairs
   drb_locate_hinted     persistent locate starting at the hinted candidate
@@ -240,25 +242,36 @@ class LearnedLocator:
         bvh = self.mesh.get_bvh()
         if order is None:
             order = self._order.order(pts, stream)
+        # Work on a Morton-ordered copy of the points: the first-candidate
+        # traversal, the guess network and the hinted locate then read and
+        # write contiguous arrays, and one scatter puts the results back in
+        # input order (each query's result does not depend on the order).
+        ol = order.long()
+        pts_s = pts.index_select(0, ol)
         first_leaf = torch.empty(n, dtype=torch.int32, device=dev)
         first_elem = torch.empty(n, dtype=torch.int32, device=dev)
-        L.check(_lib().drb_first_candidates(C.byref(bvh.desc()), _ptr(pts), n, _ptr(order),
+        L.check(_lib().drb_first_candidates(C.byref(bvh.desc()), _ptr(pts_s), n, None,
                                             _ptr(first_leaf), _ptr(first_elem), _stream(stream)),
                 "drb_first_candidates")
-        guess = self.model.guess(self.mesh, first_elem, pts, order, stream)
+        guess = self.model.guess(self.mesh, first_elem, pts_s, None, stream)
         if out is None:
             cell = torch.empty(n, dtype=torch.int32, device=dev)
             ref = torch.empty((n, 3), dtype=torch.float32, device=dev)
         else:
             cell, ref = out
+        cell_s = torch.empty(n, dtype=torch.int32, device=dev)
+        ref_s = torch.empty((n, 3), dtype=torch.float32, device=dev)
         st = [torch.empty(n, dtype=torch.int32, device=dev) for _ in range(3)] if stats else None
         qs = L.DrbQueryStats(*(t.data_ptr() for t in st)) if stats else L.DrbQueryStats()
         opts = L.DrbNewtonOpts(self.tol, self.max_steps, L.GUESS_GIVEN, guess.data_ptr())
         cfg = None if self.config is None else C.byref(self.config)
         L.check(_lib().drb_locate_hinted(C.byref(self.mesh.desc()), C.byref(bvh.desc()),
-                                         _ptr(pts), n, _ptr(order), _ptr(first_leaf),
-                                         C.byref(opts), cfg, _ptr(cell), _ptr(ref), qs,
+                                         _ptr(pts_s), n, None, _ptr(first_leaf),
+                                         C.byref(opts), cfg, _ptr(cell_s), _ptr(ref_s), qs,
                                          _stream(stream)), "drb_locate_hinted")
+        cell.index_copy_(0, ol, cell_s)
+        ref.index_copy_(0, ol, ref_s)
         if stats:
+            st = [torch.empty_like(t).index_copy_(0, ol, t) for t in st]
             return cell, ref, st[0], st[1], st[2]
         return cell, ref
