@@ -244,7 +244,7 @@ extern "C" int drb_locate_hinted (const drb_mesh *mesh, const drb_bvh *bvh, cons
   lp.guess_mode = opts->guess_mode;
   lp.guess = opts->guess;
   int nb = 0;
-  const bool reg = cfg.reg_elements != 0 && mesh->order <= 2;
+  const bool reg = cfg.reg_elements == 1 && mesh->order <= 2; // the register row mode
   const bool wide = lp.wide != nullptr;
 #define DRB_HFN(W) (mesh->order == 1 ? (reg ? (const void *)locate_hinted_kernel<1, true, W> : (const void *)locate_hinted_kernel<1, false, W>) \
                    : mesh->order == 2 ? (reg ? (const void *)locate_hinted_kernel<2, true, W> : (const void *)locate_hinted_kernel<2, false, W>) \
