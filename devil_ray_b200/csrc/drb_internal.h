@@ -77,7 +77,10 @@ struct LocateWorkspace
   int *iota;
   int *order;
   RadixWorkspace radix;
+  int *hist; // query_cell_count() cell counts of the query order
 };
+// Cells of the query order (counting sort over Morton cells).
+int query_cell_count ();
 int locate_batched_ws (const drb_mesh *mesh, const drb_bvh *bvh, const float *pts, int n,
                        const drb_newton_opts *opts, const drb_locate_config *cfg,
                        const LocateWorkspace &ws, int *cell, float *ref, drb_query_stats stats,

@@ -4,9 +4,9 @@
 // (data_model/unstructured_mesh.cpp:137-148): warps mix points from
 // unrelated parts of the mesh, and every lane waits for the slowest lane's
 // traversal and Newton iterations.  This path instead
-//   1. sorts the queries along a 30-bit Morton curve over the BVH bounds
-//      (query_codes_kernel + the radix sort), so a warp's lanes follow
-//      nearly the same BVH path and hit the same few elements (L1/L2 reuse);
+//   1. orders the queries by Morton cell (6 bits per axis over the BVH
+//      bounds, a counting sort), so a warp's lanes follow nearly the same
+//      BVH path and hit the same few elements (L1/L2 reuse);
 //   2. runs a persistent kernel, grid sized to the resident capacity of the
 //      148 SMs, whose warps pop chunks of sorted queries from a global atomic
 //      queue;
@@ -31,9 +31,20 @@ namespace drb
 namespace
 {
 
-__global__ void query_codes_kernel (const float *__restrict__ pts, int n, float x0, float y0,
-                                    float z0, float sx, float sy, float sz,
-                                    unsigned *__restrict__ codes, int *__restrict__ iota)
+// Query order by counting sort into Morton cells of 6 bits per axis
+// (2^18 cells over the BVH bounds; one cell is about one element of a 64^3
+// mesh).  The persistent kernel needs spatially coherent warps, not a
+// sorted sequence, so the order inside a cell is whatever the atomics give:
+// one counting pass, a scan of the cell counts and one scatter replace the
+// four passes of a 30-bit radix sort.  Every query's result is independent
+// of the order.
+constexpr int kCellBits = 6;
+constexpr int kCells = 1 << (3 * kCellBits);
+
+__global__ void cell_count_kernel (const float *__restrict__ pts, int n, float x0, float y0,
+                                   float z0, float sx, float sy, float sz,
+                                   unsigned *__restrict__ cell_of, int *__restrict__ rank,
+                                   int *__restrict__ hist)
 {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= n) return;
@@ -44,16 +55,58 @@ __global__ void query_codes_kernel (const float *__restrict__ pts, int n, float 
   for (int k = 0; k < 3; ++k)
   {
     float t = (pts[3 * (size_t)i + k] - lo[k]) * sc[k];
-    t = fminf (fmaxf (t * 1024.f, 0.f), 1023.f);
-    unsigned x = (t == t) ? (unsigned)t : 0u; // NaN queries sort first
-    x = (x | (x << 16)) & 0x030000FFu;
+    t = fminf (fmaxf (t * (float)(1 << kCellBits), 0.f), (float)((1 << kCellBits) - 1));
+    unsigned x = (t == t) ? (unsigned)t : 0u; // NaN queries go to cell 0
     x = (x | (x << 8)) & 0x0300F00Fu;
     x = (x | (x << 4)) & 0x030C30C3u;
     x = (x | (x << 2)) & 0x09249249u;
     e[k] = x;
   }
-  codes[i] = (e[2] << 2) | (e[1] << 1) | e[0];
-  iota[i] = i;
+  const unsigned c = (e[2] << 2) | (e[1] << 1) | e[0];
+  cell_of[i] = c;
+  rank[i] = atomicAdd (hist + c, 1);
+}
+
+__global__ void cell_scatter_kernel (const unsigned *__restrict__ cell_of, const int *__restrict__ rank,
+                                     const int *__restrict__ offset, int n, int *__restrict__ order)
+{
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  order[__ldg (offset + cell_of[i]) + rank[i]] = i;
+}
+
+// The BVH bounds as the cell grid's origin and inverse extents.
+void order_frame (const drb_bvh *bvh, float (&lo)[3], float (&sc)[3])
+{
+  const float *b = bvh->bounds;
+  for (int k = 0; k < 3; ++k)
+  {
+    const float ext = b[2 * k + 1] - b[2 * k];
+    sc[k] = (ext > 0.f && std::isfinite (ext)) ? 1.f / ext : 0.f;
+    lo[k] = std::isfinite (b[2 * k]) ? b[2 * k] : 0.f;
+  }
+}
+
+// order[0..n) over caller buffers: cell_of and rank hold n values, hist
+// kCells, scan_tmp scan_ws_ints(kCells).
+int cell_order (const drb_bvh *bvh, const float *pts, int n, int *order, unsigned *cell_of,
+                int *rank, int *hist, int *scan_tmp, cudaStream_t s)
+{
+  float lo[3], sc[3];
+  order_frame (bvh, lo, sc);
+  cudaError_t e = cudaMemsetAsync (hist, 0, sizeof (int) * kCells, s);
+  if (e != cudaSuccess)
+  {
+    set_last_error (cudaGetErrorString (e));
+    return status_from (e);
+  }
+  cell_count_kernel<<<div_up (n, 256), 256, 0, s>>> (pts, n, lo[0], lo[1], lo[2], sc[0], sc[1],
+                                                      sc[2], cell_of, rank, hist);
+  int st = check_launch ("cell_count_kernel");
+  if (st) return st;
+  if ((st = exclusive_scan_i32_ws (hist, hist, kCells, nullptr, scan_tmp, s))) return st;
+  cell_scatter_kernel<<<div_up (n, 256), 256, 0, s>>> (cell_of, rank, hist, n, order);
+  return check_launch ("cell_scatter_kernel");
 }
 
 // Element-row modes of the candidate solves (drb_locate_config.reg_elements)
@@ -348,27 +401,17 @@ drb_locate_config default_config (int order)
 } // namespace
 
 // Morton order of the queries over the BVH bounds (device int32 order[n]).
+int query_cell_count () { return kCells; }
+
 int query_morton_order (const drb_bvh *bvh, const float *pts, int n, int *order, cudaStream_t s)
 {
   Scratch scr (s);
-  unsigned *codes = scr.alloc<unsigned> (n);
-  unsigned *codes_sorted = scr.alloc<unsigned> (n);
-  int *iota = scr.alloc<int> (n);
+  unsigned *cell_of = scr.alloc<unsigned> (n);
+  int *rank = scr.alloc<int> (n);
+  int *hist = scr.alloc<int> (kCells);
+  int *tmp = scr.alloc<int> (scan_ws_ints (kCells));
   if (scr.err != cudaSuccess) return status_from (scr.err);
-  const float *b = bvh->bounds;
-  float sc[3];
-  for (int k = 0; k < 3; ++k)
-  {
-    const float ext = b[2 * k + 1] - b[2 * k];
-    sc[k] = (ext > 0.f && std::isfinite (ext)) ? 1.f / ext : 0.f;
-  }
-  const float lo[3] = { std::isfinite (b[0]) ? b[0] : 0.f, std::isfinite (b[2]) ? b[2] : 0.f,
-                        std::isfinite (b[4]) ? b[4] : 0.f };
-  query_codes_kernel<<<div_up (n, 256), 256, 0, s>>> (pts, n, lo[0], lo[1], lo[2], sc[0], sc[1],
-                                                       sc[2], codes, iota);
-  int st = check_launch ("query_codes_kernel");
-  if (st) return st;
-  return radix_sort_pairs (codes, iota, codes_sorted, order, n, 30, s);
+  return cell_order (bvh, pts, n, order, cell_of, rank, hist, tmp, s);
 }
 
 int locate_batched_impl (const drb_mesh *mesh, const drb_bvh *bvh, const float *pts, int n,
@@ -430,19 +473,7 @@ int locate_batched_ws (const drb_mesh *mesh, const drb_bvh *bvh, const float *pt
   const int *ord = nullptr;
   if (cfg.sort_queries)
   {
-    const float *b = bvh->bounds;
-    float sc[3];
-    for (int k = 0; k < 3; ++k)
-    {
-      const float ext = b[2 * k + 1] - b[2 * k];
-      sc[k] = (ext > 0.f && std::isfinite (ext)) ? 1.f / ext : 0.f;
-    }
-    const float lo[3] = { std::isfinite (b[0]) ? b[0] : 0.f, std::isfinite (b[2]) ? b[2] : 0.f,
-                          std::isfinite (b[4]) ? b[4] : 0.f };
-    query_codes_kernel<<<div_up (n, 256), 256, 0, s>>> (pts, n, lo[0], lo[1], lo[2], sc[0],
-                                                         sc[1], sc[2], ws.codes, ws.iota);
-    if ((st = check_launch ("query_codes_kernel"))) return st;
-    st = radix_sort_pairs_ws (ws.codes, ws.iota, ws.codes_sorted, ws.order, n, 30, ws.radix, s);
+    st = cell_order (bvh, pts, n, ws.order, ws.codes, ws.iota, ws.hist, ws.radix.scan_tmp, s);
     if (st) return st;
     ord = ws.order;
   }

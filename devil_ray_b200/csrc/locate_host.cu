@@ -35,8 +35,8 @@ struct Lane
 // stream-ordered pool; false (and the error set) if anything failed.
 bool open_lanes (Lane (&lane)[kLanes], int chunk, cudaEvent_t start, cudaError_t &e)
 {
-  const long long counts = radix_ws_counts (chunk);
-  const int scan_ints = scan_ws_ints ((int)counts);
+  const int cells = query_cell_count ();
+  const int scan_ints = scan_ws_ints (cells);
   const size_t q = (size_t)chunk;
   for (int l = 0; l < kLanes && e == cudaSuccess; ++l)
   {
@@ -44,25 +44,21 @@ bool open_lanes (Lane (&lane)[kLanes], int chunk, cudaEvent_t start, cudaError_t
     if (e == cudaSuccess) e = cudaEventCreateWithFlags (&lane[l].ready, cudaEventDisableTiming);
     // work queued on the caller's stream before this call comes first
     if (e == cudaSuccess) e = cudaStreamWaitEvent (lane[l].s, start, 0);
-    void *p[12] = {};
-    const size_t bytes[12] = { 3 * q * sizeof (float), q * sizeof (int), 3 * q * sizeof (float),
-                               sizeof (int), q * sizeof (unsigned), q * sizeof (unsigned),
-                               q * sizeof (int), q * sizeof (int), q * sizeof (unsigned),
-                               q * sizeof (int), sizeof (int) * (size_t)counts,
-                               sizeof (int) * (size_t)scan_ints };
-    for (int b = 0; b < 12 && e == cudaSuccess; ++b) e = cudaMallocAsync (&p[b], bytes[b], lane[l].s);
+    void *p[9] = {};
+    const size_t bytes[9] = { 3 * q * sizeof (float), q * sizeof (int), 3 * q * sizeof (float),
+                              sizeof (int), q * sizeof (unsigned), q * sizeof (int),
+                              q * sizeof (int), sizeof (int) * (size_t)cells,
+                              sizeof (int) * (size_t)scan_ints };
+    for (int b = 0; b < 9 && e == cudaSuccess; ++b) e = cudaMallocAsync (&p[b], bytes[b], lane[l].s);
     lane[l].pts = (float *)p[0];
     lane[l].cell = (int *)p[1];
     lane[l].ref = (float *)p[2];
     lane[l].ws.head = (int *)p[3];
     lane[l].ws.codes = (unsigned *)p[4];
-    lane[l].ws.codes_sorted = (unsigned *)p[5];
-    lane[l].ws.iota = (int *)p[6];
-    lane[l].ws.order = (int *)p[7];
-    lane[l].ws.radix.kbuf = (unsigned *)p[8];
-    lane[l].ws.radix.vbuf = (int *)p[9];
-    lane[l].ws.radix.counts = (int *)p[10];
-    lane[l].ws.radix.scan_tmp = (int *)p[11];
+    lane[l].ws.iota = (int *)p[5];
+    lane[l].ws.order = (int *)p[6];
+    lane[l].ws.hist = (int *)p[7];
+    lane[l].ws.radix.scan_tmp = (int *)p[8];
   }
   if (e != cudaSuccess) set_last_error (cudaGetErrorString (e));
   return e == cudaSuccess;
@@ -75,10 +71,9 @@ int close_lanes (Lane (&lane)[kLanes], cudaStream_t caller, int st)
   for (int l = 0; l < kLanes; ++l)
   {
     if (!lane[l].s) continue;
-    void *bufs[12] = { lane[l].pts, lane[l].cell, lane[l].ref, lane[l].ws.head, lane[l].ws.codes,
-                       lane[l].ws.codes_sorted, lane[l].ws.iota, lane[l].ws.order,
-                       lane[l].ws.radix.kbuf, lane[l].ws.radix.vbuf, lane[l].ws.radix.counts,
-                       lane[l].ws.radix.scan_tmp };
+    void *bufs[9] = { lane[l].pts, lane[l].cell, lane[l].ref, lane[l].ws.head, lane[l].ws.codes,
+                      lane[l].ws.iota, lane[l].ws.order, lane[l].ws.hist,
+                      lane[l].ws.radix.scan_tmp };
     for (void *b : bufs)
       if (b) cudaFreeAsync (b, lane[l].s);
     if (lane[l].ready)

@@ -14,7 +14,7 @@
 // Limits and sharing:
 //   - at most kNoAllocMaxQueries queries per call (larger calls are rejected
 //     with DRB_ERR_INVALID_ARG and a message);
-//   - the array (about 25 MB) is part of this library's device code and stays
+//   - the array (about 13 MB) is part of this library's device code and stays
 //     allocated on every device where it has been loaded, until the process
 //     exits;
 //   - every call on a device uses the same array: calls whose GPU work can
@@ -39,15 +39,13 @@ constexpr size_t align_up (size_t x) { return (x + kAlign - 1) / kAlign * kAlign
 constexpr size_t kQBytes = align_up (sizeof (int) * (size_t)kNoAllocMaxQueries);
 constexpr size_t kHeadOff = 0;
 constexpr size_t kCodesOff = kHeadOff + kAlign;
-constexpr size_t kSortedOff = kCodesOff + kQBytes;
-constexpr size_t kIotaOff = kSortedOff + kQBytes;
+constexpr size_t kIotaOff = kCodesOff + kQBytes;
 constexpr size_t kOrderOff = kIotaOff + kQBytes;
-constexpr size_t kKbufOff = kOrderOff + kQBytes;
-constexpr size_t kVbufOff = kKbufOff + kQBytes;
-constexpr size_t kCountsOff = kVbufOff + kQBytes;
-// 256 digits x ceil(max/2048) tiles, and the block sums of their scans
-constexpr size_t kCountsInts = 256 * ((kNoAllocMaxQueries + 2047) / 2048);
-constexpr size_t kScanOff = kCountsOff + align_up (sizeof (int) * kCountsInts);
+// cell counts of the query order (2^18 Morton cells), then the block sums
+// of their scan
+constexpr size_t kCellInts = 1u << 18;
+constexpr size_t kHistOff = kOrderOff + kQBytes;
+constexpr size_t kScanOff = kHistOff + align_up (sizeof (int) * kCellInts);
 constexpr size_t kScanInts = 4096;
 constexpr size_t kScratchBytes = kScanOff + align_up (sizeof (int) * kScanInts);
 
@@ -125,17 +123,18 @@ extern "C" int drb_locate_batched_noalloc (const drb_mesh *mesh, const drb_bvh *
   unsigned char *base = nullptr;
   int st = scratch_for_current_device (&base);
   if (st) return st;
-  static_assert (kScanInts >= 2 * ((kCountsInts + 2047) / 2048) + 2, "scan scratch too small");
-  LocateWorkspace ws;
+  LocateWorkspace ws{};
   ws.head = reinterpret_cast<int *> (base + kHeadOff);
   ws.codes = reinterpret_cast<unsigned *> (base + kCodesOff);
-  ws.codes_sorted = reinterpret_cast<unsigned *> (base + kSortedOff);
   ws.iota = reinterpret_cast<int *> (base + kIotaOff);
   ws.order = reinterpret_cast<int *> (base + kOrderOff);
-  ws.radix.kbuf = reinterpret_cast<unsigned *> (base + kKbufOff);
-  ws.radix.vbuf = reinterpret_cast<int *> (base + kVbufOff);
-  ws.radix.counts = reinterpret_cast<int *> (base + kCountsOff);
+  ws.hist = reinterpret_cast<int *> (base + kHistOff);
   ws.radix.scan_tmp = reinterpret_cast<int *> (base + kScanOff);
+  if ((size_t)query_cell_count () != kCellInts || scan_ws_ints ((int)kCellInts) > (int)kScanInts)
+  {
+    set_last_error ("locate_batched_noalloc: scratch layout does not match the query order");
+    return DRB_ERR_UNSUPPORTED;
+  }
   return locate_batched_ws (mesh, bvh, pts, n, opts, cfg, ws, cell, ref, stats,
                             (cudaStream_t)stream);
 }

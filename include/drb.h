@@ -187,7 +187,7 @@ typedef struct drb_locate_config
   int block;             /* threads per block, multiple of 32 */
   int blocks_per_sm;     /* resident blocks per SM, 0 = as many as fit */
   int chunk;             /* queries a warp pops from the global queue at once */
-  int sort_queries;      /* 1 = process the queries in Morton order */
+  int sort_queries;      /* 1 = process the queries in Morton-cell order */
   int reg_elements;      /* where a candidate's control points are read from
                             during its Newton solve: 0 = through L1 on every
                             step; 1 = registers (orders <= 2; fewer loads,
@@ -210,7 +210,7 @@ int drb_locate_batched (const drb_mesh *mesh, const drb_bvh *bvh, const float *p
  * record allocations, under a host application's own device-memory pool,
  * or where cudaMalloc's implicit synchronisation is not acceptable).  No
  * counterpart in the reference.  All scratch lives in one fixed array of
- * about 25 MB inside the library's device code, which stays allocated on each
+ * about 13 MB inside the library's device code, which stays allocated on each
  * device where it is loaded until the process exits.  At most
  * drb_noalloc_max_queries() (1,048,576) queries per call; more is rejected
  * with DRB_ERR_INVALID_ARG.  The first call on a device looks the array's
@@ -225,8 +225,10 @@ int drb_locate_batched_noalloc (const drb_mesh *mesh, const drb_bvh *bvh, const 
 /* Largest query count drb_locate_batched_noalloc accepts per call. */
 int drb_noalloc_max_queries (void);
 
-/* Morton order of query points over the BVH bounds: device int32 order[n]
- * (a permutation of 0..n-1).  No reference counterpart (it never reorders). */
+/* Morton-cell order of query points over the BVH bounds: device int32
+ * order[n], a permutation of 0..n-1 that lists the queries cell by cell
+ * along a Morton curve of 2^18 cells (6 bits per axis); inside a cell the
+ * order is unspecified.  No reference counterpart (it never reorders). */
 int drb_query_order (const drb_bvh *bvh, const float *pts, int n, int *order, void *stream);
 
 /* drb_locate_batched with a caller-supplied processing order (e.g. from
