@@ -404,3 +404,86 @@ class Surface:
         hits = self.nearest_hit(rays, stream=stream)
         self.shade(rays, hits, lights, fb, use_lighting, stream)
         return fb, hits
+
+
+class PointLocation:
+    """PointLocation (queries/point_location.cpp:178-287), one domain: field
+    values at arbitrary points, the empty value where no element holds the
+    point.  Locates with the reference's settings (tol 1e-4, 20 steps)
+    through the batched kernel, then evaluates each field on the device."""
+
+    def __init__(self):
+        self.vars: list[str] = []
+        self.empty = 0.0
+        self.tol, self.max_steps, self.guess_mode = 1e-4, 20, L.GUESS_ELEM_CENTER
+
+    def add_var(self, name: str):
+        self.vars.append(name)
+
+    def empty_val(self, v: float):
+        self.empty = float(v)
+
+    def execute(self, mesh: UnstructuredMesh, fields: dict, points, stream=None):
+        from .api import BatchedLocator
+        pts = _dev(points, torch.float32, mesh.device).reshape(-1, 3)
+        loc = BatchedLocator(mesh, self.tol, self.max_steps, self.guess_mode)
+        cell, ref = loc.locate(pts, stream=stream)
+        out = {}
+        for v in self.vars:
+            if v not in fields:
+                continue
+            f = fields[v]
+            vals = torch.empty(pts.shape[0], dtype=torch.float32, device=mesh.device)
+            L.check(L.lib().drb_field_eval(C.byref(f.desc()), _ptr(cell), _ptr(ref),
+                                           pts.shape[0], self.empty, _ptr(vals),
+                                           _stream(stream)), "drb_field_eval")
+            out[v] = vals
+        return out
+
+
+class Lineout:
+    """Lineout (queries/lineout.cpp): field values at samples + 2 evenly
+    spaced points along each line, start and end included."""
+
+    def __init__(self):
+        self.n_samples = 100
+        self.empty = 0.0
+        self.starts, self.ends, self.vars = [], [], []
+        self.locator = PointLocation()
+
+    def samples(self, n: int):
+        if n < 1:
+            raise ValueError("Number of samples must be positive")
+        self.n_samples = int(n)
+
+    def empty_val(self, v: float):
+        self.empty = float(v)
+
+    def add_line(self, start, end):
+        self.starts.append(tuple(float(x) for x in start))
+        self.ends.append(tuple(float(x) for x in end))
+
+    def add_var(self, name: str):
+        self.vars.append(name)
+
+    def create_points(self, device, stream=None):
+        a = torch.tensor(self.starts, dtype=torch.float32, device=device).reshape(-1, 3)
+        b = torch.tensor(self.ends, dtype=torch.float32, device=device).reshape(-1, 3)
+        pts = torch.empty((a.shape[0] * (self.n_samples + 2), 3), dtype=torch.float32,
+                          device=device)
+        L.check(L.lib().drb_lineout_points(_ptr(a), _ptr(b), a.shape[0], self.n_samples,
+                                           _ptr(pts), _stream(stream)), "drb_lineout_points")
+        return pts
+
+    def execute(self, mesh: UnstructuredMesh, fields: dict, stream=None):
+        """(points [n_lines * (samples + 2), 3], {var: values})."""
+        if not self.vars:
+            raise ValueError("Lineout: must specify at least 1 variables:")
+        if not self.starts:
+            raise ValueError("Lineout: must specify at least 1 line:")
+        if not any(v in fields for v in self.vars):
+            raise ValueError("Lineout: must specify at least one valid field.")
+        pts = self.create_points(mesh.device, stream)
+        self.locator.vars = list(self.vars)
+        self.locator.empty_val(self.empty)
+        return pts, self.locator.execute(mesh, fields, pts, stream)

@@ -431,6 +431,13 @@ int drb_mlp_guess (const float *params, const void *wbf16, const drb_mesh *mesh,
 int drb_field_eval (const drb_mesh *field, const int *cell, const float *ref, int n,
                     float empty_value, float *values, void *stream);
 
+/* Lineout::create_points (queries/lineout.cpp:98-140): samples + 2 evenly
+ * spaced points per line from start to end inclusive, bit-identical to the
+ * reference's (same operations in the same order).  starts, ends: device
+ * float[3 n_lines]; points: device float[3 n_lines (samples + 2)]. */
+int drb_lineout_points (const float *starts, const float *ends, int n_lines, int samples,
+                        float *points, void *stream);
+
 /* Physical points X_e(r) (Element::eval, pos_tensor_element.tcc:99-232). */
 int drb_map_points (const drb_mesh *mesh, const int *elem, const float *ref, int n, float *pts,
                     void *stream);

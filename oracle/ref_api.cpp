@@ -15,6 +15,7 @@
 //   MeshBoundary::execute                               filters/mesh_boundary.cpp:339
 //   Surface::nearest_hit / fragments / shade            rendering/surface.cpp:497, traceable.cpp
 //   Framebuffer::clear / composite_background           rendering/framebuffer.cpp:126,146
+#include <dray/queries/lineout.hpp>
 #include <dray/aabb.hpp>
 #include <dray/array.hpp>
 #include <dray/bvh.hpp>
@@ -509,6 +510,41 @@ int ref_surface (void *h, int w, int hgt, const float *cam9, float fov, int tf_s
 // values `vals` ((p+1)^3, u fastest) at n reference points; fixed != 0 uses
 // the fixed-order specialisation (orders 1 and 2), else Order::General.
 // This is how the reference's own t_dray_external_evals test drives it.
+// Lineout::execute (queries/lineout.cpp:114-205) on field "f": points
+// float[3 * n_lines * (samples + 2)], values float[n_lines * (samples + 2)].
+int ref_lineout (void *h, int n_lines, const float *starts, const float *ends, int samples,
+                 float empty, float *points, float *values)
+{
+  try
+  {
+    RefMesh *r = static_cast<RefMesh *> (h);
+    Lineout lo;
+    lo.samples (samples);
+    lo.empty_val (empty);
+    lo.add_var ("f");
+    for (int l = 0; l < n_lines; ++l)
+    {
+      Vec<Float, 3> a, b;
+      for (int k = 0; k < 3; ++k)
+      {
+        a[k] = starts[3 * l + k];
+        b[k] = ends[3 * l + k];
+      }
+      lo.add_line (a, b);
+    }
+    Lineout::Result res = lo.execute (r->collection);
+    const int n = (int)res.m_points.size ();
+    std::memcpy (points, (const void *)res.m_points.get_host_ptr_const (), sizeof (float) * 3 * (size_t)n);
+    std::memcpy (values, (const void *)res.m_values[0].get_host_ptr_const (), sizeof (float) * (size_t)n);
+    return n;
+  }
+  catch (const std::exception &e)
+  {
+    g_err = e.what ();
+    return -1;
+  }
+}
+
 int ref_eval_hex_scalar (int p, int fixed, const float *vals, int n, const float *ref3,
                          float *out_val, float *out_d3)
 {

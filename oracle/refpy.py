@@ -46,6 +46,7 @@ def lib():
         L.ref_surface.argtypes = [vp, C.c_int, C.c_int, vp, C.c_float, C.c_int, C.c_int, vp,
                                   C.c_int, vp, C.c_int, vp, vp, vp, vp, vp, vp]
         L.ref_eval_hex_scalar.argtypes = [C.c_int, C.c_int, vp, C.c_int, vp, vp, vp]
+        L.ref_lineout.argtypes = [vp, C.c_int, vp, vp, C.c_int, C.c_float, vp, vp]
         _lib = L
     return _lib
 
@@ -131,6 +132,18 @@ class RefHexMesh:
         if nf < 0:
             raise RuntimeError(lib().ref_last_error().decode())
         return out[: nf * (p + 1) ** 2].reshape(nf, (p + 1) ** 2)
+
+    def lineout(self, starts, ends, samples, empty=0.0):
+        """Lineout::execute on field "f": (points [n, 3], values [n])."""
+        a = np.ascontiguousarray(starts, np.float32).reshape(-1, 3)
+        b = np.ascontiguousarray(ends, np.float32).reshape(-1, 3)
+        n = a.shape[0] * (samples + 2)
+        pts = np.zeros((n, 3), np.float32)
+        vals = np.zeros(n, np.float32)
+        r = lib().ref_lineout(self.h, a.shape[0], _p(a), _p(b), samples, empty, _p(pts), _p(vals))
+        if r < 0:
+            raise RuntimeError(lib().ref_last_error().decode())
+        return pts, vals
 
     def surface(self, w, h, cam9, fov, tf_samples, rgb_pts, alpha_pts, lights13):
         rgb = np.ascontiguousarray(rgb_pts, np.float32).reshape(-1)
