@@ -307,6 +307,12 @@ class Collection
   int32 size () const { return local_size (); }
   AABB<3> bounds ();
   Range range (const std::string &field_name);
+  bool has_field (const std::string &field_name)
+  {
+    for (auto &d : m_domains)
+      if (d.has_field (field_name)) return true;
+    return false;
+  }
 };
 
 class ColorTable
@@ -456,6 +462,36 @@ class PointLocation
   void empty_val (const Float v) { m_empty_val = v; }
   void add_var (const std::string v) { m_vars.push_back (v); }
   Result execute (Collection &collection, Array<Vec<Float, 3>> &points);
+};
+
+// Lineout (queries/lineout.hpp): field values at samples + 2 evenly spaced
+// points along each line, start and end included.
+class Lineout
+{
+  int32 m_samples = 100;
+  Float m_empty_val = 0.f;
+  std::vector<Vec<Float, 3>> m_starts, m_ends;
+  std::vector<std::string> m_vars;
+  public:
+  struct Result
+  {
+    Array<Vec<Float, 3>> m_points;
+    int32 m_points_per_line;
+    std::vector<Array<Float>> m_values;
+    std::vector<std::string> m_vars;
+    Float m_empty_val;
+  };
+  int32 samples () const { return m_samples; }
+  void samples (int32 samples);
+  void empty_val (const Float val) { m_empty_val = val; }
+  void add_line (const Vec<Float, 3> start, const Vec<Float, 3> end)
+  {
+    m_starts.push_back (start);
+    m_ends.push_back (end);
+  }
+  void add_var (const std::string var) { m_vars.push_back (var); }
+  Result execute (Collection &collection);
+  Array<Vec<Float, 3>> create_points ();
 };
 
 class Renderer

@@ -665,6 +665,62 @@ PointLocation::Result PointLocation::execute (Collection &collection, Array<Vec<
 
 // ------------------------------------------------------------ renderer --
 
+// ------------------------------------------------------------ Lineout --
+
+void Lineout::samples (int32 samples)
+{
+  if (samples < 1) DRAY_ERROR ("Number of samples must be positive");
+  m_samples = samples;
+}
+
+Array<Vec<Float, 3>> Lineout::create_points ()
+{
+  // queries/lineout.cpp:98-140, on the device (drb_lineout_points)
+  const int32 n = (int32)m_starts.size ();
+  Array<Vec<Float, 3>> starts, ends, points;
+  starts.resize (n);
+  ends.resize (n);
+  Vec<Float, 3> *sp = starts.get_host_ptr ();
+  Vec<Float, 3> *ep = ends.get_host_ptr ();
+  for (int32 i = 0; i < n; ++i)
+  {
+    sp[i] = m_starts[i];
+    ep[i] = m_ends[i];
+  }
+  points.resize ((size_t)n * (m_samples + 2));
+  drb_check (drb_lineout_points ((const float *)starts.get_device_ptr_const (),
+                                 (const float *)ends.get_device_ptr_const (), n, m_samples,
+                                 (float *)points.get_device_ptr (), nullptr),
+             "drb_lineout_points");
+  return points;
+}
+
+Lineout::Result Lineout::execute (Collection &collection)
+{
+  // queries/lineout.cpp:114-205
+  if (m_vars.empty ()) DRAY_ERROR ("Lineout: must specify at least 1 variables:");
+  if (m_starts.empty ()) DRAY_ERROR ("Lineout: must specify at least 1 line:");
+  PointLocation locator;
+  int32 valid = 0;
+  for (const std::string &v : m_vars)
+    if (collection.has_field (v))
+    {
+      locator.add_var (v);
+      ++valid;
+    }
+  if (valid == 0) DRAY_ERROR ("Lineout: must specify at least one valid field.");
+  locator.empty_val (m_empty_val);
+  Array<Vec<Float, 3>> points = create_points ();
+  PointLocation::Result lres = locator.execute (collection, points);
+  Result res;
+  res.m_points = points;
+  res.m_points_per_line = m_samples + 2;
+  res.m_vars = m_vars;
+  res.m_values = lres.m_values;
+  res.m_empty_val = m_empty_val;
+  return res;
+}
+
 Framebuffer Renderer::render (Camera &camera)
 {
   // Renderer::render (rendering/renderer.cpp:229-363), single domain:

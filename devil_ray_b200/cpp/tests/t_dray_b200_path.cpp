@@ -15,6 +15,8 @@
 //            <dir>/pointloc.bin float value[n]
 //            <dir>/volume.bin   float rgba[4wh]   (Volume::integrate + save compositing)
 //            <dir>/surface.bin  float rgba[4wh]; float depth[wh]
+//            <dir>/lineout.bin  float points[3 * 4 * 39]; float values[4 * 39]
+//                               (four fixed lines, 37 samples, empty value -7)
 #include <dray/dray_b200.hpp>
 
 #include <cstdio>
@@ -201,6 +203,26 @@ int main (int argc, char **argv)
       std::ofstream fo (dir + "/surface.bin", std::ios::binary);
       wr (fo, (const float *)fb.colors ().get_host_ptr_const (), (size_t)4 * whs[0] * whs[1]);
       wr (fo, fb.depths ().get_host_ptr_const (), (size_t)whs[0] * whs[1]);
+    }
+
+    // --- Lineout::execute on four fixed lines
+    {
+      Lineout lo;
+      lo.samples (37);
+      lo.empty_val (-7.f);
+      const float a[4][3] = { { 0.f, 0.f, 0.f }, { 0.1f, 0.5f, 0.9f }, { -0.2f, 0.3f, 0.4f },
+                              { 0.5f, 0.5f, 1.3f } };
+      const float b[4][3] = { { 1.f, 1.f, 1.f }, { 1.2f, 0.5f, 0.1f }, { 1.1f, 0.35f, 0.45f },
+                              { 0.5f, 0.5f, -0.3f } };
+      for (int l = 0; l < 4; ++l)
+        lo.add_line (make_vec3f (a[l][0], a[l][1], a[l][2]), make_vec3f (b[l][0], b[l][1], b[l][2]));
+      lo.add_var ("f");
+      Lineout::Result lr = lo.execute (col);
+      EXPECT (lr.m_points_per_line == 39 && lr.m_values.size () == 1);
+      EXPECT (lr.m_points.size () == 4 * 39);
+      std::ofstream fo (dir + "/lineout.bin", std::ios::binary);
+      wr (fo, (const float *)lr.m_points.get_host_ptr_const (), (size_t)3 * 4 * 39);
+      wr (fo, lr.m_values[0].get_host_ptr_const (), (size_t)4 * 39);
     }
 
     // --- error behaviour: wrong fixed order throws DRayError

@@ -4,7 +4,7 @@
 // (data_model/unstructured_mesh.cpp:137-148): warps mix points from
 // unrelated parts of the mesh, and every lane waits for the slowest lane's
 // traversal and Newton iterations.  This path instead
-//   1. orders the queries by Morton cell (6 bits per axis over the BVH
+//   1. orders the queries by Morton cell (7 bits per axis over the BVH
 //      bounds, a counting sort), so a warp's lanes follow nearly the same
 //      BVH path and hit the same few elements (L1/L2 reuse);
 //   2. runs a persistent kernel, grid sized to the resident capacity of the
@@ -31,14 +31,14 @@ namespace drb
 namespace
 {
 
-// Query order by counting sort into Morton cells of 6 bits per axis
-// (2^18 cells over the BVH bounds; one cell is about one element of a 64^3
+// Query order by counting sort into Morton cells of 7 bits per axis
+// (2^21 cells over the BVH bounds; one cell is an eighth of an element of a 64^3
 // mesh).  The persistent kernel needs spatially coherent warps, not a
 // sorted sequence, so the order inside a cell is whatever the atomics give:
 // one counting pass, a scan of the cell counts and one scatter replace the
 // four passes of a 30-bit radix sort.  Every query's result is independent
 // of the order.
-constexpr int kCellBits = 6;
+constexpr int kCellBits = 7;
 constexpr int kCells = 1 << (3 * kCellBits);
 
 __global__ void cell_count_kernel (const float *__restrict__ pts, int n, float x0, float y0,

@@ -14,7 +14,7 @@
 // Limits and sharing:
 //   - at most kNoAllocMaxQueries queries per call (larger calls are rejected
 //     with DRB_ERR_INVALID_ARG and a message);
-//   - the array (about 13 MB) is part of this library's device code and stays
+//   - the array (about 20 MB) is part of this library's device code and stays
 //     allocated on every device where it has been loaded, until the process
 //     exits;
 //   - every call on a device uses the same array: calls whose GPU work can
@@ -41,9 +41,9 @@ constexpr size_t kHeadOff = 0;
 constexpr size_t kCodesOff = kHeadOff + kAlign;
 constexpr size_t kIotaOff = kCodesOff + kQBytes;
 constexpr size_t kOrderOff = kIotaOff + kQBytes;
-// cell counts of the query order (2^18 Morton cells), then the block sums
+// cell counts of the query order (2^21 Morton cells), then the block sums
 // of their scan
-constexpr size_t kCellInts = 1u << 18;
+constexpr size_t kCellInts = 1u << 21;
 constexpr size_t kHistOff = kOrderOff + kQBytes;
 constexpr size_t kScanOff = kHistOff + align_up (sizeof (int) * kCellInts);
 constexpr size_t kScanInts = 4096;

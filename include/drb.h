@@ -210,7 +210,7 @@ int drb_locate_batched (const drb_mesh *mesh, const drb_bvh *bvh, const float *p
  * record allocations, under a host application's own device-memory pool,
  * or where cudaMalloc's implicit synchronisation is not acceptable).  No
  * counterpart in the reference.  All scratch lives in one fixed array of
- * about 13 MB inside the library's device code, which stays allocated on each
+ * about 20 MB inside the library's device code, which stays allocated on each
  * device where it is loaded until the process exits.  At most
  * drb_noalloc_max_queries() (1,048,576) queries per call; more is rejected
  * with DRB_ERR_INVALID_ARG.  The first call on a device looks the array's
@@ -227,7 +227,7 @@ int drb_noalloc_max_queries (void);
 
 /* Morton-cell order of query points over the BVH bounds: device int32
  * order[n], a permutation of 0..n-1 that lists the queries cell by cell
- * along a Morton curve of 2^18 cells (6 bits per axis); inside a cell the
+ * along a Morton curve of 2^21 cells (7 bits per axis); inside a cell the
  * order is unspecified.  No reference counterpart (it never reorders). */
 int drb_query_order (const drb_bvh *bvh, const float *pts, int n, int *order, void *stream);
 

@@ -114,3 +114,15 @@ def test_cpp_interface_matches_reference(cuda, ref, tmp_path, name):
     assert bad.mean() < 0.005, f"surface: {bad.sum()} pixels > 1/255, max {d.max():.2e}"
     hit = np.isfinite(rs["depth"]) & np.isfinite(sdepth) & (rs["depth"] < 1e30)
     assert np.abs(sdepth[hit] - rs["depth"][hit]).max() < 1e-3
+
+    # Lineout: points bit-identical, values equal (empty value outside).
+    raw = np.fromfile(tmp_path / "lineout.bin", np.float32)
+    lp = raw[: 3 * 4 * 39].reshape(-1, 3)
+    lv = raw[3 * 4 * 39:]
+    starts = [(0.0, 0.0, 0.0), (0.1, 0.5, 0.9), (-0.2, 0.3, 0.4), (0.5, 0.5, 1.3)]
+    ends = [(1.0, 1.0, 1.0), (1.2, 0.5, 0.1), (1.1, 0.35, 0.45), (0.5, 0.5, -0.3)]
+    rp, rv = rm.lineout(starts, ends, 37, -7.0)
+    assert np.array_equal(lp.view(np.int32), rp.view(np.int32))
+    out = rv == np.float32(-7.0)
+    assert np.array_equal(lv == np.float32(-7.0), out)
+    assert np.abs(lv[~out] - rv[~out]).max() < 1e-4
