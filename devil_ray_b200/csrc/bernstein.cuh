@@ -84,6 +84,18 @@ DRB_HD constexpr int packed_stride (int nd, int ncomp)
 }
 DRB_HD constexpr int packed_origin (int nd) { return 3 * nd; }
 
+// One u-row of control points: components of points i0 .. i0 + P, point
+// major.  Element accessors whose rows are 16-byte aligned overload this
+// with vector loads (PackedCP at order 3, the volume's field rows).
+template <int P, int NC, class CP>
+DRB_D void cp_row (const CP &cp, int i0, float (&v)[(P + 1) * NC])
+{
+#pragma unroll
+  for (int a = 0; a <= P; ++a)
+#pragma unroll
+    for (int k = 0; k < NC; ++k) v[a * NC + k] = cp (i0 + a, k);
+}
+
 // Hex element: value X and the three columns dX/du, dX/dv, dX/dw.
 // `cp(i, k)` returns component k of control point i.
 template <int P, int NC, class CP>
@@ -108,14 +120,15 @@ DRB_D void hex_eval_d (const CP &cp, float u, float v, float w, float (&X)[NC],
       float s[NC], sd[NC];
 #pragma unroll
       for (int k = 0; k < NC; ++k) s[k] = sd[k] = 0.f;
+      float row[(P + 1) * NC];
+      cp_row<P, NC> (cp, (c * (P + 1) + b) * (P + 1), row);
 #pragma unroll
       for (int a = 0; a <= P; ++a)
       {
-        const int i = (c * (P + 1) + b) * (P + 1) + a;
 #pragma unroll
         for (int k = 0; k < NC; ++k)
         {
-          const float q = cp (i, k);
+          const float q = row[a * NC + k];
           s[k] = fmaf (q, bu[a], s[k]);
           sd[k] = fmaf (q, du[a], sd[k]);
         }

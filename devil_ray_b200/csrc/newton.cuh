@@ -93,6 +93,62 @@ struct PackedCP
   DRB_D float operator() (int i, int k) const { return __ldg (p + 3 * i + k); }
 };
 
+// Order-3 rows of a packed element: 12 floats at 48-byte offsets of a
+// 16-byte aligned row, so three float4 loads instead of twelve scalar ones.
+template <> DRB_D void cp_row<3, 3, PackedCP> (const PackedCP &cp, int i0, float (&v)[12])
+{
+  const float4 *q = reinterpret_cast<const float4 *> (cp.p + 3 * i0);
+  const float4 a = __ldg (q), b = __ldg (q + 1), c = __ldg (q + 2);
+  v[0] = a.x; v[1] = a.y; v[2] = a.z; v[3] = a.w;
+  v[4] = b.x; v[5] = b.y; v[6] = b.z; v[7] = b.w;
+  v[8] = c.x; v[9] = c.y; v[10] = c.z; v[11] = c.w;
+}
+
+// Order-2 rows: 9 floats at 36-byte offsets.  The offset modulo 16 bytes
+// is known once the caller's loops are unrolled, and picks the widest
+// aligned loads that cover the row (3 or 4 loads instead of 9).
+template <> DRB_D void cp_row<2, 3, PackedCP> (const PackedCP &cp, int i0, float (&v)[9])
+{
+  const float *q = cp.p + 3 * i0;
+  const int mis = (3 * i0) & 3; // floats past a 16-byte boundary
+  if (mis == 0)
+  {
+    const float4 a = __ldg (reinterpret_cast<const float4 *> (q));
+    const float4 b = __ldg (reinterpret_cast<const float4 *> (q + 4));
+    v[0] = a.x; v[1] = a.y; v[2] = a.z; v[3] = a.w;
+    v[4] = b.x; v[5] = b.y; v[6] = b.z; v[7] = b.w;
+    v[8] = __ldg (q + 8);
+  }
+  else if (mis == 1)
+  {
+    v[0] = __ldg (q);
+    const float2 a = __ldg (reinterpret_cast<const float2 *> (q + 1));
+    const float4 b = __ldg (reinterpret_cast<const float4 *> (q + 3));
+    const float2 c = __ldg (reinterpret_cast<const float2 *> (q + 7));
+    v[1] = a.x; v[2] = a.y;
+    v[3] = b.x; v[4] = b.y; v[5] = b.z; v[6] = b.w;
+    v[7] = c.x; v[8] = c.y;
+  }
+  else if (mis == 2)
+  {
+    const float2 a = __ldg (reinterpret_cast<const float2 *> (q));
+    const float4 b = __ldg (reinterpret_cast<const float4 *> (q + 2));
+    const float2 c = __ldg (reinterpret_cast<const float2 *> (q + 6));
+    v[0] = a.x; v[1] = a.y;
+    v[2] = b.x; v[3] = b.y; v[4] = b.z; v[5] = b.w;
+    v[6] = c.x; v[7] = c.y;
+    v[8] = __ldg (q + 8);
+  }
+  else
+  {
+    v[0] = __ldg (q);
+    const float4 a = __ldg (reinterpret_cast<const float4 *> (q + 1));
+    const float4 b = __ldg (reinterpret_cast<const float4 *> (q + 5));
+    v[1] = a.x; v[2] = a.y; v[3] = a.z; v[4] = a.w;
+    v[5] = b.x; v[6] = b.y; v[7] = b.z; v[8] = b.w;
+  }
+}
+
 // pt - O for a packed geometry row with ND control points (O stored at
 // packed_origin(ND)); t is the Newton target in the row's frame.
 template <int ND> DRB_D void local_target (const float *__restrict__ row, const float (&pt)[3], float (&t)[3])

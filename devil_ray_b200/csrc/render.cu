@@ -282,6 +282,16 @@ template <int P> struct FieldCP
   const float *__restrict__ row;
   DRB_D float operator() (int i, int) const { return __ldg (row + i); }
 };
+// Order-3 scalar rows: 4 values at 16-byte offsets, one float4 load.
+template <> DRB_D void cp_row<3, 1, FieldCP<3>> (const FieldCP<3> &cp, int i0, float (&v)[4])
+{
+  const float4 a = __ldg (reinterpret_cast<const float4 *> (cp.row + i0));
+  v[0] = a.x;
+  v[1] = a.y;
+  v[2] = a.z;
+  v[3] = a.w;
+}
+
 template <int P> struct FieldIndCP
 {
   const int *__restrict__ idx;
