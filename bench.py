@@ -261,6 +261,65 @@ def volume_c0(dev, with_cpu):
     return out
 
 
+def surface_c1(dev, with_cpu):
+    """The surface config: 32^3 order-3 mesh (warp 0.08, jitter 0.01), its
+    6144 boundary quads, 1024^2 rays from (2.5,2.5,2.5), 1024-entry TF, lit:
+    rays/s of the GPU nearest-hit + fragments + shade, and of the reference's
+    OpenMP Surface::nearest_hit + Traceable::shade on the host cores."""
+    import torch
+    from devil_ray_b200 import api, meshgen
+    from devil_ray_b200.render import (Camera, ColorTable, MeshBoundary, PointLight, Surface,
+                                       UnstructuredField)
+    m = meshgen.workload_mesh("surface_32")
+    c = meshgen.CAMERA
+    W = 1024
+    cam = Camera(W, W, c["pos"], c["look_at"], c["up"], c["fov"])
+    light = PointLight.default(cam)
+    mesh = api.UnstructuredMesh(m.ctrl_idx, m.xyz, m.order, device=dev)
+    field = UnstructuredField(m.ctrl_idx, m.field, m.order, device=dev)
+    faces, ff = MeshBoundary().execute(mesh, field)
+    surf = Surface(faces, ff)
+    t = ColorTable()
+    for p in meshgen.TF_RGB:
+        t.add_point(p[0], p[1:])
+    for p in meshgen.TF_ALPHA:
+        t.add_alpha(*p)
+    surf.color_map().color_table(t)
+    fb, hits = surf.render(cam, [light])
+    torch.cuda.synchronize()
+    n_hit = int((hits[:, 0].contiguous().view(torch.int32) >= 0).sum())
+    for _ in range(3):
+        surf.render(cam, [light])
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    reps = 10
+    torch.cuda.synchronize()
+    e0.record()
+    for _ in range(reps):
+        surf.render(cam, [light])
+    e1.record()
+    torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1) / reps
+    out = {"workload": "surface_32: 32^3 hex order 3, warp 0.08, jitter 0.01, 6144 boundary "
+                       "quads, 1024^2 rays, 1024-entry TF, lit",
+           "metric": "rays/s (nearest hit + fragments + shade)",
+           "value": W * W / (ms * 1e-3), "ms_per_frame": ms, "rays": W * W, "hits": n_hit}
+    if with_cpu:
+        from oracle import refpy
+        if refpy.available():
+            r = refpy.RefHexMesh(m.order, m.ctrl_idx, m.xyz, m.field)
+            cam9 = np.array([*c["pos"], *c["look_at"], *c["up"]], np.float32)
+            args = (W, W, cam9, c["fov"], 1024, np.array(meshgen.TF_RGB, np.float32),
+                    np.array(meshgen.TF_ALPHA, np.float32), light.as13()[None])
+            r.surface(*args)  # boundary + face BVH on the first call
+            t0 = time.perf_counter()
+            r.surface(*args)
+            cpu_s = time.perf_counter() - t0
+            out["cpu_reference"] = {"value": W * W / cpu_s, "unit": "rays/s", "seconds": cpu_s,
+                                    "cores": refpy.num_threads(), "kind": "reference",
+                                    "sample": "the whole 1024^2 frame"}
+    return out
+
+
 def orbit_cameras(count, width, seed=5):
     """Orbits about the mesh centre at the distance of the (2.5,2.5,2.5)
     camera: azimuth k * 22.5 degrees plus a seeded elevation jitter."""
@@ -691,6 +750,13 @@ def main():
         except Exception as exc:
             vol_c0 = {"error": repr(exc)}
 
+    surf_c1 = None
+    if not args.no_volume:
+        try:
+            surf_c1 = surface_c1(dev, rank == 0 and world == 1 and not args.no_cpu_baseline)
+        except Exception as exc:
+            surf_c1 = {"error": repr(exc)}
+
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         try:
@@ -743,6 +809,7 @@ def main():
             "learned": learned,
             "volume": vol,
             "volume_c0": vol_c0,
+            "surface": surf_c1,
             "bvh_build_ms": bvh_build_ms, "tune_ms": tune_ms,
             "cpu_baseline": cpu,
         }

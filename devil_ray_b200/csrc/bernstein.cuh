@@ -205,14 +205,15 @@ DRB_D void quad_eval_d (const CP &cp, float u, float v, float (&X)[NC], float (&
     float s[NC], sd[NC];
 #pragma unroll
     for (int k = 0; k < NC; ++k) s[k] = sd[k] = 0.f;
+    float row[(P + 1) * NC];
+    cp_row<P, NC> (cp, b * (P + 1), row);
 #pragma unroll
     for (int a = 0; a <= P; ++a)
     {
-      const int i = b * (P + 1) + a;
 #pragma unroll
       for (int k = 0; k < NC; ++k)
       {
-        const float q = cp (i, k);
+        const float q = row[a * NC + k];
         s[k] = fmaf (q, bu[a], s[k]);
         sd[k] = fmaf (q, du[a], sd[k]);
       }

@@ -184,11 +184,9 @@ DRB_D bool face_newton (const CP &cp, const Ray &ray, float (&x)[2], float &t, f
   return converged && inside && ray.near_t <= t && t < ray.far_t;
 }
 
-struct QuadPackedCP
-{
-  const float *__restrict__ p;
-  DRB_D float operator() (int i, int k) const { return __ldg (p + 3 * i + k); }
-};
+// packed face rows are read like packed hex rows (PackedCP, with its
+// vector row loads at orders 2 and 3)
+using QuadPackedCP = PackedCP;
 
 // intersect_AABB (surface.cpp:120-163), explicitly rounded slab arithmetic
 DRB_D bool node_ray_test (const float4 *__restrict__ nodes, int node, const float (&od)[3],
