@@ -340,10 +340,10 @@ def orbit_cameras(count, width, seed=5):
 
 # DRAM bytes (read + write) of one locate_persistent_kernel launch on this
 # workload (16M queries, 4-wide tree), from an ncu capture of the same launch
-# (profiles/locate_persistent_kernel__locate_64_16M_queries.md): 4.019 GB
-# read + 1.197 GB written.  Used for roofline.traffic, scaled by the query
+# (profiles/locate_persistent_kernel__locate_64_16M_queries.md): 4.016 GB
+# read + 1.194 GB written.  Used for roofline.traffic, scaled by the query
 # count when --queries differs.
-LOCATE_TRAFFIC_16M = 4.018994e9 + 1.197257e9
+LOCATE_TRAFFIC_16M = 4.016342e9 + 1.193831e9
 
 # FP32 pipe peak of a B200: 148 SMs x 128 FP32 lanes x 2 FLOP (FMA) x 1.965 GHz
 FP32_PEAK_TFLOPS = 148 * 128 * 2 * 1.965e9 / 1e12
