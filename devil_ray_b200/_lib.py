@@ -142,6 +142,8 @@ _SIGS = {
     "drb_radix_sort_pairs": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p,
                                        C.c_int, C.c_int, C.c_void_p]),
     "drb_lbvh_build": (C.c_int, [C.POINTER(DrbMesh), C.POINTER(DrbBvh), C.c_void_p, C.c_void_p]),
+    "drb_scalar_buffer_write": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_int, C.c_int,
+                                          C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]),
     "drb_lineout_points": (C.c_int, [C.c_void_p, C.c_void_p, C.c_int, C.c_int, C.c_void_p,
                                      C.c_void_p]),
     "drb_field_eval": (C.c_int, [C.POINTER(DrbMesh), C.c_void_p, C.c_void_p, C.c_int, C.c_float,

@@ -21,6 +21,7 @@
 #pragma once
 
 #include <cmath>
+#include <map>
 #include <memory>
 #include <sstream>
 #include <string>
@@ -462,6 +463,39 @@ class PointLocation
   void empty_val (const Float v) { m_empty_val = v; }
   void add_var (const std::string v) { m_vars.push_back (v); }
   Result execute (Collection &collection, Array<Vec<Float, 3>> &points);
+};
+
+// ScalarBuffer (rendering/scalar_buffer.hpp): per-pixel depth, zone id and
+// one plane per field, cleared to the clear value (zone ids to -1).
+class ScalarBuffer
+{
+  public:
+  int32 m_width = 0, m_height = 0;
+  Float m_clear_value = 0.f;
+  Array<Float> m_depths;
+  Array<int32> m_zone_ids;
+  std::map<std::string, Array<Float>> m_scalars;
+  ScalarBuffer () {}
+  ScalarBuffer (int32 width, int32 height, Float clear_value);
+  bool has_field (const std::string name) { return m_scalars.find (name) != m_scalars.end (); }
+  void add_field (const std::string name);
+  int32 size () const { return m_width * m_height; }
+};
+
+// ScalarRenderer (rendering/scalar_renderer.hpp), one domain: the nearest
+// hit of each ray, its depth and zone id, and each named field's value at
+// the hit, per pixel.
+class ScalarRenderer
+{
+  std::shared_ptr<Traceable> m_traceable;
+  std::vector<std::string> m_field_names;
+  public:
+  ScalarRenderer () {}
+  explicit ScalarRenderer (std::shared_ptr<Traceable> traceable) : m_traceable (traceable) {}
+  void set (std::shared_ptr<Traceable> traceable) { m_traceable = traceable; }
+  void field_names (const std::vector<std::string> &names) { m_field_names = names; }
+  ScalarBuffer render (Camera &camera);
+  void render (Array<Ray> &rays, ScalarBuffer &scalar_buffer);
 };
 
 // Lineout (queries/lineout.hpp): field values at samples + 2 evenly spaced

@@ -2,6 +2,7 @@
 // over the C-ABI of include/drb.h.  Every compute step is a libdrb call on
 // the legacy default stream; host synchronisation happens only where the
 // reference's API returns host-visible results.
+#include <limits>
 #include "dray/dray_b200.hpp"
 
 #include <algorithm>
@@ -664,6 +665,77 @@ PointLocation::Result PointLocation::execute (Collection &collection, Array<Vec<
 }
 
 // ------------------------------------------------------------ renderer --
+
+// ------------------------------------------------------- ScalarRenderer --
+
+ScalarBuffer::ScalarBuffer (int32 width, int32 height, Float clear_value)
+: m_width (width), m_height (height), m_clear_value (clear_value)
+{
+  m_depths.resize ((size_t)width * height);
+  m_zone_ids.resize ((size_t)width * height);
+  Float *d = m_depths.get_host_ptr ();
+  int32 *z = m_zone_ids.get_host_ptr ();
+  for (int32 i = 0; i < width * height; ++i)
+  {
+    d[i] = clear_value;
+    z[i] = -1;
+  }
+}
+
+void ScalarBuffer::add_field (const std::string name)
+{
+  Array<Float> a;
+  a.resize ((size_t)m_width * m_height);
+  Float *p = a.get_host_ptr ();
+  for (int32 i = 0; i < m_width * m_height; ++i) p[i] = m_clear_value;
+  m_scalars[name] = a;
+}
+
+ScalarBuffer ScalarRenderer::render (Camera &camera)
+{
+  // rendering/scalar_renderer.cpp:446-462
+  if (!m_traceable) DRAY_ERROR ("ScalarRenderer: traceable never set");
+  Array<Ray> rays;
+  camera.create_rays (rays);
+  ScalarBuffer buffer (camera.get_width (), camera.get_height (),
+                       std::numeric_limits<Float>::quiet_NaN ());
+  render (rays, buffer);
+  return buffer;
+}
+
+void ScalarRenderer::render (Array<Ray> &rays, ScalarBuffer &buffer)
+{
+  // rendering/scalar_renderer.cpp:296-365, one domain (zone offset 0)
+  if (!m_traceable) DRAY_ERROR ("ScalarRenderer: traceable never set");
+  Array<RayHit> hits = m_traceable->nearest_hit (rays);
+  const int n = (int)rays.size ();
+  drb_check (drb_scalar_buffer_write (rays.get_device_ptr_const (), hits.get_device_ptr_const (),
+                                      nullptr, n, 0, buffer.m_depths.get_device_ptr (),
+                                      buffer.m_zone_ids.get_device_ptr (), nullptr, nullptr),
+             "drb_scalar_buffer_write");
+  const std::string saved = m_traceable->field ();
+  for (const std::string &name : m_field_names)
+  {
+    m_traceable->field (name);
+    Array<Fragment> frags;
+    try
+    {
+      frags = m_traceable->fragments (hits);
+    }
+    catch (const DRayError &)
+    {
+      continue; // a field this surface does not carry
+    }
+    if (!buffer.has_field (name)) buffer.add_field (name);
+    drb_check (drb_scalar_buffer_write (rays.get_device_ptr_const (), hits.get_device_ptr_const (),
+                                        (const float *)frags.get_device_ptr_const (), n, 0, nullptr,
+                                        nullptr, buffer.m_scalars[name].get_device_ptr (), nullptr),
+               "drb_scalar_buffer_write");
+  }
+  m_traceable->field (saved);
+  drb_check (drb_ray_max (rays.get_device_ptr (), hits.get_device_ptr_const (), n, nullptr),
+             "drb_ray_max");
+}
 
 // ------------------------------------------------------------ Lineout --
 

@@ -15,6 +15,8 @@
 //            <dir>/pointloc.bin float value[n]
 //            <dir>/volume.bin   float rgba[4wh]   (Volume::integrate + save compositing)
 //            <dir>/surface.bin  float rgba[4wh]; float depth[wh]
+//            <dir>/scalar.bin   float depth[wh]; int32 zone[wh]; float f[wh]
+//                               (ScalarRenderer on the boundary surface)
 //            <dir>/lineout.bin  float points[3 * 4 * 39]; float values[4 * 39]
 //                               (four fixed lines, 37 samples, empty value -7)
 #include <dray/dray_b200.hpp>
@@ -203,6 +205,18 @@ int main (int argc, char **argv)
       std::ofstream fo (dir + "/surface.bin", std::ios::binary);
       wr (fo, (const float *)fb.colors ().get_host_ptr_const (), (size_t)4 * whs[0] * whs[1]);
       wr (fo, fb.depths ().get_host_ptr_const (), (size_t)whs[0] * whs[1]);
+
+      // ScalarRenderer on the same surface
+      auto tr = std::make_shared<Surface> (faces);
+      tr->field ("f");
+      ScalarRenderer sr (tr);
+      sr.field_names ({ "f" });
+      ScalarBuffer sb = sr.render (cam);
+      EXPECT (sb.has_field ("f"));
+      std::ofstream fs (dir + "/scalar.bin", std::ios::binary);
+      wr (fs, sb.m_depths.get_host_ptr_const (), (size_t)whs[0] * whs[1]);
+      wr (fs, sb.m_zone_ids.get_host_ptr_const (), (size_t)whs[0] * whs[1]);
+      wr (fs, sb.m_scalars["f"].get_host_ptr_const (), (size_t)whs[0] * whs[1]);
     }
 
     // --- Lineout::execute on four fixed lines

@@ -406,6 +406,24 @@ __global__ void shade_kernel (const Ray *__restrict__ rays, const RayHit *__rest
 }
 
 // ray_max (ray.cpp:243-259)
+// ScalarRenderer::render (rendering/scalar_renderer.cpp:296-365): per hit
+// ray, the depth and zone id of the hit and the fragment's scalar go to the
+// ray's pixel.
+__global__ void scalar_buffer_kernel (const Ray *__restrict__ rays, const RayHit *__restrict__ hits,
+                                      const float4 *__restrict__ frags, int n, int zone_offset,
+                                      float *__restrict__ depths, int *__restrict__ zone_ids,
+                                      float *__restrict__ scalars)
+{
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const RayHit h = hits[i];
+  if (h.hit_idx <= -1) return;
+  const int pid = rays[i].pixel_id;
+  if (depths) depths[pid] = h.dist;
+  if (zone_ids) zone_ids[pid] = h.hit_idx + zone_offset;
+  if (scalars && frags) scalars[pid] = frags[i].x;
+}
+
 __global__ void ray_max_kernel (Ray *rays, const RayHit *hits, int n)
 {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
@@ -569,4 +587,20 @@ extern "C" int drb_ray_max (void *rays, const void *hits, int n, void *stream)
   if (n == 0) return DRB_OK;
   ray_max_kernel<<<div_up (n, 256), 256, 0, (cudaStream_t)stream>>> ((Ray *)rays, (const RayHit *)hits, n);
   return check_launch ("ray_max_kernel");
+}
+
+extern "C" int drb_scalar_buffer_write (const void *rays, const void *hits, const float *frags4,
+                                        int n, int zone_offset, float *depths, int *zone_ids,
+                                        float *scalars, void *stream)
+{
+  if (n < 0 || (n > 0 && (!rays || !hits)) || (scalars && !frags4))
+  {
+    set_last_error ("scalar_buffer_write: bad arguments");
+    return DRB_ERR_INVALID_ARG;
+  }
+  if (n == 0) return DRB_OK;
+  scalar_buffer_kernel<<<div_up (n, 256), 256, 0, (cudaStream_t)stream>>> (
+  (const Ray *)rays, (const RayHit *)hits, (const float4 *)frags4, n, zone_offset, depths, zone_ids,
+  scalars);
+  return check_launch ("scalar_buffer_kernel");
 }

@@ -406,6 +406,72 @@ class Surface:
         return fb, hits
 
 
+class ScalarBuffer:
+    """ScalarBuffer (rendering/scalar_buffer.cpp): per-pixel depth, zone id
+    and one plane per field, cleared to clear_value (zone ids to -1)."""
+
+    def __init__(self, width, height, clear_value=float("nan"), device="cuda"):
+        self.width, self.height, self.clear_value = width, height, clear_value
+        self.device = torch.device(device)
+        n = width * height
+        self.depths = torch.full((n,), clear_value, dtype=torch.float32, device=self.device)
+        self.zone_ids = torch.full((n,), -1, dtype=torch.int32, device=self.device)
+        self.scalars: dict[str, torch.Tensor] = {}
+
+    def has_field(self, name):
+        return name in self.scalars
+
+    def add_field(self, name):
+        self.scalars[name] = torch.full((self.width * self.height,), self.clear_value,
+                                        dtype=torch.float32, device=self.device)
+
+
+class ScalarRenderer:
+    """ScalarRenderer (rendering/scalar_renderer.cpp:296-462) over one
+    surface: the nearest hit of every camera ray, its depth and zone id, and
+    the value of each named field at the hit, per pixel (no colour map)."""
+
+    def __init__(self, surface: Surface, fields: dict):
+        self.surface = surface
+        self.fields = dict(fields)     # name -> face field on the surface's quads
+        self.names: list[str] = []
+
+    def field_names(self, names):
+        self.names = list(names)
+
+    def render(self, camera: Camera, stream=None) -> ScalarBuffer:
+        rays = camera.create_rays(self.surface.faces.device, stream)
+        buf = ScalarBuffer(camera.width, camera.height, device=self.surface.faces.device)
+        self.render_rays(rays, buf, stream)
+        return buf
+
+    def render_rays(self, rays, buf: ScalarBuffer, stream=None):
+        n = rays.shape[0]
+        dev = self.surface.faces.device
+        hits = self.surface.nearest_hit(rays, stream=stream)
+        L.check(L.lib().drb_scalar_buffer_write(_ptr(rays), _ptr(hits), None, n, 0,
+                                                _ptr(buf.depths), _ptr(buf.zone_ids), None,
+                                                _stream(stream)), "drb_scalar_buffer_write")
+        tf = torch.zeros((1, 4), dtype=torch.float32, device=dev)
+        rng = np.zeros(2, np.float32)
+        for name in self.names:
+            if name not in self.fields:
+                continue
+            frags = torch.empty((n, 4), dtype=torch.float32, device=dev)
+            L.check(L.lib().drb_surface_shade(C.byref(self.surface.faces.desc()),
+                                              C.byref(self.fields[name].desc()), None, _ptr(hits),
+                                              n, _ptr(tf), 1, rng.ctypes.data_as(C.c_void_p),
+                                              None, 0, 0, _ptr(frags), None, None,
+                                              _stream(stream)), "drb_surface_shade")
+            if not buf.has_field(name):
+                buf.add_field(name)
+            L.check(L.lib().drb_scalar_buffer_write(_ptr(rays), _ptr(hits), _ptr(frags), n, 0,
+                                                    None, None, _ptr(buf.scalars[name]),
+                                                    _stream(stream)), "drb_scalar_buffer_write")
+        L.check(L.lib().drb_ray_max(_ptr(rays), _ptr(hits), n, _stream(stream)), "drb_ray_max")
+        return buf
+
+
 class PointLocation:
     """PointLocation (queries/point_location.cpp:178-287), one domain: field
     values at arbitrary points, the empty value where no element holds the

@@ -390,6 +390,15 @@ int drb_surface_shade (const drb_mesh *faces, const drb_mesh *face_field, const 
                        const float *range2, const void *lights, int n_lights, int use_lighting,
                        float *fragments, float *fb_rgba, float *fb_depth, void *stream);
 
+/* The writes of ScalarRenderer::render (rendering/scalar_renderer.cpp:
+ * 296-365) for the rays that hit: depths[pid] = dist and zone_ids[pid] =
+ * hit_idx + zone_offset (each optional), and scalars[pid] = the fragment's
+ * scalar (frags4: {scalar, normal} per ray from drb_surface_shade) when
+ * scalars is given.  pid is the ray's pixel id. */
+int drb_scalar_buffer_write (const void *rays, const void *hits, const float *frags4, int n,
+                             int zone_offset, float *depths, int *zone_ids, float *scalars,
+                             void *stream);
+
 /* ray_max (ray.cpp:243-259): far = hit distance for rays that hit. */
 int drb_ray_max (void *rays, const void *hits, int n, void *stream);
 

@@ -510,6 +510,55 @@ int ref_surface (void *h, int w, int hgt, const float *cam9, float fov, int tf_s
 // values `vals` ((p+1)^3, u fastest) at n reference points; fixed != 0 uses
 // the fixed-order specialisation (orders 1 and 2), else Order::General.
 // This is how the reference's own t_dray_external_evals test drives it.
+// The per-pixel writes of ScalarRenderer::render (rendering/scalar_renderer.cpp
+// :296-365) on the boundary surface and field "f", driven through the same
+// public calls (Surface::nearest_hit, Traceable::fragments): depth and
+// scalar start at NaN and zone ids at -1 (ScalarBuffer's clear values).
+int ref_scalar_render (void *h, int w, int hgt, const float *cam9, float fov, float *depth,
+                       int *zone_id, float *scalar)
+{
+  try
+  {
+    RefMesh *r = static_cast<RefMesh *> (h);
+    MeshBoundary mb;
+    Collection faces = mb.execute (r->collection);
+    Camera cam;
+    setup_camera (cam, w, hgt, cam9, fov);
+    Array<Ray> rays;
+    cam.create_rays (rays);
+    Surface surf (faces);
+    surf.field ("f");
+    Array<RayHit> hits = surf.nearest_hit (rays);
+    Array<Fragment> frags = surf.fragments (hits);
+    const int npix = w * hgt;
+    for (int i = 0; i < npix; ++i)
+    {
+      depth[i] = nan<Float> ();
+      scalar[i] = nan<Float> ();
+      zone_id[i] = -1;
+    }
+    const RayHit *hp = hits.get_host_ptr_const ();
+    const Ray *rp = rays.get_host_ptr_const ();
+    const Fragment *fp = frags.get_host_ptr_const ();
+    for (int i = 0; i < (int)hits.size (); ++i)
+    {
+      if (hp[i].m_hit_idx > -1)
+      {
+        const int pid = rp[i].m_pixel_id;
+        depth[pid] = hp[i].m_dist;
+        zone_id[pid] = hp[i].m_hit_idx;
+        scalar[pid] = fp[i].m_scalar;
+      }
+    }
+    return npix;
+  }
+  catch (const std::exception &e)
+  {
+    g_err = e.what ();
+    return -1;
+  }
+}
+
 // Lineout::execute (queries/lineout.cpp:114-205) on field "f": points
 // float[3 * n_lines * (samples + 2)], values float[n_lines * (samples + 2)].
 int ref_lineout (void *h, int n_lines, const float *starts, const float *ends, int samples,

@@ -47,6 +47,7 @@ def lib():
                                   C.c_int, vp, C.c_int, vp, vp, vp, vp, vp, vp]
         L.ref_eval_hex_scalar.argtypes = [C.c_int, C.c_int, vp, C.c_int, vp, vp, vp]
         L.ref_lineout.argtypes = [vp, C.c_int, vp, vp, C.c_int, C.c_float, vp, vp]
+        L.ref_scalar_render.argtypes = [vp, C.c_int, C.c_int, vp, C.c_float, vp, vp, vp]
         _lib = L
     return _lib
 
@@ -132,6 +133,17 @@ class RefHexMesh:
         if nf < 0:
             raise RuntimeError(lib().ref_last_error().decode())
         return out[: nf * (p + 1) ** 2].reshape(nf, (p + 1) ** 2)
+
+    def scalar_render(self, w, h, cam9, fov):
+        """ScalarRenderer::render's buffers on the boundary surface, field "f":
+        (depth [h, w], zone id [h, w], scalar [h, w])."""
+        cam = np.ascontiguousarray(cam9, np.float32)
+        depth = np.zeros((h, w), np.float32)
+        zone = np.zeros((h, w), np.int32)
+        scal = np.zeros((h, w), np.float32)
+        if lib().ref_scalar_render(self.h, w, h, _p(cam), fov, _p(depth), _p(zone), _p(scal)) < 0:
+            raise RuntimeError(lib().ref_last_error().decode())
+        return depth, zone, scal
 
     def lineout(self, starts, ends, samples, empty=0.0):
         """Lineout::execute on field "f": (points [n, 3], values [n])."""

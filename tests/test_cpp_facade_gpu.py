@@ -115,6 +115,22 @@ def test_cpp_interface_matches_reference(cuda, ref, tmp_path, name):
     hit = np.isfinite(rs["depth"]) & np.isfinite(sdepth) & (rs["depth"] < 1e30)
     assert np.abs(sdepth[hit] - rs["depth"][hit]).max() < 1e-3
 
+    # ScalarRenderer: per-pixel depth, zone id and field value at the hit.
+    raw = np.fromfile(tmp_path / "scalar.bin", np.uint8)
+    npx = w * w
+    sd = raw[: 4 * npx].view(np.float32)
+    sz = raw[4 * npx: 8 * npx].view(np.int32)
+    sv = raw[8 * npx:].view(np.float32)
+    rd, rz, rv = rm.scalar_render(w, w, np.array([*CAM["pos"], *CAM["look_at"], *CAM["up"]],
+                                                 np.float32), CAM["fov"])
+    rd, rz, rv = rd.reshape(-1), rz.reshape(-1), rv.reshape(-1)
+    same = sz == rz
+    assert same.mean() > 0.995
+    hitp = same & (sz >= 0)
+    assert np.abs(sd[hitp] - rd[hitp]).max() < 1e-4
+    assert np.abs(sv[hitp] - rv[hitp]).max() < 1e-4
+    assert np.isnan(sd[sz < 0]).all() and np.isnan(sv[sz < 0]).all()
+
     # Lineout: points bit-identical, values equal (empty value outside).
     raw = np.fromfile(tmp_path / "lineout.bin", np.float32)
     lp = raw[: 3 * 4 * 39].reshape(-1, 3)
