@@ -184,6 +184,121 @@ DRB_D bool face_newton (const CP &cp, const Ray &ray, float (&x)[2], float &t, f
   return converged && inside && ray.near_t <= t && t < ray.far_t;
 }
 
+// ---- order-1 faces: Lagae & Dutre ray/bilinear-patch test ----
+// The reference intersects order-1 quads in closed form ("An Efficient
+// Ray-Quadrilateral Intersection Test", Lagae and Dutre 2005;
+// rendering/low_order_intersectors.hpp:20-206, used by
+// FaceIntersector<Quad_P1>, rendering/surface.cpp:253-300) instead of
+// Newton.  Restated with every operation rounded in the reference's order
+// (Vec dot: running sum from 0; cross: a1 b2 - a2 b1, ...), on the absolute
+// corner coordinates, so distances and (u, v) match its float results.
+struct V3
+{
+  float x, y, z;
+};
+DRB_D V3 vsub (V3 a, V3 b) { return { __fsub_rn (a.x, b.x), __fsub_rn (a.y, b.y), __fsub_rn (a.z, b.z) }; }
+DRB_D V3 vcross (V3 a, V3 b)
+{
+  return { __fsub_rn (__fmul_rn (a.y, b.z), __fmul_rn (a.z, b.y)),
+           __fsub_rn (__fmul_rn (a.z, b.x), __fmul_rn (a.x, b.z)),
+           __fsub_rn (__fmul_rn (a.x, b.y), __fmul_rn (a.y, b.x)) };
+}
+DRB_D float vdot (V3 a, V3 b)
+{
+  float r = 0.f;
+  r = __fadd_rn (r, __fmul_rn (a.x, b.x));
+  r = __fadd_rn (r, __fmul_rn (a.y, b.y));
+  r = __fadd_rn (r, __fmul_rn (a.z, b.z));
+  return r;
+}
+
+// distance (INFINITY on a miss), alpha, beta, e01, e03 of the quad
+// v00 v10 v11 v01
+DRB_D float ld_intersect (V3 v00, V3 v10, V3 v11, V3 v01, V3 o, V3 d, float &alpha, float &beta,
+                          V3 &e01, V3 &e03)
+{
+  const float eps = 0.00001f;
+  float distance = INFINITY;
+  e03 = vsub (v01, v00);
+  const V3 p = vcross (d, e03);
+  e01 = vsub (v10, v00);
+  const float det = vdot (e01, p);
+  bool hit = true;
+  const float rel_eps = __fmul_rn (__fsqrt_rn (vdot (e03, e03)), eps);
+  if (fabsf (det) < rel_eps) hit = false;
+  const float inv_det = __fdiv_rn (1.0f, det);
+  const V3 t = vsub (o, v00);
+  alpha = __fmul_rn (vdot (t, p), inv_det);
+  if (alpha < 0.f) hit = false;
+  const V3 q = vcross (t, e01);
+  beta = __fmul_rn (vdot (d, q), inv_det);
+  if (beta < 0.f) hit = false;
+  if (__fadd_rn (alpha, beta) > 1.0f)
+  {
+    const V3 e23 = vsub (v01, v11);
+    const V3 e21 = vsub (v10, v11);
+    const V3 pp = vcross (d, e21);
+    const float detp = vdot (e23, pp);
+    if (fabsf (detp) < rel_eps) hit = false;
+    const float inv_detp = __fdiv_rn (1.0f, detp);
+    const V3 tp = vsub (o, v11);
+    const float alpha_p = __fmul_rn (vdot (tp, pp), inv_detp);
+    if (alpha_p < 0.f) hit = false;
+    const V3 qp = vcross (tp, e23);
+    const float beta_p = __fmul_rn (vdot (d, qp), inv_detp);
+    if (beta_p < 0.f) hit = false;
+  }
+  if (hit) distance = __fmul_rn (vdot (e03, q), inv_det);
+  return distance;
+}
+
+// bilinear (u, v) of the hit from its barycentric alpha, beta (quad_ref_point)
+DRB_D void ld_ref_point (V3 v00, V3 v11, float alpha, float beta, V3 e01, V3 e03, float &u, float &v)
+{
+  const float eps = 0.00001f;
+  float a11, b11;
+  const V3 e02 = vsub (v11, v00);
+  const V3 n = vcross (e01, e02);
+  if (fabsf (n.x) >= fabsf (n.y) && fabsf (n.x) >= fabsf (n.z))
+  {
+    a11 = __fdiv_rn (__fsub_rn (__fmul_rn (e02.y, e03.z), __fmul_rn (e02.z, e03.y)), n.x);
+    b11 = __fdiv_rn (__fsub_rn (__fmul_rn (e01.y, e02.z), __fmul_rn (e01.z, e02.y)), n.x);
+  }
+  else if (fabsf (n.y) >= fabsf (n.x) && fabsf (n.y) >= fabsf (n.z))
+  {
+    a11 = __fdiv_rn (__fsub_rn (__fmul_rn (e02.z, e03.x), __fmul_rn (e02.x, e03.z)), n.y);
+    b11 = __fdiv_rn (__fsub_rn (__fmul_rn (e01.z, e02.x), __fmul_rn (e01.x, e02.z)), n.y);
+  }
+  else
+  {
+    a11 = __fdiv_rn (__fsub_rn (__fmul_rn (e02.x, e03.y), __fmul_rn (e02.y, e03.x)), n.z);
+    b11 = __fdiv_rn (__fsub_rn (__fmul_rn (e01.x, e02.y), __fmul_rn (e01.y, e02.x)), n.z);
+  }
+  if (fabsf (__fsub_rn (a11, 1.0f)) < eps)
+  {
+    u = alpha;
+    if (fabsf (__fsub_rn (b11, 1.0f)) < eps) v = beta;
+    else v = __fdiv_rn (beta, __fadd_rn (__fmul_rn (u, __fsub_rn (b11, 1.0f)), 1.0f));
+  }
+  else if (fabsf (__fsub_rn (b11, 1.0f)) < eps)
+  {
+    v = beta;
+    u = __fdiv_rn (alpha, __fadd_rn (__fmul_rn (v, __fsub_rn (a11, 1.0f)), 1.0f));
+  }
+  else
+  {
+    const float A = __fsub_rn (1.0f, b11);
+    const float B = __fsub_rn (__fsub_rn (__fmul_rn (alpha, __fsub_rn (b11, 1.0f)),
+                                          __fmul_rn (beta, __fsub_rn (a11, 1.0f))), 1.0f);
+    const float Cc = alpha;
+    const float D = __fsub_rn (__fmul_rn (B, B), __fmul_rn (__fmul_rn (4.0f, A), Cc));
+    const float Q = __fmul_rn (-0.5f, __fadd_rn (B, __fmul_rn (B < 0.f ? -1.0f : 1.0f, __fsqrt_rn (D))));
+    u = __fdiv_rn (Q, A);
+    if (u < 0.f || u > 1.f) u = __fdiv_rn (Cc, Q);
+    v = __fdiv_rn (beta, __fadd_rn (__fmul_rn (u, __fsub_rn (b11, 1.0f)), 1.0f));
+  }
+}
+
 // packed face rows are read like packed hex rows (PackedCP, with its
 // vector row loads at orders 2 and 3)
 using QuadPackedCP = PackedCP;
@@ -275,7 +390,30 @@ surface_kernel (SurfParams sp, const Ray *__restrict__ rays, int n, RayHit *__re
       int steps = 0;
       ++cands;
       bool inside;
-      if (sp.packed)
+      if (P == 1)
+      {
+        // closed form on the absolute corners (dofs (0,0) (1,0) (0,1) (1,1))
+        const int *ci = sp.ctrl_idx + (size_t)el * 4;
+        V3 c[4];
+#pragma unroll
+        for (int k = 0; k < 4; ++k)
+        {
+          const float *q = sp.xyz + 3 * (size_t)__ldg (ci + k);
+          c[k] = { __ldg (q), __ldg (q + 1), __ldg (q + 2) };
+        }
+        float alpha, beta;
+        V3 e01, e03;
+        const V3 o = { ray.orig.x, ray.orig.y, ray.orig.z }, dd = { ray.dir.x, ray.dir.y, ray.dir.z };
+        const float dist = ld_intersect (c[0], c[1], c[3], c[2], o, dd, alpha, beta, e01, e03);
+        inside = false;
+        if (dist != INFINITY)
+        {
+          ld_ref_point (c[0], c[3], alpha, beta, e01, e03, x[0], x[1]);
+          inside = dist < ray.far_t;
+          t = dist;
+        }
+      }
+      else if (sp.packed)
       {
         // packed rows are relative to the face's first control point
         const float *row = sp.packed + (size_t)el * sp.stride;

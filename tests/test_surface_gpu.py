@@ -15,10 +15,12 @@ def _mesh(name):
         return meshgen.warped_mesh(8, 3, 0.08, jitter=0.01, seed=1)
     if name == "p2_8":
         return meshgen.workload_mesh("volume_8")
+    if name == "p1_8":
+        return meshgen.warped_mesh(8, 1, 0.05, jitter=0.01, seed=3)
     raise KeyError(name)
 
 
-@pytest.mark.parametrize("name", ["p3_8", "p2_8"])
+@pytest.mark.parametrize("name", ["p3_8", "p2_8", "p1_8"])
 def test_boundary_faces_identical(cuda, ref, name):
     import torch
     from devil_ray_b200 import api
@@ -34,7 +36,7 @@ def test_boundary_faces_identical(cuda, ref, name):
     assert np.array_equal(g, rf)
 
 
-@pytest.mark.parametrize("name", ["p3_8", "p2_8"])
+@pytest.mark.parametrize("name", ["p3_8", "p2_8", "p1_8"])
 def test_surface_render_matches_reference(cuda, ref, name):
     import torch
     from devil_ray_b200 import api, meshgen
@@ -68,6 +70,11 @@ def test_surface_render_matches_reference(cuda, ref, name):
     both = same & (gidx >= 0)
     assert np.abs(h[both, 1] - rs["dist"][both]).max() < 1e-4
     assert np.abs(h[both, 2:4] - rs["ref"][both]).max() < 1e-3
+    if name == "p1_8":
+        # order-1 faces: the closed-form test restated operation for
+        # operation, so distances and (u, v) are the reference's bit for bit
+        assert np.array_equal(h[both, 1].view(np.int32), rs["dist"][both].view(np.int32))
+        assert np.array_equal(h[both, 2:4].view(np.int32), rs["ref"][both].view(np.int32))
     img = fb.image()
     d = np.abs(img - rs["rgba"])
     bad = np.any(d > 1.0 / 255.0, axis=-1)
