@@ -128,6 +128,10 @@ class ClockSampler:
                 "reasons": sorted(reasons), "samples": len(sm)}
 
 
+WORKLOAD_DESC = ("locate_64: 64^3 hex order 2, trilinear distortion 15%, 16M uniform queries "
+                 "(8% outside), tol 1e-5, 20 steps")
+
+
 def reference_arm(args, rank, world):
     """--impl reference: the reference's CPU Mesh::locate (oracle/_ref)."""
     if rank != 0:
@@ -157,12 +161,15 @@ def reference_arm(args, rank, world):
     t = float(np.mean(times))
     value = located / t
     line = {"impl": "reference", "metric": METRIC, "value": value, "unit": "points/s",
-            "n_gpus": 0, "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * t,
+            "n_gpus": world, "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * t,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
             "data": "synthetic",
-            "config": {"workload": WORKLOAD + " (reference CPU, sample per step)",
-                       "queries_per_step": sample, "tol": 1e-4, "max_steps": 20,
-                       "note": "reference Newton tolerance is hard-coded to 1e-4"},
+            "config": {"workload": WORKLOAD_DESC, "queries_per_gpu": args.queries,
+                       "elements": m.n_elem, "queries_per_step": sample,
+                       "path": "reference OpenMP Mesh::locate on the host cores",
+                       "tol": 1e-4, "max_steps": 20,
+                       "note": "reference Newton tolerance is hard-coded to 1e-4; each step "
+                               "locates a bounded sample of the workload's queries"},
             "cpu_baseline": {"value": value, "unit": "points/s", "cores": threads,
                              "kind": "reference",
                              "sample": f"{sample} of the 16M queries per step, BVH built once "
@@ -770,8 +777,7 @@ def main():
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_step,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
             "dtype": "f32", "data": "synthetic",
-            "config": {"workload": "locate_64: 64^3 hex order 2, trilinear distortion 15%, "
-                                   "16M uniform queries (8% outside), tol 1e-5, 20 steps",
+            "config": {"workload": WORKLOAD_DESC,
                        "queries_per_gpu": n, "elements": m.n_elem, "bvh_leaves": bvh.n_leaf,
                        "path": head_name, "launch_config": best_cfg.as_dict(),
                        "l2": "inputs larger than L2 (201 MB queries, 553 MB BVH nodes)",
