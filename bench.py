@@ -69,10 +69,8 @@ def parse():
 
 
 def dist_info():
-    rank = int(os.environ.get("RANK", "0"))
-    world = int(os.environ.get("WORLD_SIZE", "1"))
-    local = int(os.environ.get("LOCAL_RANK", "0"))
-    return rank, world, local
+    from devil_ray_b200 import dist as D
+    return D.dist_info()
 
 
 class ClockSampler:
@@ -149,7 +147,8 @@ def reference_arm(args, rank, world):
     build_s = time.perf_counter() - t0
     threads = refpy.num_threads()
     sample = args.cpu_sample or 131072
-    q = meshgen.uniform_queries(args.queries, 1000 + rank)[:sample]
+    from devil_ray_b200 import dist as D
+    q = meshgen.uniform_queries(args.queries, D.shard_seed(rank))[:sample]
     for _ in range(max(args.warmup, 0) and 1):
         r.locate(q[:4096])
     times, located = [], 0
@@ -530,15 +529,11 @@ def main():
     torch.cuda.set_device(dev)
     if args.profile_volume:
         return profile_volume(dev, args)
-    pg = None
-    if world > 1:
-        import torch.distributed as dist
-        from datetime import timedelta
-        dist.init_process_group("nccl", timeout=timedelta(seconds=120))
-        pg = dist
+    from devil_ray_b200 import dist as D
+    pg = D.init("nccl", timeout_s=120)  # None on one GPU
 
     m = meshgen.workload_mesh(WORKLOAD)
-    queries = meshgen.uniform_queries(args.queries, 1000 + rank)
+    queries = meshgen.uniform_queries(args.queries, D.shard_seed(rank))
     mesh = api.UnstructuredMesh(m.ctrl_idx, m.xyz, m.order, device=dev)
     bvh = mesh.get_bvh()
     # BVH build timed warm (the first call includes lazy module loading)
@@ -570,12 +565,11 @@ def main():
             fn()
         s1.record()
         torch.cuda.synchronize()
-        ms = s0.elapsed_time(s1)
-        if pg:
-            t = torch.tensor([ms], device=dev)
-            pg.all_reduce(t, op=pg.ReduceOp.MAX)
-            ms = float(t.item())
-        return ms
+        return D.max_over_ranks(pg, s0.elapsed_time(s1), dev)
+
+    def job_located(count):
+        """All ranks' located points (each rank locates its own shard)."""
+        return D.sum_over_ranks(pg, count, dev)
 
     def batched_step():
         loc.locate(pts, out=(cell, ref))
@@ -602,7 +596,7 @@ def main():
     # batched path (element-centre guess)
     batched_ms = timed(batched_step, args.steps) / args.steps
     located = int((cell >= 0).sum().item())
-    batched_value = world * located / (batched_ms * 1e-3)
+    batched_value = job_located(located) / (batched_ms * 1e-3)
     # binary-tree node visits of the same queries (the reference's traversal),
     # for the algorithmic bytes; the timed path walks the 4-wide tree
     _, _, _, _, nd_bin = api.BatchedLocator(mesh, TOL, MAX_STEPS, L.GUESS_ELEM_CENTER,
@@ -618,7 +612,7 @@ def main():
         plain_step()
     k_plain = max(2, args.steps // 5)
     plain_ms = timed(plain_step, k_plain) / k_plain
-    plain_value = world * located / (plain_ms * 1e-3)
+    plain_value = job_located(located) / (plain_ms * 1e-3)
     # persistent kernel alone (roofline), queries already ordered
     order = loc.order(pts)
     kern_ms = timed(lambda: loc.locate(pts, order=order, out=(cell, ref)), args.steps) / args.steps
@@ -632,7 +626,7 @@ def main():
     sub_ms = timed(lambda: loc_sub.locate(pts, out=(cell, ref)), args.steps) / args.steps
     sub_located = int((cell >= 0).sum().item())
     _, _, it_s, _, _ = loc_sub.locate(pts, stats=True)
-    sub_value = world * sub_located / (sub_ms * 1e-3)
+    sub_value = job_located(sub_located) / (sub_ms * 1e-3)
     batched_sub = {"value": sub_value, "ms_per_step": sub_ms,
                    "mean_newton_iters": float(it_s.float().mean()),
                    "note": "Morton-ordered persistent kernel, sub-box-centre guess"}
@@ -669,7 +663,7 @@ def main():
         _, fg, ig = LG.newton_pairs(mesh, he, hp, TOL, MAX_STEPS, gss)
         _, fc, ic = LG.newton_pairs(mesh, he, hp, TOL, MAX_STEPS)
         ok = fc
-        learned_value = world * located_l / (ms_l * 1e-3)
+        learned_value = job_located(located_l) / (ms_l * 1e-3)
         learned = {"value": learned_value, "ms_per_step": ms_l, "located": located_l,
                    "cell_agreement_with_centre_guess": agree,
                    "mean_newton_iters": float(it_l.float().mean()),
@@ -699,7 +693,7 @@ def main():
     launches = L.lib().drb_kernel_launches() - launches0
     clk = clocks.stop()
     located = int((cell >= 0).sum().item())
-    value = world * located / (ms_step * 1e-3)
+    value = job_located(located) / (ms_step * 1e-3)
 
     # algorithmic bytes per located point: point 12 B + Location 16 B + one
     # element's control-point indices and coordinates nd x (4 + 12) B + its
@@ -741,7 +735,7 @@ def main():
     e2e_step()
     e2e_ms = timed(e2e_step, args.steps) / args.steps
     e2e_located = int((host_cell >= 0).sum())
-    e2e_value = world * e2e_located / (e2e_ms * 1e-3)
+    e2e_value = job_located(e2e_located) / (e2e_ms * 1e-3)
 
     vol = None
     if not args.no_volume:
