@@ -23,12 +23,15 @@ GUESS_ELEM_CENTER = 1
 GUESS_SUBREF_CENTER = 2
 GUESS_GIVEN = 3
 
+SHAPE_TENSOR = 0
+SHAPE_SIMPLEX = 1
+
 
 class DrbMesh(C.Structure):
     _fields_ = [("dim", C.c_int), ("order", C.c_int), ("ncomp", C.c_int),
                 ("n_elem", C.c_int), ("n_ctrl", C.c_int),
                 ("ctrl_idx", C.c_void_p), ("values", C.c_void_p), ("packed", C.c_void_p),
-                ("face_neighbors", C.c_void_p)]
+                ("face_neighbors", C.c_void_p), ("shape", C.c_int)]
 
 
 class DrbBvh(C.Structure):
@@ -134,6 +137,9 @@ _SIGS = {
                                   C.POINTER(DrbNewtonOpts), C.c_void_p, C.POINTER(C.c_float),
                                   C.c_void_p]),
     "drb_packed_stride": (C.c_int, [C.c_int, C.c_int, C.c_int]),
+    "drb_elem_dofs": (C.c_int, [C.c_int, C.c_int, C.c_int]),
+    "drb_packed_stride_shape": (C.c_int, [C.c_int, C.c_int, C.c_int, C.c_int]),
+    "drb_ref_box_floats": (C.c_int, [C.c_int, C.c_int]),
     "drb_pack_elements": (C.c_int, [C.POINTER(DrbMesh), C.c_void_p, C.c_void_p]),
     "drb_bvh_sizes": (C.c_int, [C.c_int, C.c_int, C.POINTER(C.c_int), C.POINTER(C.c_int)]),
     "drb_elem_subboxes": (C.c_int, [C.POINTER(DrbMesh), C.c_void_p, C.c_void_p, C.c_void_p,

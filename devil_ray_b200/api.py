@@ -53,14 +53,15 @@ class GridFunction:
 class BVH:
     """Device BVH in the reference layout (4 x float4 per inner node)."""
 
-    def __init__(self, dim: int, n_elem: int, device):
+    def __init__(self, dim: int, n_elem: int, device, shape: int = L.SHAPE_TENSOR):
         ni, nl = C.c_int(), C.c_int()
         L.check(L.lib().drb_bvh_sizes(dim, n_elem, C.byref(ni), C.byref(nl)), "drb_bvh_sizes")
         self.n_inner, self.n_leaf = ni.value, nl.value
         self.inner_nodes = torch.empty((self.n_inner, 16), dtype=torch.float32, device=device)
         self.leaf_nodes = torch.empty(self.n_leaf, dtype=torch.int32, device=device)
         self.aabb_ids = torch.empty(self.n_leaf, dtype=torch.int32, device=device)
-        self.ref_boxes = torch.empty((self.n_leaf, 2 * dim), dtype=torch.float32, device=device)
+        rbf = L.lib().drb_ref_box_floats(shape, dim)
+        self.ref_boxes = torch.empty((self.n_leaf, rbf), dtype=torch.float32, device=device)
         self.bounds = np.zeros(6, np.float32)
         self.sorted_codes = None
         # optional 4-wide traversal tree (drb_bvh_widen)
@@ -103,12 +104,18 @@ class BVH:
 
 
 class UnstructuredMesh:
-    """Tensor Bernstein hex (dim 3) or quad (dim 2) mesh of order 1..3."""
+    """Bernstein mesh of order 1..3: tensor hex (dim 3) or quad (dim 2)
+    elements, or with shape=SHAPE_SIMPLEX tets (dim 3) - the reference's
+    UnstructuredMesh<Hex*/Quad*/Tet*> (data_model/unstructured_mesh.hpp)."""
 
-    def __init__(self, ctrl_idx, xyz, order: int, dim: int = 3, device="cuda", pack: bool = True):
+    def __init__(self, ctrl_idx, xyz, order: int, dim: int = 3, device="cuda", pack: bool = True,
+                 shape: int = L.SHAPE_TENSOR):
         self.dim = dim
         self.order = int(order)
-        nd = (self.order + 1) ** dim
+        self.shape = int(shape)
+        nd = L.lib().drb_elem_dofs(self.shape, dim, self.order)
+        if nd < 0:
+            raise ValueError(f"unsupported mesh: shape {shape}, dim {dim}, order {order}")
         self.dof_data = GridFunction(_dev(ctrl_idx, torch.int32, device),
                                      _dev(xyz, torch.float32, device).reshape(-1, 3), nd)
         self.device = torch.device(device)
@@ -128,6 +135,7 @@ class UnstructuredMesh:
     def desc(self, packed: bool = True) -> L.DrbMesh:
         m = L.DrbMesh()
         m.dim, m.order, m.ncomp = self.dim, self.order, 3
+        m.shape = self.shape
         m.n_elem = self.n_elem
         m.n_ctrl = self.dof_data.values.shape[0]
         m.ctrl_idx = self.dof_data.ctrl_idx.data_ptr()
@@ -150,7 +158,7 @@ class UnstructuredMesh:
         return self._neighbors
 
     def pack(self, stream=None):
-        stride = L.lib().drb_packed_stride(self.dim, self.order, 3)
+        stride = L.lib().drb_packed_stride_shape(self.shape, self.dim, self.order, 3)
         self.packed = torch.empty((max(self.n_elem, 1), stride), dtype=torch.float32,
                                   device=self.device)
         d = self.desc(packed=False)
@@ -159,8 +167,8 @@ class UnstructuredMesh:
 
     def get_bvh(self, stream=None, keep_codes: bool = False) -> BVH:
         """Lazily build the LBVH (UnstructuredMesh::get_bvh,
-        data_model/unstructured_mesh.cpp:23-31), and for hex meshes its
-        4-wide traversal tree."""
+        data_model/unstructured_mesh.cpp:23-31), and for hex and tet meshes
+        its 4-wide traversal tree."""
         if self._bvh is None:
             self._bvh = self.build_bvh(stream, keep_codes)
             if self.dim == 3:
@@ -168,7 +176,7 @@ class UnstructuredMesh:
         return self._bvh
 
     def build_bvh(self, stream=None, keep_codes: bool = False) -> BVH:
-        b = BVH(self.dim, self.n_elem, self.device)
+        b = BVH(self.dim, self.n_elem, self.device, self.shape)
         codes = None
         if keep_codes:
             codes = torch.empty(b.n_leaf, dtype=torch.int32, device=self.device)
@@ -309,7 +317,8 @@ def elem_subboxes(mesh: UnstructuredMesh, stream=None):
     dev = mesh.device
     aabbs = torch.empty((n, 6), dtype=torch.float32, device=dev)
     prim = torch.empty(n, dtype=torch.int32, device=dev)
-    refb = torch.empty((n, 2 * mesh.dim), dtype=torch.float32, device=dev)
+    rbf = L.lib().drb_ref_box_floats(mesh.shape, mesh.dim)
+    refb = torch.empty((n, rbf), dtype=torch.float32, device=dev)
     bounds = torch.empty(6, dtype=torch.float32, device=dev)
     d = mesh.desc()
     L.check(L.lib().drb_elem_subboxes(C.byref(d), _ptr(aabbs), _ptr(prim), _ptr(refb),

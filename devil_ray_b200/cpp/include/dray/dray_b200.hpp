@@ -97,6 +97,15 @@ using HexScalar_P2 = Element<3, 1, Tensor, Order::Quadratic>;
 using QuadScalar = Element<2, 1, Tensor, Order::General>;
 using QuadScalar_P1 = Element<2, 1, Tensor, Order::Linear>;
 using QuadScalar_P2 = Element<2, 1, Tensor, Order::Quadratic>;
+// Tets (data_model/unstructured_mesh.hpp:121-124, unstructured_field.hpp:95-98).
+// The fixed-order Linear type evaluates like the general one here: the
+// reference's Tet_P1 eval_d leaves two derivatives unset (elem_ops.hpp:785-815).
+using Tet3 = Element<3, 3, Simplex, Order::General>;
+using Tet_P1 = Element<3, 3, Simplex, Order::Linear>;
+using Tet_P2 = Element<3, 3, Simplex, Order::Quadratic>;
+using TetScalar = Element<3, 1, Simplex, Order::General>;
+using TetScalar_P1 = Element<3, 1, Simplex, Order::Linear>;
+using TetScalar_P2 = Element<3, 1, Simplex, Order::Quadratic>;
 
 template <int32 PhysDim> struct GridFunction
 {
@@ -198,18 +207,20 @@ class Field
   virtual void eval (const Array<Location> locs, Array<Float> &values) = 0;
 };
 
-// Non-template core of UnstructuredMesh (dim 3 hex or dim 2 quad).
-class TensorMesh : public Mesh
+// Non-template core of UnstructuredMesh (dim 3 hex or tet, dim 2 quad).
+class ElementMesh : public Mesh
 {
   protected:
   GridFunction<3> m_dof_data;
   int32 m_poly_order;
   int32 m_dim;
+  ElemType m_etype;
   std::shared_ptr<DeviceGeometry> m_dev;
   public:
   LocateSettings m_locate;
-  TensorMesh (const GridFunction<3> &dof, int32 order, int32 dim);
-  ~TensorMesh () override;
+  ElementMesh (const GridFunction<3> &dof, int32 order, int32 dim, ElemType etype = Tensor);
+  ElemType etype () const { return m_etype; }
+  ~ElementMesh () override;
   int32 cells () const override { return m_dof_data.get_num_elem (); }
   int32 order () const override { return m_poly_order; }
   int32 dims () const override { return m_dim; }
@@ -221,20 +232,22 @@ class TensorMesh : public Mesh
   const drb_bvh *device_bvh ();
 };
 
-template <class ElemT> class UnstructuredMesh : public TensorMesh
+template <class ElemT> class UnstructuredMesh : public ElementMesh
 {
-  static_assert (ElemT::get_etype () == Tensor, "only tensor (hex/quad) elements are on this path");
+  static_assert (ElemT::get_etype () == Tensor || ElemT::get_dim () == 3,
+                 "hex, quad and tet elements are on this path (no triangles)");
   static_assert (ElemT::get_ncomp () == 3, "meshes have 3 components");
   public:
   UnstructuredMesh (const GridFunction<3> &dof, int32 order)
-  : TensorMesh (dof, order, ElemT::get_dim ())
+  : ElementMesh (dof, order, ElemT::get_dim (), ElemT::get_etype ())
   {
     if (ElemT::get_P () != Order::General && ElemT::get_P () != order)
       DRAY_ERROR ("Fixed order mismatch. Poly order " << order << " template " << ElemT::get_P ());
   }
   std::string type_name () const override
   {
-    return std::string (ElemT::get_dim () == 3 ? "Hex" : "Quad") + "_P" + std::to_string (m_poly_order);
+    const char *n = ElemT::get_etype () == Simplex ? "Tet" : ElemT::get_dim () == 3 ? "Hex" : "Quad";
+    return std::string (n) + "_P" + std::to_string (m_poly_order);
   }
 };
 using HexMesh = UnstructuredMesh<Hex3>;
@@ -243,18 +256,23 @@ using HexMesh_P2 = UnstructuredMesh<Hex_P2>;
 using QuadMesh = UnstructuredMesh<Quad3>;
 using QuadMesh_P1 = UnstructuredMesh<Quad_P1>;
 using QuadMesh_P2 = UnstructuredMesh<Quad_P2>;
+using TetMesh = UnstructuredMesh<Tet3>;
+using TetMesh_P1 = UnstructuredMesh<Tet_P1>;
+using TetMesh_P2 = UnstructuredMesh<Tet_P2>;
 
-class TensorField : public Field
+class ElementField : public Field
 {
   protected:
   GridFunction<1> m_dof_data;
   int32 m_poly_order;
   int32 m_dim;
+  ElemType m_etype;
   std::shared_ptr<DeviceGeometry> m_dev;
   mutable std::vector<Range> m_range;
   public:
-  TensorField (const GridFunction<1> &dof, int32 order, int32 dim, const std::string &name);
-  ~TensorField () override;
+  ElementField (const GridFunction<1> &dof, int32 order, int32 dim, const std::string &name,
+                ElemType etype = Tensor);
+  ~ElementField () override;
   std::vector<Range> range () const override;
   int32 order () const override { return m_poly_order; }
   int32 components () const override { return 1; }
@@ -263,19 +281,21 @@ class TensorField : public Field
   const drb_mesh *device_field ();
 };
 
-template <class ElemT> class UnstructuredField : public TensorField
+template <class ElemT> class UnstructuredField : public ElementField
 {
-  static_assert (ElemT::get_etype () == Tensor && ElemT::get_ncomp () == 1,
-                 "only scalar tensor fields are on this path");
+  static_assert ((ElemT::get_etype () == Tensor || ElemT::get_dim () == 3) && ElemT::get_ncomp () == 1,
+                 "only scalar hex, quad and tet fields are on this path");
   public:
   UnstructuredField (const GridFunction<1> &dof, int32 order, const std::string &name = "")
-  : TensorField (dof, order, ElemT::get_dim (), name)
+  : ElementField (dof, order, ElemT::get_dim (), name, ElemT::get_etype ())
   {
   }
   std::string type_name () const override
   {
-    return std::string (ElemT::get_dim () == 3 ? "HexScalar" : "QuadScalar") + "_P" +
-           std::to_string (m_poly_order);
+    const char *n = ElemT::get_etype () == Simplex ? "TetScalar"
+                    : ElemT::get_dim () == 3      ? "HexScalar"
+                                                  : "QuadScalar";
+    return std::string (n) + "_P" + std::to_string (m_poly_order);
   }
 };
 

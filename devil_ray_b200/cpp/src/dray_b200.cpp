@@ -44,12 +44,12 @@ template <typename T> struct DevBuf
   ~DevBuf () { release (); }
 };
 
-int32 nd_of (int32 dim, int32 order)
+int32 nd_of (int32 dim, int32 order, ElemType etype)
 {
-  int32 nd = 1;
-  for (int d = 0; d < dim; ++d) nd *= order + 1;
-  return nd;
+  return drb_elem_dofs (etype == Simplex ? DRB_SHAPE_SIMPLEX : DRB_SHAPE_TENSOR, dim, order);
 }
+
+int shape_of (ElemType etype) { return etype == Simplex ? DRB_SHAPE_SIMPLEX : DRB_SHAPE_TENSOR; }
 } // namespace
 
 // Device copies, packed element rows and (for meshes) the lazily built BVH.
@@ -65,30 +65,32 @@ struct DeviceGeometry
 
 // ------------------------------------------------------------ meshes --
 
-TensorMesh::TensorMesh (const GridFunction<3> &dof, int32 order, int32 dim)
-: m_dof_data (dof), m_poly_order (order), m_dim (dim), m_dev (std::make_shared<DeviceGeometry> ())
+ElementMesh::ElementMesh (const GridFunction<3> &dof, int32 order, int32 dim, ElemType etype)
+: m_dof_data (dof), m_poly_order (order), m_dim (dim), m_etype (etype),
+  m_dev (std::make_shared<DeviceGeometry> ())
 {
   if (order < 1 || order > 3) DRAY_ERROR ("polynomial order " << order << " is outside 1..3");
-  if (dof.m_el_dofs != nd_of (dim, order))
+  if (dof.m_el_dofs != nd_of (dim, order, etype))
     DRAY_ERROR ("GridFunction has " << dof.m_el_dofs << " dofs per element, order " << order
-                                    << " needs " << nd_of (dim, order));
+                                    << " needs " << nd_of (dim, order, etype));
 }
 
-TensorMesh::~TensorMesh () {}
+ElementMesh::~ElementMesh () {}
 
-const drb_mesh *TensorMesh::device_mesh ()
+const drb_mesh *ElementMesh::device_mesh ()
 {
   DeviceGeometry &g = *m_dev;
   if (!g.mesh.ctrl_idx || g.mesh.n_elem != cells ())
   {
     g.mesh.dim = m_dim;
+    g.mesh.shape = shape_of (m_etype);
     g.mesh.order = m_poly_order;
     g.mesh.ncomp = 3;
     g.mesh.n_elem = cells ();
     g.mesh.n_ctrl = (int)m_dof_data.m_values.size ();
     g.mesh.ctrl_idx = m_dof_data.m_ctrl_idx.get_device_ptr_const ();
     g.mesh.values = (const float *)m_dof_data.m_values.get_device_ptr_const ();
-    const int stride = drb_packed_stride (m_dim, m_poly_order, 3);
+    const int stride = drb_packed_stride_shape (g.mesh.shape, m_dim, m_poly_order, 3);
     g.packed.alloc ((size_t)std::max (cells (), 1) * stride);
     g.mesh.packed = nullptr;
     drb_check (drb_pack_elements (&g.mesh, g.packed.p, nullptr), "drb_pack_elements");
@@ -97,7 +99,7 @@ const drb_mesh *TensorMesh::device_mesh ()
   return &g.mesh;
 }
 
-const drb_bvh *TensorMesh::device_bvh ()
+const drb_bvh *ElementMesh::device_bvh ()
 {
   DeviceGeometry &g = *m_dev;
   device_mesh ();
@@ -108,7 +110,7 @@ const drb_bvh *TensorMesh::device_bvh ()
     g.inner.alloc ((size_t)16 * ni);
     g.leaf.alloc (nl);
     g.ids.alloc (nl);
-    g.refb.alloc ((size_t)2 * m_dim * nl);
+    g.refb.alloc ((size_t)drb_ref_box_floats (g.mesh.shape, m_dim) * nl);
     g.bvh.n_inner = ni;
     g.bvh.n_leaf = nl;
     g.bvh.inner_nodes = g.inner.p;
@@ -122,6 +124,9 @@ const drb_bvh *TensorMesh::device_bvh ()
       drb_check (drb_bvh_widen (&g.bvh, nullptr, 0, nullptr), "drb_bvh_widen");
       g.wide.alloc ((size_t)32 * g.bvh.n_wide);
       drb_check (drb_bvh_widen (&g.bvh, g.wide.p, g.bvh.n_wide, nullptr), "drb_bvh_widen");
+    }
+    if (m_dim == 3 && m_etype == Tensor)
+    {
       // face neighbours: the volume march steps across faces with them
       g.nbr.alloc ((size_t)6 * cells ());
       drb_check (drb_mesh_face_neighbors (&g.mesh, g.nbr.p, nullptr), "drb_mesh_face_neighbors");
@@ -132,7 +137,7 @@ const drb_bvh *TensorMesh::device_bvh ()
   return &g.bvh;
 }
 
-AABB<3> TensorMesh::bounds ()
+AABB<3> ElementMesh::bounds ()
 {
   const drb_bvh *b = device_bvh ();
   AABB<3> r;
@@ -147,9 +152,9 @@ AABB<3> TensorMesh::bounds ()
   return r;
 }
 
-Array<Location> TensorMesh::locate (Array<Vec<Float, 3>> &wpoints)
+Array<Location> ElementMesh::locate (Array<Vec<Float, 3>> &wpoints)
 {
-  if (m_dim != 3) DRAY_ERROR ("locate needs a volume (hex) mesh");
+  if (m_dim != 3) DRAY_ERROR ("locate needs a volume (hex or tet) mesh");
   const int n = (int)wpoints.size ();
   Array<Location> out;
   out.resize (n);
@@ -178,28 +183,31 @@ Array<Location> TensorMesh::locate (Array<Vec<Float, 3>> &wpoints)
 
 // ------------------------------------------------------------ fields --
 
-TensorField::TensorField (const GridFunction<1> &dof, int32 order, int32 dim, const std::string &name)
-: m_dof_data (dof), m_poly_order (order), m_dim (dim), m_dev (std::make_shared<DeviceGeometry> ())
+ElementField::ElementField (const GridFunction<1> &dof, int32 order, int32 dim, const std::string &name,
+                            ElemType etype)
+: m_dof_data (dof), m_poly_order (order), m_dim (dim), m_etype (etype),
+  m_dev (std::make_shared<DeviceGeometry> ())
 {
   m_name = name;
   if (order < 1 || order > 3) DRAY_ERROR ("polynomial order " << order << " is outside 1..3");
 }
 
-TensorField::~TensorField () {}
+ElementField::~ElementField () {}
 
-const drb_mesh *TensorField::device_field ()
+const drb_mesh *ElementField::device_field ()
 {
   DeviceGeometry &g = *m_dev;
   if (!g.mesh.ctrl_idx)
   {
     g.mesh.dim = m_dim;
+    g.mesh.shape = shape_of (m_etype);
     g.mesh.order = m_poly_order;
     g.mesh.ncomp = 1;
     g.mesh.n_elem = m_dof_data.get_num_elem ();
     g.mesh.n_ctrl = (int)m_dof_data.m_values.size ();
     g.mesh.ctrl_idx = m_dof_data.m_ctrl_idx.get_device_ptr_const ();
     g.mesh.values = (const float *)m_dof_data.m_values.get_device_ptr_const ();
-    const int stride = drb_packed_stride (m_dim, m_poly_order, 1);
+    const int stride = drb_packed_stride_shape (g.mesh.shape, m_dim, m_poly_order, 1);
     g.packed.alloc ((size_t)std::max (g.mesh.n_elem, 1) * stride);
     drb_check (drb_pack_elements (&g.mesh, g.packed.p, nullptr), "drb_pack_elements");
     g.mesh.packed = g.packed.p;
@@ -207,14 +215,14 @@ const drb_mesh *TensorField::device_field ()
   return &g.mesh;
 }
 
-std::vector<Range> TensorField::range () const
+std::vector<Range> ElementField::range () const
 {
   if (m_range.empty ())
   {
     float r[2];
     DevBuf<float> d;
     d.alloc (2);
-    drb_check (drb_field_range (const_cast<TensorField *> (this)->device_field (), d.p, nullptr),
+    drb_check (drb_field_range (const_cast<ElementField *> (this)->device_field (), d.p, nullptr),
                "drb_field_range");
     cuda_check (cudaMemcpy (r, d.p, sizeof (r), cudaMemcpyDeviceToHost), "copy");
     Range rr;
@@ -228,9 +236,9 @@ std::vector<Range> TensorField::range () const
   return m_range;
 }
 
-void TensorField::eval (const Array<Location> locs, Array<Float> &values)
+void ElementField::eval (const Array<Location> locs, Array<Float> &values)
 {
-  if (m_dim != 3) DRAY_ERROR ("field eval at locations needs a hex field");
+  if (m_dim != 3) DRAY_ERROR ("field eval at locations needs a hex or tet field");
   const int n = (int)locs.size ();
   values.resize (n);
   if (n == 0) return;
@@ -420,15 +428,15 @@ Volume::Volume (Collection &c) : m_collection (c)
   m_color_map.color_table (t);
 }
 
-static TensorMesh *as_tensor_mesh (Mesh *m)
+static ElementMesh *as_tensor_mesh (Mesh *m)
 {
-  TensorMesh *t = dynamic_cast<TensorMesh *> (m);
+  ElementMesh *t = dynamic_cast<ElementMesh *> (m);
   if (!t) DRAY_ERROR ("mesh type is not a tensor mesh of this path");
   return t;
 }
-static TensorField *as_tensor_field (Field *f)
+static ElementField *as_tensor_field (Field *f)
 {
-  TensorField *t = dynamic_cast<TensorField *> (f);
+  ElementField *t = dynamic_cast<ElementField *> (f);
   if (!t) DRAY_ERROR ("field type is not a scalar tensor field of this path");
   return t;
 }
@@ -437,8 +445,8 @@ Array<VolumePartial> Volume::integrate (Array<Ray> &rays, Array<PointLight> &lig
 {
   if (m_field == "") DRAY_ERROR ("Field never set");
   DataSet ds = m_collection.domain (0);
-  TensorMesh *mesh = as_tensor_mesh (ds.mesh ());
-  TensorField *field = as_tensor_field (ds.field (m_field));
+  ElementMesh *mesh = as_tensor_mesh (ds.mesh ());
+  ElementField *field = as_tensor_field (ds.field (m_field));
   Range r = m_color_map.range_set () ? m_color_map.scalar_range () : m_collection.range (m_field);
   const AABB<3> bounds = m_collection.bounds ();
   const drb_bvh *bvh = mesh->device_bvh ();
@@ -501,7 +509,7 @@ Framebuffer Volume::composite (Array<VolumePartial> partials, int32 w, int32 h)
 Array<RayHit> Surface::nearest_hit (Array<Ray> &rays)
 {
   DataSet ds = m_collection.domain (0);
-  TensorMesh *faces = as_tensor_mesh (ds.mesh ());
+  ElementMesh *faces = as_tensor_mesh (ds.mesh ());
   if (faces->dims () != 2) DRAY_ERROR ("Surface needs a quad (boundary) mesh");
   Array<RayHit> hits;
   hits.resize (rays.size ());
@@ -517,8 +525,8 @@ void Traceable::shade_impl (const Array<Ray> *rays, const Array<RayHit> &hits,
                             const Array<PointLight> *lights, Framebuffer *fb, Array<Fragment> *frags)
 {
   DataSet ds = m_collection.domain (0);
-  TensorMesh *faces = as_tensor_mesh (ds.mesh ());
-  TensorField *field = as_tensor_field (ds.field (m_field_name));
+  ElementMesh *faces = as_tensor_mesh (ds.mesh ());
+  ElementField *field = as_tensor_field (ds.field (m_field_name));
   Range r = m_color_map.range_set () ? m_color_map.scalar_range () : m_collection.range (m_field_name);
   std::vector<float32> tf = m_color_map.color_table ().sample (m_color_map.samples ());
   Array<Vec4f> tfa ((const Vec4f *)tf.data (), m_color_map.samples ());
@@ -573,7 +581,7 @@ Collection MeshBoundary::execute (Collection &collection)
   for (int32 i = 0; i < collection.local_size (); ++i)
   {
     DataSet ds = collection.domain (i);
-    TensorMesh *hex = dynamic_cast<TensorMesh *> (ds.mesh ());
+    ElementMesh *hex = dynamic_cast<ElementMesh *> (ds.mesh ());
     if (!hex || hex->dims () != 3)
     {
       res.add_domain (ds);
@@ -605,7 +613,7 @@ Collection MeshBoundary::execute (Collection &collection)
     out.add_mesh (qm);
     for (int32 k = 0; k < ds.number_of_fields (); ++k)
     {
-      TensorField *f = dynamic_cast<TensorField *> (ds.field (k));
+      ElementField *f = dynamic_cast<ElementField *> (ds.field (k));
       if (!f || f->order () != p) continue;
       GridFunction<1> vf = f->get_dof_data ();
       GridFunction<1> ff;

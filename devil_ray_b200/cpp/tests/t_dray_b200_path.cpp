@@ -106,7 +106,7 @@ int main (int argc, char **argv)
     Array<Vec<Float, 3>> pts;
     pts.resize (n);
     rd (fp, (float *)pts.get_host_ptr (), (size_t)3 * n);
-    static_cast<TensorMesh *> (mesh.get ())->m_locate.guess_mode = 0;
+    static_cast<ElementMesh *> (mesh.get ())->m_locate.guess_mode = 0;
     Array<Location> locs = mesh->locate (pts);
     EXPECT ((int32)locs.size () == n);
     {

@@ -83,7 +83,7 @@ using namespace drb;
 extern "C" int drb_mesh_face_neighbors (const drb_mesh *mesh, int *neighbors, void *stream)
 {
   if (!mesh || mesh->dim != 3 || mesh->order < 1 || mesh->order > 3 || mesh->n_elem < 0 ||
-      (mesh->n_elem > 0 && (!mesh->ctrl_idx || !neighbors)))
+      mesh->shape != DRB_SHAPE_TENSOR || (mesh->n_elem > 0 && (!mesh->ctrl_idx || !neighbors)))
   {
     set_last_error ("mesh_face_neighbors: needs a hex mesh of order 1..3 and an output array");
     return DRB_ERR_INVALID_ARG;

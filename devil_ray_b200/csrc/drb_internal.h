@@ -88,4 +88,7 @@ int locate_batched_ws (const drb_mesh *mesh, const drb_bvh *bvh, const float *pt
 
 int sm_count ();
 
+// Dofs per element of a mesh of either shape (drb_elem_dofs).
+int mesh_nd (const drb_mesh *m);
+
 } // namespace drb

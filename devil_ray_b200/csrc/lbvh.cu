@@ -19,6 +19,7 @@
 #include "bernstein.cuh"
 #include "drb_common.cuh"
 #include "drb_internal.h"
+#include "simplex.cuh"
 
 #include <cstdio>
 #include <cstring>
@@ -154,6 +155,41 @@ DRB_D void split_half (float *cps, int axis, bool left, int item)
   for (int ii = 0; ii <= P; ++ii) cps[3 * (base + ii * stride) + k] = d[ii];
 }
 
+// Scene bounds (reduce, linear_bvh_builder.cpp:19-58) of the boxes a block
+// wrote: warp, then block, then ordered-integer atomics into bounds_ord.
+DRB_D void reduce_scene_bounds (float (&bmn)[3], float (&bmx)[3], float (*s_bounds)[6], int warp,
+                                int lane, unsigned *bounds_ord)
+{
+#pragma unroll
+  for (int k = 0; k < 3; ++k)
+  {
+    bmn[k] = warp_min (bmn[k]);
+    bmx[k] = warp_max (bmx[k]);
+  }
+  if (lane == 0)
+  {
+#pragma unroll
+    for (int k = 0; k < 3; ++k)
+    {
+      s_bounds[warp][2 * k] = bmn[k];
+      s_bounds[warp][2 * k + 1] = bmx[k];
+    }
+  }
+  __syncthreads ();
+  if (threadIdx.x < 6)
+  {
+    const int q = threadIdx.x;
+    float v = s_bounds[0][q];
+    for (int w = 1; w < kSubboxWarps; ++w)
+      v = (q & 1) ? fmaxf (v, s_bounds[w][q]) : fminf (v, s_bounds[w][q]);
+    if (!isinf (v))
+    {
+      if (q & 1) atomicMax (bounds_ord + q, float_to_ordered (v));
+      else atomicMin (bounds_ord + q, float_to_ordered (v));
+    }
+  }
+}
+
 template <int DIM, int P>
 __global__ void __launch_bounds__ (kSubboxWarps * kWarp)
 subbox_kernel (const int *__restrict__ ctrl_idx, const float *__restrict__ xyz, int n_elem,
@@ -274,35 +310,212 @@ subbox_kernel (const int *__restrict__ ctrl_idx, const float *__restrict__ xyz, 
       }
     }
   }
-  // scene bounds (reduce, linear_bvh_builder.cpp:19-58): warp, block, atomics
+  reduce_scene_bounds (bmn, bmx, s_bounds, warp, lane, bounds_ord);
+}
+
+// ---- simplex (tet) sub-boxes -------------------------------------------
+//
+// Same forall as the tensor case (mesh_utils.cpp:557-670, 33 boxes per tet)
+// with the simplex split: the reference sub-simplex is four vertices (u, v,
+// w axis vertices, then the origin; ref_space.hpp:36-46); the split halves
+// its longest edge (first pair v1 < v2 on ties, mesh_utils.cpp:455-480) and
+// moves the `displaced` vertex to the midpoint (split_subref<Simplex>,
+// ref_space.hpp:133-146); the control points of both halves come from
+// de Casteljau along that edge (split_inplace<3,Simplex>,
+// elem_ops.hpp:1270-1311).  The reference linearises the dof multi-index
+// there with cartesian_to_tet_idx (elem_ops.hpp:32-47), whose in-layer term
+// uses the full edge length instead of the layer's: for orders >= 2 it
+// addresses the wrong dofs (e.g. order 2 maps (0,1,1) and (0,0,2) both to
+// 9) and order 3 reaches index 20 of a 20-dof element.  The layout every
+// evaluator uses (the general-order eval_d walk, elem_ops.hpp:945-1030) is
+// the layered one of tet_index, which this kernel uses, so its sub-boxes
+// bound the split geometry at every order; at order 1 the two indexings
+// coincide and the boxes are bit-identical to the reference's.
+
+constexpr int kTetRefFloats = 12; // SubRef<3,Simplex>: four vertices
+
+// One line of a tet split: the dofs with fixed exponents g, h of the two
+// vertices off the split edge, ordered by the exponent a of the displaced
+// vertex v0 (the tradeoff vertex v1 gets m - a).  De Casteljau at 0.5 in the
+// reference's update order: for nu = m..1, a = m down to m - nu + 1,
+//   C[a] = C[a] * f + C[a - 1] * (1 - f).
+template <int P>
+DRB_D void tet_split_line (float *cps, int v0, int v1, int g, int h, int comp)
+{
+  const int avail = 0xf & ~(1 << v0) & ~(1 << v1);
+  const int v2 = (avail & 1) ? 0 : (avail & 2) ? 1 : (avail & 4) ? 2 : 3;
+  const int v3 = 6 - v0 - v1 - v2;
+  const int m = P - g - h;
+  int ids[P + 1];
+  float d[P + 1];
 #pragma unroll
-  for (int k = 0; k < 3; ++k)
+  for (int a = 0; a <= P; ++a)
   {
-    bmn[k] = warp_min (bmn[k]);
-    bmx[k] = warp_max (bmx[k]);
+    if (a > m) break;
+    int b[4];
+    b[v0] = a;
+    b[v1] = m - a;
+    b[v2] = g;
+    b[v3] = h;
+    ids[a] = tet_index (b[0], b[1], b[2], P);
+    d[a] = cps[3 * ids[a] + comp];
   }
-  if (lane == 0)
-  {
 #pragma unroll
-    for (int k = 0; k < 3; ++k)
+  for (int nu = P; nu >= 1; --nu)
+  {
+    if (nu > m) continue;
+#pragma unroll
+    for (int a = P; a >= 1; --a)
     {
-      s_bounds[warp][2 * k] = bmn[k];
-      s_bounds[warp][2 * k + 1] = bmx[k];
+      if (a > m || a < m - nu + 1) continue;
+      d[a] = __fadd_rn (__fmul_rn (d[a], 0.5f), __fmul_rn (d[a - 1], 0.5f));
     }
   }
-  __syncthreads ();
-  if (threadIdx.x < 6)
+#pragma unroll
+  for (int a = 0; a <= P; ++a)
   {
-    const int q = threadIdx.x;
-    float v = s_bounds[0][q];
-    for (int w = 1; w < kSubboxWarps; ++w)
-      v = (q & 1) ? fmaxf (v, s_bounds[w][q]) : fminf (v, s_bounds[w][q]);
-    if (!isinf (v))
+    if (a > m) break;
+    cps[3 * ids[a] + comp] = d[a];
+  }
+}
+
+template <int P>
+__global__ void __launch_bounds__ (kSubboxWarps * kWarp)
+tet_subbox_kernel (const int *__restrict__ ctrl_idx, const float *__restrict__ xyz, int n_elem,
+                   float *__restrict__ aabbs6, int *__restrict__ prim_ids,
+                   float *__restrict__ ref_out, unsigned *__restrict__ bounds_ord)
+{
+  constexpr int ND = tet_dofs<P> ();
+  constexpr int NB = SplitCount<3>::boxes;
+  constexpr int NL = P * (P + 1) / 2; // lines per split: g + h < P
+  constexpr int CPW = NB * ND * 3;
+  extern __shared__ float smem[];
+  __shared__ float s_bounds[kSubboxWarps][6];
+
+  const int warp = threadIdx.x >> 5;
+  const int lane = threadIdx.x & 31;
+  float *cps = smem + warp * CPW;
+  float *boxes = smem + kSubboxWarps * CPW + warp * NB * 6;
+  float *refs = smem + kSubboxWarps * (CPW + NB * 6) + warp * NB * kTetRefFloats;
+
+  const int el = blockIdx.x * kSubboxWarps + warp;
+  float bmn[3] = { INFINITY, INFINITY, INFINITY };
+  float bmx[3] = { -INFINITY, -INFINITY, -INFINITY };
+
+  if (el < n_elem)
+  {
+    for (int t = lane; t < ND * 3; t += kWarp)
     {
-      if (q & 1) atomicMax (bounds_ord + q, float_to_ordered (v));
-      else atomicMin (bounds_ord + q, float_to_ordered (v));
+      const int i = t / 3;
+      const int k = t - 3 * i;
+      cps[t] = __ldg (xyz + 3 * (size_t)__ldg (ctrl_idx + (size_t)el * ND + i) + k);
+    }
+    // ref_universe<Simplex>: unit axis vertices, then the origin
+    if (lane < kTetRefFloats) refs[lane] = (lane < 9 && lane % 4 == 0) ? 1.f : 0.f;
+    __syncwarp ();
+    warp_hull<ND> (cps, boxes, lane);
+    __syncwarp ();
+
+    for (int count = 1; count < NB; ++count)
+    {
+      int max_id = 0;
+      float max_measure = box_measure (boxes);
+      for (int b = 1; b < count; ++b)
+      {
+        const float mm = box_measure (boxes + 6 * b);
+        if (mm > max_measure)
+        {
+          max_id = b;
+          max_measure = mm;
+        }
+      }
+      // pick_binary_split<Simplex>: longest reference edge (squared length
+      // summed in component order), first pair on ties
+      const float *rm = refs + max_id * kTetRefFloats;
+      int dv = 0, tv = 1;
+      float max_l2 = 0.f;
+      for (int a = 0; a < 3; ++a)
+        for (int b = a + 1; b < 4; ++b)
+        {
+          const float e0 = __fsub_rn (rm[3 * a], rm[3 * b]);
+          const float e1 = __fsub_rn (rm[3 * a + 1], rm[3 * b + 1]);
+          const float e2 = __fsub_rn (rm[3 * a + 2], rm[3 * b + 2]);
+          const float l2 = __fadd_rn (__fadd_rn (__fmul_rn (e0, e0), __fmul_rn (e1, e1)), __fmul_rn (e2, e2));
+          if (l2 > max_l2)
+          {
+            dv = a;
+            tv = b;
+            max_l2 = l2;
+          }
+        }
+      __syncwarp ();
+      if (lane == 0)
+      {
+        float *rmw = refs + max_id * kTetRefFloats;
+        float *rd = refs + count * kTetRefFloats;
+        float sp[3];
+#pragma unroll
+        for (int k = 0; k < 3; ++k)
+          sp[k] = __fadd_rn (__fmul_rn (rmw[3 * tv + k], 0.5f), __fmul_rn (rmw[3 * dv + k], 0.5f));
+#pragma unroll
+        for (int q = 0; q < kTetRefFloats; ++q) rd[q] = rmw[q];
+#pragma unroll
+        for (int k = 0; k < 3; ++k)
+        {
+          rmw[3 * dv + k] = sp[k];
+          rd[3 * tv + k] = sp[k];
+        }
+      }
+      float *mother = cps + max_id * ND * 3;
+      float *dghter = cps + count * ND * 3;
+      for (int t = lane; t < ND * 3; t += kWarp) dghter[t] = mother[t];
+      __syncwarp ();
+      // mother: split (displaced dv, tradeoff tv); daughter: the complement
+      // (displaced tv, tradeoff dv); one (line, component) per lane
+      for (int item = lane; item < 2 * NL * 3; item += kWarp)
+      {
+        const bool is_mother = item < NL * 3;
+        const int it = is_mother ? item : item - NL * 3;
+        const int line = it / 3;
+        const int comp = it - 3 * line;
+        int h = 0, g = line;
+        while (g >= P - h)
+        {
+          g -= P - h;
+          ++h;
+        }
+        if (is_mother) tet_split_line<P> (mother, dv, tv, g, h, comp);
+        else tet_split_line<P> (dghter, tv, dv, g, h, comp);
+      }
+      __syncwarp ();
+      warp_hull<ND> (mother, boxes + 6 * max_id, lane);
+      warp_hull<ND> (dghter, boxes + 6 * count, lane);
+      __syncwarp ();
+    }
+
+    const float s = (float)1.000001;
+    for (int b = lane; b < NB; b += kWarp)
+    {
+      float bx[6];
+#pragma unroll
+      for (int q = 0; q < 6; ++q) bx[q] = boxes[6 * b + q];
+#pragma unroll
+      for (int k = 0; k < 3; ++k) scale_range (bx[2 * k], bx[2 * k + 1], s);
+      const size_t o = (size_t)el * NB + b;
+#pragma unroll
+      for (int q = 0; q < 6; ++q) aabbs6[6 * o + q] = bx[q];
+      prim_ids[o] = el;
+#pragma unroll
+      for (int q = 0; q < kTetRefFloats; ++q) ref_out[kTetRefFloats * o + q] = refs[kTetRefFloats * b + q];
+#pragma unroll
+      for (int k = 0; k < 3; ++k)
+      {
+        bmn[k] = fminf (bmn[k], bx[2 * k]);
+        bmx[k] = fmaxf (bmx[k], bx[2 * k + 1]);
+      }
     }
   }
+  reduce_scene_bounds (bmn, bmx, s_bounds, warp, lane, bounds_ord);
 }
 
 __global__ void bounds_init_kernel (unsigned *bounds_ord)
@@ -542,6 +755,26 @@ template <int DIM, int P> size_t subbox_smem ()
   return sizeof (float) * kSubboxWarps * (NB * ND * 3 + NB * 6 + NB * 2 * DIM);
 }
 
+template <int P> size_t tet_subbox_smem ()
+{
+  constexpr int NB = SplitCount<3>::boxes;
+  return sizeof (float) * kSubboxWarps * (NB * tet_dofs<P> () * 3 + NB * 6 + NB * kTetRefFloats);
+}
+
+template <int P>
+int launch_tet_subbox (const drb_mesh *m, float *aabbs6, int *prim_ids, float *ref_boxes,
+                       unsigned *bounds_ord, cudaStream_t s)
+{
+  const size_t smem = tet_subbox_smem<P> ();
+  cudaFuncSetAttribute (tet_subbox_kernel<P>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                        (int)smem);
+  const int blocks = div_up (m->n_elem, kSubboxWarps);
+  if (blocks > 0)
+    tet_subbox_kernel<P><<<blocks, kSubboxWarps * kWarp, smem, s>>> (
+    m->ctrl_idx, m->values, m->n_elem, aabbs6, prim_ids, ref_boxes, bounds_ord);
+  return check_launch ("tet_subbox_kernel");
+}
+
 template <int DIM, int P>
 int launch_subbox (const drb_mesh *m, float *aabbs6, int *prim_ids, float *ref_boxes,
                    unsigned *bounds_ord, cudaStream_t s)
@@ -559,7 +792,18 @@ int launch_subbox (const drb_mesh *m, float *aabbs6, int *prim_ids, float *ref_b
 int dispatch_subbox (const drb_mesh *m, float *aabbs6, int *prim_ids, float *ref_boxes,
                      unsigned *bounds_ord, cudaStream_t s)
 {
-  if (m->dim == 3)
+  if (m->shape == DRB_SHAPE_SIMPLEX && m->dim == 3)
+  {
+    if (m->order == 1) return launch_tet_subbox<1> (m, aabbs6, prim_ids, ref_boxes, bounds_ord, s);
+    if (m->order == 2) return launch_tet_subbox<2> (m, aabbs6, prim_ids, ref_boxes, bounds_ord, s);
+    if (m->order == 3) return launch_tet_subbox<3> (m, aabbs6, prim_ids, ref_boxes, bounds_ord, s);
+  }
+  else if (m->shape != DRB_SHAPE_TENSOR)
+  {
+    set_last_error ("subbox: simplex meshes must be tets (dim 3)");
+    return DRB_ERR_UNSUPPORTED;
+  }
+  else if (m->dim == 3)
   {
     if (m->order == 1) return launch_subbox<3, 1> (m, aabbs6, prim_ids, ref_boxes, bounds_ord, s);
     if (m->order == 2) return launch_subbox<3, 2> (m, aabbs6, prim_ids, ref_boxes, bounds_ord, s);
@@ -579,6 +823,11 @@ int validate_mesh (const drb_mesh *m, int want_ncomp)
 {
   if (!m) { set_last_error ("mesh is NULL"); return DRB_ERR_INVALID_ARG; }
   if (m->dim != 2 && m->dim != 3) { set_last_error ("mesh dim must be 2 or 3"); return DRB_ERR_INVALID_ARG; }
+  if (m->shape != DRB_SHAPE_TENSOR && !(m->shape == DRB_SHAPE_SIMPLEX && m->dim == 3))
+  {
+    set_last_error ("mesh shape must be tensor, or simplex with dim 3 (tets)");
+    return DRB_ERR_UNSUPPORTED;
+  }
   if (m->order < 1 || m->order > 3) { set_last_error ("mesh order must be 1..3"); return DRB_ERR_UNSUPPORTED; }
   if (m->ncomp != want_ncomp) { set_last_error ("mesh ncomp mismatch"); return DRB_ERR_INVALID_ARG; }
   if (m->n_elem < 0 || m->n_ctrl < 0) { set_last_error ("negative mesh size"); return DRB_ERR_INVALID_ARG; }
@@ -597,6 +846,11 @@ int mesh_nd (int dim, int order)
   return nd;
 }
 
+int mesh_nd (const drb_mesh *m)
+{
+  return m->shape == DRB_SHAPE_SIMPLEX ? tet_dofs (m->order) : mesh_nd (m->dim, m->order);
+}
+
 } // namespace drb
 
 using namespace drb;
@@ -607,6 +861,29 @@ extern "C" int drb_packed_stride (int dim, int order, int ncomp)
   return packed_stride (mesh_nd (dim, order), ncomp);
 }
 
+extern "C" int drb_elem_dofs (int shape, int dim, int order)
+{
+  if (order < 1 || order > 3) return -1;
+  if (shape == DRB_SHAPE_TENSOR && (dim == 2 || dim == 3)) return mesh_nd (dim, order);
+  if (shape == DRB_SHAPE_SIMPLEX && dim == 3) return tet_dofs (order);
+  return -1;
+}
+
+extern "C" int drb_packed_stride_shape (int shape, int dim, int order, int ncomp)
+{
+  const int nd = drb_elem_dofs (shape, dim, order);
+  if (nd < 0 || ncomp < 1) return -1;
+  return packed_stride (nd, ncomp);
+}
+
+extern "C" int drb_ref_box_floats (int shape, int dim)
+{
+  if (dim != 2 && dim != 3) return -1;
+  if (shape == DRB_SHAPE_TENSOR) return 2 * dim;
+  if (shape == DRB_SHAPE_SIMPLEX) return dim * (dim + 1);
+  return -1;
+}
+
 extern "C" int drb_pack_elements (const drb_mesh *mesh, float *packed, void *stream)
 {
   if (!mesh || (mesh->ncomp != 1 && mesh->ncomp != 3)) { set_last_error ("pack: bad mesh"); return DRB_ERR_INVALID_ARG; }
@@ -614,7 +891,7 @@ extern "C" int drb_pack_elements (const drb_mesh *mesh, float *packed, void *str
   if (st) return st;
   if (mesh->n_elem == 0) return DRB_OK;
   if (!packed) { set_last_error ("pack: output NULL"); return DRB_ERR_INVALID_ARG; }
-  const int nd = mesh_nd (mesh->dim, mesh->order);
+  const int nd = mesh_nd (mesh);
   const int stride = packed_stride (nd, mesh->ncomp);
   const long long total = (long long)mesh->n_elem * stride;
   cudaStream_t s = (cudaStream_t)stream;
@@ -704,10 +981,14 @@ extern "C" int drb_lbvh_build (const drb_mesh *mesh, drb_bvh *bvh, unsigned *sor
     const int leaf[2] = { 0, 0 };
     const int ids[2] = { 0, 1 };
     const float ref3[12] = { 0, 0, 0, 1, 1, 1, 0, 0, 0, 1, 1, 1 };
+    // ref_universe<Simplex>: axis vertices, then the origin
+    const float tet_ref[24] = { 1, 0, 0, 0, 1, 0, 0, 0, 1, 0, 0, 0, 1, 0, 0, 0, 1, 0, 0, 0, 1, 0, 0, 0 };
+    const bool simplex = mesh->shape == DRB_SHAPE_SIMPLEX;
     cudaMemcpyAsync (bvh->inner_nodes, node, sizeof (node), cudaMemcpyHostToDevice, s);
     cudaMemcpyAsync (bvh->leaf_nodes, leaf, sizeof (leaf), cudaMemcpyHostToDevice, s);
     cudaMemcpyAsync (bvh->aabb_ids, ids, sizeof (ids), cudaMemcpyHostToDevice, s);
-    cudaMemcpyAsync (bvh->ref_boxes, ref3, sizeof (float) * 4 * mesh->dim, cudaMemcpyHostToDevice, s);
+    cudaMemcpyAsync (bvh->ref_boxes, simplex ? tet_ref : ref3,
+                     sizeof (float) * (simplex ? 24 : 4 * mesh->dim), cudaMemcpyHostToDevice, s);
     if (sorted_codes) cudaMemsetAsync (sorted_codes, 0, sizeof (unsigned) * 2, s);
     const float empty[6] = { INFINITY, -INFINITY, INFINITY, -INFINITY, INFINITY, -INFINITY };
     for (int q = 0; q < 6; ++q) bvh->bounds[q] = empty[q];

@@ -15,7 +15,7 @@
 namespace drb
 {
 
-template <int P>
+template <int P, int S>
 __global__ void __launch_bounds__ (128)
 locate_kernel (LocateParams lp, const float *__restrict__ pts, int n, int *__restrict__ cell,
                float *__restrict__ ref, int *__restrict__ iters_out, int *__restrict__ cands_out,
@@ -26,7 +26,7 @@ locate_kernel (LocateParams lp, const float *__restrict__ pts, int n, int *__res
   const float pt[3] = { pts[3 * (size_t)i], pts[3 * (size_t)i + 1], pts[3 * (size_t)i + 2] };
   float r[3] = { -1.f, -1.f, -1.f };
   int iters = 0, cands = 0, nodes = 0;
-  const int c = locate_point<P> (lp, i, pt, r, iters, cands, nodes);
+  const int c = locate_point<P, false, S> (lp, i, pt, r, iters, cands, nodes);
   cell[i] = c;
   if (c < 0) r[0] = r[1] = r[2] = -1.f;
   ref[3 * (size_t)i] = r[0];
@@ -50,9 +50,10 @@ extern "C" int drb_locate (const drb_mesh *mesh, const drb_bvh *bvh, const float
     set_last_error ("locate: bad arguments");
     return DRB_ERR_INVALID_ARG;
   }
-  if (mesh->dim != 3 || mesh->ncomp != 3 || mesh->order < 1 || mesh->order > 3)
+  if (mesh->dim != 3 || mesh->ncomp != 3 || mesh->order < 1 || mesh->order > 3 ||
+      (mesh->shape != DRB_SHAPE_TENSOR && mesh->shape != DRB_SHAPE_SIMPLEX))
   {
-    set_last_error ("locate: needs a hex geometry mesh of order 1..3");
+    set_last_error ("locate: needs a hex or tet geometry mesh of order 1..3");
     return DRB_ERR_UNSUPPORTED;
   }
   if (opts->guess_mode == DRB_GUESS_GIVEN && !opts->guess)
@@ -75,18 +76,23 @@ extern "C" int drb_locate (const drb_mesh *mesh, const drb_bvh *bvh, const float
   lp.packed = mesh->packed;
   lp.ctrl_idx = mesh->ctrl_idx;
   lp.xyz = mesh->values;
-  lp.stride = packed_stride ((mesh->order + 1) * (mesh->order + 1) * (mesh->order + 1), 3);
+  lp.stride = packed_stride (mesh_nd (mesh), 3);
   lp.tol = opts->tol;
   lp.max_steps = opts->max_steps;
   lp.guess_mode = opts->guess_mode;
   lp.guess = opts->guess;
   cudaStream_t s = (cudaStream_t)stream;
   const int blocks = div_up (n, 128);
-  if (mesh->order == 1)
-    locate_kernel<1><<<blocks, 128, 0, s>>> (lp, pts, n, cell, ref, stats.iters, stats.candidates, stats.nodes);
-  else if (mesh->order == 2)
-    locate_kernel<2><<<blocks, 128, 0, s>>> (lp, pts, n, cell, ref, stats.iters, stats.candidates, stats.nodes);
-  else
-    locate_kernel<3><<<blocks, 128, 0, s>>> (lp, pts, n, cell, ref, stats.iters, stats.candidates, stats.nodes);
+#define DRB_LK(P, S) locate_kernel<P, S><<<blocks, 128, 0, s>>> (lp, pts, n, cell, ref, stats.iters, stats.candidates, stats.nodes)
+  if (mesh->shape == DRB_SHAPE_SIMPLEX)
+  {
+    if (mesh->order == 1) DRB_LK (1, kSimplex);
+    else if (mesh->order == 2) DRB_LK (2, kSimplex);
+    else DRB_LK (3, kSimplex);
+  }
+  else if (mesh->order == 1) DRB_LK (1, kTensor);
+  else if (mesh->order == 2) DRB_LK (2, kTensor);
+  else DRB_LK (3, kTensor);
+#undef DRB_LK
   return check_launch ("locate_kernel");
 }

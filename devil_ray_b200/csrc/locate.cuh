@@ -5,6 +5,7 @@
 
 #include "drb_common.cuh"
 #include "newton.cuh"
+#include "simplex.cuh"
 #include "../../include/drb.h"
 
 namespace drb
@@ -136,12 +137,49 @@ struct LocateParams
   const float *guess;
 };
 
+// Element shapes of the locate templates (drb_shape).
+constexpr int kTensor = DRB_SHAPE_TENSOR;
+constexpr int kSimplex = DRB_SHAPE_SIMPLEX;
+
+// Dofs of an order-P element of shape S, and its reference centre
+// coordinate (hex (0.5,0.5,0.5), tet centroid (0.25,0.25,0.25)).
+template <int S, int P> constexpr int shape_dofs ()
+{
+  return S == kSimplex ? tet_dofs<P> () : (P + 1) * (P + 1) * (P + 1);
+}
+template <int S> constexpr float shape_centre () { return S == kSimplex ? 0.25f : 0.5f; }
+
+// Tet Newton solve (simplex counterpart of the tensor path below).
+template <int P, bool REG>
+DRB_D bool solve_in_tet (const LocateParams &lp, int el, const float (&pt)[3], float (&x)[3],
+                         int &steps, LU3 &lu)
+{
+  constexpr int ND = tet_dofs<P> ();
+  if (lp.packed)
+  {
+    const float *row = lp.packed + (size_t)el * lp.stride;
+    float t[3];
+    local_target<ND> (row, pt, t);
+    if (REG && P <= 2)
+    {
+      RegCP<3 * ND> r;
+      load_reg_tet<P> (r, row);
+      return tet_newton<P> (r, t, x, lp.tol, lp.max_steps, steps, lu);
+    }
+    PackedCP cp{ row };
+    return tet_newton<P> (cp, t, x, lp.tol, lp.max_steps, steps, lu);
+  }
+  IndirectCP cp{ lp.ctrl_idx + (size_t)el * ND, lp.xyz, 3 };
+  return tet_newton<P> (cp, pt, x, lp.tol, lp.max_steps, steps, lu);
+}
+
 // Newton solve of one point in one element, choosing register-resident or
 // L1-read control points by order.
-template <int P, bool REG = (P <= 2)>
+template <int P, bool REG = (P <= 2), int S = kTensor>
 DRB_D bool solve_in_element (const LocateParams &lp, int el, const float (&pt)[3], float (&x)[3],
                              int &steps, LU3 &lu)
 {
+  if (S == kSimplex) return solve_in_tet<P, REG> (lp, el, pt, x, steps, lu);
   constexpr int ND = (P + 1) * (P + 1) * (P + 1);
   if (lp.packed)
   {
@@ -196,6 +234,7 @@ DRB_D bool solve_in_smem_row (const LocateParams &lp, const float *row, const fl
 }
 
 // Initial guess of a candidate leaf's Newton solve (drb_guess_mode).
+template <int S = kTensor>
 DRB_D void candidate_guess (const LocateParams &lp, int leaf, long long qi, bool first,
                             float (&x)[3], bool &given)
 {
@@ -203,6 +242,20 @@ DRB_D void candidate_guess (const LocateParams &lp, int leaf, long long qi, bool
   if (lp.guess_mode == DRB_GUESS_ZERO)
   {
     x[0] = x[1] = x[2] = 0.f;
+  }
+  else if (lp.guess_mode == DRB_GUESS_SUBREF_CENTER && S == kSimplex)
+  {
+    // subref_center<Simplex> (data_model/subref.hpp:39-48): the origin
+    // vertex plus the three axis vertices, times 1/4
+    const float *rb = lp.ref_boxes + 12 * (size_t)__ldg (lp.aabb_ids + leaf);
+#pragma unroll
+    for (int d = 0; d < 3; ++d)
+    {
+      float sum = __fadd_rn (rb[9 + d], rb[d]);
+      sum = __fadd_rn (sum, rb[3 + d]);
+      sum = __fadd_rn (sum, rb[6 + d]);
+      x[d] = __fmul_rn (sum, 0.25f);
+    }
   }
   else if (lp.guess_mode == DRB_GUESS_SUBREF_CENTER)
   {
@@ -218,36 +271,36 @@ DRB_D void candidate_guess (const LocateParams &lp, int leaf, long long qi, bool
   }
   else
   {
-    x[0] = x[1] = x[2] = 0.5f;
+    x[0] = x[1] = x[2] = shape_centre<S> ();
   }
 }
 
 // Newton in one candidate element with the guess-mode fallback: a given
 // guess that does not converge is retried from the element centre.
-template <int P, bool REG = (P <= 2)>
+template <int P, bool REG = (P <= 2), int S = kTensor>
 DRB_D bool solve_candidate (const LocateParams &lp, int leaf, int el, long long qi, bool first,
                             const float (&pt)[3], float (&x)[3], int &iters, LU3 &lu)
 {
   bool given;
-  candidate_guess (lp, leaf, qi, first, x, given);
+  candidate_guess<S> (lp, leaf, qi, first, x, given);
   int steps = 0;
-  bool found = solve_in_element<P, REG> (lp, el, pt, x, steps, lu);
+  bool found = solve_in_element<P, REG, S> (lp, el, pt, x, steps, lu);
   iters += steps;
   if (!found && given)
   {
-    x[0] = x[1] = x[2] = 0.5f;
-    found = solve_in_element<P, REG> (lp, el, pt, x, steps, lu);
+    x[0] = x[1] = x[2] = shape_centre<S> ();
+    found = solve_in_element<P, REG, S> (lp, el, pt, x, steps, lu);
     iters += steps;
   }
   return found;
 }
 
-template <int P, bool REG = (P <= 2)>
+template <int P, bool REG = (P <= 2), int S = kTensor>
 DRB_D bool solve_candidate (const LocateParams &lp, int leaf, int el, long long qi, bool first,
                             const float (&pt)[3], float (&x)[3], int &iters)
 {
   LU3 lu;
-  return solve_candidate<P, REG> (lp, leaf, el, qi, first, pt, x, iters, lu);
+  return solve_candidate<P, REG, S> (lp, leaf, el, qi, first, pt, x, iters, lu);
 }
 
 // solve_candidate on a shared-memory row (same guess and fallback rule).
@@ -256,7 +309,7 @@ DRB_D bool solve_candidate_smem (const LocateParams &lp, int leaf, const float *
                                  bool first, const float (&pt)[3], float (&x)[3], int &iters)
 {
   bool given;
-  candidate_guess (lp, leaf, qi, first, x, given);
+  candidate_guess<kTensor> (lp, leaf, qi, first, x, given);
   int steps = 0;
   bool found = solve_in_smem_row<P> (lp, row, pt, x, steps);
   iters += steps;
@@ -271,7 +324,7 @@ DRB_D bool solve_candidate_smem (const LocateParams &lp, int leaf, const float *
 
 // Full point location of one query (DeviceMesh::locate, device_mesh.hpp:248-354):
 // traversal left child first, first converged+inside candidate wins.
-template <int P, bool WIDE = false>
+template <int P, bool WIDE = false, int S = kTensor>
 DRB_D int locate_point (const LocateParams &lp, int qi, const float (&pt)[3], float (&out_ref)[3],
                         int &iters, int &cands, int &nodes, LU3 &lu)
 {
@@ -289,7 +342,7 @@ DRB_D int locate_point (const LocateParams &lp, int qi, const float (&pt)[3], fl
     const int el = __ldg (lp.leaf_nodes + leaf);
     ++cands;
     float x[3];
-    const bool found = solve_candidate<P> (lp, leaf, el, qi, first_candidate, pt, x, iters, lu);
+    const bool found = solve_candidate<P, (P <= 2), S> (lp, leaf, el, qi, first_candidate, pt, x, iters, lu);
     first_candidate = false;
     if (found)
     {
@@ -304,12 +357,12 @@ DRB_D int locate_point (const LocateParams &lp, int qi, const float (&pt)[3], fl
   return -1;
 }
 
-template <int P, bool WIDE = false>
+template <int P, bool WIDE = false, int S = kTensor>
 DRB_D int locate_point (const LocateParams &lp, int qi, const float (&pt)[3], float (&out_ref)[3],
                         int &iters, int &cands, int &nodes)
 {
   LU3 lu;
-  return locate_point<P, WIDE> (lp, qi, pt, out_ref, iters, cands, nodes, lu);
+  return locate_point<P, WIDE, S> (lp, qi, pt, out_ref, iters, cands, nodes, lu);
 }
 
 } // namespace drb

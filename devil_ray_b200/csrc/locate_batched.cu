@@ -128,7 +128,7 @@ template <int P> constexpr size_t smem_rows_bytes_per_warp ()
   return sizeof (float) * 32 * (size_t)smem_row_stride<P> ();
 }
 
-template <int P, int MODE, bool WIDE>
+template <int P, int MODE, bool WIDE, int S = kTensor>
 __global__ void locate_persistent_kernel (LocateParams lp, const float *__restrict__ pts,
                                           const int *__restrict__ order, int n, int chunk,
                                           int *__restrict__ queue_head, int *__restrict__ cell,
@@ -239,7 +239,7 @@ __global__ void locate_persistent_kernel (LocateParams lp, const float *__restri
         ++cands;
         const bool found = (MODE == kRowsShared)
                            ? solve_candidate_smem<P> (lp, leaf, my_row, qi, first, pt, x, iters)
-                           : solve_candidate<P, MODE == kRowsReg> (lp, leaf, el, qi, first, pt, x, iters);
+                           : solve_candidate<P, MODE == kRowsReg, S> (lp, leaf, el, qi, first, pt, x, iters);
         first = false;
         if (found)
         {
@@ -272,26 +272,33 @@ __global__ void locate_persistent_kernel (LocateParams lp, const float *__restri
   }
 }
 
-template <int P, bool W> const void *persistent_fn_pw (int mode)
+// Tets run the L1 and register row modes (shared rows are tensor-only).
+template <int P, bool W, int S> const void *persistent_fn_pw (int mode)
 {
-  if (mode == kRowsShared) return (const void *)locate_persistent_kernel<P, kRowsShared, W>;
-  if (mode == kRowsReg && P <= 2) return (const void *)locate_persistent_kernel<P, kRowsReg, W>;
-  return (const void *)locate_persistent_kernel<P, kRowsL1, W>;
+  if (S == kTensor && mode == kRowsShared) return (const void *)locate_persistent_kernel<P, kRowsShared, W>;
+  if (mode == kRowsReg && P <= 2) return (const void *)locate_persistent_kernel<P, kRowsReg, W, S>;
+  return (const void *)locate_persistent_kernel<P, kRowsL1, W, S>;
 }
 
-const void *persistent_fn (int order, int mode, bool wide)
+template <int S> const void *persistent_fn_s (int order, int mode, bool wide)
 {
-  if (order == 1) return wide ? persistent_fn_pw<1, true> (mode) : persistent_fn_pw<1, false> (mode);
-  if (order == 2) return wide ? persistent_fn_pw<2, true> (mode) : persistent_fn_pw<2, false> (mode);
-  return wide ? persistent_fn_pw<3, true> (mode) : persistent_fn_pw<3, false> (mode);
+  if (order == 1) return wide ? persistent_fn_pw<1, true, S> (mode) : persistent_fn_pw<1, false, S> (mode);
+  if (order == 2) return wide ? persistent_fn_pw<2, true, S> (mode) : persistent_fn_pw<2, false, S> (mode);
+  return wide ? persistent_fn_pw<3, true, S> (mode) : persistent_fn_pw<3, false, S> (mode);
+}
+
+const void *persistent_fn (const drb_mesh *mesh, int mode, bool wide)
+{
+  return mesh->shape == DRB_SHAPE_SIMPLEX ? persistent_fn_s<kSimplex> (mesh->order, mode, wide)
+                                          : persistent_fn_s<kTensor> (mesh->order, mode, wide);
 }
 
 // Row mode actually used: registers only for orders 1-2, shared rows only
-// with a packed element copy.
+// for hexes with a packed element copy.
 int effective_mode (const drb_mesh *mesh, int requested)
 {
   if (requested == kRowsReg && mesh->order <= 2) return kRowsReg;
-  if (requested == kRowsShared && mesh->packed) return kRowsShared;
+  if (requested == kRowsShared && mesh->packed && mesh->shape == DRB_SHAPE_TENSOR) return kRowsShared;
   return kRowsL1;
 }
 
@@ -303,37 +310,49 @@ size_t dynamic_smem (int order, int mode, int block)
   return per_warp * (size_t)(block / 32);
 }
 
-template <int P, bool W>
+template <int P, bool W, int S>
 void launch_pw (int mode, dim3 grid, int block, size_t smem, cudaStream_t s, const LocateParams &lp,
                 const float *pts, const int *ord, int n, int chunk, int *head, int *cell, float *ref,
                 drb_query_stats st)
 {
-#define DRB_LP(M) locate_persistent_kernel<P, M, W><<<grid, block, smem, s>>> (lp, pts, ord, n, chunk, head, cell, ref, st.iters, st.candidates, st.nodes)
-  if (mode == kRowsShared) DRB_LP (kRowsShared);
-  else if (mode == kRowsReg && P <= 2) DRB_LP (P <= 2 ? kRowsReg : kRowsL1);
-  else DRB_LP (kRowsL1);
+#define DRB_LP(M, SS) locate_persistent_kernel<P, M, W, SS><<<grid, block, smem, s>>> (lp, pts, ord, n, chunk, head, cell, ref, st.iters, st.candidates, st.nodes)
+  if (S == kTensor && mode == kRowsShared) DRB_LP (kRowsShared, kTensor);
+  else if (mode == kRowsReg && P <= 2) DRB_LP (P <= 2 ? kRowsReg : kRowsL1, S);
+  else DRB_LP (kRowsL1, S);
 #undef DRB_LP
 }
 
-int launch_persistent (int order, int mode, dim3 grid, int block, cudaStream_t s,
+template <int S>
+void launch_s (int order, bool wide, int mode, dim3 grid, int block, size_t smem, cudaStream_t s,
+               const LocateParams &lp, const float *pts, const int *ord, int n, int chunk, int *head,
+               int *cell, float *ref, drb_query_stats st)
+{
+  if (order == 1) { if (wide) launch_pw<1, true, S> (mode, grid, block, smem, s, lp, pts, ord, n, chunk, head, cell, ref, st); else launch_pw<1, false, S> (mode, grid, block, smem, s, lp, pts, ord, n, chunk, head, cell, ref, st); }
+  else if (order == 2) { if (wide) launch_pw<2, true, S> (mode, grid, block, smem, s, lp, pts, ord, n, chunk, head, cell, ref, st); else launch_pw<2, false, S> (mode, grid, block, smem, s, lp, pts, ord, n, chunk, head, cell, ref, st); }
+  else { if (wide) launch_pw<3, true, S> (mode, grid, block, smem, s, lp, pts, ord, n, chunk, head, cell, ref, st); else launch_pw<3, false, S> (mode, grid, block, smem, s, lp, pts, ord, n, chunk, head, cell, ref, st); }
+}
+
+int launch_persistent (const drb_mesh *mesh, int mode, dim3 grid, int block, cudaStream_t s,
                        const LocateParams &lp, const float *pts, const int *ord, int n, int chunk,
                        int *head, int *cell, float *ref, drb_query_stats st)
 {
+  const int order = mesh->order;
   const size_t smem = dynamic_smem (order, mode, block);
   const bool wide = lp.wide != nullptr;
   if (smem > 48 * 1024)
-    cudaFuncSetAttribute (persistent_fn (order, mode, wide), cudaFuncAttributeMaxDynamicSharedMemorySize,
+    cudaFuncSetAttribute (persistent_fn (mesh, mode, wide), cudaFuncAttributeMaxDynamicSharedMemorySize,
                           (int)smem);
-  if (order == 1) { if (wide) launch_pw<1, true> (mode, grid, block, smem, s, lp, pts, ord, n, chunk, head, cell, ref, st); else launch_pw<1, false> (mode, grid, block, smem, s, lp, pts, ord, n, chunk, head, cell, ref, st); }
-  else if (order == 2) { if (wide) launch_pw<2, true> (mode, grid, block, smem, s, lp, pts, ord, n, chunk, head, cell, ref, st); else launch_pw<2, false> (mode, grid, block, smem, s, lp, pts, ord, n, chunk, head, cell, ref, st); }
-  else { if (wide) launch_pw<3, true> (mode, grid, block, smem, s, lp, pts, ord, n, chunk, head, cell, ref, st); else launch_pw<3, false> (mode, grid, block, smem, s, lp, pts, ord, n, chunk, head, cell, ref, st); }
+  if (mesh->shape == DRB_SHAPE_SIMPLEX)
+    launch_s<kSimplex> (order, wide, mode, grid, block, smem, s, lp, pts, ord, n, chunk, head, cell, ref, st);
+  else
+    launch_s<kTensor> (order, wide, mode, grid, block, smem, s, lp, pts, ord, n, chunk, head, cell, ref, st);
   return check_launch ("locate_persistent_kernel");
 }
 
-int resident_blocks (int order, int mode, bool wide, int block)
+int resident_blocks (const drb_mesh *mesh, int mode, bool wide, int block)
 {
-  const size_t smem = dynamic_smem (order, mode, block);
-  const void *fn = persistent_fn (order, mode, wide);
+  const size_t smem = dynamic_smem (mesh->order, mode, block);
+  const void *fn = persistent_fn (mesh, mode, wide);
   if (smem > 48 * 1024)
     cudaFuncSetAttribute (fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
   int nb = 0;
@@ -352,7 +371,7 @@ LocateParams make_params (const drb_mesh *mesh, const drb_bvh *bvh, const drb_ne
   lp.packed = mesh->packed;
   lp.ctrl_idx = mesh->ctrl_idx;
   lp.xyz = mesh->values;
-  lp.stride = packed_stride ((mesh->order + 1) * (mesh->order + 1) * (mesh->order + 1), 3);
+  lp.stride = packed_stride (mesh_nd (mesh), 3);
   lp.tol = opts->tol;
   lp.max_steps = opts->max_steps;
   lp.guess_mode = opts->guess_mode;
@@ -368,9 +387,10 @@ int check_args (const drb_mesh *mesh, const drb_bvh *bvh, const float *pts, int 
     set_last_error ("locate_batched: bad arguments");
     return DRB_ERR_INVALID_ARG;
   }
-  if (mesh->dim != 3 || mesh->ncomp != 3 || mesh->order < 1 || mesh->order > 3)
+  if (mesh->dim != 3 || mesh->ncomp != 3 || mesh->order < 1 || mesh->order > 3 ||
+      (mesh->shape != DRB_SHAPE_TENSOR && mesh->shape != DRB_SHAPE_SIMPLEX))
   {
-    set_last_error ("locate_batched: needs a hex geometry mesh of order 1..3");
+    set_last_error ("locate_batched: needs a hex or tet geometry mesh of order 1..3");
     return DRB_ERR_UNSUPPORTED;
   }
   if (opts->guess_mode == DRB_GUESS_GIVEN && !opts->guess)
@@ -442,7 +462,7 @@ int locate_batched_impl (const drb_mesh *mesh, const drb_bvh *bvh, const float *
   if (scr.err != cudaSuccess) return status_from (scr.err);
   cudaMemsetAsync (head, 0, sizeof (int), s);
   const int mode = effective_mode (mesh, cfg.reg_elements);
-  const int per_sm = resident_blocks (mesh->order, mode, bvh->wide_nodes != nullptr, cfg.block);
+  const int per_sm = resident_blocks (mesh, mode, bvh->wide_nodes != nullptr, cfg.block);
   const int bps = (cfg.blocks_per_sm > 0) ? min (cfg.blocks_per_sm, per_sm) : per_sm;
   const long long warps_needed = ((long long)n + 31) / 32;
   long long blocks = (long long)bps * sm_count ();
@@ -450,7 +470,7 @@ int locate_batched_impl (const drb_mesh *mesh, const drb_bvh *bvh, const float *
   if (blocks > blocks_needed) blocks = blocks_needed;
   if (blocks < 1) blocks = 1;
   const LocateParams lp = make_params (mesh, bvh, opts);
-  return launch_persistent (mesh->order, mode, dim3 ((unsigned)blocks), cfg.block, s, lp, pts, ord, n,
+  return launch_persistent (mesh, mode, dim3 ((unsigned)blocks), cfg.block, s, lp, pts, ord, n,
                             cfg.chunk, head, cell, ref, stats);
 }
 
@@ -480,7 +500,7 @@ int locate_batched_ws (const drb_mesh *mesh, const drb_bvh *bvh, const float *pt
   cudaError_t e = cudaMemsetAsync (ws.head, 0, sizeof (int), s);
   if (e != cudaSuccess) return status_from (e);
   const int mode = effective_mode (mesh, cfg.reg_elements);
-  const int per_sm = resident_blocks (mesh->order, mode, bvh->wide_nodes != nullptr, cfg.block);
+  const int per_sm = resident_blocks (mesh, mode, bvh->wide_nodes != nullptr, cfg.block);
   const int bps = (cfg.blocks_per_sm > 0) ? min (cfg.blocks_per_sm, per_sm) : per_sm;
   const long long warps_needed = ((long long)n + 31) / 32;
   long long blocks = (long long)bps * sm_count ();
@@ -488,7 +508,7 @@ int locate_batched_ws (const drb_mesh *mesh, const drb_bvh *bvh, const float *pt
   if (blocks > blocks_needed) blocks = blocks_needed;
   if (blocks < 1) blocks = 1;
   const LocateParams lp = make_params (mesh, bvh, opts);
-  return launch_persistent (mesh->order, mode, dim3 ((unsigned)blocks), cfg.block, s, lp, pts, ord, n,
+  return launch_persistent (mesh, mode, dim3 ((unsigned)blocks), cfg.block, s, lp, pts, ord, n,
                             cfg.chunk, ws.head, cell, ref, stats);
 }
 

@@ -198,7 +198,8 @@ extern "C" int drb_locate_hinted (const drb_mesh *mesh, const drb_bvh *bvh, cons
     set_last_error ("locate_hinted: bad arguments");
     return DRB_ERR_INVALID_ARG;
   }
-  if (mesh->dim != 3 || mesh->ncomp != 3 || mesh->order < 1 || mesh->order > 3)
+  if (mesh->dim != 3 || mesh->ncomp != 3 || mesh->order < 1 || mesh->order > 3 ||
+      mesh->shape != DRB_SHAPE_TENSOR)
   {
     set_last_error ("locate_hinted: needs a hex geometry mesh of order 1..3");
     return DRB_ERR_UNSUPPORTED;

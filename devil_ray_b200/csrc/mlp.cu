@@ -709,7 +709,8 @@ extern "C" int drb_mlp_features (const drb_mesh *mesh, const int *elem, const fl
                                  int n_pad, void *X, void *stream)
 {
   if (!mesh || !mesh->packed || mesh->dim != 3 || mesh->order != 2 || mesh->ncomp != 3 ||
-      n < 0 || n_pad < n || (n_pad > 0 && !X) || (n > 0 && (!elem || !pts)))
+      mesh->shape != DRB_SHAPE_TENSOR || n < 0 || n_pad < n || (n_pad > 0 && !X) ||
+      (n > 0 && (!elem || !pts)))
   {
     set_last_error ("mlp_features: needs a packed order-2 hex mesh and n <= n_pad");
     return DRB_ERR_INVALID_ARG;
@@ -894,7 +895,8 @@ extern "C" int drb_mlp_guess (const float *params, const void *wbf16, const drb_
                               float *guess, int *err, void *stream)
 {
   if (!params || !wbf16 || !mesh || !mesh->packed || mesh->dim != 3 || mesh->order != 2 ||
-      mesh->ncomp != 3 || n < 0 || (n > 0 && (!elem || !pts || !guess)))
+      mesh->ncomp != 3 || mesh->shape != DRB_SHAPE_TENSOR || n < 0 ||
+      (n > 0 && (!elem || !pts || !guess)))
   {
     set_last_error ("mlp_guess: needs a packed order-2 hex mesh");
     return DRB_ERR_INVALID_ARG;

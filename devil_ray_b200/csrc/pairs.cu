@@ -8,13 +8,14 @@
 #include "drb_common.cuh"
 #include "drb_internal.h"
 #include "newton.cuh"
+#include "simplex.cuh"
 
 namespace drb
 {
 namespace
 {
 
-template <int P>
+template <int P, bool TET>
 __global__ void map_points_kernel (const float *__restrict__ packed, int stride,
                                    const int *__restrict__ elem, const float *__restrict__ ref,
                                    int n, float *__restrict__ pts)
@@ -27,8 +28,18 @@ __global__ void map_points_kernel (const float *__restrict__ packed, int stride,
   {
     const float *row = packed + (size_t)e * stride;
     PackedCP cp{ row };
-    hex_eval<P, 3> (cp, ref[3 * (size_t)i], ref[3 * (size_t)i + 1], ref[3 * (size_t)i + 2], X);
-    to_world<(P + 1) * (P + 1) * (P + 1)> (row, X);
+    const float u = ref[3 * (size_t)i], v = ref[3 * (size_t)i + 1], w = ref[3 * (size_t)i + 2];
+    if (TET)
+    {
+      float Ju[3], Jv[3], Jw[3];
+      tet_eval_d<P, 3> (cp, u, v, w, X, Ju, Jv, Jw);
+      to_world<tet_dofs<P> ()> (row, X);
+    }
+    else
+    {
+      hex_eval<P, 3> (cp, u, v, w, X);
+      to_world<(P + 1) * (P + 1) * (P + 1)> (row, X);
+    }
   }
   pts[3 * (size_t)i] = X[0];
   pts[3 * (size_t)i + 1] = X[1];
@@ -81,7 +92,7 @@ __global__ void newton_pairs_kernel (const float *__restrict__ packed, int strid
 
 // UnstructuredField::eval at located points (unstructured_field.cpp:214-245):
 // value of the scalar field at (cell, ref); cell -1 -> empty value.
-template <int P>
+template <int P, bool TET>
 __global__ void field_eval_kernel (const float *__restrict__ packed, int stride,
                                    const int *__restrict__ cell, const float *__restrict__ ref,
                                    int n, float empty, float *__restrict__ out)
@@ -98,18 +109,32 @@ __global__ void field_eval_kernel (const float *__restrict__ packed, int stride,
       DRB_D float operator() (int q, int) const { return __ldg (p + q); }
     } cp{ packed + (size_t)e * stride };
     float X[1];
-    hex_eval<P, 1> (cp, ref[3 * (size_t)i], ref[3 * (size_t)i + 1], ref[3 * (size_t)i + 2], X);
+    const float u = ref[3 * (size_t)i], vv = ref[3 * (size_t)i + 1], w = ref[3 * (size_t)i + 2];
+    if (TET)
+    {
+      float Ju[1], Jv[1], Jw[1];
+      tet_eval_d<P, 1> (cp, u, vv, w, X, Ju, Jv, Jw);
+    }
+    else
+    {
+      hex_eval<P, 1> (cp, u, vv, w, X);
+    }
     v = X[0];
   }
   out[i] = v;
 }
 
-int check_pairs (const drb_mesh *m, int n)
+int check_pairs (const drb_mesh *m, int n, bool tets_ok = false)
 {
   if (!m || !m->packed || m->dim != 3 || m->ncomp != 3 || m->order < 1 || m->order > 3 || n < 0)
   {
     set_last_error ("pairs: needs a packed hex geometry mesh of order 1..3");
     return DRB_ERR_INVALID_ARG;
+  }
+  if (m->shape != DRB_SHAPE_TENSOR && !(tets_ok && m->shape == DRB_SHAPE_SIMPLEX))
+  {
+    set_last_error ("pairs: element shape not supported here");
+    return DRB_ERR_UNSUPPORTED;
   }
   return DRB_OK;
 }
@@ -122,7 +147,7 @@ using namespace drb;
 extern "C" int drb_map_points (const drb_mesh *mesh, const int *elem, const float *ref, int n,
                                float *pts, void *stream)
 {
-  int st = check_pairs (mesh, n);
+  int st = check_pairs (mesh, n, true);
   if (st) return st;
   if (n == 0) return DRB_OK;
   if (!elem || !ref || !pts)
@@ -130,13 +155,20 @@ extern "C" int drb_map_points (const drb_mesh *mesh, const int *elem, const floa
     set_last_error ("map_points: NULL array");
     return DRB_ERR_INVALID_ARG;
   }
-  const int nd = (mesh->order + 1) * (mesh->order + 1) * (mesh->order + 1);
-  const int stride = packed_stride (nd, 3);
+  const int stride = packed_stride (mesh_nd (mesh), 3);
   cudaStream_t s = (cudaStream_t)stream;
   const int b = div_up (n, 256);
-  if (mesh->order == 1) map_points_kernel<1><<<b, 256, 0, s>>> (mesh->packed, stride, elem, ref, n, pts);
-  else if (mesh->order == 2) map_points_kernel<2><<<b, 256, 0, s>>> (mesh->packed, stride, elem, ref, n, pts);
-  else map_points_kernel<3><<<b, 256, 0, s>>> (mesh->packed, stride, elem, ref, n, pts);
+#define DRB_MP(P, T) map_points_kernel<P, T><<<b, 256, 0, s>>> (mesh->packed, stride, elem, ref, n, pts)
+  if (mesh->shape == DRB_SHAPE_SIMPLEX)
+  {
+    if (mesh->order == 1) DRB_MP (1, true);
+    else if (mesh->order == 2) DRB_MP (2, true);
+    else DRB_MP (3, true);
+  }
+  else if (mesh->order == 1) DRB_MP (1, false);
+  else if (mesh->order == 2) DRB_MP (2, false);
+  else DRB_MP (3, false);
+#undef DRB_MP
   return check_launch ("map_points_kernel");
 }
 
@@ -169,18 +201,26 @@ extern "C" int drb_field_eval (const drb_mesh *field, const int *cell, const flo
                                float empty_value, float *values, void *stream)
 {
   if (!field || !field->packed || field->dim != 3 || field->ncomp != 1 || field->order < 1 ||
-      field->order > 3 || n < 0 || (n > 0 && (!cell || !ref || !values)))
+      field->order > 3 || n < 0 || (n > 0 && (!cell || !ref || !values)) ||
+      (field->shape != DRB_SHAPE_TENSOR && field->shape != DRB_SHAPE_SIMPLEX))
   {
-    set_last_error ("field_eval: needs a packed scalar hex field of order 1..3");
+    set_last_error ("field_eval: needs a packed scalar hex or tet field of order 1..3");
     return DRB_ERR_INVALID_ARG;
   }
   if (n == 0) return DRB_OK;
-  const int nd = (field->order + 1) * (field->order + 1) * (field->order + 1);
-  const int stride = packed_stride (nd, 1);
+  const int stride = packed_stride (mesh_nd (field), 1);
   cudaStream_t s = (cudaStream_t)stream;
   const int b = div_up (n, 256);
-  if (field->order == 1) field_eval_kernel<1><<<b, 256, 0, s>>> (field->packed, stride, cell, ref, n, empty_value, values);
-  else if (field->order == 2) field_eval_kernel<2><<<b, 256, 0, s>>> (field->packed, stride, cell, ref, n, empty_value, values);
-  else field_eval_kernel<3><<<b, 256, 0, s>>> (field->packed, stride, cell, ref, n, empty_value, values);
+#define DRB_FE(P, T) field_eval_kernel<P, T><<<b, 256, 0, s>>> (field->packed, stride, cell, ref, n, empty_value, values)
+  if (field->shape == DRB_SHAPE_SIMPLEX)
+  {
+    if (field->order == 1) DRB_FE (1, true);
+    else if (field->order == 2) DRB_FE (2, true);
+    else DRB_FE (3, true);
+  }
+  else if (field->order == 1) DRB_FE (1, false);
+  else if (field->order == 2) DRB_FE (2, false);
+  else DRB_FE (3, false);
+#undef DRB_FE
   return check_launch ("field_eval_kernel");
 }

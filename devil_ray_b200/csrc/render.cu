@@ -1049,7 +1049,7 @@ static int volume_common (const drb_mesh *mesh, const drb_mesh *field, const drb
   }
   if (mesh->dim != 3 || mesh->ncomp != 3 || field->dim != 3 || field->ncomp != 1 ||
       mesh->order != field->order || mesh->n_elem != field->n_elem || mesh->order < 1 ||
-      mesh->order > 3)
+      mesh->order > 3 || mesh->shape != DRB_SHAPE_TENSOR || field->shape != DRB_SHAPE_TENSOR)
   {
     set_last_error ("volume: needs a hex mesh and a scalar hex field of the same order 1..3");
     return DRB_ERR_UNSUPPORTED;

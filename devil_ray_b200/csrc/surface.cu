@@ -578,7 +578,7 @@ extern "C" int drb_mesh_boundary (const drb_mesh *hex, const int *field_ctrl_idx
                                   int *n_faces, void *stream)
 {
   if (!hex || hex->dim != 3 || hex->order < 1 || hex->order > 3 || hex->n_elem < 0 || !n_faces ||
-      (hex->n_elem > 0 && !hex->ctrl_idx))
+      hex->shape != DRB_SHAPE_TENSOR || (hex->n_elem > 0 && !hex->ctrl_idx))
   {
     set_last_error ("mesh_boundary: needs a hex mesh of order 1..3");
     return DRB_ERR_INVALID_ARG;
@@ -648,7 +648,8 @@ extern "C" int drb_surface_intersect (const drb_mesh *faces, const drb_bvh *bvh,
     set_last_error ("surface_intersect: bad arguments");
     return DRB_ERR_INVALID_ARG;
   }
-  if (faces->dim != 2 || faces->ncomp != 3 || faces->order < 1 || faces->order > 3)
+  if (faces->dim != 2 || faces->ncomp != 3 || faces->order < 1 || faces->order > 3 ||
+      faces->shape != DRB_SHAPE_TENSOR)
   {
     set_last_error ("surface_intersect: needs a quad mesh of order 1..3");
     return DRB_ERR_UNSUPPORTED;
@@ -689,7 +690,8 @@ extern "C" int drb_surface_shade (const drb_mesh *faces, const drb_mesh *face_fi
     return DRB_ERR_INVALID_ARG;
   }
   if (!faces->packed || !face_field->packed || faces->order != face_field->order ||
-      faces->dim != 2 || face_field->ncomp != 1)
+      faces->dim != 2 || face_field->ncomp != 1 || faces->shape != DRB_SHAPE_TENSOR ||
+      face_field->shape != DRB_SHAPE_TENSOR)
   {
     set_last_error ("surface_shade: needs packed quad geometry and scalar field of one order");
     return DRB_ERR_INVALID_ARG;

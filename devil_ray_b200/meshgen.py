@@ -159,6 +159,86 @@ def trilinear_distorted_mesh(n: int, p: int, distortion: float, seed: int) -> He
                        xyz=xyz.astype(np.float32), field=f.astype(np.float32), meta=meta)
 
 
+@dataclass
+class TetMeshData:
+    order: int
+    n: int                      # cubes per axis (6 tets each)
+    ctrl_idx: np.ndarray        # int32 [n_elem * (p+1)(p+2)(p+3)/6]
+    xyz: np.ndarray             # float32 [n_ctrl, 3]
+    field: np.ndarray           # float32 [n_ctrl]
+    meta: dict = field(default_factory=dict)
+
+    @property
+    def n_elem(self) -> int:
+        return 6 * self.n ** 3
+
+    @property
+    def n_ctrl(self) -> int:
+        return self.xyz.shape[0]
+
+    @property
+    def nd(self) -> int:
+        return tet_dofs(self.order)
+
+
+def tet_dofs(p: int) -> int:
+    return (p + 1) * (p + 2) * (p + 3) // 6
+
+
+def tet_multi_indices(p: int):
+    """Dof multi-indices (i, j, k) of an order-p tet in the reference's dof
+    order: i (power of u) fastest, then j (v), then k (w)."""
+    return [(i, j, k) for k in range(p + 1) for j in range(p + 1 - k) for i in range(p + 1 - k - j)]
+
+
+# The six tets of a cube (Kuhn subdivision): for a permutation (a, b, c) of
+# the axes, vertices v0 = cube origin, v1 = v0 + e_a, v2 = v1 + e_b,
+# v3 = v2 + e_c.  Every cube uses the same diagonal, so faces match.
+KUHN_PERMS = ((0, 1, 2), (0, 2, 1), (1, 0, 2), (1, 2, 0), (2, 0, 1), (2, 1, 0))
+
+
+def tet_lattice_ctrl_idx(n: int, p: int) -> np.ndarray:
+    """ctrl_idx of the 6 n^3 order-p tets of an n^3 cube lattice over the
+    (p n + 1)^3 lattice points of lattice_points(n, p).  Tet (cube c, perm
+    q) has id 6 * ((ck n + cj) n + ci) + q; its reference vertices are
+    origin -> v0, u = 1 -> v1, v = 1 -> v2, w = 1 -> v3, so dof (i, j, k)
+    sits at lattice point p v0 + i e_a + j (e_a + e_b) + k (e_a + e_b + e_c)."""
+    m = p * n + 1
+    mi = np.array(tet_multi_indices(p), np.int64)             # [nd, 3]
+    out = np.empty((n, n, n, 6, mi.shape[0]), np.int64)
+    c = np.arange(n, dtype=np.int64)
+    CK, CJ, CI = np.meshgrid(c, c, c, indexing="ij")
+    for q, (a, b, cc) in enumerate(KUHN_PERMS):
+        off = np.zeros((mi.shape[0], 3), np.int64)            # lattice offset (x, y, z)
+        off[:, a] += mi[:, 0] + mi[:, 1] + mi[:, 2]
+        off[:, b] += mi[:, 1] + mi[:, 2]
+        off[:, cc] += mi[:, 2]
+        X = p * CI[..., None] + off[None, None, None, :, 0]
+        Y = p * CJ[..., None] + off[None, None, None, :, 1]
+        Z = p * CK[..., None] + off[None, None, None, :, 2]
+        out[:, :, :, q, :] = (Z * m + Y) * m + X
+    return out.reshape(-1).astype(np.int32)
+
+
+def tet_warped_mesh(n: int, p: int, amp: float, jitter: float = 0.0, seed: int = 0) -> TetMeshData:
+    """6 n^3 order-p tets filling [0,1]^3, interior lattice points displaced
+    by amp * sin(2pi x) sin(2pi y) sin(2pi z) on every axis (plus optional
+    uniform jitter), f = sin(3x)cos(2y)+z^2 at the displaced points."""
+    base = lattice_points(n, p)
+    inner = interior_mask(n, p)
+    s = np.sin(TWO_PI * base[:, 0]) * np.sin(TWO_PI * base[:, 1]) * np.sin(TWO_PI * base[:, 2])
+    xyz = base.copy()
+    xyz[inner] += (amp * s)[inner, None]
+    if jitter > 0.0:
+        rng = np.random.default_rng(seed)
+        xyz[inner] += rng.uniform(-jitter, jitter, size=(int(inner.sum()), 3))
+    meta = {"warp_amplitude": amp, "jitter": jitter, "seed": seed,
+            "field": "sin(3x)cos(2y)+z^2", "cells": "6 Kuhn tets per cube"}
+    return TetMeshData(order=p, n=n, ctrl_idx=tet_lattice_ctrl_idx(n, p),
+                       xyz=xyz.astype(np.float32), field=field_sincos(xyz).astype(np.float32),
+                       meta=meta)
+
+
 # outside fraction of uniform queries: the meshes fill [0,1]^3, so queries are
 # drawn from a cube padded so that about 8% of its volume lies outside
 OUTSIDE_FRACTION = 0.08

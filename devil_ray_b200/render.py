@@ -111,17 +111,22 @@ class ColorMap:
 
 
 class UnstructuredField:
-    """Scalar hex field on the mesh's element layout (UnstructuredField<HexScalar>)."""
+    """Scalar field on the mesh's element layout: UnstructuredField<HexScalar*>,
+    or with shape=SHAPE_SIMPLEX UnstructuredField<TetScalar*>."""
 
-    def __init__(self, ctrl_idx, values, order: int, name: str = "f", device="cuda"):
+    def __init__(self, ctrl_idx, values, order: int, name: str = "f", device="cuda",
+                 shape: int = L.SHAPE_TENSOR):
         self.order = int(order)
         self.name = name
+        self.shape = int(shape)
         self.device = torch.device(device)
         self.ctrl_idx = _dev(ctrl_idx, torch.int32, device)
         self.values = _dev(values, torch.float32, device).reshape(-1)
-        nd = (self.order + 1) ** 3
+        nd = L.lib().drb_elem_dofs(self.shape, 3, self.order)
+        if nd < 0:
+            raise ValueError(f"unsupported field: shape {shape}, order {order}")
         self.n_elem = self.ctrl_idx.numel() // nd
-        stride = L.lib().drb_packed_stride(3, self.order, 1)
+        stride = L.lib().drb_packed_stride_shape(self.shape, 3, self.order, 1)
         self.packed = torch.empty((max(self.n_elem, 1), stride), dtype=torch.float32,
                                   device=self.device)
         d = self.desc(packed=False)
@@ -132,6 +137,7 @@ class UnstructuredField:
     def desc(self, packed=True) -> L.DrbMesh:
         m = L.DrbMesh()
         m.dim, m.order, m.ncomp = 3, self.order, 1
+        m.shape = self.shape
         m.n_elem = self.n_elem
         m.n_ctrl = self.values.numel()
         m.ctrl_idx = self.ctrl_idx.data_ptr()
@@ -337,6 +343,7 @@ class QuadField(UnstructuredField):
     def __init__(self, ctrl_idx, values, order: int, name: str = "f", device="cuda"):
         self.order = int(order)
         self.name = name
+        self.shape = L.SHAPE_TENSOR
         self.device = torch.device(device)
         self.ctrl_idx = _dev(ctrl_idx, torch.int32, device)
         self.values = _dev(values, torch.float32, device).reshape(-1)

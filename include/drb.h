@@ -37,7 +37,8 @@ enum drb_guess_mode
    * DeviceMesh::locate passes use_init_guess=true with an uninitialised
    * guess (data_model/device_mesh.hpp:327-334). */
   DRB_GUESS_ZERO = 0,
-  /* element centre (0.5,0.5,0.5): the plain GPU path. */
+  /* element centre: (0.5,0.5,0.5) for tensor elements, the centroid
+   * (0.25,0.25,0.25) for tets; the plain GPU path. */
   DRB_GUESS_ELEM_CENTER = 1,
   /* centre of the candidate leaf's reference sub-box, the reference's
    * intended guess (device_mesh.hpp:161-162). */
@@ -48,21 +49,37 @@ enum drb_guess_mode
   DRB_GUESS_GIVEN = 3
 };
 
-/* A tensor-product Bernstein mesh or field: GridFunction<ncomp> of the
- * reference (data_model/grid_function.hpp:19-30).  dim 3 = hex, dim 2 = quad. */
+/* Element shape of a drb_mesh (ElemType, data_model/elem_attr.hpp). */
+enum drb_shape
+{
+  DRB_SHAPE_TENSOR = 0,  /* hex (dim 3), quad (dim 2): (order+1)^dim dofs */
+  DRB_SHAPE_SIMPLEX = 1  /* tet (dim 3): (order+1)(order+2)(order+3)/6 dofs in
+                            the reference's order (i fastest, then j, then k;
+                            elem_ops.hpp:901-1030) */
+};
+
+/* A Bernstein mesh or field: GridFunction<ncomp> of the reference
+ * (data_model/grid_function.hpp:19-30).  dim 3 = hex or tet, dim 2 = quad;
+ * shape (drb_shape) selects tensor or simplex elements.  Tet meshes are
+ * accepted by drb_pack_elements, drb_elem_subboxes, drb_lbvh_build,
+ * drb_bvh_widen, drb_locate, drb_locate_batched (and its ordered, host and
+ * allocation-free forms, and drb_locate_tune), drb_field_eval and
+ * drb_map_points; the other entry points return DRB_ERR_UNSUPPORTED for
+ * them. */
 typedef struct drb_mesh
 {
-  int dim;               /* 3 hex, 2 quad */
+  int dim;               /* 3 hex or tet, 2 quad */
   int order;             /* polynomial order 1..3 */
   int ncomp;             /* 3 geometry, 1 scalar field */
   int n_elem;
   int n_ctrl;
-  const int *ctrl_idx;   /* device int32[n_elem * (order+1)^dim] */
+  const int *ctrl_idx;   /* device int32[n_elem * drb_elem_dofs()] */
   const float *values;   /* device float[n_ctrl * ncomp] */
-  const float *packed;   /* optional device float[n_elem * drb_packed_stride()]:
+  const float *packed;   /* optional device float[n_elem * drb_packed_stride_shape()]:
                             element-major copy made by drb_pack_elements(), or NULL */
   const int *face_neighbors; /* optional device int32[6 * n_elem] of a hex geometry
                             mesh (drb_mesh_face_neighbors), or NULL */
+  int shape;             /* drb_shape; 0 (tensor) when zero-initialised */
 } drb_mesh;
 
 /* Face neighbours of a hex mesh (no reference counterpart; faces are
@@ -82,7 +99,9 @@ typedef struct drb_bvh
   float *inner_nodes;    /* device float[16 * n_inner]: 4 x float4 per node */
   int *leaf_nodes;       /* device int32[n_leaf]: element id per sorted leaf */
   int *aabb_ids;         /* device int32[n_leaf]: sub-box id per sorted leaf */
-  float *ref_boxes;      /* device float[n_leaf * 2 * dim]: reference sub-box per sub-box id */
+  float *ref_boxes;      /* device float[n_leaf * drb_ref_box_floats()]: reference
+                            sub-box per sub-box id (tensor: low then high corner;
+                            simplex: u, v, w axis vertices, then the origin) */
   float bounds[6];       /* host: xmin,xmax,ymin,ymax,zmin,zmax (filled by the build) */
   /* Optional 4-wide collapse of the same tree for the batched kernels
    * (drb_bvh_widen); NULL: they traverse the binary nodes. */
@@ -132,6 +151,15 @@ unsigned long long drb_kernel_launches (void);
  * origin), scalar fields nd. */
 int drb_packed_stride (int dim, int order, int ncomp);
 
+/* Dofs per element and packed-row stride for any shape (drb_shape);
+ * drb_packed_stride is the tensor case.  -1 for unsupported arguments. */
+int drb_elem_dofs (int shape, int dim, int order);
+int drb_packed_stride_shape (int shape, int dim, int order, int ncomp);
+
+/* Floats per reference sub-box: SubRef<dim,Tensor> 2 dim,
+ * SubRef<dim,Simplex> dim (dim + 1) (data_model/subref.hpp:26-35). */
+int drb_ref_box_floats (int shape, int dim);
+
 /* Gather the element control points into an element-major array
  * (replaces the double indirection val[ctrl_idx[e*nd+i]] of SharedDofPtr,
  * data_model/dof_access.hpp:23-54).  Geometry rows hold P_i - P_0 (FP32)
@@ -140,7 +168,7 @@ int drb_packed_stride (int dim, int order, int ncomp);
  * size rather than to the domain.  Scalar rows hold the values. */
 int drb_pack_elements (const drb_mesh *mesh, float *packed, void *stream);
 
-/* Sizes of the BVH over a mesh's sub-boxes: 33 per hex, 17 per quad
+/* Sizes of the BVH over a mesh's sub-boxes: 33 per hex or tet, 17 per quad
  * (construct_bvh, data_model/mesh_utils.cpp:527-531). */
 int drb_bvh_sizes (int dim, int n_elem, int *n_inner, int *n_leaf);
 
@@ -148,8 +176,14 @@ int drb_bvh_sizes (int dim, int n_elem, int *n_inner, int *n_leaf);
  * data_model/mesh_utils.cpp:557-670): 32 (hex) / 16 (quad) de Casteljau
  * splits of the largest box, convex-hull AABBs scaled by 1.000001.
  * Outputs per sub-box (element-major, e*(splits+1)+i): aabbs6 device
- * float[6*n], prim_ids device int32[n], ref_boxes device float[2*dim*n];
- * bounds6 device float[6] receives the reduction of linear_bvh_builder.cpp:19-58. */
+ * float[6*n], prim_ids device int32[n], ref_boxes device
+ * float[drb_ref_box_floats()*n]; bounds6 device float[6] receives the
+ * reduction of linear_bvh_builder.cpp:19-58.  Tets split the longest edge of
+ * the reference sub-simplex (mesh_utils.cpp:455-480, elem_ops.hpp:1270-1311)
+ * with the dof layout of the element evaluators; at order 1 the boxes are
+ * bit-identical to the reference's, at orders 2-3 the reference's split
+ * indexes the wrong dofs (cartesian_to_tet_idx, elem_ops.hpp:32-47) and its
+ * boxes differ. */
 int drb_elem_subboxes (const drb_mesh *mesh, float *aabbs6, int *prim_ids, float *ref_boxes,
                        float *bounds6, void *stream);
 
@@ -447,7 +481,8 @@ int drb_field_eval (const drb_mesh *field, const int *cell, const float *ref, in
 int drb_lineout_points (const float *starts, const float *ends, int n_lines, int samples,
                         float *points, void *stream);
 
-/* Physical points X_e(r) (Element::eval, pos_tensor_element.tcc:99-232). */
+/* Physical points X_e(r) (Element::eval, pos_tensor_element.tcc:99-232;
+ * tets elem_ops.hpp:901-1030). */
 int drb_map_points (const drb_mesh *mesh, const int *elem, const float *ref, int n, float *pts,
                     void *stream);
 /* Newton in a given element per point (eval_inverse_local,

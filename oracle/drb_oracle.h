@@ -38,6 +38,30 @@ void orc_locate (int p, int n_elem, const int *ctrl_idx, const float *xyz, int n
 void orc_newton_fp64 (int p, const int *ctrl_idx, const float *xyz, int n, const int *elem,
                       const float *pts, double *ref_out, int *ok);
 
+/* Per-tet sub-boxes of construct_bvh (mesh_utils.cpp:514-677) for order-p
+ * tets: 33 per element, aabbs6 (scaled by 1.000001) and ref12 (the
+ * reference sub-simplex: u, v, w axis vertices, then the origin), element
+ * major.  reference_index != 0 linearises the split's dof multi-indices with
+ * the reference's cartesian_to_tet_idx (elem_ops.hpp:32-47), which for
+ * orders >= 2 addresses other dofs than the evaluators' layout; 0 uses that
+ * layout.  float arithmetic in the reference's operation order. */
+void orc_tet_subboxes (int p, int n_elem, const int *ctrl_idx, const float *xyz,
+                       int reference_index, float *aabbs6, float *ref12);
+
+/* Bernstein tet eval with derivatives at n reference points, order p (any
+ * p >= 0), ncomp components; cp = (p+1)(p+2)(p+3)/6 * ncomp values of one
+ * element in the reference's dof order.  X: n*ncomp, J: n*3*ncomp.  double. */
+void orc_tet_eval_d (int p, int ncomp, const double *cp, int n, const double *ref, double *X,
+                     double *J);
+
+/* orc_locate for order-p tets: simplex evaluation, inside test and
+ * sub-simplex centre guess (ref_boxes 12 floats per sub-box), element centre
+ * (0.25,0.25,0.25). */
+void orc_locate_tet (int p, const int *ctrl_idx, const float *xyz, const float *inner_nodes,
+                     const int *leaf_nodes, const int *aabb_ids, const float *ref_boxes, int n,
+                     const float *pts, float tol, int max_steps, int guess_mode, const float *guess,
+                     int use_double, int local_frame, int *cell, float *ref, int *iters, int *cands);
+
 #ifdef __cplusplus
 }
 #endif

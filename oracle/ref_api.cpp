@@ -103,6 +103,25 @@ std::shared_ptr<Field> make_hex_field (int order, const GridFunction<1> &gf, con
   return std::make_shared<UnstructuredField<HexScalar>> (gf, order, name);
 }
 
+// Tet meshes: the fixed-order specialisations (TetMesh_P1/_P2) when
+// `fixed`, else the general-order TetMesh (UnstructuredMesh<Tet3>).
+std::shared_ptr<Mesh> make_tet_mesh (int order, int fixed, const GridFunction<3> &gf)
+{
+  if (fixed && order == 1) return std::make_shared<TetMesh_P1> (gf, 1);
+  if (fixed && order == 2) return std::make_shared<TetMesh_P2> (gf, 2);
+  return std::make_shared<TetMesh> (gf, order);
+}
+
+std::shared_ptr<Field> make_tet_field (int order, int fixed, const GridFunction<1> &gf,
+                                       const char *name)
+{
+  if (fixed && order == 1)
+    return std::make_shared<UnstructuredField<TetScalar_P1>> (gf, 1, name);
+  if (fixed && order == 2)
+    return std::make_shared<UnstructuredField<TetScalar_P2>> (gf, 2, name);
+  return std::make_shared<UnstructuredField<TetScalar>> (gf, order, name);
+}
+
 template <typename MeshT> BVH bvh_of (Mesh *m)
 {
   return dynamic_cast<MeshT *> (m)->get_bvh ();
@@ -116,6 +135,9 @@ BVH get_bvh_any (Mesh *m)
   if (auto *p = dynamic_cast<QuadMesh_P1 *> (m)) return p->get_bvh ();
   if (auto *p = dynamic_cast<QuadMesh_P2 *> (m)) return p->get_bvh ();
   if (auto *p = dynamic_cast<QuadMesh *> (m)) return p->get_bvh ();
+  if (auto *p = dynamic_cast<TetMesh_P1 *> (m)) return p->get_bvh ();
+  if (auto *p = dynamic_cast<TetMesh_P2 *> (m)) return p->get_bvh ();
+  if (auto *p = dynamic_cast<TetMesh *> (m)) return p->get_bvh ();
   throw std::runtime_error ("unsupported mesh type");
 }
 
@@ -134,6 +156,13 @@ int copy_ref_boxes (Mesh *m, float *out)
   { auto a = p->get_ref_aabbs (); std::memcpy (out, (const void *)a.get_host_ptr_const (), a.size () * 16); return 2; }
   if (auto *p = dynamic_cast<QuadMesh *> (m))
   { auto a = p->get_ref_aabbs (); std::memcpy (out, (const void *)a.get_host_ptr_const (), a.size () * 16); return 2; }
+  // SubRef<3,Simplex>: four vertices (u, v, w axis vertices, then the origin)
+  if (auto *p = dynamic_cast<TetMesh_P1 *> (m))
+  { auto a = p->get_ref_aabbs (); std::memcpy (out, (const void *)a.get_host_ptr_const (), a.size () * 48); return 4; }
+  if (auto *p = dynamic_cast<TetMesh_P2 *> (m))
+  { auto a = p->get_ref_aabbs (); std::memcpy (out, (const void *)a.get_host_ptr_const (), a.size () * 48); return 4; }
+  if (auto *p = dynamic_cast<TetMesh *> (m))
+  { auto a = p->get_ref_aabbs (); std::memcpy (out, (const void *)a.get_host_ptr_const (), a.size () * 48); return 4; }
   return 0;
 }
 
@@ -217,6 +246,35 @@ void *ref_hex_create (int order, int n_el, const int *ctrl_idx, int n_ctrl, cons
     if (field_vals != nullptr)
     {
       ds.add_field (make_hex_field (order, make_gf1 (n_el, nd, field_idx, n_field_ctrl, field_vals), "f"));
+      r->has_field = true;
+    }
+    r->collection.add_domain (ds);
+    return r;
+  }
+  catch (const std::exception &e)
+  {
+    g_err = e.what ();
+    return nullptr;
+  }
+}
+
+// Create a tet mesh (and optional scalar field "f") of polynomial order
+// `order`; `fixed` picks the fixed-order P1/P2 element types, otherwise the
+// general-order ones.
+void *ref_tet_create (int order, int fixed, int n_el, const int *ctrl_idx, int n_ctrl,
+                      const float *xyz, const int *field_idx, int n_field_ctrl,
+                      const float *field_vals)
+{
+  try
+  {
+    const int nd = (order + 1) * (order + 2) * (order + 3) / 6;
+    RefMesh *r = new RefMesh ();
+    r->order = order;
+    r->mesh = make_tet_mesh (order, fixed, make_gf3 (n_el, nd, ctrl_idx, n_ctrl, xyz));
+    DataSet ds (r->mesh);
+    if (field_vals != nullptr)
+    {
+      ds.add_field (make_tet_field (order, fixed, make_gf1 (n_el, nd, field_idx, n_field_ctrl, field_vals), "f"));
       r->has_field = true;
     }
     r->collection.add_domain (ds);
@@ -621,6 +679,48 @@ int ref_eval_hex_scalar (int p, int fixed, const float *vals, int n, const float
         v = Element<3, 1, ElemType::Tensor, Order::Quadratic>::create (0, rdp, p).eval_d (r, d);
       else
         v = Element<3, 1, ElemType::Tensor, Order::General>::create (0, rdp, p).eval_d (r, d);
+      out_val[q] = v[0];
+      for (int k = 0; k < 3; ++k) out_d3[3 * q + k] = d[k][0];
+    }
+    return 0;
+  }
+  catch (const std::exception &e)
+  {
+    g_err = e.what ();
+    return -1;
+  }
+}
+
+// Element<3,1,Simplex,*>::eval_d of one tet scalar element (dofs in the
+// reference's order) at n reference points.
+int ref_eval_tet_scalar (int p, int fixed, const float *vals, int n, const float *ref3,
+                         float *out_val, float *out_d3)
+{
+  try
+  {
+    const int nd = (p + 1) * (p + 2) * (p + 3) / 6;
+    std::vector<int32> ids (nd);
+    std::vector<Vec<Float, 1>> data (nd);
+    for (int i = 0; i < nd; ++i)
+    {
+      ids[i] = i;
+      data[i][0] = vals[i];
+    }
+    ReadDofPtr<Vec<Float, 1>> rdp;
+    rdp.m_offset_ptr = ids.data ();
+    rdp.m_dof_ptr = data.data ();
+    for (int q = 0; q < n; ++q)
+    {
+      Vec<Float, 3> r = { { ref3[3 * q], ref3[3 * q + 1], ref3[3 * q + 2] } };
+      Vec<Vec<Float, 1>, 3> d;
+      d = Vec<Float, 1>{ { 0.f } };
+      Vec<Float, 1> v;
+      if (fixed && p == 1)
+        v = Element<3, 1, ElemType::Simplex, Order::Linear>::create (0, rdp, p).eval_d (r, d);
+      else if (fixed && p == 2)
+        v = Element<3, 1, ElemType::Simplex, Order::Quadratic>::create (0, rdp, p).eval_d (r, d);
+      else
+        v = Element<3, 1, ElemType::Simplex, Order::General>::create (0, rdp, p).eval_d (r, d);
       out_val[q] = v[0];
       for (int k = 0; k < 3; ++k) out_d3[3 * q + k] = d[k][0];
     }

@@ -48,6 +48,9 @@ def lib():
         L.ref_eval_hex_scalar.argtypes = [C.c_int, C.c_int, vp, C.c_int, vp, vp, vp]
         L.ref_lineout.argtypes = [vp, C.c_int, vp, vp, C.c_int, C.c_float, vp, vp]
         L.ref_scalar_render.argtypes = [vp, C.c_int, C.c_int, vp, C.c_float, vp, vp, vp]
+        L.ref_tet_create.restype = vp
+        L.ref_tet_create.argtypes = [C.c_int, C.c_int, C.c_int, vp, C.c_int, vp, vp, C.c_int, vp]
+        L.ref_eval_tet_scalar.argtypes = [C.c_int, C.c_int, vp, C.c_int, vp, vp, vp]
         _lib = L
     return _lib
 
@@ -86,6 +89,8 @@ class RefHexMesh:
             lib().ref_free(self.h)
             self.h = None
 
+    ref_box_floats = 6
+
     def bvh(self):
         ni, nl = C.c_int(), C.c_int()
         if lib().ref_bvh_sizes(self.h, C.byref(ni), C.byref(nl)) != 0:
@@ -94,7 +99,7 @@ class RefHexMesh:
         leaf = np.zeros(nl.value, np.int32)
         ids = np.zeros(nl.value, np.int32)
         bounds = np.zeros(6, np.float32)
-        refb = np.zeros((nl.value, 6), np.float32)
+        refb = np.zeros((nl.value, self.ref_box_floats), np.float32)
         if lib().ref_bvh_copy(self.h, _p(inner), _p(leaf), _p(ids), _p(bounds), _p(refb)) != 0:
             raise RuntimeError(lib().ref_last_error().decode())
         return {"inner": inner, "leaf_nodes": leaf, "aabb_ids": ids, "bounds": bounds,
@@ -174,6 +179,40 @@ class RefHexMesh:
         if r < 0:
             raise RuntimeError(lib().ref_last_error().decode())
         return {"hit_idx": hit, "dist": dist, "ref": ref2, "rgba": img, "depth": depth}
+
+
+class RefTetMesh(RefHexMesh):
+    """The reference's UnstructuredMesh<Tet> (+ scalar field "f"): the
+    general-order element types, or with fixed=True the fixed-order P1/P2
+    specialisations the reference's dispatcher also offers."""
+
+    ref_box_floats = 12   # SubRef<3,Simplex>: u, v, w axis vertices, origin
+
+    def __init__(self, order, ctrl_idx, xyz, field=None, fixed=False):
+        self.order = int(order)
+        self.ctrl_idx = np.ascontiguousarray(ctrl_idx, dtype=np.int32)
+        self.xyz = np.ascontiguousarray(xyz, dtype=np.float32).reshape(-1, 3)
+        self.field = None if field is None else np.ascontiguousarray(field, dtype=np.float32)
+        nd = (self.order + 1) * (self.order + 2) * (self.order + 3) // 6
+        self.n_elem = self.ctrl_idx.size // nd
+        fptr = None if self.field is None else _p(self.field)
+        self.h = lib().ref_tet_create(self.order, int(fixed), self.n_elem, _p(self.ctrl_idx),
+                                      self.xyz.shape[0], _p(self.xyz), _p(self.ctrl_idx),
+                                      0 if self.field is None else self.field.size, fptr)
+        if not self.h:
+            raise RuntimeError(lib().ref_last_error().decode())
+
+
+def eval_tet_scalar(p, vals, refs, fixed=False):
+    """The reference's Element<3,1,Simplex,P>::eval_d of one scalar element."""
+    vals = np.ascontiguousarray(vals, np.float32)
+    refs = np.ascontiguousarray(refs, np.float32).reshape(-1, 3)
+    n = refs.shape[0]
+    v = np.zeros(n, np.float32)
+    d = np.zeros((n, 3), np.float32)
+    if lib().ref_eval_tet_scalar(p, int(fixed), _p(vals), n, _p(refs), _p(v), _p(d)) != 0:
+        raise RuntimeError(lib().ref_last_error().decode())
+    return v, d
 
 
 def morton(aabbs6):

@@ -1,0 +1,252 @@
+"""Tet (simplex) elements on the GPU, through the C-ABI, against the oracle.
+
+  - sub-boxes (drb_elem_subboxes / drb_lbvh_build on a DRB_SHAPE_SIMPLEX
+    mesh) bit-exact against the restated construct_bvh with the
+    evaluators' dof layout at orders 1-3, and against the reference's own
+    BVH (oracle/_ref) at order 1, where both layouts coincide;
+  - point location (drb_locate, drb_locate_batched in both row modes)
+    against the restated DeviceMesh::locate for tets over the same BVH, and
+    against the reference's UnstructuredMesh<Tet> (general-order element
+    type) at orders 1-2; order 3 is not run on the reference, whose order-3
+    tet BVH build writes past its scratch array;
+  - field values at located points (drb_field_eval) against the reference's
+    Element<3,1,Simplex,General>::eval_d, and the forward map of located
+    points (drb_map_points) back onto the queries.
+Tolerances: cells identical on >= 99.9 % of queries (the rest must be valid
+answers of the other side: the query maps into that element within 1e-4);
+reference coordinates within 1e-4 of the FP32 oracle and 1e-3 of the
+reference; field values within 1e-4.
+"""
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+
+ORDERS = [1, 2, 3]
+
+
+def _mesh(p, n=6):
+    from devil_ray_b200 import meshgen
+    return meshgen.tet_warped_mesh(n, p, 0.05, jitter=0.01, seed=3 + p)
+
+
+def _gpu(m, cuda):
+    from devil_ray_b200 import _lib as L
+    from devil_ray_b200 import api
+    return api.UnstructuredMesh(m.ctrl_idx, m.xyz, m.order, device=cuda, shape=L.SHAPE_SIMPLEX)
+
+
+def _bvh_np(b):
+    return {"inner": b.inner_nodes.cpu().numpy(), "leaf_nodes": b.leaf_nodes.cpu().numpy(),
+            "aabb_ids": b.aabb_ids.cpu().numpy(), "ref_boxes": b.ref_boxes.cpu().numpy()}
+
+
+def _maps_back(g, cell, ref, pts, tol=1e-4):
+    """The forward map X_cell(ref) of each located query lands on it."""
+    import torch
+    from devil_ray_b200.learned import map_points
+    sel = cell >= 0
+    X = map_points(g, torch.as_tensor(cell[sel], device=g.device),
+                   torch.as_tensor(ref[sel], device=g.device)).cpu().numpy()
+    return np.abs(X - pts[sel]).max(axis=1) < tol
+
+
+@pytest.mark.parametrize("p", ORDERS)
+def test_tet_subboxes_bit_exact(cuda, p):
+    import torch
+    from devil_ray_b200 import api
+    from oracle import restate
+    from tests.bvh_util import subbox_aabbs
+    m = _mesh(p)
+    g = _gpu(m, cuda)
+    aabbs, prim, refb, bounds = api.elem_subboxes(g)
+    b = g.build_bvh()
+    torch.cuda.synchronize()
+    a0, r0 = restate.tet_subboxes(p, m.ctrl_idx, m.xyz)
+    assert np.array_equal(aabbs.cpu().numpy().view(np.int32), a0.view(np.int32))
+    assert np.array_equal(refb.cpu().numpy().view(np.int32), r0.view(np.int32))
+    assert np.array_equal(prim.cpu().numpy(), np.repeat(np.arange(m.n_elem, dtype=np.int32), 33))
+    lo, hi = a0[:, 0::2].min(0), a0[:, 1::2].max(0)
+    assert np.array_equal(bounds.cpu().numpy(), np.stack([lo, hi], 1).reshape(-1))
+    # the built tree holds exactly these boxes, under their sub-box ids
+    bn = _bvh_np(b)
+    assert np.array_equal(subbox_aabbs(bn["inner"], bn["aabb_ids"]).view(np.int32), a0.view(np.int32))
+    assert np.array_equal(bn["ref_boxes"].view(np.int32), r0.view(np.int32))
+
+
+def test_tet_order1_bvh_matches_reference(cuda, ref):
+    import torch
+    from tests.bvh_util import subbox_aabbs
+    m = _mesh(1)
+    g = _gpu(m, cuda)
+    b = g.build_bvh(keep_codes=True)
+    torch.cuda.synchronize()
+    rb = ref.RefTetMesh(1, m.ctrl_idx, m.xyz).bvh()
+    bn = _bvh_np(b)
+    ra = subbox_aabbs(rb["inner"], rb["aabb_ids"])
+    assert np.array_equal(subbox_aabbs(bn["inner"], bn["aabb_ids"]).view(np.int32), ra.view(np.int32))
+    assert np.array_equal(bn["ref_boxes"].view(np.int32), rb["ref_boxes"].view(np.int32))
+    assert np.array_equal(b.bounds, rb["bounds"])
+    codes, _ = ref.morton(ra)
+    assert np.array_equal(np.sort(codes), b.sorted_codes.cpu().numpy().view(np.uint32))
+
+
+@pytest.mark.parametrize("p", ORDERS)
+@pytest.mark.parametrize("guess", ["zero", "elem_center", "subref_center"])
+def test_tet_locate_matches_restated_oracle(cuda, p, guess):
+    import torch
+    from devil_ray_b200 import _lib as L
+    from devil_ray_b200 import meshgen
+    from oracle import restate
+    mode = {"zero": L.GUESS_ZERO, "elem_center": L.GUESS_ELEM_CENTER,
+            "subref_center": L.GUESS_SUBREF_CENTER}[guess]
+    m = _mesh(p)
+    g = _gpu(m, cuda)
+    pts = meshgen.uniform_queries(40000, 17 + p)
+    cell, rp = g.locate(pts, tol=1e-4, max_steps=20, guess_mode=mode)
+    torch.cuda.synchronize()
+    cell, rp = cell.cpu().numpy(), rp.cpu().numpy()
+    oc, orf, _, _ = restate.locate_tet(p, m.ctrl_idx, m.xyz, _bvh_np(g.get_bvh()), pts, tol=1e-4,
+                                       max_steps=20, guess_mode=mode, local_frame=True)
+    same = cell == oc
+    assert same.mean() > 0.999, f"{(~same).sum()} cell mismatches"
+    both = same & (cell >= 0)
+    assert np.abs(rp[both] - orf[both]).max() < 1e-4
+    assert np.all(rp[cell < 0] == -1.0)
+    assert 0.85 < (cell >= 0).mean() < 0.95
+    assert _maps_back(g, cell, rp, pts).all()
+
+
+@pytest.mark.parametrize("p", [1, 2])
+def test_tet_locate_matches_reference(cuda, ref, p):
+    import torch
+    from devil_ray_b200 import _lib as L
+    from devil_ray_b200 import meshgen
+    m = _mesh(p)
+    g = _gpu(m, cuda)
+    pts = meshgen.uniform_queries(40000, 29 + p)
+    cell, rp = g.locate(pts, tol=1e-4, max_steps=20, guess_mode=L.GUESS_ZERO)
+    torch.cuda.synchronize()
+    cell, rp = cell.cpu().numpy(), rp.cpu().numpy()
+    rc, rr = ref.RefTetMesh(p, m.ctrl_idx, m.xyz).locate(pts)
+    same = cell == rc
+    assert same.mean() > 0.999, f"{(~same).sum()} cell mismatches"
+    both = same & (cell >= 0)
+    assert np.abs(rp[both] - rr[both]).max() < 1e-3
+    # where the answers differ (order 2: the reference's boxes come from its
+    # misindexed split, so candidates come in another order) ours is valid
+    diff = ~same & (cell >= 0)
+    if diff.any():
+        assert _maps_back(g, np.where(diff, cell, -1), rp, pts).all()
+    assert (cell >= 0).sum() >= (rc >= 0).sum()
+
+
+@pytest.mark.parametrize("p", ORDERS)
+@pytest.mark.parametrize("row_mode", [0, 1])
+def test_tet_batched_identical_to_plain(cuda, p, row_mode):
+    import torch
+    from devil_ray_b200 import _lib as L
+    from devil_ray_b200 import api, meshgen
+    m = _mesh(p)
+    g = _gpu(m, cuda)
+    pts = meshgen.uniform_queries(60000, 41 + p)
+    cell0, ref0 = g.locate(pts, tol=1e-5, max_steps=20, guess_mode=L.GUESS_ELEM_CENTER)
+    cfg = L.DrbLocateConfig()
+    cfg.block, cfg.blocks_per_sm, cfg.chunk, cfg.sort_queries, cfg.reg_elements = 128, 0, 64, 1, row_mode
+    bl = api.BatchedLocator(g, tol=1e-5, max_steps=20, config=cfg)
+    cell1, ref1 = bl.locate(pts)
+    torch.cuda.synchronize()
+    assert torch.equal(cell0, cell1)
+    assert torch.equal(ref0.view(torch.int32), ref1.view(torch.int32))
+
+
+@pytest.mark.parametrize("p", ORDERS)
+def test_tet_point_location_field_values(cuda, ref, p):
+    import torch
+    from devil_ray_b200 import _lib as L
+    from devil_ray_b200 import meshgen
+    from devil_ray_b200.render import PointLocation, UnstructuredField
+    from oracle import restate
+    m = _mesh(p, n=4)
+    g = _gpu(m, cuda)
+    f = UnstructuredField(m.ctrl_idx, m.field, p, device=cuda, shape=L.SHAPE_SIMPLEX)
+    pts = meshgen.uniform_queries(8000, 53 + p)
+    q = PointLocation()
+    q.add_var("f")
+    q.empty_val(-7.0)
+    vals = q.execute(g, {"f": f}, pts)["f"]
+    from devil_ray_b200.api import BatchedLocator
+    cell, rp = BatchedLocator(g, 1e-4, 20, L.GUESS_ELEM_CENTER).locate(pts)
+    torch.cuda.synchronize()
+    vals, cell, rp = vals.cpu().numpy(), cell.cpu().numpy(), rp.cpu().numpy()
+    assert np.all(vals[cell < 0] == np.float32(-7.0))
+    nd = meshgen.tet_dofs(p)
+    conn = m.ctrl_idx.reshape(-1, nd)
+    for e in np.unique(cell[cell >= 0])[:80]:
+        sel = cell == e
+        fv = m.field[conn[e]]
+        X, _ = restate.tet_eval_d(p, fv.astype(np.float64), rp[sel].astype(np.float64))
+        assert np.abs(vals[sel] - X[:, 0]).max() < 1e-4
+        if p < 3:
+            rv, _ = ref.eval_tet_scalar(p, fv, rp[sel])
+            assert np.abs(vals[sel] - rv).max() < 1e-4
+
+
+def test_tet_unsupported_entry_points_fail_loudly(cuda):
+    import ctypes as C
+    from devil_ray_b200 import _lib as L
+    m = _mesh(1, n=2)
+    g = _gpu(m, cuda)
+    d = g.desc()
+    nb = C.c_void_p(g.packed.data_ptr())
+    st = L.lib().drb_mesh_face_neighbors(C.byref(d), nb, None)
+    assert st != 0
+    assert "hex" in L.lib().drb_last_error().decode()
+
+
+@pytest.mark.parametrize("p", [1, 2, 3])
+def test_cpp_tet_mesh_interface(cuda, ref, tmp_path, p):
+    """UnstructuredMesh<Tet*> / UnstructuredField<TetScalar*> through the C++
+    host interface (t_dray_b200_tet): Mesh::locate against the restated
+    oracle (and the reference at orders 1-2), PointLocation values against
+    the element evaluation."""
+    import subprocess
+    from pathlib import Path
+    from devil_ray_b200 import meshgen
+    from oracle import restate
+    exe = Path(__file__).resolve().parent.parent / "devil_ray_b200" / "cpp" / "tests" / "t_dray_b200_tet"
+    if not exe.exists():
+        pytest.fail("C++ test program missing: build with make -C devil_ray_b200/cpp")
+    m = _mesh(p, n=5)
+    pts = meshgen.uniform_queries(20000, 61 + p)
+    with open(tmp_path / "mesh.bin", "wb") as f:
+        np.array([p, m.n_elem, m.n_ctrl], np.int32).tofile(f)
+        np.ascontiguousarray(m.ctrl_idx, np.int32).tofile(f)
+        np.ascontiguousarray(m.xyz, np.float32).tofile(f)
+        np.ascontiguousarray(m.field, np.float32).tofile(f)
+    with open(tmp_path / "points.bin", "wb") as f:
+        np.array([pts.shape[0]], np.int32).tofile(f)
+        pts.tofile(f)
+    r = subprocess.run([str(exe), str(tmp_path)], capture_output=True, text=True, timeout=300)
+    assert r.returncode == 0, r.stdout + r.stderr
+    n = pts.shape[0]
+    raw = np.fromfile(tmp_path / "locate.bin", np.uint8)
+    cell = raw[: 4 * n].view(np.int32)
+    refp = raw[4 * n:].view(np.float32).reshape(n, 3)
+    g = _gpu(m, cuda)
+    oc, orf, _, _ = restate.locate_tet(p, m.ctrl_idx, m.xyz, _bvh_np(g.get_bvh()), pts, tol=1e-4,
+                                       max_steps=20, guess_mode=0, local_frame=True)
+    same = cell == oc
+    assert same.mean() > 0.999
+    assert np.abs(refp[same & (cell >= 0)] - orf[same & (cell >= 0)]).max() < 1e-4
+    if p < 3:
+        rc, _ = ref.RefTetMesh(p, m.ctrl_idx, m.xyz).locate(pts)
+        assert (cell == rc).mean() > 0.999
+    vals = np.fromfile(tmp_path / "pointloc.bin", np.float32)
+    assert np.all(vals[cell < 0] == np.float32(-1e30))
+    nd = meshgen.tet_dofs(p)
+    conn = m.ctrl_idx.reshape(-1, nd)
+    for e in np.unique(cell[cell >= 0])[:50]:
+        sel = cell == e
+        X, _ = restate.tet_eval_d(p, m.field[conn[e]].astype(np.float64), refp[sel].astype(np.float64))
+        assert np.abs(vals[sel] - X[:, 0]).max() < 1e-4
