@@ -57,6 +57,7 @@ def parse():
                     help="reference CPU sample size (0 = sized for ~15 s)")
     ap.add_argument("--no-learned", action="store_true", help="skip the learned-guess path")
     ap.add_argument("--no-volume", action="store_true", help="skip the volume workload")
+    ap.add_argument("--no-tet", action="store_true", help="skip the tet locate workload")
     ap.add_argument("--train-samples", type=int, default=1 << 22)
     ap.add_argument("--orbits", type=int, default=16)
     ap.add_argument("--profile-volume", type=int, default=0, metavar="N",
@@ -323,6 +324,65 @@ def surface_c1(dev, with_cpu):
             out["cpu_reference"] = {"value": W * W / cpu_s, "unit": "rays/s", "seconds": cpu_s,
                                     "cores": refpy.num_threads(), "kind": "reference",
                                     "sample": "the whole 1024^2 frame"}
+    return out
+
+
+def tet_locate(dev, args, with_cpu):
+    """Tet point location: 32^3 cubes x 6 = 196,608 order-2 tets (warp 0.05,
+    jitter 0.01), 16M uniform queries (8 % outside), tol 1e-5, 20 steps,
+    through the tuned persistent kernel (drb_locate_batched on a
+    DRB_SHAPE_SIMPLEX mesh); the reference's OpenMP UnstructuredMesh<Tet>
+    ::locate (general-order element type, its fixed tol 1e-4) on the host
+    cores over the same queries."""
+    import torch
+    from devil_ray_b200 import _lib as L
+    from devil_ray_b200 import api, meshgen
+    m = meshgen.tet_warped_mesh(32, 2, 0.05, jitter=0.01, seed=9)
+    mesh = api.UnstructuredMesh(m.ctrl_idx, m.xyz, m.order, device=dev, shape=L.SHAPE_SIMPLEX)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    torch.cuda.synchronize()
+    e0.record()
+    mesh.get_bvh()
+    e1.record()
+    torch.cuda.synchronize()
+    build_ms = e0.elapsed_time(e1)
+    n = min(args.queries, N_QUERIES)
+    q = meshgen.uniform_queries(n, 77)
+    qd = torch.as_tensor(q, device=dev)
+    loc = api.BatchedLocator(mesh, tol=1e-5, max_steps=20, guess_mode=L.GUESS_ELEM_CENTER)
+    cfg, _ = loc.tune(qd[: min(n, 1 << 20)])
+    cell, ref = loc.locate(qd)
+    for _ in range(max(args.warmup, 3)):
+        loc.locate(qd, out=(cell, ref))
+    reps = 5
+    torch.cuda.synchronize()
+    e0.record()
+    for _ in range(reps):
+        loc.locate(qd, out=(cell, ref))
+    e1.record()
+    torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1) / reps
+    located = int((cell >= 0).sum())
+    out = {"workload": "tet_32: 32^3 cubes x 6 = 196,608 tets order 2, warp 0.05, jitter 0.01, "
+                       f"{n} uniform queries (8% outside), tol 1e-5, 20 steps",
+           "metric": "located pts/s (Newton-resolved, tol 1e-5)", "unit": "points/s",
+           "value": located / (ms * 1e-3), "ms_per_step": ms, "located_fraction": located / n,
+           "elements": m.n_elem, "bvh_build_ms": build_ms, "launch_config": cfg.as_dict(),
+           "l2": "inputs larger than L2 (201 MB queries)"}
+    if with_cpu:
+        from oracle import refpy
+        if refpy.available():
+            s = n
+            r = refpy.RefTetMesh(m.order, m.ctrl_idx, m.xyz)
+            r.locate(q[:1024])  # builds the BVH
+            t0 = time.perf_counter()
+            rc, _ = r.locate(q[:s])
+            cpu_s = time.perf_counter() - t0
+            out["cpu_reference"] = {"value": int((rc >= 0).sum()) / cpu_s, "unit": "points/s",
+                                    "seconds": cpu_s, "cores": refpy.num_threads(),
+                                    "kind": "reference",
+                                    "sample": f"all {s} queries, tol 1e-4 (fixed in the "
+                                              "reference)"}
     return out
 
 
@@ -758,6 +818,13 @@ def main():
         except Exception as exc:
             surf_c1 = {"error": repr(exc)}
 
+    tet = None
+    if not args.no_tet:
+        try:
+            tet = tet_locate(dev, args, rank == 0 and world == 1 and not args.no_cpu_baseline)
+        except Exception as exc:
+            tet = {"error": repr(exc)}
+
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         try:
@@ -810,6 +877,7 @@ def main():
             "volume": vol,
             "volume_c0": vol_c0,
             "surface": surf_c1,
+            "tet": tet,
             "bvh_build_ms": bvh_build_ms, "tune_ms": tune_ms,
             "cpu_baseline": cpu,
         }

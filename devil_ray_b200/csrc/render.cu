@@ -309,20 +309,22 @@ DRB_D float4 colormap (const VolumeParams &vp, float s)
   return __ldg (vp.tf + idx);
 }
 
-template <int P>
+template <int P, int S = kTensor>
 DRB_D void field_eval_d (const VolumeParams &vp, int el, const float (&r)[3], float &f, float (&g)[3])
 {
-  constexpr int ND = (P + 1) * (P + 1) * (P + 1);
+  constexpr int ND = shape_dofs<S, P> ();
   float X[1], Ju[1], Jv[1], Jw[1];
   if (vp.field_packed)
   {
     FieldCP<P> cp{ vp.field_packed + (size_t)el * vp.fstride };
-    hex_eval_d<P, 1> (cp, r[0], r[1], r[2], X, Ju, Jv, Jw);
+    if (S == kSimplex) tet_eval_d<P, 1> (cp, r[0], r[1], r[2], X, Ju, Jv, Jw);
+    else hex_eval_d<P, 1> (cp, r[0], r[1], r[2], X, Ju, Jv, Jw);
   }
   else
   {
     FieldIndCP<P> cp{ vp.field_idx + (size_t)el * ND, vp.field_vals };
-    hex_eval_d<P, 1> (cp, r[0], r[1], r[2], X, Ju, Jv, Jw);
+    if (S == kSimplex) tet_eval_d<P, 1> (cp, r[0], r[1], r[2], X, Ju, Jv, Jw);
+    else hex_eval_d<P, 1> (cp, r[0], r[1], r[2], X, Ju, Jv, Jw);
   }
   f = X[0];
   g[0] = Ju[0];
@@ -334,12 +336,12 @@ DRB_D void field_eval_d (const VolumeParams &vp, int el, const float (&r)[3], fl
 // geometry Jacobian is not evaluated again: lu is the factorised Jacobian of
 // the located sample's last Newton step, taken within tol of ref, and the
 // world position is the sample point itself (the solve's target).
-template <int P>
+template <int P, int S = kTensor>
 DRB_D float4 shade_sample (const VolumeParams &vp, int el, const float (&r)[3], const Ray &ray,
                            const LU3 &lu, const float (&wpos)[3])
 {
   float f, gref[3];
-  field_eval_d<P> (vp, el, r, f, gref);
+  field_eval_d<P, S> (vp, el, r, f, gref);
   const float4 c = colormap (vp, f);
   if (!vp.use_lighting) return c;
   float4 acc = make_float4 (0.f, 0.f, 0.f, 0.f);
@@ -459,8 +461,9 @@ DRB_D int step_across (const VolumeParams &vp, int el, int f, float (&x)[3])
 // or in plain mode, the BVH candidates in the reference's order; the same
 // acceptance rule throughout.  All candidates go through one Newton call
 // site, which keeps the kernel's code small.  On success lu holds the
-// located solve's Jacobian.
-template <int P, bool WIDE>
+// located solve's Jacobian.  Tets (S = kSimplex) have no face table: a
+// prediction outside the previous element goes straight to the BVH.
+template <int P, bool WIDE, int S = kTensor>
 DRB_D int locate_sample (const VolumeParams &vp, const float (&pt)[3], const float (&step)[3],
                          int prev_el, const float (&prev_ref)[3], LU3 &lu, float (&ref)[3],
                          int &iters, int &cands, int &nodes)
@@ -478,13 +481,13 @@ DRB_D int locate_sample (const VolumeParams &vp, const float (&pt)[3], const flo
     x[0] = prev_ref[0] + dr[0];
     x[1] = prev_ref[1] + dr[1];
     x[2] = prev_ref[2] + dr[2];
-    if (is_inside_ref (x, kCoherentMargin))
+    if (S == kSimplex ? is_inside_simplex (x, kCoherentMargin) : is_inside_ref (x, kCoherentMargin))
     {
       el = prev_el;
     }
     else
     {
-      el = step_across (vp, prev_el, exit_face (x), x);
+      el = S == kSimplex ? -1 : step_across (vp, prev_el, exit_face (x), x);
       crossed = true;
     }
   }
@@ -496,13 +499,13 @@ DRB_D int locate_sample (const VolumeParams &vp, const float (&pt)[3], const flo
       if (leaf < 0) return -1;
       el = __ldg (vp.lp.leaf_nodes + leaf);
       bool given;
-      candidate_guess (vp.lp, leaf, 0, false, x, given);
+      candidate_guess<S> (vp.lp, leaf, 0, false, x, given);
     }
     int steps = 0;
     ++cands;
     // order 2 and 3 rows are read through L1: keeping 81+ values in
     // registers would halve the resident warps of this kernel
-    const bool found = solve_in_element<P, (P == 1)> (vp.lp, el, pt, x, steps, lu);
+    const bool found = solve_in_element<P, (P == 1), S> (vp.lp, el, pt, x, steps, lu);
     iters += steps;
     if (found)
     {
@@ -511,7 +514,7 @@ DRB_D int locate_sample (const VolumeParams &vp, const float (&pt)[3], const flo
       ref[2] = x[2];
       return el;
     }
-    if (leaf < 0 && !crossed)
+    if (S == kTensor && leaf < 0 && !crossed)
     {
       // the previous element's solve ended outside it: step across
       crossed = true;
@@ -603,7 +606,7 @@ DRB_D void finish_ray (RayMarch &s, float4 *__restrict__ fb_color, float *__rest
 // 0.95; the ray ends after 5 segments, at far, or when alpha exceeds 0.95.
 // Partials go to slot 5 i + segment of ray i and the framebuffer pixel gets
 // their front-to-back composite, so the processing order changes nothing.
-template <int P, bool WIDE>
+template <int P, bool WIDE, int S>
 __global__ void __launch_bounds__ (128)
 volume_kernel (VolumeParams vp, const Ray *__restrict__ rays, int n_rays, int *__restrict__ queue,
                VolumePartial *__restrict__ partials, float4 *__restrict__ fb_color,
@@ -682,8 +685,8 @@ volume_kernel (VolumeParams vp, const Ray *__restrict__ rays, int n_rays, int *_
                           s.ray.orig.y + s.distance * s.ray.dir.y,
                           s.ray.orig.z + s.distance * s.ray.dir.z };
     float ref[3];
-    const int el = locate_sample<P, WIDE> (vp, pt, step, s.prev_el, s.prev_ref, lu, ref, s.iters,
-                                           s.cands, s.nodes);
+    const int el = locate_sample<P, WIDE, S> (vp, pt, step, s.prev_el, s.prev_ref, lu, ref, s.iters,
+                                              s.cands, s.nodes);
     bool done = false;
     if (el >= 0)
     {
@@ -694,7 +697,7 @@ volume_kernel (VolumeParams vp, const Ray *__restrict__ rays, int n_rays, int *_
         s.color = make_float4 (0.f, 0.f, 0.f, 0.f);
       }
       ++s.n_samples;
-      const float4 sc = shade_sample<P> (vp, el, ref, s.ray, lu, pt);
+      const float4 sc = shade_sample<P, S> (vp, el, ref, s.ray, lu, pt);
       blend (s.color, sc);
       s.prev_el = el;
       s.prev_ref[0] = ref[0];
@@ -820,31 +823,42 @@ __global__ void fb_background_kernel (float4 *c, int n, float4 bg)
   }
 }
 
-template <int P, bool WIDE>
+template <int P, bool WIDE, int S>
 int launch_volume_w (const VolumeParams &vp, const Ray *rays, int n, int *queue,
                      VolumePartial *partials, float4 *fb, float *depth, const drb_ray_stats &st,
                      cudaStream_t s)
 {
   int nb = 0;
-  cudaOccupancyMaxActiveBlocksPerMultiprocessor (&nb, volume_kernel<P, WIDE>, 128, 0);
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor (&nb, volume_kernel<P, WIDE, S>, 128, 0);
   if (nb < 1) nb = 1;
   long long blocks = (long long)nb * sm_count ();
   const long long need = ((long long)n + 127) / 128;
   if (blocks > need) blocks = need;
   if (blocks < 1) blocks = 1;
-  volume_kernel<P, WIDE><<<(unsigned)blocks, 128, 0, s>>> (vp, rays, n, queue, partials, fb, depth,
-                                                           st.samples, st.iters, st.candidates);
+  volume_kernel<P, WIDE, S><<<(unsigned)blocks, 128, 0, s>>> (vp, rays, n, queue, partials, fb, depth,
+                                                              st.samples, st.iters, st.candidates);
   return check_launch ("volume_kernel");
 }
 
 // full locates of the march walk the 4-wide tree when the BVH has one
-template <int P>
-int launch_volume (const VolumeParams &vp, const Ray *rays, int n, int *queue,
-                   VolumePartial *partials, float4 *fb, float *depth, const drb_ray_stats &st,
-                   cudaStream_t s)
+template <int P, int S>
+int launch_volume_s (const VolumeParams &vp, const Ray *rays, int n, int *queue,
+                     VolumePartial *partials, float4 *fb, float *depth, const drb_ray_stats &st,
+                     cudaStream_t s)
 {
-  if (vp.lp.wide) return launch_volume_w<P, true> (vp, rays, n, queue, partials, fb, depth, st, s);
-  return launch_volume_w<P, false> (vp, rays, n, queue, partials, fb, depth, st, s);
+  if (vp.lp.wide) return launch_volume_w<P, true, S> (vp, rays, n, queue, partials, fb, depth, st, s);
+  return launch_volume_w<P, false, S> (vp, rays, n, queue, partials, fb, depth, st, s);
+}
+
+int launch_volume (const drb_mesh *mesh, const VolumeParams &vp, const Ray *rays, int n,
+                   int *queue, VolumePartial *partials, float4 *fb, float *depth,
+                   const drb_ray_stats &st, cudaStream_t s)
+{
+#define DRB_LV(P, S) launch_volume_s<P, S> (vp, rays, n, queue, partials, fb, depth, st, s)
+  if (mesh->shape == DRB_SHAPE_SIMPLEX)
+    return mesh->order == 1 ? DRB_LV (1, kSimplex) : mesh->order == 2 ? DRB_LV (2, kSimplex) : DRB_LV (3, kSimplex);
+  return mesh->order == 1 ? DRB_LV (1, kTensor) : mesh->order == 2 ? DRB_LV (2, kTensor) : DRB_LV (3, kTensor);
+#undef DRB_LV
 }
 
 } // namespace drb
@@ -1049,9 +1063,11 @@ static int volume_common (const drb_mesh *mesh, const drb_mesh *field, const drb
   }
   if (mesh->dim != 3 || mesh->ncomp != 3 || field->dim != 3 || field->ncomp != 1 ||
       mesh->order != field->order || mesh->n_elem != field->n_elem || mesh->order < 1 ||
-      mesh->order > 3 || mesh->shape != DRB_SHAPE_TENSOR || field->shape != DRB_SHAPE_TENSOR)
+      mesh->order > 3 || mesh->shape != field->shape ||
+      (mesh->shape != DRB_SHAPE_TENSOR && mesh->shape != DRB_SHAPE_SIMPLEX))
   {
-    set_last_error ("volume: needs a hex mesh and a scalar hex field of the same order 1..3");
+    set_last_error ("volume: needs a hex (or tet) mesh and a scalar field of the same shape and "
+                    "order 1..3");
     return DRB_ERR_UNSUPPORTED;
   }
   if (o->samples < 1 || !(o->tol > 0.f) || o->max_steps < 0)
@@ -1073,7 +1089,7 @@ static int volume_common (const drb_mesh *mesh, const drb_mesh *field, const drb
   lp.packed = mesh->packed;
   lp.ctrl_idx = mesh->ctrl_idx;
   lp.xyz = mesh->values;
-  const int nd = (mesh->order + 1) * (mesh->order + 1) * (mesh->order + 1);
+  const int nd = mesh_nd (mesh);
   lp.stride = packed_stride (nd, 3);
   lp.tol = no.tol;
   lp.max_steps = no.max_steps;
@@ -1083,7 +1099,7 @@ static int volume_common (const drb_mesh *mesh, const drb_mesh *field, const drb
   vp.field_idx = field->ctrl_idx;
   vp.field_vals = field->values;
   vp.fstride = packed_stride (nd, 1);
-  vp.nbr = mesh->face_neighbors;
+  vp.nbr = mesh->shape == DRB_SHAPE_TENSOR ? mesh->face_neighbors : nullptr;
   vp.tf = (const float4 *)tf;
   vp.tf_size = tf_size;
   // DeviceColorMap: range of the field's control values, rcp_safe(length)
@@ -1147,9 +1163,7 @@ extern "C" int drb_volume_integrate (const drb_mesh *mesh, const drb_mesh *field
   if ((st = check_launch ("init_partials_kernel"))) return st;
   cudaMemsetAsync (queue, 0, sizeof (int), s);
   const Ray *rays = (const Ray *)active_rays;
-  if (mesh->order == 1) st = launch_volume<1> (vp, rays, n_rays, queue, raw, nullptr, nullptr, stats, s);
-  else if (mesh->order == 2) st = launch_volume<2> (vp, rays, n_rays, queue, raw, nullptr, nullptr, stats, s);
-  else st = launch_volume<3> (vp, rays, n_rays, queue, raw, nullptr, nullptr, stats, s);
+  st = launch_volume (mesh, vp, rays, n_rays, queue, raw, nullptr, nullptr, stats, s);
   if (st) return st;
   // compact_partials (volume.cpp:42-67)
   partial_flags_kernel<<<div_up (np, 256), 256, 0, s>>> (raw, (int)np, flags);
@@ -1189,9 +1203,7 @@ extern "C" int drb_volume_render (const drb_mesh *mesh, const drb_mesh *field, c
   cudaMemsetAsync (queue, 0, sizeof (int), s);
   const Ray *rays = (const Ray *)active_rays;
   float4 *fb = (float4 *)fb_rgba;
-  if (mesh->order == 1) st = launch_volume<1> (vp, rays, n_rays, queue, nullptr, fb, fb_depth, stats, s);
-  else if (mesh->order == 2) st = launch_volume<2> (vp, rays, n_rays, queue, nullptr, fb, fb_depth, stats, s);
-  else st = launch_volume<3> (vp, rays, n_rays, queue, nullptr, fb, fb_depth, stats, s);
+  st = launch_volume (mesh, vp, rays, n_rays, queue, nullptr, fb, fb_depth, stats, s);
   return st;
 }
 

@@ -63,9 +63,10 @@ enum drb_shape
  * shape (drb_shape) selects tensor or simplex elements.  Tet meshes are
  * accepted by drb_pack_elements, drb_elem_subboxes, drb_lbvh_build,
  * drb_bvh_widen, drb_locate, drb_locate_batched (and its ordered, host and
- * allocation-free forms, and drb_locate_tune), drb_field_eval and
- * drb_map_points; the other entry points return DRB_ERR_UNSUPPORTED for
- * them. */
+ * allocation-free forms, and drb_locate_tune), drb_field_eval,
+ * drb_map_points and the volume renderer (drb_volume_integrate,
+ * drb_volume_render, with a tet scalar field); the other entry points return
+ * DRB_ERR_UNSUPPORTED for them. */
 typedef struct drb_mesh
 {
   int dim;               /* 3 hex or tet, 2 quad */
@@ -363,7 +364,10 @@ int drb_color_table_sample (int n_rgb, const float *rgb_pts, int n_alpha, const 
  * rays: partials compacted in ray then depth order (device
  * dray::VolumePartial[5*n_rays] capacity); *n_partials returned after a
  * stream synchronise.  tf: device float4[tf_size] (opacity corrected);
- * range2: host float[2] scalar range; lights: device PointLight[n_lights]. */
+ * range2: host float[2] scalar range; lights: device PointLight[n_lights].
+ * Hex or tet (dispatch_3d, dispatcher.hpp:209-219) mesh and field of one
+ * shape and order; tet samples are located through the BVH whenever the
+ * previous sample's element does not hold them (no face table). */
 int drb_volume_integrate (const drb_mesh *mesh, const drb_mesh *field, const drb_bvh *bvh,
                           const void *active_rays, int n_rays, const drb_volume_opts *opts,
                           const float *tf, int tf_size, const float *range2, const void *lights,
