@@ -31,7 +31,8 @@ class DrbMesh(C.Structure):
     _fields_ = [("dim", C.c_int), ("order", C.c_int), ("ncomp", C.c_int),
                 ("n_elem", C.c_int), ("n_ctrl", C.c_int),
                 ("ctrl_idx", C.c_void_p), ("values", C.c_void_p), ("packed", C.c_void_p),
-                ("face_neighbors", C.c_void_p), ("shape", C.c_int)]
+                ("face_neighbors", C.c_void_p), ("shape", C.c_int),
+                ("hull_planes", C.c_void_p)]
 
 
 class DrbBvh(C.Structure):
@@ -140,6 +141,7 @@ _SIGS = {
     "drb_elem_dofs": (C.c_int, [C.c_int, C.c_int, C.c_int]),
     "drb_packed_stride_shape": (C.c_int, [C.c_int, C.c_int, C.c_int, C.c_int]),
     "drb_ref_box_floats": (C.c_int, [C.c_int, C.c_int]),
+    "drb_tet_hull_planes": (C.c_int, [C.POINTER(DrbMesh), C.c_void_p, C.c_void_p]),
     "drb_pack_elements": (C.c_int, [C.POINTER(DrbMesh), C.c_void_p, C.c_void_p]),
     "drb_bvh_sizes": (C.c_int, [C.c_int, C.c_int, C.POINTER(C.c_int), C.POINTER(C.c_int)]),
     "drb_elem_subboxes": (C.c_int, [C.POINTER(DrbMesh), C.c_void_p, C.c_void_p, C.c_void_p,

@@ -121,6 +121,7 @@ class UnstructuredMesh:
         self.device = torch.device(device)
         self.packed = None
         self._neighbors = None
+        self._hull = None
         self._bvh = None
         if pack:
             self.pack()
@@ -143,6 +144,8 @@ class UnstructuredMesh:
         m.packed = self.packed.data_ptr() if (packed and self.packed is not None) else None
         nb = getattr(self, "_neighbors", None)
         m.face_neighbors = nb.data_ptr() if nb is not None else None
+        hp = getattr(self, "_hull", None)
+        m.hull_planes = hp.data_ptr() if hp is not None else None
         return m
 
     def face_neighbors(self, stream=None):
@@ -156,6 +159,17 @@ class UnstructuredMesh:
                     "drb_mesh_face_neighbors")
             self._neighbors = nb
         return self._neighbors
+
+    def hull_planes(self, stream=None):
+        """Tets: the bounding planes of every element (drb_tet_hull_planes),
+        built once; the batched locate filters its candidates with them."""
+        if self._hull is None and self.shape == L.SHAPE_SIMPLEX:
+            hp = torch.empty((max(self.n_elem, 1), 20), dtype=torch.float32, device=self.device)
+            d = self.desc()
+            L.check(L.lib().drb_tet_hull_planes(C.byref(d), _ptr(hp), _stream(stream)),
+                    "drb_tet_hull_planes")
+            self._hull = hp
+        return self._hull
 
     def pack(self, stream=None):
         stride = L.lib().drb_packed_stride_shape(self.shape, self.dim, self.order, 3)
@@ -173,6 +187,8 @@ class UnstructuredMesh:
             self._bvh = self.build_bvh(stream, keep_codes)
             if self.dim == 3:
                 self._bvh.widen(stream)
+            if self.shape == L.SHAPE_SIMPLEX:
+                self.hull_planes(stream)
         return self._bvh
 
     def build_bvh(self, stream=None, keep_codes: bool = False) -> BVH:

@@ -59,7 +59,7 @@ struct DeviceGeometry
   DevBuf<float> packed;
   bool has_bvh = false;
   drb_bvh bvh{};
-  DevBuf<float> inner, refb, wide;
+  DevBuf<float> inner, refb, wide, hull;
   DevBuf<int32> leaf, ids, nbr;
 };
 
@@ -124,6 +124,13 @@ const drb_bvh *ElementMesh::device_bvh ()
       drb_check (drb_bvh_widen (&g.bvh, nullptr, 0, nullptr), "drb_bvh_widen");
       g.wide.alloc ((size_t)32 * g.bvh.n_wide);
       drb_check (drb_bvh_widen (&g.bvh, g.wide.p, g.bvh.n_wide, nullptr), "drb_bvh_widen");
+    }
+    if (m_etype == Simplex)
+    {
+      // bounding planes: the batched locate's candidate filter for tets
+      g.hull.alloc ((size_t)20 * std::max (cells (), 1));
+      drb_check (drb_tet_hull_planes (&g.mesh, g.hull.p, nullptr), "drb_tet_hull_planes");
+      g.mesh.hull_planes = g.hull.p;
     }
     if (m_dim == 3 && m_etype == Tensor)
     {

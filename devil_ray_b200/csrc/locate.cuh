@@ -135,7 +135,26 @@ struct LocateParams
   int max_steps;
   int guess_mode;
   const float *guess;
+  const float4 *hull = nullptr; // tet hull planes (drb_tet_hull_planes) or NULL
 };
+
+// Candidate filter of the batched locate (drb_tet_hull_planes): true when
+// the query lies more than kHullMargin * tol * D outside one of the tet's
+// hull planes, where no Newton solve can be accepted.
+constexpr float kHullMargin = 128.f;
+DRB_D bool hull_rejects (const LocateParams &lp, int el, const float (&pt)[3])
+{
+  const float4 *h = lp.hull + 5 * (size_t)el;
+  const float margin = kHullMargin * lp.tol * __ldg (h + 4).x;
+  bool out = false;
+#pragma unroll
+  for (int f = 0; f < 4; ++f)
+  {
+    const float4 q = __ldg (h + f);
+    out |= q.x * pt[0] + q.y * pt[1] + q.z * pt[2] - q.w > margin;
+  }
+  return out;
+}
 
 // Element shapes of the locate templates (drb_shape).
 constexpr int kTensor = DRB_SHAPE_TENSOR;

@@ -237,7 +237,9 @@ __global__ void locate_persistent_kernel (LocateParams lp, const float *__restri
       if (leaf >= 0)
       {
         ++cands;
-        const bool found = (MODE == kRowsShared)
+        const bool found = (S == kSimplex && lp.hull && hull_rejects (lp, el, pt))
+                           ? false
+                           : (MODE == kRowsShared)
                            ? solve_candidate_smem<P> (lp, leaf, my_row, qi, first, pt, x, iters)
                            : solve_candidate<P, MODE == kRowsReg, S> (lp, leaf, el, qi, first, pt, x, iters);
         first = false;
@@ -376,6 +378,7 @@ LocateParams make_params (const drb_mesh *mesh, const drb_bvh *bvh, const drb_ne
   lp.max_steps = opts->max_steps;
   lp.guess_mode = opts->guess_mode;
   lp.guess = opts->guess;
+  lp.hull = mesh->shape == DRB_SHAPE_SIMPLEX ? (const float4 *)mesh->hull_planes : nullptr;
   return lp;
 }
 

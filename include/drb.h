@@ -81,7 +81,20 @@ typedef struct drb_mesh
   const int *face_neighbors; /* optional device int32[6 * n_elem] of a hex geometry
                             mesh (drb_mesh_face_neighbors), or NULL */
   int shape;             /* drb_shape; 0 (tensor) when zero-initialised */
+  const float *hull_planes; /* optional device float[20 * n_elem] of a tet geometry
+                            mesh (drb_tet_hull_planes), or NULL */
 } drb_mesh;
+
+/* Bounding planes of each tet of a geometry mesh (no reference counterpart):
+ * four outward unit normals n_f with offsets d_f such that n_f . x <= d_f on
+ * the whole element (the vertex tet's face planes pushed out to the farthest
+ * control point; Bernstein elements lie in their control points' hull), then
+ * (D, 0, 0, 0) with D the diagonal of the control points' box; 20 floats per
+ * tet.  With drb_mesh.hull_planes set, the batched locate skips the Newton
+ * solve of a candidate tet whose planes put the query more than 128 tol D
+ * outside: such a solve cannot be accepted, so the results are those of the
+ * unfiltered solve. */
+int drb_tet_hull_planes (const drb_mesh *mesh, float *planes, void *stream);
 
 /* Face neighbours of a hex mesh (no reference counterpart; faces are
  * matched by their four corner control points, as MeshBoundary matches

@@ -311,3 +311,35 @@ def test_tet_volume_order3_coherent_equals_plain(cuda):
     d = np.abs(a - b)
     assert np.any(d > 1.0 / 255.0, axis=-1).mean() < 0.005
     assert (np.abs(a - a[0, 0]).max(-1) > 1e-3).mean() > 0.1
+
+
+@pytest.mark.parametrize("p", ORDERS)
+def test_tet_hull_filter_changes_nothing(cuda, p):
+    """The batched locate's hull-plane filter (drb_tet_hull_planes) only
+    skips solves that fail: results are bit-identical with and without it,
+    with far fewer Newton steps; every control point is behind its planes."""
+    import torch
+    from devil_ray_b200 import _lib as L
+    from devil_ray_b200 import api, meshgen
+    m = _mesh(p)
+    g = _gpu(m, cuda)
+    g.get_bvh()
+    hp = g.hull_planes().cpu().numpy().reshape(-1, 5, 4)
+    nd = meshgen.tet_dofs(p)
+    cps = m.xyz[m.ctrl_idx.reshape(-1, nd)].astype(np.float64)          # [n, nd, 3]
+    side = np.einsum("efk,eik->efi", hp[:, :4, :3].astype(np.float64), cps) - hp[:, :4, 3:4]
+    assert side.max() < 1e-6
+    assert np.all(np.abs(np.linalg.norm(hp[:, :4, :3], axis=-1) - 1.0) < 1e-5)
+    pts = meshgen.uniform_queries(60000, 71 + p)
+    bl = api.BatchedLocator(g, tol=1e-5, max_steps=20)
+    c1, r1, it1, ca1, _ = bl.locate(pts, stats=True)
+    saved, g._hull = g._hull, None
+    try:
+        c0, r0, it0, ca0, _ = bl.locate(pts, stats=True)
+    finally:
+        g._hull = saved
+    torch.cuda.synchronize()
+    assert torch.equal(c0, c1)
+    assert torch.equal(r0.view(torch.int32), r1.view(torch.int32))
+    assert torch.equal(ca0, ca1)
+    assert it1.sum().item() < 0.6 * it0.sum().item()
