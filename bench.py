@@ -692,6 +692,37 @@ def main():
                    "note": "Morton-ordered persistent kernel, sub-box-centre guess"}
     del it_s
 
+    # many small batches: 64K queries per call, eager calls vs one CUDA graph
+    # replay per batch (BatchedLocator.capture); same results either way
+    graph_small = None
+    try:
+        nb = 1 << 16
+        small = [pts[k * nb:(k + 1) * nb] for k in range(16)]
+        sc = torch.empty(nb, dtype=torch.int32, device=dev)
+        sr = torch.empty((nb, 3), dtype=torch.float32, device=dev)
+        lg = loc.capture(nb)
+
+        def eager_batches():
+            for b in small:
+                loc.locate(b, out=(sc, sr))
+
+        def graph_batches():
+            for b in small:
+                lg.points.copy_(b, non_blocking=True)
+                lg.graph.replay()
+
+        eager_batches()
+        graph_batches()
+        ms_e = timed(eager_batches, 3) / (3 * len(small))
+        ms_g = timed(graph_batches, 3) / (3 * len(small))
+        graph_small = {"batch": nb, "eager_ms_per_batch": ms_e, "graph_ms_per_batch": ms_g,
+                       "eager_pts_per_s": nb / (ms_e * 1e-3), "graph_pts_per_s": nb / (ms_g * 1e-3),
+                       "note": "element-centre guess; the graph replay includes the copy of "
+                               "the batch into the graph's static buffer"}
+        del lg
+    except Exception as exc:
+        graph_small = {"error": repr(exc)}
+
     head_name, head_locate, head_loc, head_value = ("batched (element-centre guess)", loc.locate,
                                                     loc, batched_value)
     if sub_value > head_value:
@@ -873,6 +904,7 @@ def main():
             "batched_subref": batched_sub,
             "batched": {"value": batched_value, "ms_per_step": batched_ms,
                         "note": "Morton-ordered persistent kernel, element-centre guess"},
+            "graph_small_batches": graph_small,
             "learned": learned,
             "volume": vol,
             "volume_c0": vol_c0,

@@ -308,6 +308,12 @@ class BatchedLocator:
         return cell, ref
 
 
+    def capture(self, n: int) -> "LocateGraph":
+        """A CUDA graph of this locator's batched locate over a static buffer
+        of n queries (query order, persistent kernel and their scratch
+        allocations), for callers that locate many batches of one size."""
+        return LocateGraph(self, n)
+
     def locate_host(self, host_points, out, chunk: int = 0, stream=None):
         """Locate points held in (page-locked) host memory, writing cell ids
         and reference points into the host tensors out = (cell, ref); the
@@ -324,6 +330,40 @@ class BatchedLocator:
                                         C.byref(opts), cfg, chunk, _ptr(cell), _ptr(ref),
                                         _stream(stream)), "drb_locate_host")
         return cell, ref
+
+
+class LocateGraph:
+    """Batched locate of a fixed-size query buffer captured once into a CUDA
+    graph and replayed per batch: the queries go into `points` (or are
+    passed to run()), results come back in `cell` / `ref`.  The graph holds
+    the Morton ordering, the persistent kernel and their stream-ordered
+    scratch allocations, so a replay is one launch from the host."""
+
+    def __init__(self, locator: BatchedLocator, n: int):
+        dev = locator.mesh.device
+        self.locator = locator
+        self.points = torch.zeros((n, 3), dtype=torch.float32, device=dev)
+        self.cell = torch.empty(n, dtype=torch.int32, device=dev)
+        self.ref = torch.empty((n, 3), dtype=torch.float32, device=dev)
+        # warm up outside the capture: lazy BVH build and one-time pool setup
+        locator.locate(self.points, out=(self.cell, self.ref))
+        torch.cuda.synchronize(dev)
+        self.graph = torch.cuda.CUDAGraph()
+        side = torch.cuda.Stream(dev)
+        side.wait_stream(torch.cuda.current_stream(dev))
+        with torch.cuda.stream(side):
+            locator.locate(self.points, out=(self.cell, self.ref))
+        torch.cuda.current_stream(dev).wait_stream(side)
+        torch.cuda.synchronize(dev)
+        with torch.cuda.graph(self.graph):
+            locator.locate(self.points, out=(self.cell, self.ref))
+
+    def run(self, points=None):
+        if points is not None:
+            self.points.copy_(_dev(points, torch.float32, self.points.device).reshape(-1, 3),
+                              non_blocking=True)
+        self.graph.replay()
+        return self.cell, self.ref
 
 
 def elem_subboxes(mesh: UnstructuredMesh, stream=None):

@@ -4,9 +4,9 @@
 // (data_model/unstructured_mesh.cpp:137-148): warps mix points from
 // unrelated parts of the mesh, and every lane waits for the slowest lane's
 // traversal and Newton iterations.  This path instead
-//   1. orders the queries by Morton cell (7 bits per axis over the BVH
-//      bounds, a counting sort), so a warp's lanes follow nearly the same
-//      BVH path and hit the same few elements (L1/L2 reuse);
+//   1. orders the queries by Morton cell (up to 7 bits per axis over the
+//      BVH bounds, a counting sort), so a warp's lanes follow nearly the
+//      same BVH path and hit the same few elements (L1/L2 reuse);
 //   2. runs a persistent kernel, grid sized to the resident capacity of the
 //      148 SMs, whose warps pop chunks of sorted queries from a global atomic
 //      queue;
@@ -31,9 +31,11 @@ namespace drb
 namespace
 {
 
-// Query order by counting sort into Morton cells of 7 bits per axis
-// (2^21 cells over the BVH bounds; one cell is an eighth of an element of a 64^3
-// mesh).  The persistent kernel needs spatially coherent warps, not a
+// Query order by counting sort into Morton cells over the BVH bounds: 7 bits
+// per axis for 16M queries (2^21 cells, one cell an eighth of an element of
+// a 64^3 mesh), fewer for smaller batches so that a cell holds about eight
+// queries (cell_bits: 3..7), which keeps the cell scan proportional to the
+// batch.  The persistent kernel needs spatially coherent warps, not a
 // sorted sequence, so the order inside a cell is whatever the atomics give:
 // one counting pass, a scan of the cell counts and one scatter replace the
 // four passes of a 30-bit radix sort.  Every query's result is independent
@@ -41,10 +43,17 @@ namespace
 constexpr int kCellBits = 7;
 constexpr int kCells = 1 << (3 * kCellBits);
 
+int cell_bits (int n)
+{
+  int bits = 3;
+  while (bits < kCellBits && (8ll << (3 * bits)) < (long long)n) ++bits;
+  return bits;
+}
+
 __global__ void cell_count_kernel (const float *__restrict__ pts, int n, float x0, float y0,
                                    float z0, float sx, float sy, float sz,
-                                   unsigned *__restrict__ cell_of, int *__restrict__ rank,
-                                   int *__restrict__ hist)
+                                   int bits, unsigned *__restrict__ cell_of,
+                                   int *__restrict__ rank, int *__restrict__ hist)
 {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= n) return;
@@ -55,7 +64,7 @@ __global__ void cell_count_kernel (const float *__restrict__ pts, int n, float x
   for (int k = 0; k < 3; ++k)
   {
     float t = (pts[3 * (size_t)i + k] - lo[k]) * sc[k];
-    t = fminf (fmaxf (t * (float)(1 << kCellBits), 0.f), (float)((1 << kCellBits) - 1));
+    t = fminf (fmaxf (t * (float)(1 << bits), 0.f), (float)((1 << bits) - 1));
     unsigned x = (t == t) ? (unsigned)t : 0u; // NaN queries go to cell 0
     x = (x | (x << 8)) & 0x0300F00Fu;
     x = (x | (x << 4)) & 0x030C30C3u;
@@ -88,23 +97,25 @@ void order_frame (const drb_bvh *bvh, float (&lo)[3], float (&sc)[3])
 }
 
 // order[0..n) over caller buffers: cell_of and rank hold n values, hist
-// kCells, scan_tmp scan_ws_ints(kCells).
+// kCells, scan_tmp scan_ws_ints(kCells) (enough for every batch size).
 int cell_order (const drb_bvh *bvh, const float *pts, int n, int *order, unsigned *cell_of,
                 int *rank, int *hist, int *scan_tmp, cudaStream_t s)
 {
   float lo[3], sc[3];
   order_frame (bvh, lo, sc);
-  cudaError_t e = cudaMemsetAsync (hist, 0, sizeof (int) * kCells, s);
+  const int bits = cell_bits (n);
+  const int cells = 1 << (3 * bits);
+  cudaError_t e = cudaMemsetAsync (hist, 0, sizeof (int) * cells, s);
   if (e != cudaSuccess)
   {
     set_last_error (cudaGetErrorString (e));
     return status_from (e);
   }
   cell_count_kernel<<<div_up (n, 256), 256, 0, s>>> (pts, n, lo[0], lo[1], lo[2], sc[0], sc[1],
-                                                      sc[2], cell_of, rank, hist);
+                                                      sc[2], bits, cell_of, rank, hist);
   int st = check_launch ("cell_count_kernel");
   if (st) return st;
-  if ((st = exclusive_scan_i32_ws (hist, hist, kCells, nullptr, scan_tmp, s))) return st;
+  if ((st = exclusive_scan_i32_ws (hist, hist, cells, nullptr, scan_tmp, s))) return st;
   cell_scatter_kernel<<<div_up (n, 256), 256, 0, s>>> (cell_of, rank, hist, n, order);
   return check_launch ("cell_scatter_kernel");
 }

@@ -220,3 +220,31 @@ def test_row_modes_identical(cuda, name):
         assert torch.equal(c, c0)
         assert torch.equal(r.view(torch.int32), r0.view(torch.int32))
         assert torch.equal(i, i0) and torch.equal(a, a0) and torch.equal(nd, n0)
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("shape", ["hex", "tet"])
+def test_locate_graph_replay_matches_eager(cuda, shape):
+    """The batched locate captured into a CUDA graph (BatchedLocator.capture)
+    gives the eager results bit for bit on new queries at every replay."""
+    import torch
+    from devil_ray_b200 import _lib as L
+    from devil_ray_b200 import api, meshgen
+    if shape == "hex":
+        m = meshgen.trilinear_distorted_mesh(12, 2, 0.15, seed=11)
+        g = api.UnstructuredMesh(m.ctrl_idx, m.xyz, m.order, device=cuda)
+    else:
+        m = meshgen.tet_warped_mesh(6, 2, 0.05, jitter=0.01, seed=5)
+        g = api.UnstructuredMesh(m.ctrl_idx, m.xyz, m.order, device=cuda, shape=L.SHAPE_SIMPLEX)
+    loc = api.BatchedLocator(g, tol=1e-5, max_steps=20)
+    n = 50000
+    lg = loc.capture(n)
+    for seed in (3, 4, 5):
+        q = meshgen.uniform_queries(n, seed)
+        c1, r1 = lg.run(q)
+        c1, r1 = c1.clone(), r1.clone()
+        c0, r0 = loc.locate(q)
+        torch.cuda.synchronize()
+        assert torch.equal(c0, c1)
+        assert torch.equal(r0.view(torch.int32), r1.view(torch.int32))
+        assert (c1 >= 0).float().mean() > 0.85
