@@ -181,12 +181,11 @@ class UnstructuredMesh:
 
     def get_bvh(self, stream=None, keep_codes: bool = False) -> BVH:
         """Lazily build the LBVH (UnstructuredMesh::get_bvh,
-        data_model/unstructured_mesh.cpp:23-31), and for hex and tet meshes
-        its 4-wide traversal tree."""
+        data_model/unstructured_mesh.cpp:23-31) and its 4-wide traversal
+        tree."""
         if self._bvh is None:
             self._bvh = self.build_bvh(stream, keep_codes)
-            if self.dim == 3:
-                self._bvh.widen(stream)
+            self._bvh.widen(stream)
             if self.shape == L.SHAPE_SIMPLEX:
                 self.hull_planes(stream)
         return self._bvh

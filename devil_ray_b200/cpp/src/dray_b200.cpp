@@ -118,7 +118,6 @@ const drb_bvh *ElementMesh::device_bvh ()
     g.bvh.aabb_ids = g.ids.p;
     g.bvh.ref_boxes = g.refb.p;
     drb_check (drb_lbvh_build (&g.mesh, &g.bvh, nullptr, nullptr), "drb_lbvh_build");
-    if (m_dim == 3)
     {
       // 4-wide traversal tree for the batched locate and the volume march
       drb_check (drb_bvh_widen (&g.bvh, nullptr, 0, nullptr), "drb_bvh_widen");
@@ -161,7 +160,6 @@ AABB<3> ElementMesh::bounds ()
 
 Array<Location> ElementMesh::locate (Array<Vec<Float, 3>> &wpoints)
 {
-  if (m_dim != 3) DRAY_ERROR ("locate needs a volume (hex or tet) mesh");
   const int n = (int)wpoints.size ();
   Array<Location> out;
   out.resize (n);
@@ -245,7 +243,6 @@ std::vector<Range> ElementField::range () const
 
 void ElementField::eval (const Array<Location> locs, Array<Float> &values)
 {
-  if (m_dim != 3) DRAY_ERROR ("field eval at locations needs a hex or tet field");
   const int n = (int)locs.size ();
   values.resize (n);
   if (n == 0) return;

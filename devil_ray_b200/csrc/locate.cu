@@ -50,10 +50,11 @@ extern "C" int drb_locate (const drb_mesh *mesh, const drb_bvh *bvh, const float
     set_last_error ("locate: bad arguments");
     return DRB_ERR_INVALID_ARG;
   }
-  if (mesh->dim != 3 || mesh->ncomp != 3 || mesh->order < 1 || mesh->order > 3 ||
-      (mesh->shape != DRB_SHAPE_TENSOR && mesh->shape != DRB_SHAPE_SIMPLEX))
+  if (mesh->ncomp != 3 || mesh->order < 1 || mesh->order > 3 ||
+      !((mesh->dim == 3 && (mesh->shape == DRB_SHAPE_TENSOR || mesh->shape == DRB_SHAPE_SIMPLEX)) ||
+        (mesh->dim == 2 && mesh->shape == DRB_SHAPE_TENSOR)))
   {
-    set_last_error ("locate: needs a hex or tet geometry mesh of order 1..3");
+    set_last_error ("locate: needs a hex, tet or quad geometry mesh of order 1..3");
     return DRB_ERR_UNSUPPORTED;
   }
   if (opts->guess_mode == DRB_GUESS_GIVEN && !opts->guess)
@@ -89,6 +90,12 @@ extern "C" int drb_locate (const drb_mesh *mesh, const drb_bvh *bvh, const float
     if (mesh->order == 1) DRB_LK (1, kSimplex);
     else if (mesh->order == 2) DRB_LK (2, kSimplex);
     else DRB_LK (3, kSimplex);
+  }
+  else if (mesh->dim == 2)
+  {
+    if (mesh->order == 1) DRB_LK (1, kQuad2D);
+    else if (mesh->order == 2) DRB_LK (2, kQuad2D);
+    else DRB_LK (3, kQuad2D);
   }
   else if (mesh->order == 1) DRB_LK (1, kTensor);
   else if (mesh->order == 2) DRB_LK (2, kTensor);

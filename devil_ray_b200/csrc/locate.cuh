@@ -156,15 +156,17 @@ DRB_D bool hull_rejects (const LocateParams &lp, int el, const float (&pt)[3])
   return out;
 }
 
-// Element shapes of the locate templates (drb_shape).
+// Element kinds of the locate templates: drb_shape for volume elements,
+// plus the quads of 2D meshes (tensor shape, dim 2).
 constexpr int kTensor = DRB_SHAPE_TENSOR;
 constexpr int kSimplex = DRB_SHAPE_SIMPLEX;
+constexpr int kQuad2D = 2;
 
-// Dofs of an order-P element of shape S, and its reference centre
+// Dofs of an order-P element of kind S, and its reference centre
 // coordinate (hex (0.5,0.5,0.5), tet centroid (0.25,0.25,0.25)).
 template <int S, int P> constexpr int shape_dofs ()
 {
-  return S == kSimplex ? tet_dofs<P> () : (P + 1) * (P + 1) * (P + 1);
+  return S == kSimplex ? tet_dofs<P> () : S == kQuad2D ? (P + 1) * (P + 1) : (P + 1) * (P + 1) * (P + 1);
 }
 template <int S> constexpr float shape_centre () { return S == kSimplex ? 0.25f : 0.5f; }
 
@@ -192,6 +194,30 @@ DRB_D bool solve_in_tet (const LocateParams &lp, int el, const float (&pt)[3], f
   return tet_newton<P> (cp, pt, x, lp.tol, lp.max_steps, steps, lu);
 }
 
+// Quad of a 2D mesh (LocateHack<2>): quad_newton on the packed row.
+template <int P, bool REG>
+DRB_D bool solve_in_quad (const LocateParams &lp, int el, const float (&pt)[3], float (&x)[3],
+                          int &steps, LU3 &lu)
+{
+  constexpr int ND = (P + 1) * (P + 1);
+  if (lp.packed)
+  {
+    const float *row = lp.packed + (size_t)el * lp.stride;
+    float t[3];
+    local_target<ND> (row, pt, t);
+    if (REG)
+    {
+      RegCP<3 * ND> r;
+      load_reg_rows<3 * ND> (r, row);
+      return quad_newton<P> (r, t, x, lp.tol, lp.max_steps, steps, lu);
+    }
+    PackedCP cp{ row };
+    return quad_newton<P> (cp, t, x, lp.tol, lp.max_steps, steps, lu);
+  }
+  IndirectCP cp{ lp.ctrl_idx + (size_t)el * ND, lp.xyz, 3 };
+  return quad_newton<P> (cp, pt, x, lp.tol, lp.max_steps, steps, lu);
+}
+
 // Newton solve of one point in one element, choosing register-resident or
 // L1-read control points by order.
 template <int P, bool REG = (P <= 2), int S = kTensor>
@@ -199,6 +225,7 @@ DRB_D bool solve_in_element (const LocateParams &lp, int el, const float (&pt)[3
                              int &steps, LU3 &lu)
 {
   if (S == kSimplex) return solve_in_tet<P, REG> (lp, el, pt, x, steps, lu);
+  if (S == kQuad2D) return solve_in_quad<P, REG> (lp, el, pt, x, steps, lu);
   constexpr int ND = (P + 1) * (P + 1) * (P + 1);
   if (lp.packed)
   {
@@ -275,6 +302,14 @@ DRB_D void candidate_guess (const LocateParams &lp, int leaf, long long qi, bool
       sum = __fadd_rn (sum, rb[6 + d]);
       x[d] = __fmul_rn (sum, 0.25f);
     }
+  }
+  else if (lp.guess_mode == DRB_GUESS_SUBREF_CENTER && S == kQuad2D)
+  {
+    // SubRef<2,Tensor>: low (u, v), then high (u, v)
+    const float *rb = lp.ref_boxes + 4 * (size_t)__ldg (lp.aabb_ids + leaf);
+    x[0] = (rb[0] + rb[2]) * 0.5f;
+    x[1] = (rb[1] + rb[3]) * 0.5f;
+    x[2] = 0.f;
   }
   else if (lp.guess_mode == DRB_GUESS_SUBREF_CENTER)
   {

@@ -302,8 +302,9 @@ template <int S> const void *persistent_fn_s (int order, int mode, bool wide)
 
 const void *persistent_fn (const drb_mesh *mesh, int mode, bool wide)
 {
-  return mesh->shape == DRB_SHAPE_SIMPLEX ? persistent_fn_s<kSimplex> (mesh->order, mode, wide)
-                                          : persistent_fn_s<kTensor> (mesh->order, mode, wide);
+  if (mesh->shape == DRB_SHAPE_SIMPLEX) return persistent_fn_s<kSimplex> (mesh->order, mode, wide);
+  if (mesh->dim == 2) return persistent_fn_s<kQuad2D> (mesh->order, mode, wide);
+  return persistent_fn_s<kTensor> (mesh->order, mode, wide);
 }
 
 // Row mode actually used: registers only for orders 1-2, shared rows only
@@ -311,7 +312,8 @@ const void *persistent_fn (const drb_mesh *mesh, int mode, bool wide)
 int effective_mode (const drb_mesh *mesh, int requested)
 {
   if (requested == kRowsReg && mesh->order <= 2) return kRowsReg;
-  if (requested == kRowsShared && mesh->packed && mesh->shape == DRB_SHAPE_TENSOR) return kRowsShared;
+  if (requested == kRowsShared && mesh->packed && mesh->shape == DRB_SHAPE_TENSOR && mesh->dim == 3)
+    return kRowsShared;
   return kRowsL1;
 }
 
@@ -357,6 +359,8 @@ int launch_persistent (const drb_mesh *mesh, int mode, dim3 grid, int block, cud
                           (int)smem);
   if (mesh->shape == DRB_SHAPE_SIMPLEX)
     launch_s<kSimplex> (order, wide, mode, grid, block, smem, s, lp, pts, ord, n, chunk, head, cell, ref, st);
+  else if (mesh->dim == 2)
+    launch_s<kQuad2D> (order, wide, mode, grid, block, smem, s, lp, pts, ord, n, chunk, head, cell, ref, st);
   else
     launch_s<kTensor> (order, wide, mode, grid, block, smem, s, lp, pts, ord, n, chunk, head, cell, ref, st);
   return check_launch ("locate_persistent_kernel");
@@ -401,10 +405,11 @@ int check_args (const drb_mesh *mesh, const drb_bvh *bvh, const float *pts, int 
     set_last_error ("locate_batched: bad arguments");
     return DRB_ERR_INVALID_ARG;
   }
-  if (mesh->dim != 3 || mesh->ncomp != 3 || mesh->order < 1 || mesh->order > 3 ||
-      (mesh->shape != DRB_SHAPE_TENSOR && mesh->shape != DRB_SHAPE_SIMPLEX))
+  if (mesh->ncomp != 3 || mesh->order < 1 || mesh->order > 3 ||
+      !((mesh->dim == 3 && (mesh->shape == DRB_SHAPE_TENSOR || mesh->shape == DRB_SHAPE_SIMPLEX)) ||
+        (mesh->dim == 2 && mesh->shape == DRB_SHAPE_TENSOR)))
   {
-    set_last_error ("locate_batched: needs a hex or tet geometry mesh of order 1..3");
+    set_last_error ("locate_batched: needs a hex, tet or quad geometry mesh of order 1..3");
     return DRB_ERR_UNSUPPORTED;
   }
   if (opts->guess_mode == DRB_GUESS_GIVEN && !opts->guess)

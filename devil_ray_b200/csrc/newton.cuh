@@ -86,6 +86,51 @@ DRB_D bool hex_newton (const CP &cp, const float (&target)[3], float (&x)[3], fl
   return hex_newton<P> (cp, target, x, tol, max_steps, steps, lu);
 }
 
+// LocateHack<2>::eval_inverse (data_model/device_mesh.hpp:166-238): a quad
+// of a 2D mesh in 3D space with z ignored.  The 3x3 Jacobian is
+// [dX/du, dX/dv, e_z]; only the u and v of the LUP solution step x;
+// converged when the inf-norm of that 2D step is below tol, accepted if
+// converged and inside [0,1]^2 within tol (QuadRefSpace<2>::is_inside,
+// pos_tensor_element.tcc:49-61).  x[2] is left at -1, as the reference
+// leaves the third coordinate of a 2D Location.
+template <int P, class CP>
+DRB_D bool quad_newton (const CP &cp, const float (&target)[3], float (&x)[3], float tol,
+                        int max_steps, int &steps, LU3 &lu)
+{
+  float prev[2] = { x[0], x[1] };
+  bool converged = false;
+  steps = 0;
+  while (steps < max_steps && !converged)
+  {
+    x[0] = fminf (1.f, fmaxf (x[0], 0.f));
+    x[1] = fminf (1.f, fmaxf (x[1], 0.f));
+    float X[3], Ju[3], Jv[3];
+    quad_eval_d<P, 3> (cp, x[0], x[1], X, Ju, Jv);
+    float dy[3], J[3][3], dx[3];
+#pragma unroll
+    for (int r = 0; r < 3; ++r)
+    {
+      dy[r] = target[r] - X[r];
+      J[r][0] = Ju[r];
+      J[r][1] = Jv[r];
+      J[r][2] = (r == 2) ? 1.f : 0.f;
+    }
+    lu.factor (J);
+    lu.solve (dy, dx);
+    x[0] += dx[0];
+    x[1] += dx[1];
+    ++steps;
+    const float a = x[0] - prev[0], b = x[1] - prev[1];
+    converged = fmaxf (fmaxf (-a, a), fmaxf (-b, b)) < tol;
+    prev[0] = x[0];
+    prev[1] = x[1];
+  }
+  x[2] = -1.f;
+  const float mn = fminf (fminf (x[0], 2.f), x[1]);
+  const float mx = fmaxf (fmaxf (x[0], -1.f), x[1]);
+  return converged && mn >= 0.f - tol && mx <= 1.f + tol;
+}
+
 // Control points of one element read through the packed element-major copy.
 struct PackedCP
 {
@@ -183,6 +228,23 @@ template <int N> struct RegCP
   float v[N];
   DRB_D float operator() (int i, int k) const { return v[3 * i + k]; }
 };
+
+// The first N floats of a packed row (16-byte aligned) into registers.
+template <int N> DRB_D void load_reg_rows (RegCP<N> &r, const float *p)
+{
+  const float4 *p4 = reinterpret_cast<const float4 *> (p);
+#pragma unroll
+  for (int q = 0; q < N / 4; ++q)
+  {
+    const float4 t = __ldg (p4 + q);
+    r.v[4 * q] = t.x;
+    r.v[4 * q + 1] = t.y;
+    r.v[4 * q + 2] = t.z;
+    r.v[4 * q + 3] = t.w;
+  }
+#pragma unroll
+  for (int q = (N / 4) * 4; q < N; ++q) r.v[q] = __ldg (p + q);
+}
 
 template <int P> DRB_D void load_reg_cp (RegCP<3 * (P + 1) * (P + 1) * (P + 1)> &r, const float *p)
 {

@@ -15,7 +15,8 @@ namespace drb
 namespace
 {
 
-template <int P, bool TET>
+// K: 0 hex, 1 tet, 2 quad of a 2D mesh
+template <int P, int K>
 __global__ void map_points_kernel (const float *__restrict__ packed, int stride,
                                    const int *__restrict__ elem, const float *__restrict__ ref,
                                    int n, float *__restrict__ pts)
@@ -29,11 +30,17 @@ __global__ void map_points_kernel (const float *__restrict__ packed, int stride,
     const float *row = packed + (size_t)e * stride;
     PackedCP cp{ row };
     const float u = ref[3 * (size_t)i], v = ref[3 * (size_t)i + 1], w = ref[3 * (size_t)i + 2];
-    if (TET)
+    if (K == 1)
     {
       float Ju[3], Jv[3], Jw[3];
       tet_eval_d<P, 3> (cp, u, v, w, X, Ju, Jv, Jw);
       to_world<tet_dofs<P> ()> (row, X);
+    }
+    else if (K == 2)
+    {
+      float Ju[3], Jv[3];
+      quad_eval_d<P, 3> (cp, u, v, X, Ju, Jv);
+      to_world<(P + 1) * (P + 1)> (row, X);
     }
     else
     {
@@ -92,7 +99,7 @@ __global__ void newton_pairs_kernel (const float *__restrict__ packed, int strid
 
 // UnstructuredField::eval at located points (unstructured_field.cpp:214-245):
 // value of the scalar field at (cell, ref); cell -1 -> empty value.
-template <int P, bool TET>
+template <int P, int K>
 __global__ void field_eval_kernel (const float *__restrict__ packed, int stride,
                                    const int *__restrict__ cell, const float *__restrict__ ref,
                                    int n, float empty, float *__restrict__ out)
@@ -110,10 +117,15 @@ __global__ void field_eval_kernel (const float *__restrict__ packed, int stride,
     } cp{ packed + (size_t)e * stride };
     float X[1];
     const float u = ref[3 * (size_t)i], vv = ref[3 * (size_t)i + 1], w = ref[3 * (size_t)i + 2];
-    if (TET)
+    if (K == 1)
     {
       float Ju[1], Jv[1], Jw[1];
       tet_eval_d<P, 1> (cp, u, vv, w, X, Ju, Jv, Jw);
+    }
+    else if (K == 2)
+    {
+      float Ju[1], Jv[1];
+      quad_eval_d<P, 1> (cp, u, vv, X, Ju, Jv);
     }
     else
     {
@@ -124,19 +136,26 @@ __global__ void field_eval_kernel (const float *__restrict__ packed, int stride,
   out[i] = v;
 }
 
-int check_pairs (const drb_mesh *m, int n, bool tets_ok = false)
+int check_pairs (const drb_mesh *m, int n, bool any_kind = false)
 {
-  if (!m || !m->packed || m->dim != 3 || m->ncomp != 3 || m->order < 1 || m->order > 3 || n < 0)
+  if (!m || !m->packed || m->ncomp != 3 || m->order < 1 || m->order > 3 || n < 0 ||
+      (m->dim != 3 && !(any_kind && m->dim == 2)))
   {
     set_last_error ("pairs: needs a packed hex geometry mesh of order 1..3");
     return DRB_ERR_INVALID_ARG;
   }
-  if (m->shape != DRB_SHAPE_TENSOR && !(tets_ok && m->shape == DRB_SHAPE_SIMPLEX))
+  if (m->shape != DRB_SHAPE_TENSOR && !(any_kind && m->shape == DRB_SHAPE_SIMPLEX && m->dim == 3))
   {
     set_last_error ("pairs: element shape not supported here");
     return DRB_ERR_UNSUPPORTED;
   }
   return DRB_OK;
+}
+
+// 0 hex, 1 tet, 2 quad (the K of the kernels above)
+int kind_of (const drb_mesh *m)
+{
+  return m->shape == DRB_SHAPE_SIMPLEX ? 1 : m->dim == 2 ? 2 : 0;
 }
 
 } // namespace
@@ -158,16 +177,13 @@ extern "C" int drb_map_points (const drb_mesh *mesh, const int *elem, const floa
   const int stride = packed_stride (mesh_nd (mesh), 3);
   cudaStream_t s = (cudaStream_t)stream;
   const int b = div_up (n, 256);
-#define DRB_MP(P, T) map_points_kernel<P, T><<<b, 256, 0, s>>> (mesh->packed, stride, elem, ref, n, pts)
-  if (mesh->shape == DRB_SHAPE_SIMPLEX)
-  {
-    if (mesh->order == 1) DRB_MP (1, true);
-    else if (mesh->order == 2) DRB_MP (2, true);
-    else DRB_MP (3, true);
-  }
-  else if (mesh->order == 1) DRB_MP (1, false);
-  else if (mesh->order == 2) DRB_MP (2, false);
-  else DRB_MP (3, false);
+#define DRB_MP(P, K) map_points_kernel<P, K><<<b, 256, 0, s>>> (mesh->packed, stride, elem, ref, n, pts)
+#define DRB_MPK(K) (mesh->order == 1 ? DRB_MP (1, K) : mesh->order == 2 ? DRB_MP (2, K) : DRB_MP (3, K))
+  const int kind = kind_of (mesh);
+  if (kind == 1) DRB_MPK (1);
+  else if (kind == 2) DRB_MPK (2);
+  else DRB_MPK (0);
+#undef DRB_MPK
 #undef DRB_MP
   return check_launch ("map_points_kernel");
 }
@@ -200,27 +216,25 @@ extern "C" int drb_newton_pairs (const drb_mesh *mesh, const int *elem, const fl
 extern "C" int drb_field_eval (const drb_mesh *field, const int *cell, const float *ref, int n,
                                float empty_value, float *values, void *stream)
 {
-  if (!field || !field->packed || field->dim != 3 || field->ncomp != 1 || field->order < 1 ||
-      field->order > 3 || n < 0 || (n > 0 && (!cell || !ref || !values)) ||
-      (field->shape != DRB_SHAPE_TENSOR && field->shape != DRB_SHAPE_SIMPLEX))
+  if (!field || !field->packed || field->ncomp != 1 || field->order < 1 || field->order > 3 ||
+      n < 0 || (n > 0 && (!cell || !ref || !values)) ||
+      !((field->dim == 3 && (field->shape == DRB_SHAPE_TENSOR || field->shape == DRB_SHAPE_SIMPLEX)) ||
+        (field->dim == 2 && field->shape == DRB_SHAPE_TENSOR)))
   {
-    set_last_error ("field_eval: needs a packed scalar hex or tet field of order 1..3");
+    set_last_error ("field_eval: needs a packed scalar hex, tet or quad field of order 1..3");
     return DRB_ERR_INVALID_ARG;
   }
   if (n == 0) return DRB_OK;
   const int stride = packed_stride (mesh_nd (field), 1);
   cudaStream_t s = (cudaStream_t)stream;
   const int b = div_up (n, 256);
-#define DRB_FE(P, T) field_eval_kernel<P, T><<<b, 256, 0, s>>> (field->packed, stride, cell, ref, n, empty_value, values)
-  if (field->shape == DRB_SHAPE_SIMPLEX)
-  {
-    if (field->order == 1) DRB_FE (1, true);
-    else if (field->order == 2) DRB_FE (2, true);
-    else DRB_FE (3, true);
-  }
-  else if (field->order == 1) DRB_FE (1, false);
-  else if (field->order == 2) DRB_FE (2, false);
-  else DRB_FE (3, false);
+#define DRB_FE(P, K) field_eval_kernel<P, K><<<b, 256, 0, s>>> (field->packed, stride, cell, ref, n, empty_value, values)
+#define DRB_FEK(K) (field->order == 1 ? DRB_FE (1, K) : field->order == 2 ? DRB_FE (2, K) : DRB_FE (3, K))
+  const int kind = kind_of (field);
+  if (kind == 1) DRB_FEK (1);
+  else if (kind == 2) DRB_FEK (2);
+  else DRB_FEK (0);
+#undef DRB_FEK
 #undef DRB_FE
   return check_launch ("field_eval_kernel");
 }

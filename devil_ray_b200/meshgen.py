@@ -239,6 +239,50 @@ def tet_warped_mesh(n: int, p: int, amp: float, jitter: float = 0.0, seed: int =
                        meta=meta)
 
 
+@dataclass
+class QuadMeshData:
+    order: int
+    n: int                      # quads per axis
+    ctrl_idx: np.ndarray        # int32 [n^2 * (p+1)^2], u fastest
+    xyz: np.ndarray             # float32 [(p n + 1)^2, 3], z = 0
+    field: np.ndarray           # float32 [n_ctrl]
+    meta: dict = field(default_factory=dict)
+
+    @property
+    def n_elem(self) -> int:
+        return self.n ** 2
+
+
+def quad_warped_mesh(n: int, p: int, amp: float, jitter: float = 0.0, seed: int = 0) -> QuadMeshData:
+    """A 2D mesh of n^2 order-p quads over [0,1]^2 in the z = 0 plane:
+    lattice (p n + 1)^2, point (I, J) at index J (p n + 1) + I, element
+    (ei, ej) with id ej n + ei and dof (a, b) (u fastest) at lattice point
+    (p ei + a, p ej + b); interior points displaced by
+    amp sin(2pi x) sin(2pi y) in x and y (plus optional uniform jitter);
+    f = sin(3x)cos(2y) + x y."""
+    m = p * n + 1
+    t = np.linspace(0.0, 1.0, m)
+    Y, X = np.meshgrid(t, t, indexing="ij")
+    xyz = np.stack([X.ravel(), Y.ravel(), np.zeros(m * m)], axis=1)
+    i = np.arange(m)
+    inner1 = (i > 0) & (i < m - 1)
+    inner = (inner1[:, None] & inner1[None, :]).ravel()
+    s = np.sin(TWO_PI * xyz[:, 0]) * np.sin(TWO_PI * xyz[:, 1])
+    xyz[inner, :2] += (amp * s)[inner, None]
+    if jitter > 0.0:
+        rng = np.random.default_rng(seed)
+        xyz[inner, :2] += rng.uniform(-jitter, jitter, size=(int(inner.sum()), 2))
+    e = np.arange(n, dtype=np.int64)
+    a = np.arange(p + 1, dtype=np.int64)
+    J = p * e[:, None, None, None] + a[None, None, :, None]
+    I = p * e[None, :, None, None] + a[None, None, None, :]
+    idx = (J * m + I).reshape(-1).astype(np.int32)
+    f = np.sin(3.0 * xyz[:, 0]) * np.cos(2.0 * xyz[:, 1]) + xyz[:, 0] * xyz[:, 1]
+    meta = {"warp_amplitude": amp, "jitter": jitter, "seed": seed, "field": "sin(3x)cos(2y)+xy"}
+    return QuadMeshData(order=p, n=n, ctrl_idx=idx, xyz=xyz.astype(np.float32),
+                        field=f.astype(np.float32), meta=meta)
+
+
 # outside fraction of uniform queries: the meshes fill [0,1]^3, so queries are
 # drawn from a cube padded so that about 8% of its volume lies outside
 OUTSIDE_FRACTION = 0.08

@@ -66,7 +66,9 @@ enum drb_shape
  * allocation-free forms, and drb_locate_tune), drb_field_eval,
  * drb_map_points and the volume renderer (drb_volume_integrate,
  * drb_volume_render, with a tet scalar field); the other entry points return
- * DRB_ERR_UNSUPPORTED for them. */
+ * DRB_ERR_UNSUPPORTED for them.  2D quad meshes (dim 2) are located by the
+ * same locate entry points and evaluated by drb_field_eval and
+ * drb_map_points, besides their use as surfaces. */
 typedef struct drb_mesh
 {
   int dim;               /* 3 hex or tet, 2 quad */
@@ -222,7 +224,9 @@ int drb_lbvh_build (const drb_mesh *mesh, drb_bvh *bvh, unsigned *sorted_codes, 
  * DeviceMesh::locate device_mesh.hpp:248-354).  One thread per point, BVH
  * traversal left child first, first leaf whose Newton solve converges and is
  * inside wins.  pts device float[3n]; cell device int32[n] (-1 = not found);
- * ref device float[3n] (-1 for misses). */
+ * ref device float[3n] (-1 for misses).  Hex, tet and 2D quad meshes; a quad
+ * mesh is located as LocateHack<2> does (device_mesh.hpp:166-238): z is
+ * ignored and the third reference coordinate stays -1. */
 int drb_locate (const drb_mesh *mesh, const drb_bvh *bvh, const float *pts, int n,
                 const drb_newton_opts *opts, int *cell, float *ref, drb_query_stats stats,
                 void *stream);

@@ -287,6 +287,42 @@ void *ref_tet_create (int order, int fixed, int n_el, const int *ctrl_idx, int n
   }
 }
 
+// Create a quad (2D) mesh and optional scalar field "f": QuadMesh_P1/P2
+// for orders 1-2, QuadMesh (general order) otherwise, as the dispatcher
+// picks them.
+void *ref_quad_create (int order, int n_el, const int *ctrl_idx, int n_ctrl, const float *xyz,
+                       const int *field_idx, int n_field_ctrl, const float *field_vals)
+{
+  try
+  {
+    const int nd = (order + 1) * (order + 1);
+    RefMesh *r = new RefMesh ();
+    r->order = order;
+    GridFunction<3> gf = make_gf3 (n_el, nd, ctrl_idx, n_ctrl, xyz);
+    if (order == 1) r->mesh = std::make_shared<QuadMesh_P1> (gf, 1);
+    else if (order == 2) r->mesh = std::make_shared<QuadMesh_P2> (gf, 2);
+    else r->mesh = std::make_shared<QuadMesh> (gf, order);
+    DataSet ds (r->mesh);
+    if (field_vals != nullptr)
+    {
+      GridFunction<1> ff = make_gf1 (n_el, nd, field_idx, n_field_ctrl, field_vals);
+      std::shared_ptr<Field> f;
+      if (order == 1) f = std::make_shared<UnstructuredField<QuadScalar_P1>> (ff, 1, "f");
+      else if (order == 2) f = std::make_shared<UnstructuredField<QuadScalar_P2>> (ff, 2, "f");
+      else f = std::make_shared<UnstructuredField<QuadScalar>> (ff, order, "f");
+      ds.add_field (f);
+      r->has_field = true;
+    }
+    r->collection.add_domain (ds);
+    return r;
+  }
+  catch (const std::exception &e)
+  {
+    g_err = e.what ();
+    return nullptr;
+  }
+}
+
 void ref_free (void *h) { delete static_cast<RefMesh *> (h); }
 
 // Builds (if needed) the mesh BVH and reports its sizes.

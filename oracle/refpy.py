@@ -48,6 +48,8 @@ def lib():
         L.ref_eval_hex_scalar.argtypes = [C.c_int, C.c_int, vp, C.c_int, vp, vp, vp]
         L.ref_lineout.argtypes = [vp, C.c_int, vp, vp, C.c_int, C.c_float, vp, vp]
         L.ref_scalar_render.argtypes = [vp, C.c_int, C.c_int, vp, C.c_float, vp, vp, vp]
+        L.ref_quad_create.restype = vp
+        L.ref_quad_create.argtypes = [C.c_int, C.c_int, vp, C.c_int, vp, vp, C.c_int, vp]
         L.ref_tet_create.restype = vp
         L.ref_tet_create.argtypes = [C.c_int, C.c_int, C.c_int, vp, C.c_int, vp, vp, C.c_int, vp]
         L.ref_eval_tet_scalar.argtypes = [C.c_int, C.c_int, vp, C.c_int, vp, vp, vp]
@@ -199,6 +201,25 @@ class RefTetMesh(RefHexMesh):
         self.h = lib().ref_tet_create(self.order, int(fixed), self.n_elem, _p(self.ctrl_idx),
                                       self.xyz.shape[0], _p(self.xyz), _p(self.ctrl_idx),
                                       0 if self.field is None else self.field.size, fptr)
+        if not self.h:
+            raise RuntimeError(lib().ref_last_error().decode())
+
+
+class RefQuadMesh(RefHexMesh):
+    """The reference's UnstructuredMesh<Quad> of a 2D mesh (+ scalar field "f")."""
+
+    ref_box_floats = 4    # SubRef<2,Tensor>: low (u, v), high (u, v)
+
+    def __init__(self, order, ctrl_idx, xyz, field=None):
+        self.order = int(order)
+        self.ctrl_idx = np.ascontiguousarray(ctrl_idx, dtype=np.int32)
+        self.xyz = np.ascontiguousarray(xyz, dtype=np.float32).reshape(-1, 3)
+        self.field = None if field is None else np.ascontiguousarray(field, dtype=np.float32)
+        self.n_elem = self.ctrl_idx.size // ((self.order + 1) ** 2)
+        fptr = None if self.field is None else _p(self.field)
+        self.h = lib().ref_quad_create(self.order, self.n_elem, _p(self.ctrl_idx),
+                                       self.xyz.shape[0], _p(self.xyz), _p(self.ctrl_idx),
+                                       0 if self.field is None else self.field.size, fptr)
         if not self.h:
             raise RuntimeError(lib().ref_last_error().decode())
 
