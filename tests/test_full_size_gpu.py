@@ -1,0 +1,151 @@
+"""The benchmark configurations at their full sizes.
+
+  C2 locate_64   262,144 order-2 hexes, 8.65M sub-box leaves, 16M queries:
+                 cells against the reference itself (oracle/_ref, OpenMP on
+                 the host cores, its fixed tol 1e-4 and zero first guess,
+                 which the plain kernel is given too), the persistent kernel
+                 against the plain one, and the forward map of every located
+                 query back onto it.
+  C1 surface_32  32,768 order-3 hexes, 6,144 boundary quads, 1024^2 rays:
+                 hits and image against the reference's Surface.
+  C4 volume_128  2.1M order-3 hexes, 69.2M sub-box leaves, 2048^2 rays,
+                 1000 samples: the reference cannot run this size in a test,
+                 so size-independent properties: the Morton codes of the
+                 tree are sorted, aabb_ids is a permutation of the sub-boxes,
+                 the coherent march (previous element first, face steps)
+                 renders the plain march's image (a full BVH locate per
+                 sample) within 1/255 on >= 99.5 % of pixels.
+Each test builds its mesh on the host first (C4 about 20 s) and holds a few
+GB on the device.
+"""
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+
+
+def test_c2_locate_full_size(cuda, ref):
+    import torch
+    from devil_ray_b200 import _lib as L
+    from devil_ray_b200 import api, meshgen
+    from devil_ray_b200.learned import map_points
+    m = meshgen.workload_mesh("locate_64")
+    q = meshgen.uniform_queries(1 << 24, 1000)
+    g = api.UnstructuredMesh(m.ctrl_idx, m.xyz, m.order, device=cuda)
+    pts = torch.as_tensor(q, device=cuda)
+    # the reference's settings on the plain kernel
+    c_plain, r_plain = g.locate(pts, tol=1e-4, max_steps=20, guess_mode=L.GUESS_ZERO)
+    torch.cuda.synchronize()
+    rc, rr = ref.RefHexMesh(m.order, m.ctrl_idx, m.xyz).locate(q)
+    cp = c_plain.cpu().numpy()
+    same = cp == rc
+    print(f"C2: {(~same).sum()} of {q.shape[0]} cells differ from the reference")
+    assert same.mean() > 0.9999
+    both = same & (cp >= 0)
+    assert np.abs(r_plain.cpu().numpy()[both] - rr[both]).max() < 1e-3
+    # the persistent kernel at tol 1e-5 against the plain kernel at tol 1e-5
+    c0, r0 = g.locate(pts, tol=1e-5, max_steps=20, guess_mode=L.GUESS_ELEM_CENTER)
+    c1, r1 = api.BatchedLocator(g, tol=1e-5, max_steps=20).locate(pts)
+    torch.cuda.synchronize()
+    assert torch.equal(c0, c1)
+    assert torch.equal(r0.view(torch.int32), r1.view(torch.int32))
+    # every located query maps back onto itself; the mesh fills [0,1]^3
+    sel = c1 >= 0
+    X = map_points(g, c1[sel], r1[sel])
+    err = (X - pts[sel]).abs().max().item()
+    assert err < 1e-4, err
+    inside = ((pts > 1e-3) & (pts < 1 - 1e-3)).all(dim=1)
+    outside = ((pts < -1e-3) | (pts > 1 + 1e-3)).any(dim=1)
+    assert sel[inside].float().mean().item() > 0.99999
+    assert sel[outside].float().mean().item() < 1e-5
+
+
+def test_c1_surface_full_size(cuda, ref):
+    import torch
+    from devil_ray_b200 import api, meshgen
+    from devil_ray_b200.render import (Camera, ColorTable, MeshBoundary, PointLight, Surface,
+                                       UnstructuredField)
+    m = meshgen.workload_mesh("surface_32")
+    c = meshgen.CAMERA
+    w = 1024
+    cam = Camera(w, w, c["pos"], c["look_at"], c["up"], c["fov"])
+    light = PointLight.default(cam)
+    cam9 = np.array([*c["pos"], *c["look_at"], *c["up"]], np.float32)
+    rs = ref.RefHexMesh(m.order, m.ctrl_idx, m.xyz, m.field).surface(
+        w, w, cam9, c["fov"], 1024, np.array(meshgen.TF_RGB, np.float32),
+        np.array(meshgen.TF_ALPHA, np.float32), light.as13()[None])
+    mesh = api.UnstructuredMesh(m.ctrl_idx, m.xyz, m.order, device=cuda)
+    field = UnstructuredField(m.ctrl_idx, m.field, m.order, device=cuda)
+    faces, ff = MeshBoundary().execute(mesh, field)
+    assert faces.n_elem == 6 * 32 * 32
+    surf = Surface(faces, ff)
+    t = ColorTable()
+    for p in meshgen.TF_RGB:
+        t.add_point(p[0], p[1:])
+    for p in meshgen.TF_ALPHA:
+        t.add_alpha(*p)
+    surf.color_map().color_table(t)
+    fb, hits = surf.render(cam, [light])
+    torch.cuda.synchronize()
+    h = hits.cpu().numpy()
+    gidx = h[:, 0].view(np.int32)
+    same = gidx == rs["hit_idx"]
+    print(f"C1: {(~same).sum()} of {w * w} hits differ from the reference")
+    assert same.mean() > 0.999
+    both = same & (gidx >= 0)
+    assert np.abs(h[both, 1] - rs["dist"][both]).max() < 1e-4
+    d = np.abs(fb.image() - rs["rgba"])
+    assert np.any(d > 1.0 / 255.0, axis=-1).mean() < 0.005
+
+
+def test_c4_volume_full_size_properties(cuda):
+    import torch
+    from devil_ray_b200 import _lib as L
+    from devil_ray_b200 import api, meshgen
+    from devil_ray_b200.render import Camera, ColorTable, PointLight, UnstructuredField, Volume
+    m = meshgen.workload_mesh("volume_128")
+    g = api.UnstructuredMesh(m.ctrl_idx, m.xyz, m.order, device=cuda)
+    b = g.build_bvh(keep_codes=True)
+    torch.cuda.synchronize()
+    assert b.n_leaf == 33 * 128 ** 3
+    codes = b.sorted_codes.view(torch.int32).to(torch.int64) & 0xFFFFFFFF
+    assert bool((codes[1:] >= codes[:-1]).all())
+    ids = b.aabb_ids.to(torch.int64)
+    seen = torch.zeros(b.n_leaf, dtype=torch.int32, device=cuda)
+    seen.index_add_(0, ids, torch.ones_like(ids, dtype=torch.int32))
+    assert bool((seen == 1).all())
+    del codes, ids, seen, b
+    f = UnstructuredField(m.ctrl_idx, m.field, m.order, device=cuda)
+    c = meshgen.CAMERA
+    w = 2048
+    cam = Camera(w, w, c["pos"], c["look_at"], c["up"], c["fov"])
+    light = PointLight.default(cam)
+    vol = Volume(g, f)
+    vol.samples(1000)
+    vol.use_lighting(True)
+    t = ColorTable()
+    for p in meshgen.TF_RGB:
+        t.add_point(p[0], p[1:])
+    for p in meshgen.TF_ALPHA:
+        t.add_alpha(*p)
+    vol.color_map().color_table(t)
+    vol.color_map().samples(1024)
+    vol.tol = 1e-5
+    imgs, samples = [], []
+    for coherent in (True, False):
+        vol.coherent = coherent
+        vol.guess_mode = L.GUESS_ELEM_CENTER
+        fb, st = vol.render(cam, [light], stats=True)
+        torch.cuda.synchronize()
+        imgs.append(fb.colors.cpu().numpy())      # before the background composite
+        samples.append(int(st[0].long().sum()))
+    a, pl = imgs
+    assert np.all((a >= 0) & (a <= 1))
+    d = np.abs(a - pl)
+    bad = np.any(d > 1.0 / 255.0, axis=-1)
+    print(f"C4: coherent vs plain march, {bad.sum()} of {w * w} pixels differ by > 1/255, "
+          f"max {d.max():.2e}; samples {samples[0]} vs {samples[1]}")
+    assert bad.mean() < 0.005
+    # the blobs cover part of the view; both marches take the same samples
+    assert (a[:, 3] > 0.01).mean() > 0.05
+    assert abs(samples[0] - samples[1]) < 1e-5 * samples[1]
