@@ -63,6 +63,10 @@ def parse():
     ap.add_argument("--profile-volume", type=int, default=0, metavar="N",
                     help="profiling run of the volume march alone: one coherent 1024^2 frame "
                          "of the order-3 warped mesh at N^3 elements, timed --steps times")
+    ap.add_argument("--profile-tet", type=int, default=0, metavar="N",
+                    help="profiling run of the tet locate alone: the tet workload's mesh "
+                         "(32^3 cubes x 6 order-2 tets), N uniform queries, one batched "
+                         "locate at a fixed launch shape")
     ap.add_argument("--profile", action="store_true",
                     help="profiling run: fixed launch shape, only the timed steps "
                          "(no tuning, plain/e2e/statistics/CPU legs)")
@@ -534,6 +538,25 @@ def volume_bench(dev, args, timed):
     }
 
 
+def profile_tet(dev, args):
+    """One batched locate of N queries in the tet workload's mesh (196,608
+    order-2 tets), block 256, all resident blocks, chunk 32, register rows."""
+    import torch
+    from devil_ray_b200 import _lib as L
+    from devil_ray_b200 import api, meshgen
+    m = meshgen.tet_warped_mesh(32, 2, 0.05, jitter=0.01, seed=9)
+    mesh = api.UnstructuredMesh(m.ctrl_idx, m.xyz, m.order, device=dev, shape=L.SHAPE_SIMPLEX)
+    mesh.get_bvh()
+    q = torch.as_tensor(meshgen.uniform_queries(args.profile_tet, 77), device=dev)
+    loc = api.BatchedLocator(mesh, tol=TOL, max_steps=MAX_STEPS,
+                             config=L.DrbLocateConfig(256, 0, 32, 1, 1))
+    cell, _ = loc.locate(q)
+    torch.cuda.synchronize()
+    print(json.dumps({"profile_tet": args.profile_tet,
+                      "located_fraction": float((cell >= 0).float().mean())}))
+    return 0
+
+
 def profile_volume(dev, args):
     """One coherent 1024^2 frame of the volume workload's mesh family at
     N^3 elements (order 3, warp 0.05, Gaussian field), 1000 samples."""
@@ -589,6 +612,8 @@ def main():
     torch.cuda.set_device(dev)
     if args.profile_volume:
         return profile_volume(dev, args)
+    if args.profile_tet:
+        return profile_tet(dev, args)
     from devil_ray_b200 import dist as D
     pg = D.init("nccl", timeout_s=120)  # None on one GPU
 

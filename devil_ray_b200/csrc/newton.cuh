@@ -43,6 +43,40 @@ DRB_D float norm_linf3 (float a, float b, float c)
 // (in reference space) of the returned x when the solve converged: the
 // volume renderer reuses it for the world-space gradient and for the next
 // sample's predictor instead of evaluating the geometry again.
+// One step of the hex iteration: clamp x to [0,1]^3, evaluate, LUP-solve
+// J dx = target - X(x), x += dx.  hex_newton loops over it; the step-wise
+// locate kernel calls it once per round, so both run the same arithmetic.
+template <int P, class CP>
+DRB_D void hex_step (const CP &cp, const float (&target)[3], float (&x)[3], LU3 &lu)
+{
+#pragma unroll
+  for (int d = 0; d < 3; ++d) x[d] = fminf (1.f, fmaxf (x[d], 0.f));
+  float X[3], Ju[3], Jv[3], Jw[3];
+  hex_eval_d<P, 3> (cp, x[0], x[1], x[2], X, Ju, Jv, Jw);
+  float dy[3], J[3][3], dx[3];
+#pragma unroll
+  for (int r = 0; r < 3; ++r)
+  {
+    dy[r] = target[r] - X[r];
+    J[r][0] = Ju[r];
+    J[r][1] = Jv[r];
+    J[r][2] = Jw[r];
+  }
+  lu.factor (J);
+  lu.solve (dy, dx);
+#pragma unroll
+  for (int d = 0; d < 3; ++d) x[d] += dx[d];
+}
+
+// Change of the iterate from prev (inf-norm over 3 coordinates), then prev = x.
+DRB_D float step_change3 (const float (&x)[3], float (&prev)[3])
+{
+  const float res = norm_linf3 (x[0] - prev[0], x[1] - prev[1], x[2] - prev[2]);
+#pragma unroll
+  for (int d = 0; d < 3; ++d) prev[d] = x[d];
+  return res;
+}
+
 template <int P, class CP>
 DRB_D bool hex_newton (const CP &cp, const float (&target)[3], float (&x)[3], float tol,
                        int max_steps, int &steps, LU3 &lu)
@@ -52,28 +86,9 @@ DRB_D bool hex_newton (const CP &cp, const float (&target)[3], float (&x)[3], fl
   steps = 0;
   while (steps < max_steps && !converged)
   {
-#pragma unroll
-    for (int d = 0; d < 3; ++d) x[d] = fminf (1.f, fmaxf (x[d], 0.f));
-    float X[3], Ju[3], Jv[3], Jw[3];
-    hex_eval_d<P, 3> (cp, x[0], x[1], x[2], X, Ju, Jv, Jw);
-    float dy[3], J[3][3], dx[3];
-#pragma unroll
-    for (int r = 0; r < 3; ++r)
-    {
-      dy[r] = target[r] - X[r];
-      J[r][0] = Ju[r];
-      J[r][1] = Jv[r];
-      J[r][2] = Jw[r];
-    }
-    lu.factor (J);
-    lu.solve (dy, dx);
-#pragma unroll
-    for (int d = 0; d < 3; ++d) x[d] += dx[d];
+    hex_step<P> (cp, target, x, lu);
     ++steps;
-    const float res = norm_linf3 (x[0] - prev[0], x[1] - prev[1], x[2] - prev[2]);
-    converged = res < tol;
-#pragma unroll
-    for (int d = 0; d < 3; ++d) prev[d] = x[d];
+    converged = step_change3 (x, prev) < tol;
   }
   return converged && is_inside_ref (x, tol);
 }
@@ -94,41 +109,58 @@ DRB_D bool hex_newton (const CP &cp, const float (&target)[3], float (&x)[3], fl
 // pos_tensor_element.tcc:49-61).  x[2] is left at -1, as the reference
 // leaves the third coordinate of a 2D Location.
 template <int P, class CP>
+DRB_D void quad_step (const CP &cp, const float (&target)[3], float (&x)[3], LU3 &lu)
+{
+  x[0] = fminf (1.f, fmaxf (x[0], 0.f));
+  x[1] = fminf (1.f, fmaxf (x[1], 0.f));
+  float X[3], Ju[3], Jv[3];
+  quad_eval_d<P, 3> (cp, x[0], x[1], X, Ju, Jv);
+  float dy[3], J[3][3], dx[3];
+#pragma unroll
+  for (int r = 0; r < 3; ++r)
+  {
+    dy[r] = target[r] - X[r];
+    J[r][0] = Ju[r];
+    J[r][1] = Jv[r];
+    J[r][2] = (r == 2) ? 1.f : 0.f;
+  }
+  lu.factor (J);
+  lu.solve (dy, dx);
+  x[0] += dx[0];
+  x[1] += dx[1];
+}
+
+// Change over the two reference coordinates of a quad, then prev = x.
+DRB_D float step_change2 (const float (&x)[3], float (&prev)[3])
+{
+  const float a = x[0] - prev[0], b = x[1] - prev[1];
+  prev[0] = x[0];
+  prev[1] = x[1];
+  return fmaxf (fmaxf (-a, a), fmaxf (-b, b));
+}
+
+DRB_D bool quad_inside (const float (&x)[3], float tol)
+{
+  const float mn = fminf (fminf (x[0], 2.f), x[1]);
+  const float mx = fmaxf (fmaxf (x[0], -1.f), x[1]);
+  return mn >= 0.f - tol && mx <= 1.f + tol;
+}
+
+template <int P, class CP>
 DRB_D bool quad_newton (const CP &cp, const float (&target)[3], float (&x)[3], float tol,
                         int max_steps, int &steps, LU3 &lu)
 {
-  float prev[2] = { x[0], x[1] };
+  float prev[3] = { x[0], x[1], x[2] };
   bool converged = false;
   steps = 0;
   while (steps < max_steps && !converged)
   {
-    x[0] = fminf (1.f, fmaxf (x[0], 0.f));
-    x[1] = fminf (1.f, fmaxf (x[1], 0.f));
-    float X[3], Ju[3], Jv[3];
-    quad_eval_d<P, 3> (cp, x[0], x[1], X, Ju, Jv);
-    float dy[3], J[3][3], dx[3];
-#pragma unroll
-    for (int r = 0; r < 3; ++r)
-    {
-      dy[r] = target[r] - X[r];
-      J[r][0] = Ju[r];
-      J[r][1] = Jv[r];
-      J[r][2] = (r == 2) ? 1.f : 0.f;
-    }
-    lu.factor (J);
-    lu.solve (dy, dx);
-    x[0] += dx[0];
-    x[1] += dx[1];
+    quad_step<P> (cp, target, x, lu);
     ++steps;
-    const float a = x[0] - prev[0], b = x[1] - prev[1];
-    converged = fmaxf (fmaxf (-a, a), fmaxf (-b, b)) < tol;
-    prev[0] = x[0];
-    prev[1] = x[1];
+    converged = step_change2 (x, prev) < tol;
   }
   x[2] = -1.f;
-  const float mn = fminf (fminf (x[0], 2.f), x[1]);
-  const float mx = fmaxf (fmaxf (x[0], -1.f), x[1]);
-  return converged && mn >= 0.f - tol && mx <= 1.f + tol;
+  return converged && quad_inside (x, tol);
 }
 
 // Control points of one element read through the packed element-major copy.

@@ -119,6 +119,28 @@ DRB_D bool is_inside_simplex (const float (&x)[3], float eps)
 }
 
 template <int P, class CP>
+DRB_D void tet_step (const CP &cp, const float (&target)[3], float (&x)[3], LU3 &lu)
+{
+#pragma unroll
+  for (int d = 0; d < 3; ++d) x[d] = fminf (1.f, fmaxf (x[d], 0.f));
+  float X[3], Ju[3], Jv[3], Jw[3];
+  tet_eval_d<P, 3> (cp, x[0], x[1], x[2], X, Ju, Jv, Jw);
+  float dy[3], J[3][3], dx[3];
+#pragma unroll
+  for (int r = 0; r < 3; ++r)
+  {
+    dy[r] = target[r] - X[r];
+    J[r][0] = Ju[r];
+    J[r][1] = Jv[r];
+    J[r][2] = Jw[r];
+  }
+  lu.factor (J);
+  lu.solve (dy, dx);
+#pragma unroll
+  for (int d = 0; d < 3; ++d) x[d] += dx[d];
+}
+
+template <int P, class CP>
 DRB_D bool tet_newton (const CP &cp, const float (&target)[3], float (&x)[3], float tol,
                        int max_steps, int &steps, LU3 &lu)
 {
@@ -127,28 +149,9 @@ DRB_D bool tet_newton (const CP &cp, const float (&target)[3], float (&x)[3], fl
   steps = 0;
   while (steps < max_steps && !converged)
   {
-#pragma unroll
-    for (int d = 0; d < 3; ++d) x[d] = fminf (1.f, fmaxf (x[d], 0.f));
-    float X[3], Ju[3], Jv[3], Jw[3];
-    tet_eval_d<P, 3> (cp, x[0], x[1], x[2], X, Ju, Jv, Jw);
-    float dy[3], J[3][3], dx[3];
-#pragma unroll
-    for (int r = 0; r < 3; ++r)
-    {
-      dy[r] = target[r] - X[r];
-      J[r][0] = Ju[r];
-      J[r][1] = Jv[r];
-      J[r][2] = Jw[r];
-    }
-    lu.factor (J);
-    lu.solve (dy, dx);
-#pragma unroll
-    for (int d = 0; d < 3; ++d) x[d] += dx[d];
+    tet_step<P> (cp, target, x, lu);
     ++steps;
-    const float res = norm_linf3 (x[0] - prev[0], x[1] - prev[1], x[2] - prev[2]);
-    converged = res < tol;
-#pragma unroll
-    for (int d = 0; d < 3; ++d) prev[d] = x[d];
+    converged = step_change3 (x, prev) < tol;
   }
   return converged && is_inside_simplex (x, tol);
 }

@@ -245,7 +245,8 @@ typedef struct drb_locate_config
                             step; 1 = registers (orders <= 2; fewer loads,
                             more registers); 2 = shared memory: the warp
                             stages each distinct element row of its lanes'
-                            candidates once (packed meshes; falls back to 0) */
+                            candidates once (packed hex meshes; falls back
+                            to 0) */
 } drb_locate_config;
 
 /* Batched point location, same results as drb_locate (same traversal order
