@@ -1,6 +1,7 @@
 // Drives the C++ host interface with a tet mesh the way a Devil Ray user
 // does: UnstructuredMesh<Tet*> and UnstructuredField<TetScalar*> in a
-// DataSet/Collection, Mesh::locate and PointLocation.  Raw binary inputs and
+// DataSet/Collection, Mesh::locate, PointLocation and Volume::integrate.
+// Raw binary inputs and
 // outputs, compared with the reference oracle by tests/test_tet_gpu.py.
 //
 //   t_dray_b200_tet <dir>
@@ -8,8 +9,13 @@
 //                               float xyz[3*n_ctrl]; float field[n_ctrl]
 //                               (nd = (order+1)(order+2)(order+3)/6)
 //            <dir>/points.bin   int32 n; float pts[3n]
+//            <dir>/render.bin   (optional) int32 w, h, samples; float cam9[9], fov;
+//                               float light13[13]; int32 n_rgb; float rgb[4 n_rgb];
+//                               int32 n_alpha; float alpha[2 n_alpha]
 //     writes <dir>/locate.bin   int32 cell[n]; float ref[3n]
 //            <dir>/pointloc.bin float value[n]
+//            <dir>/volume.bin   float rgba[4wh]  (Volume::integrate + save
+//                               compositing, when render.bin is given)
 #include <dray/dray_b200.hpp>
 
 #include <fstream>
@@ -107,6 +113,59 @@ int main (int argc, char **argv)
     {
       std::ofstream fo (dir + "/pointloc.bin", std::ios::binary);
       wr (fo, res.m_values[0].get_host_ptr_const (), (size_t)n);
+    }
+
+    // Volume::integrate over the tet mesh (dispatch_3d's TetMesh case)
+    std::ifstream fr (dir + "/render.bin", std::ios::binary);
+    if (fr)
+    {
+      int32 whs[3];
+      rd (fr, whs, 3);
+      float cam9[9], fov, light13[13];
+      rd (fr, cam9, 9);
+      rd (fr, &fov, 1);
+      rd (fr, light13, 13);
+      int32 nrgb = 0, nal = 0;
+      rd (fr, &nrgb, 1);
+      std::vector<float> rgb ((size_t)4 * nrgb);
+      rd (fr, rgb.data (), rgb.size ());
+      rd (fr, &nal, 1);
+      std::vector<float> al ((size_t)2 * nal);
+      rd (fr, al.data (), al.size ());
+      ColorTable table;
+      for (int i = 0; i < nrgb; ++i)
+        table.add_point (rgb[4 * i], make_vec3f (rgb[4 * i + 1], rgb[4 * i + 2], rgb[4 * i + 3]));
+      for (int i = 0; i < nal; ++i) table.add_alpha (al[2 * i], al[2 * i + 1]);
+      Camera cam;
+      cam.set_width (whs[0]);
+      cam.set_height (whs[1]);
+      cam.set_pos (make_vec3f (cam9[0], cam9[1], cam9[2]));
+      cam.set_look_at (make_vec3f (cam9[3], cam9[4], cam9[5]));
+      cam.set_up (make_vec3f (cam9[6], cam9[7], cam9[8]));
+      cam.set_fov (fov);
+      PointLight light;
+      for (int k = 0; k < 3; ++k)
+      {
+        light.m_pos[k] = light13[k];
+        light.m_amb[k] = light13[3 + k];
+        light.m_diff[k] = light13[6 + k];
+        light.m_spec[k] = light13[9 + k];
+      }
+      light.m_spec_pow = light13[12];
+      Array<PointLight> lights (&light, 1);
+      Array<Ray> rays;
+      cam.create_rays (rays);
+      Volume vol (col);
+      vol.field ("f");
+      vol.samples (whs[2]);
+      vol.use_lighting (true);
+      vol.color_map ().color_table (table);
+      vol.m_locate.guess_mode = 0;
+      Array<VolumePartial> parts = vol.integrate (rays, lights);
+      if (parts.size () == 0) throw std::runtime_error ("no partials");
+      Framebuffer fb = Volume::composite (parts, whs[0], whs[1]);
+      std::ofstream fo (dir + "/volume.bin", std::ios::binary);
+      wr (fo, (const float *)fb.colors ().get_host_ptr_const (), (size_t)4 * whs[0] * whs[1]);
     }
   }
   catch (const std::exception &e)

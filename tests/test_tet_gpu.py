@@ -227,6 +227,22 @@ def test_cpp_tet_mesh_interface(cuda, ref, tmp_path, p):
     with open(tmp_path / "points.bin", "wb") as f:
         np.array([pts.shape[0]], np.int32).tofile(f)
         pts.tofile(f)
+    from devil_ray_b200.render import Camera, PointLight
+    cam_d = dict(pos=(2.5, 2.5, 2.5), look_at=(0.5, 0.5, 0.5), up=(0.0, 1.0, 0.0), fov=30.0)
+    w, samples = 96, 300
+    cam = Camera(w, w, cam_d["pos"], cam_d["look_at"], cam_d["up"], cam_d["fov"])
+    light13 = PointLight.default(cam).as13()
+    rgb = np.array(meshgen.TF_RGB, np.float32)
+    alpha = np.array(meshgen.TF_ALPHA, np.float32)
+    cam9 = np.array([*cam_d["pos"], *cam_d["look_at"], *cam_d["up"]], np.float32)
+    with open(tmp_path / "render.bin", "wb") as f:
+        np.array([w, w, samples], np.int32).tofile(f)
+        np.array([*cam9, cam_d["fov"]], np.float32).tofile(f)
+        np.asarray(light13, np.float32).reshape(13).tofile(f)
+        np.array([rgb.shape[0]], np.int32).tofile(f)
+        rgb.tofile(f)
+        np.array([alpha.shape[0]], np.int32).tofile(f)
+        alpha.tofile(f)
     r = subprocess.run([str(exe), str(tmp_path)], capture_output=True, text=True, timeout=300)
     assert r.returncode == 0, r.stdout + r.stderr
     n = pts.shape[0]
@@ -250,6 +266,14 @@ def test_cpp_tet_mesh_interface(cuda, ref, tmp_path, p):
         sel = cell == e
         X, _ = restate.tet_eval_d(p, m.field[conn[e]].astype(np.float64), refp[sel].astype(np.float64))
         assert np.abs(vals[sel] - X[:, 0]).max() < 1e-4
+    # Volume::integrate + composite over the tet mesh == the reference's image
+    img = np.fromfile(tmp_path / "volume.bin", np.float32).reshape(w, w, 4)
+    if p < 3:
+        rimg, _ = ref.RefTetMesh(p, m.ctrl_idx, m.xyz, m.field).volume(
+            w, w, cam9, cam_d["fov"], samples, True, 1024, rgb, alpha, light13[None])
+        d = np.abs(img - rimg)
+        assert np.any(d > 1.0 / 255.0, axis=-1).mean() < 0.005
+    assert img[..., 3].max() > 0.1
 
 
 def _tet_volume(cuda, m, w, samples, lighting, coherent):
