@@ -163,7 +163,7 @@ class UnstructuredMesh:
     def hull_planes(self, stream=None):
         """Tets: the bounding planes of every element (drb_tet_hull_planes),
         built once; the batched locate filters its candidates with them."""
-        if self._hull is None and self.shape == L.SHAPE_SIMPLEX:
+        if self._hull is None and self.shape == L.SHAPE_SIMPLEX and self.dim == 3:
             hp = torch.empty((max(self.n_elem, 1), 20), dtype=torch.float32, device=self.device)
             d = self.desc()
             L.check(L.lib().drb_tet_hull_planes(C.byref(d), _ptr(hp), _stream(stream)),
@@ -186,7 +186,7 @@ class UnstructuredMesh:
         if self._bvh is None:
             self._bvh = self.build_bvh(stream, keep_codes)
             self._bvh.widen(stream)
-            if self.shape == L.SHAPE_SIMPLEX:
+            if self.shape == L.SHAPE_SIMPLEX and self.dim == 3:
                 self.hull_planes(stream)
         return self._bvh
 

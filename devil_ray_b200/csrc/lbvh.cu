@@ -518,6 +518,182 @@ tet_subbox_kernel (const int *__restrict__ ctrl_idx, const float *__restrict__ x
   reduce_scene_bounds (bmn, bmx, s_bounds, warp, lane, bounds_ord);
 }
 
+// ---- simplex faces (triangles): 17 sub-boxes per triangle ----
+//
+// The same split with dim 2: the reference sub-triangle is three vertices
+// (u and v axis vertices, then the origin), the longest of its three edges
+// is halved, and split_inplace<2,Simplex> (elem_ops.hpp:1216-1250) runs de
+// Casteljau along it on the rows parallel to it.  Its triangle index
+// (cartesian_to_tri_idx) is the evaluators' layout, so these boxes match the
+// reference's at every order.
+
+constexpr int kTriRefFloats = 6; // SubRef<2,Simplex>: three vertices
+
+template <int P>
+DRB_D void tri_split_line (float *cps, int v0, int v1, int g, int comp)
+{
+  const int v2 = 3 - v0 - v1;
+  const int m = P - g;
+  int ids[P + 1];
+  float d[P + 1];
+#pragma unroll
+  for (int a = 0; a <= P; ++a)
+  {
+    if (a > m) break;
+    int b[3];
+    b[v0] = a;
+    b[v1] = m - a;
+    b[v2] = g;
+    ids[a] = tri_index (b[0], b[1], P);
+    d[a] = cps[3 * ids[a] + comp];
+  }
+#pragma unroll
+  for (int nu = P; nu >= 1; --nu)
+  {
+    if (nu > m) continue;
+#pragma unroll
+    for (int a = P; a >= 1; --a)
+    {
+      if (a > m || a < m - nu + 1) continue;
+      d[a] = __fadd_rn (__fmul_rn (d[a], 0.5f), __fmul_rn (d[a - 1], 0.5f));
+    }
+  }
+#pragma unroll
+  for (int a = 0; a <= P; ++a)
+  {
+    if (a > m) break;
+    cps[3 * ids[a] + comp] = d[a];
+  }
+}
+
+template <int P>
+__global__ void __launch_bounds__ (kSubboxWarps * kWarp)
+tri_subbox_kernel (const int *__restrict__ ctrl_idx, const float *__restrict__ xyz, int n_elem,
+                   float *__restrict__ aabbs6, int *__restrict__ prim_ids,
+                   float *__restrict__ ref_out, unsigned *__restrict__ bounds_ord)
+{
+  constexpr int ND = tri_dofs<P> ();
+  constexpr int NB = SplitCount<2>::boxes;
+  constexpr int CPW = NB * ND * 3;
+  extern __shared__ float smem[];
+  __shared__ float s_bounds[kSubboxWarps][6];
+
+  const int warp = threadIdx.x >> 5;
+  const int lane = threadIdx.x & 31;
+  float *cps = smem + warp * CPW;
+  float *boxes = smem + kSubboxWarps * CPW + warp * NB * 6;
+  float *refs = smem + kSubboxWarps * (CPW + NB * 6) + warp * NB * kTriRefFloats;
+
+  const int el = blockIdx.x * kSubboxWarps + warp;
+  float bmn[3] = { INFINITY, INFINITY, INFINITY };
+  float bmx[3] = { -INFINITY, -INFINITY, -INFINITY };
+
+  if (el < n_elem)
+  {
+    for (int t = lane; t < ND * 3; t += kWarp)
+    {
+      const int i = t / 3;
+      const int k = t - 3 * i;
+      cps[t] = __ldg (xyz + 3 * (size_t)__ldg (ctrl_idx + (size_t)el * ND + i) + k);
+    }
+    // ref_universe<Simplex> in 2D: (1,0), (0,1), then the origin
+    if (lane < kTriRefFloats) refs[lane] = (lane == 0 || lane == 3) ? 1.f : 0.f;
+    __syncwarp ();
+    warp_hull<ND> (cps, boxes, lane);
+    __syncwarp ();
+
+    for (int count = 1; count < NB; ++count)
+    {
+      int max_id = 0;
+      float max_measure = box_measure (boxes);
+      for (int b = 1; b < count; ++b)
+      {
+        const float mm = box_measure (boxes + 6 * b);
+        if (mm > max_measure)
+        {
+          max_id = b;
+          max_measure = mm;
+        }
+      }
+      const float *rm = refs + max_id * kTriRefFloats;
+      int dv = 0, tv = 1;
+      float max_l2 = 0.f;
+      for (int a = 0; a < 2; ++a)
+        for (int b = a + 1; b < 3; ++b)
+        {
+          const float e0 = __fsub_rn (rm[2 * a], rm[2 * b]);
+          const float e1 = __fsub_rn (rm[2 * a + 1], rm[2 * b + 1]);
+          const float l2 = __fadd_rn (__fmul_rn (e0, e0), __fmul_rn (e1, e1));
+          if (l2 > max_l2)
+          {
+            dv = a;
+            tv = b;
+            max_l2 = l2;
+          }
+        }
+      __syncwarp ();
+      if (lane == 0)
+      {
+        float *rmw = refs + max_id * kTriRefFloats;
+        float *rd = refs + count * kTriRefFloats;
+        float sp[2];
+#pragma unroll
+        for (int k = 0; k < 2; ++k)
+          sp[k] = __fadd_rn (__fmul_rn (rmw[2 * tv + k], 0.5f), __fmul_rn (rmw[2 * dv + k], 0.5f));
+#pragma unroll
+        for (int q = 0; q < kTriRefFloats; ++q) rd[q] = rmw[q];
+#pragma unroll
+        for (int k = 0; k < 2; ++k)
+        {
+          rmw[2 * dv + k] = sp[k];
+          rd[2 * tv + k] = sp[k];
+        }
+      }
+      float *mother = cps + max_id * ND * 3;
+      float *dghter = cps + count * ND * 3;
+      for (int t = lane; t < ND * 3; t += kWarp) dghter[t] = mother[t];
+      __syncwarp ();
+      // P lines (fixed exponent g < P of the third vertex) x 3 components
+      for (int item = lane; item < 2 * P * 3; item += kWarp)
+      {
+        const bool is_mother = item < P * 3;
+        const int it = is_mother ? item : item - P * 3;
+        const int g = it / 3;
+        const int comp = it - 3 * g;
+        if (is_mother) tri_split_line<P> (mother, dv, tv, g, comp);
+        else tri_split_line<P> (dghter, tv, dv, g, comp);
+      }
+      __syncwarp ();
+      warp_hull<ND> (mother, boxes + 6 * max_id, lane);
+      warp_hull<ND> (dghter, boxes + 6 * count, lane);
+      __syncwarp ();
+    }
+
+    const float s = (float)1.000001;
+    for (int b = lane; b < NB; b += kWarp)
+    {
+      float bx[6];
+#pragma unroll
+      for (int q = 0; q < 6; ++q) bx[q] = boxes[6 * b + q];
+#pragma unroll
+      for (int k = 0; k < 3; ++k) scale_range (bx[2 * k], bx[2 * k + 1], s);
+      const size_t o = (size_t)el * NB + b;
+#pragma unroll
+      for (int q = 0; q < 6; ++q) aabbs6[6 * o + q] = bx[q];
+      prim_ids[o] = el;
+#pragma unroll
+      for (int q = 0; q < kTriRefFloats; ++q) ref_out[kTriRefFloats * o + q] = refs[kTriRefFloats * b + q];
+#pragma unroll
+      for (int k = 0; k < 3; ++k)
+      {
+        bmn[k] = fminf (bmn[k], bx[2 * k]);
+        bmx[k] = fmaxf (bmx[k], bx[2 * k + 1]);
+      }
+    }
+  }
+  reduce_scene_bounds (bmn, bmx, s_bounds, warp, lane, bounds_ord);
+}
+
 __global__ void bounds_init_kernel (unsigned *bounds_ord)
 {
   const int q = threadIdx.x;
@@ -762,6 +938,20 @@ template <int P> size_t tet_subbox_smem ()
 }
 
 template <int P>
+int launch_tri_subbox (const drb_mesh *m, float *aabbs6, int *prim_ids, float *ref_boxes,
+                       unsigned *bounds_ord, cudaStream_t s)
+{
+  constexpr int NB = SplitCount<2>::boxes;
+  const size_t smem = sizeof (float) * kSubboxWarps * (NB * tri_dofs<P> () * 3 + NB * 6 + NB * kTriRefFloats);
+  cudaFuncSetAttribute (tri_subbox_kernel<P>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  const int blocks = div_up (m->n_elem, kSubboxWarps);
+  if (blocks > 0)
+    tri_subbox_kernel<P><<<blocks, kSubboxWarps * kWarp, smem, s>>> (
+    m->ctrl_idx, m->values, m->n_elem, aabbs6, prim_ids, ref_boxes, bounds_ord);
+  return check_launch ("tri_subbox_kernel");
+}
+
+template <int P>
 int launch_tet_subbox (const drb_mesh *m, float *aabbs6, int *prim_ids, float *ref_boxes,
                        unsigned *bounds_ord, cudaStream_t s)
 {
@@ -798,9 +988,15 @@ int dispatch_subbox (const drb_mesh *m, float *aabbs6, int *prim_ids, float *ref
     if (m->order == 2) return launch_tet_subbox<2> (m, aabbs6, prim_ids, ref_boxes, bounds_ord, s);
     if (m->order == 3) return launch_tet_subbox<3> (m, aabbs6, prim_ids, ref_boxes, bounds_ord, s);
   }
+  else if (m->shape == DRB_SHAPE_SIMPLEX && m->dim == 2)
+  {
+    if (m->order == 1) return launch_tri_subbox<1> (m, aabbs6, prim_ids, ref_boxes, bounds_ord, s);
+    if (m->order == 2) return launch_tri_subbox<2> (m, aabbs6, prim_ids, ref_boxes, bounds_ord, s);
+    if (m->order == 3) return launch_tri_subbox<3> (m, aabbs6, prim_ids, ref_boxes, bounds_ord, s);
+  }
   else if (m->shape != DRB_SHAPE_TENSOR)
   {
-    set_last_error ("subbox: simplex meshes must be tets (dim 3)");
+    set_last_error ("subbox: unknown element shape");
     return DRB_ERR_UNSUPPORTED;
   }
   else if (m->dim == 3)
@@ -823,9 +1019,9 @@ int validate_mesh (const drb_mesh *m, int want_ncomp)
 {
   if (!m) { set_last_error ("mesh is NULL"); return DRB_ERR_INVALID_ARG; }
   if (m->dim != 2 && m->dim != 3) { set_last_error ("mesh dim must be 2 or 3"); return DRB_ERR_INVALID_ARG; }
-  if (m->shape != DRB_SHAPE_TENSOR && !(m->shape == DRB_SHAPE_SIMPLEX && m->dim == 3))
+  if (m->shape != DRB_SHAPE_TENSOR && m->shape != DRB_SHAPE_SIMPLEX)
   {
-    set_last_error ("mesh shape must be tensor, or simplex with dim 3 (tets)");
+    set_last_error ("mesh shape must be tensor or simplex");
     return DRB_ERR_UNSUPPORTED;
   }
   if (m->order < 1 || m->order > 3) { set_last_error ("mesh order must be 1..3"); return DRB_ERR_UNSUPPORTED; }
@@ -848,7 +1044,8 @@ int mesh_nd (int dim, int order)
 
 int mesh_nd (const drb_mesh *m)
 {
-  return m->shape == DRB_SHAPE_SIMPLEX ? tet_dofs (m->order) : mesh_nd (m->dim, m->order);
+  if (m->shape == DRB_SHAPE_SIMPLEX) return m->dim == 2 ? tri_dofs (m->order) : tet_dofs (m->order);
+  return mesh_nd (m->dim, m->order);
 }
 
 } // namespace drb
@@ -866,6 +1063,7 @@ extern "C" int drb_elem_dofs (int shape, int dim, int order)
   if (order < 1 || order > 3) return -1;
   if (shape == DRB_SHAPE_TENSOR && (dim == 2 || dim == 3)) return mesh_nd (dim, order);
   if (shape == DRB_SHAPE_SIMPLEX && dim == 3) return tet_dofs (order);
+  if (shape == DRB_SHAPE_SIMPLEX && dim == 2) return tri_dofs (order);
   return -1;
 }
 
@@ -983,12 +1181,14 @@ extern "C" int drb_lbvh_build (const drb_mesh *mesh, drb_bvh *bvh, unsigned *sor
     const float ref3[12] = { 0, 0, 0, 1, 1, 1, 0, 0, 0, 1, 1, 1 };
     // ref_universe<Simplex>: axis vertices, then the origin
     const float tet_ref[24] = { 1, 0, 0, 0, 1, 0, 0, 0, 1, 0, 0, 0, 1, 0, 0, 0, 1, 0, 0, 0, 1, 0, 0, 0 };
+    const float tri_ref[12] = { 1, 0, 0, 1, 0, 0, 1, 0, 0, 1, 0, 0 };
     const bool simplex = mesh->shape == DRB_SHAPE_SIMPLEX;
     cudaMemcpyAsync (bvh->inner_nodes, node, sizeof (node), cudaMemcpyHostToDevice, s);
     cudaMemcpyAsync (bvh->leaf_nodes, leaf, sizeof (leaf), cudaMemcpyHostToDevice, s);
     cudaMemcpyAsync (bvh->aabb_ids, ids, sizeof (ids), cudaMemcpyHostToDevice, s);
-    cudaMemcpyAsync (bvh->ref_boxes, simplex ? tet_ref : ref3,
-                     sizeof (float) * (simplex ? 24 : 4 * mesh->dim), cudaMemcpyHostToDevice, s);
+    cudaMemcpyAsync (bvh->ref_boxes, simplex ? (mesh->dim == 3 ? tet_ref : tri_ref) : ref3,
+                     sizeof (float) * (simplex ? 4 * mesh->dim * (mesh->dim + 1) / 2 : 4 * mesh->dim),
+                     cudaMemcpyHostToDevice, s);
     if (sorted_codes) cudaMemsetAsync (sorted_codes, 0, sizeof (unsigned) * 2, s);
     const float empty[6] = { INFINITY, -INFINITY, INFINITY, -INFINITY, INFINITY, -INFINITY };
     for (int q = 0; q < 6; ++q) bvh->bounds[q] = empty[q];

@@ -103,6 +103,74 @@ DRB_D void tet_eval_d (const CP &cp, float u, float v, float w, float (&X)[NC], 
   }
 }
 
+// ---- triangles (the faces of tets) ----
+DRB_HD constexpr int tri_dofs (int p) { return (p + 1) * (p + 2) / 2; }
+template <int P> constexpr int tri_dofs () { return (P + 1) * (P + 2) / 2; }
+
+// Position of multi-index (i, j) in an order-p triangle's dof list: i
+// fastest, then j (cartesian_to_tri_idx, elem_ops.hpp:19-30).
+DRB_HD constexpr int tri_index (int i, int j, int p) { return (2 * p + 3 - j) * j / 2 + i; }
+
+// X(u,v) and its derivatives for an order-P triangle, with t = 1 - u - v
+// and B the order P-1 basis: X = sum_a B_a (u C[a+e_u] + v C[a+e_v] +
+// t C[a+e_t]), dX/du = P sum_a B_a (C[a+e_u] - C[a+e_t]), likewise v
+// (Element_impl<2,ncomp,Simplex,*>::eval_d, elem_ops.hpp:700-780,
+// pos_simplex_element.tcc:510-600).
+template <int P, int NC, class CP>
+DRB_D void tri_eval_d (const CP &cp, float u, float v, float (&X)[NC], float (&Ju)[NC],
+                       float (&Jv)[NC])
+{
+  const float t = 1.f - (u + v);
+  float pu[P], pv[P], pt[P];
+  pu[0] = pv[0] = pt[0] = 1.f;
+#pragma unroll
+  for (int q = 1; q < P; ++q)
+  {
+    pu[q] = pu[q - 1] * u;
+    pv[q] = pv[q - 1] * v;
+    pt[q] = pt[q - 1] * t;
+  }
+#pragma unroll
+  for (int c = 0; c < NC; ++c) X[c] = Ju[c] = Jv[c] = 0.f;
+#pragma unroll
+  for (int j = 0; j < P; ++j)
+#pragma unroll
+    for (int i = 0; i < P - j; ++i)
+    {
+      const int l = P - 1 - i - j;
+      const float B = multinomial (P - 1, i, j, 0) * pu[i] * pv[j] * pt[l];
+      const int it = tri_index (i, j, P);
+      const int iu = tri_index (i + 1, j, P);
+      const int iv = tri_index (i, j + 1, P);
+#pragma unroll
+      for (int c = 0; c < NC; ++c)
+      {
+        const float ct = cp (it, c), cu = cp (iu, c), cv = cp (iv, c);
+        X[c] += B * (u * cu + v * cv + t * ct);
+        Ju[c] += B * (cu - ct);
+        Jv[c] += B * (cv - ct);
+      }
+    }
+#pragma unroll
+  for (int c = 0; c < NC; ++c)
+  {
+    Ju[c] *= (float)P;
+    Jv[c] *= (float)P;
+  }
+}
+
+// TriRefSpace<2>::is_inside (pos_simplex_element.tcc:479-491), eps =
+// epsilon<Float>() = 1e-4 when called without one.
+DRB_D bool is_inside_tri (float u, float v, float eps)
+{
+  float mn = fminf (u, 2.f);
+  float t = __fsub_rn (1.f, u);
+  mn = fminf (v, mn);
+  t = __fsub_rn (t, v);
+  mn = fminf (t, mn);
+  return mn >= 0.f - eps;
+}
+
 // TriRefSpace<3>::is_inside(ref, eps) (pos_simplex_element.tcc:493-505).
 DRB_D bool is_inside_simplex (const float (&x)[3], float eps)
 {

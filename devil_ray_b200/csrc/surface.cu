@@ -19,6 +19,7 @@
 #include "drb_common.cuh"
 #include "drb_internal.h"
 #include "newton.cuh"
+#include "simplex.cuh"
 
 namespace drb
 {
@@ -54,6 +55,30 @@ __global__ void extract_faces_kernel (const int *__restrict__ ctrl_idx, int n_el
     int t[4] = { c[idx[f][0]], c[idx[f][1]], c[idx[f][2]], c[idx[f][3]] };
     sort4 (t);
     faces[(size_t)6 * e + f] = make_int4 (t[0], t[1], t[2], t[3]);
+  }
+}
+
+// extract_faces (Tet -> Simplex), mesh_utils.cpp:282-344: four sorted corner
+// triples per tet (fourth component -1), face f opposite corner f of
+// (u = 1, v = 1, w = 1, origin).
+__global__ void extract_tet_faces_kernel (const int *__restrict__ ctrl_idx, int n_elem, int p,
+                                          int4 *__restrict__ faces)
+{
+  const int e = blockIdx.x * blockDim.x + threadIdx.x;
+  if (e >= n_elem) return;
+  const int nd = tet_dofs (p);
+  const int *el = ctrl_idx + (size_t)nd * e;
+  const int c[4] = { el[tet_index (p, 0, 0, p)], el[tet_index (0, p, 0, p)],
+                     el[tet_index (0, 0, p, p)], el[0] };
+  const int idx[4][3] = { { 1, 2, 3 }, { 0, 2, 3 }, { 0, 1, 3 }, { 0, 1, 2 } };
+#pragma unroll
+  for (int f = 0; f < 4; ++f)
+  {
+    int t[3] = { c[idx[f][0]], c[idx[f][1]], c[idx[f][2]] };
+#define DRB_SWAP(a, b) if (t[a] > t[b]) { const int q = t[a]; t[a] = t[b]; t[b] = q; }
+    DRB_SWAP (0, 1) DRB_SWAP (1, 2) DRB_SWAP (0, 1)
+#undef DRB_SWAP
+    faces[(size_t)4 * e + f] = make_int4 (t[0], t[1], t[2], -1);
   }
 }
 
@@ -125,6 +150,56 @@ __global__ void face_dofs_kernel (const int *__restrict__ perm, const int *__res
   }
 }
 
+// reconstruct + extract_face_dofs<Simplex> (mesh_boundary.cpp:102-185): the
+// triangle's dofs (ii, jj), i fastest, are the tet dofs with the face's
+// opposite exponent 0, the next two following the face's axes and the
+// third the rest.  The reference looks the tet dofs up with
+// cartesian_to_tet_idx, which for orders >= 2 is not the layout the
+// evaluators use (see lbvh.cu); here they come from the layered index, so
+// at order 1 the faces are the reference's and at orders 2-3 they are the
+// tets' own boundary.
+__global__ void tet_face_dofs_kernel (const int *__restrict__ perm, const int *__restrict__ flags,
+                                      const int *__restrict__ offs, int n, int p,
+                                      const int *__restrict__ ctrl_idx,
+                                      const int *__restrict__ field_idx, int *__restrict__ out_idx,
+                                      int *__restrict__ out_field_idx, int *__restrict__ elid_faceid)
+{
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n || !flags[i]) return;
+  const int face_idx = offs[i];
+  const int flat = perm[i];
+  const int el = flat / 4;
+  const int faceid = flat - 4 * el;
+  const int nd3 = tet_dofs (p), nd2 = tri_dofs (p);
+  int pi[3];
+  switch (faceid)
+  {
+  case 0: pi[0] = 1; pi[1] = 2; pi[2] = 3; break;
+  case 1: pi[0] = 0; pi[1] = 2; pi[2] = 3; break;
+  case 2: pi[0] = 0; pi[1] = 1; pi[2] = 3; break;
+  default: pi[0] = 0; pi[1] = 1; pi[2] = 2; break;
+  }
+  const size_t orig = (size_t)el * nd3;
+  const size_t outo = (size_t)face_idx * nd2;
+  int b[4];
+  b[faceid] = 0;
+  for (int jj = 0; jj <= p; ++jj)
+    for (int ii = 0; ii <= p - jj; ++ii)
+    {
+      b[pi[1]] = jj;
+      b[pi[0]] = ii;
+      b[pi[2]] = p - ii - jj;
+      const size_t src = orig + tet_index (b[0], b[1], b[2], p);
+      out_idx[outo + tri_index (ii, jj, p)] = ctrl_idx[src];
+      if (out_field_idx) out_field_idx[outo + tri_index (ii, jj, p)] = field_idx[src];
+    }
+  if (elid_faceid)
+  {
+    elid_faceid[2 * face_idx] = el;
+    elid_faceid[2 * face_idx + 1] = faceid;
+  }
+}
+
 // -------------------------------------------------------------- surface --
 
 struct SurfParams
@@ -141,7 +216,9 @@ struct SurfParams
   int max_steps;
 };
 
-template <int P, class CP>
+// TRI: a triangle face (Element<2,3,Simplex,P>), evaluated by tri_eval_d and
+// tested with TriRefSpace<2>::is_inside; else a quad.
+template <int P, bool TRI, class CP>
 DRB_D bool face_newton (const CP &cp, const Ray &ray, float (&x)[2], float &t, float tol,
                         int max_steps, int &steps)
 {
@@ -156,7 +233,8 @@ DRB_D bool face_newton (const CP &cp, const Ray &ray, float (&x)[2], float &t, f
     x[0] = fminf (1.f, fmaxf (x[0], 0.f));
     x[1] = fminf (1.f, fmaxf (x[1], 0.f));
     float X[3], Ju[3], Jv[3];
-    quad_eval_d<P, 3> (cp, x[0], x[1], X, Ju, Jv);
+    if (TRI) tri_eval_d<P, 3> (cp, x[0], x[1], X, Ju, Jv);
+    else quad_eval_d<P, 3> (cp, x[0], x[1], X, Ju, Jv);
     float J[3][3], dy[3], dx[3];
 #pragma unroll
     for (int r = 0; r < 3; ++r)
@@ -179,8 +257,9 @@ DRB_D bool face_newton (const CP &cp, const Ray &ray, float (&x)[2], float &t, f
     prev[1] = x[1];
     prev[2] = t;
   }
-  // QuadRefSpace::is_inside without eps uses epsilon<Float>() = 1e-4
-  const bool inside = fminf (x[0], x[1]) >= 0.f - kEpsilon && fmaxf (x[0], x[1]) <= 1.f + kEpsilon;
+  // QuadRefSpace / TriRefSpace::is_inside without eps use epsilon<Float>() = 1e-4
+  const bool inside = TRI ? is_inside_tri (x[0], x[1], kEpsilon)
+                          : fminf (x[0], x[1]) >= 0.f - kEpsilon && fmaxf (x[0], x[1]) <= 1.f + kEpsilon;
   return converged && inside && ray.near_t <= t && t < ray.far_t;
 }
 
@@ -299,6 +378,34 @@ DRB_D void ld_ref_point (V3 v00, V3 v11, float alpha, float beta, V3 e01, V3 e03
   }
 }
 
+// intersect_tri (rendering/low_order_intersectors.hpp:228-277, Moller and
+// Trumbore), used by FaceIntersector<Tri_P1> (rendering/surface.cpp:205-250):
+// distance (INFINITY on a miss) and (u, v) along b - a and c - a, every
+// operation rounded in the reference's order.
+DRB_D float mt_intersect (V3 a, V3 b, V3 c, V3 o, V3 d, float &u, float &v)
+{
+  const float eps2 = 0.0001f;
+  float distance = INFINITY;
+  const V3 e1 = vsub (b, a);
+  const V3 e2 = vsub (c, a);
+  const V3 p = vcross (d, e2);
+  float dot = vdot (e1, p);
+  if (dot != 0.f)
+  {
+    dot = __fdiv_rn (1.f, dot);
+    const V3 t = vsub (o, a);
+    u = __fmul_rn (vdot (t, p), dot);
+    if (u >= (0.f - eps2) && u <= (1.f + eps2))
+    {
+      const V3 q = vcross (t, e1);
+      v = __fmul_rn (vdot (d, q), dot);
+      if (v >= (0.f - eps2) && v <= (1.f + eps2) && !(__fadd_rn (u, v) > 1.f))
+        distance = __fmul_rn (vdot (e2, q), dot);
+    }
+  }
+  return distance;
+}
+
 // packed face rows are read like packed hex rows (PackedCP, with its
 // vector row loads at orders 2 and 3)
 using QuadPackedCP = PackedCP;
@@ -326,7 +433,7 @@ DRB_D bool node_ray_test (const float4 *__restrict__ nodes, int node, const floa
   return min0 > min1;
 }
 
-template <int P>
+template <int P, bool TRI>
 __global__ void __launch_bounds__ (128)
 surface_kernel (SurfParams sp, const Ray *__restrict__ rays, int n, RayHit *__restrict__ hits,
                 int *__restrict__ it_out, int *__restrict__ ca_out)
@@ -348,7 +455,7 @@ surface_kernel (SurfParams sp, const Ray *__restrict__ rays, int n, RayHit *__re
   int cur = 0;
   todo[0] = kBarrier;
   int iters = 0, cands = 0;
-  constexpr int ND = (P + 1) * (P + 1);
+  constexpr int ND = TRI ? tri_dofs<P> () : (P + 1) * (P + 1);
   while (cur != kBarrier)
   {
     if (cur > -1)
@@ -384,13 +491,50 @@ surface_kernel (SurfParams sp, const Ray *__restrict__ rays, int n, RayHit *__re
     {
       const int leaf = -cur - 1;
       const int el = __ldg (sp.leaf_nodes + leaf);
-      const float *rb = sp.ref_boxes + 4 * (size_t)__ldg (sp.aabb_ids + leaf);
-      float x[2] = { (rb[0] + rb[2]) * 0.5f, (rb[1] + rb[3]) * 0.5f };
+      float x[2];
+      if (TRI)
+      {
+        // subref_center<Simplex> (subref.hpp:39-48): origin, then the axis
+        // vertices, times (float)(1.0 / 3)
+        const float *rb = sp.ref_boxes + 6 * (size_t)__ldg (sp.aabb_ids + leaf);
+#pragma unroll
+        for (int d = 0; d < 2; ++d)
+          x[d] = __fmul_rn (__fadd_rn (__fadd_rn (rb[4 + d], rb[d]), rb[2 + d]), (float)(1.0 / 3));
+      }
+      else
+      {
+        const float *rb = sp.ref_boxes + 4 * (size_t)__ldg (sp.aabb_ids + leaf);
+        x[0] = (rb[0] + rb[2]) * 0.5f;
+        x[1] = (rb[1] + rb[3]) * 0.5f;
+      }
       float t = ray.near_t;
       int steps = 0;
       ++cands;
       bool inside;
-      if (P == 1)
+      if (TRI && P == 1)
+      {
+        // closed form on the absolute vertices (dofs (0,0) (1,0) (0,1))
+        const int *ci = sp.ctrl_idx + (size_t)el * 3;
+        V3 c[3];
+#pragma unroll
+        for (int k = 0; k < 3; ++k)
+        {
+          const float *q = sp.xyz + 3 * (size_t)__ldg (ci + k);
+          c[k] = { __ldg (q), __ldg (q + 1), __ldg (q + 2) };
+        }
+        const V3 o = { ray.orig.x, ray.orig.y, ray.orig.z }, dd = { ray.dir.x, ray.dir.y, ray.dir.z };
+        float u = 0.f, v = 0.f;
+        const float dist = mt_intersect (c[0], c[1], c[2], o, dd, u, v);
+        inside = false;
+        if (dist != INFINITY)
+        {
+          x[0] = u;
+          x[1] = v;
+          inside = dist < ray.far_t;
+          t = dist;
+        }
+      }
+      else if (P == 1)
       {
         // closed form on the absolute corners (dofs (0,0) (1,0) (0,1) (1,1))
         const int *ci = sp.ctrl_idx + (size_t)el * 4;
@@ -422,12 +566,12 @@ surface_kernel (SurfParams sp, const Ray *__restrict__ rays, int n, RayHit *__re
         lr.orig.y = __fsub_rn (ray.orig.y, __ldg (row + packed_origin (ND) + 1));
         lr.orig.z = __fsub_rn (ray.orig.z, __ldg (row + packed_origin (ND) + 2));
         QuadPackedCP cp{ row };
-        inside = face_newton<P> (cp, lr, x, t, sp.tol, sp.max_steps, steps);
+        inside = face_newton<P, TRI> (cp, lr, x, t, sp.tol, sp.max_steps, steps);
       }
       else
       {
         IndirectCP cp{ sp.ctrl_idx + (size_t)el * ND, sp.xyz, 3 };
-        inside = face_newton<P> (cp, ray, x, t, sp.tol, sp.max_steps, steps);
+        inside = face_newton<P, TRI> (cp, ray, x, t, sp.tol, sp.max_steps, steps);
       }
       iters += steps;
       if (inside && t < closest && t > min_dist)
@@ -450,7 +594,7 @@ surface_kernel (SurfParams sp, const Ray *__restrict__ rays, int n, RayHit *__re
 
 // get_fragments (traceable.cpp:49-147) for dim 2 + Traceable::shade
 // (traceable.cpp:242-338) fused: one thread per ray.
-template <int P>
+template <int P, bool TRI>
 __global__ void shade_kernel (const Ray *__restrict__ rays, const RayHit *__restrict__ hits, int n,
                               const float *__restrict__ geo_packed, int gstride,
                               const float *__restrict__ fld_packed, int fstride,
@@ -468,14 +612,16 @@ __global__ void shade_kernel (const Ray *__restrict__ rays, const RayHit *__rest
   {
     QuadPackedCP gcp{ geo_packed + (size_t)h.hit_idx * gstride };
     float X[3], Ju[3], Jv[3];
-    quad_eval_d<P, 3> (gcp, h.ref[0], h.ref[1], X, Ju, Jv);
+    if (TRI) tri_eval_d<P, 3> (gcp, h.ref[0], h.ref[1], X, Ju, Jv);
+    else quad_eval_d<P, 3> (gcp, h.ref[0], h.ref[1], X, Ju, Jv);
     struct FCP
     {
       const float *p;
       DRB_D float operator() (int q, int) const { return __ldg (p + q); }
     } fcp{ fld_packed + (size_t)h.hit_idx * fstride };
     float F[1], Fu[1], Fv[1];
-    quad_eval_d<P, 1> (fcp, h.ref[0], h.ref[1], F, Fu, Fv);
+    if (TRI) tri_eval_d<P, 1> (fcp, h.ref[0], h.ref[1], F, Fu, Fv);
+    else quad_eval_d<P, 1> (fcp, h.ref[0], h.ref[1], F, Fu, Fv);
     scalar = F[0];
     normal = cross (make3 (Ju[0], Ju[1], Ju[2]), make3 (Jv[0], Jv[1], Jv[2]));
     const float m = sqrtf (dot (normal, normal));
@@ -578,12 +724,15 @@ extern "C" int drb_mesh_boundary (const drb_mesh *hex, const int *field_ctrl_idx
                                   int *n_faces, void *stream)
 {
   if (!hex || hex->dim != 3 || hex->order < 1 || hex->order > 3 || hex->n_elem < 0 || !n_faces ||
-      hex->shape != DRB_SHAPE_TENSOR || (hex->n_elem > 0 && !hex->ctrl_idx))
+      (hex->shape != DRB_SHAPE_TENSOR && hex->shape != DRB_SHAPE_SIMPLEX) ||
+      (hex->n_elem > 0 && !hex->ctrl_idx))
   {
-    set_last_error ("mesh_boundary: needs a hex mesh of order 1..3");
+    set_last_error ("mesh_boundary: needs a hex or tet mesh of order 1..3");
     return DRB_ERR_INVALID_ARG;
   }
-  const long long nf = 6ll * hex->n_elem;
+  const bool tets = hex->shape == DRB_SHAPE_SIMPLEX;
+  const int faces_per = tets ? 4 : 6;
+  const long long nf = (long long)faces_per * hex->n_elem;
   if (nf >= (1ll << 31))
   {
     set_last_error ("mesh_boundary: too many faces");
@@ -606,7 +755,10 @@ extern "C" int drb_mesh_boundary (const drb_mesh *hex, const int *field_ctrl_idx
   int *offs = scr.alloc<int> (n);
   int *total = scr.alloc<int> (1);
   if (scr.err != cudaSuccess) return status_from (scr.err);
-  extract_faces_kernel<<<div_up (hex->n_elem, 128), 128, 0, s>>> (hex->ctrl_idx, hex->n_elem, hex->order, faces);
+  if (tets)
+    extract_tet_faces_kernel<<<div_up (hex->n_elem, 128), 128, 0, s>>> (hex->ctrl_idx, hex->n_elem, hex->order, faces);
+  else
+    extract_faces_kernel<<<div_up (hex->n_elem, 128), 128, 0, s>>> (hex->ctrl_idx, hex->n_elem, hex->order, faces);
   int st = check_launch ("extract_faces_kernel");
   if (st) return st;
   iota_kernel<<<div_up (n, 256), 256, 0, s>>> (perm_a, n);
@@ -629,7 +781,14 @@ extern "C" int drb_mesh_boundary (const drb_mesh *hex, const int *field_ctrl_idx
   if (e == cudaSuccess) e = cudaStreamSynchronize (s);
   if (e != cudaSuccess) return status_from (e);
   *n_faces = h;
-  if (face_ctrl_idx)
+  if (face_ctrl_idx && tets)
+  {
+    tet_face_dofs_kernel<<<div_up (n, 256), 256, 0, s>>> (perm_a, flags, offs, n, hex->order,
+                                                          hex->ctrl_idx, field_ctrl_idx,
+                                                          face_ctrl_idx, face_field_idx, elid_faceid);
+    if ((st = check_launch ("tet_face_dofs_kernel"))) return st;
+  }
+  else if (face_ctrl_idx)
   {
     face_dofs_kernel<<<div_up (n, 256), 256, 0, s>>> (perm_a, flags, offs, n, hex->order,
                                                       hex->ctrl_idx, field_ctrl_idx, face_ctrl_idx,
@@ -649,11 +808,12 @@ extern "C" int drb_surface_intersect (const drb_mesh *faces, const drb_bvh *bvh,
     return DRB_ERR_INVALID_ARG;
   }
   if (faces->dim != 2 || faces->ncomp != 3 || faces->order < 1 || faces->order > 3 ||
-      faces->shape != DRB_SHAPE_TENSOR)
+      (faces->shape != DRB_SHAPE_TENSOR && faces->shape != DRB_SHAPE_SIMPLEX))
   {
-    set_last_error ("surface_intersect: needs a quad mesh of order 1..3");
+    set_last_error ("surface_intersect: needs a quad or triangle mesh of order 1..3");
     return DRB_ERR_UNSUPPORTED;
   }
+  const bool tri = faces->shape == DRB_SHAPE_SIMPLEX;
   if (n == 0) return DRB_OK;
   SurfParams sp;
   sp.nodes = (const float4 *)bvh->inner_nodes;
@@ -663,17 +823,22 @@ extern "C" int drb_surface_intersect (const drb_mesh *faces, const drb_bvh *bvh,
   sp.packed = faces->packed;
   sp.ctrl_idx = faces->ctrl_idx;
   sp.xyz = faces->values;
-  sp.stride = packed_stride ((faces->order + 1) * (faces->order + 1), 3);
+  sp.stride = packed_stride (mesh_nd (faces), 3);
   sp.tol = tol;
   sp.max_steps = max_steps;
   cudaStream_t s = (cudaStream_t)stream;
   const int blocks = div_up (n, 128);
-  if (faces->order == 1)
-    surface_kernel<1><<<blocks, 128, 0, s>>> (sp, (const Ray *)rays, n, (RayHit *)hits, stats.iters, stats.candidates);
-  else if (faces->order == 2)
-    surface_kernel<2><<<blocks, 128, 0, s>>> (sp, (const Ray *)rays, n, (RayHit *)hits, stats.iters, stats.candidates);
-  else
-    surface_kernel<3><<<blocks, 128, 0, s>>> (sp, (const Ray *)rays, n, (RayHit *)hits, stats.iters, stats.candidates);
+#define DRB_SK(P, T) surface_kernel<P, T><<<blocks, 128, 0, s>>> (sp, (const Ray *)rays, n, (RayHit *)hits, stats.iters, stats.candidates)
+  if (tri)
+  {
+    if (faces->order == 1) DRB_SK (1, true);
+    else if (faces->order == 2) DRB_SK (2, true);
+    else DRB_SK (3, true);
+  }
+  else if (faces->order == 1) DRB_SK (1, false);
+  else if (faces->order == 2) DRB_SK (2, false);
+  else DRB_SK (3, false);
+#undef DRB_SK
   return check_launch ("surface_kernel");
 }
 
@@ -690,29 +855,37 @@ extern "C" int drb_surface_shade (const drb_mesh *faces, const drb_mesh *face_fi
     return DRB_ERR_INVALID_ARG;
   }
   if (!faces->packed || !face_field->packed || faces->order != face_field->order ||
-      faces->dim != 2 || face_field->ncomp != 1 || faces->shape != DRB_SHAPE_TENSOR ||
-      face_field->shape != DRB_SHAPE_TENSOR)
+      faces->dim != 2 || face_field->ncomp != 1 || faces->shape != face_field->shape ||
+      (faces->shape != DRB_SHAPE_TENSOR && faces->shape != DRB_SHAPE_SIMPLEX))
   {
-    set_last_error ("surface_shade: needs packed quad geometry and scalar field of one order");
+    set_last_error ("surface_shade: needs packed quad (or triangle) geometry and scalar field "
+                    "of one order");
     return DRB_ERR_INVALID_ARG;
   }
   if (n == 0) return DRB_OK;
-  const int nd = (faces->order + 1) * (faces->order + 1);
+  const int nd = mesh_nd (faces);
+  const bool tri = faces->shape == DRB_SHAPE_SIMPLEX;
   const float fmin = range2[0], fmax = range2[1];
   float len = fmax - fmin;
   const float g = (fabsf (len) < 1e-8f) ? (std::signbit (len) ? -1e-8f : 1e-8f) : len;
   const float inv_range = 1.0f / g;
   cudaStream_t s = (cudaStream_t)stream;
   const int blocks = div_up (n, 128);
-#define DRB_SHADE(P)                                                                                   \
-  shade_kernel<P><<<blocks, 128, 0, s>>> ((const Ray *)rays, (const RayHit *)hits, n, faces->packed, \
+#define DRB_SHADE(P, T)                                                                                \
+  shade_kernel<P, T><<<blocks, 128, 0, s>>> ((const Ray *)rays, (const RayHit *)hits, n, faces->packed, \
                                           packed_stride (nd, 3), face_field->packed,                 \
                                           packed_stride (nd, 1), (const float4 *)tf, tf_size, fmin,  \
                                           fmax, inv_range, (const PointLight *)lights, n_lights,     \
                                           use_lighting, fragments, (float4 *)fb_rgba, fb_depth)
-  if (faces->order == 1) DRB_SHADE (1);
-  else if (faces->order == 2) DRB_SHADE (2);
-  else DRB_SHADE (3);
+  if (tri)
+  {
+    if (faces->order == 1) DRB_SHADE (1, true);
+    else if (faces->order == 2) DRB_SHADE (2, true);
+    else DRB_SHADE (3, true);
+  }
+  else if (faces->order == 1) DRB_SHADE (1, false);
+  else if (faces->order == 2) DRB_SHADE (2, false);
+  else DRB_SHADE (3, false);
 #undef DRB_SHADE
   return check_launch ("shade_kernel");
 }

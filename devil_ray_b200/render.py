@@ -309,8 +309,9 @@ class Volume:
 
 
 class MeshBoundary:
-    """MeshBoundary::execute for one hex mesh (+ scalar field): boundary quad
-    mesh and face field sharing the volume's value arrays."""
+    """MeshBoundary::execute for one hex or tet mesh (+ scalar field): the
+    boundary quad (or triangle) mesh and face field sharing the volume's
+    value arrays."""
 
     def execute(self, mesh: UnstructuredMesh, field: UnstructuredField | None = None,
                 stream=None):
@@ -321,35 +322,40 @@ class MeshBoundary:
         p = mesh.order
         n = nf.value
         dev = mesh.device
-        fidx = torch.empty((max(n, 1), (p + 1) ** 2), dtype=torch.int32, device=dev)
+        shape = getattr(mesh, "shape", L.SHAPE_TENSOR)
+        nd2 = L.lib().drb_elem_dofs(shape, 2, p)
+        fidx = torch.empty((max(n, 1), nd2), dtype=torch.int32, device=dev)
         ffidx = torch.empty_like(fidx) if field is not None else None
         elface = torch.empty((max(n, 1), 2), dtype=torch.int32, device=dev)
         L.check(L.lib().drb_mesh_boundary(C.byref(d),
                                           None if field is None else _ptr(field.ctrl_idx),
                                           _ptr(fidx), _ptr(ffidx), _ptr(elface), C.byref(nf),
                                           _stream(stream)), "drb_mesh_boundary")
-        faces = UnstructuredMesh(fidx[:n].reshape(-1), mesh.dof_data.values, p, dim=2, device=dev)
+        faces = UnstructuredMesh(fidx[:n].reshape(-1), mesh.dof_data.values, p, dim=2, device=dev,
+                                 shape=shape)
         face_field = None
         if field is not None:
             face_field = QuadField(ffidx[:n].reshape(-1), field.values, p, name=field.name,
-                                   device=dev)
+                                   device=dev, shape=shape)
         self.elid_faceid = elface[:n]
         return faces, face_field
 
 
 class QuadField(UnstructuredField):
-    """Scalar field on quad faces (UnstructuredField<QuadScalar>)."""
+    """Scalar field on the faces of a 2D mesh: UnstructuredField<QuadScalar*>,
+    or with shape=SHAPE_SIMPLEX UnstructuredField<TriScalar*>."""
 
-    def __init__(self, ctrl_idx, values, order: int, name: str = "f", device="cuda"):
+    def __init__(self, ctrl_idx, values, order: int, name: str = "f", device="cuda",
+                 shape: int = L.SHAPE_TENSOR):
         self.order = int(order)
         self.name = name
-        self.shape = L.SHAPE_TENSOR
+        self.shape = int(shape)
         self.device = torch.device(device)
         self.ctrl_idx = _dev(ctrl_idx, torch.int32, device)
         self.values = _dev(values, torch.float32, device).reshape(-1)
-        nd = (self.order + 1) ** 2
+        nd = L.lib().drb_elem_dofs(self.shape, 2, self.order)
         self.n_elem = self.ctrl_idx.numel() // nd
-        stride = L.lib().drb_packed_stride(2, self.order, 1)
+        stride = L.lib().drb_packed_stride_shape(self.shape, 2, self.order, 1)
         self.packed = torch.empty((max(self.n_elem, 1), stride), dtype=torch.float32,
                                   device=self.device)
         d = self.desc(packed=False)
@@ -364,7 +370,7 @@ class QuadField(UnstructuredField):
 
 
 class Surface:
-    """Surface of a quad mesh (Surface / Traceable)."""
+    """Surface of a quad or triangle mesh (Surface / Traceable)."""
 
     def __init__(self, faces: UnstructuredMesh, field: UnstructuredField):
         self.faces, self.field_ = faces, field

@@ -424,7 +424,10 @@ int drb_framebuffer_composite_background (float *rgba, int n_pixels, const float
  * field_ctrl_idx (optional) is the scalar field's ctrl_idx, mapped to
  * face_field_idx the same way; elid_faceid (optional) receives (element,
  * face id 0..5) pairs.  Outputs need capacity 6*n_elem faces; *n_faces is
- * returned after a stream synchronise (call once with NULL outputs to size). */
+ * returned after a stream synchronise (call once with NULL outputs to size).
+ * For a tet mesh the faces are triangles, (p+1)(p+2)/2 indices each (the
+ * triangle dof order of cartesian_to_tri_idx), face ids 0..3, capacity
+ * 4*n_elem; the face mesh is then a dim-2 simplex mesh. */
 int drb_mesh_boundary (const drb_mesh *hex, const int *field_ctrl_idx, int *face_ctrl_idx,
                        int *face_field_idx, int *elid_faceid, int *n_faces, void *stream);
 

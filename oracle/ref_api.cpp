@@ -526,6 +526,9 @@ int ref_boundary (void *h, int *face_ctrl_idx, int max_faces)
     if (auto *p = dynamic_cast<QuadMesh_P1 *> (m)) gf = p->get_dof_data ();
     else if (auto *p = dynamic_cast<QuadMesh_P2 *> (m)) gf = p->get_dof_data ();
     else if (auto *p = dynamic_cast<QuadMesh *> (m)) gf = p->get_dof_data ();
+    else if (auto *p = dynamic_cast<TriMesh_P1 *> (m)) gf = p->get_dof_data ();
+    else if (auto *p = dynamic_cast<TriMesh_P2 *> (m)) gf = p->get_dof_data ();
+    else if (auto *p = dynamic_cast<TriMesh *> (m)) gf = p->get_dof_data ();
     else throw std::runtime_error ("boundary: unexpected mesh type");
     const int nf = gf.get_num_elem ();
     if (face_ctrl_idx && nf <= max_faces)

@@ -224,6 +224,20 @@ class RefQuadMesh(RefHexMesh):
             raise RuntimeError(lib().ref_last_error().decode())
 
 
+def _tet_boundary_ctrl_idx(self):
+    p = self.order
+    nd2 = (p + 1) * (p + 2) // 2
+    maxf = 4 * self.n_elem
+    out = np.zeros(maxf * nd2, np.int32)
+    nf = lib().ref_boundary(self.h, _p(out), maxf)
+    if nf < 0:
+        raise RuntimeError(lib().ref_last_error().decode())
+    return out[: nf * nd2].reshape(nf, nd2)
+
+
+RefTetMesh.boundary_ctrl_idx = _tet_boundary_ctrl_idx
+
+
 def eval_tet_scalar(p, vals, refs, fixed=False):
     """The reference's Element<3,1,Simplex,P>::eval_d of one scalar element."""
     vals = np.ascontiguousarray(vals, np.float32)

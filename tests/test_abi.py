@@ -60,25 +60,26 @@ def test_widen_rejects_missing_bvh():
 
 
 def test_shape_queries_and_tet_rejections_without_gpu():
-    """Dof counts, packed strides and reference-box sizes per element shape,
-    and tets refused by the tensor-only entry points before any GPU work."""
+    """Dof counts, packed strides and reference-box sizes per element shape
+    (tets, their triangle faces), and tets refused by a hex-only entry point
+    before any GPU work."""
     from devil_ray_b200 import _lib as L
     lib = L.lib()
     T, S = L.SHAPE_TENSOR, L.SHAPE_SIMPLEX
     assert [lib.drb_elem_dofs(S, 3, p) for p in (1, 2, 3)] == [4, 10, 20]
     assert [lib.drb_elem_dofs(T, 3, p) for p in (1, 2, 3)] == [8, 27, 64]
-    assert lib.drb_elem_dofs(S, 2, 1) == -1           # triangles are not built
+    assert [lib.drb_elem_dofs(S, 2, p) for p in (1, 2, 3)] == [3, 6, 10]   # triangle faces
     assert lib.drb_elem_dofs(S, 3, 4) == -1
     assert [lib.drb_packed_stride_shape(S, 3, p, 3) for p in (1, 2, 3)] == [16, 36, 64]
     assert [lib.drb_packed_stride_shape(S, 3, p, 1) for p in (1, 2, 3)] == [4, 12, 20]
     assert lib.drb_packed_stride_shape(T, 3, 2, 3) == lib.drb_packed_stride(3, 2, 3)
     assert lib.drb_ref_box_floats(T, 3) == 6 and lib.drb_ref_box_floats(T, 2) == 4
-    assert lib.drb_ref_box_floats(S, 3) == 12
+    assert lib.drb_ref_box_floats(S, 3) == 12 and lib.drb_ref_box_floats(S, 2) == 6
     m = L.DrbMesh()
     m.dim, m.order, m.ncomp, m.n_elem, m.shape = 3, 2, 3, 1, S
     assert lib.drb_mesh_face_neighbors(C.byref(m), None, None) == L.DRB_ERR_INVALID_ARG
-    assert lib.drb_mesh_boundary(C.byref(m), None, None, None, None, None, None) == L.DRB_ERR_INVALID_ARG
+    assert b"hex" in lib.drb_last_error()
     m.shape = 7
     assert lib.drb_pack_elements(C.byref(m), None, None) == L.DRB_ERR_UNSUPPORTED
-    m.dim, m.shape = 2, S
-    assert lib.drb_pack_elements(C.byref(m), None, None) == L.DRB_ERR_UNSUPPORTED
+    m.dim, m.shape, m.n_elem = 2, S, 0
+    assert lib.drb_pack_elements(C.byref(m), None, None) == L.DRB_OK   # triangle faces

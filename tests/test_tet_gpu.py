@@ -367,3 +367,120 @@ def test_tet_hull_filter_changes_nothing(cuda, p):
     assert torch.equal(r0.view(torch.int32), r1.view(torch.int32))
     assert torch.equal(ca0, ca1)
     assert it1.sum().item() < 0.6 * it0.sum().item()
+
+
+def _tet_surface(cuda, m, w):
+    import torch
+    from devil_ray_b200 import _lib as L
+    from devil_ray_b200 import meshgen
+    from devil_ray_b200.render import (Camera, ColorTable, MeshBoundary, PointLight, Surface,
+                                       UnstructuredField)
+    c = dict(pos=(2.5, 2.5, 2.5), look_at=(0.5, 0.5, 0.5), up=(0.0, 1.0, 0.0), fov=30.0)
+    cam = Camera(w, w, c["pos"], c["look_at"], c["up"], c["fov"])
+    light = PointLight.default(cam)
+    g = _gpu(m, cuda)
+    f = UnstructuredField(m.ctrl_idx, m.field, m.order, device=cuda, shape=L.SHAPE_SIMPLEX)
+    mb = MeshBoundary()
+    faces, ff = mb.execute(g, f)
+    surf = Surface(faces, ff)
+    t = ColorTable()
+    for p in meshgen.TF_RGB:
+        t.add_point(p[0], p[1:])
+    for p in meshgen.TF_ALPHA:
+        t.add_alpha(*p)
+    surf.color_map().color_table(t)
+    fb, hits = surf.render(cam, [light])
+    torch.cuda.synchronize()
+    cam9 = np.array([*c["pos"], *c["look_at"], *c["up"]], np.float32)
+    return g, faces, fb, hits, cam, cam9, c["fov"], light
+
+
+@pytest.mark.parametrize("p", [1, 2, 3])
+def test_tet_boundary_faces(cuda, ref, p):
+    """MeshBoundary on a tet mesh: 2 triangles per boundary square; at order
+    1 the face list is the reference's (same order, same vertex order)."""
+    import torch
+    from devil_ray_b200 import _lib as L
+    from devil_ray_b200.render import MeshBoundary
+    m = _mesh(p, n=3)
+    g = _gpu(m, cuda)
+    faces, _ = MeshBoundary().execute(g)
+    torch.cuda.synchronize()
+    fi = faces.dof_data.ctrl_idx.cpu().numpy().reshape(faces.n_elem, -1)
+    assert fi.shape == (6 * 2 * 9, (p + 1) * (p + 2) // 2)
+    assert faces.shape == L.SHAPE_SIMPLEX and faces.dim == 2
+    # every face dof lies on the cube's boundary (lattice coordinate 0 or max)
+    mm = p * 3 + 1
+    K, r = np.divmod(fi, mm * mm)
+    J, I = np.divmod(r, mm)
+    on = (I == 0) | (I == mm - 1) | (J == 0) | (J == mm - 1) | (K == 0) | (K == mm - 1)
+    assert on.all()
+    if p == 1:
+        rb = ref.RefTetMesh(1, m.ctrl_idx, m.xyz, fixed=True).boundary_ctrl_idx()
+        assert np.array_equal(fi, rb)
+
+
+def test_tet_surface_order1_matches_reference(cuda, ref):
+    """Triangle faces of order-1 tets through the closed-form ray/triangle
+    test (FaceIntersector<Tri_P1>, restated operation for operation): hits,
+    distances and (u, v) bit for bit; image within 1/255."""
+    from devil_ray_b200 import meshgen
+    m = _mesh(1, n=5)
+    w = 128
+    g, faces, fb, hits, cam, cam9, fov, light = _tet_surface(cuda, m, w)
+    rs = ref.RefTetMesh(1, m.ctrl_idx, m.xyz, m.field, fixed=True).surface(
+        w, w, cam9, fov, 1024, np.array(meshgen.TF_RGB, np.float32),
+        np.array(meshgen.TF_ALPHA, np.float32), light.as13()[None])
+    h = hits.cpu().numpy()
+    gidx = h[:, 0].view(np.int32)
+    same = gidx == rs["hit_idx"]
+    assert same.mean() > 0.998, f"{(~same).sum()} hit mismatches"
+    both = same & (gidx >= 0)
+    assert both.mean() > 0.2
+    assert np.array_equal(h[both, 1].view(np.int32), rs["dist"][both].view(np.int32))
+    assert np.array_equal(h[both, 2:4].view(np.int32), rs["ref"][both].view(np.int32))
+    d = np.abs(fb.image() - rs["rgba"])
+    assert np.any(d > 1.0 / 255.0, axis=-1).mean() < 0.005
+
+
+@pytest.mark.parametrize("p", [2, 3])
+def test_tet_surface_curved_faces_lie_on_rays(cuda, p):
+    """Curved triangle faces (Newton ray/face solve): every hit's face point
+    X(u, v) is the ray's point at the hit distance, (u, v) lies in the
+    triangle, and a query just past the hit is located inside the tet mesh
+    while one just before it is not (the face is the mesh's boundary)."""
+    import torch
+    from math import factorial
+    from devil_ray_b200 import meshgen
+    m = _mesh(p, n=5)
+    w = 128
+    g, faces, fb, hits, cam, cam9, fov, light = _tet_surface(cuda, m, w)
+    h = hits.cpu().numpy()
+    gidx = h[:, 0].view(np.int32)
+    sel = np.nonzero(gidx >= 0)[0]
+    assert sel.size > 0.2 * w * w
+    rays = cam.create_rays(cuda).cpu().numpy()
+    orig, dirs = rays[sel, 4:7].astype(np.float64), rays[sel, 0:3].astype(np.float64)
+    tdist = h[sel, 1].astype(np.float64)
+    u, v = h[sel, 2].astype(np.float64), h[sel, 3].astype(np.float64)
+    fi = faces.dof_data.ctrl_idx.cpu().numpy().reshape(faces.n_elem, -1)
+    cp = m.xyz[fi[gidx[sel]]].astype(np.float64)                 # [k, nd2, 3]
+    t = 1 - u - v
+    X = np.zeros((sel.size, 3))
+    for j in range(p + 1):
+        for i in range(p + 1 - j):
+            l = p - i - j
+            B = factorial(p) / (factorial(i) * factorial(j) * factorial(l)) * u ** i * v ** j * t ** l
+            X += B[:, None] * cp[:, (2 * p + 3 - j) * j // 2 + i]
+    on_ray = orig + tdist[:, None] * dirs
+    assert np.abs(X - on_ray).max() < 2e-4
+    assert (np.minimum(np.minimum(u, v), t) >= -1.1e-4).all()
+    eps = 2e-3
+    q_in = torch.as_tensor((on_ray + eps * dirs).astype(np.float32), device=cuda)
+    q_out = torch.as_tensor((on_ray - eps * dirs).astype(np.float32), device=cuda)
+    from devil_ray_b200 import api
+    c_in, _ = api.BatchedLocator(g).locate(q_in)
+    c_out, _ = api.BatchedLocator(g).locate(q_out)
+    torch.cuda.synchronize()
+    assert (c_in >= 0).float().mean().item() > 0.98
+    assert (c_out < 0).float().mean().item() > 0.98
