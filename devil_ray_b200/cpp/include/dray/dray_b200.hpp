@@ -106,6 +106,13 @@ using Tet_P2 = Element<3, 3, Simplex, Order::Quadratic>;
 using TetScalar = Element<3, 1, Simplex, Order::General>;
 using TetScalar_P1 = Element<3, 1, Simplex, Order::Linear>;
 using TetScalar_P2 = Element<3, 1, Simplex, Order::Quadratic>;
+// Triangles: the boundary faces of tet meshes (unstructured_mesh.hpp:129-131).
+using Tri3 = Element<2, 3, Simplex, Order::General>;
+using Tri_P1 = Element<2, 3, Simplex, Order::Linear>;
+using Tri_P2 = Element<2, 3, Simplex, Order::Quadratic>;
+using TriScalar = Element<2, 1, Simplex, Order::General>;
+using TriScalar_P1 = Element<2, 1, Simplex, Order::Linear>;
+using TriScalar_P2 = Element<2, 1, Simplex, Order::Quadratic>;
 
 template <int32 PhysDim> struct GridFunction
 {
@@ -234,8 +241,7 @@ class ElementMesh : public Mesh
 
 template <class ElemT> class UnstructuredMesh : public ElementMesh
 {
-  static_assert (ElemT::get_etype () == Tensor || ElemT::get_dim () == 3,
-                 "hex, quad and tet elements are on this path (no triangles)");
+  static_assert (ElemT::get_dim () == 2 || ElemT::get_dim () == 3, "2D or 3D elements");
   static_assert (ElemT::get_ncomp () == 3, "meshes have 3 components");
   public:
   UnstructuredMesh (const GridFunction<3> &dof, int32 order)
@@ -246,7 +252,9 @@ template <class ElemT> class UnstructuredMesh : public ElementMesh
   }
   std::string type_name () const override
   {
-    const char *n = ElemT::get_etype () == Simplex ? "Tet" : ElemT::get_dim () == 3 ? "Hex" : "Quad";
+    const char *n = ElemT::get_etype () == Simplex ? (ElemT::get_dim () == 3 ? "Tet" : "Tri")
+                    : ElemT::get_dim () == 3                ? "Hex"
+                                                            : "Quad";
     return std::string (n) + "_P" + std::to_string (m_poly_order);
   }
 };
@@ -259,6 +267,9 @@ using QuadMesh_P2 = UnstructuredMesh<Quad_P2>;
 using TetMesh = UnstructuredMesh<Tet3>;
 using TetMesh_P1 = UnstructuredMesh<Tet_P1>;
 using TetMesh_P2 = UnstructuredMesh<Tet_P2>;
+using TriMesh = UnstructuredMesh<Tri3>;
+using TriMesh_P1 = UnstructuredMesh<Tri_P1>;
+using TriMesh_P2 = UnstructuredMesh<Tri_P2>;
 
 class ElementField : public Field
 {
@@ -283,8 +294,7 @@ class ElementField : public Field
 
 template <class ElemT> class UnstructuredField : public ElementField
 {
-  static_assert ((ElemT::get_etype () == Tensor || ElemT::get_dim () == 3) && ElemT::get_ncomp () == 1,
-                 "only scalar hex, quad and tet fields are on this path");
+  static_assert (ElemT::get_ncomp () == 1, "only scalar fields are on this path");
   public:
   UnstructuredField (const GridFunction<1> &dof, int32 order, const std::string &name = "")
   : ElementField (dof, order, ElemT::get_dim (), name, ElemT::get_etype ())
@@ -292,9 +302,9 @@ template <class ElemT> class UnstructuredField : public ElementField
   }
   std::string type_name () const override
   {
-    const char *n = ElemT::get_etype () == Simplex ? "TetScalar"
-                    : ElemT::get_dim () == 3      ? "HexScalar"
-                                                  : "QuadScalar";
+    const char *n = ElemT::get_etype () == Simplex ? (ElemT::get_dim () == 3 ? "TetScalar" : "TriScalar")
+                    : ElemT::get_dim () == 3                ? "HexScalar"
+                                                            : "QuadScalar";
     return std::string (n) + "_P" + std::to_string (m_poly_order);
   }
 };

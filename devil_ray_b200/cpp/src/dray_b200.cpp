@@ -124,7 +124,7 @@ const drb_bvh *ElementMesh::device_bvh ()
       g.wide.alloc ((size_t)32 * g.bvh.n_wide);
       drb_check (drb_bvh_widen (&g.bvh, g.wide.p, g.bvh.n_wide, nullptr), "drb_bvh_widen");
     }
-    if (m_etype == Simplex)
+    if (m_etype == Simplex && m_dim == 3)
     {
       // bounding planes: the batched locate's candidate filter for tets
       g.hull.alloc ((size_t)20 * std::max (cells (), 1));
@@ -596,7 +596,8 @@ Collection MeshBoundary::execute (Collection &collection)
     drb_check (drb_mesh_boundary (dm, nullptr, nullptr, nullptr, nullptr, &nf, nullptr),
                "drb_mesh_boundary");
     const int p = hex->order ();
-    const int fd = (p + 1) * (p + 1);
+    const bool tets = hex->etype () == Simplex;
+    const int fd = tets ? (p + 1) * (p + 2) / 2 : (p + 1) * (p + 1);
     GridFunction<3> fg;
     GridFunction<3> vol = hex->get_dof_data ();
     fg.m_values = vol.m_values; // the quads index the volume's value array
@@ -611,7 +612,14 @@ Collection MeshBoundary::execute (Collection &collection)
     int32 *fi = fg.m_ctrl_idx.get_device_ptr ();
     drb_check (drb_mesh_boundary (dm, nullptr, fi, nullptr, nullptr, &nf, nullptr), "drb_mesh_boundary");
     std::shared_ptr<Mesh> qm;
-    if (p == 1) qm = std::make_shared<QuadMesh_P1> (fg, 1);
+    if (tets)
+    {
+      // a tet mesh's boundary is triangles (mesh_boundary.cpp:102-185)
+      if (p == 1) qm = std::make_shared<TriMesh_P1> (fg, 1);
+      else if (p == 2) qm = std::make_shared<TriMesh_P2> (fg, 2);
+      else qm = std::make_shared<TriMesh> (fg, p);
+    }
+    else if (p == 1) qm = std::make_shared<QuadMesh_P1> (fg, 1);
     else if (p == 2) qm = std::make_shared<QuadMesh_P2> (fg, 2);
     else qm = std::make_shared<QuadMesh> (fg, p);
     out.add_mesh (qm);
@@ -631,7 +639,10 @@ Collection MeshBoundary::execute (Collection &collection)
                                     nullptr, &nf, nullptr),
                  "drb_mesh_boundary");
       std::shared_ptr<Field> qf;
-      if (p == 1) qf = std::make_shared<UnstructuredField<QuadScalar_P1>> (ff, 1, f->name ());
+      if (tets && p == 1) qf = std::make_shared<UnstructuredField<TriScalar_P1>> (ff, 1, f->name ());
+      else if (tets && p == 2) qf = std::make_shared<UnstructuredField<TriScalar_P2>> (ff, 2, f->name ());
+      else if (tets) qf = std::make_shared<UnstructuredField<TriScalar>> (ff, p, f->name ());
+      else if (p == 1) qf = std::make_shared<UnstructuredField<QuadScalar_P1>> (ff, 1, f->name ());
       else if (p == 2) qf = std::make_shared<UnstructuredField<QuadScalar_P2>> (ff, 2, f->name ());
       else qf = std::make_shared<UnstructuredField<QuadScalar>> (ff, p, f->name ());
       out.add_field (qf);

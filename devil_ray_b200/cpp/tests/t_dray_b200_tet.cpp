@@ -1,6 +1,7 @@
 // Drives the C++ host interface with a tet mesh the way a Devil Ray user
 // does: UnstructuredMesh<Tet*> and UnstructuredField<TetScalar*> in a
-// DataSet/Collection, Mesh::locate, PointLocation and Volume::integrate.
+// DataSet/Collection, Mesh::locate, PointLocation, Volume::integrate, and
+// MeshBoundary + Surface on the tets' triangle faces.
 // Raw binary inputs and
 // outputs, compared with the reference oracle by tests/test_tet_gpu.py.
 //
@@ -16,6 +17,8 @@
 //            <dir>/pointloc.bin float value[n]
 //            <dir>/volume.bin   float rgba[4wh]  (Volume::integrate + save
 //                               compositing, when render.bin is given)
+//            <dir>/surface.bin  float rgba[4wh]; float depth[wh]  (MeshBoundary +
+//                               Surface, when render.bin is given)
 #include <dray/dray_b200.hpp>
 
 #include <fstream>
@@ -166,6 +169,25 @@ int main (int argc, char **argv)
       Framebuffer fb = Volume::composite (parts, whs[0], whs[1]);
       std::ofstream fo (dir + "/volume.bin", std::ios::binary);
       wr (fo, (const float *)fb.colors ().get_host_ptr_const (), (size_t)4 * whs[0] * whs[1]);
+
+      // MeshBoundary (triangle faces) + Surface
+      MeshBoundary mb;
+      Collection faces = mb.execute (col);
+      if (faces.domain (0).mesh ()->type_name ().rfind ("Tri_P", 0) != 0)
+        throw std::runtime_error ("boundary type " + faces.domain (0).mesh ()->type_name ());
+      Surface surf (faces);
+      surf.field ("f");
+      surf.color_map ().color_table (table);
+      surf.color_map ().samples (1024);
+      Array<Ray> srays;
+      cam.create_rays (srays);
+      Array<RayHit> hits = surf.nearest_hit (srays);
+      Array<Fragment> frags = surf.fragments (hits);
+      Framebuffer sfb (whs[0], whs[1]);
+      surf.shade (srays, hits, frags, lights, sfb);
+      std::ofstream fs (dir + "/surface.bin", std::ios::binary);
+      wr (fs, (const float *)sfb.colors ().get_host_ptr_const (), (size_t)4 * whs[0] * whs[1]);
+      wr (fs, sfb.depths ().get_host_ptr_const (), (size_t)whs[0] * whs[1]);
     }
   }
   catch (const std::exception &e)

@@ -274,6 +274,16 @@ def test_cpp_tet_mesh_interface(cuda, ref, tmp_path, p):
         d = np.abs(img - rimg)
         assert np.any(d > 1.0 / 255.0, axis=-1).mean() < 0.005
     assert img[..., 3].max() > 0.1
+    # MeshBoundary + Surface on the triangle faces; order 1 against the
+    # reference's fixed-order tets (closed-form ray/triangle test)
+    raw = np.fromfile(tmp_path / "surface.bin", np.float32)
+    simg = raw[: 4 * w * w].reshape(w, w, 4)
+    assert (simg[..., 3] > 0).mean() > 0.2
+    if p == 1:
+        rs = ref.RefTetMesh(1, m.ctrl_idx, m.xyz, m.field, fixed=True).surface(
+            w, w, cam9, cam_d["fov"], 1024, rgb, alpha, light13[None])
+        d = np.abs(simg - rs["rgba"])
+        assert np.any(d > 1.0 / 255.0, axis=-1).mean() < 0.005
 
 
 def _tet_volume(cuda, m, w, samples, lighting, coherent):
