@@ -51,10 +51,10 @@ extern "C" int drb_locate (const drb_mesh *mesh, const drb_bvh *bvh, const float
     return DRB_ERR_INVALID_ARG;
   }
   if (mesh->ncomp != 3 || mesh->order < 1 || mesh->order > 3 ||
-      !((mesh->dim == 3 && (mesh->shape == DRB_SHAPE_TENSOR || mesh->shape == DRB_SHAPE_SIMPLEX)) ||
-        (mesh->dim == 2 && mesh->shape == DRB_SHAPE_TENSOR)))
+      !((mesh->dim == 3 || mesh->dim == 2) &&
+        (mesh->shape == DRB_SHAPE_TENSOR || mesh->shape == DRB_SHAPE_SIMPLEX)))
   {
-    set_last_error ("locate: needs a hex, tet or quad geometry mesh of order 1..3");
+    set_last_error ("locate: needs a hex, tet, quad or triangle geometry mesh of order 1..3");
     return DRB_ERR_UNSUPPORTED;
   }
   if (opts->guess_mode == DRB_GUESS_GIVEN && !opts->guess)
@@ -85,7 +85,13 @@ extern "C" int drb_locate (const drb_mesh *mesh, const drb_bvh *bvh, const float
   cudaStream_t s = (cudaStream_t)stream;
   const int blocks = div_up (n, 128);
 #define DRB_LK(P, S) locate_kernel<P, S><<<blocks, 128, 0, s>>> (lp, pts, n, cell, ref, stats.iters, stats.candidates, stats.nodes)
-  if (mesh->shape == DRB_SHAPE_SIMPLEX)
+  if (mesh->shape == DRB_SHAPE_SIMPLEX && mesh->dim == 2)
+  {
+    if (mesh->order == 1) DRB_LK (1, kTri2D);
+    else if (mesh->order == 2) DRB_LK (2, kTri2D);
+    else DRB_LK (3, kTri2D);
+  }
+  else if (mesh->shape == DRB_SHAPE_SIMPLEX)
   {
     if (mesh->order == 1) DRB_LK (1, kSimplex);
     else if (mesh->order == 2) DRB_LK (2, kSimplex);

@@ -161,14 +161,19 @@ DRB_D bool hull_rejects (const LocateParams &lp, int el, const float (&pt)[3])
 constexpr int kTensor = DRB_SHAPE_TENSOR;
 constexpr int kSimplex = DRB_SHAPE_SIMPLEX;
 constexpr int kQuad2D = 2;
+constexpr int kTri2D = 3;
 
 // Dofs of an order-P element of kind S, and its reference centre
 // coordinate (hex (0.5,0.5,0.5), tet centroid (0.25,0.25,0.25)).
 template <int S, int P> constexpr int shape_dofs ()
 {
-  return S == kSimplex ? tet_dofs<P> () : S == kQuad2D ? (P + 1) * (P + 1) : (P + 1) * (P + 1) * (P + 1);
+  return S == kSimplex ? tet_dofs<P> () : S == kQuad2D ? (P + 1) * (P + 1)
+         : S == kTri2D ? tri_dofs<P> () : (P + 1) * (P + 1) * (P + 1);
 }
-template <int S> constexpr float shape_centre () { return S == kSimplex ? 0.25f : 0.5f; }
+template <int S> constexpr float shape_centre ()
+{
+  return S == kSimplex ? 0.25f : S == kTri2D ? (float)(1.0 / 3) : 0.5f;
+}
 
 // Tet Newton solve (simplex counterpart of the tensor path below).
 template <int P, bool REG>
@@ -218,6 +223,30 @@ DRB_D bool solve_in_quad (const LocateParams &lp, int el, const float (&pt)[3], 
   return quad_newton<P> (cp, pt, x, lp.tol, lp.max_steps, steps, lu);
 }
 
+// Triangle of a 2D mesh (LocateHack<2>): tri_newton on the packed row.
+template <int P, bool REG>
+DRB_D bool solve_in_tri (const LocateParams &lp, int el, const float (&pt)[3], float (&x)[3],
+                         int &steps, LU3 &lu)
+{
+  constexpr int ND = tri_dofs<P> ();
+  if (lp.packed)
+  {
+    const float *row = lp.packed + (size_t)el * lp.stride;
+    float t[3];
+    local_target<ND> (row, pt, t);
+    if (REG)
+    {
+      RegCP<3 * ND> r;
+      load_reg_rows<3 * ND> (r, row);
+      return tri_newton<P> (r, t, x, lp.tol, lp.max_steps, steps, lu);
+    }
+    PackedCP cp{ row };
+    return tri_newton<P> (cp, t, x, lp.tol, lp.max_steps, steps, lu);
+  }
+  IndirectCP cp{ lp.ctrl_idx + (size_t)el * ND, lp.xyz, 3 };
+  return tri_newton<P> (cp, pt, x, lp.tol, lp.max_steps, steps, lu);
+}
+
 // Newton solve of one point in one element, choosing register-resident or
 // L1-read control points by order.
 template <int P, bool REG = (P <= 2), int S = kTensor>
@@ -226,6 +255,7 @@ DRB_D bool solve_in_element (const LocateParams &lp, int el, const float (&pt)[3
 {
   if (S == kSimplex) return solve_in_tet<P, REG> (lp, el, pt, x, steps, lu);
   if (S == kQuad2D) return solve_in_quad<P, REG> (lp, el, pt, x, steps, lu);
+  if (S == kTri2D) return solve_in_tri<P, REG> (lp, el, pt, x, steps, lu);
   constexpr int ND = (P + 1) * (P + 1) * (P + 1);
   if (lp.packed)
   {
@@ -302,6 +332,15 @@ DRB_D void candidate_guess (const LocateParams &lp, int leaf, long long qi, bool
       sum = __fadd_rn (sum, rb[6 + d]);
       x[d] = __fmul_rn (sum, 0.25f);
     }
+  }
+  else if (lp.guess_mode == DRB_GUESS_SUBREF_CENTER && S == kTri2D)
+  {
+    // subref_center<Simplex> in 2D: origin, then the axis vertices, times 1/3
+    const float *rb = lp.ref_boxes + 6 * (size_t)__ldg (lp.aabb_ids + leaf);
+#pragma unroll
+    for (int d = 0; d < 2; ++d)
+      x[d] = __fmul_rn (__fadd_rn (__fadd_rn (rb[4 + d], rb[d]), rb[2 + d]), (float)(1.0 / 3));
+    x[2] = 0.f;
   }
   else if (lp.guess_mode == DRB_GUESS_SUBREF_CENTER && S == kQuad2D)
   {

@@ -302,6 +302,7 @@ template <int S> const void *persistent_fn_s (int order, int mode, bool wide)
 
 const void *persistent_fn (const drb_mesh *mesh, int mode, bool wide)
 {
+  if (mesh->shape == DRB_SHAPE_SIMPLEX && mesh->dim == 2) return persistent_fn_s<kTri2D> (mesh->order, mode, wide);
   if (mesh->shape == DRB_SHAPE_SIMPLEX) return persistent_fn_s<kSimplex> (mesh->order, mode, wide);
   if (mesh->dim == 2) return persistent_fn_s<kQuad2D> (mesh->order, mode, wide);
   return persistent_fn_s<kTensor> (mesh->order, mode, wide);
@@ -357,7 +358,9 @@ int launch_persistent (const drb_mesh *mesh, int mode, dim3 grid, int block, cud
   if (smem > 48 * 1024)
     cudaFuncSetAttribute (persistent_fn (mesh, mode, wide), cudaFuncAttributeMaxDynamicSharedMemorySize,
                           (int)smem);
-  if (mesh->shape == DRB_SHAPE_SIMPLEX)
+  if (mesh->shape == DRB_SHAPE_SIMPLEX && mesh->dim == 2)
+    launch_s<kTri2D> (order, wide, mode, grid, block, smem, s, lp, pts, ord, n, chunk, head, cell, ref, st);
+  else if (mesh->shape == DRB_SHAPE_SIMPLEX)
     launch_s<kSimplex> (order, wide, mode, grid, block, smem, s, lp, pts, ord, n, chunk, head, cell, ref, st);
   else if (mesh->dim == 2)
     launch_s<kQuad2D> (order, wide, mode, grid, block, smem, s, lp, pts, ord, n, chunk, head, cell, ref, st);
@@ -393,7 +396,8 @@ LocateParams make_params (const drb_mesh *mesh, const drb_bvh *bvh, const drb_ne
   lp.max_steps = opts->max_steps;
   lp.guess_mode = opts->guess_mode;
   lp.guess = opts->guess;
-  lp.hull = mesh->shape == DRB_SHAPE_SIMPLEX ? (const float4 *)mesh->hull_planes : nullptr;
+  lp.hull = (mesh->shape == DRB_SHAPE_SIMPLEX && mesh->dim == 3) ? (const float4 *)mesh->hull_planes
+                                                                   : nullptr;
   return lp;
 }
 
@@ -406,10 +410,10 @@ int check_args (const drb_mesh *mesh, const drb_bvh *bvh, const float *pts, int 
     return DRB_ERR_INVALID_ARG;
   }
   if (mesh->ncomp != 3 || mesh->order < 1 || mesh->order > 3 ||
-      !((mesh->dim == 3 && (mesh->shape == DRB_SHAPE_TENSOR || mesh->shape == DRB_SHAPE_SIMPLEX)) ||
-        (mesh->dim == 2 && mesh->shape == DRB_SHAPE_TENSOR)))
+      !((mesh->dim == 3 || mesh->dim == 2) &&
+        (mesh->shape == DRB_SHAPE_TENSOR || mesh->shape == DRB_SHAPE_SIMPLEX)))
   {
-    set_last_error ("locate_batched: needs a hex, tet or quad geometry mesh of order 1..3");
+    set_last_error ("locate_batched: needs a hex, tet, quad or triangle geometry mesh of order 1..3");
     return DRB_ERR_UNSUPPORTED;
   }
   if (opts->guess_mode == DRB_GUESS_GIVEN && !opts->guess)

@@ -42,6 +42,12 @@ __global__ void map_points_kernel (const float *__restrict__ packed, int stride,
       quad_eval_d<P, 3> (cp, u, v, X, Ju, Jv);
       to_world<(P + 1) * (P + 1)> (row, X);
     }
+    else if (K == 3)
+    {
+      float Ju[3], Jv[3];
+      tri_eval_d<P, 3> (cp, u, v, X, Ju, Jv);
+      to_world<tri_dofs<P> ()> (row, X);
+    }
     else
     {
       hex_eval<P, 3> (cp, u, v, w, X);
@@ -127,6 +133,11 @@ __global__ void field_eval_kernel (const float *__restrict__ packed, int stride,
       float Ju[1], Jv[1];
       quad_eval_d<P, 1> (cp, u, vv, X, Ju, Jv);
     }
+    else if (K == 3)
+    {
+      float Ju[1], Jv[1];
+      tri_eval_d<P, 1> (cp, u, vv, X, Ju, Jv);
+    }
     else
     {
       hex_eval<P, 1> (cp, u, vv, w, X);
@@ -144,7 +155,7 @@ int check_pairs (const drb_mesh *m, int n, bool any_kind = false)
     set_last_error ("pairs: needs a packed hex geometry mesh of order 1..3");
     return DRB_ERR_INVALID_ARG;
   }
-  if (m->shape != DRB_SHAPE_TENSOR && !(any_kind && m->shape == DRB_SHAPE_SIMPLEX && m->dim == 3))
+  if (m->shape != DRB_SHAPE_TENSOR && !(any_kind && m->shape == DRB_SHAPE_SIMPLEX))
   {
     set_last_error ("pairs: element shape not supported here");
     return DRB_ERR_UNSUPPORTED;
@@ -152,10 +163,11 @@ int check_pairs (const drb_mesh *m, int n, bool any_kind = false)
   return DRB_OK;
 }
 
-// 0 hex, 1 tet, 2 quad (the K of the kernels above)
+// 0 hex, 1 tet, 2 quad, 3 triangle (the K of the kernels above)
 int kind_of (const drb_mesh *m)
 {
-  return m->shape == DRB_SHAPE_SIMPLEX ? 1 : m->dim == 2 ? 2 : 0;
+  if (m->shape == DRB_SHAPE_SIMPLEX) return m->dim == 2 ? 3 : 1;
+  return m->dim == 2 ? 2 : 0;
 }
 
 } // namespace
@@ -182,6 +194,7 @@ extern "C" int drb_map_points (const drb_mesh *mesh, const int *elem, const floa
   const int kind = kind_of (mesh);
   if (kind == 1) DRB_MPK (1);
   else if (kind == 2) DRB_MPK (2);
+  else if (kind == 3) DRB_MPK (3);
   else DRB_MPK (0);
 #undef DRB_MPK
 #undef DRB_MP
@@ -218,8 +231,8 @@ extern "C" int drb_field_eval (const drb_mesh *field, const int *cell, const flo
 {
   if (!field || !field->packed || field->ncomp != 1 || field->order < 1 || field->order > 3 ||
       n < 0 || (n > 0 && (!cell || !ref || !values)) ||
-      !((field->dim == 3 && (field->shape == DRB_SHAPE_TENSOR || field->shape == DRB_SHAPE_SIMPLEX)) ||
-        (field->dim == 2 && field->shape == DRB_SHAPE_TENSOR)))
+      !((field->dim == 3 || field->dim == 2) &&
+        (field->shape == DRB_SHAPE_TENSOR || field->shape == DRB_SHAPE_SIMPLEX)))
   {
     set_last_error ("field_eval: needs a packed scalar hex, tet or quad field of order 1..3");
     return DRB_ERR_INVALID_ARG;
@@ -233,6 +246,7 @@ extern "C" int drb_field_eval (const drb_mesh *field, const int *cell, const flo
   const int kind = kind_of (field);
   if (kind == 1) DRB_FEK (1);
   else if (kind == 2) DRB_FEK (2);
+  else if (kind == 3) DRB_FEK (3);
   else DRB_FEK (0);
 #undef DRB_FEK
 #undef DRB_FE

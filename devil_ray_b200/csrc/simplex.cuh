@@ -171,6 +171,42 @@ DRB_D bool is_inside_tri (float u, float v, float eps)
   return mn >= 0.f - eps;
 }
 
+// LocateHack<2> (data_model/device_mesh.hpp:166-238) on a triangle of a 2D
+// mesh: the quad_newton iteration with the triangle's evaluation and
+// TriRefSpace<2>::is_inside(ref, tol).
+template <int P, class CP>
+DRB_D bool tri_newton (const CP &cp, const float (&target)[3], float (&x)[3], float tol,
+                       int max_steps, int &steps, LU3 &lu)
+{
+  float prev[3] = { x[0], x[1], x[2] };
+  bool converged = false;
+  steps = 0;
+  while (steps < max_steps && !converged)
+  {
+    x[0] = fminf (1.f, fmaxf (x[0], 0.f));
+    x[1] = fminf (1.f, fmaxf (x[1], 0.f));
+    float X[3], Ju[3], Jv[3];
+    tri_eval_d<P, 3> (cp, x[0], x[1], X, Ju, Jv);
+    float dy[3], J[3][3], dx[3];
+#pragma unroll
+    for (int r = 0; r < 3; ++r)
+    {
+      dy[r] = target[r] - X[r];
+      J[r][0] = Ju[r];
+      J[r][1] = Jv[r];
+      J[r][2] = (r == 2) ? 1.f : 0.f;
+    }
+    lu.factor (J);
+    lu.solve (dy, dx);
+    x[0] += dx[0];
+    x[1] += dx[1];
+    ++steps;
+    converged = step_change2 (x, prev) < tol;
+  }
+  x[2] = -1.f;
+  return converged && is_inside_tri (x[0], x[1], tol);
+}
+
 // TriRefSpace<3>::is_inside(ref, eps) (pos_simplex_element.tcc:493-505).
 DRB_D bool is_inside_simplex (const float (&x)[3], float eps)
 {

@@ -283,6 +283,30 @@ def quad_warped_mesh(n: int, p: int, amp: float, jitter: float = 0.0, seed: int 
                         field=f.astype(np.float32), meta=meta)
 
 
+def tri_warped_mesh(n: int, p: int, amp: float, jitter: float = 0.0, seed: int = 0) -> QuadMeshData:
+    """The lattice of quad_warped_mesh(n, p, ...) cut into 2 n^2 order-p
+    triangles along each cell's (0,0)-(1,1) diagonal.  Triangle 2 c of cell
+    c has vertices (0,0), (1,0), (1,1) (origin, u = 1, v = 1), triangle
+    2 c + 1 has (0,0), (1,1), (0,1); dof (i, j) (i fastest) sits at lattice
+    offset (i + j, j) and (i, i + j) respectively."""
+    q = quad_warped_mesh(n, p, amp, jitter, seed)
+    m = p * n + 1
+    mi = [(i, j) for j in range(p + 1) for i in range(p + 1 - j)]
+    off0 = np.array([(i + j, j) for i, j in mi], np.int64)        # (dx, dy)
+    off1 = np.array([(i, i + j) for i, j in mi], np.int64)
+    c = np.arange(n, dtype=np.int64)
+    CJ, CI = np.meshgrid(c, c, indexing="ij")
+    out = np.empty((n, n, 2, len(mi)), np.int64)
+    for t, off in enumerate((off0, off1)):
+        X = p * CI[..., None] + off[None, None, :, 0]
+        Y = p * CJ[..., None] + off[None, None, :, 1]
+        out[:, :, t, :] = Y * m + X
+    meta = dict(q.meta)
+    meta["cells"] = "2 triangles per square"
+    return QuadMeshData(order=p, n=n, ctrl_idx=out.reshape(-1).astype(np.int32), xyz=q.xyz,
+                        field=q.field, meta=meta)
+
+
 # outside fraction of uniform queries: the meshes fill [0,1]^3, so queries are
 # drawn from a cube padded so that about 8% of its volume lies outside
 OUTSIDE_FRACTION = 0.08

@@ -138,6 +138,9 @@ BVH get_bvh_any (Mesh *m)
   if (auto *p = dynamic_cast<TetMesh_P1 *> (m)) return p->get_bvh ();
   if (auto *p = dynamic_cast<TetMesh_P2 *> (m)) return p->get_bvh ();
   if (auto *p = dynamic_cast<TetMesh *> (m)) return p->get_bvh ();
+  if (auto *p = dynamic_cast<TriMesh_P1 *> (m)) return p->get_bvh ();
+  if (auto *p = dynamic_cast<TriMesh_P2 *> (m)) return p->get_bvh ();
+  if (auto *p = dynamic_cast<TriMesh *> (m)) return p->get_bvh ();
   throw std::runtime_error ("unsupported mesh type");
 }
 
@@ -163,6 +166,13 @@ int copy_ref_boxes (Mesh *m, float *out)
   { auto a = p->get_ref_aabbs (); std::memcpy (out, (const void *)a.get_host_ptr_const (), a.size () * 48); return 4; }
   if (auto *p = dynamic_cast<TetMesh *> (m))
   { auto a = p->get_ref_aabbs (); std::memcpy (out, (const void *)a.get_host_ptr_const (), a.size () * 48); return 4; }
+  // SubRef<2,Simplex>: three vertices of two floats
+  if (auto *p = dynamic_cast<TriMesh_P1 *> (m))
+  { auto a = p->get_ref_aabbs (); std::memcpy (out, (const void *)a.get_host_ptr_const (), a.size () * 24); return 3; }
+  if (auto *p = dynamic_cast<TriMesh_P2 *> (m))
+  { auto a = p->get_ref_aabbs (); std::memcpy (out, (const void *)a.get_host_ptr_const (), a.size () * 24); return 3; }
+  if (auto *p = dynamic_cast<TriMesh *> (m))
+  { auto a = p->get_ref_aabbs (); std::memcpy (out, (const void *)a.get_host_ptr_const (), a.size () * 24); return 3; }
   return 0;
 }
 
@@ -310,6 +320,41 @@ void *ref_quad_create (int order, int n_el, const int *ctrl_idx, int n_ctrl, con
       if (order == 1) f = std::make_shared<UnstructuredField<QuadScalar_P1>> (ff, 1, "f");
       else if (order == 2) f = std::make_shared<UnstructuredField<QuadScalar_P2>> (ff, 2, "f");
       else f = std::make_shared<UnstructuredField<QuadScalar>> (ff, order, "f");
+      ds.add_field (f);
+      r->has_field = true;
+    }
+    r->collection.add_domain (ds);
+    return r;
+  }
+  catch (const std::exception &e)
+  {
+    g_err = e.what ();
+    return nullptr;
+  }
+}
+
+// Create a triangle (2D) mesh and optional scalar field "f": TriMesh_P1/P2
+// for orders 1-2, TriMesh (general order) otherwise.
+void *ref_tri_create (int order, int n_el, const int *ctrl_idx, int n_ctrl, const float *xyz,
+                      const int *field_idx, int n_field_ctrl, const float *field_vals)
+{
+  try
+  {
+    const int nd = (order + 1) * (order + 2) / 2;
+    RefMesh *r = new RefMesh ();
+    r->order = order;
+    GridFunction<3> gf = make_gf3 (n_el, nd, ctrl_idx, n_ctrl, xyz);
+    if (order == 1) r->mesh = std::make_shared<TriMesh_P1> (gf, 1);
+    else if (order == 2) r->mesh = std::make_shared<TriMesh_P2> (gf, 2);
+    else r->mesh = std::make_shared<TriMesh> (gf, order);
+    DataSet ds (r->mesh);
+    if (field_vals != nullptr)
+    {
+      GridFunction<1> ff = make_gf1 (n_el, nd, field_idx, n_field_ctrl, field_vals);
+      std::shared_ptr<Field> f;
+      if (order == 1) f = std::make_shared<UnstructuredField<TriScalar_P1>> (ff, 1, "f");
+      else if (order == 2) f = std::make_shared<UnstructuredField<TriScalar_P2>> (ff, 2, "f");
+      else f = std::make_shared<UnstructuredField<TriScalar>> (ff, order, "f");
       ds.add_field (f);
       r->has_field = true;
     }

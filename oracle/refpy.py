@@ -48,6 +48,8 @@ def lib():
         L.ref_eval_hex_scalar.argtypes = [C.c_int, C.c_int, vp, C.c_int, vp, vp, vp]
         L.ref_lineout.argtypes = [vp, C.c_int, vp, vp, C.c_int, C.c_float, vp, vp]
         L.ref_scalar_render.argtypes = [vp, C.c_int, C.c_int, vp, C.c_float, vp, vp, vp]
+        L.ref_tri_create.restype = vp
+        L.ref_tri_create.argtypes = [C.c_int, C.c_int, vp, C.c_int, vp, vp, C.c_int, vp]
         L.ref_quad_create.restype = vp
         L.ref_quad_create.argtypes = [C.c_int, C.c_int, vp, C.c_int, vp, vp, C.c_int, vp]
         L.ref_tet_create.restype = vp
@@ -236,6 +238,25 @@ def _tet_boundary_ctrl_idx(self):
 
 
 RefTetMesh.boundary_ctrl_idx = _tet_boundary_ctrl_idx
+
+
+class RefTriMesh(RefHexMesh):
+    """The reference's UnstructuredMesh<Tri> of a 2D mesh (+ scalar field "f")."""
+
+    ref_box_floats = 6    # SubRef<2,Simplex>: u, v axis vertices, origin
+
+    def __init__(self, order, ctrl_idx, xyz, field=None):
+        self.order = int(order)
+        self.ctrl_idx = np.ascontiguousarray(ctrl_idx, dtype=np.int32)
+        self.xyz = np.ascontiguousarray(xyz, dtype=np.float32).reshape(-1, 3)
+        self.field = None if field is None else np.ascontiguousarray(field, dtype=np.float32)
+        self.n_elem = self.ctrl_idx.size // ((self.order + 1) * (self.order + 2) // 2)
+        fptr = None if self.field is None else _p(self.field)
+        self.h = lib().ref_tri_create(self.order, self.n_elem, _p(self.ctrl_idx),
+                                      self.xyz.shape[0], _p(self.xyz), _p(self.ctrl_idx),
+                                      0 if self.field is None else self.field.size, fptr)
+        if not self.h:
+            raise RuntimeError(lib().ref_last_error().decode())
 
 
 def eval_tet_scalar(p, vals, refs, fixed=False):
