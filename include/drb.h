@@ -55,7 +55,8 @@ enum drb_shape
   DRB_SHAPE_TENSOR = 0,  /* hex (dim 3), quad (dim 2): (order+1)^dim dofs */
   DRB_SHAPE_SIMPLEX = 1  /* tet (dim 3): (order+1)(order+2)(order+3)/6 dofs in
                             the reference's order (i fastest, then j, then k;
-                            elem_ops.hpp:901-1030) */
+                            elem_ops.hpp:901-1030); triangle (dim 2):
+                            (order+1)(order+2)/2 dofs, i fastest */
 };
 
 /* A Bernstein mesh or field: GridFunction<ncomp> of the reference
@@ -64,14 +65,16 @@ enum drb_shape
  * accepted by drb_pack_elements, drb_elem_subboxes, drb_lbvh_build,
  * drb_bvh_widen, drb_locate, drb_locate_batched (and its ordered, host and
  * allocation-free forms, and drb_locate_tune), drb_field_eval,
- * drb_map_points and the volume renderer (drb_volume_integrate,
- * drb_volume_render, with a tet scalar field); the other entry points return
- * DRB_ERR_UNSUPPORTED for them.  2D quad meshes (dim 2) are located by the
- * same locate entry points and evaluated by drb_field_eval and
- * drb_map_points, besides their use as surfaces. */
+ * drb_map_points, the volume renderer (drb_volume_integrate,
+ * drb_volume_render, with a tet scalar field) and drb_mesh_boundary, whose
+ * triangle faces (dim 2, simplex) drb_surface_intersect and
+ * drb_surface_shade render; the hex-only face-neighbour table and the
+ * learned guess return DRB_ERR_UNSUPPORTED for them.  2D quad and triangle
+ * meshes (dim 2) are located by the same locate entry points and evaluated
+ * by drb_field_eval and drb_map_points, besides their use as surfaces. */
 typedef struct drb_mesh
 {
-  int dim;               /* 3 hex or tet, 2 quad */
+  int dim;               /* 3 hex or tet, 2 quad or triangle */
   int order;             /* polynomial order 1..3 */
   int ncomp;             /* 3 geometry, 1 scalar field */
   int n_elem;
