@@ -52,6 +52,43 @@ def test_noalloc_matches_allocating_path_twice(cuda):
         assert 0.85 < (c1 >= 0).float().mean().item() < 0.95
 
 
+@pytest.mark.parametrize("kind", ["tet", "quad"])
+def test_noalloc_other_element_types(cuda, kind):
+    """Tet and 2D quad meshes through the allocation-free entry point give
+    the allocating path's results."""
+    import torch
+    from devil_ray_b200 import _lib as L
+    from devil_ray_b200 import api, meshgen
+    lib = L.lib()
+    if kind == "tet":
+        m = meshgen.tet_warped_mesh(8, 2, 0.05, jitter=0.01, seed=4)
+        mesh = api.UnstructuredMesh(m.ctrl_idx, m.xyz, m.order, device=cuda, shape=L.SHAPE_SIMPLEX)
+        pts = torch.as_tensor(meshgen.uniform_queries(200_000, 8), device=cuda)
+    else:
+        m = meshgen.quad_warped_mesh(24, 2, 0.04, jitter=0.004, seed=4)
+        mesh = api.UnstructuredMesh(m.ctrl_idx, m.xyz, m.order, dim=2, device=cuda)
+        rng = np.random.default_rng(8)
+        xy = rng.uniform(-0.05, 1.05, size=(200_000, 2))
+        pts = torch.as_tensor(np.concatenate([xy, np.zeros((200_000, 1))], 1).astype(np.float32),
+                              device=cuda)
+    bvh = mesh.get_bvh()
+    mesh_d, bvh_d = mesh.desc(), bvh.desc()
+    stream = torch.cuda.current_stream().cuda_stream
+    opts = L.DrbNewtonOpts(1e-5, 20, L.GUESS_ELEM_CENTER, None)
+    n = pts.shape[0]
+    c0 = torch.empty(n, dtype=torch.int32, device=cuda)
+    r0 = torch.empty((n, 3), dtype=torch.float32, device=cuda)
+    c1 = torch.full_like(c0, -7)
+    r1 = torch.full_like(r0, 7.0)
+    assert _call(lib, L, "drb_locate_batched", mesh_d, bvh_d, pts, opts, c0, r0, stream) == 0
+    assert _call(lib, L, "drb_locate_batched_noalloc", mesh_d, bvh_d, pts, opts, c1, r1,
+                 stream) == 0, lib.drb_last_error()
+    torch.cuda.synchronize()
+    assert torch.equal(c0, c1)
+    assert torch.equal(r0.view(torch.int32), r1.view(torch.int32))
+    assert (c1 >= 0).float().mean().item() > 0.8
+
+
 def test_noalloc_rejects_oversized_call(cuda):
     import torch
     from devil_ray_b200 import _lib as L
