@@ -159,6 +159,16 @@ __global__ void locate_persistent_kernel (LocateParams lp, const float *__restri
   int sp = 0, cur = kBarrier;
   int iters = 0, cands = 0, nodes = 0;
   bool first = true;
+  // The last two elements whose solve failed for this query.  With a guess
+  // that does not depend on the leaf (zero, element centre, or a given
+  // guess whose centre fallback also ran) a repeat of one of them fails
+  // again the same way, so its solve is skipped.  Simplex kinds only: the
+  // sub-boxes of a tet or triangle overlap heavily (a query lies in about
+  // 20 tet sub-boxes of 3.6 distinct tets), those of a hex barely (1.3
+  // boxes of 1.04 hexes), where the check would only cost registers.
+  constexpr bool kSkipRepeats = (S == kSimplex || S == kTri2D);
+  const bool leaf_free_guess = kSkipRepeats && lp.guess_mode != DRB_GUESS_SUBREF_CENTER;
+  int failed0 = -1, failed1 = -1;
 
   while (true)
   {
@@ -193,6 +203,7 @@ __global__ void locate_persistent_kernel (LocateParams lp, const float *__restri
         cur = 0;
         iters = cands = nodes = 0;
         first = true;
+        failed0 = failed1 = -1;
       }
       pool_next += min (__popc (need), avail);
       need = __ballot_sync (FULL, qi < 0);
@@ -248,7 +259,8 @@ __global__ void locate_persistent_kernel (LocateParams lp, const float *__restri
       if (leaf >= 0)
       {
         ++cands;
-        const bool found = (S == kSimplex && lp.hull && hull_rejects (lp, el, pt))
+        const bool repeat = leaf_free_guess && (el == failed0 || el == failed1);
+        const bool found = (repeat || (S == kSimplex && lp.hull && hull_rejects (lp, el, pt)))
                            ? false
                            : (MODE == kRowsShared)
                            ? solve_candidate_smem<P> (lp, leaf, my_row, qi, first, pt, x, iters)
@@ -261,6 +273,11 @@ __global__ void locate_persistent_kernel (LocateParams lp, const float *__restri
         }
         else
         {
+          if (kSkipRepeats && !repeat)
+          {
+            failed1 = failed0;
+            failed0 = el;
+          }
           cur = todo[sp];
           --sp;
         }
