@@ -494,3 +494,31 @@ def test_tet_surface_curved_faces_lie_on_rays(cuda, p):
     torch.cuda.synchronize()
     assert (c_in >= 0).float().mean().item() > 0.98
     assert (c_out < 0).float().mean().item() > 0.98
+
+
+@pytest.mark.parametrize("p", ORDERS)
+@pytest.mark.parametrize("guess", ["zero", "center", "subref"])
+def test_tet_batched_skips_only_failing_solves(cuda, p, guess):
+    """The batched locate skips a candidate tet whose solve already failed
+    for the query (leaf-independent guesses) and tets whose hull planes
+    reject the query. Against the plain kernel, which solves every
+    candidate: the same cells and reference points bit for bit, the same
+    candidate counts, and never more Newton steps for any query."""
+    import torch
+    from devil_ray_b200 import _lib as L
+    from devil_ray_b200 import api, meshgen
+    m = _mesh(p)
+    g = _gpu(m, cuda)
+    mode = {"zero": L.GUESS_ZERO, "center": L.GUESS_ELEM_CENTER,
+            "subref": L.GUESS_SUBREF_CENTER}[guess]
+    pts = torch.as_tensor(meshgen.uniform_queries(60000, 91 + p), device=cuda)
+    c0, r0, it0, ca0, _ = g.locate(pts, tol=1e-5, max_steps=20, guess_mode=mode, stats=True)
+    bl = api.BatchedLocator(g, tol=1e-5, max_steps=20, guess_mode=mode)
+    c1, r1, it1, ca1, _ = bl.locate(pts, stats=True)
+    torch.cuda.synchronize()
+    assert torch.equal(c0, c1)
+    assert torch.equal(r0.view(torch.int32), r1.view(torch.int32))
+    assert torch.equal(ca0, ca1)
+    assert bool((it1 <= it0).all())
+    if guess != "subref":
+        assert it1.sum().item() < it0.sum().item()
