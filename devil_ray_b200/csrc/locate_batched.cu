@@ -159,7 +159,7 @@ __global__ void locate_persistent_kernel (LocateParams lp, const float *__restri
   int sp = 0, cur = kBarrier;
   int iters = 0, cands = 0, nodes = 0;
   bool first = true;
-  // The last two elements whose solve failed for this query.  With a guess
+  // The last three elements whose solve failed for this query.  With a guess
   // that does not depend on the leaf (zero, element centre, or a given
   // guess whose centre fallback also ran) a repeat of one of them fails
   // again the same way, so its solve is skipped.  Simplex kinds only: the
@@ -168,7 +168,7 @@ __global__ void locate_persistent_kernel (LocateParams lp, const float *__restri
   // boxes of 1.04 hexes), where the check would only cost registers.
   constexpr bool kSkipRepeats = (S == kSimplex || S == kTri2D);
   const bool leaf_free_guess = kSkipRepeats && lp.guess_mode != DRB_GUESS_SUBREF_CENTER;
-  int failed0 = -1, failed1 = -1;
+  int failed0 = -1, failed1 = -1, failed2 = -1;
 
   while (true)
   {
@@ -203,7 +203,7 @@ __global__ void locate_persistent_kernel (LocateParams lp, const float *__restri
         cur = 0;
         iters = cands = nodes = 0;
         first = true;
-        failed0 = failed1 = -1;
+        failed0 = failed1 = failed2 = -1;
       }
       pool_next += min (__popc (need), avail);
       need = __ballot_sync (FULL, qi < 0);
@@ -259,7 +259,7 @@ __global__ void locate_persistent_kernel (LocateParams lp, const float *__restri
       if (leaf >= 0)
       {
         ++cands;
-        const bool repeat = leaf_free_guess && (el == failed0 || el == failed1);
+        const bool repeat = leaf_free_guess && (el == failed0 || el == failed1 || el == failed2);
         const bool found = (repeat || (S == kSimplex && lp.hull && hull_rejects (lp, el, pt)))
                            ? false
                            : (MODE == kRowsShared)
@@ -275,6 +275,7 @@ __global__ void locate_persistent_kernel (LocateParams lp, const float *__restri
         {
           if (kSkipRepeats && !repeat)
           {
+            failed2 = failed1;
             failed1 = failed0;
             failed0 = el;
           }
