@@ -70,6 +70,11 @@ def parse():
     ap.add_argument("--profile", action="store_true",
                     help="profiling run: fixed launch shape, only the timed steps "
                          "(no tuning, plain/e2e/statistics/CPU legs)")
+    ap.add_argument("--launch", default="128,4,64,0", metavar="B,BPS,CHUNK,ROWS[,SORT]",
+                    help="launch shape of --profile: block, blocks per SM (0 = all "
+                         "resident), chunk, row mode, query order mode (default 1)")
+    ap.add_argument("--guess", default="centre", choices=["centre", "subref"],
+                    help="first guess of --profile")
     return ap.parse_args()
 
 
@@ -175,7 +180,7 @@ def reference_arm(args, rank, world):
                        "note": "reference Newton tolerance is hard-coded to 1e-4; each step "
                                "locates a bounded sample of the workload's queries"},
             "cpu_baseline": {"value": value, "unit": "points/s", "cores": threads,
-                             "kind": "reference",
+                             "kind": "reference", "threads_used": threads, **host_info(),
                              "sample": f"{sample} of the 16M queries per step, BVH built once "
                                        f"({build_s:.1f} s, not timed)"},
             "e2e": {"value": value, "unit": "points/s", "h2d_bytes_per_step": 0,
@@ -184,8 +189,34 @@ def reference_arm(args, rank, world):
     return 0
 
 
-def cpu_baseline(mesh_data, queries, bvh_np):
-    """Reference CPU locate on a bounded sample (about 10-20 s of work)."""
+def host_info():
+    """The host the CPU legs run on: logical CPUs, the ones this process may
+    use, OpenMP's thread count in the reference build, and the CPU model."""
+    model = None
+    try:
+        for ln in Path("/proc/cpuinfo").read_text().splitlines():
+            if ln.startswith("model name"):
+                model = ln.split(":", 1)[1].strip()
+                break
+    except OSError:
+        pass
+    try:
+        usable = len(os.sched_getaffinity(0))
+    except AttributeError:
+        usable = os.cpu_count()
+    info = {"nproc": os.cpu_count(), "usable_cpus": usable, "cpu_model": model}
+    try:
+        from oracle import refpy
+        if refpy.available():
+            info["omp_max_threads"] = refpy.num_threads()
+    except Exception:
+        pass
+    return info
+
+
+def cpu_baseline(mesh_data, queries, bvh):
+    """Reference CPU locate on a bounded sample (about 10-20 s of work), plus
+    the restated locate at the GPU path's tol 1e-5 on the same host cores."""
     from oracle import refpy
     if not refpy.available():
         return None
@@ -203,10 +234,39 @@ def cpu_baseline(mesh_data, queries, bvh_np):
     cell, _ = r.locate(q)
     t = time.perf_counter() - t0
     located = int((cell >= 0).sum())
-    return {"value": located / t, "unit": "points/s", "cores": refpy.num_threads(),
-            "kind": "reference",
-            "sample": f"{sample} of the 16M queries (reference tol 1e-4, 20 steps), "
-                      f"{t:.1f} s; reference BVH build {build_s:.1f} s not timed"}
+    threads = refpy.num_threads()
+    out = {"value": located / t, "unit": "points/s", "cores": threads,
+           "kind": "reference", "threads_used": threads, **host_info(),
+           "sample": f"{sample} of the 16M queries (reference tol 1e-4, 20 steps), "
+                     f"{t:.1f} s; reference BVH build {build_s:.1f} s not timed"}
+    # tol 1e-5: the reference fixes 1e-4, so this figure comes from the
+    # restated locate (same traversal and Newton steps, tol and steps as
+    # parameters, element-centre guess, local frame) over the GPU's BVH
+    try:
+        from oracle import restate
+        if restate.available():
+            bvh_np = {"inner": bvh.inner_nodes.cpu().numpy(),
+                      "leaf_nodes": bvh.leaf_nodes.cpu().numpy(),
+                      "aabb_ids": bvh.aabb_ids.cpu().numpy(),
+                      "ref_boxes": bvh.ref_boxes.cpu().numpy()}
+            qs = queries[:8192]
+            t0 = time.perf_counter()
+            restate.locate(mesh_data.order, mesh_data.ctrl_idx, mesh_data.xyz, bvh_np, qs, TOL,
+                           MAX_STEPS, 1, local_frame=True)
+            tp = time.perf_counter() - t0
+            s5 = int(min(len(queries), max(8192, 8192 * 8.0 / max(tp, 1e-3))))
+            t0 = time.perf_counter()
+            c5, _, it5, _ = restate.locate(mesh_data.order, mesh_data.ctrl_idx, mesh_data.xyz,
+                                           bvh_np, queries[:s5], TOL, MAX_STEPS, 1,
+                                           local_frame=True)
+            t5 = time.perf_counter() - t0
+            out["restated_tol_1e-5"] = {
+                "value": int((c5 >= 0).sum()) / t5, "unit": "points/s", "cores": threads,
+                "kind": "port", "seconds": t5, "mean_newton_iters": float(it5.mean()),
+                "sample": f"{s5} of the 16M queries, tol 1e-5, 20 steps, element-centre guess"}
+    except Exception as exc:
+        out["restated_tol_1e-5"] = {"error": repr(exc)}
+    return out
 
 
 def volume_c0(dev, with_cpu):
@@ -390,6 +450,96 @@ def tet_locate(dev, args, with_cpu):
     return out
 
 
+def learned_leg(dev, args, mesh, pts, cfg, timed, job_located, baselines, plain_value,
+                mean_it_centre):
+    """Train the guess network on the mesh (4M Newton solutions of the
+    method itself, the library's tcgen05 kernels) and time the learned-guess
+    path on the held-out queries: located pts/s, its iteration histogram,
+    the fallback rate of the guessed solves on held-out in-element pairs, and
+    its ratio to the plain kernel and to the batched paths without it."""
+    import torch
+    from devil_ray_b200 import learned as LG
+    n = pts.shape[0]
+    t0 = time.perf_counter()
+    model = LG.GuessMLP(dev, seed=1)
+    losses = LG.train(model, mesh, samples=args.train_samples, batch=16384, epochs=3, lr=3e-3)
+    torch.cuda.synchronize()
+    train_s = time.perf_counter() - t0
+    model.check_err()
+    ll = LG.LearnedLocator(mesh, model, TOL, MAX_STEPS, config=cfg)
+    cell_l = torch.empty(n, dtype=torch.int32, device=dev)
+    ref_l = torch.empty((n, 3), dtype=torch.float32, device=dev)
+    for _ in range(3):
+        ll.locate(pts, out=(cell_l, ref_l))
+    ms_l = timed(lambda: ll.locate(pts, out=(cell_l, ref_l)), args.steps) / args.steps
+    located_l = int((cell_l >= 0).sum().item())
+    _, _, it_l, _, _ = ll.locate(pts, stats=True)
+    hist_l = torch.bincount(it_l.long().clamp(max=40), minlength=41).cpu().numpy().tolist()
+    he, hp, hl, hw = LG.training_set(mesh, 1 << 20, seed=12345)
+    gss = model.guess(mesh, he, hp)
+    _, fg, ig = LG.newton_pairs(mesh, he, hp, TOL, MAX_STEPS, gss)
+    _, fc, ic = LG.newton_pairs(mesh, he, hp, TOL, MAX_STEPS)
+    ok = fc
+    value = job_located(located_l) / (ms_l * 1e-3)
+    out = {"value": value, "ms_per_step": ms_l, "located": located_l,
+           "mean_newton_iters": float(it_l.float().mean()),
+           "mean_newton_iters_centre": mean_it_centre,
+           "iteration_histogram": hist_l,
+           "held_out_pairs": {"fallback_rate": float(1.0 - fg[ok].float().mean()),
+                              "mean_iters_guess": float(ig[ok].float().mean()),
+                              "mean_iters_centre": float(ic[ok].float().mean())},
+           "train": {"samples": args.train_samples, "epochs": 3, "batch": 16384,
+                     "seconds": train_s, "first_loss": losses[0], "final_loss": losses[-1]},
+           "speedup_vs_plain": value / plain_value,
+           "_locate": ll.locate}
+    for k, v in baselines.items():
+        out[f"ratio_vs_{k}"] = value / v
+    return out
+
+
+def second_mesh_leg(dev, args, pts, cfg, timed, job_located):
+    """The learned-guess config's second mesh (64^3 order 2, 25 % trilinear
+    distortion): the same held-out queries located by the plain kernel, the
+    batched kernel with the sub-box-centre guess, and the learned path
+    trained on this mesh."""
+    import torch
+    from devil_ray_b200 import _lib as L
+    from devil_ray_b200 import api, meshgen
+    m = meshgen.workload_mesh("locate_64_d25")
+    mesh = api.UnstructuredMesh(m.ctrl_idx, m.xyz, m.order, device=dev)
+    mesh.get_bvh()
+    n = pts.shape[0]
+    cell = torch.empty(n, dtype=torch.int32, device=dev)
+    ref = torch.empty((n, 3), dtype=torch.float32, device=dev)
+    plain = lambda: mesh.locate(pts, tol=TOL, max_steps=MAX_STEPS,
+                                guess_mode=L.GUESS_ELEM_CENTER)
+    plain()
+    k = max(2, args.steps // 5)
+    plain_ms = timed(plain, k) / k
+    sub = api.BatchedLocator(mesh, tol=TOL, max_steps=MAX_STEPS,
+                             guess_mode=L.GUESS_SUBREF_CENTER, config=cfg)
+    for _ in range(2):
+        sub.locate(pts, out=(cell, ref))
+    sub_ms = timed(lambda: sub.locate(pts, out=(cell, ref)), args.steps) / args.steps
+    located = int((cell >= 0).sum().item())
+    _, _, it_s, _, _ = sub.locate(pts, stats=True)
+    plain_value = job_located(located) / (plain_ms * 1e-3)
+    sub_value = job_located(located) / (sub_ms * 1e-3)
+    centre = api.BatchedLocator(mesh, tol=TOL, max_steps=MAX_STEPS,
+                                guess_mode=L.GUESS_ELEM_CENTER, config=cfg)
+    _, _, it_c, _, _ = centre.locate(pts, stats=True)
+    lg = learned_leg(dev, args, mesh, pts, cfg, timed, job_located,
+                     {"batched_subref": sub_value}, plain_value, float(it_c.float().mean()))
+    lg.pop("_locate", None)
+    return {"workload": "locate_64_d25: 64^3 hex order 2, trilinear distortion 25%, the same "
+                        f"{n} held-out queries, tol 1e-5, 20 steps",
+            "located_fraction": located / n,
+            "plain": {"value": plain_value, "ms_per_step": plain_ms},
+            "batched_subref": {"value": sub_value, "ms_per_step": sub_ms,
+                               "mean_newton_iters": float(it_s.float().mean())},
+            "learned": lg}
+
+
 def orbit_cameras(count, width, seed=5):
     """Orbits about the mesh centre at the distance of the (2.5,2.5,2.5)
     camera: azimuth k * 22.5 degrees plus a seeded elevation jitter."""
@@ -408,12 +558,60 @@ def orbit_cameras(count, width, seed=5):
     return cams
 
 
-# DRAM bytes (read + write) of one locate_persistent_kernel launch on this
-# workload (16M queries, 4-wide tree), from an ncu capture of the same launch
-# (profiles/locate_persistent_kernel__locate_64_16M_queries.md): 4.016 GB
-# read + 1.194 GB written.  Used for roofline.traffic, scaled by the query
-# count when --queries differs.
-LOCATE_TRAFFIC_16M = 4.016342e9 + 1.193831e9
+class DramMeter:
+    """DRAM bytes moved on one GPU over an interval, measured live through
+    NVML's GPU performance monitoring (GPM): the DRAM bandwidth utilisation
+    between two samples, times the memory's theoretical bandwidth (bus width
+    x memory clock x 2), times the interval.  Read-only counters; returns
+    None where the device or driver does not offer GPM."""
+
+    def __init__(self, gpu_index: int):
+        self.ok = False
+        try:
+            import pynvml as N
+            N.nvmlInit()
+            self.N = N
+            self.h = N.nvmlDeviceGetHandleByIndex(gpu_index)
+            sup = N.nvmlGpmQueryDeviceSupport(self.h)
+            if not getattr(sup, "isSupportedDevice", 0):
+                return
+            bus_bits = N.nvmlDeviceGetMemoryBusWidth(self.h)
+            mem_mhz = N.nvmlDeviceGetMaxClockInfo(self.h, N.NVML_CLOCK_MEM)
+            self.theoretical_gbs = bus_bits / 8 * mem_mhz * 1e6 * 2 / 1e9
+            self.s0 = N.nvmlGpmSampleAlloc()
+            self.s1 = N.nvmlGpmSampleAlloc()
+            self.ok = True
+        except Exception:
+            self.ok = False
+
+    def start(self):
+        if self.ok:
+            try:
+                self.N.nvmlGpmSampleGet(self.h, self.s0)
+                self.t0 = time.perf_counter()
+            except Exception:
+                self.ok = False
+
+    def stop(self):
+        """(DRAM GB/s averaged over the interval, seconds), or None."""
+        if not self.ok:
+            return None
+        try:
+            N = self.N
+            N.nvmlGpmSampleGet(self.h, self.s1)
+            dt = time.perf_counter() - self.t0
+            mg = N.c_nvmlGpmMetricsGet_t()
+            mg.version = N.NVML_GPM_METRICS_GET_VERSION
+            mg.numMetrics = 1
+            mg.sample1 = self.s0
+            mg.sample2 = self.s1
+            mg.metrics[0].metricId = N.NVML_GPM_METRIC_DRAM_BW_UTIL
+            N.nvmlGpmMetricsGet(mg)
+            util = float(mg.metrics[0].value)
+            return util / 100.0 * self.theoretical_gbs, dt
+        except Exception:
+            return None
+
 
 # FP32 pipe peak of a B200: 148 SMs x 128 FP32 lanes x 2 FLOP (FMA) x 1.965 GHz
 FP32_PEAK_TFLOPS = 148 * 128 * 2 * 1.965e9 / 1e12
@@ -431,8 +629,60 @@ def newton_step_flops(p):
     return basis + eval_d + 3 + 40 + 18
 
 
-def volume_bench(dev, args, timed):
-    """128^3 order-3 volume (SURVEY config 4): 2048^2 rays, 1000 samples,
+def volume_cpu_tiles(m, bvh, cams, lights, samp, args, tile=64, seed=6):
+    """The reference's OpenMP Volume::integrate on one seeded tile x tile
+    block of each orbit's rays (the 2048^2 frame's own ray records), over
+    the GPU-built BVH installed in the reference mesh: its own build cannot
+    run at 69.2M sub-boxes.  The rate is per resolved sample, counted by
+    the GPU march on the same rays, so it stands for the full frames as an
+    extrapolation from the tiles."""
+    import torch
+    from oracle import refpy
+    from devil_ray_b200 import _lib as L
+    from devil_ray_b200 import meshgen
+    from devil_ray_b200.api import _ptr
+    need = 40 << 30
+    try:
+        avail = int([ln for ln in Path("/proc/meminfo").read_text().splitlines()
+                     if ln.startswith("MemAvailable")][0].split()[1]) * 1024
+    except Exception:
+        avail = 0
+    if avail < need:
+        return {"skipped": f"host memory available {avail / 2**30:.0f} GiB < 40 GiB"}
+    r = refpy.RefHexMesh(m.order, m.ctrl_idx, m.xyz, m.field)
+    t0 = time.perf_counter()
+    r.set_bvh(bvh.inner_nodes.cpu().numpy(), bvh.leaf_nodes.cpu().numpy(),
+              bvh.aabb_ids.cpu().numpy(), bvh.bounds, bvh.ref_boxes.cpu().numpy())
+    install_s = time.perf_counter() - t0
+    W = cams[0].width
+    rng = np.random.default_rng(seed)
+    rays = torch.empty((W * W, 9), dtype=torch.float32, device=samp[0].device)
+    seconds, samples, partials = 0.0, 0, 0
+    import ctypes as C
+    for k, cam in enumerate(cams):
+        L.check(L.lib().drb_camera_rays(C.byref(cam.desc()), _ptr(rays), None), "rays")
+        # a tile inside the central half of the frame, where the mesh projects
+        i0, j0 = (int(x) for x in rng.integers(W // 4, 3 * W // 4 - tile, size=2))
+        pix = (np.arange(j0, j0 + tile)[:, None] * W + np.arange(i0, i0 + tile)[None, :]).ravel()
+        pix_t = torch.as_tensor(pix, device=rays.device)
+        tr = rays[pix_t].cpu().numpy()
+        samples += int(samp[k][pix_t].sum().item())
+        t1 = time.perf_counter()
+        parts = r.volume_rays(tr, 1000, True, 1024, np.array(meshgen.TF_RGB, np.float32),
+                              np.array(meshgen.TF_ALPHA, np.float32), lights[k].as13()[None])
+        seconds += time.perf_counter() - t1
+        partials += parts.shape[0]
+    return {"value": samples / seconds, "unit": "samples/s", "seconds": seconds,
+            "samples": samples, "partials": partials, "cores": refpy.num_threads(),
+            "kind": "reference", "bvh_install_s": install_s,
+            "sample": f"one seeded {tile}x{tile} ray tile of each of the {len(cams)} orbits "
+                      f"({len(cams) * tile * tile} rays), extrapolated to the 2048^2 frames "
+                      "by the per-sample rate; reference tol 1e-4 (fixed), samples counted by "
+                      "the GPU's coherent march on the same rays"}
+
+
+def volume_bench(dev, args, timed, with_cpu=False):
+    """128^3 order-3 volume: 2048^2 rays, 1000 samples,
     1024-entry transfer function, `orbits` seeded cameras replayed from one
     CUDA graph; Newton-resolved samples/s of the coherent march and of the
     plain march (a full BVH locate per sample, one frame)."""
@@ -446,7 +696,8 @@ def volume_bench(dev, args, timed):
     gen_s = time.perf_counter() - t0
     mesh = api.UnstructuredMesh(m.ctrl_idx, m.xyz, m.order, device=dev)
     field = UnstructuredField(m.ctrl_idx, m.field, m.order, device=dev)
-    del m
+    if not with_cpu:
+        del m
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     e0.record()
     mesh.get_bvh()
@@ -522,7 +773,18 @@ def volume_bench(dev, args, timed):
     ms_plain = timed(lambda: frame(0, False), 1)
     samples_plain = int(samp[0].sum().item())
     img = fbs[0].image()
+    cpu = None
+    if with_cpu:
+        # per-ray sample counts of the coherent orbits, for the CPU tiles
+        g.replay()
+        torch.cuda.synchronize()
+        try:
+            cpu = volume_cpu_tiles(m, mesh.get_bvh(), cams, lights, samp, args)
+        except Exception as exc:
+            cpu = {"error": repr(exc)}
+        del m
     return {
+        "cpu_reference": cpu,
         "workload": "volume_128: 128^3 hex order 3 (2.1M elements, 69.2M sub-box leaves), "
                     "warp 0.05, 8 Gaussian blobs; 2048^2 rays, 1000 samples, 1024-entry TF, "
                     f"{len(cams)} orbits in one CUDA graph, tol 1e-5",
@@ -633,8 +895,12 @@ def main():
     n = pts.shape[0]
     loc = api.BatchedLocator(mesh, tol=TOL, max_steps=MAX_STEPS, guess_mode=L.GUESS_ELEM_CENTER)
     if args.profile:
-        best_cfg = L.DrbLocateConfig(128, 4, 64, 1, 0)
+        shape = [int(x) for x in args.launch.split(",")]
+        b, bps, ch, rows = shape[:4]
+        best_cfg = L.DrbLocateConfig(b, bps, ch, shape[4] if len(shape) > 4 else 1, rows)
         loc.config, tune_ms = best_cfg, 0.0
+        if args.guess == "subref":
+            loc.guess_mode = L.GUESS_SUBREF_CENTER
     else:
         best_cfg, tune_ms = loc.tune(pts[: min(n, 1 << 21)])
     cell = torch.empty(n, dtype=torch.int32, device=dev)
@@ -669,10 +935,24 @@ def main():
         launches0 = L.lib().drb_kernel_launches()
         ms_step = timed(batched_step, args.steps) / args.steps
         launches = L.lib().drb_kernel_launches() - launches0
+        # the kernel alone on staged records, with the live DRAM meter
+        staged = loc.stage(pts)
+        records = best_cfg.sort_queries == 2
+        res4 = torch.empty((n, 4), dtype=torch.float32, device=dev) if records else (cell, ref)
+        loc.locate_staged(staged, out=res4, records=records)
+        dram = DramMeter(local)
+        dram.start()
+        kern_ms = timed(lambda: loc.locate_staged(staged, out=res4, records=records),
+                        args.steps) / args.steps
+        dr = dram.stop()
         if rank == 0:
             print(json.dumps({"profile": True, "ms_per_step": ms_step, "queries": n,
                               "located": int((cell >= 0).sum().item()),
-                              "launches_per_step": launches / args.steps}))
+                              "launches_per_step": launches / args.steps,
+                              "kernel_ms": kern_ms, "launch": args.launch, "guess": args.guess,
+                              "gpm_dram_gbs": dr[0] if dr else None,
+                              "gpm_dram_bytes_per_launch":
+                                  dr[0] * 1e9 * dr[1] / args.steps if dr else None}))
         if pg:
             pg.barrier()
             pg.destroy_process_group()
@@ -698,9 +978,6 @@ def main():
     k_plain = max(2, args.steps // 5)
     plain_ms = timed(plain_step, k_plain) / k_plain
     plain_value = job_located(located) / (plain_ms * 1e-3)
-    # persistent kernel alone (roofline), queries already ordered
-    order = loc.order(pts)
-    kern_ms = timed(lambda: loc.locate(pts, order=order, out=(cell, ref)), args.steps) / args.steps
 
     # the sub-box-centre first guess: the centre of the candidate leaf's
     # reference sub-box, the reference's intent (device_mesh.hpp:161-162)
@@ -710,12 +987,14 @@ def main():
         loc_sub.locate(pts, out=(cell, ref))
     sub_ms = timed(lambda: loc_sub.locate(pts, out=(cell, ref)), args.steps) / args.steps
     sub_located = int((cell >= 0).sum().item())
-    _, _, it_s, _, _ = loc_sub.locate(pts, stats=True)
+    _, _, it_s, ca_s, nd_s = loc_sub.locate(pts, stats=True)
+    sub_stats = (float(it_s.float().mean()), float(ca_s.float().mean()),
+                 float(nd_s.float().mean()))
     sub_value = job_located(sub_located) / (sub_ms * 1e-3)
     batched_sub = {"value": sub_value, "ms_per_step": sub_ms,
-                   "mean_newton_iters": float(it_s.float().mean()),
+                   "mean_newton_iters": sub_stats[0],
                    "note": "Morton-ordered persistent kernel, sub-box-centre guess"}
-    del it_s
+    del it_s, ca_s, nd_s
 
     # many small batches: 64K queries per call, eager calls vs one CUDA graph
     # replay per batch (BatchedLocator.capture); same results either way
@@ -753,48 +1032,38 @@ def main():
     if sub_value > head_value:
         head_name, head_locate, head_loc, head_value = ("batched (sub-box-centre guess)",
                                                         loc_sub.locate, loc_sub, sub_value)
+    # the kernel of the faster batched path alone (roofline): its queries
+    # already staged in processing order, the same launch shape
+    roof_loc = head_loc
+    roof_stats = sub_stats if roof_loc is loc_sub else (mean_it, mean_ca, mean_nd)
+    staged = roof_loc.stage(pts)
+    for _ in range(2):
+        roof_loc.locate_staged(staged, out=(cell, ref))
+    dram = DramMeter(local)
+    dram.start()
+    kern_ms = timed(lambda: roof_loc.locate_staged(staged, out=(cell, ref)),
+                    args.steps) / args.steps
+    dram_read = dram.stop()
+    del staged
     learned = None
     if not args.no_learned and m.order == 2:
-        from devil_ray_b200 import learned as LG
-        t0 = time.perf_counter()
-        model = LG.GuessMLP(dev, seed=1)
-        losses = LG.train(model, mesh, samples=args.train_samples, batch=16384, epochs=3,
-                          lr=3e-3)
-        torch.cuda.synchronize()
-        train_s = time.perf_counter() - t0
-        model.check_err()
-        ll = LG.LearnedLocator(mesh, model, TOL, MAX_STEPS, config=best_cfg)
-        cell_l = torch.empty_like(cell)
-        ref_l = torch.empty_like(ref)
-        for _ in range(3):
-            ll.locate(pts, out=(cell_l, ref_l))
-        ms_l = timed(lambda: ll.locate(pts, out=(cell_l, ref_l)), args.steps) / args.steps
-        located_l = int((cell_l >= 0).sum().item())
-        _, _, it_l, ca_l, nd_l = ll.locate(pts, stats=True)
-        agree = float((cell_l == cell).float().mean().item())
-        hist_l = torch.bincount(it_l.long().clamp(max=40), minlength=41).cpu().numpy().tolist()
-        # fallback rate of the guessed first-candidate solves (held-out pairs)
-        he, hp, hl, hw = LG.training_set(mesh, 1 << 20, seed=12345)
-        gss = model.guess(mesh, he, hp)
-        _, fg, ig = LG.newton_pairs(mesh, he, hp, TOL, MAX_STEPS, gss)
-        _, fc, ic = LG.newton_pairs(mesh, he, hp, TOL, MAX_STEPS)
-        ok = fc
-        learned_value = job_located(located_l) / (ms_l * 1e-3)
-        learned = {"value": learned_value, "ms_per_step": ms_l, "located": located_l,
-                   "cell_agreement_with_centre_guess": agree,
-                   "mean_newton_iters": float(it_l.float().mean()),
-                   "mean_newton_iters_centre": mean_it,
-                   "iteration_histogram": hist_l,
-                   "held_out_pairs": {"fallback_rate": float(1.0 - fg[ok].float().mean()),
-                                      "mean_iters_guess": float(ig[ok].float().mean()),
-                                      "mean_iters_centre": float(ic[ok].float().mean())},
-                   "train": {"samples": args.train_samples, "epochs": 3, "batch": 16384,
-                             "seconds": train_s, "first_loss": losses[0],
-                             "final_loss": losses[-1]},
-                   "speedup_vs_plain": learned_value / plain_value}
-        if learned_value > head_value:
-            head_name, head_locate, head_loc, head_value = ("learned guess + batched", ll.locate,
-                                                            None, learned_value)
+        try:
+            learned = learned_leg(dev, args, mesh, pts, best_cfg, timed, job_located,
+                                  {"batched_subref": sub_value, "batched_centre": batched_value},
+                                  plain_value, mean_it)
+        except Exception as exc:
+            learned = {"error": repr(exc)}
+        if learned.get("value", 0.0) > head_value:
+            head_name, head_locate, head_loc, head_value = ("learned guess + batched",
+                                                            learned.pop("_locate"), None,
+                                                            learned["value"])
+        learned.pop("_locate", None)
+    learned_d25 = None
+    if not args.no_learned:
+        try:
+            learned_d25 = second_mesh_leg(dev, args, pts, best_cfg, timed, job_located)
+        except Exception as exc:
+            learned_d25 = {"error": repr(exc)}
 
     # headline: the faster path, timed again with clock sampling
     def head_step():
@@ -811,16 +1080,28 @@ def main():
     located = int((cell >= 0).sum().item())
     value = job_located(located) / (ms_step * 1e-3)
 
-    # algorithmic bytes per located point: point 12 B + Location 16 B + one
-    # element's control-point indices and coordinates nd x (4 + 12) B + its
-    # reference box 24 B + 64 B per binary inner node the reference's
-    # traversal visits
+    # Compulsory DRAM bytes of one kernel launch: each staged query record
+    # read (16 B) and result record written (16 B) once, and the arrays the
+    # traversal and the solves read at least once over a batch that covers
+    # the mesh: the 4-wide tree (128 B per node), the leaf element ids, the
+    # packed element rows, and for the sub-box-centre guess the leaf sub-box
+    # ids and reference boxes.  Repeated visits are served by the caches, so
+    # these bytes are the floor of the launch's DRAM traffic.
+    stride = L.lib().drb_packed_stride(3, m.order, 3)
+    sub_guess = roof_loc is loc_sub
+    compulsory = (n * (16 + 16) + bvh.n_wide * 128 + bvh.n_leaf * 4 + m.n_elem * stride * 4
+                  + (bvh.n_leaf * (4 + 24) if sub_guess else 0))
+    achieved_gbs = compulsory / (kern_ms * 1e-3) / 1e9
+    # the per-query figure of the algorithmic byte formula (point 12 B +
+    # Location 16 B + one element's indices and coordinates nd x (4 + 12) B +
+    # its reference box 24 B + 64 B per binary inner node the reference's
+    # traversal visits): every visit counted, cache hits included
     nd_dofs = (m.order + 1) ** 3
     bytes_q = 12 + 16 + nd_dofs * 16 + 24 + 64 * mean_nd_binary
-    achieved_gbs = n * bytes_q / (kern_ms * 1e-3) / 1e9
+    r_it, r_ca, r_nd = roof_stats
     # FP32 work of the same launch: Newton steps, inside tests (6 compares
     # per candidate) and box tests (24 compares per 4-wide node visited)
-    flops_q = mean_it * newton_step_flops(m.order) + 6 * mean_ca + 24 * mean_nd
+    flops_q = r_it * newton_step_flops(m.order) + 6 * r_ca + 24 * r_nd
     achieved_tflops = n * flops_q / (kern_ms * 1e-3) / 1e12
     peaks = {}
     try:
@@ -829,6 +1110,10 @@ def main():
         pass
     peak = peaks.get("hbm_gbs", 6650.0)
     peak_src = "measured" if "hbm_gbs" in peaks else "fallback"
+    traffic = None
+    if dram_read is not None:
+        dram_gbs, dram_s = dram_read
+        traffic = dram_gbs * 1e9 * dram_s / args.steps
 
     # end to end through the public API: pinned host queries -> device ->
     # locate -> cell ids and reference points back to pinned host memory
@@ -856,7 +1141,8 @@ def main():
     vol = None
     if not args.no_volume:
         try:
-            vol = volume_bench(dev, args, timed)
+            vol = volume_bench(dev, args, timed,
+                               with_cpu=rank == 0 and world == 1 and not args.no_cpu_baseline)
         except Exception as exc:
             vol = {"error": repr(exc)}
 
@@ -884,7 +1170,7 @@ def main():
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         try:
-            cpu = cpu_baseline(m, queries, None)
+            cpu = cpu_baseline(m, queries, bvh)
         except Exception as exc:  # the baseline is reported, never required
             cpu = {"error": str(exc)}
 
@@ -901,12 +1187,28 @@ def main():
                        "parallelism": f"replicas x{world}, queries sharded, no collective"},
             "roofline": {"bound": "hbm", "achieved": achieved_gbs, "peak": peak, "unit": "GB/s",
                          "frac": achieved_gbs / peak,
-                         "traffic": LOCATE_TRAFFIC_16M * n / float(1 << 24),
-                         "traffic_source": "ncu capture of the same kernel on 16M queries, "
-                                           "scaled by queries",
-                         "peak_source": peak_src, "kernel": "locate_persistent_kernel",
-                         "bytes_per_query": bytes_q, "kernel_ms": kern_ms,
-                         "kernel_guess": "element centre",
+                         "traffic": traffic,
+                         "achieved_bytes": "compulsory DRAM bytes per launch: 16 B query "
+                                           "record in + 16 B result (cell + reference point) "
+                                           "out per query, the 4-wide tree, leaf ids and "
+                                           "packed rows once"
+                                           + (", leaf sub-box ids and reference boxes once"
+                                              if sub_guess else ""),
+                         "compulsory_bytes_per_launch": compulsory,
+                         "traffic_source": "DRAM bytes per launch measured live over the timed "
+                                           "kernel loop (NVML GPM DRAM bandwidth utilisation x "
+                                           "theoretical bandwidth x interval)"
+                                           if traffic is not None else
+                                           "not measurable inside the run (NVML GPM sampling "
+                                           "refused); measured by ncu outside the timed run",
+                         "dram_gbs": (traffic / (kern_ms * 1e-3) / 1e9) if traffic else None,
+                         "dram_frac": (traffic / (kern_ms * 1e-3) / 1e9 / peak) if traffic
+                         else None,
+                         "peak_source": peak_src, "kernel": "locate_persistent_kernel (staged)",
+                         "kernel_ms": kern_ms, "kernel_guess": "sub-box centre" if sub_guess
+                         else "element centre", "launch_config": roof_loc.config.as_dict(),
+                         "cache_inclusive_bytes_per_query": bytes_q,
+                         "cache_inclusive_gbs": n * bytes_q / (kern_ms * 1e-3) / 1e9,
                          "fp32": {"flops_per_query": flops_q, "achieved_tflops": achieved_tflops,
                                   "peak_tflops": FP32_PEAK_TFLOPS,
                                   "frac": achieved_tflops / FP32_PEAK_TFLOPS,
@@ -931,6 +1233,7 @@ def main():
                         "note": "Morton-ordered persistent kernel, element-centre guess"},
             "graph_small_batches": graph_small,
             "learned": learned,
+            "learned_d25": learned_d25,
             "volume": vol,
             "volume_c0": vol_c0,
             "surface": surf_c1,

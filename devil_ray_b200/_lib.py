@@ -105,6 +105,10 @@ _SIGS = {
     "drb_ray_max": (C.c_int, [C.c_void_p, C.c_void_p, C.c_int, C.c_void_p]),
     "drb_camera_rays": (C.c_int, [C.POINTER(DrbCamera), C.c_void_p, C.c_void_p]),
     "drb_default_light": (C.c_int, [C.POINTER(DrbCamera), C.c_void_p]),
+    "drb_camera_elevate": (C.c_int, [C.POINTER(DrbCamera), C.c_float]),
+    "drb_camera_azimuth": (C.c_int, [C.POINTER(DrbCamera), C.c_float]),
+    "drb_camera_reset_to_bounds": (C.c_int, [C.POINTER(DrbCamera), C.c_void_p, C.c_double,
+                                             C.c_double, C.c_double]),
     "drb_cull_rays": (C.c_int, [C.c_void_p, C.c_int, C.c_void_p, C.c_void_p,
                                 C.POINTER(C.c_int), C.c_void_p]),
     "drb_field_range": (C.c_int, [C.POINTER(DrbMesh), C.c_void_p, C.c_void_p]),
@@ -128,6 +132,11 @@ _SIGS = {
                                      C.c_void_p, DrbQueryStats, C.c_void_p]),
     "drb_query_order": (C.c_int, [C.POINTER(DrbBvh), C.c_void_p, C.c_int, C.c_void_p,
                                   C.c_void_p]),
+    "drb_query_stage": (C.c_int, [C.POINTER(DrbBvh), C.c_void_p, C.c_int, C.c_void_p,
+                                  C.c_void_p]),
+    "drb_locate_staged": (C.c_int, [C.POINTER(DrbMesh), C.POINTER(DrbBvh), C.c_void_p, C.c_int,
+                                    C.POINTER(DrbNewtonOpts), C.c_void_p, C.c_void_p,
+                                    C.c_void_p, C.c_void_p, DrbQueryStats, C.c_void_p]),
     "drb_locate_ordered": (C.c_int, [C.POINTER(DrbMesh), C.POINTER(DrbBvh), C.c_void_p, C.c_int,
                                      C.c_void_p, C.POINTER(DrbNewtonOpts), C.c_void_p,
                                      C.c_void_p, C.c_void_p, DrbQueryStats, C.c_void_p]),

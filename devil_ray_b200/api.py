@@ -279,6 +279,41 @@ class BatchedLocator:
                                         _stream(stream)), "drb_query_order")
         return o
 
+    def stage(self, points, stream=None):
+        """Query records (x, y, z, input index bits) in processing order
+        (drb_query_stage), as a float32 tensor of shape (n, 4)."""
+        pts = _dev(points, torch.float32, self.mesh.device).reshape(-1, 3)
+        rec = torch.empty((pts.shape[0], 4), dtype=torch.float32, device=self.mesh.device)
+        bd = self._bvh(stream).desc()
+        L.check(L.lib().drb_query_stage(C.byref(bd), _ptr(pts), pts.shape[0], _ptr(rec),
+                                        _stream(stream)), "drb_query_stage")
+        return rec
+
+    def locate_staged(self, staged, out=None, records=False, stream=None):
+        """The persistent kernel alone on staged records (drb_locate_staged).
+        records=True: returns (n, 4) records (cell bits, r, s, t) in the
+        staged order; else (cell, ref) at the queries' input indices, as
+        drb_locate_batched writes them (out = (cell, ref) to reuse)."""
+        n = staged.shape[0]
+        dev = self.mesh.device
+        opts = L.DrbNewtonOpts(self.tol, self.max_steps, self.guess_mode, None)
+        cfg = None if self.config is None else C.byref(self.config)
+        d = self.mesh.desc()
+        bd = self._bvh(stream).desc()
+        if records:
+            res = torch.empty((n, 4), dtype=torch.float32, device=dev) if out is None else out
+            cell = ref = None
+        else:
+            res = None
+            cell, ref = out if out is not None else (
+                torch.empty(n, dtype=torch.int32, device=dev),
+                torch.empty((n, 3), dtype=torch.float32, device=dev))
+        L.check(L.lib().drb_locate_staged(C.byref(d), C.byref(bd), _ptr(staged), n,
+                                          C.byref(opts), cfg, _ptr(res), _ptr(cell), _ptr(ref),
+                                          L.DrbQueryStats(), _stream(stream)),
+                "drb_locate_staged")
+        return res if records else (cell, ref)
+
     def locate(self, points, order=None, guess=None, stats=False, out=None, stream=None):
         pts = _dev(points, torch.float32, self.mesh.device).reshape(-1, 3)
         n = pts.shape[0]

@@ -396,6 +396,13 @@ class Camera
   Vec3f get_look_at () const { return m_look_at; }
   Vec3f get_up () const { return m_up; }
   void create_rays (Array<Ray> &rays);
+  // the bounds are accepted and, as in the reference, not used
+  void create_rays (Array<Ray> &rays, AABB<> bounds);
+  // Camera::reset_to_bounds / elevate / azimuth (rendering/camera.cpp:485-555)
+  void reset_to_bounds (const AABB<> bounds, const float64 xpad = 0., const float64 ypad = 0.,
+                        const float64 zpad = 0.);
+  void elevate (const float32 degrees);
+  void azimuth (const float32 degrees);
 };
 
 class Framebuffer
@@ -414,6 +421,11 @@ class Framebuffer
   void background_color (const Vec4f &c) { m_bg_color = c; }
   Array<Vec<float32, 4>> colors () const { return m_colors; }
   Array<float32> depths () const { return m_depths; }
+  // Framebuffer::save / save_depth (rendering/framebuffer.cpp:45-105):
+  // <name>.png, 8-bit RGBA, first image row at the top (the framebuffer's
+  // last row); the depth image is the finite depths scaled to [0, 1] as grey
+  void save (const std::string name);
+  void save_depth (const std::string name);
 };
 
 // Default point light above the camera (detail::default_light,
@@ -427,8 +439,13 @@ class Volume
   int32 m_samples = 100;
   bool m_use_lighting = true;
   ColorMap m_color_map;
+  int32 m_active_domain = 0;
   public:
   explicit Volume (Collection &c);
+  // the domain integrate() works on (volume.hpp:36-38)
+  void active_domain (int32 domain_index);
+  int32 active_domain () const { return m_active_domain; }
+  int32 num_domains () const { return m_collection.local_size (); }
   void field (const std::string f) { m_field = f; }
   std::string field () const { return m_field; }
   void samples (int32 n) { m_samples = n; }
@@ -439,6 +456,9 @@ class Volume
   Array<VolumePartial> integrate (Array<Ray> &rays, Array<PointLight> &lights);
   // Volume::save without the PNG: partials composited over white
   static Framebuffer composite (Array<VolumePartial> partials, int32 width, int32 height);
+  // Volume::save (rendering/volume.cpp:369-416): composite, then <name>.png
+  static void save (const std::string name, Array<VolumePartial> partials, const int32 width,
+                    const int32 height);
 };
 
 class Traceable
@@ -447,9 +467,14 @@ class Traceable
   Collection m_collection;
   std::string m_field_name;
   ColorMap m_color_map;
+  int32 m_active_domain = 0;
   public:
   explicit Traceable (Collection &c) : m_collection (c) {}
   virtual ~Traceable () {}
+  // the domain nearest_hit/fragments/shade work on (traceable.hpp:63-65)
+  void active_domain (int32 domain_index);
+  int32 active_domain () const { return m_active_domain; }
+  int32 num_domains () const { return m_collection.local_size (); }
   void field (const std::string &f) { m_field_name = f; }
   std::string field () const { return m_field_name; }
   ColorMap &color_map () { return m_color_map; }
@@ -467,9 +492,23 @@ class Traceable
 
 class Surface : public Traceable
 {
+  bool m_draw_mesh = false;
+  float32 m_line_thickness = 0.05f;
+  float32 m_sub_res = 1.f;
+  Vec4f m_line_color = { { 0.f, 0.f, 0.f, 1.f } };
+  void draw_mesh (const Array<Ray> &rays, const Array<RayHit> &hits, Framebuffer &fb);
   public:
   explicit Surface (Collection &c) : Traceable (c) {}
   Array<RayHit> nearest_hit (Array<Ray> &rays) override;
+  // mesh lines over the shaded faces (rendering/surface.cpp:507-627)
+  void draw_mesh (bool on) { m_draw_mesh = on; }
+  void line_thickness (const float32 thickness);
+  void line_color (const Vec4f &color) { m_line_color = color; }
+  void mesh_sub_res (float32 sub_res);
+  void shade (const Array<Ray> &rays, const Array<RayHit> &hits, const Array<Fragment> &fragments,
+              const Array<PointLight> &lights, Framebuffer &fb) override;
+  void shade (const Array<Ray> &rays, const Array<RayHit> &hits, const Array<Fragment> &fragments,
+              Framebuffer &fb) override;
 };
 
 class MeshBoundary
@@ -564,7 +603,14 @@ class Renderer
   std::shared_ptr<Volume> m_volume;
   std::vector<PointLight> m_lights;
   bool m_use_lighting = true;
+  bool m_color_bar = false;
   public:
+  // Colour bars, triad and world annotations draw text and are not on this
+  // path: asking for them raises DRayError (the reference draws colour bars
+  // by default; renderer.cpp:166-169).
+  void color_bar (bool on);
+  void triad (bool on);
+  void world_annotations (bool on);
   void add (std::shared_ptr<Traceable> t) { m_traceables.push_back (t); }
   void volume (std::shared_ptr<Volume> v) { m_volume = v; }
   void add_light (const PointLight &l) { m_lights.push_back (l); }

@@ -2,11 +2,14 @@
 // over the C-ABI of include/drb.h.  Every compute step is a libdrb call on
 // the legacy default stream; host synchronisation happens only where the
 // reference's API returns host-visible results.
-#include <limits>
 #include "dray/dray_b200.hpp"
+
+#include <zlib.h>
 
 #include <algorithm>
 #include <cstring>
+#include <fstream>
+#include <limits>
 
 #include "drb.h"
 
@@ -377,6 +380,42 @@ void Camera::create_rays (Array<Ray> &rays)
   drb_check (drb_camera_rays (&d, rays.get_device_ptr (), nullptr), "drb_camera_rays");
 }
 
+void Camera::create_rays (Array<Ray> &rays, AABB<> bounds)
+{
+  (void)bounds; // create_rays_imp ignores them (camera.cpp:219-242)
+  create_rays (rays);
+}
+
+void Camera::reset_to_bounds (const AABB<> bounds, const float64 xpad, const float64 ypad,
+                              const float64 zpad)
+{
+  drb_camera d = to_drb (*this);
+  float b6[6];
+  for (int k = 0; k < 3; ++k)
+  {
+    b6[2 * k] = bounds.m_ranges[k].min ();
+    b6[2 * k + 1] = bounds.m_ranges[k].max ();
+  }
+  drb_check (drb_camera_reset_to_bounds (&d, b6, xpad, ypad, zpad), "drb_camera_reset_to_bounds");
+  m_pos = make_vec3f (d.pos[0], d.pos[1], d.pos[2]);
+  m_look_at = make_vec3f (d.look_at[0], d.look_at[1], d.look_at[2]);
+  set_fov (d.fov_y);
+}
+
+void Camera::elevate (const float32 degrees)
+{
+  drb_camera d = to_drb (*this);
+  drb_check (drb_camera_elevate (&d, degrees), "drb_camera_elevate");
+  m_pos = make_vec3f (d.pos[0], d.pos[1], d.pos[2]);
+}
+
+void Camera::azimuth (const float32 degrees)
+{
+  drb_camera d = to_drb (*this);
+  drb_check (drb_camera_azimuth (&d, degrees), "drb_camera_azimuth");
+  m_pos = make_vec3f (d.pos[0], d.pos[1], d.pos[2]);
+}
+
 PointLight default_light (Camera &camera)
 {
   drb_camera d = to_drb (camera);
@@ -421,6 +460,98 @@ void Framebuffer::composite_background ()
              "drb_framebuffer_composite_background");
 }
 
+// PNG file of 8-bit RGBA rows (top row first): signature, IHDR, one zlib
+// IDAT of filter-0 scanlines, IEND, each chunk with its CRC-32.
+static void write_png (const std::string &path, const std::vector<unsigned char> &rgba, int w,
+                       int h)
+{
+  std::vector<unsigned char> raw ((size_t)h * (1 + 4 * (size_t)w));
+  for (int y = 0; y < h; ++y)
+  {
+    unsigned char *row = raw.data () + (size_t)y * (1 + 4 * (size_t)w);
+    row[0] = 0; // filter: none
+    std::memcpy (row + 1, rgba.data () + (size_t)y * 4 * w, 4 * (size_t)w);
+  }
+  uLongf zlen = compressBound ((uLong)raw.size ());
+  std::vector<unsigned char> z (zlen);
+  if (compress2 (z.data (), &zlen, raw.data (), (uLong)raw.size (), 6) != Z_OK)
+    DRAY_ERROR ("png: compression failed");
+  z.resize (zlen);
+  std::ofstream f (path, std::ios::binary);
+  if (!f) DRAY_ERROR ("png: cannot open '" << path << "'");
+  auto be32 = [&] (uint32_t v) {
+    const unsigned char b[4] = { (unsigned char)(v >> 24), (unsigned char)(v >> 16),
+                                 (unsigned char)(v >> 8), (unsigned char)v };
+    f.write ((const char *)b, 4);
+  };
+  auto chunk = [&] (const char *type, const unsigned char *data, size_t len) {
+    be32 ((uint32_t)len);
+    f.write (type, 4);
+    if (len) f.write ((const char *)data, len);
+    uLong c = crc32 (0L, (const Bytef *)type, 4);
+    if (len) c = crc32 (c, data, (uInt)len);
+    be32 ((uint32_t)c);
+  };
+  const unsigned char sig[8] = { 0x89, 'P', 'N', 'G', '\r', '\n', 0x1a, '\n' };
+  f.write ((const char *)sig, 8);
+  unsigned char ihdr[13] = { (unsigned char)(w >> 24), (unsigned char)(w >> 16),
+                             (unsigned char)(w >> 8),  (unsigned char)w,
+                             (unsigned char)(h >> 24), (unsigned char)(h >> 16),
+                             (unsigned char)(h >> 8),  (unsigned char)h,
+                             8, 6, 0, 0, 0 }; // 8-bit RGBA, deflate, no interlace
+  chunk ("IHDR", ihdr, 13);
+  chunk ("IDAT", z.data (), z.size ());
+  chunk ("IEND", nullptr, 0);
+  if (!f) DRAY_ERROR ("png: write failed for '" << path << "'");
+}
+
+// PNGEncoder::encode (utils/png_encoder.cpp:61-97): 255 * value truncated
+// to 8 bits, framebuffer rows flipped so its last row comes first.
+static std::vector<unsigned char> to_rgba8 (const float *rgba, int w, int h)
+{
+  std::vector<unsigned char> out ((size_t)4 * w * h);
+  for (int y = 0; y < h; ++y)
+    for (int x = 0; x < w; ++x)
+      for (int c = 0; c < 4; ++c)
+      {
+        float v = rgba[((size_t)y * w + x) * 4 + c] * 255.f;
+        v = v < 0.f ? 0.f : v > 255.f ? 255.f : v; // out-of-range colours saturate
+        out[((size_t)(h - y - 1) * w + x) * 4 + c] = (unsigned char)v;
+      }
+  return out;
+}
+
+void Framebuffer::save (const std::string name)
+{
+  write_png (name + ".png", to_rgba8 ((const float *)m_colors.get_host_ptr_const (), m_width,
+                                      m_height),
+             m_width, m_height);
+}
+
+void Framebuffer::save_depth (const std::string name)
+{
+  // finite depths scaled to [0, 1] as grey, infinite ones black, alpha 1
+  // (framebuffer.cpp:54-105)
+  const size_t n = (size_t)m_width * m_height;
+  const float *d = m_depths.get_host_ptr_const ();
+  float lo = std::numeric_limits<float>::infinity (), hi = -lo;
+  for (size_t i = 0; i < n; ++i)
+    if (d[i] != std::numeric_limits<float>::infinity ())
+    {
+      lo = std::min (lo, d[i]);
+      hi = std::max (hi, d[i]);
+    }
+  const float len = hi - lo;
+  std::vector<float> g (4 * n);
+  for (size_t i = 0; i < n; ++i)
+  {
+    const float v = d[i] != std::numeric_limits<float>::infinity () ? (d[i] - lo) / len : 0.f;
+    g[4 * i] = g[4 * i + 1] = g[4 * i + 2] = v;
+    g[4 * i + 3] = 1.f;
+  }
+  write_png (name + ".png", to_rgba8 (g.data (), m_width, m_height), m_width, m_height);
+}
+
 // ------------------------------------------------------------- volume --
 
 Volume::Volume (Collection &c) : m_collection (c)
@@ -445,10 +576,24 @@ static ElementField *as_tensor_field (Field *f)
   return t;
 }
 
+void Volume::active_domain (int32 domain_index)
+{
+  if (domain_index < 0 || domain_index >= num_domains ())
+    DRAY_ERROR ("Volume: domain " << domain_index << " of " << num_domains ());
+  m_active_domain = domain_index;
+}
+
+void Traceable::active_domain (int32 domain_index)
+{
+  if (domain_index < 0 || domain_index >= num_domains ())
+    DRAY_ERROR ("Traceable: domain " << domain_index << " of " << num_domains ());
+  m_active_domain = domain_index;
+}
+
 Array<VolumePartial> Volume::integrate (Array<Ray> &rays, Array<PointLight> &lights)
 {
   if (m_field == "") DRAY_ERROR ("Field never set");
-  DataSet ds = m_collection.domain (0);
+  DataSet ds = m_collection.domain (m_active_domain);
   ElementMesh *mesh = as_tensor_mesh (ds.mesh ());
   ElementField *field = as_tensor_field (ds.field (m_field));
   Range r = m_color_map.range_set () ? m_color_map.scalar_range () : m_collection.range (m_field);
@@ -497,6 +642,12 @@ Array<VolumePartial> Volume::integrate (Array<Ray> &rays, Array<PointLight> &lig
   return res;
 }
 
+void Volume::save (const std::string name, Array<VolumePartial> partials, const int32 w,
+                   const int32 h)
+{
+  composite (partials, w, h).save (name);
+}
+
 Framebuffer Volume::composite (Array<VolumePartial> partials, int32 w, int32 h)
 {
   Framebuffer fb (w, h);
@@ -512,7 +663,7 @@ Framebuffer Volume::composite (Array<VolumePartial> partials, int32 w, int32 h)
 
 Array<RayHit> Surface::nearest_hit (Array<Ray> &rays)
 {
-  DataSet ds = m_collection.domain (0);
+  DataSet ds = m_collection.domain (m_active_domain);
   ElementMesh *faces = as_tensor_mesh (ds.mesh ());
   if (faces->dims () != 2) DRAY_ERROR ("Surface needs a quad (boundary) mesh");
   Array<RayHit> hits;
@@ -528,7 +679,7 @@ Array<RayHit> Surface::nearest_hit (Array<Ray> &rays)
 void Traceable::shade_impl (const Array<Ray> *rays, const Array<RayHit> &hits,
                             const Array<PointLight> *lights, Framebuffer *fb, Array<Fragment> *frags)
 {
-  DataSet ds = m_collection.domain (0);
+  DataSet ds = m_collection.domain (m_active_domain);
   ElementMesh *faces = as_tensor_mesh (ds.mesh ());
   ElementField *field = as_tensor_field (ds.field (m_field_name));
   Range r = m_color_map.range_set () ? m_color_map.scalar_range () : m_collection.range (m_field_name);
@@ -575,6 +726,43 @@ void Traceable::shade (const Array<Ray> &rays, const Array<RayHit> &hits, const 
                        Framebuffer &fb)
 {
   shade_impl (&rays, hits, nullptr, &fb, nullptr);
+}
+
+void Surface::line_thickness (const float32 thickness)
+{
+  if (thickness <= 0.f) DRAY_ERROR ("Cannot have 0 thickness");
+  m_line_thickness = thickness;
+}
+
+void Surface::mesh_sub_res (float32 sub_res)
+{
+  if (sub_res < 1.f) DRAY_ERROR ("Sub resolution is a number greater than 1");
+  m_sub_res = sub_res;
+}
+
+void Surface::draw_mesh (const Array<Ray> &rays, const Array<RayHit> &hits, Framebuffer &fb)
+{
+  const float lc[4] = { m_line_color[0], m_line_color[1], m_line_color[2], m_line_color[3] };
+  Array<Vec<float32, 4>> c = fb.colors ();
+  drb_check (drb_surface_mesh_lines (rays.get_device_ptr_const (), hits.get_device_ptr_const (),
+                                     (int)hits.size (), lc, m_line_thickness, m_sub_res,
+                                     (float *)c.get_device_ptr (), nullptr),
+             "drb_surface_mesh_lines");
+}
+
+void Surface::shade (const Array<Ray> &rays, const Array<RayHit> &hits,
+                     const Array<Fragment> &fragments, const Array<PointLight> &lights,
+                     Framebuffer &fb)
+{
+  Traceable::shade (rays, hits, fragments, lights, fb);
+  if (m_draw_mesh) draw_mesh (rays, hits, fb);
+}
+
+void Surface::shade (const Array<Ray> &rays, const Array<RayHit> &hits,
+                     const Array<Fragment> &fragments, Framebuffer &fb)
+{
+  Traceable::shade (rays, hits, fragments, fb);
+  if (m_draw_mesh) draw_mesh (rays, hits, fb);
 }
 
 // ------------------------------------------------------------ filters --
@@ -816,11 +1004,27 @@ Lineout::Result Lineout::execute (Collection &collection)
   return res;
 }
 
+void Renderer::color_bar (bool on)
+{
+  if (on) DRAY_ERROR ("colour bars draw text, which is not on this path");
+  m_color_bar = on;
+}
+void Renderer::triad (bool on)
+{
+  if (on) DRAY_ERROR ("the triad annotation is not on this path");
+}
+void Renderer::world_annotations (bool on)
+{
+  if (on) DRAY_ERROR ("world annotations are not on this path");
+}
+
 Framebuffer Renderer::render (Camera &camera)
 {
-  // Renderer::render (rendering/renderer.cpp:229-363), single domain:
-  // surfaces shade and shorten the rays, then the volume composites in
-  // front of them (partials_to_framebuffer with blending)
+  // Renderer::render (rendering/renderer.cpp:229-363): every domain of
+  // every surface shades and shortens the rays to its hits (ray_max), so a
+  // later domain only wins where it is closer; then the volume's partials
+  // of all domains, ordered by pixel and depth, are blended per pixel and
+  // composited in front of the surfaces (partials_to_framebuffer).
   Array<Ray> rays;
   camera.create_rays (rays);
   Framebuffer fb (camera.get_width (), camera.get_height ());
@@ -829,21 +1033,53 @@ Framebuffer Renderer::render (Camera &camera)
   Array<PointLight> lights (lv.data (), lv.size ());
   for (auto &t : m_traceables)
   {
-    Array<RayHit> hits = t->nearest_hit (rays);
-    Array<Fragment> frags;
-    if (m_use_lighting) t->shade (rays, hits, frags, lights, fb);
-    else t->shade (rays, hits, frags, fb);
-    drb_check (drb_ray_max (rays.get_device_ptr (), hits.get_device_ptr_const (), (int)rays.size (),
-                            nullptr),
-               "drb_ray_max");
+    for (int32 d = 0; d < t->num_domains (); ++d)
+    {
+      t->active_domain (d);
+      Array<RayHit> hits = t->nearest_hit (rays);
+      Array<Fragment> frags;
+      if (m_use_lighting) t->shade (rays, hits, frags, lights, fb);
+      else t->shade (rays, hits, frags, fb);
+      drb_check (drb_ray_max (rays.get_device_ptr (), hits.get_device_ptr_const (),
+                              (int)rays.size (), nullptr),
+                 "drb_ray_max");
+    }
   }
   if (m_volume)
   {
-    Array<VolumePartial> parts = m_volume->integrate (rays, lights);
+    std::vector<Array<VolumePartial>> per_domain;
+    size_t total = 0;
+    for (int32 d = 0; d < m_volume->num_domains (); ++d)
+    {
+      m_volume->active_domain (d);
+      per_domain.push_back (m_volume->integrate (rays, lights));
+      total += per_domain.back ().size ();
+    }
+    Array<VolumePartial> parts;
+    if (per_domain.size () == 1)
+      parts = per_domain[0];
+    else
+    {
+      Array<VolumePartial> all;
+      all.resize (total);
+      size_t off = 0;
+      for (auto &p : per_domain)
+      {
+        if (p.size ())
+          cuda_check (cudaMemcpy (all.get_device_ptr () + off, p.get_device_ptr_const (),
+                                  sizeof (VolumePartial) * p.size (), cudaMemcpyDeviceToDevice),
+                      "copy partials");
+        off += p.size ();
+      }
+      parts.resize (total);
+      drb_check (drb_sort_partials (all.get_device_ptr_const (), (int)total,
+                                    parts.get_device_ptr (), nullptr),
+                 "drb_sort_partials");
+    }
     Array<Vec<float32, 4>> c = fb.colors ();
-    Array<float32> d = fb.depths ();
+    Array<float32> dep = fb.depths ();
     drb_check (drb_partials_to_framebuffer (parts.get_device_ptr_const (), (int)parts.size (),
-                                            (float *)c.get_device_ptr (), d.get_device_ptr (),
+                                            (float *)c.get_device_ptr (), dep.get_device_ptr (),
                                             m_traceables.empty () ? 0 : 1, nullptr),
                "drb_partials_to_framebuffer");
   }

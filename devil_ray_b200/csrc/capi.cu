@@ -52,18 +52,28 @@ void keep_pool_reserved ()
   done.fetch_or (bit);
 }
 
+// SM count of the current device, looked up once per device ordinal, so
+// persistent grids are sized for the device they launch on.
 int sm_count ()
 {
-  static int cached = 0;
-  if (cached == 0)
+  static std::atomic<int> cached[64] = {};
+  int dev = 0;
+  if (cudaGetDevice (&dev) != cudaSuccess) dev = 0;
+  if (dev < 0 || dev >= 64)
   {
-    int dev = 0;
-    cudaGetDevice (&dev);
     int v = 0;
     cudaDeviceGetAttribute (&v, cudaDevAttrMultiProcessorCount, dev);
-    cached = v > 0 ? v : 148;
+    return v > 0 ? v : 148;
   }
-  return cached;
+  int c = cached[dev].load (std::memory_order_relaxed);
+  if (c == 0)
+  {
+    int v = 0;
+    cudaDeviceGetAttribute (&v, cudaDevAttrMultiProcessorCount, dev);
+    c = v > 0 ? v : 148;
+    cached[dev].store (c, std::memory_order_relaxed);
+  }
+  return c;
 }
 
 } // namespace drb

@@ -25,6 +25,7 @@
 #include <cmath>
 #include <cstdio>
 #include <cstring>
+#include <cstdint>
 
 namespace drb
 {
@@ -84,6 +85,39 @@ __global__ void cell_scatter_kernel (const unsigned *__restrict__ cell_of, const
   order[__ldg (offset + cell_of[i]) + rank[i]] = i;
 }
 
+// Query records in processing order, (x, y, z, input index as int bits), so
+// the locate kernel reads its queries as consecutive 16-byte records.  They
+// are gathered through the order (random reads, coalesced writes): a scatter
+// of the records themselves would write 16 bytes at random into an array
+// larger than L2, a read-modify-write of a DRAM sector per query, whereas the
+// index scatter before it writes 4 bytes into an array that stays in L2.
+__global__ void stage_gather_kernel (const float *__restrict__ pts, const int *__restrict__ order,
+                                     int n, float4 *__restrict__ staged)
+{
+  const int k = blockIdx.x * blockDim.x + threadIdx.x;
+  if (k >= n) return;
+  const int i = __ldg (order + k);
+  const float x = __ldg (pts + 3 * (size_t)i), y = __ldg (pts + 3 * (size_t)i + 1),
+              z = __ldg (pts + 3 * (size_t)i + 2);
+  staged[k] = make_float4 (x, y, z, __int_as_float (i));
+}
+
+// Results back to input order: query i's record (cell as int bits, then the
+// reference point) sits at its processing position offset[cell] + rank.
+// Reads of cell_of, rank and the outputs' writes run in input order.
+__global__ void unstage_kernel (const unsigned *__restrict__ cell_of, const int *__restrict__ rank,
+                                const int *__restrict__ offset, const float4 *__restrict__ res, int n,
+                                int *__restrict__ cell, float *__restrict__ ref)
+{
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const float4 r = __ldg (res + __ldg (offset + cell_of[i]) + rank[i]);
+  cell[i] = __float_as_int (r.x);
+  ref[3 * (size_t)i] = r.y;
+  ref[3 * (size_t)i + 1] = r.z;
+  ref[3 * (size_t)i + 2] = r.w;
+}
+
 // The BVH bounds as the cell grid's origin and inverse extents.
 void order_frame (const drb_bvh *bvh, float (&lo)[3], float (&sc)[3])
 {
@@ -96,10 +130,12 @@ void order_frame (const drb_bvh *bvh, float (&lo)[3], float (&sc)[3])
   }
 }
 
-// order[0..n) over caller buffers: cell_of and rank hold n values, hist
-// kCells, scan_tmp scan_ws_ints(kCells) (enough for every batch size).
-int cell_order (const drb_bvh *bvh, const float *pts, int n, int *order, unsigned *cell_of,
-                int *rank, int *hist, int *scan_tmp, cudaStream_t s)
+// Cell of every query, its rank inside the cell, and the cells' start
+// offsets (exclusive scan of the counts, in hist): cell_of and rank hold n
+// values, hist kCells, scan_tmp scan_ws_ints(kCells) (enough for every
+// batch size).  Query i's processing position is hist[cell_of[i]] + rank[i].
+int cell_positions (const drb_bvh *bvh, const float *pts, int n, unsigned *cell_of, int *rank,
+                    int *hist, int *scan_tmp, cudaStream_t s)
 {
   float lo[3], sc[3];
   order_frame (bvh, lo, sc);
@@ -115,9 +151,35 @@ int cell_order (const drb_bvh *bvh, const float *pts, int n, int *order, unsigne
                                                       sc[2], bits, cell_of, rank, hist);
   int st = check_launch ("cell_count_kernel");
   if (st) return st;
-  if ((st = exclusive_scan_i32_ws (hist, hist, cells, nullptr, scan_tmp, s))) return st;
+  return exclusive_scan_i32_ws (hist, hist, cells, nullptr, scan_tmp, s);
+}
+
+// order[0..n) over caller buffers (as cell_positions).
+int cell_order (const drb_bvh *bvh, const float *pts, int n, int *order, unsigned *cell_of,
+                int *rank, int *hist, int *scan_tmp, cudaStream_t s)
+{
+  int st = cell_positions (bvh, pts, n, cell_of, rank, hist, scan_tmp, s);
+  if (st) return st;
   cell_scatter_kernel<<<div_up (n, 256), 256, 0, s>>> (cell_of, rank, hist, n, order);
   return check_launch ("cell_scatter_kernel");
+}
+
+// The queries staged in processing order (buffers as cell_order's, plus
+// the order itself).
+int cell_stage (const drb_bvh *bvh, const float *pts, int n, float4 *staged, int *order,
+                unsigned *cell_of, int *rank, int *hist, int *scan_tmp, cudaStream_t s)
+{
+  int st = cell_order (bvh, pts, n, order, cell_of, rank, hist, scan_tmp, s);
+  if (st) return st;
+  stage_gather_kernel<<<div_up (n, 256), 256, 0, s>>> (pts, order, n, staged);
+  return check_launch ("stage_gather_kernel");
+}
+
+int unstage (const unsigned *cell_of, const int *rank, const int *hist, const float4 *res, int n,
+             int *cell, float *ref, cudaStream_t s)
+{
+  unstage_kernel<<<div_up (n, 256), 256, 0, s>>> (cell_of, rank, hist, res, n, cell, ref);
+  return check_launch ("unstage_kernel");
 }
 
 // Element-row modes of the candidate solves (drb_locate_config.reg_elements)
@@ -139,12 +201,20 @@ template <int P> constexpr size_t smem_rows_bytes_per_warp ()
   return sizeof (float) * 32 * (size_t)smem_row_stride<P> ();
 }
 
+// Staged queries (staged != NULL): the queries are read from staged[pos],
+// already in processing order with the input index in w, so a warp reads
+// its queries as one contiguous block (`order` and `pts` are unused).  With
+// res == NULL the results go to cell/ref at the input index (scattered
+// writes, which the kernel's latency-bound loop absorbs); with res set they
+// go to res[pos] as (cell as int bits, reference point), contiguous, for a
+// separate pass to put back.  Statistics always go to the input index.
 template <int P, int MODE, bool WIDE, int S = kTensor>
 __global__ void locate_persistent_kernel (LocateParams lp, const float *__restrict__ pts,
                                           const int *__restrict__ order, int n, int chunk,
                                           int *__restrict__ queue_head, int *__restrict__ cell,
                                           float *__restrict__ ref, int *__restrict__ it_out,
-                                          int *__restrict__ ca_out, int *__restrict__ nd_out)
+                                          int *__restrict__ ca_out, int *__restrict__ nd_out,
+                                          const float4 *__restrict__ staged, float4 *__restrict__ res)
 {
   const unsigned FULL = 0xffffffffu;
   const int lane = threadIdx.x & 31;
@@ -194,10 +264,23 @@ __global__ void locate_persistent_kernel (LocateParams lp, const float *__restri
       if (qi < 0 && rank < avail)
       {
         const int pos = pool_next + rank;
-        qi = order ? __ldg (order + pos) : pos;
-        pt[0] = __ldg (pts + 3 * (size_t)qi);
-        pt[1] = __ldg (pts + 3 * (size_t)qi + 1);
-        pt[2] = __ldg (pts + 3 * (size_t)qi + 2);
+        if (staged)
+        {
+          // qi: the processing position when the results are staged (the
+          // guess mode is then never DRB_GUESS_GIVEN), else the input index
+          const float4 v = __ldg (staged + pos);
+          qi = res ? pos : __float_as_int (v.w);
+          pt[0] = v.x;
+          pt[1] = v.y;
+          pt[2] = v.z;
+        }
+        else
+        {
+          qi = order ? __ldg (order + pos) : pos;
+          pt[0] = __ldg (pts + 3 * (size_t)qi);
+          pt[1] = __ldg (pts + 3 * (size_t)qi + 1);
+          pt[2] = __ldg (pts + 3 * (size_t)qi + 2);
+        }
         sp = 0;
         todo[0] = kBarrier;
         cur = 0;
@@ -289,14 +372,23 @@ __global__ void locate_persistent_kernel (LocateParams lp, const float *__restri
       }
       if (done)
       {
-        cell[qi] = found_el;
         if (found_el < 0) x[0] = x[1] = x[2] = -1.f;
-        ref[3 * (size_t)qi] = x[0];
-        ref[3 * (size_t)qi + 1] = x[1];
-        ref[3 * (size_t)qi + 2] = x[2];
-        if (it_out) it_out[qi] = iters;
-        if (ca_out) ca_out[qi] = cands;
-        if (nd_out) nd_out[qi] = nodes;
+        int q = qi;
+        if (res)
+        {
+          res[qi] = make_float4 (__int_as_float (found_el), x[0], x[1], x[2]);
+          if (it_out || ca_out || nd_out) q = __float_as_int (__ldg (&staged[qi].w));
+        }
+        else
+        {
+          cell[qi] = found_el;
+          ref[3 * (size_t)qi] = x[0];
+          ref[3 * (size_t)qi + 1] = x[1];
+          ref[3 * (size_t)qi + 2] = x[2];
+        }
+        if (it_out) it_out[q] = iters;
+        if (ca_out) ca_out[q] = cands;
+        if (nd_out) nd_out[q] = nodes;
         qi = -1;
       }
     }
@@ -344,12 +436,19 @@ size_t dynamic_smem (int order, int mode, int block)
   return per_warp * (size_t)(block / 32);
 }
 
+// Query records of a staged launch (both NULL: unstaged).
+struct Staging
+{
+  const float4 *staged = nullptr;
+  float4 *res = nullptr;
+};
+
 template <int P, bool W, int S>
 void launch_pw (int mode, dim3 grid, int block, size_t smem, cudaStream_t s, const LocateParams &lp,
                 const float *pts, const int *ord, int n, int chunk, int *head, int *cell, float *ref,
-                drb_query_stats st)
+                drb_query_stats st, Staging sg)
 {
-#define DRB_LP(M, SS) locate_persistent_kernel<P, M, W, SS><<<grid, block, smem, s>>> (lp, pts, ord, n, chunk, head, cell, ref, st.iters, st.candidates, st.nodes)
+#define DRB_LP(M, SS) locate_persistent_kernel<P, M, W, SS><<<grid, block, smem, s>>> (lp, pts, ord, n, chunk, head, cell, ref, st.iters, st.candidates, st.nodes, sg.staged, sg.res)
   if (S == kTensor && mode == kRowsShared) DRB_LP (kRowsShared, kTensor);
   else if (mode == kRowsReg && P <= 2) DRB_LP (P <= 2 ? kRowsReg : kRowsL1, S);
   else DRB_LP (kRowsL1, S);
@@ -359,16 +458,16 @@ void launch_pw (int mode, dim3 grid, int block, size_t smem, cudaStream_t s, con
 template <int S>
 void launch_s (int order, bool wide, int mode, dim3 grid, int block, size_t smem, cudaStream_t s,
                const LocateParams &lp, const float *pts, const int *ord, int n, int chunk, int *head,
-               int *cell, float *ref, drb_query_stats st)
+               int *cell, float *ref, drb_query_stats st, Staging sg)
 {
-  if (order == 1) { if (wide) launch_pw<1, true, S> (mode, grid, block, smem, s, lp, pts, ord, n, chunk, head, cell, ref, st); else launch_pw<1, false, S> (mode, grid, block, smem, s, lp, pts, ord, n, chunk, head, cell, ref, st); }
-  else if (order == 2) { if (wide) launch_pw<2, true, S> (mode, grid, block, smem, s, lp, pts, ord, n, chunk, head, cell, ref, st); else launch_pw<2, false, S> (mode, grid, block, smem, s, lp, pts, ord, n, chunk, head, cell, ref, st); }
-  else { if (wide) launch_pw<3, true, S> (mode, grid, block, smem, s, lp, pts, ord, n, chunk, head, cell, ref, st); else launch_pw<3, false, S> (mode, grid, block, smem, s, lp, pts, ord, n, chunk, head, cell, ref, st); }
+  if (order == 1) { if (wide) launch_pw<1, true, S> (mode, grid, block, smem, s, lp, pts, ord, n, chunk, head, cell, ref, st, sg); else launch_pw<1, false, S> (mode, grid, block, smem, s, lp, pts, ord, n, chunk, head, cell, ref, st, sg); }
+  else if (order == 2) { if (wide) launch_pw<2, true, S> (mode, grid, block, smem, s, lp, pts, ord, n, chunk, head, cell, ref, st, sg); else launch_pw<2, false, S> (mode, grid, block, smem, s, lp, pts, ord, n, chunk, head, cell, ref, st, sg); }
+  else { if (wide) launch_pw<3, true, S> (mode, grid, block, smem, s, lp, pts, ord, n, chunk, head, cell, ref, st, sg); else launch_pw<3, false, S> (mode, grid, block, smem, s, lp, pts, ord, n, chunk, head, cell, ref, st, sg); }
 }
 
 int launch_persistent (const drb_mesh *mesh, int mode, dim3 grid, int block, cudaStream_t s,
                        const LocateParams &lp, const float *pts, const int *ord, int n, int chunk,
-                       int *head, int *cell, float *ref, drb_query_stats st)
+                       int *head, int *cell, float *ref, drb_query_stats st, Staging sg = Staging ())
 {
   const int order = mesh->order;
   const size_t smem = dynamic_smem (order, mode, block);
@@ -377,13 +476,13 @@ int launch_persistent (const drb_mesh *mesh, int mode, dim3 grid, int block, cud
     cudaFuncSetAttribute (persistent_fn (mesh, mode, wide), cudaFuncAttributeMaxDynamicSharedMemorySize,
                           (int)smem);
   if (mesh->shape == DRB_SHAPE_SIMPLEX && mesh->dim == 2)
-    launch_s<kTri2D> (order, wide, mode, grid, block, smem, s, lp, pts, ord, n, chunk, head, cell, ref, st);
+    launch_s<kTri2D> (order, wide, mode, grid, block, smem, s, lp, pts, ord, n, chunk, head, cell, ref, st, sg);
   else if (mesh->shape == DRB_SHAPE_SIMPLEX)
-    launch_s<kSimplex> (order, wide, mode, grid, block, smem, s, lp, pts, ord, n, chunk, head, cell, ref, st);
+    launch_s<kSimplex> (order, wide, mode, grid, block, smem, s, lp, pts, ord, n, chunk, head, cell, ref, st, sg);
   else if (mesh->dim == 2)
-    launch_s<kQuad2D> (order, wide, mode, grid, block, smem, s, lp, pts, ord, n, chunk, head, cell, ref, st);
+    launch_s<kQuad2D> (order, wide, mode, grid, block, smem, s, lp, pts, ord, n, chunk, head, cell, ref, st, sg);
   else
-    launch_s<kTensor> (order, wide, mode, grid, block, smem, s, lp, pts, ord, n, chunk, head, cell, ref, st);
+    launch_s<kTensor> (order, wide, mode, grid, block, smem, s, lp, pts, ord, n, chunk, head, cell, ref, st, sg);
   return check_launch ("locate_persistent_kernel");
 }
 
@@ -475,6 +574,71 @@ int query_morton_order (const drb_bvh *bvh, const float *pts, int n, int *order,
   return cell_order (bvh, pts, n, order, cell_of, rank, hist, tmp, s);
 }
 
+int check_config (const drb_locate_config &cfg)
+{
+  if (cfg.block < 32 || cfg.block > 1024 || (cfg.block % 32) || cfg.chunk < 1)
+  {
+    set_last_error ("locate_batched: block must be a multiple of 32 in [32,1024], chunk >= 1");
+    return DRB_ERR_INVALID_ARG;
+  }
+  return DRB_OK;
+}
+
+// Persistent grid of a launch: the resident blocks of the configured shape
+// on every SM (or cfg.blocks_per_sm of them), no more than the queries fill.
+int persistent_blocks (const drb_mesh *mesh, const drb_bvh *bvh, const drb_locate_config &cfg,
+                       int mode, int n)
+{
+  const int per_sm = resident_blocks (mesh, mode, bvh->wide_nodes != nullptr, cfg.block);
+  const int bps = (cfg.blocks_per_sm > 0) ? min (cfg.blocks_per_sm, per_sm) : per_sm;
+  const long long warps_needed = ((long long)n + 31) / 32;
+  long long blocks = (long long)bps * sm_count ();
+  const long long blocks_needed = (warps_needed * 32 + cfg.block - 1) / cfg.block;
+  if (blocks > blocks_needed) blocks = blocks_needed;
+  if (blocks < 1) blocks = 1;
+  return (int)blocks;
+}
+
+// The persistent kernel over staged query records (head: the queue counter,
+// cleared here on the stream): results to res in the staged order, or with
+// res NULL to cell/ref at the input index.
+int locate_staged_launch (const drb_mesh *mesh, const drb_bvh *bvh, const float4 *staged, int n,
+                          const drb_newton_opts *opts, const drb_locate_config &cfg, int *head,
+                          float4 *res, int *cell, float *ref, drb_query_stats stats,
+                          cudaStream_t s)
+{
+  cudaError_t e = cudaMemsetAsync (head, 0, sizeof (int), s);
+  if (e != cudaSuccess) return status_from (e);
+  const int mode = effective_mode (mesh, cfg.reg_elements);
+  const int blocks = persistent_blocks (mesh, bvh, cfg, mode, n);
+  const LocateParams lp = make_params (mesh, bvh, opts);
+  Staging sg;
+  sg.staged = staged;
+  sg.res = res;
+  return launch_persistent (mesh, mode, dim3 ((unsigned)blocks), cfg.block, s, lp, nullptr,
+                            nullptr, n, cfg.chunk, head, cell, ref, stats, sg);
+}
+
+// Sorted, staged batch over caller buffers: stage the queries in Morton-cell
+// order and locate them; with res set (sort_queries == 2) the results are
+// staged too and put back in input order by a separate pass.
+int locate_staged_batch (const drb_mesh *mesh, const drb_bvh *bvh, const float *pts, int n,
+                         const drb_newton_opts *opts, const drb_locate_config &cfg, int *order,
+                         unsigned *cell_of, int *rank, int *hist, int *scan_tmp, int *head,
+                         float4 *staged, float4 *res, int *cell, float *ref, drb_query_stats stats,
+                         cudaStream_t s)
+{
+  int st = cell_stage (bvh, pts, n, staged, order, cell_of, rank, hist, scan_tmp, s);
+  if (st) return st;
+  st = locate_staged_launch (mesh, bvh, staged, n, opts, cfg, head, res, cell, ref, stats, s);
+  if (st || !res) return st;
+  return unstage (cell_of, rank, hist, res, n, cell, ref, s);
+}
+
+// Result staging of a query order mode (drb_locate_config.sort_queries).
+constexpr int kSortStaged = 1;        // query records staged, results in place
+constexpr int kSortStagedResults = 2; // results staged too, put back in a pass
+
 int locate_batched_impl (const drb_mesh *mesh, const drb_bvh *bvh, const float *pts, int n,
                          const drb_newton_opts *opts, const drb_locate_config *cfg_in,
                          const int *order_in, int *cell, float *ref, drb_query_stats stats,
@@ -483,14 +647,28 @@ int locate_batched_impl (const drb_mesh *mesh, const drb_bvh *bvh, const float *
   int st = check_args (mesh, bvh, pts, n, opts, cell, ref);
   if (st) return st;
   if (n == 0) return DRB_OK;
-  drb_locate_config cfg = cfg_in ? *cfg_in : default_config (mesh->order);
-  if (cfg.block < 32 || cfg.block > 1024 || (cfg.block % 32) || cfg.chunk < 1)
-  {
-    set_last_error ("locate_batched: block must be a multiple of 32 in [32,1024], chunk >= 1");
-    return DRB_ERR_INVALID_ARG;
-  }
+  const drb_locate_config cfg = cfg_in ? *cfg_in : default_config (mesh->order);
+  if ((st = check_config (cfg))) return st;
   Scratch scr (s);
   int *head = scr.alloc<int> (1);
+  if (!order_in && cfg.sort_queries)
+  {
+    // staged: query records read in processing order; results written in
+    // place, or staged as well when asked for (not with given guesses,
+    // which are indexed by the input order)
+    const bool stage_res = cfg.sort_queries == kSortStagedResults &&
+                           opts->guess_mode != DRB_GUESS_GIVEN;
+    int *ord = scr.alloc<int> (n);
+    unsigned *cell_of = scr.alloc<unsigned> (n);
+    int *rank = scr.alloc<int> (n);
+    int *hist = scr.alloc<int> (kCells);
+    int *tmp = scr.alloc<int> (scan_ws_ints (kCells));
+    float4 *staged = scr.alloc<float4> (n);
+    float4 *res = stage_res ? scr.alloc<float4> (n) : nullptr;
+    if (scr.err != cudaSuccess) return status_from (scr.err);
+    return locate_staged_batch (mesh, bvh, pts, n, opts, cfg, ord, cell_of, rank, hist, tmp,
+                                head, staged, res, cell, ref, stats, s);
+  }
   const int *ord = order_in;
   if (!ord && cfg.sort_queries)
   {
@@ -503,20 +681,16 @@ int locate_batched_impl (const drb_mesh *mesh, const drb_bvh *bvh, const float *
   if (scr.err != cudaSuccess) return status_from (scr.err);
   cudaMemsetAsync (head, 0, sizeof (int), s);
   const int mode = effective_mode (mesh, cfg.reg_elements);
-  const int per_sm = resident_blocks (mesh, mode, bvh->wide_nodes != nullptr, cfg.block);
-  const int bps = (cfg.blocks_per_sm > 0) ? min (cfg.blocks_per_sm, per_sm) : per_sm;
-  const long long warps_needed = ((long long)n + 31) / 32;
-  long long blocks = (long long)bps * sm_count ();
-  const long long blocks_needed = (warps_needed * 32 + cfg.block - 1) / cfg.block;
-  if (blocks > blocks_needed) blocks = blocks_needed;
-  if (blocks < 1) blocks = 1;
+  const int blocks = persistent_blocks (mesh, bvh, cfg, mode, n);
   const LocateParams lp = make_params (mesh, bvh, opts);
   return launch_persistent (mesh, mode, dim3 ((unsigned)blocks), cfg.block, s, lp, pts, ord, n,
                             cfg.chunk, head, cell, ref, stats);
 }
 
 // Same as locate_batched_impl with sorting, but over caller-provided
-// workspace (used by the allocation-free entry point).
+// workspace.  With ws.staged set the queries are staged like
+// locate_batched_impl's (the results too when sort_queries asks for it and
+// ws.res is set); otherwise the kernel reads them through ws.order.
 int locate_batched_ws (const drb_mesh *mesh, const drb_bvh *bvh, const float *pts, int n,
                        const drb_newton_opts *opts, const drb_locate_config *cfg_in,
                        const LocateWorkspace &ws, int *cell, float *ref, drb_query_stats stats,
@@ -525,11 +699,17 @@ int locate_batched_ws (const drb_mesh *mesh, const drb_bvh *bvh, const float *pt
   int st = check_args (mesh, bvh, pts, n, opts, cell, ref);
   if (st) return st;
   if (n == 0) return DRB_OK;
-  drb_locate_config cfg = cfg_in ? *cfg_in : default_config (mesh->order);
-  if (cfg.block < 32 || cfg.block > 1024 || (cfg.block % 32) || cfg.chunk < 1)
+  const drb_locate_config cfg = cfg_in ? *cfg_in : default_config (mesh->order);
+  if ((st = check_config (cfg))) return st;
+  if (cfg.sort_queries && ws.staged)
   {
-    set_last_error ("locate_batched: block must be a multiple of 32 in [32,1024], chunk >= 1");
-    return DRB_ERR_INVALID_ARG;
+    const bool stage_res = cfg.sort_queries == kSortStagedResults && ws.res &&
+                           opts->guess_mode != DRB_GUESS_GIVEN;
+    return locate_staged_batch (mesh, bvh, pts, n, opts, cfg, ws.order, ws.codes, ws.iota,
+                                ws.hist, ws.radix.scan_tmp, ws.head,
+                                reinterpret_cast<float4 *> (ws.staged),
+                                stage_res ? reinterpret_cast<float4 *> (ws.res) : nullptr, cell,
+                                ref, stats, s);
   }
   const int *ord = nullptr;
   if (cfg.sort_queries)
@@ -541,13 +721,7 @@ int locate_batched_ws (const drb_mesh *mesh, const drb_bvh *bvh, const float *pt
   cudaError_t e = cudaMemsetAsync (ws.head, 0, sizeof (int), s);
   if (e != cudaSuccess) return status_from (e);
   const int mode = effective_mode (mesh, cfg.reg_elements);
-  const int per_sm = resident_blocks (mesh, mode, bvh->wide_nodes != nullptr, cfg.block);
-  const int bps = (cfg.blocks_per_sm > 0) ? min (cfg.blocks_per_sm, per_sm) : per_sm;
-  const long long warps_needed = ((long long)n + 31) / 32;
-  long long blocks = (long long)bps * sm_count ();
-  const long long blocks_needed = (warps_needed * 32 + cfg.block - 1) / cfg.block;
-  if (blocks > blocks_needed) blocks = blocks_needed;
-  if (blocks < 1) blocks = 1;
+  const int blocks = persistent_blocks (mesh, bvh, cfg, mode, n);
   const LocateParams lp = make_params (mesh, bvh, opts);
   return launch_persistent (mesh, mode, dim3 ((unsigned)blocks), cfg.block, s, lp, pts, ord, n,
                             cfg.chunk, ws.head, cell, ref, stats);
@@ -592,6 +766,63 @@ extern "C" int drb_locate_ordered (const drb_mesh *mesh, const drb_bvh *bvh, con
                               (cudaStream_t)stream);
 }
 
+extern "C" int drb_query_stage (const drb_bvh *bvh, const float *pts, int n, float *staged,
+                                void *stream)
+{
+  if (!bvh || n < 0 || (n > 0 && (!pts || !staged)))
+  {
+    set_last_error ("query_stage: bad arguments");
+    return DRB_ERR_INVALID_ARG;
+  }
+  if (n == 0) return DRB_OK;
+  if (reinterpret_cast<uintptr_t> (staged) % 16)
+  {
+    set_last_error ("query_stage: staged must be 16-byte aligned");
+    return DRB_ERR_INVALID_ARG;
+  }
+  cudaStream_t s = (cudaStream_t)stream;
+  Scratch scr (s);
+  int *ord = scr.alloc<int> (n);
+  unsigned *cell_of = scr.alloc<unsigned> (n);
+  int *rank = scr.alloc<int> (n);
+  int *hist = scr.alloc<int> (kCells);
+  int *tmp = scr.alloc<int> (scan_ws_ints (kCells));
+  if (scr.err != cudaSuccess) return status_from (scr.err);
+  return cell_stage (bvh, pts, n, reinterpret_cast<float4 *> (staged), ord, cell_of, rank, hist,
+                     tmp, s);
+}
+
+extern "C" int drb_locate_staged (const drb_mesh *mesh, const drb_bvh *bvh, const float *staged,
+                                  int n, const drb_newton_opts *opts, const drb_locate_config *cfg_in,
+                                  float *res, int *cell, float *ref, drb_query_stats stats,
+                                  void *stream)
+{
+  const bool to_res = res != nullptr;
+  int st = check_args (mesh, bvh, staged, n, opts, to_res ? (const int *)res : cell,
+                       to_res ? res : ref);
+  if (st) return st;
+  if (to_res && opts->guess_mode == DRB_GUESS_GIVEN)
+  {
+    set_last_error ("locate_staged: DRB_GUESS_GIVEN needs the results at the input index "
+                    "(res NULL)");
+    return DRB_ERR_INVALID_ARG;
+  }
+  if ((reinterpret_cast<uintptr_t> (staged) | reinterpret_cast<uintptr_t> (res)) % 16)
+  {
+    set_last_error ("locate_staged: staged and res must be 16-byte aligned");
+    return DRB_ERR_INVALID_ARG;
+  }
+  if (n == 0) return DRB_OK;
+  const drb_locate_config cfg = cfg_in ? *cfg_in : default_config (mesh->order);
+  if ((st = check_config (cfg))) return st;
+  cudaStream_t s = (cudaStream_t)stream;
+  Scratch scr (s);
+  int *head = scr.alloc<int> (1);
+  if (scr.err != cudaSuccess) return status_from (scr.err);
+  return locate_staged_launch (mesh, bvh, reinterpret_cast<const float4 *> (staged), n, opts, cfg,
+                               head, reinterpret_cast<float4 *> (res), cell, ref, stats, s);
+}
+
 // Autotuner: times every (block, blocks/SM, chunk) candidate on the given
 // sample with CUDA events and returns the fastest.  The sample is located
 // in Morton order once; each candidate runs twice and the second run counts.
@@ -608,11 +839,19 @@ extern "C" int drb_locate_tune (const drb_mesh *mesh, const drb_bvh *bvh, const 
   }
   cudaStream_t s = (cudaStream_t)stream;
   Scratch scr (s);
-  int *ord = scr.alloc<int> (n);
+  // the kernel as drb_locate_batched runs it: on query records staged in
+  // Morton-cell order once, results written in place
   int *cell = scr.alloc<int> (n);
   float *ref = scr.alloc<float> ((size_t)3 * n);
+  float4 *srec = scr.alloc<float4> (n);
+  int *head = scr.alloc<int> (1);
+  int *ord = scr.alloc<int> (n);
+  unsigned *cell_of = scr.alloc<unsigned> (n);
+  int *rank = scr.alloc<int> (n);
+  int *hist = scr.alloc<int> (kCells);
+  int *tmp = scr.alloc<int> (scan_ws_ints (kCells));
   if (scr.err != cudaSuccess) return status_from (scr.err);
-  st = query_morton_order (bvh, pts, n, ord, s);
+  st = cell_stage (bvh, pts, n, srec, ord, cell_of, rank, hist, tmp, s);
   if (st) return st;
   const int blocks[] = { 64, 128, 256 };
   const int per_sm[] = { 0, 4, 2 };
@@ -639,8 +878,8 @@ extern "C" int drb_locate_tune (const drb_mesh *mesh, const drb_bvh *bvh, const 
         for (int rep = 0; rep < 2 && st == DRB_OK; ++rep)
         {
           cudaEventRecord (e0, s);
-          st = locate_batched_impl (mesh, bvh, pts, n, opts, &cfg, ord, cell, ref,
-                                    drb_query_stats{ nullptr, nullptr, nullptr }, s);
+          st = locate_staged_launch (mesh, bvh, srec, n, opts, cfg, head, nullptr, cell, ref,
+                                     drb_query_stats{ nullptr, nullptr, nullptr }, s);
           cudaEventRecord (e1, s);
           cudaEventSynchronize (e1);
           cudaEventElapsedTime (&t, e0, e1);

@@ -1,10 +1,9 @@
 // Allocation-free batched point location.
 //
 // Some callers of this library cannot allocate device memory at the time they
-// locate points: code running inside a CUDA stream capture that must not
-// record allocation nodes, hosts whose device memory is owned by another
-// allocator (a simulation code's pool, an in-situ framework) that forbids
-// side allocations, or real-time paths where cudaMalloc's implicit
+// locate points: hosts whose device memory is owned by another allocator (a
+// simulation code's pool, an in-situ framework) that forbids side
+// allocations, or real-time paths where cudaMalloc's implicit
 // synchronisation is not acceptable.  drb_locate_batched needs scratch
 // memory (query Morton codes, the sort's ping-pong buffers and histograms,
 // the work-queue counter) and obtains it with cudaMallocAsync.  This entry

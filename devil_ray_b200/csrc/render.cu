@@ -119,6 +119,65 @@ static int camera_setup (const drb_camera *cam, CamSetup &cs)
   return DRB_OK;
 }
 
+// Rotation of v about the unit-length-normalised axis by `degrees`
+// (Rodrigues' formula as the 4x4 matrix of transform_3d.hpp:126-157,
+// applied with a zero w: transform_3d.hpp:54-60).  Single precision in the
+// reference's operation order, so camera moves match it bit for bit.
+static void h_rotate (float degrees, const float *axis_in, float *v)
+{
+  const float pi_180 = 0.01745329251994329547437168059786927f;
+  const float rad = pi_180 * degrees;
+  float a[3] = { axis_in[0], axis_in[1], axis_in[2] };
+  h_normalize (a);
+  const float sn = sinf (rad);
+  const float cs = cosf (rad);
+  float m[3][4];
+  m[0][0] = a[0] * a[0] * (1 - cs) + cs;
+  m[0][1] = a[0] * a[1] * (1 - cs) - a[2] * sn;
+  m[0][2] = a[0] * a[2] * (1 - cs) + a[1] * sn;
+  m[1][0] = a[1] * a[0] * (1 - cs) + a[2] * sn;
+  m[1][1] = a[1] * a[1] * (1 - cs) + cs;
+  m[1][2] = a[1] * a[2] * (1 - cs) - a[0] * sn;
+  m[2][0] = a[2] * a[0] * (1 - cs) - a[1] * sn;
+  m[2][1] = a[2] * a[1] * (1 - cs) + a[0] * sn;
+  m[2][2] = a[2] * a[2] * (1 - cs) + cs;
+  m[0][3] = m[1][3] = m[2][3] = 0.f;
+  const float hv[4] = { v[0], v[1], v[2], 0.f };
+  for (int r = 0; r < 3; ++r)
+  {
+    float acc = 0.f;
+    for (int c = 0; c < 4; ++c) acc += m[r][c] * hv[c];
+    v[r] = acc;
+  }
+}
+
+// Camera::elevate / azimuth (rendering/camera.cpp:516-555): turn the view
+// direction about the camera's right (elevate, by -degrees) or up (azimuth)
+// axis and put the camera back at the same distance from look_at.
+static int camera_turn (drb_camera *cam, float degrees, bool about_right)
+{
+  if (!cam)
+  {
+    set_last_error ("camera: NULL camera");
+    return DRB_ERR_INVALID_ARG;
+  }
+  float up[3] = { cam->up[0], cam->up[1], cam->up[2] };
+  h_normalize (up); // the reference stores its up vector normalised
+  float look[3];
+  for (int i = 0; i < 3; ++i) look[i] = cam->look_at[i] - cam->pos[i];
+  const float distance = h_mag (look);
+  float right[3], vup[3];
+  h_cross (look, up, right);
+  h_cross (right, look, vup);
+  h_normalize (look);
+  h_normalize (right);
+  h_normalize (vup);
+  if (about_right) h_rotate (-degrees, right, look);
+  else h_rotate (degrees, vup, look);
+  for (int i = 0; i < 3; ++i) cam->pos[i] = cam->look_at[i] - look[i] * distance;
+  return DRB_OK;
+}
+
 __global__ void camera_rays_kernel (CamSetup cs, Ray *__restrict__ rays)
 {
   const long long idx = (long long)blockIdx.x * blockDim.x + threadIdx.x;
@@ -1261,4 +1320,195 @@ extern "C" int drb_partials_to_framebuffer (const void *partials, int n, float *
   partials_to_fb_kernel<<<div_up (n, 256), 256, 0, (cudaStream_t)stream>>> (
   (const VolumePartial *)partials, n, (float4 *)fb_rgba, fb_depth, blend_over);
   return check_launch ("partials_to_fb_kernel");
+}
+
+extern "C" int drb_camera_elevate (drb_camera *cam, float degrees)
+{
+  return drb::camera_turn (cam, degrees, true);
+}
+
+extern "C" int drb_camera_azimuth (drb_camera *cam, float degrees)
+{
+  return drb::camera_turn (cam, degrees, false);
+}
+
+// Camera::reset_to_bounds (rendering/camera.cpp:485-514): pad the bounds
+// by a fraction of each extent, look at their centre from the current
+// direction at one diagonal's distance, field of view 60 degrees.  The pads
+// are double and the padded bounds single precision, as in the reference.
+extern "C" int drb_camera_reset_to_bounds (drb_camera *cam, const float *bounds6, double xpad,
+                                           double ypad, double zpad)
+{
+  if (!cam || !bounds6)
+  {
+    set_last_error ("camera_reset_to_bounds: NULL camera or bounds");
+    return DRB_ERR_INVALID_ARG;
+  }
+  const double pads[3] = { xpad, ypad, zpad };
+  float lo[3], hi[3], center[3], extent[3];
+  for (int d = 0; d < 3; ++d)
+  {
+    const float bmin = bounds6[2 * d], bmax = bounds6[2 * d + 1];
+    if (!(bmin <= bmax))
+    {
+      set_last_error ("camera_reset_to_bounds: empty bounds");
+      return DRB_ERR_INVALID_ARG;
+    }
+    const double pad = pads[d] * (bmax - bmin);
+    const float a = (float)(bmax + pad), b = (float)(bmin - pad);
+    lo[d] = fminf (INFINITY, a);
+    hi[d] = fmaxf (-INFINITY, a);
+    lo[d] = fminf (lo[d], b);
+    hi[d] = fmaxf (hi[d], b);
+    center[d] = 0.5f * (lo[d] + hi[d]);
+    extent[d] = hi[d] - lo[d];
+  }
+  float dir[3];
+  for (int i = 0; i < 3; ++i) dir[i] = cam->pos[i] - cam->look_at[i];
+  drb::h_normalize (dir);
+  const float diagonal = drb::h_mag (extent);
+  for (int i = 0; i < 3; ++i)
+  {
+    cam->look_at[i] = center[i];
+    cam->pos[i] = center[i] + dir[i] * diagonal * 1.0f;
+  }
+  cam->fov_y = 60.0f;
+  return DRB_OK;
+}
+
+// ------------------------------------------------------------ mesh lines --
+
+namespace drb
+{
+namespace
+{
+
+// Surface::draw_mesh (rendering/surface.cpp:25-111, 522-550): a line colour
+// whose alpha falls off with the distance of the hit's reference point to
+// the nearest face edge (second-nearest of the three coordinates, cubic
+// smoothstep over `rcp`), blended over the pixel's colour.  The reference
+// rounds through double in its shader; the same steps are taken here with
+// explicitly rounded operations so no multiply-add is fused.
+__device__ float edge_term (float p)
+{
+  // 0.5 - |p - 0.5| in double, on the fractional part inside [0, 1]
+  const double d = p;
+  return (float)(d < 0.0 ? 0.0 : d > 1.0 ? 0.0 : __dsub_rn (0.5, fabs (__dsub_rn (d, 0.5))));
+}
+
+__global__ void mesh_lines_kernel (const Ray *__restrict__ rays, const RayHit *__restrict__ hits,
+                                   int n, float4 line, float rcp, int grid_res,
+                                   float4 *__restrict__ fb)
+{
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const RayHit h = hits[i];
+  if (h.hit_idx == -1) return;
+  float d[3];
+#pragma unroll
+  for (int k = 0; k < 3; ++k)
+  {
+    float p = __fmul_rn ((float)grid_res, h.ref[k]);
+    p = __fsub_rn (p, floorf (p));
+    d[k] = edge_term (p);
+  }
+  const float min2 = d[0] < d[1] ? d[0] : d[1];
+  const float max2 = d[0] < d[1] ? d[1] : d[0];
+  float edge = d[2] < min2 ? min2 : max2 < d[2] ? max2 : d[2];
+  edge = __fmul_rn (edge, rcp);
+  const double x = fminf (edge, 1.0f);
+  const float w = (float)__dadd_rn (__dmul_rn (__dmul_rn (__dsub_rn (__dmul_rn (2.0, x), 3.0), x), x), 1.0);
+  float4 f = make_float4 (line.x, line.y, line.z, __fmul_rn (line.w, w));
+  const int pix = rays[i].pixel_id;
+  const float4 b = fb[pix];
+  // blend (rendering/colors.hpp:15-23): front over back
+  const float a = __fmul_rn (b.w, __fsub_rn (1.f, f.w));
+  f.x = __fadd_rn (f.x, __fmul_rn (b.x, a));
+  f.y = __fadd_rn (f.y, __fmul_rn (b.y, a));
+  f.z = __fadd_rn (f.z, __fmul_rn (b.z, a));
+  f.w = __fadd_rn (a, f.w);
+  fb[pix] = f;
+}
+
+// Order-preserving unsigned key of a float (negative values flipped).
+__global__ void partial_depth_keys_kernel (const VolumePartial *__restrict__ p, int n,
+                                           unsigned *__restrict__ key, int *__restrict__ idx)
+{
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const unsigned b = __float_as_uint (p[i].depth);
+  key[i] = (b & 0x80000000u) ? ~b : (b | 0x80000000u);
+  idx[i] = i;
+}
+
+__global__ void partial_pixel_keys_kernel (const VolumePartial *__restrict__ p, const int *__restrict__ idx,
+                                           int n, unsigned *__restrict__ key)
+{
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  key[i] = (unsigned)p[idx[i]].pixel_id;
+}
+
+__global__ void partial_order_gather_kernel (const VolumePartial *__restrict__ p, const int *__restrict__ idx,
+                                       int n, VolumePartial *__restrict__ out)
+{
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  out[i] = p[idx[i]];
+}
+
+} // namespace
+} // namespace drb
+
+extern "C" int drb_surface_mesh_lines (const void *rays, const void *hits, int n,
+                                       const float *line_color4, float line_thickness,
+                                       float sub_res, float *fb_rgba, void *stream)
+{
+  if (n < 0 || (n > 0 && (!rays || !hits || !fb_rgba || !line_color4)))
+  {
+    set_last_error ("surface_mesh_lines: bad arguments");
+    return DRB_ERR_INVALID_ARG;
+  }
+  if (!(line_thickness > 0.f) || !(sub_res >= 1.f))
+  {
+    set_last_error ("surface_mesh_lines: thickness must be > 0 and sub resolution >= 1");
+    return DRB_ERR_INVALID_ARG;
+  }
+  if (n == 0) return DRB_OK;
+  // ShadeMeshLines::set_uniforms (surface.cpp:34-40): the reciprocal in
+  // double times the integer grid resolution, stored as float
+  const int grid_res = (int)sub_res;
+  const float rcp = (float)((line_thickness > 0.0 ? 1.0 / (double)line_thickness : 0.05) * grid_res);
+  const float4 line = make_float4 (line_color4[0], line_color4[1], line_color4[2], line_color4[3]);
+  drb::mesh_lines_kernel<<<div_up (n, 256), 256, 0, (cudaStream_t)stream>>> (
+  (const drb::Ray *)rays, (const drb::RayHit *)hits, n, line, rcp, grid_res, (float4 *)fb_rgba);
+  return check_launch ("mesh_lines_kernel");
+}
+
+extern "C" int drb_sort_partials (const void *partials, int n, void *sorted, void *stream)
+{
+  if (n < 0 || (n > 0 && (!partials || !sorted)) || partials == sorted)
+  {
+    set_last_error ("sort_partials: bad arguments (the output may not alias the input)");
+    return DRB_ERR_INVALID_ARG;
+  }
+  if (n == 0) return DRB_OK;
+  cudaStream_t s = (cudaStream_t)stream;
+  Scratch scr (s);
+  unsigned *k0 = scr.alloc<unsigned> (n);
+  unsigned *k1 = scr.alloc<unsigned> (n);
+  int *i0 = scr.alloc<int> (n);
+  int *i1 = scr.alloc<int> (n);
+  if (scr.err != cudaSuccess) return status_from (scr.err);
+  const VolumePartial *p = (const VolumePartial *)partials;
+  // stable by depth, then stable by pixel: (pixel, depth) order
+  drb::partial_depth_keys_kernel<<<div_up (n, 256), 256, 0, s>>> (p, n, k0, i0);
+  int st = check_launch ("partial_depth_keys_kernel");
+  if (st) return st;
+  if ((st = radix_sort_pairs (k0, i0, k1, i1, n, 32, s))) return st;
+  drb::partial_pixel_keys_kernel<<<div_up (n, 256), 256, 0, s>>> (p, i1, n, k0);
+  if ((st = check_launch ("partial_pixel_keys_kernel"))) return st;
+  if ((st = radix_sort_pairs (k0, i1, k1, i0, n, 32, s))) return st;
+  drb::partial_order_gather_kernel<<<div_up (n, 256), 256, 0, s>>> (p, i0, n, (VolumePartial *)sorted);
+  return check_launch ("partial_order_gather_kernel");
 }

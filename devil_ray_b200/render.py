@@ -38,7 +38,35 @@ class Camera:
         c.fov_y, c.zoom = self.fov, self.zoom
         return c
 
-    def create_rays(self, device="cuda", stream=None) -> torch.Tensor:
+    def _take(self, d: L.DrbCamera):
+        self.pos = tuple(float(d.pos[i]) for i in range(3))
+        self.look_at = tuple(float(d.look_at[i]) for i in range(3))
+        self.fov = float(d.fov_y)
+
+    def reset_to_bounds(self, bounds6, xpad=0.0, ypad=0.0, zpad=0.0):
+        """Camera::reset_to_bounds: bounds6 = (xmin, xmax, ymin, ymax, zmin,
+        zmax); look at their padded centre from the current direction, one
+        diagonal away, with a 60-degree field of view."""
+        d = self.desc()
+        b = np.ascontiguousarray(bounds6, np.float32)
+        L.check(L.lib().drb_camera_reset_to_bounds(C.byref(d), b.ctypes.data_as(C.c_void_p),
+                                                   xpad, ypad, zpad),
+                "drb_camera_reset_to_bounds")
+        self._take(d)
+
+    def elevate(self, degrees: float):
+        d = self.desc()
+        L.check(L.lib().drb_camera_elevate(C.byref(d), degrees), "drb_camera_elevate")
+        self._take(d)
+
+    def azimuth(self, degrees: float):
+        d = self.desc()
+        L.check(L.lib().drb_camera_azimuth(C.byref(d), degrees), "drb_camera_azimuth")
+        self._take(d)
+
+    def create_rays(self, device="cuda", stream=None, bounds=None) -> torch.Tensor:
+        """Camera::create_rays (rays, bounds): the bounds argument is
+        accepted and, as in the reference, not used."""
         n = self.width * self.height
         rays = torch.empty((n, RAY_WORDS), dtype=torch.float32, device=device)
         d = self.desc()

@@ -242,7 +242,14 @@ typedef struct drb_locate_config
   int block;             /* threads per block, multiple of 32 */
   int blocks_per_sm;     /* resident blocks per SM, 0 = as many as fit */
   int chunk;             /* queries a warp pops from the global queue at once */
-  int sort_queries;      /* 1 = process the queries in Morton-cell order */
+  int sort_queries;      /* 0 = process the queries in input order; 1 =
+                            in Morton-cell order, the query records staged
+                            in that order (one coalesced read per warp) and
+                            the results written at each query's input
+                            index; 2 = as 1 with the results also staged
+                            contiguously and put back in input order by a
+                            separate pass (not with DRB_GUESS_GIVEN, which
+                            then runs as 1) */
   int reg_elements;      /* where a candidate's control points are read from
                             during its Newton solve: 0 = through L1 on every
                             step; 1 = registers (orders <= 2; fewer loads,
@@ -262,9 +269,10 @@ int drb_locate_batched (const drb_mesh *mesh, const drb_bvh *bvh, const float *p
                         float *ref, drb_query_stats stats, void *stream);
 
 /* drb_locate_batched without any device allocation, for callers that cannot
- * allocate when they locate points (inside a stream capture that must not
- * record allocations, under a host application's own device-memory pool,
- * or where cudaMalloc's implicit synchronisation is not acceptable).  No
+ * allocate when they locate points: a host application whose device memory
+ * is owned by its own allocator or pool (a simulation code, an in-situ
+ * framework) that forbids side allocations, or a latency-critical path where
+ * cudaMalloc's implicit synchronisation is not acceptable.  No
  * counterpart in the reference.  All scratch lives in one fixed array of
  * about 20 MB inside the library's device code, which stays allocated on each
  * device where it is loaded until the process exits.  At most
@@ -293,6 +301,26 @@ int drb_locate_ordered (const drb_mesh *mesh, const drb_bvh *bvh, const float *p
                         const int *order, const drb_newton_opts *opts,
                         const drb_locate_config *cfg, int *cell, float *ref,
                         drb_query_stats stats, void *stream);
+
+/* Query records in processing order: staged[4 * k .. 4 * k + 3] = (x, y, z,
+ * input index as int32 bits) of the k-th query of the Morton-cell order
+ * (drb_query_order's order, with the same unspecified order inside a cell).
+ * staged: device float[4n], 16-byte aligned.  drb_locate_batched stages its
+ * queries this way internally, so the kernel reads and writes consecutive
+ * records.  No reference counterpart (it never reorders). */
+int drb_query_stage (const drb_bvh *bvh, const float *pts, int n, float *staged, void *stream);
+
+/* The persistent locate kernel of drb_locate_batched on staged records
+ * (drb_query_stage).  res non-NULL: res[4 * k .. 4 * k + 3] = (cell as int32
+ * bits, r, s, t) of staged query k, in the staged order (not for
+ * DRB_GUESS_GIVEN); res NULL: cell[i] and ref[3 * i ..] at each query's input
+ * index i, as drb_locate_batched writes them.  Statistics, when requested, go
+ * to the input index.  staged and res 16-byte aligned.  Replaces the forall
+ * body of UnstructuredMesh::locate (data_model/unstructured_mesh.cpp:137-148)
+ * for callers that keep their queries in processing order. */
+int drb_locate_staged (const drb_mesh *mesh, const drb_bvh *bvh, const float *staged, int n,
+                       const drb_newton_opts *opts, const drb_locate_config *cfg, float *res,
+                       int *cell, float *ref, drb_query_stats stats, void *stream);
 
 /* UnstructuredMesh::locate (unstructured_mesh.cpp:124-148) on points that
  * live in host memory: host_pts float[3n] in, host_cell int32[n] and
@@ -359,6 +387,35 @@ typedef struct drb_volume_opts
 /* Camera::create_rays / gen_perspective (rendering/camera.cpp:219-483):
  * width*height rays, pixel id j*width+i.  rays: device dray::Ray[w*h]. */
 int drb_camera_rays (const drb_camera *cam, void *rays, void *stream);
+
+/* Surface::draw_mesh (rendering/surface.cpp:25-111, 522-550): for every
+ * ray whose hit is valid, the mesh-line colour line_color4 with its alpha
+ * scaled by the smoothed distance of the hit's reference point to the
+ * nearest face edge (line_thickness in reference units, sub_res >= 1 lines
+ * per unit) is blended over fb_rgba at the ray's pixel.  rays/hits: device
+ * dray::Ray / dray::RayHit [n]. */
+int drb_surface_mesh_lines (const void *rays, const void *hits, int n, const float *line_color4,
+                            float line_thickness, float sub_res, float *fb_rgba, void *stream);
+
+/* Volume partials ordered by pixel id, then depth (stable): the single-rank
+ * order the reference's partial compositor works in before blending each
+ * pixel front to back (rendering/renderer.cpp:323-335).  Needed when the
+ * partials of several domains are concatenated.  sorted must not alias
+ * partials. */
+int drb_sort_partials (const void *partials, int n, void *sorted, void *stream);
+
+/* Camera::elevate and Camera::azimuth (rendering/camera.cpp:516-555): turn
+ * the view about the camera's right axis (by -degrees) or its up axis and
+ * keep the distance to look_at; updates cam->pos (host only). */
+int drb_camera_elevate (drb_camera *cam, float degrees);
+int drb_camera_azimuth (drb_camera *cam, float degrees);
+
+/* Camera::reset_to_bounds (rendering/camera.cpp:485-514): bounds6 = (xmin,
+ * xmax, ymin, ymax, zmin, zmax), padded by the given fractions of each
+ * extent; look_at becomes their centre, pos one diagonal away along the
+ * current view direction, fov_y 60 (host only). */
+int drb_camera_reset_to_bounds (drb_camera *cam, const float *bounds6, double xpad, double ypad,
+                                double zpad);
 
 /* detail::default_light (rendering/renderer.cpp:141-159) on the host:
  * light13 = pos[3], amb[3], diff[3], spec[3], spec_pow (PointLight defaults). */

@@ -37,6 +37,7 @@
 #include <dray/rendering/fragment.hpp>
 #include <dray/rendering/framebuffer.hpp>
 #include <dray/rendering/point_light.hpp>
+#include <dray/rendering/renderer.hpp>
 #include <dray/rendering/surface.hpp>
 #include <dray/rendering/volume.hpp>
 #include <dray/rendering/volume_partial.hpp>
@@ -462,6 +463,46 @@ int ref_locate (void *h, int n, const float *pts, int *cell, float *ref3)
 }
 
 // Camera::create_rays: rays as (dir3, near, orig3, far, pixel_id) = 9 words.
+// Camera moves through the reference's Camera: optional reset_to_bounds
+// (bounds6 = xmin,xmax,ymin,ymax,zmin,zmax; pads3 as doubles), then elevate
+// and azimuth; out9 = position, look_at, up, *out_fov = field of view.
+int ref_camera_move (int w, int h, const float *cam9, float fov, const float *bounds6,
+                     const double *pads3, float elevate_deg, float azimuth_deg, float *out9,
+                     float *out_fov)
+{
+  try
+  {
+    Camera cam;
+    setup_camera (cam, w, h, cam9, fov);
+    if (bounds6)
+    {
+      AABB<> b;
+      for (int d = 0; d < 3; ++d)
+      {
+        b.m_ranges[d].include (bounds6[2 * d]);
+        b.m_ranges[d].include (bounds6[2 * d + 1]);
+      }
+      cam.reset_to_bounds (b, pads3[0], pads3[1], pads3[2]);
+    }
+    if (elevate_deg != 0.f) cam.elevate (elevate_deg);
+    if (azimuth_deg != 0.f) cam.azimuth (azimuth_deg);
+    const Vec<float32, 3> p = cam.get_pos (), l = cam.get_look_at (), u = cam.get_up ();
+    for (int i = 0; i < 3; ++i)
+    {
+      out9[i] = p[i];
+      out9[3 + i] = l[i];
+      out9[6 + i] = u[i];
+    }
+    *out_fov = cam.get_fov ();
+    return 0;
+  }
+  catch (const std::exception &e)
+  {
+    g_err = e.what ();
+    return -1;
+  }
+}
+
 int ref_camera_rays (int w, int h, const float *cam9, float fov, float *rays9)
 {
   try
@@ -547,6 +588,187 @@ int ref_volume (void *h, int w, int hgt, const float *cam9, float fov, int sampl
       std::memcpy (rgba, (const void *)fb.colors ().get_host_ptr_const (), sizeof (float) * 4 * (size_t)w * hgt);
     }
     return size;
+  }
+  catch (const std::exception &e)
+  {
+    g_err = e.what ();
+    return -1;
+  }
+}
+
+} // extern "C" (reopened below)
+
+// Installs a BVH built elsewhere (the same record layout: inner nodes of
+// 16 floats, leaf element ids, leaf sub-box ids, bounds, and one SubRef
+// reference box of 6 floats per sub-box) into a hex mesh, in place of the
+// lazy UnstructuredMesh::get_bvh build.  The reference's own build cannot
+// run at the 128^3 order-3 size: its split scratch holds
+// num_els * 33 * (p+1)^3 control points, 53 GB there, indexed by int32
+// (data_model/mesh_utils.cpp:552-569).  The fields are protected; member
+// pointers taken through a derived type reach them.
+template <typename MeshT> struct BvhAccess : MeshT
+{
+  static void install (Mesh *m, const BVH &b, const float *ref6, int n_leaf)
+  {
+    MeshT *mesh = dynamic_cast<MeshT *> (m);
+    if (!mesh) throw std::runtime_error ("set_bvh: not this mesh type");
+    mesh->*(&BvhAccess::m_bvh) = b;
+    Array<SubRef<3, ElemType::Tensor>> &ra = mesh->*(&BvhAccess::m_ref_aabbs);
+    ra.resize (n_leaf);
+    std::memcpy ((void *)ra.get_host_ptr (), ref6, sizeof (float) * 6 * (size_t)n_leaf);
+    mesh->*(&BvhAccess::m_is_constructed) = true;
+  }
+};
+
+extern "C" {
+
+int ref_hex_set_bvh (void *h, int n_inner, const float *inner, int n_leaf, const int *leaf_nodes,
+                     const int *aabb_ids, const float *bounds6, const float *ref6)
+{
+  try
+  {
+    RefMesh *r = static_cast<RefMesh *> (h);
+    BVH b;
+    b.m_inner_nodes.resize ((size_t)4 * n_inner);
+    std::memcpy ((void *)b.m_inner_nodes.get_host_ptr (), inner, sizeof (float) * 16 * (size_t)n_inner);
+    b.m_leaf_nodes.resize (n_leaf);
+    std::memcpy (b.m_leaf_nodes.get_host_ptr (), leaf_nodes, sizeof (int) * (size_t)n_leaf);
+    b.m_aabb_ids.resize (n_leaf);
+    std::memcpy (b.m_aabb_ids.get_host_ptr (), aabb_ids, sizeof (int) * (size_t)n_leaf);
+    for (int d = 0; d < 3; ++d)
+    {
+      b.m_bounds.m_ranges[d].reset ();
+      b.m_bounds.m_ranges[d].include (bounds6[2 * d]);
+      b.m_bounds.m_ranges[d].include (bounds6[2 * d + 1]);
+    }
+    Mesh *m = r->mesh.get ();
+    if (dynamic_cast<HexMesh_P1 *> (m)) BvhAccess<HexMesh_P1>::install (m, b, ref6, n_leaf);
+    else if (dynamic_cast<HexMesh_P2 *> (m)) BvhAccess<HexMesh_P2>::install (m, b, ref6, n_leaf);
+    else BvhAccess<HexMesh>::install (m, b, ref6, n_leaf);
+    return 0;
+  }
+  catch (const std::exception &e)
+  {
+    g_err = e.what ();
+    return -1;
+  }
+}
+
+// Volume::integrate on given rays (the reference's 36-byte Ray records:
+// dir, near, orig, far, pixel id), e.g. a tile of a camera's rays; the
+// partials as (pixel, depth, r, g, b, a) records.  Returns their count.
+int ref_volume_rays (void *h, int n_rays, const float *rays9, int samples, int use_lighting,
+                     int tf_samples, int n_rgb, const float *rgb_pts, int n_alpha,
+                     const float *alpha_pts, int n_lights, const float *lights13,
+                     float *partials6, int max_partials)
+{
+  try
+  {
+    static_assert (sizeof (Ray) == 36, "Ray record");
+    RefMesh *r = static_cast<RefMesh *> (h);
+    Array<Ray> rays;
+    rays.resize (n_rays);
+    std::memcpy ((void *)rays.get_host_ptr (), rays9, sizeof (float) * 9 * (size_t)n_rays);
+    Volume vol (r->collection);
+    vol.field ("f");
+    vol.samples (samples);
+    vol.use_lighting (use_lighting != 0);
+    ColorMap &cmap = vol.color_map ();
+    cmap.samples (tf_samples);
+    cmap.color_table (make_table (n_rgb, rgb_pts, n_alpha, alpha_pts));
+    Array<PointLight> lights = make_lights (n_lights, lights13);
+    Array<VolumePartial> partials = vol.integrate (rays, lights);
+    const int size = partials.size ();
+    const VolumePartial *pp = partials.get_host_ptr_const ();
+    if (partials6)
+      for (int i = 0; i < size && i < max_partials; ++i)
+      {
+        partials6[6 * i] = (float)pp[i].m_pixel_id;
+        partials6[6 * i + 1] = pp[i].m_depth;
+        for (int c = 0; c < 4; ++c) partials6[6 * i + 2 + c] = pp[i].m_color[c];
+      }
+    return size;
+  }
+  catch (const std::exception &e)
+  {
+    g_err = e.what ();
+    return -1;
+  }
+}
+
+// Renderer::render (rendering/renderer.cpp:229-363) over a collection of
+// n_dom hex-mesh domains (arrays concatenated: orders, n_elem and n_ctrl per
+// domain; their control indices, coordinates and field "f" values one after
+// the other), with an optional boundary Surface (MeshBoundary of the
+// collection; mesh lines when draw_mesh), an optional Volume, and the camera
+// moved by reset_to_bounds(collection bounds, pads3) when pads3 is given,
+// then elevate and azimuth.  Colour bars off.  Writes the framebuffer's
+// colours and depths; with save_prefix set, also <prefix>.png and
+// <prefix>_depth.png through Framebuffer::save / save_depth.
+int ref_render_scene (int n_dom, const int *orders, const int *n_elems, const int *n_ctrls,
+                      const int *ctrl_idx, const float *xyz, const float *field, int w, int h,
+                      const float *cam9, float fov, const double *pads3, float elevate_deg,
+                      float azimuth_deg, int surface, int draw_mesh, float line_thickness,
+                      int volume, int samples, int use_lighting, int tf_samples, int n_rgb,
+                      const float *rgb_pts, int n_alpha, const float *alpha_pts, float *rgba,
+                      float *depth, const char *save_prefix)
+{
+  try
+  {
+    Collection col;
+    size_t oi = 0, oc = 0;
+    for (int d = 0; d < n_dom; ++d)
+    {
+      const int nd = (orders[d] + 1) * (orders[d] + 1) * (orders[d] + 1);
+      GridFunction<3> gf = make_gf3 (n_elems[d], nd, ctrl_idx + oi, n_ctrls[d], xyz + 3 * oc);
+      GridFunction<1> ff = make_gf1 (n_elems[d], nd, ctrl_idx + oi, n_ctrls[d], field + oc);
+      DataSet ds (make_hex_mesh (orders[d], gf));
+      ds.add_field (make_hex_field (orders[d], ff, "f"));
+      col.add_domain (ds);
+      oi += (size_t)n_elems[d] * nd;
+      oc += (size_t)n_ctrls[d];
+    }
+    Camera cam;
+    setup_camera (cam, w, h, cam9, fov);
+    if (pads3) cam.reset_to_bounds (col.bounds (), pads3[0], pads3[1], pads3[2]);
+    if (elevate_deg != 0.f) cam.elevate (elevate_deg);
+    if (azimuth_deg != 0.f) cam.azimuth (azimuth_deg);
+    ColorTable table = make_table (n_rgb, rgb_pts, n_alpha, alpha_pts);
+    Renderer renderer;
+    renderer.color_bar (false);
+    renderer.use_lighting (use_lighting != 0);
+    Collection faces;
+    if (surface)
+    {
+      MeshBoundary boundary;
+      faces = boundary.execute (col);
+      std::shared_ptr<Surface> surf = std::make_shared<Surface> (faces);
+      surf->field ("f");
+      surf->color_map ().color_table (table);
+      surf->draw_mesh (draw_mesh != 0);
+      if (draw_mesh) surf->line_thickness (line_thickness);
+      renderer.add (surf);
+    }
+    if (volume)
+    {
+      std::shared_ptr<Volume> vol = std::make_shared<Volume> (col);
+      vol->field ("f");
+      vol->samples (samples);
+      vol->use_lighting (use_lighting != 0);
+      vol->color_map ().samples (tf_samples);
+      vol->color_map ().color_table (table);
+      renderer.volume (vol);
+    }
+    Framebuffer fb = renderer.render (cam);
+    std::memcpy (rgba, (const void *)fb.colors ().get_host_ptr_const (),
+                 sizeof (float) * 4 * (size_t)w * h);
+    std::memcpy (depth, fb.depths ().get_host_ptr_const (), sizeof (float) * (size_t)w * h);
+    if (save_prefix)
+    {
+      fb.save (std::string (save_prefix));
+      fb.save_depth (std::string (save_prefix) + "_depth");
+    }
+    return 0;
   }
   catch (const std::exception &e)
   {

@@ -55,6 +55,15 @@ def lib():
         L.ref_tet_create.restype = vp
         L.ref_tet_create.argtypes = [C.c_int, C.c_int, C.c_int, vp, C.c_int, vp, vp, C.c_int, vp]
         L.ref_eval_tet_scalar.argtypes = [C.c_int, C.c_int, vp, C.c_int, vp, vp, vp]
+        L.ref_camera_move.argtypes = [C.c_int, C.c_int, vp, C.c_float, vp, vp, C.c_float,
+                                      C.c_float, vp, vp]
+        L.ref_render_scene.argtypes = [C.c_int, vp, vp, vp, vp, vp, vp, C.c_int, C.c_int, vp,
+                                       C.c_float, vp, C.c_float, C.c_float, C.c_int, C.c_int,
+                                       C.c_float, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int,
+                                       vp, C.c_int, vp, vp, vp, C.c_char_p]
+        L.ref_hex_set_bvh.argtypes = [vp, C.c_int, vp, C.c_int, vp, vp, vp, vp]
+        L.ref_volume_rays.argtypes = [vp, C.c_int, vp, C.c_int, C.c_int, C.c_int, C.c_int, vp,
+                                      C.c_int, vp, C.c_int, vp, vp, C.c_int]
         _lib = L
     return _lib
 
@@ -117,6 +126,36 @@ class RefHexMesh:
         if lib().ref_locate(self.h, n, _p(pts), _p(cell), _p(ref)) != 0:
             raise RuntimeError(lib().ref_last_error().decode())
         return cell, ref
+
+    def set_bvh(self, inner, leaf_nodes, aabb_ids, bounds6, ref_boxes):
+        """Install a BVH in the reference's record layout (inner [n,16],
+        leaf element ids, leaf sub-box ids, bounds (xmin,xmax,...), reference
+        boxes [n_leaf,6]) instead of the mesh's lazy build."""
+        inner = np.ascontiguousarray(inner, np.float32).reshape(-1, 16)
+        leaf = np.ascontiguousarray(leaf_nodes, np.int32)
+        ids = np.ascontiguousarray(aabb_ids, np.int32)
+        b6 = np.ascontiguousarray(bounds6, np.float32)
+        rb = np.ascontiguousarray(ref_boxes, np.float32).reshape(-1, 6)
+        if lib().ref_hex_set_bvh(self.h, inner.shape[0], _p(inner), leaf.size, _p(leaf), _p(ids),
+                                 _p(b6), _p(rb)) != 0:
+            raise RuntimeError(lib().ref_last_error().decode())
+
+    def volume_rays(self, rays9, samples, use_lighting, tf_samples, rgb_pts, alpha_pts,
+                    lights13):
+        """Volume::integrate on the given rays (reference Ray records, 9
+        floats each); returns the partials as (pixel, depth, r, g, b, a)."""
+        rays = np.ascontiguousarray(rays9, np.float32).reshape(-1, 9)
+        rgb = np.ascontiguousarray(rgb_pts, np.float32).reshape(-1)
+        alp = np.ascontiguousarray(alpha_pts, np.float32).reshape(-1)
+        lights = np.ascontiguousarray(lights13, np.float32).reshape(-1)
+        maxp = 5 * rays.shape[0]
+        parts = np.zeros((max(maxp, 1), 6), np.float32)
+        n = lib().ref_volume_rays(self.h, rays.shape[0], _p(rays), samples, int(use_lighting),
+                                  tf_samples, rgb.size // 4, _p(rgb), alp.size // 2, _p(alp),
+                                  lights.size // 13, _p(lights), _p(parts), maxp)
+        if n < 0:
+            raise RuntimeError(lib().ref_last_error().decode())
+        return parts[:n]
 
     def volume(self, w, h, cam9, fov, samples, use_lighting, tf_samples, rgb_pts, alpha_pts,
                lights13, want_partials=False):
@@ -257,6 +296,53 @@ class RefTriMesh(RefHexMesh):
                                       0 if self.field is None else self.field.size, fptr)
         if not self.h:
             raise RuntimeError(lib().ref_last_error().decode())
+
+
+def camera_move(w, h, cam9, fov, bounds6=None, pads=(0.0, 0.0, 0.0), elevate=0.0, azimuth=0.0):
+    """The reference Camera after reset_to_bounds (when bounds6 is given),
+    elevate and azimuth: (pos, look_at, up) as 9 floats, and the fov."""
+    cam = np.ascontiguousarray(cam9, np.float32)
+    out = np.zeros(9, np.float32)
+    fov_out = np.zeros(1, np.float32)
+    b6 = None if bounds6 is None else np.ascontiguousarray(bounds6, np.float32)
+    p3 = np.ascontiguousarray(pads, np.float64)
+    if lib().ref_camera_move(w, h, _p(cam), fov, None if b6 is None else _p(b6), _p(p3),
+                             elevate, azimuth, _p(out), _p(fov_out)) != 0:
+        raise RuntimeError(lib().ref_last_error().decode())
+    return out, float(fov_out[0])
+
+
+def render_scene(domains, w, h, cam9, fov, pads=None, elevate=0.0, azimuth=0.0, surface=True,
+                 draw_mesh=False, line_thickness=0.05, volume=True, samples=200,
+                 use_lighting=True, tf_samples=1024, rgb_pts=None, alpha_pts=None,
+                 save_prefix=None):
+    """The reference's Renderer::render over hex-mesh domains, each a tuple
+    (order, ctrl_idx, xyz, field): returns (rgba [h, w, 4], depth [h, w])."""
+    orders = np.array([d[0] for d in domains], np.int32)
+    nds = (orders + 1) ** 3
+    n_el = np.array([np.asarray(d[1]).size // nd for d, nd in zip(domains, nds)], np.int32)
+    n_ctrl = np.array([np.asarray(d[2]).reshape(-1, 3).shape[0] for d in domains], np.int32)
+    ci = np.ascontiguousarray(np.concatenate([np.asarray(d[1], np.int32).ravel() for d in domains]))
+    xyz = np.ascontiguousarray(np.concatenate([np.asarray(d[2], np.float32).ravel()
+                                               for d in domains]))
+    fld = np.ascontiguousarray(np.concatenate([np.asarray(d[3], np.float32).ravel()
+                                               for d in domains]))
+    rgb = np.ascontiguousarray(rgb_pts, np.float32).reshape(-1)
+    alp = np.ascontiguousarray(alpha_pts, np.float32).reshape(-1)
+    cam = np.ascontiguousarray(cam9, np.float32)
+    p3 = None if pads is None else np.ascontiguousarray(pads, np.float64)
+    rgba = np.zeros((h, w, 4), np.float32)
+    depth = np.zeros((h, w), np.float32)
+    st = lib().ref_render_scene(len(domains), _p(orders), _p(n_el), _p(n_ctrl), _p(ci), _p(xyz),
+                                _p(fld), w, h, _p(cam), fov, None if p3 is None else _p(p3),
+                                elevate, azimuth, int(surface), int(draw_mesh), line_thickness,
+                                int(volume), samples, int(use_lighting), tf_samples,
+                                rgb.size // 4, _p(rgb), alp.size // 2, _p(alp), _p(rgba),
+                                _p(depth),
+                                None if save_prefix is None else str(save_prefix).encode())
+    if st != 0:
+        raise RuntimeError(lib().ref_last_error().decode())
+    return rgba, depth
 
 
 def eval_tet_scalar(p, vals, refs, fixed=False):

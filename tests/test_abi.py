@@ -83,3 +83,32 @@ def test_shape_queries_and_tet_rejections_without_gpu():
     assert lib.drb_pack_elements(C.byref(m), None, None) == L.DRB_ERR_UNSUPPORTED
     m.dim, m.shape, m.n_elem = 2, S, 0
     assert lib.drb_pack_elements(C.byref(m), None, None) == L.DRB_OK   # triangle faces
+
+
+def test_camera_moves_match_reference():
+    """reset_to_bounds, elevate and azimuth give the reference Camera's
+    position, look_at and field of view bit for bit."""
+    import numpy as np
+    from oracle import refpy
+    from devil_ray_b200.render import Camera
+    if not refpy.available():
+        import pytest
+        pytest.skip("reference oracle not built")
+    cases = [((2.5, 2.5, 2.5), (0.5, 0.5, 0.5), None, (0, 0, 0), 10.0, 30.0),
+             ((0.0, 0.0, 5.0), (0.0, 0.0, 0.0), (-1, 8, 0, 1, 0, 1), (0.1, 0.2, 0.0), 0.0, 0.0),
+             ((3.0, -2.0, 1.0), (0.2, 0.1, -0.3), (-1, 1, -1, 1, -1, 1), (0.05, 0.0, 0.3),
+              -25.0, 47.5),
+             ((1.0, 2.0, 3.0), (0.0, 0.0, 0.0), (0, 1, 0, 2, 0, 0.5), (0, 0, 0), 89.0, -120.0)]
+    for pos, look, bounds, pads, el, az in cases:
+        c = Camera(320, 200, pos, look, (0.0, 1.0, 0.0), 30.0)
+        if bounds is not None:
+            c.reset_to_bounds(bounds, *pads)
+        if el:
+            c.elevate(el)
+        if az:
+            c.azimuth(az)
+        cam9 = np.array([*pos, *look, 0.0, 1.0, 0.0], np.float32)
+        want, fov = refpy.camera_move(320, 200, cam9, 30.0, bounds, pads, el, az)
+        got = np.array([*c.pos, *c.look_at], np.float32)
+        assert np.array_equal(got.view(np.uint32), want[:6].view(np.uint32)), (got, want[:6])
+        assert np.float32(c.fov) == np.float32(fov)

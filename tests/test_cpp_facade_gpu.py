@@ -142,3 +142,143 @@ def test_cpp_interface_matches_reference(cuda, ref, tmp_path, name):
     out = rv == np.float32(-7.0)
     assert np.array_equal(lv == np.float32(-7.0), out)
     assert np.abs(lv[~out] - rv[~out]).max() < 1e-4
+
+
+RENDER_EXE = ROOT / "devil_ray_b200" / "cpp" / "tests" / "t_dray_b200_render"
+
+
+def _scene_domains(name):
+    """(order, ctrl_idx, xyz, field) per domain: the mesh's elements split in
+    two halves by element index for the two-domain scenes."""
+    from devil_ray_b200 import meshgen
+    if name == "two_domains":
+        m = meshgen.warped_mesh(6, 2, 0.05, jitter=0.01, seed=2)
+        nd = (m.order + 1) ** 3
+        cut = (m.ctrl_idx.size // nd // 2) * nd
+        return [(m.order, m.ctrl_idx[:cut], m.xyz, m.field),
+                (m.order, m.ctrl_idx[cut:], m.xyz, m.field)]
+    m = meshgen.warped_mesh(5, 3, 0.05, gaussian_field_seed=4)
+    return [(m.order, m.ctrl_idx, m.xyz, m.field)]
+
+
+def _write_scene(d, doms, w, cam9, fov, pads, elevate, azimuth, surface, draw_mesh, thickness,
+                 volume, samples, lighting, tf_samples, rgb, alpha):
+    with open(d / "scene.bin", "wb") as f:
+        np.array([len(doms)], np.int32).tofile(f)
+        for order, ci, xyz, fld in doms:
+            nd = (order + 1) ** 3
+            np.array([order, ci.size // nd, xyz.shape[0]], np.int32).tofile(f)
+            np.ascontiguousarray(ci, np.int32).tofile(f)
+            np.ascontiguousarray(xyz, np.float32).tofile(f)
+            np.ascontiguousarray(fld, np.float32).tofile(f)
+        np.array([w, w], np.int32).tofile(f)
+        np.asarray(cam9, np.float32).tofile(f)
+        np.array([fov], np.float32).tofile(f)
+        np.array([pads is not None], np.int32).tofile(f)
+        np.asarray(pads if pads is not None else (0, 0, 0), np.float64).tofile(f)
+        np.array([elevate, azimuth], np.float32).tofile(f)
+        np.array([surface, draw_mesh], np.int32).tofile(f)
+        np.array([thickness], np.float32).tofile(f)
+        np.array([volume, samples, lighting, tf_samples], np.int32).tofile(f)
+        np.array([rgb.shape[0]], np.int32).tofile(f)
+        rgb.tofile(f)
+        np.array([alpha.shape[0]], np.int32).tofile(f)
+        alpha.tofile(f)
+
+
+SCENES = {
+    # two domains, camera on the collection's padded bounds then turned;
+    # surfaces of both domains (their cut faces too) and the volume in front
+    "two_domain_surface_volume": dict(mesh="two_domains", pads=(0.1, 0.05, 0.2), elevate=15.0,
+                                      azimuth=30.0, surface=1, draw_mesh=0, volume=1,
+                                      lighting=1),
+    # one domain, mesh lines over the shaded boundary, the volume in front
+    "mesh_lines": dict(mesh="one_domain", pads=None, elevate=0.0, azimuth=-20.0, surface=1,
+                       draw_mesh=1, volume=1, lighting=1),
+    # two domains, volume alone, unlit
+    "two_domain_volume": dict(mesh="two_domains", pads=(0.0, 0.0, 0.0), elevate=-10.0,
+                              azimuth=0.0, surface=0, draw_mesh=0, volume=1, lighting=0),
+}
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("scene", list(SCENES))
+def test_cpp_renderer_matches_reference(cuda, ref, tmp_path, scene):
+    """Renderer::render through the C++ interface against the reference's own
+    Renderer::render (colour bars off; its single-rank partial compositor is
+    the Volume::save blend): camera moves bit for bit, framebuffer colours
+    within 1/255 per channel, depths equal where both have a hit, and the
+    PNG files Framebuffer::save / save_depth / Volume::save write decode to
+    the framebuffers they were written from."""
+    from devil_ray_b200 import meshgen
+    from png_util import read_png_rgba, to_rgba8
+    if not RENDER_EXE.exists():
+        pytest.fail("C++ test program missing: build with make -C devil_ray_b200/cpp")
+    sc = SCENES[scene]
+    doms = _scene_domains(sc["mesh"])
+    w, fov, samples, tf_samples, thickness = 128, 30.0, 300, 256, 0.08
+    cam9 = np.array([*CAM["pos"], *CAM["look_at"], *CAM["up"]], np.float32)
+    rgb = np.array(meshgen.TF_RGB, np.float32)
+    alpha = np.array(meshgen.TF_ALPHA, np.float32)
+    _write_scene(tmp_path, doms, w, cam9, fov, sc["pads"], sc["elevate"], sc["azimuth"],
+                 sc["surface"], sc["draw_mesh"], thickness, sc["volume"], samples,
+                 sc["lighting"], tf_samples, rgb, alpha)
+    out = subprocess.run([str(RENDER_EXE), str(tmp_path)], capture_output=True, text=True,
+                         timeout=300)
+    assert out.returncode == 0, out.stderr
+    raw = np.fromfile(tmp_path / "render.bin", np.float32)
+    img = raw[:4 * w * w].reshape(w, w, 4)
+    dep = raw[4 * w * w:].reshape(w, w)
+    camf = np.fromfile(tmp_path / "camera.bin", np.float32)
+
+    # the reference: its camera moves, its Renderer, its PNG writer
+    bounds = None
+    if sc["pads"] is not None:
+        b6 = np.array([ref.RefHexMesh(o, ci, xyz).bvh()["bounds"] for o, ci, xyz, _ in doms])
+        bounds = np.array([b6[:, 0].min(), b6[:, 1].max(), b6[:, 2].min(), b6[:, 3].max(),
+                           b6[:, 4].min(), b6[:, 5].max()], np.float32)
+    want_cam, want_fov = ref.camera_move(w, w, cam9, fov, bounds,
+                                         sc["pads"] if sc["pads"] is not None else (0, 0, 0),
+                                         sc["elevate"], sc["azimuth"])
+    assert np.array_equal(camf[:6].view(np.uint32), want_cam[:6].view(np.uint32))
+    assert camf[6] == np.float32(want_fov)
+    rimg, rdep = ref.render_scene(doms, w, w, cam9, fov, pads=sc["pads"], elevate=sc["elevate"],
+                                  azimuth=sc["azimuth"], surface=bool(sc["surface"]),
+                                  draw_mesh=bool(sc["draw_mesh"]), line_thickness=thickness,
+                                  volume=bool(sc["volume"]), samples=samples,
+                                  use_lighting=bool(sc["lighting"]), tf_samples=tf_samples,
+                                  rgb_pts=rgb, alpha_pts=alpha,
+                                  save_prefix=tmp_path / "ref_render")
+    d = np.abs(img - rimg)
+    bad = np.any(d > 1.0 / 255.0, axis=-1)
+    hit, rhit = np.isfinite(dep) & (dep < 1e30), np.isfinite(rdep) & (rdep < 1e30)
+    print(f"{scene}: alpha>0 pixels {np.mean(img[..., 3] > 0):.3f}, "
+          f"pixels > 1/255: {bad.sum()} of {bad.size}, max diff {d.max():.2e}, "
+          f"depth coverage {hit.mean():.3f} vs {rhit.mean():.3f}")
+    assert np.mean(img[..., 3] > 0) > 0.1
+    assert bad.mean() < 0.005
+    both = hit & rhit
+    assert (hit != rhit).mean() < 0.005
+    assert np.allclose(dep[both], rdep[both], rtol=1e-4, atol=1e-4)
+    # the PNG files decode to what was rendered
+    assert np.array_equal(read_png_rgba(tmp_path / "render.png"), to_rgba8(img))
+    ref_png = read_png_rgba(tmp_path / "ref_render.png")
+    assert np.array_equal(ref_png, to_rgba8(rimg))
+    dpng = read_png_rgba(tmp_path / "render_depth.png")
+    assert np.all(dpng[..., 3] == 255) and np.all(dpng[..., 0] == dpng[..., 1])
+    if sc["mesh"] == "one_domain":
+        # Volume::save of the single domain's partials against the
+        # reference's Volume::integrate + save compositing on the same camera
+        vimg = read_png_rgba(tmp_path / "volume.png")
+        o, ci, xyz, fld = doms[0]
+        from devil_ray_b200.render import Camera, PointLight
+        cam = Camera(w, w, tuple(camf[:3]), tuple(camf[3:6]), CAM["up"], float(camf[6]))
+        light = PointLight.default(cam)
+        cam9m = np.array([*camf[:6], *CAM["up"]], np.float32)
+        rv, _ = ref.RefHexMesh(o, ci, xyz, fld).volume(
+            w, w, cam9m, float(camf[6]), samples, bool(sc["lighting"]), tf_samples, rgb, alpha,
+            light.as13()[None])
+        vd = np.abs(vimg.astype(np.int32) - to_rgba8(rv).astype(np.int32))
+        print(f"{scene}: Volume::save pixels off by more than 1 level: "
+              f"{np.any(vd > 1, axis=-1).sum()}")
+        assert np.any(vd > 1, axis=-1).mean() < 0.005

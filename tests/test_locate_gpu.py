@@ -43,7 +43,7 @@ def _shared_face_ok(m, cell_a, ref_a, cell_b, ref_b, band=2e-3):
     return ok
 
 
-@pytest.mark.parametrize("name", ["volume_8", "trilinear_12", "p3_10", "p1_9"])
+@pytest.mark.parametrize("name", ["volume_8", "trilinear_12", "trilinear_12_d25", "p3_10", "p1_9"])
 def test_locate_matches_reference(cuda, ref, name):
     import torch
     from devil_ray_b200 import _lib as L
@@ -248,3 +248,74 @@ def test_locate_graph_replay_matches_eager(cuda, shape):
         assert torch.equal(c0, c1)
         assert torch.equal(r0.view(torch.int32), r1.view(torch.int32))
         assert (c1 >= 0).float().mean() > 0.85
+
+
+@pytest.mark.parametrize("name", ["volume_8", "p3_10", "p1_9"])
+@pytest.mark.parametrize("guess", ["centre", "subref"])
+def test_staged_equals_ordered_and_plain(cuda, name, guess):
+    """drb_locate_batched stages its queries in processing order and writes
+    its results contiguously; the answers equal the query-order path's
+    (drb_locate_ordered, which reads the queries where they lie) and the
+    plain one-thread-per-query kernel's bit for bit, statistics included."""
+    import torch
+    from devil_ray_b200 import _lib as L
+    from devil_ray_b200 import api
+    m, q, g = _setup(cuda, name, 60000, 23)
+    mode = L.GUESS_ELEM_CENTER if guess == "centre" else L.GUESS_SUBREF_CENTER
+    loc = api.BatchedLocator(g, tol=1e-5, max_steps=20, guess_mode=mode)
+    c0, r0, i0, a0, n0 = loc.locate(q, stats=True)
+    order = loc.order(q)
+    c1, r1, i1, a1, n1 = loc.locate(q, order=order, stats=True)
+    c2, r2 = g.locate(q, tol=1e-5, max_steps=20, guess_mode=mode)
+    # results staged as well and put back by a separate pass (sort_queries 2)
+    loc2 = api.BatchedLocator(g, tol=1e-5, max_steps=20, guess_mode=mode,
+                              config=L.DrbLocateConfig(128, 0, 64, 2, 0))
+    c3, r3, i3, a3, n3 = loc2.locate(q, stats=True)
+    torch.cuda.synchronize()
+    for c, r in ((c1, r1), (c2, r2), (c3, r3)):
+        assert torch.equal(c0, c)
+        assert torch.equal(r0.view(torch.int32), r.view(torch.int32))
+    for i, a, nd in ((i1, a1, n1), (i3, a3, n3)):
+        assert torch.equal(i0, i) and torch.equal(a0, a) and torch.equal(n0, nd)
+
+
+def test_stage_records_and_staged_kernel(cuda):
+    """drb_query_stage lists every query once, cell by cell along the Morton
+    curve, with its input index in w; drb_locate_staged on those records
+    gives each query the answer drb_locate_batched gives it."""
+    import torch
+    from devil_ray_b200 import api
+    m, q, g = _setup(cuda, "trilinear_12", 80000, 29)
+    loc = api.BatchedLocator(g, tol=1e-5, max_steps=20)
+    rec = loc.stage(q)
+    res = loc.locate_staged(rec, records=True)
+    cs, rs = loc.locate_staged(rec)
+    c0, r0 = loc.locate(q)
+    torch.cuda.synchronize()
+    assert torch.equal(cs, c0) and torch.equal(rs.view(torch.int32), r0.view(torch.int32))
+    idx = rec[:, 3].contiguous().view(torch.int32).long()
+    assert torch.equal(torch.sort(idx).values, torch.arange(q.shape[0], device=cuda))
+    qd = torch.as_tensor(q, device=cuda)
+    assert torch.equal(rec[:, :3].contiguous().view(torch.int32), qd[idx].view(torch.int32))
+    cell_of = res[:, 0].contiguous().view(torch.int32)
+    assert torch.equal(cell_of, c0[idx])
+    assert torch.equal(res[:, 1:].contiguous().view(torch.int32), r0[idx].view(torch.int32))
+
+
+def test_autotuner_config_is_valid_and_exact(cuda):
+    """drb_locate_tune returns a launch shape from its candidate set, and the
+    tuned locate's results equal the default shape's bit for bit."""
+    import torch
+    from devil_ray_b200 import api
+    m, q, g = _setup(cuda, "trilinear_12", 120000, 31)
+    base = api.BatchedLocator(g, tol=1e-5, max_steps=20)
+    c0, r0 = base.locate(q)
+    tuned = api.BatchedLocator(g, tol=1e-5, max_steps=20)
+    cfg, ms = tuned.tune(q[:50000])
+    assert cfg.block in (64, 128, 256) and cfg.blocks_per_sm in (0, 2, 4)
+    assert cfg.chunk in (32, 64, 128, 256) and cfg.reg_elements in (0, 1, 2)
+    assert cfg.sort_queries == 1 and ms > 0.0
+    c1, r1 = tuned.locate(q)
+    torch.cuda.synchronize()
+    assert torch.equal(c0, c1)
+    assert torch.equal(r0.view(torch.int32), r1.view(torch.int32))

@@ -58,11 +58,57 @@ def _volume_case(cuda, ref, mesh_name, w, samples, lighting, coherent, guess):
     return rimg, rparts, img, parts
 
 
+def _near_face_rays(cuda, ref, m, w, samples, pixels, band=2e-4):
+    """For each pixel, whether its ray has a sample point that the
+    reference's locate puts within `band` of a face of its element (a point
+    on a face shared by two elements, which either may own within the
+    Newton tolerance).  The sample points are the reference march's:
+    near + k * dt with dt = |bounds diagonal| / samples, accumulated in
+    float32 (rendering/volume.cpp:89-99,148-205)."""
+    from devil_ray_b200 import api
+    from devil_ray_b200.render import Camera, cull_rays
+    g = api.UnstructuredMesh(m.ctrl_idx, m.xyz, m.order, device=cuda)
+    b = g.bounds()
+    cam = Camera(w, w, CAM["pos"], CAM["look_at"], CAM["up"], CAM["fov"])
+    active = cull_rays(cam.create_rays(cuda), b).cpu().numpy()
+    pid = active[:, 8].view(np.int32)
+    lo = np.array(b[0::2], np.float32)
+    hi = np.array(b[1::2], np.float32)
+    e = (hi - lo).astype(np.float32)
+    mag = np.sqrt(np.float32(e[0] * e[0] + e[1] * e[1] + e[2] * e[2]), dtype=np.float32)
+    dt = np.float32(mag / np.float32(samples))
+    rm = ref.RefHexMesh(m.order, m.ctrl_idx, m.xyz)
+    out = np.zeros(len(pixels), bool)
+    for k, px in enumerate(pixels):
+        sel = np.nonzero(pid == px)[0]
+        if sel.size == 0:
+            continue
+        r = active[sel[0]]
+        d = np.float32(r[3]) + dt
+        pts = []
+        while d < np.float32(r[7]):
+            pts.append(r[4:7] + d * r[0:3])
+            d = np.float32(d + dt)
+        if not pts:
+            continue
+        cell, rr = rm.locate(np.asarray(pts, np.float32))
+        ins = rr[cell >= 0]
+        out[k] = bool(np.any((ins < band) | (ins > 1.0 - band)))
+    return out
+
+
 @pytest.mark.parametrize("coherent", [False, True])
 @pytest.mark.parametrize("lighting", [True, False])
 def test_volume_image_matches_reference(cuda, ref, coherent, lighting):
+    """Images within 1/255 per channel, except pixels whose ray samples a
+    point on a face shared by two elements: there the element that owns the
+    sample may differ, and with lighting so does the field gradient (the
+    field is only continuous across faces).  Every such pixel is checked to
+    be one of those rays."""
     from devil_ray_b200 import _lib as L
-    rimg, rparts, img, parts = _volume_case(cuda, ref, "volume_8", 128, 500, lighting,
+    from devil_ray_b200 import meshgen
+    w, samples = 128, 500
+    rimg, rparts, img, parts = _volume_case(cuda, ref, "volume_8", w, samples, lighting,
                                             coherent, L.GUESS_ZERO)
     d = np.abs(img - rimg)
     bad = np.any(d > 1.0 / 255.0, axis=-1)
@@ -71,6 +117,12 @@ def test_volume_image_matches_reference(cuda, ref, coherent, lighting):
     assert bad.mean() < 0.002
     assert d.max() < 0.05
     assert abs(parts.shape[0] - len(rparts)) <= max(2, 0.002 * len(rparts))
+    pixels = np.nonzero(bad.ravel())[0]
+    if pixels.size:
+        on_face = _near_face_rays(cuda, ref, meshgen.workload_mesh("volume_8"), w, samples,
+                                  pixels)
+        print(f"  of those, rays through a shared face: {on_face.sum()}")
+        assert on_face.all(), f"pixels {pixels[~on_face]} differ without a shared-face sample"
 
 
 def test_volume_partials_match_reference(cuda, ref):
@@ -80,12 +132,22 @@ def test_volume_partials_match_reference(cuda, ref):
     p = parts.cpu().numpy()
     pix = p[:, 0].view(np.int32)
     rpix = rparts[:, 0].astype(np.int32)
-    if len(pix) == len(rpix):
-        same = pix == rpix
-        assert same.mean() > 0.998
-        dd = np.abs(p[same, 1] - rparts[same, 1])
-        assert np.median(dd) == 0.0
-        assert np.abs(p[same, 2:] - rparts[same, 2:]).max() < 0.05
+    # the same segments: counts equal, and per pixel the same number of
+    # partials (a shared-face sample may split or join a segment: at most a
+    # few pixels differ)
+    assert abs(len(pix) - len(rpix)) <= max(2, 0.002 * len(rpix))
+    cnt = np.bincount(pix, minlength=96 * 96)
+    rcnt = np.bincount(rpix, minlength=96 * 96)
+    assert (cnt != rcnt).mean() < 0.002
+    # pixels with the same segments: depths bit-equal in the main, colours close
+    same_pix = np.nonzero(cnt == rcnt)[0]
+    keep = np.isin(pix, same_pix)
+    rkeep = np.isin(rpix, same_pix)
+    a, b = p[keep], rparts[rkeep]
+    assert np.array_equal(a[:, 0].view(np.int32), b[:, 0].astype(np.int32))
+    dd = np.abs(a[:, 1] - b[:, 1])
+    assert np.median(dd) == 0.0
+    assert np.abs(a[:, 2:] - b[:, 2:]).max() < 0.05
 
 
 def test_volume_order3(cuda, ref):

@@ -1,11 +1,13 @@
 """The allocation-free batched locate, called through the C-ABI.
 
 It exists for callers that cannot allocate device memory while they locate
-points (stream capture without allocation nodes, a host application's own
-memory pool, latency-critical paths).  Its answers must equal those of the
-allocating drb_locate_batched on the same inputs, on consecutive calls that
-reuse the library's fixed scratch array.  This file is collected last so a
-failure here cannot hide the result of another test.
+points: a host application whose device memory belongs to its own pool or
+allocator, or a latency-critical path that cannot absorb cudaMalloc's
+implicit synchronisation.  Its answers must equal those of the allocating
+drb_locate_batched on the same inputs, bit for bit, on consecutive calls that
+reuse the library's fixed scratch array, and a call must leave the device's
+stream-ordered pool and torch's allocator untouched.  This file is collected
+last so a failure here cannot hide the result of another test.
 """
 import ctypes as C
 
@@ -20,6 +22,31 @@ def _call(lib, L, fn, mesh_d, bvh_d, pts, opts, cell, ref, stream):
             C.byref(opts), None, C.c_void_p(cell.data_ptr()), C.c_void_p(ref.data_ptr()),
             L.DrbQueryStats(), C.c_void_p(stream)]
     return getattr(lib, fn)(*args)
+
+
+def _pool_used_high(device_index):
+    """(used bytes now, high-water mark) of the device's default
+    stream-ordered pool, where the allocating entry points take scratch."""
+    from cuda.bindings import runtime as rt
+    err, pool = rt.cudaDeviceGetDefaultMemPool(device_index)
+    assert err == rt.cudaError_t.cudaSuccess
+    out = []
+    for attr in (rt.cudaMemPoolAttr.cudaMemPoolAttrUsedMemCurrent,
+                 rt.cudaMemPoolAttr.cudaMemPoolAttrUsedMemHigh):
+        err, v = rt.cudaMemPoolGetAttribute(pool, attr)
+        assert err == rt.cudaError_t.cudaSuccess
+        out.append(int(v))
+    return out
+
+
+def _reset_pool_high(device_index):
+    from cuda.bindings import driver
+    from cuda.bindings import runtime as rt
+    err, pool = rt.cudaDeviceGetDefaultMemPool(device_index)
+    assert err == rt.cudaError_t.cudaSuccess
+    (err,) = rt.cudaMemPoolSetAttribute(pool, rt.cudaMemPoolAttr.cudaMemPoolAttrUsedMemHigh,
+                                        driver.cuuint64_t(0))
+    assert err == rt.cudaError_t.cudaSuccess
 
 
 def test_noalloc_matches_allocating_path_twice(cuda):
@@ -42,13 +69,24 @@ def test_noalloc_matches_allocating_path_twice(cuda):
         c1 = torch.full_like(c0, -7)
         r1 = torch.full_like(r0, 7.0)
         assert _call(lib, L, "drb_locate_batched", mesh_d, bvh_d, pts, opts, c0, r0, stream) == 0
+        torch.cuda.synchronize()
+        # the allocating call has returned its scratch; the allocation-free
+        # call must take none from the pool nor from torch's allocator
+        _reset_pool_high(cuda.index or 0)
+        used0, _ = _pool_used_high(cuda.index or 0)
+        torch_used0 = torch.cuda.memory_allocated(cuda)
         assert _call(lib, L, "drb_locate_batched_noalloc", mesh_d, bvh_d, pts, opts, c1, r1,
                      stream) == 0, lib.drb_last_error()
         torch.cuda.synchronize()
-        # same kernels, same processing order: identical results (tolerance 0,
-        # within the 1e-5 reference-space tolerance used by the other tests)
+        used1, high1 = _pool_used_high(cuda.index or 0)
+        assert used1 == used0 and high1 <= used0, \
+            f"call {call}: pool use moved {used0} -> {used1} (high {high1})"
+        assert torch.cuda.memory_allocated(cuda) == torch_used0
+        # every query's answer is independent of the processing order, so the
+        # two paths agree bit for bit
         assert torch.equal(c0, c1), f"call {call}: cell ids differ"
-        assert torch.allclose(r0, r1, rtol=0, atol=1e-5), f"call {call}: ref points differ"
+        assert torch.equal(r0.view(torch.int32), r1.view(torch.int32)), \
+            f"call {call}: ref points differ"
         assert 0.85 < (c1 >= 0).float().mean().item() < 0.95
 
 
