@@ -73,7 +73,7 @@ def parse():
     ap.add_argument("--launch", default="128,4,64,0", metavar="B,BPS,CHUNK,ROWS[,SORT]",
                     help="launch shape of --profile: block, blocks per SM (0 = all "
                          "resident), chunk, row mode, query order mode (default 1)")
-    ap.add_argument("--guess", default="centre", choices=["centre", "subref"],
+    ap.add_argument("--guess", default="centre", choices=["centre", "subref", "linear"],
                     help="first guess of --profile")
     return ap.parse_args()
 
@@ -525,11 +525,19 @@ def second_mesh_leg(dev, args, pts, cfg, timed, job_located):
     _, _, it_s, _, _ = sub.locate(pts, stats=True)
     plain_value = job_located(located) / (plain_ms * 1e-3)
     sub_value = job_located(located) / (sub_ms * 1e-3)
+    lin = api.BatchedLocator(mesh, tol=TOL, max_steps=MAX_STEPS,
+                             guess_mode=L.GUESS_SUBBOX_LINEAR, config=cfg)
+    for _ in range(2):
+        lin.locate(pts, out=(cell, ref))
+    lin_ms = timed(lambda: lin.locate(pts, out=(cell, ref)), args.steps) / args.steps
+    _, _, it_l, _, _ = lin.locate(pts, stats=True)
+    lin_value = job_located(located) / (lin_ms * 1e-3)
     centre = api.BatchedLocator(mesh, tol=TOL, max_steps=MAX_STEPS,
                                 guess_mode=L.GUESS_ELEM_CENTER, config=cfg)
     _, _, it_c, _, _ = centre.locate(pts, stats=True)
     lg = learned_leg(dev, args, mesh, pts, cfg, timed, job_located,
-                     {"batched_subref": sub_value}, plain_value, float(it_c.float().mean()))
+                     {"batched_subref": sub_value, "batched_linear": lin_value}, plain_value,
+                     float(it_c.float().mean()))
     lg.pop("_locate", None)
     return {"workload": "locate_64_d25: 64^3 hex order 2, trilinear distortion 25%, the same "
                         f"{n} held-out queries, tol 1e-5, 20 steps",
@@ -537,6 +545,8 @@ def second_mesh_leg(dev, args, pts, cfg, timed, job_located):
             "plain": {"value": plain_value, "ms_per_step": plain_ms},
             "batched_subref": {"value": sub_value, "ms_per_step": sub_ms,
                                "mean_newton_iters": float(it_s.float().mean())},
+            "batched_linear": {"value": lin_value, "ms_per_step": lin_ms,
+                               "mean_newton_iters": float(it_l.float().mean())},
             "learned": lg}
 
 
@@ -681,6 +691,89 @@ def volume_cpu_tiles(m, bvh, cams, lights, samp, args, tile=64, seed=6):
                       "the GPU's coherent march on the same rays"}
 
 
+def volume_learned_leg(dev, args, mesh, cam, timed, samples=1000, ray_stride=32):
+    """The learned guess on the volume workload: the sample positions of
+    every ray_stride-th ray of one orbit (near + k dt up to far, dt the
+    bounds diagonal / samples; the march stops earlier where the opacity
+    saturates) are located at tol 1e-5 by the learned-guess path (the
+    order-3 network trained on 4M of the method's own solutions in this
+    mesh) and, on the same points, by the plain kernel (one thread per
+    point, element-centre guess) and the batched kernel with the element-
+    and sub-box-centre guesses.  Located samples/s, locate only (no
+    shading or compositing)."""
+    import torch
+    from devil_ray_b200 import _lib as L
+    from devil_ray_b200 import api
+    from devil_ray_b200 import learned as LG
+    from devil_ray_b200.render import cull_rays
+    b = mesh.bounds()
+    rays = cull_rays(cam.create_rays(dev), b)
+    rays = rays[::ray_stride].contiguous()
+    e = torch.tensor([b[1] - b[0], b[3] - b[2], b[5] - b[4]], dtype=torch.float32)
+    dt = float(torch.sqrt((e * e).sum()) / samples)
+    near, far = rays[:, 3], rays[:, 7]
+    count = torch.clamp(torch.ceil((far - near) / dt) - 1, min=0).long()
+    ray_of = torch.repeat_interleave(torch.arange(rays.shape[0], device=dev), count)
+    first = torch.cumsum(count, 0) - count
+    k = torch.arange(ray_of.numel(), device=dev) - first[ray_of] + 1
+    t = near[ray_of] + k.float() * dt
+    pts = (rays[ray_of, 4:7] + t[:, None] * rays[ray_of, 0:3]).contiguous()
+    del ray_of, k, t, first
+    n = pts.shape[0]
+    cell = torch.empty(n, dtype=torch.int32, device=dev)
+    ref = torch.empty((n, 3), dtype=torch.float32, device=dev)
+    out = {"workload": f"sample positions of every {ray_stride}th ray of the first orbit "
+                       f"({rays.shape[0]} rays, {n} points) in the 128^3 order-3 mesh, "
+                       "tol 1e-5, 20 steps; locate only",
+           "points": n}
+    reps = max(2, args.steps // 5)
+
+    def leg(name, fn, stats_fn):
+        fn()
+        ms = timed(fn, reps) / reps
+        located = int((cell >= 0).sum().item())
+        res = stats_fn()
+        it = res[2]
+        out[name] = {"value": located / (ms * 1e-3), "ms": ms, "located": located,
+                     "mean_newton_iters": float(it.float().mean()),
+                     "iteration_histogram": torch.bincount(it.long().clamp(max=40),
+                                                           minlength=41).cpu().tolist()}
+
+    leg("plain", lambda: mesh.locate(pts, tol=TOL, max_steps=MAX_STEPS,
+                                     guess_mode=L.GUESS_ELEM_CENTER),
+        lambda: mesh.locate(pts, tol=TOL, max_steps=MAX_STEPS, guess_mode=L.GUESS_ELEM_CENTER,
+                            stats=True))
+    # the plain leg's locate returns new arrays: count its located points
+    c_plain, _ = mesh.locate(pts, tol=TOL, max_steps=MAX_STEPS, guess_mode=L.GUESS_ELEM_CENTER)
+    out["plain"]["located"] = int((c_plain >= 0).sum().item())
+    out["plain"]["value"] = out["plain"]["located"] / (out["plain"]["ms"] * 1e-3)
+    del c_plain
+    for name, mode in (("batched_centre", L.GUESS_ELEM_CENTER),
+                       ("batched_subref", L.GUESS_SUBREF_CENTER)):
+        loc = api.BatchedLocator(mesh, tol=TOL, max_steps=MAX_STEPS, guess_mode=mode)
+        leg(name, lambda: loc.locate(pts, out=(cell, ref)), lambda: loc.locate(pts, stats=True))
+    t0 = time.perf_counter()
+    model = LG.GuessMLP(dev, seed=1, order=3)
+    losses = LG.train(model, mesh, samples=args.train_samples, batch=16384, epochs=3, lr=3e-3)
+    torch.cuda.synchronize()
+    model.check_err()
+    ll = LG.LearnedLocator(mesh, model, TOL, MAX_STEPS)
+    leg("learned", lambda: ll.locate(pts, out=(cell, ref)), lambda: ll.locate(pts, stats=True))
+    out["learned"]["train"] = {"samples": args.train_samples, "epochs": 3,
+                               "seconds": time.perf_counter() - t0, "first_loss": losses[0],
+                               "final_loss": losses[-1]}
+    he, hp, _, _ = LG.training_set(mesh, 1 << 20, seed=12345)
+    gss = model.guess(mesh, he, hp)
+    _, fg, ig = LG.newton_pairs(mesh, he, hp, TOL, MAX_STEPS, gss)
+    _, fc, ic = LG.newton_pairs(mesh, he, hp, TOL, MAX_STEPS)
+    out["learned"]["held_out_pairs"] = {"fallback_rate": float(1.0 - fg[fc].float().mean()),
+                                        "mean_iters_guess": float(ig[fc].float().mean()),
+                                        "mean_iters_centre": float(ic[fc].float().mean())}
+    for k in ("plain", "batched_centre", "batched_subref"):
+        out["learned"][f"ratio_vs_{k}"] = out["learned"]["value"] / out[k]["value"]
+    return out
+
+
 def volume_bench(dev, args, timed, with_cpu=False):
     """128^3 order-3 volume: 2048^2 rays, 1000 samples,
     1024-entry transfer function, `orbits` seeded cameras replayed from one
@@ -773,6 +866,12 @@ def volume_bench(dev, args, timed, with_cpu=False):
     ms_plain = timed(lambda: frame(0, False), 1)
     samples_plain = int(samp[0].sum().item())
     img = fbs[0].image()
+    learned_leg_out = None
+    if not args.no_learned:
+        try:
+            learned_leg_out = volume_learned_leg(dev, args, mesh, cams[0], timed)
+        except Exception as exc:
+            learned_leg_out = {"error": repr(exc)}
     cpu = None
     if with_cpu:
         # per-ray sample counts of the coherent orbits, for the CPU tiles
@@ -785,6 +884,7 @@ def volume_bench(dev, args, timed, with_cpu=False):
         del m
     return {
         "cpu_reference": cpu,
+        "learned_locate_on_samples": learned_leg_out,
         "workload": "volume_128: 128^3 hex order 3 (2.1M elements, 69.2M sub-box leaves), "
                     "warp 0.05, 8 Gaussian blobs; 2048^2 rays, 1000 samples, 1024-entry TF, "
                     f"{len(cams)} orbits in one CUDA graph, tol 1e-5",
@@ -901,6 +1001,8 @@ def main():
         loc.config, tune_ms = best_cfg, 0.0
         if args.guess == "subref":
             loc.guess_mode = L.GUESS_SUBREF_CENTER
+        elif args.guess == "linear":
+            loc.guess_mode = L.GUESS_SUBBOX_LINEAR
     else:
         best_cfg, tune_ms = loc.tune(pts[: min(n, 1 << 21)])
     cell = torch.empty(n, dtype=torch.int32, device=dev)
@@ -935,15 +1037,21 @@ def main():
         launches0 = L.lib().drb_kernel_launches()
         ms_step = timed(batched_step, args.steps) / args.steps
         launches = L.lib().drb_kernel_launches() - launches0
-        # the kernel alone on staged records, with the live DRAM meter
-        staged = loc.stage(pts)
-        records = best_cfg.sort_queries == 2
-        res4 = torch.empty((n, 4), dtype=torch.float32, device=dev) if records else (cell, ref)
-        loc.locate_staged(staged, out=res4, records=records)
+        # the kernel alone: on queries already in processing order (read
+        # through the order, or staged records for sort modes 2 and 3)
+        if best_cfg.sort_queries >= 2:
+            staged = loc.stage(pts)
+            records = best_cfg.sort_queries == 3
+            res4 = torch.empty((n, 4), dtype=torch.float32, device=dev) if records else \
+                (cell, ref)
+            kern = lambda: loc.locate_staged(staged, out=res4, records=records)
+        else:
+            qorder = loc.order(pts)
+            kern = lambda: loc.locate(pts, order=qorder, out=(cell, ref))
+        kern()
         dram = DramMeter(local)
         dram.start()
-        kern_ms = timed(lambda: loc.locate_staged(staged, out=res4, records=records),
-                        args.steps) / args.steps
+        kern_ms = timed(kern, args.steps) / args.steps
         dr = dram.stop()
         if rank == 0:
             print(json.dumps({"profile": True, "ms_per_step": ms_step, "queries": n,
@@ -1027,29 +1135,57 @@ def main():
     except Exception as exc:
         graph_small = {"error": repr(exc)}
 
+    # the sub-box linear first guess: each leaf's element map linearised at
+    # its sub-box centre (per-leaf maps built once with the BVH)
+    loc_lin = api.BatchedLocator(mesh, tol=TOL, max_steps=MAX_STEPS,
+                                 guess_mode=L.GUESS_SUBBOX_LINEAR, config=best_cfg)
+    ev0.record()
+    bvh.build_leaf_maps(mesh)
+    ev1.record()
+    torch.cuda.synchronize()
+    leaf_maps_ms = ev0.elapsed_time(ev1)
+    for _ in range(2):
+        loc_lin.locate(pts, out=(cell, ref))
+    lin_ms = timed(lambda: loc_lin.locate(pts, out=(cell, ref)), args.steps) / args.steps
+    lin_located = int((cell >= 0).sum().item())
+    _, _, it_l, ca_l, nd_l = loc_lin.locate(pts, stats=True)
+    lin_stats = (float(it_l.float().mean()), float(ca_l.float().mean()),
+                 float(nd_l.float().mean()))
+    lin_value = job_located(lin_located) / (lin_ms * 1e-3)
+    batched_lin = {"value": lin_value, "ms_per_step": lin_ms, "mean_newton_iters": lin_stats[0],
+                   "leaf_maps_build_ms": leaf_maps_ms,
+                   "note": "Morton-ordered persistent kernel, first guess from each leaf's "
+                           "element map linearised at its sub-box centre"}
+    del it_l, ca_l, nd_l
+
     head_name, head_locate, head_loc, head_value = ("batched (element-centre guess)", loc.locate,
                                                     loc, batched_value)
     if sub_value > head_value:
         head_name, head_locate, head_loc, head_value = ("batched (sub-box-centre guess)",
                                                         loc_sub.locate, loc_sub, sub_value)
+    if lin_value > head_value:
+        head_name, head_locate, head_loc, head_value = ("batched (sub-box linear guess)",
+                                                        loc_lin.locate, loc_lin, lin_value)
     # the kernel of the faster batched path alone (roofline): its queries
-    # already staged in processing order, the same launch shape
+    # already in Morton-cell order (drb_locate_ordered), the same launch shape
     roof_loc = head_loc
-    roof_stats = sub_stats if roof_loc is loc_sub else (mean_it, mean_ca, mean_nd)
-    staged = roof_loc.stage(pts)
+    roof_stats = sub_stats if roof_loc is loc_sub else lin_stats if roof_loc is loc_lin else \
+        (mean_it, mean_ca, mean_nd)
+    qorder = roof_loc.order(pts)
     for _ in range(2):
-        roof_loc.locate_staged(staged, out=(cell, ref))
+        roof_loc.locate(pts, order=qorder, out=(cell, ref))
     dram = DramMeter(local)
     dram.start()
-    kern_ms = timed(lambda: roof_loc.locate_staged(staged, out=(cell, ref)),
+    kern_ms = timed(lambda: roof_loc.locate(pts, order=qorder, out=(cell, ref)),
                     args.steps) / args.steps
     dram_read = dram.stop()
-    del staged
+    del qorder
     learned = None
     if not args.no_learned and m.order == 2:
         try:
             learned = learned_leg(dev, args, mesh, pts, best_cfg, timed, job_located,
-                                  {"batched_subref": sub_value, "batched_centre": batched_value},
+                                  {"batched_subref": sub_value, "batched_centre": batched_value,
+                                   "batched_linear": lin_value},
                                   plain_value, mean_it)
         except Exception as exc:
             learned = {"error": repr(exc)}
@@ -1080,8 +1216,8 @@ def main():
     located = int((cell >= 0).sum().item())
     value = job_located(located) / (ms_step * 1e-3)
 
-    # Compulsory DRAM bytes of one kernel launch: each staged query record
-    # read (16 B) and result record written (16 B) once, and the arrays the
+    # Compulsory DRAM bytes of one kernel launch: each query's order entry
+    # (4 B) and point (12 B) read and its result (16 B) written once, and the arrays the
     # traversal and the solves read at least once over a batch that covers
     # the mesh: the 4-wide tree (128 B per node), the leaf element ids, the
     # packed element rows, and for the sub-box-centre guess the leaf sub-box
@@ -1089,8 +1225,10 @@ def main():
     # these bytes are the floor of the launch's DRAM traffic.
     stride = L.lib().drb_packed_stride(3, m.order, 3)
     sub_guess = roof_loc is loc_sub
+    lin_guess = roof_loc is loc_lin
     compulsory = (n * (16 + 16) + bvh.n_wide * 128 + bvh.n_leaf * 4 + m.n_elem * stride * 4
-                  + (bvh.n_leaf * (4 + 24) if sub_guess else 0))
+                  + (bvh.n_leaf * (4 + 24) if sub_guess else 0)
+                  + (bvh.n_leaf * 64 if lin_guess else 0))
     achieved_gbs = compulsory / (kern_ms * 1e-3) / 1e9
     # the per-query figure of the algorithmic byte formula (point 12 B +
     # Location 16 B + one element's indices and coordinates nd x (4 + 12) B +
@@ -1188,12 +1326,14 @@ def main():
             "roofline": {"bound": "hbm", "achieved": achieved_gbs, "peak": peak, "unit": "GB/s",
                          "frac": achieved_gbs / peak,
                          "traffic": traffic,
-                         "achieved_bytes": "compulsory DRAM bytes per launch: 16 B query "
-                                           "record in + 16 B result (cell + reference point) "
-                                           "out per query, the 4-wide tree, leaf ids and "
-                                           "packed rows once"
+                         "achieved_bytes": "compulsory DRAM bytes per launch: 4 B order "
+                                           "entry + 12 B point in and 16 B result (cell + "
+                                           "reference point) out per query, the 4-wide "
+                                           "tree, leaf ids and packed rows once"
                                            + (", leaf sub-box ids and reference boxes once"
-                                              if sub_guess else ""),
+                                              if sub_guess else "")
+                                           + (", the 64-byte leaf maps once" if lin_guess
+                                              else ""),
                          "compulsory_bytes_per_launch": compulsory,
                          "traffic_source": "DRAM bytes per launch measured live over the timed "
                                            "kernel loop (NVML GPM DRAM bandwidth utilisation x "
@@ -1204,9 +1344,10 @@ def main():
                          "dram_gbs": (traffic / (kern_ms * 1e-3) / 1e9) if traffic else None,
                          "dram_frac": (traffic / (kern_ms * 1e-3) / 1e9 / peak) if traffic
                          else None,
-                         "peak_source": peak_src, "kernel": "locate_persistent_kernel (staged)",
+                         "peak_source": peak_src, "kernel": "locate_persistent_kernel",
                          "kernel_ms": kern_ms, "kernel_guess": "sub-box centre" if sub_guess
-                         else "element centre", "launch_config": roof_loc.config.as_dict(),
+                         else "sub-box linear" if lin_guess else "element centre",
+                         "launch_config": roof_loc.config.as_dict(),
                          "cache_inclusive_bytes_per_query": bytes_q,
                          "cache_inclusive_gbs": n * bytes_q / (kern_ms * 1e-3) / 1e9,
                          "fp32": {"flops_per_query": flops_q, "achieved_tflops": achieved_tflops,
@@ -1229,6 +1370,7 @@ def main():
                       "note": "one thread per query in input order (reference launch pattern), "
                               "element-centre guess"},
             "batched_subref": batched_sub,
+            "batched_linear": batched_lin,
             "batched": {"value": batched_value, "ms_per_step": batched_ms,
                         "note": "Morton-ordered persistent kernel, element-centre guess"},
             "graph_small_batches": graph_small,

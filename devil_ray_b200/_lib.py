@@ -22,6 +22,7 @@ GUESS_ZERO = 0
 GUESS_ELEM_CENTER = 1
 GUESS_SUBREF_CENTER = 2
 GUESS_GIVEN = 3
+GUESS_SUBBOX_LINEAR = 4
 
 SHAPE_TENSOR = 0
 SHAPE_SIMPLEX = 1
@@ -40,7 +41,7 @@ class DrbBvh(C.Structure):
                 ("inner_nodes", C.c_void_p), ("leaf_nodes", C.c_void_p),
                 ("aabb_ids", C.c_void_p), ("ref_boxes", C.c_void_p),
                 ("bounds", C.c_float * 6), ("wide_nodes", C.c_void_p), ("n_wide", C.c_int),
-                ("wide_depth", C.c_int)]
+                ("wide_depth", C.c_int), ("leaf_maps", C.c_void_p)]
 
 
 class DrbNewtonOpts(C.Structure):
@@ -132,6 +133,8 @@ _SIGS = {
                                      C.c_void_p, DrbQueryStats, C.c_void_p]),
     "drb_query_order": (C.c_int, [C.POINTER(DrbBvh), C.c_void_p, C.c_int, C.c_void_p,
                                   C.c_void_p]),
+    "drb_bvh_leaf_maps": (C.c_int, [C.POINTER(DrbMesh), C.POINTER(DrbBvh), C.c_void_p,
+                                    C.c_void_p]),
     "drb_query_stage": (C.c_int, [C.POINTER(DrbBvh), C.c_void_p, C.c_int, C.c_void_p,
                                   C.c_void_p]),
     "drb_locate_staged": (C.c_int, [C.POINTER(DrbMesh), C.POINTER(DrbBvh), C.c_void_p, C.c_int,

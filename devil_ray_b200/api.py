@@ -68,6 +68,8 @@ class BVH:
         self.wide_nodes = None
         self.n_wide = 0
         self.wide_depth = 0
+        # optional per-leaf linear maps (drb_bvh_leaf_maps)
+        self.leaf_maps = None
 
     def desc(self) -> L.DrbBvh:
         d = L.DrbBvh()
@@ -81,7 +83,19 @@ class BVH:
         if self.wide_nodes is not None:
             d.wide_nodes = self.wide_nodes.data_ptr()
             d.n_wide, d.wide_depth = self.n_wide, self.wide_depth
+        if self.leaf_maps is not None:
+            d.leaf_maps = self.leaf_maps.data_ptr()
         return d
+
+    def build_leaf_maps(self, mesh: "UnstructuredMesh", stream=None):
+        """Per-leaf linear maps of the element maps at the reference
+        sub-box centres (drb_bvh_leaf_maps), for GUESS_SUBBOX_LINEAR."""
+        maps = torch.empty((self.n_leaf, 16), dtype=torch.float32,
+                           device=self.inner_nodes.device)
+        L.check(L.lib().drb_bvh_leaf_maps(C.byref(mesh.desc()), C.byref(self.desc()),
+                                          _ptr(maps), _stream(stream)), "drb_bvh_leaf_maps")
+        self.leaf_maps = maps
+        return self
 
     def widen(self, stream=None):
         """Build the 4-wide traversal tree of this BVH (same candidates in
@@ -256,7 +270,11 @@ class BatchedLocator:
         self.bvh = bvh  # None: the mesh's own BVH (with its wide tree)
 
     def _bvh(self, stream=None) -> BVH:
-        return self.bvh if self.bvh is not None else self.mesh.get_bvh(stream)
+        b = self.bvh if self.bvh is not None else self.mesh.get_bvh(stream)
+        if (self.guess_mode == L.GUESS_SUBBOX_LINEAR and b.leaf_maps is None
+                and self.mesh.shape == L.SHAPE_TENSOR and self.mesh.dim == 3):
+            b.build_leaf_maps(self.mesh, stream)
+        return b
 
     def tune(self, sample_points, stream=None):
         pts = _dev(sample_points, torch.float32, self.mesh.device).reshape(-1, 3)

@@ -1,8 +1,9 @@
 // Drives the C++ host interface's rendering classes the way a Devil Ray
 // user does: a Collection of several hex-mesh domains, a camera placed with
-// reset_to_bounds / elevate / azimuth, a boundary Surface with mesh lines and
-// a Volume handed to a Renderer, the framebuffer saved as PNG images, and a
-// Volume::save of one domain's partials.  Inputs and outputs are raw binary
+// reset_to_bounds / elevate / azimuth, a boundary Surface with mesh lines
+// and a Volume handed to a Renderer (the surface may cover a subset of the
+// domains, so that a volume in front of it shows), the framebuffer saved as
+// PNG images, and a Volume::save of one domain's partials.  Inputs and outputs are raw binary
 // files so the Python test (tests/test_cpp_facade_gpu.py) can compare each
 // result with the same calls made on the reference.
 //
@@ -12,7 +13,8 @@
 //                              float field[n_ctrl];
 //                              int32 w, h; float cam9[9], fov; int32 has_pads;
 //                              double pads[3]; float elevate, azimuth;
-//                              int32 surface, draw_mesh; float line_thickness;
+//                              int32 surface, surf_first, surf_count, draw_mesh;
+//                              float line_thickness;
 //                              int32 volume, samples, lighting, tf_samples;
 //                              int32 n_rgb; float rgb[4 n_rgb]; int32 n_alpha;
 //                              float alpha[2 n_alpha]
@@ -98,7 +100,8 @@ int main (int argc, char **argv)
     double pads[3];
     rd (f, pads, 3);
     const float elevate = rd1<float> (f), azimuth = rd1<float> (f);
-    const int32 surface = rd1<int32> (f), draw_mesh = rd1<int32> (f);
+    const int32 surface = rd1<int32> (f), surf_first = rd1<int32> (f);
+    const int32 surf_count = rd1<int32> (f), draw_mesh = rd1<int32> (f);
     const float thickness = rd1<float> (f);
     const int32 volume = rd1<int32> (f), samples = rd1<int32> (f), lighting = rd1<int32> (f);
     const int32 tf_samples = rd1<int32> (f);
@@ -134,15 +137,17 @@ int main (int argc, char **argv)
     std::shared_ptr<Volume> vol;
     if (surface)
     {
+      Collection part;
+      for (int32 d = surf_first; d < surf_first + surf_count; ++d) part.add_domain (col.domain (d));
       MeshBoundary boundary;
-      Collection faces = boundary.execute (col);
-      if (faces.local_size () != n_dom) throw std::runtime_error ("boundary domain count");
+      Collection faces = boundary.execute (part);
+      if (faces.local_size () != surf_count) throw std::runtime_error ("boundary domain count");
       auto surf = std::make_shared<Surface> (faces);
       surf->field ("f");
       surf->color_map ().color_table (table);
       surf->draw_mesh (draw_mesh != 0);
       if (draw_mesh) surf->line_thickness (thickness);
-      if (surf->num_domains () != n_dom) throw std::runtime_error ("surface domain count");
+      if (surf->num_domains () != surf_count) throw std::runtime_error ("surface domain count");
       renderer.add (surf);
     }
     if (volume)

@@ -78,10 +78,6 @@ struct LocateWorkspace
   int *order;
   RadixWorkspace radix;
   int *hist; // query_cell_count() cell counts of the query order
-  // optional staged query and result records (float4[n] each, 16-byte
-  // aligned); both NULL: the kernel reads the queries through `order`
-  float *staged = nullptr;
-  float *res = nullptr;
 };
 // Cells of the query order (counting sort over Morton cells).
 int query_cell_count ();

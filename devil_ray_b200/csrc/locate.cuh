@@ -136,6 +136,7 @@ struct LocateParams
   int guess_mode;
   const float *guess;
   const float4 *hull = nullptr; // tet hull planes (drb_tet_hull_planes) or NULL
+  const float4 *leaf_maps = nullptr; // per-leaf linear maps (drb_bvh_leaf_maps) or NULL
 };
 
 // Candidate filter of the batched locate (drb_tet_hull_planes): true when
@@ -312,14 +313,26 @@ DRB_D bool solve_in_smem_row (const LocateParams &lp, const float *row, const fl
 // Initial guess of a candidate leaf's Newton solve (drb_guess_mode).
 template <int S = kTensor>
 DRB_D void candidate_guess (const LocateParams &lp, int leaf, long long qi, bool first,
-                            float (&x)[3], bool &given)
+                            const float (&pt)[3], float (&x)[3], bool &given)
 {
   given = false;
   if (lp.guess_mode == DRB_GUESS_ZERO)
   {
     x[0] = x[1] = x[2] = 0.f;
   }
-  else if (lp.guess_mode == DRB_GUESS_SUBREF_CENTER && S == kSimplex)
+  else if (lp.guess_mode == DRB_GUESS_SUBBOX_LINEAR && S == kTensor && lp.leaf_maps)
+  {
+    // the element map linearised at the leaf's sub-box centre c:
+    // x = c + J(c)^-1 (p - X(c)); record (c, X(c), J^-1 row-major, 0)
+    const float4 *m = lp.leaf_maps + 4 * (size_t)leaf;
+    const float4 a = __ldg (m), b = __ldg (m + 1), c = __ldg (m + 2), d = __ldg (m + 3);
+    const float r0 = pt[0] - a.w, r1 = pt[1] - b.x, r2 = pt[2] - b.y;
+    x[0] = a.x + (b.z * r0 + b.w * r1 + c.x * r2);
+    x[1] = a.y + (c.y * r0 + c.z * r1 + c.w * r2);
+    x[2] = a.z + (d.x * r0 + d.y * r1 + d.z * r2);
+  }
+  else if ((lp.guess_mode == DRB_GUESS_SUBREF_CENTER || lp.guess_mode == DRB_GUESS_SUBBOX_LINEAR) &&
+           S == kSimplex)
   {
     // subref_center<Simplex> (data_model/subref.hpp:39-48): the origin
     // vertex plus the three axis vertices, times 1/4
@@ -333,7 +346,8 @@ DRB_D void candidate_guess (const LocateParams &lp, int leaf, long long qi, bool
       x[d] = __fmul_rn (sum, 0.25f);
     }
   }
-  else if (lp.guess_mode == DRB_GUESS_SUBREF_CENTER && S == kTri2D)
+  else if ((lp.guess_mode == DRB_GUESS_SUBREF_CENTER || lp.guess_mode == DRB_GUESS_SUBBOX_LINEAR) &&
+           S == kTri2D)
   {
     // subref_center<Simplex> in 2D: origin, then the axis vertices, times 1/3
     const float *rb = lp.ref_boxes + 6 * (size_t)__ldg (lp.aabb_ids + leaf);
@@ -342,7 +356,8 @@ DRB_D void candidate_guess (const LocateParams &lp, int leaf, long long qi, bool
       x[d] = __fmul_rn (__fadd_rn (__fadd_rn (rb[4 + d], rb[d]), rb[2 + d]), (float)(1.0 / 3));
     x[2] = 0.f;
   }
-  else if (lp.guess_mode == DRB_GUESS_SUBREF_CENTER && S == kQuad2D)
+  else if ((lp.guess_mode == DRB_GUESS_SUBREF_CENTER || lp.guess_mode == DRB_GUESS_SUBBOX_LINEAR) &&
+           S == kQuad2D)
   {
     // SubRef<2,Tensor>: low (u, v), then high (u, v)
     const float *rb = lp.ref_boxes + 4 * (size_t)__ldg (lp.aabb_ids + leaf);
@@ -350,7 +365,7 @@ DRB_D void candidate_guess (const LocateParams &lp, int leaf, long long qi, bool
     x[1] = (rb[1] + rb[3]) * 0.5f;
     x[2] = 0.f;
   }
-  else if (lp.guess_mode == DRB_GUESS_SUBREF_CENTER)
+  else if (lp.guess_mode == DRB_GUESS_SUBREF_CENTER || lp.guess_mode == DRB_GUESS_SUBBOX_LINEAR)
   {
     const float *rb = lp.ref_boxes + 6 * (size_t)__ldg (lp.aabb_ids + leaf);
 #pragma unroll
@@ -369,17 +384,20 @@ DRB_D void candidate_guess (const LocateParams &lp, int leaf, long long qi, bool
 }
 
 // Newton in one candidate element with the guess-mode fallback: a given
-// guess that does not converge is retried from the element centre.
+// guess whose solve does not converge within the step budget is retried
+// from the element centre.  A guessed solve that converged (it stopped
+// before the budget) to a point outside the element has shown that the
+// point is not in it, so it is not retried.
 template <int P, bool REG = (P <= 2), int S = kTensor>
 DRB_D bool solve_candidate (const LocateParams &lp, int leaf, int el, long long qi, bool first,
                             const float (&pt)[3], float (&x)[3], int &iters, LU3 &lu)
 {
   bool given;
-  candidate_guess<S> (lp, leaf, qi, first, x, given);
+  candidate_guess<S> (lp, leaf, qi, first, pt, x, given);
   int steps = 0;
   bool found = solve_in_element<P, REG, S> (lp, el, pt, x, steps, lu);
   iters += steps;
-  if (!found && given)
+  if (!found && given && steps >= lp.max_steps)
   {
     x[0] = x[1] = x[2] = shape_centre<S> ();
     found = solve_in_element<P, REG, S> (lp, el, pt, x, steps, lu);
@@ -402,11 +420,11 @@ DRB_D bool solve_candidate_smem (const LocateParams &lp, int leaf, const float *
                                  bool first, const float (&pt)[3], float (&x)[3], int &iters)
 {
   bool given;
-  candidate_guess<kTensor> (lp, leaf, qi, first, x, given);
+  candidate_guess<kTensor> (lp, leaf, qi, first, pt, x, given);
   int steps = 0;
   bool found = solve_in_smem_row<P> (lp, row, pt, x, steps);
   iters += steps;
-  if (!found && given)
+  if (!found && given && steps >= lp.max_steps)
   {
     x[0] = x[1] = x[2] = 0.5f;
     found = solve_in_smem_row<P> (lp, row, pt, x, steps);

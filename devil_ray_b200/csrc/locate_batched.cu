@@ -51,6 +51,34 @@ int cell_bits (int n)
   return bits;
 }
 
+// Grid of the query order: origin and inverse extents of the BVH bounds,
+// bits per axis.
+struct CellFrame
+{
+  float lo[3], sc[3];
+  int bits;
+};
+
+// Morton code (x in the lowest bit) of the cell of a point; NaN queries go
+// to cell 0.
+DRB_D unsigned point_cell (float px, float py, float pz, const CellFrame &f)
+{
+  const float p[3] = { px, py, pz };
+  unsigned e[3];
+#pragma unroll
+  for (int k = 0; k < 3; ++k)
+  {
+    float t = (p[k] - f.lo[k]) * f.sc[k];
+    t = fminf (fmaxf (t * (float)(1 << f.bits), 0.f), (float)((1 << f.bits) - 1));
+    unsigned x = (t == t) ? (unsigned)t : 0u;
+    x = (x | (x << 8)) & 0x0300F00Fu;
+    x = (x | (x << 4)) & 0x030C30C3u;
+    x = (x | (x << 2)) & 0x09249249u;
+    e[k] = x;
+  }
+  return (e[2] << 2) | (e[1] << 1) | e[0];
+}
+
 __global__ void cell_count_kernel (const float *__restrict__ pts, int n, float x0, float y0,
                                    float z0, float sx, float sy, float sz,
                                    int bits, unsigned *__restrict__ cell_of,
@@ -58,21 +86,8 @@ __global__ void cell_count_kernel (const float *__restrict__ pts, int n, float x
 {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= n) return;
-  const float lo[3] = { x0, y0, z0 };
-  const float sc[3] = { sx, sy, sz };
-  unsigned e[3];
-#pragma unroll
-  for (int k = 0; k < 3; ++k)
-  {
-    float t = (pts[3 * (size_t)i + k] - lo[k]) * sc[k];
-    t = fminf (fmaxf (t * (float)(1 << bits), 0.f), (float)((1 << bits) - 1));
-    unsigned x = (t == t) ? (unsigned)t : 0u; // NaN queries go to cell 0
-    x = (x | (x << 8)) & 0x0300F00Fu;
-    x = (x | (x << 4)) & 0x030C30C3u;
-    x = (x | (x << 2)) & 0x09249249u;
-    e[k] = x;
-  }
-  const unsigned c = (e[2] << 2) | (e[1] << 1) | e[0];
+  const CellFrame f{ { x0, y0, z0 }, { sx, sy, sz }, bits };
+  const unsigned c = point_cell (pts[3 * (size_t)i], pts[3 * (size_t)i + 1], pts[3 * (size_t)i + 2], f);
   cell_of[i] = c;
   rank[i] = atomicAdd (hist + c, 1);
 }
@@ -85,14 +100,16 @@ __global__ void cell_scatter_kernel (const unsigned *__restrict__ cell_of, const
   order[__ldg (offset + cell_of[i]) + rank[i]] = i;
 }
 
-// Query records in processing order, (x, y, z, input index as int bits), so
-// the locate kernel reads its queries as consecutive 16-byte records.  They
-// are gathered through the order (random reads, coalesced writes): a scatter
-// of the records themselves would write 16 bytes at random into an array
-// larger than L2, a read-modify-write of a DRAM sector per query, whereas the
-// index scatter before it writes 4 bytes into an array that stays in L2.
+// ------------------------------------------------------- staged queries --
+//
+// Query records in processing order, (x, y, z, input index as int bits), for
+// the staged modes (drb_locate_config.sort_queries 2 and 3): the locate
+// kernel then reads its queries as consecutive 16-byte records.  They are
+// gathered through the index order (random reads, coalesced writes);
+// scattering the records themselves would write 16 bytes at random into an
+// array larger than L2, a DRAM read-modify-write per record.
 __global__ void stage_gather_kernel (const float *__restrict__ pts, const int *__restrict__ order,
-                                     int n, float4 *__restrict__ staged)
+                                     int n, float4 *__restrict__ staged, int *__restrict__ pos_of)
 {
   const int k = blockIdx.x * blockDim.x + threadIdx.x;
   if (k >= n) return;
@@ -100,18 +117,17 @@ __global__ void stage_gather_kernel (const float *__restrict__ pts, const int *_
   const float x = __ldg (pts + 3 * (size_t)i), y = __ldg (pts + 3 * (size_t)i + 1),
               z = __ldg (pts + 3 * (size_t)i + 2);
   staged[k] = make_float4 (x, y, z, __int_as_float (i));
+  if (pos_of) pos_of[i] = k;
 }
 
 // Results back to input order: query i's record (cell as int bits, then the
-// reference point) sits at its processing position offset[cell] + rank.
-// Reads of cell_of, rank and the outputs' writes run in input order.
-__global__ void unstage_kernel (const unsigned *__restrict__ cell_of, const int *__restrict__ rank,
-                                const int *__restrict__ offset, const float4 *__restrict__ res, int n,
+// reference point) sits at its processing position pos_of[i].
+__global__ void unstage_kernel (const int *__restrict__ pos_of, const float4 *__restrict__ res, int n,
                                 int *__restrict__ cell, float *__restrict__ ref)
 {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= n) return;
-  const float4 r = __ldg (res + __ldg (offset + cell_of[i]) + rank[i]);
+  const float4 r = __ldg (res + __ldg (pos_of + i));
   cell[i] = __float_as_int (r.x);
   ref[3 * (size_t)i] = r.y;
   ref[3 * (size_t)i + 1] = r.z;
@@ -164,21 +180,22 @@ int cell_order (const drb_bvh *bvh, const float *pts, int n, int *order, unsigne
   return check_launch ("cell_scatter_kernel");
 }
 
-// The queries staged in processing order (buffers as cell_order's, plus
-// the order itself).
+// The queries staged in processing order: staged[k] = (x, y, z, input
+// index bits) of the k-th query in Morton-cell order (the order inside a
+// cell is unspecified); order, cell_of, rank, hist and scan_tmp as
+// cell_order's; pos_of (optional): each query's processing position.
 int cell_stage (const drb_bvh *bvh, const float *pts, int n, float4 *staged, int *order,
-                unsigned *cell_of, int *rank, int *hist, int *scan_tmp, cudaStream_t s)
+                unsigned *cell_of, int *rank, int *hist, int *scan_tmp, int *pos_of, cudaStream_t s)
 {
   int st = cell_order (bvh, pts, n, order, cell_of, rank, hist, scan_tmp, s);
   if (st) return st;
-  stage_gather_kernel<<<div_up (n, 256), 256, 0, s>>> (pts, order, n, staged);
+  stage_gather_kernel<<<div_up (n, 256), 256, 0, s>>> (pts, order, n, staged, pos_of);
   return check_launch ("stage_gather_kernel");
 }
 
-int unstage (const unsigned *cell_of, const int *rank, const int *hist, const float4 *res, int n,
-             int *cell, float *ref, cudaStream_t s)
+int unstage (const int *pos_of, const float4 *res, int n, int *cell, float *ref, cudaStream_t s)
 {
-  unstage_kernel<<<div_up (n, 256), 256, 0, s>>> (cell_of, rank, hist, res, n, cell, ref);
+  unstage_kernel<<<div_up (n, 256), 256, 0, s>>> (pos_of, res, n, cell, ref);
   return check_launch ("unstage_kernel");
 }
 
@@ -237,7 +254,8 @@ __global__ void locate_persistent_kernel (LocateParams lp, const float *__restri
   // 20 tet sub-boxes of 3.6 distinct tets), those of a hex barely (1.3
   // boxes of 1.04 hexes), where the check would only cost registers.
   constexpr bool kSkipRepeats = (S == kSimplex || S == kTri2D);
-  const bool leaf_free_guess = kSkipRepeats && lp.guess_mode != DRB_GUESS_SUBREF_CENTER;
+  const bool leaf_free_guess = kSkipRepeats && lp.guess_mode != DRB_GUESS_SUBREF_CENTER &&
+                               lp.guess_mode != DRB_GUESS_SUBBOX_LINEAR;
   int failed0 = -1, failed1 = -1, failed2 = -1;
 
   while (true)
@@ -515,6 +533,8 @@ LocateParams make_params (const drb_mesh *mesh, const drb_bvh *bvh, const drb_ne
   lp.guess = opts->guess;
   lp.hull = (mesh->shape == DRB_SHAPE_SIMPLEX && mesh->dim == 3) ? (const float4 *)mesh->hull_planes
                                                                    : nullptr;
+  lp.leaf_maps = (mesh->shape == DRB_SHAPE_TENSOR && mesh->dim == 3) ? (const float4 *)bvh->leaf_maps
+                                                                     : nullptr;
   return lp;
 }
 
@@ -620,24 +640,26 @@ int locate_staged_launch (const drb_mesh *mesh, const drb_bvh *bvh, const float4
 }
 
 // Sorted, staged batch over caller buffers: stage the queries in Morton-cell
-// order and locate them; with res set (sort_queries == 2) the results are
+// order and locate them; with res set (sort_queries 3) the results are
 // staged too and put back in input order by a separate pass.
 int locate_staged_batch (const drb_mesh *mesh, const drb_bvh *bvh, const float *pts, int n,
                          const drb_newton_opts *opts, const drb_locate_config &cfg, int *order,
-                         unsigned *cell_of, int *rank, int *hist, int *scan_tmp, int *head,
-                         float4 *staged, float4 *res, int *cell, float *ref, drb_query_stats stats,
-                         cudaStream_t s)
+                         unsigned *cell_of, int *rank, int *hist, int *scan_tmp, int *pos_of,
+                         int *head, float4 *staged, float4 *res, int *cell, float *ref,
+                         drb_query_stats stats, cudaStream_t s)
 {
-  int st = cell_stage (bvh, pts, n, staged, order, cell_of, rank, hist, scan_tmp, s);
+  int st = cell_stage (bvh, pts, n, staged, order, cell_of, rank, hist, scan_tmp,
+                       res ? pos_of : nullptr, s);
   if (st) return st;
   st = locate_staged_launch (mesh, bvh, staged, n, opts, cfg, head, res, cell, ref, stats, s);
   if (st || !res) return st;
-  return unstage (cell_of, rank, hist, res, n, cell, ref, s);
+  return unstage (pos_of, res, n, cell, ref, s);
 }
 
-// Result staging of a query order mode (drb_locate_config.sort_queries).
-constexpr int kSortStaged = 1;        // query records staged, results in place
-constexpr int kSortStagedResults = 2; // results staged too, put back in a pass
+// Query order modes (drb_locate_config.sort_queries).
+constexpr int kSortIndexed = 1;       // Morton order; queries read through the order
+constexpr int kSortStaged = 2;        // query records staged, results in place
+constexpr int kSortStagedResults = 3; // results staged too, put back in a pass
 
 int locate_batched_impl (const drb_mesh *mesh, const drb_bvh *bvh, const float *pts, int n,
                          const drb_newton_opts *opts, const drb_locate_config *cfg_in,
@@ -651,11 +673,11 @@ int locate_batched_impl (const drb_mesh *mesh, const drb_bvh *bvh, const float *
   if ((st = check_config (cfg))) return st;
   Scratch scr (s);
   int *head = scr.alloc<int> (1);
-  if (!order_in && cfg.sort_queries)
+  if (!order_in && cfg.sort_queries >= kSortStaged)
   {
     // staged: query records read in processing order; results written in
-    // place, or staged as well when asked for (not with given guesses,
-    // which are indexed by the input order)
+    // place, or staged as well (not with given guesses, which are indexed
+    // by the input order)
     const bool stage_res = cfg.sort_queries == kSortStagedResults &&
                            opts->guess_mode != DRB_GUESS_GIVEN;
     int *ord = scr.alloc<int> (n);
@@ -665,9 +687,10 @@ int locate_batched_impl (const drb_mesh *mesh, const drb_bvh *bvh, const float *
     int *tmp = scr.alloc<int> (scan_ws_ints (kCells));
     float4 *staged = scr.alloc<float4> (n);
     float4 *res = stage_res ? scr.alloc<float4> (n) : nullptr;
+    int *pos_of = stage_res ? scr.alloc<int> (n) : nullptr;
     if (scr.err != cudaSuccess) return status_from (scr.err);
     return locate_staged_batch (mesh, bvh, pts, n, opts, cfg, ord, cell_of, rank, hist, tmp,
-                                head, staged, res, cell, ref, stats, s);
+                                pos_of, head, staged, res, cell, ref, stats, s);
   }
   const int *ord = order_in;
   if (!ord && cfg.sort_queries)
@@ -687,10 +710,8 @@ int locate_batched_impl (const drb_mesh *mesh, const drb_bvh *bvh, const float *
                             cfg.chunk, head, cell, ref, stats);
 }
 
-// Same as locate_batched_impl with sorting, but over caller-provided
-// workspace.  With ws.staged set the queries are staged like
-// locate_batched_impl's (the results too when sort_queries asks for it and
-// ws.res is set); otherwise the kernel reads them through ws.order.
+// Same as locate_batched_impl with sorting (queries read through the index
+// order), but over caller-provided workspace.
 int locate_batched_ws (const drb_mesh *mesh, const drb_bvh *bvh, const float *pts, int n,
                        const drb_newton_opts *opts, const drb_locate_config *cfg_in,
                        const LocateWorkspace &ws, int *cell, float *ref, drb_query_stats stats,
@@ -701,16 +722,6 @@ int locate_batched_ws (const drb_mesh *mesh, const drb_bvh *bvh, const float *pt
   if (n == 0) return DRB_OK;
   const drb_locate_config cfg = cfg_in ? *cfg_in : default_config (mesh->order);
   if ((st = check_config (cfg))) return st;
-  if (cfg.sort_queries && ws.staged)
-  {
-    const bool stage_res = cfg.sort_queries == kSortStagedResults && ws.res &&
-                           opts->guess_mode != DRB_GUESS_GIVEN;
-    return locate_staged_batch (mesh, bvh, pts, n, opts, cfg, ws.order, ws.codes, ws.iota,
-                                ws.hist, ws.radix.scan_tmp, ws.head,
-                                reinterpret_cast<float4 *> (ws.staged),
-                                stage_res ? reinterpret_cast<float4 *> (ws.res) : nullptr, cell,
-                                ref, stats, s);
-  }
   const int *ord = nullptr;
   if (cfg.sort_queries)
   {
@@ -789,7 +800,7 @@ extern "C" int drb_query_stage (const drb_bvh *bvh, const float *pts, int n, flo
   int *tmp = scr.alloc<int> (scan_ws_ints (kCells));
   if (scr.err != cudaSuccess) return status_from (scr.err);
   return cell_stage (bvh, pts, n, reinterpret_cast<float4 *> (staged), ord, cell_of, rank, hist,
-                     tmp, s);
+                     tmp, nullptr, s);
 }
 
 extern "C" int drb_locate_staged (const drb_mesh *mesh, const drb_bvh *bvh, const float *staged,
@@ -839,19 +850,13 @@ extern "C" int drb_locate_tune (const drb_mesh *mesh, const drb_bvh *bvh, const 
   }
   cudaStream_t s = (cudaStream_t)stream;
   Scratch scr (s);
-  // the kernel as drb_locate_batched runs it: on query records staged in
-  // Morton-cell order once, results written in place
+  // the kernel as drb_locate_batched runs it by default: the sample in
+  // Morton-cell order once, read through that order
+  int *ord = scr.alloc<int> (n);
   int *cell = scr.alloc<int> (n);
   float *ref = scr.alloc<float> ((size_t)3 * n);
-  float4 *srec = scr.alloc<float4> (n);
-  int *head = scr.alloc<int> (1);
-  int *ord = scr.alloc<int> (n);
-  unsigned *cell_of = scr.alloc<unsigned> (n);
-  int *rank = scr.alloc<int> (n);
-  int *hist = scr.alloc<int> (kCells);
-  int *tmp = scr.alloc<int> (scan_ws_ints (kCells));
   if (scr.err != cudaSuccess) return status_from (scr.err);
-  st = cell_stage (bvh, pts, n, srec, ord, cell_of, rank, hist, tmp, s);
+  st = query_morton_order (bvh, pts, n, ord, s);
   if (st) return st;
   const int blocks[] = { 64, 128, 256 };
   const int per_sm[] = { 0, 4, 2 };
@@ -878,8 +883,8 @@ extern "C" int drb_locate_tune (const drb_mesh *mesh, const drb_bvh *bvh, const 
         for (int rep = 0; rep < 2 && st == DRB_OK; ++rep)
         {
           cudaEventRecord (e0, s);
-          st = locate_staged_launch (mesh, bvh, srec, n, opts, cfg, head, nullptr, cell, ref,
-                                     drb_query_stats{ nullptr, nullptr, nullptr }, s);
+          st = locate_batched_impl (mesh, bvh, pts, n, opts, &cfg, ord, cell, ref,
+                                    drb_query_stats{ nullptr, nullptr, nullptr }, s);
           cudaEventRecord (e1, s);
           cudaEventSynchronize (e1);
           cudaEventElapsedTime (&t, e0, e1);

@@ -244,6 +244,7 @@ extern "C" int drb_locate_hinted (const drb_mesh *mesh, const drb_bvh *bvh, cons
   lp.max_steps = opts->max_steps;
   lp.guess_mode = opts->guess_mode;
   lp.guess = opts->guess;
+  lp.leaf_maps = (const float4 *)bvh->leaf_maps;
   int nb = 0;
   const bool reg = cfg.reg_elements == 1 && mesh->order <= 2; // the register row mode
   const bool wide = lp.wide != nullptr;

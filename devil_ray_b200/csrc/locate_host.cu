@@ -44,13 +44,12 @@ bool open_lanes (Lane (&lane)[kLanes], int chunk, cudaEvent_t start, cudaError_t
     if (e == cudaSuccess) e = cudaEventCreateWithFlags (&lane[l].ready, cudaEventDisableTiming);
     // work queued on the caller's stream before this call comes first
     if (e == cudaSuccess) e = cudaStreamWaitEvent (lane[l].s, start, 0);
-    void *p[11] = {};
-    const size_t bytes[11] = { 3 * q * sizeof (float), q * sizeof (int), 3 * q * sizeof (float),
-                               sizeof (int), q * sizeof (unsigned), q * sizeof (int),
-                               q * sizeof (int), sizeof (int) * (size_t)cells,
-                               sizeof (int) * (size_t)scan_ints, 4 * q * sizeof (float),
-                               4 * q * sizeof (float) };
-    for (int b = 0; b < 11 && e == cudaSuccess; ++b) e = cudaMallocAsync (&p[b], bytes[b], lane[l].s);
+    void *p[9] = {};
+    const size_t bytes[9] = { 3 * q * sizeof (float), q * sizeof (int), 3 * q * sizeof (float),
+                              sizeof (int), q * sizeof (unsigned), q * sizeof (int),
+                              q * sizeof (int), sizeof (int) * (size_t)cells,
+                              sizeof (int) * (size_t)scan_ints };
+    for (int b = 0; b < 9 && e == cudaSuccess; ++b) e = cudaMallocAsync (&p[b], bytes[b], lane[l].s);
     lane[l].pts = (float *)p[0];
     lane[l].cell = (int *)p[1];
     lane[l].ref = (float *)p[2];
@@ -60,8 +59,6 @@ bool open_lanes (Lane (&lane)[kLanes], int chunk, cudaEvent_t start, cudaError_t
     lane[l].ws.order = (int *)p[6];
     lane[l].ws.hist = (int *)p[7];
     lane[l].ws.radix.scan_tmp = (int *)p[8];
-    lane[l].ws.staged = (float *)p[9];
-    lane[l].ws.res = (float *)p[10];
   }
   if (e != cudaSuccess) set_last_error (cudaGetErrorString (e));
   return e == cudaSuccess;
@@ -74,9 +71,9 @@ int close_lanes (Lane (&lane)[kLanes], cudaStream_t caller, int st)
   for (int l = 0; l < kLanes; ++l)
   {
     if (!lane[l].s) continue;
-    void *bufs[11] = { lane[l].pts, lane[l].cell, lane[l].ref, lane[l].ws.head, lane[l].ws.codes,
-                       lane[l].ws.iota, lane[l].ws.order, lane[l].ws.hist,
-                       lane[l].ws.radix.scan_tmp, lane[l].ws.staged, lane[l].ws.res };
+    void *bufs[9] = { lane[l].pts, lane[l].cell, lane[l].ref, lane[l].ws.head, lane[l].ws.codes,
+                      lane[l].ws.iota, lane[l].ws.order, lane[l].ws.hist,
+                      lane[l].ws.radix.scan_tmp };
     for (void *b : bufs)
       if (b) cudaFreeAsync (b, lane[l].s);
     if (lane[l].ready)

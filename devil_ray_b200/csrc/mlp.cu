@@ -1,6 +1,7 @@
 // Learned initial guess for the Newton inversion: a small MLP
-// (84 -> 128 -> 128 -> 3, GELU) mapping an order-2 hex element's 27 control
-// points plus a physical point to a reference-space guess.  No counterpart
+// (3 (P+1)^3 + 3 -> 128 -> 128 -> 3, GELU) mapping an order-P hex element's
+// control points plus a physical point to a reference-space guess: 84
+// inputs at order 2 (27 control points), 195 at order 3 (64).  No counterpart
 // in the reference; it feeds DRB_GUESS_GIVEN, with plain Newton from the
 // element centre as the fallback whenever the guessed solve fails.
 //
@@ -19,6 +20,8 @@
 // flag, frees its tensor memory and returns.
 #include <cuda_bf16.h>
 
+#include <cstdio>
+
 #include "bernstein.cuh"
 #include "drb_common.cuh"
 #include "drb_internal.h"
@@ -29,23 +32,44 @@ namespace drb
 namespace mlp
 {
 
-constexpr int kIn = 84;      // 27 control points x 3 + point x 3
-constexpr int kInPad = 96;   // K padded to a multiple of 16
 constexpr int kHid = 128;
 constexpr int kOut = 3;
-// parameter offsets in the fp32 master vector
-constexpr int kW1 = 0;
-constexpr int kB1 = kW1 + kHid * kIn;
-constexpr int kW2 = kB1 + kHid;
-constexpr int kB2 = kW2 + kHid * kHid;
-constexpr int kW3 = kB2 + kHid;
-constexpr int kB3 = kW3 + kOut * kHid;
-constexpr int kParams = kB3 + kOut;
-// bf16 operand copies: W1 [128 x 96], W2 [128 x 128], W2^T [128 x 128]
-constexpr int kBW1 = 0;
-constexpr int kBW2 = kBW1 + kHid * kInPad;
-constexpr int kBW2T = kBW2 + kHid * kHid;
-constexpr int kBf16 = kBW2T + kHid * kHid;
+
+// Dimensions and parameter layout of the network for order-P hex elements.
+// Inputs: the (P+1)^3 control points' 3 coordinates, then the point; K
+// padded to a multiple of 16 for the UMMA K steps.  Parameters, in one fp32
+// vector: W1 [128 x kIn], b1, W2 [128 x 128], b2, W3 [3 x 128], b3.  bf16
+// operand copies: W1 [128 x kInPad], W2, W2^T.
+template <int P> struct Net
+{
+  static constexpr int kNd = (P + 1) * (P + 1) * (P + 1);
+  static constexpr int kCoords = 3 * kNd;
+  static constexpr int kIn = kCoords + 3;
+  static constexpr int kInPad = (kIn + 15) / 16 * 16;
+  static constexpr int kW1 = 0;
+  static constexpr int kB1 = kW1 + kHid * kIn;
+  static constexpr int kW2 = kB1 + kHid;
+  static constexpr int kB2 = kW2 + kHid * kHid;
+  static constexpr int kW3 = kB2 + kHid;
+  static constexpr int kB3 = kW3 + kOut * kHid;
+  static constexpr int kParams = kB3 + kOut;
+  static constexpr int kBW1 = 0;
+  static constexpr int kBW2 = kBW1 + kHid * kInPad;
+  static constexpr int kBW2T = kBW2 + kHid * kHid;
+  static constexpr int kBf16 = kBW2T + kHid * kHid;
+  // packed geometry rows: kCoords relative coordinates, then the origin
+  static constexpr int kRowF4 = packed_stride (kNd, 3) / 4;
+  // activation tile width: the layer-1 input, then the layer-2 input in
+  // the same bytes
+  static constexpr int kActW = kInPad > kHid ? kInPad : kHid;
+  // 128-row tiles in flight per CTA in the fused inference (shared memory:
+  // W1, W2 and one activation tile per group within 227 KB)
+  static constexpr int kGroups = kActW > kHid ? 2 : 4;
+};
+static_assert (Net<2>::kIn == 84 && Net<2>::kInPad == 96 && Net<3>::kIn == 195 &&
+               Net<3>::kInPad == 208, "network input widths");
+static_assert (packed_origin (27) == 81 && packed_origin (64) == 192,
+               "geometry rows: relative coordinates, then the origin");
 
 constexpr uint32_t kWaitTries = 1u << 22;
 
@@ -75,20 +99,17 @@ DRB_D float gelu_grad (float x)
 
 // Features of one (element, point) pair: control points and point relative
 // to the centre of the element's control-point box, scaled by its largest
-// half-extent.  27 x 3 control coordinates, then the point, then zeros.
-// The packed row holds 84 floats (81 coordinates relative to the first
-// control point O, then O), 16-byte aligned, so it is read as float4.
-constexpr int kRowF4 = 21;
-static_assert (packed_stride (27, 3) == 4 * kRowF4 && packed_origin (27) == 81,
-               "order-2 geometry rows: 81 relative coordinates, then the origin");
+// half-extent.  (P+1)^3 x 3 control coordinates, then the point, then zeros.
+// The packed row holds the relative coordinates, then the origin O, 16-byte
+// aligned, so it is read as float4.
 
 // Centre and inverse largest half-extent of the control-point box.
-DRB_D void pair_frame (const float *__restrict__ row, float (&c)[3], float &inv)
+template <int P> DRB_D void pair_frame (const float *__restrict__ row, float (&c)[3], float &inv)
 {
   const float4 *r4 = reinterpret_cast<const float4 *> (row);
   float mn[3] = { INFINITY, INFINITY, INFINITY }, mx[3] = { -INFINITY, -INFINITY, -INFINITY };
 #pragma unroll
-  for (int j = 0; j < kRowF4; ++j)
+  for (int j = 0; j < Net<P>::kRowF4; ++j)
   {
     const float4 v4 = __ldg (r4 + j);
     const float v[4] = { v4.x, v4.y, v4.z, v4.w };
@@ -96,7 +117,7 @@ DRB_D void pair_frame (const float *__restrict__ row, float (&c)[3], float &inv)
     for (int t = 0; t < 4; ++t)
     {
       const int q = 4 * j + t;
-      if (q < 81)
+      if (q < Net<P>::kCoords)
       {
         mn[q % 3] = fminf (mn[q % 3], v[t]);
         mx[q % 3] = fmaxf (mx[q % 3], v[t]);
@@ -113,39 +134,30 @@ DRB_D void pair_frame (const float *__restrict__ row, float (&c)[3], float &inv)
   inv = h > 0.f ? 1.f / h : 0.f;
 }
 
-// Features [8 k8, 8 k8 + 8) of one pair as eight packed bf16 (k8 < 12).
+// Features [8 k8, 8 k8 + 8) of one pair as eight packed bf16.  The point
+// enters in the row's frame, pt - O (O follows the coordinates in the row).
+template <int P>
 DRB_D uint4 pair_features8 (const float *__restrict__ row, const float (&pt)[3], const float (&c)[3],
                             float inv, int k8)
 {
-  float v[8];
-  if (k8 < 10)
-  {
-    const float4 a = __ldg (reinterpret_cast<const float4 *> (row) + 2 * k8);
-    const float4 b = __ldg (reinterpret_cast<const float4 *> (row) + 2 * k8 + 1);
-    v[0] = a.x; v[1] = a.y; v[2] = a.z; v[3] = a.w;
-    v[4] = b.x; v[5] = b.y; v[6] = b.z; v[7] = b.w;
-  }
-  else if (k8 == 10)
-  {
-    // floats 80..83: the last coordinate, then the row's origin O; the
-    // point enters in the row's frame, pt - O
-    const float4 a = __ldg (reinterpret_cast<const float4 *> (row) + 20);
-    v[0] = a.x;
-    v[1] = __fsub_rn (pt[0], a.y);
-    v[2] = __fsub_rn (pt[1], a.z);
-    v[3] = __fsub_rn (pt[2], a.w);
-    v[4] = v[5] = v[6] = v[7] = 0.f;
-  }
-  else
-  {
+  constexpr int RF = 4 * Net<P>::kRowF4;
+  const int f0 = 8 * k8;
+  const float4 z4 = make_float4 (0.f, 0.f, 0.f, 0.f);
+  const float4 a = f0 < RF ? __ldg (reinterpret_cast<const float4 *> (row) + 2 * k8) : z4;
+  const float4 b = f0 + 4 < RF ? __ldg (reinterpret_cast<const float4 *> (row) + 2 * k8 + 1) : z4;
+  float v[8] = { a.x, a.y, a.z, a.w, b.x, b.y, b.z, b.w };
 #pragma unroll
-    for (int t = 0; t < 8; ++t) v[t] = 0.f;
+  for (int t = 0; t < 8; ++t)
+  {
+    const int q = f0 + t;
+    if (q >= Net<P>::kIn) v[t] = 0.f;
+    else if (q >= Net<P>::kCoords) v[t] = __fsub_rn (pt[q - Net<P>::kCoords], v[t]);
   }
 #pragma unroll
   for (int t = 0; t < 8; ++t)
   {
-    const int q = 8 * k8 + t;
-    if (q < 84) v[t] = (v[t] - c[q % 3]) * inv;
+    const int q = f0 + t;
+    if (q < Net<P>::kIn) v[t] = (v[t] - c[q % 3]) * inv;
   }
   uint4 out;
   __nv_bfloat162 p0 = __floats2bfloat162_rn (v[0], v[1]), p1 = __floats2bfloat162_rn (v[2], v[3]);
@@ -159,44 +171,48 @@ DRB_D uint4 pair_features8 (const float *__restrict__ row, const float (&pt)[3],
 
 // ------------------------------------------------------------ prepare --
 
+template <int P>
 __global__ void prepare_kernel (const float *__restrict__ p, __nv_bfloat16 *__restrict__ wb)
 {
+  using N = Net<P>;
   const int t = blockIdx.x * blockDim.x + threadIdx.x;
-  if (t < kHid * kInPad)
+  if (t < kHid * N::kInPad)
   {
-    const int r = t / kInPad, k = t - r * kInPad;
-    wb[kBW1 + t] = __float2bfloat16_rn (k < kIn ? p[kW1 + r * kIn + k] : 0.f);
+    const int r = t / N::kInPad, k = t - r * N::kInPad;
+    wb[N::kBW1 + t] = __float2bfloat16_rn (k < N::kIn ? p[N::kW1 + r * N::kIn + k] : 0.f);
   }
   if (t < kHid * kHid)
   {
     const int r = t / kHid, k = t - r * kHid;
-    wb[kBW2 + t] = __float2bfloat16_rn (p[kW2 + t]);
-    wb[kBW2T + t] = __float2bfloat16_rn (p[kW2 + k * kHid + r]);
+    wb[N::kBW2 + t] = __float2bfloat16_rn (p[N::kW2 + t]);
+    wb[N::kBW2T + t] = __float2bfloat16_rn (p[N::kW2 + k * kHid + r]);
   }
 }
 
 // ----------------------------------------------------------- features --
 
+template <int P>
 __global__ void features_kernel (const float *__restrict__ packed, int stride,
                                  const int *__restrict__ elem, const float *__restrict__ pts, int n,
                                  int n_pad, __nv_bfloat16 *__restrict__ X)
 {
+  using N = Net<P>;
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= n_pad) return;
   const int e = i < n ? elem[i] : -1;
-  uint4 *dst = reinterpret_cast<uint4 *> (X + (size_t)i * kInPad);
+  uint4 *dst = reinterpret_cast<uint4 *> (X + (size_t)i * N::kInPad);
   if (e < 0)
   {
 #pragma unroll
-    for (int k8 = 0; k8 < kInPad / 8; ++k8) dst[k8] = make_uint4 (0u, 0u, 0u, 0u);
+    for (int k8 = 0; k8 < N::kInPad / 8; ++k8) dst[k8] = make_uint4 (0u, 0u, 0u, 0u);
     return;
   }
   const float *row = packed + (size_t)e * stride;
   const float pt[3] = { pts[3 * (size_t)i], pts[3 * (size_t)i + 1], pts[3 * (size_t)i + 2] };
   float c[3], inv;
-  pair_frame (row, c, inv);
+  pair_frame<P> (row, c, inv);
 #pragma unroll
-  for (int k8 = 0; k8 < kInPad / 8; ++k8) dst[k8] = pair_features8 (row, pt, c, inv, k8);
+  for (int k8 = 0; k8 < N::kInPad / 8; ++k8) dst[k8] = pair_features8<P> (row, pt, c, inv, k8);
 }
 
 // --------------------------------------------------------------- GEMM --
@@ -206,7 +222,8 @@ enum Epilogue
   EPI_STORE = 0,     // C[r, c] = D (+ bias[c])                 fp32
   EPI_BIAS_GELU = 1, // Z[r, c] = D + bias[c], H = bf16(gelu(Z))
   EPI_GELU_GRAD = 2, // H[r, c] = bf16(D * gelu'(Z[r, c]))
-  EPI_ATOMIC = 3     // atomicAdd(C[r * ldc + c], D) for c < ncols
+  EPI_ATOMIC = 3,    // atomicAdd(C[r * ldc + c], D) for c < ncols
+  EPI_ATOMIC_T = 4   // atomicAdd(C[c * ldc + r], D) for r < ncols (transposed)
 };
 
 struct GemmArgs
@@ -317,8 +334,12 @@ __global__ void __launch_bounds__ (128) gemm_kernel (GemmArgs g)
         }
         else if (EPI == EPI_GELU_GRAD)
           g.H[(size_t)r * g.N + c] = __float2bfloat16_rn (d[j] * gelu_grad (g.Zin[(size_t)r * g.N + c]));
-        else if (c < g.ncols)
-          atomicAdd (g.C + (size_t)r * g.ldc + c, d[j]);
+        else if (EPI == EPI_ATOMIC)
+        {
+          if (c < g.ncols) atomicAdd (g.C + (size_t)r * g.ldc + c, d[j]);
+        }
+        else if (r < g.ncols)
+          atomicAdd (g.C + (size_t)c * g.ldc + r, d[j]);
       }
     }
   }
@@ -335,11 +356,13 @@ __global__ void __launch_bounds__ (128) gemm_kernel (GemmArgs g)
 // float4, the 3 dot products reduced by shuffles), then a thread per column
 // over the block's rows for dZ2 and the weight-gradient column sums, so the
 // block adds one partial per parameter to the global gradient.
+template <int P>
 __global__ void __launch_bounds__ (128)
 head_kernel (const float *__restrict__ p, const float *__restrict__ Z2, const float *__restrict__ target,
              const float *__restrict__ weight, int n, int n_pad, float inv_count, float *__restrict__ y_out,
              float *__restrict__ grad, __nv_bfloat16 *__restrict__ dZ2, float *__restrict__ loss)
 {
+  constexpr int kW3 = Net<P>::kW3, kB3 = Net<P>::kB3, kB2 = Net<P>::kB2;
   __shared__ float s_w3[kOut * kHid];
   __shared__ float s_dy[128][kOut];
   __shared__ float s_loss;
@@ -485,18 +508,23 @@ struct GuessArgs
   int *err;
 };
 
-// Fused inference keeps four 128-row tiles in flight per CTA, one per
-// warpgroup, with the bf16 weights resident once per CTA.  Each warpgroup
-// owns one activation tile (the 96-wide layer-1 input, then the 128-wide
-// layer-2 input in the same bytes) and 128 TMEM columns (D1, then D2 in the
-// same columns), and synchronises only with itself (named barrier 1 + g),
-// so one group's gathers and epilogues overlap the others' MMAs.
-constexpr int kGuessGroups = 4;
-constexpr int kGuessThreads = 128 * kGuessGroups;
-constexpr size_t kGuessW1 = (size_t)kHid * kInPad * 2;
-constexpr size_t kGuessW2 = (size_t)kHid * kHid * 2;
-constexpr size_t kGuessAct = (size_t)128 * kHid * 2;
-constexpr size_t kGuessSmem = kGuessW1 + kGuessW2 + kGuessGroups * kGuessAct;
+// Fused inference keeps Net<P>::kGroups 128-row tiles in flight per CTA
+// (four at orders 1-2, two at order 3, whose 208-wide layer-1 input needs
+// wider tiles), one per warpgroup, with the bf16 weights resident once per
+// CTA.  Each warpgroup owns one activation tile (the layer-1 input, then
+// the 128-wide layer-2 input in the same bytes) and 128 TMEM columns (D1,
+// then D2 in the same columns), and synchronises only with itself (named
+// barrier 1 + g), so one group's gathers and epilogues overlap the others'
+// MMAs.
+template <int P> constexpr size_t guess_w1_bytes () { return (size_t)kHid * Net<P>::kInPad * 2; }
+constexpr size_t guess_w2_bytes () { return (size_t)kHid * kHid * 2; }
+template <int P> constexpr size_t guess_act_bytes () { return (size_t)128 * Net<P>::kActW * 2; }
+template <int P> constexpr size_t guess_smem ()
+{
+  return guess_w1_bytes<P> () + guess_w2_bytes () + Net<P>::kGroups * guess_act_bytes<P> ();
+}
+static_assert (guess_smem<3> () <= 227 * 1024 && guess_smem<2> () <= 227 * 1024 &&
+               guess_smem<1> () <= 227 * 1024, "fused inference fits in shared memory");
 
 DRB_D void group_sync (int g)
 {
@@ -514,8 +542,16 @@ DRB_D bool group_and (int g, bool v)
   return r != 0;
 }
 
-__global__ void __launch_bounds__ (kGuessThreads, 1) mlp_guess_kernel (GuessArgs a)
+template <int P>
+__global__ void __launch_bounds__ (128 * Net<P>::kGroups, 1) mlp_guess_kernel (GuessArgs a)
 {
+  using N = Net<P>;
+  constexpr int kGuessGroups = N::kGroups;
+  constexpr int kGuessThreads = 128 * kGuessGroups;
+  constexpr int kInPad = N::kInPad;
+  constexpr size_t kGuessW1 = guess_w1_bytes<P> ();
+  constexpr size_t kGuessW2 = guess_w2_bytes ();
+  constexpr size_t kGuessAct = guess_act_bytes<P> ();
   extern __shared__ __align__ (1024) unsigned char smem[];
   unsigned char *sW1 = smem;                     // 128 x 96
   unsigned char *sW2 = sW1 + kGuessW1;           // 128 x 128
@@ -531,21 +567,21 @@ __global__ void __launch_bounds__ (kGuessThreads, 1) mlp_guess_kernel (GuessArgs
   {
     const int r = v / (kInPad / 8), j = v - r * (kInPad / 8);
     *reinterpret_cast<uint4 *> (sW1 + umma::tile_offset (r, 8 * j, kInPad)) =
-    *reinterpret_cast<const uint4 *> (a.wb + kBW1 + (size_t)r * kInPad + 8 * j);
+    *reinterpret_cast<const uint4 *> (a.wb + N::kBW1 + (size_t)r * kInPad + 8 * j);
   }
   for (int v = tid; v < kHid * (kHid / 8); v += kGuessThreads)
   {
     const int r = v / (kHid / 8), j = v - r * (kHid / 8);
     *reinterpret_cast<uint4 *> (sW2 + umma::tile_offset (r, 8 * j, kHid)) =
-    *reinterpret_cast<const uint4 *> (a.wb + kBW2 + (size_t)r * kHid + 8 * j);
+    *reinterpret_cast<const uint4 *> (a.wb + N::kBW2 + (size_t)r * kHid + 8 * j);
   }
   for (int q = tid; q < kHid; q += kGuessThreads)
   {
-    s_b1[q] = a.params[kB1 + q];
-    s_b2[q] = a.params[kB2 + q];
+    s_b1[q] = a.params[N::kB1 + q];
+    s_b2[q] = a.params[N::kB2 + q];
   }
-  for (int q = tid; q < kOut * kHid; q += kGuessThreads) s_w3[q] = a.params[kW3 + q];
-  if (tid < kOut) s_b3[tid] = a.params[kB3 + tid];
+  for (int q = tid; q < kOut * kHid; q += kGuessThreads) s_w3[q] = a.params[N::kW3 + q];
+  if (tid < kOut) s_b3[tid] = a.params[N::kB3 + tid];
   if (warp == 0) umma::tmem_alloc (&tmem_base, kGuessGroups * kHid);
   if (tid < kGuessGroups) umma::mbar_init (&mbar[tid], 1);
   umma::fence_before_sync ();
@@ -572,11 +608,11 @@ __global__ void __launch_bounds__ (kGuessThreads, 1) mlp_guess_kernel (GuessArgs
       pt[2] = __ldg (a.pts + 3 * (size_t)q + 2);
       const float *er = a.packed + (size_t)e * a.stride;
       float c[3], inv;
-      pair_frame (er, c, inv);
+      pair_frame<P> (er, c, inv);
 #pragma unroll
       for (int k8 = 0; k8 < kInPad / 8; ++k8)
         *reinterpret_cast<uint4 *> (sAct + umma::tile_offset (row, 8 * k8, kInPad)) =
-        pair_features8 (er, pt, c, inv, k8);
+        pair_features8<P> (er, pt, c, inv, k8);
     }
     else
     {
@@ -690,100 +726,90 @@ template <int EPI> int launch_gemm (const GemmArgs &g, cudaStream_t s)
 using namespace drb;
 using namespace drb::mlp;
 
-extern "C" int drb_mlp_param_count (void) { return kParams; }
-extern "C" int drb_mlp_bf16_count (void) { return kBf16; }
-
-extern "C" int drb_mlp_prepare (const float *params, void *wbf16, void *stream)
+namespace
 {
-  if (!params || !wbf16)
-  {
-    set_last_error ("mlp_prepare: bad arguments");
-    return DRB_ERR_INVALID_ARG;
-  }
-  prepare_kernel<<<div_up (kHid * kHid, 256), 256, 0, (cudaStream_t)stream>>> (
-  params, (__nv_bfloat16 *)wbf16);
+
+bool mlp_order_ok (int order)
+{
+  if (order >= 1 && order <= 3) return true;
+  set_last_error ("mlp: the network is defined for hex orders 1..3");
+  return false;
+}
+
+template <int P> int prepare_p (const float *params, void *wbf16, cudaStream_t s)
+{
+  const int n = kHid * (Net<P>::kInPad > kHid ? Net<P>::kInPad : kHid);
+  prepare_kernel<P><<<div_up (n, 256), 256, 0, s>>> (params, (__nv_bfloat16 *)wbf16);
   return check_launch ("prepare_kernel");
 }
 
-extern "C" int drb_mlp_features (const drb_mesh *mesh, const int *elem, const float *pts, int n,
-                                 int n_pad, void *X, void *stream)
+template <int P>
+int features_p (const drb_mesh *mesh, const int *elem, const float *pts, int n, int n_pad, void *X,
+                cudaStream_t s)
 {
-  if (!mesh || !mesh->packed || mesh->dim != 3 || mesh->order != 2 || mesh->ncomp != 3 ||
-      mesh->shape != DRB_SHAPE_TENSOR || n < 0 || n_pad < n || (n_pad > 0 && !X) ||
-      (n > 0 && (!elem || !pts)))
-  {
-    set_last_error ("mlp_features: needs a packed order-2 hex mesh and n <= n_pad");
-    return DRB_ERR_INVALID_ARG;
-  }
-  if (n_pad == 0) return DRB_OK;
-  features_kernel<<<div_up (n_pad, 128), 128, 0, (cudaStream_t)stream>>> (
-  mesh->packed, packed_stride (27, 3), elem, pts, n, n_pad, (__nv_bfloat16 *)X);
+  features_kernel<P><<<div_up (n_pad, 128), 128, 0, s>>> (
+  mesh->packed, packed_stride (Net<P>::kNd, 3), elem, pts, n, n_pad, (__nv_bfloat16 *)X);
   return check_launch ("features_kernel");
 }
 
-// Workspace of one training step over n_pad rows (multiple of 128):
-// Z1, Z2 fp32 [n_pad x 128]; H1, H2, dZ2, dZ1 bf16 [n_pad x 128];
-// transposes dZ2T, H1T, dZ1T bf16 [128 x n_pad], XT bf16 [96 x n_pad].
-extern "C" long long drb_mlp_workspace_bytes (int n_pad)
+template <int P> long long workspace_p (int n_pad)
 {
   const long long r = n_pad;
-  return r * kHid * 4 * 2 + r * kHid * 2 * 4 + r * kHid * 2 * 3 + r * kInPad * 2 + 4096;
+  return r * kHid * 4 * 2 + r * kHid * 2 * 4 + r * kHid * 2 * 3 + r * Net<P>::kInPad * 2 + 4096;
 }
 
-extern "C" int drb_mlp_forward (const float *params, const void *wbf16, const void *X, int n,
-                                int n_pad, float *y, void *workspace, int *err, void *stream)
+// The two layers of the forward pass into Z1/H1 and Z2/H2.
+template <int P>
+int forward_layers (const float *params, const __nv_bfloat16 *wb, const void *X, int n_pad,
+                    float *Z1, __nv_bfloat16 *H1, float *Z2, __nv_bfloat16 *H2, int *err,
+                    cudaStream_t s)
 {
-  if (!params || !wbf16 || !X || !y || !workspace || n < 0 || n_pad < n || (n_pad % 128))
-  {
-    set_last_error ("mlp_forward: bad arguments (n_pad must be a multiple of 128 and >= n)");
-    return DRB_ERR_INVALID_ARG;
-  }
-  if (n_pad == 0) return DRB_OK;
-  cudaStream_t s = (cudaStream_t)stream;
-  unsigned char *w = (unsigned char *)workspace;
-  float *Z1 = (float *)w;
-  float *Z2 = Z1 + (size_t)n_pad * kHid;
-  __nv_bfloat16 *H1 = (__nv_bfloat16 *)(Z2 + (size_t)n_pad * kHid);
-  __nv_bfloat16 *H2 = H1 + (size_t)n_pad * kHid;
-  const __nv_bfloat16 *wb = (const __nv_bfloat16 *)wbf16;
+  using N = Net<P>;
   GemmArgs g{};
   g.A = (const __nv_bfloat16 *)X;
-  g.B = wb + kBW1;
+  g.B = wb + N::kBW1;
   g.M = n_pad;
   g.N = kHid;
-  g.K = kInPad;
-  g.k_split = kInPad;
-  g.bias = params + kB1;
+  g.K = N::kInPad;
+  g.k_split = ((N::kInPad + kKC - 1) / kKC) * kKC;
+  g.bias = params + N::kB1;
   g.C = Z1;
   g.H = H1;
   g.err = err;
   int st = launch_gemm<EPI_BIAS_GELU> (g, s);
   if (st) return st;
   g.A = H1;
-  g.B = wb + kBW2;
+  g.B = wb + N::kBW2;
   g.K = kHid;
   g.k_split = kHid;
-  g.bias = params + kB2;
+  g.bias = params + N::kB2;
   g.C = Z2;
   g.H = H2;
-  if ((st = launch_gemm<EPI_BIAS_GELU> (g, s))) return st;
-  head_kernel<<<div_up (n_pad, 128), 128, 0, s>>> (params, Z2, nullptr, nullptr, n, n_pad, 0.f, y,
-                                                   nullptr, nullptr, nullptr);
+  return launch_gemm<EPI_BIAS_GELU> (g, s);
+}
+
+template <int P>
+int forward_p (const float *params, const void *wbf16, const void *X, int n, int n_pad, float *y,
+               void *workspace, int *err, cudaStream_t s)
+{
+  unsigned char *w = (unsigned char *)workspace;
+  float *Z1 = (float *)w;
+  float *Z2 = Z1 + (size_t)n_pad * kHid;
+  __nv_bfloat16 *H1 = (__nv_bfloat16 *)(Z2 + (size_t)n_pad * kHid);
+  __nv_bfloat16 *H2 = H1 + (size_t)n_pad * kHid;
+  int st = forward_layers<P> (params, (const __nv_bfloat16 *)wbf16, X, n_pad, Z1, H1, Z2, H2, err, s);
+  if (st) return st;
+  head_kernel<P><<<div_up (n_pad, 128), 128, 0, s>>> (params, Z2, nullptr, nullptr, n, n_pad, 0.f, y,
+                                                      nullptr, nullptr, nullptr);
   return check_launch ("head_kernel");
 }
 
-extern "C" int drb_mlp_train_step (const float *params, const void *wbf16, const void *X,
-                                   const float *target, const float *weight, int n, int n_pad,
-                                   float *grad, float *loss, void *workspace, int *err,
-                                   void *stream)
+template <int P>
+int train_step_p (const float *params, const void *wbf16, const void *X, const float *target,
+                  const float *weight, int n, int n_pad, float *grad, float *loss, void *workspace,
+                  int *err, cudaStream_t s)
 {
-  if (!params || !wbf16 || !X || !target || !grad || !workspace || n < 1 || n_pad < n ||
-      (n_pad % 128))
-  {
-    set_last_error ("mlp_train_step: bad arguments (n_pad must be a multiple of 128 and >= n)");
-    return DRB_ERR_INVALID_ARG;
-  }
-  cudaStream_t s = (cudaStream_t)stream;
+  using N = Net<P>;
   unsigned char *w = (unsigned char *)workspace;
   const size_t R = (size_t)n_pad;
   float *Z1 = (float *)w;
@@ -797,38 +823,18 @@ extern "C" int drb_mlp_train_step (const float *params, const void *wbf16, const
   __nv_bfloat16 *dZ1T = H1T + R * kHid;
   __nv_bfloat16 *XT = dZ1T + R * kHid;
   const __nv_bfloat16 *wb = (const __nv_bfloat16 *)wbf16;
-  cudaMemsetAsync (grad, 0, sizeof (float) * kParams, s);
+  cudaMemsetAsync (grad, 0, sizeof (float) * N::kParams, s);
   if (loss) cudaMemsetAsync (loss, 0, sizeof (float), s);
-  // forward
-  GemmArgs g{};
-  g.A = (const __nv_bfloat16 *)X;
-  g.B = wb + kBW1;
-  g.M = n_pad;
-  g.N = kHid;
-  g.K = kInPad;
-  g.k_split = kInPad;
-  g.bias = params + kB1;
-  g.C = Z1;
-  g.H = H1;
-  g.err = err;
-  int st = launch_gemm<EPI_BIAS_GELU> (g, s);
+  int st = forward_layers<P> (params, wb, X, n_pad, Z1, H1, Z2, H2, err, s);
   if (st) return st;
-  g.A = H1;
-  g.B = wb + kBW2;
-  g.K = kHid;
-  g.k_split = kHid;
-  g.bias = params + kB2;
-  g.C = Z2;
-  g.H = H2;
-  if ((st = launch_gemm<EPI_BIAS_GELU> (g, s))) return st;
   // head, loss, dW3, db3, dZ2, db2
-  head_kernel<<<div_up (n_pad, 128), 128, 0, s>>> (params, Z2, target, weight, n, n_pad,
-                                                   1.f / (float)n, nullptr, grad, dZ2, loss);
+  head_kernel<P><<<div_up (n_pad, 128), 128, 0, s>>> (params, Z2, target, weight, n, n_pad,
+                                                      1.f / (float)n, nullptr, grad, dZ2, loss);
   if ((st = check_launch ("head_kernel"))) return st;
   // dZ1 = (dZ2 W2) x gelu'(Z1): B operand is W2^T
   GemmArgs b{};
   b.A = dZ2;
-  b.B = wb + kBW2T;
+  b.B = wb + N::kBW2T;
   b.M = n_pad;
   b.N = kHid;
   b.K = kHid;
@@ -837,14 +843,15 @@ extern "C" int drb_mlp_train_step (const float *params, const void *wbf16, const
   b.H = dZ1;
   b.err = err;
   if ((st = launch_gemm<EPI_GELU_GRAD> (b, s))) return st;
-  colsum_kernel<<<min (div_up (n_pad, 2), 1024), 256, 0, s>>> (dZ1, n_pad, grad + kB1);
+  colsum_kernel<<<min (div_up (n_pad, 2), 1024), 256, 0, s>>> (dZ1, n_pad, grad + N::kB1);
   if ((st = check_launch ("colsum_kernel"))) return st;
   // transposes for the weight gradients (K = batch)
   dim3 tb (32, 8);
   transpose_kernel<<<dim3 (kHid / 32, div_up (n_pad, 32)), tb, 0, s>>> (dZ2, n_pad, kHid, dZ2T);
   transpose_kernel<<<dim3 (kHid / 32, div_up (n_pad, 32)), tb, 0, s>>> (H1, n_pad, kHid, H1T);
   transpose_kernel<<<dim3 (kHid / 32, div_up (n_pad, 32)), tb, 0, s>>> (dZ1, n_pad, kHid, dZ1T);
-  transpose_kernel<<<dim3 (kInPad / 32, div_up (n_pad, 32)), tb, 0, s>>> ((const __nv_bfloat16 *)X, n_pad, kInPad, XT);
+  transpose_kernel<<<dim3 (div_up (N::kInPad, 32), div_up (n_pad, 32)), tb, 0, s>>> (
+  (const __nv_bfloat16 *)X, n_pad, N::kInPad, XT);
   if ((st = check_launch ("transpose_kernel"))) return st;
   const int ksplit = n_pad <= 1024 ? ((n_pad + kKC - 1) / kKC) * kKC : 1024;
   // dW2 = dZ2^T H1
@@ -855,38 +862,180 @@ extern "C" int drb_mlp_train_step (const float *params, const void *wbf16, const
   d2.N = kHid;
   d2.K = n_pad;
   d2.k_split = ksplit;
-  d2.C = grad + kW2;
+  d2.C = grad + N::kW2;
   d2.ldc = kHid;
   d2.ncols = kHid;
   d2.err = err;
   if ((st = launch_gemm<EPI_ATOMIC> (d2, s))) return st;
-  // dW1 = dZ1^T X (first 84 of 96 columns)
   GemmArgs d1{};
-  d1.A = dZ1T;
-  d1.B = XT;
-  d1.M = kHid;
-  d1.N = kInPad;
   d1.K = n_pad;
   d1.k_split = ksplit;
-  d1.C = grad + kW1;
-  d1.ldc = kIn;
-  d1.ncols = kIn;
+  d1.C = grad + N::kW1;
+  d1.ldc = N::kIn;
+  d1.ncols = N::kIn;
   d1.err = err;
-  return launch_gemm<EPI_ATOMIC> (d1, s);
+  if (N::kInPad <= kGemmN)
+  {
+    // dW1 = dZ1^T X (the first kIn of kInPad columns)
+    d1.A = dZ1T;
+    d1.B = XT;
+    d1.M = kHid;
+    d1.N = N::kInPad;
+    return launch_gemm<EPI_ATOMIC> (d1, s);
+  }
+  // wider inputs: dW1^T = X^T dZ1, rows of the input dimension in 128-row
+  // tiles, stored transposed (the first kIn rows)
+  d1.A = XT;
+  d1.B = dZ1T;
+  d1.M = N::kInPad;
+  d1.N = kHid;
+  return launch_gemm<EPI_ATOMIC_T> (d1, s);
 }
 
-extern "C" int drb_mlp_adam (float *params, const float *grad, float *m, float *v, float lr,
-                             float beta1, float beta2, float eps, int step, void *stream)
+template <int P>
+int guess_p (const float *params, const void *wbf16, const drb_mesh *mesh, const int *elem,
+             const float *pts, const int *order, int n, float *guess, int *err, cudaStream_t s)
 {
+  GuessArgs a;
+  a.params = params;
+  a.wb = (const __nv_bfloat16 *)wbf16;
+  a.packed = mesh->packed;
+  a.stride = packed_stride (Net<P>::kNd, 3);
+  a.elem = elem;
+  a.pts = pts;
+  a.order = order;
+  a.n = n;
+  a.guess = guess;
+  a.err = err;
+  constexpr size_t smem = guess_smem<P> ();
+  cudaFuncSetAttribute (mlp_guess_kernel<P>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  const int tiles = div_up (n, 128);
+  const int grid = min (div_up (tiles, Net<P>::kGroups), sm_count ());
+  mlp_guess_kernel<P><<<grid, 128 * Net<P>::kGroups, smem, s>>> (a);
+  return check_launch ("mlp_guess_kernel");
+}
+
+bool mesh_ok (const drb_mesh *mesh, const char *what)
+{
+  if (mesh && mesh->packed && mesh->dim == 3 && mesh->order >= 1 && mesh->order <= 3 &&
+      mesh->ncomp == 3 && mesh->shape == DRB_SHAPE_TENSOR)
+    return true;
+  char buf[160];
+  std::snprintf (buf, sizeof (buf), "%s: needs a packed hex geometry mesh of order 1..3", what);
+  set_last_error (buf);
+  return false;
+}
+
+} // namespace
+
+extern "C" int drb_mlp_param_count (int order)
+{
+  return !mlp_order_ok (order) ? -1 : order == 1 ? Net<1>::kParams : order == 2 ? Net<2>::kParams
+                                                                                  : Net<3>::kParams;
+}
+extern "C" int drb_mlp_bf16_count (int order)
+{
+  return !mlp_order_ok (order) ? -1 : order == 1 ? Net<1>::kBf16 : order == 2 ? Net<2>::kBf16
+                                                                                : Net<3>::kBf16;
+}
+extern "C" int drb_mlp_input_width (int order)
+{
+  return !mlp_order_ok (order) ? -1 : order == 1 ? Net<1>::kInPad : order == 2 ? Net<2>::kInPad
+                                                                                 : Net<3>::kInPad;
+}
+
+extern "C" int drb_mlp_prepare (int order, const float *params, void *wbf16, void *stream)
+{
+  if (!mlp_order_ok (order)) return DRB_ERR_INVALID_ARG;
+  if (!params || !wbf16)
+  {
+    set_last_error ("mlp_prepare: bad arguments");
+    return DRB_ERR_INVALID_ARG;
+  }
+  cudaStream_t s = (cudaStream_t)stream;
+  return order == 1 ? prepare_p<1> (params, wbf16, s) : order == 2 ? prepare_p<2> (params, wbf16, s)
+                                                                   : prepare_p<3> (params, wbf16, s);
+}
+
+extern "C" int drb_mlp_features (const drb_mesh *mesh, const int *elem, const float *pts, int n,
+                                 int n_pad, void *X, void *stream)
+{
+  if (!mesh_ok (mesh, "mlp_features")) return DRB_ERR_INVALID_ARG;
+  if (n < 0 || n_pad < n || (n_pad > 0 && !X) || (n > 0 && (!elem || !pts)))
+  {
+    set_last_error ("mlp_features: bad arguments (n <= n_pad)");
+    return DRB_ERR_INVALID_ARG;
+  }
+  if (n_pad == 0) return DRB_OK;
+  cudaStream_t s = (cudaStream_t)stream;
+  const int o = mesh->order;
+  return o == 1 ? features_p<1> (mesh, elem, pts, n, n_pad, X, s)
+         : o == 2 ? features_p<2> (mesh, elem, pts, n, n_pad, X, s)
+                  : features_p<3> (mesh, elem, pts, n, n_pad, X, s);
+}
+
+// Workspace of one training step over n_pad rows (multiple of 128):
+// Z1, Z2 fp32 [n_pad x 128]; H1, H2, dZ2, dZ1 bf16 [n_pad x 128];
+// transposes dZ2T, H1T, dZ1T bf16 [128 x n_pad], XT bf16 [kInPad x n_pad].
+extern "C" long long drb_mlp_workspace_bytes (int order, int n_pad)
+{
+  if (!mlp_order_ok (order) || n_pad < 0) return -1;
+  return order == 1 ? workspace_p<1> (n_pad) : order == 2 ? workspace_p<2> (n_pad)
+                                                          : workspace_p<3> (n_pad);
+}
+
+extern "C" int drb_mlp_forward (int order, const float *params, const void *wbf16, const void *X,
+                                int n, int n_pad, float *y, void *workspace, int *err,
+                                void *stream)
+{
+  if (!mlp_order_ok (order)) return DRB_ERR_INVALID_ARG;
+  if (!params || !wbf16 || !X || !y || !workspace || n < 0 || n_pad < n || (n_pad % 128))
+  {
+    set_last_error ("mlp_forward: bad arguments (n_pad must be a multiple of 128 and >= n)");
+    return DRB_ERR_INVALID_ARG;
+  }
+  if (n_pad == 0) return DRB_OK;
+  cudaStream_t s = (cudaStream_t)stream;
+  return order == 1 ? forward_p<1> (params, wbf16, X, n, n_pad, y, workspace, err, s)
+         : order == 2 ? forward_p<2> (params, wbf16, X, n, n_pad, y, workspace, err, s)
+                      : forward_p<3> (params, wbf16, X, n, n_pad, y, workspace, err, s);
+}
+
+extern "C" int drb_mlp_train_step (int order, const float *params, const void *wbf16, const void *X,
+                                   const float *target, const float *weight, int n, int n_pad,
+                                   float *grad, float *loss, void *workspace, int *err,
+                                   void *stream)
+{
+  if (!mlp_order_ok (order)) return DRB_ERR_INVALID_ARG;
+  if (!params || !wbf16 || !X || !target || !grad || !workspace || n < 1 || n_pad < n ||
+      (n_pad % 128))
+  {
+    set_last_error ("mlp_train_step: bad arguments (n_pad must be a multiple of 128 and >= n)");
+    return DRB_ERR_INVALID_ARG;
+  }
+  cudaStream_t s = (cudaStream_t)stream;
+  return order == 1 ? train_step_p<1> (params, wbf16, X, target, weight, n, n_pad, grad, loss,
+                                       workspace, err, s)
+         : order == 2 ? train_step_p<2> (params, wbf16, X, target, weight, n, n_pad, grad, loss,
+                                         workspace, err, s)
+                      : train_step_p<3> (params, wbf16, X, target, weight, n, n_pad, grad, loss,
+                                         workspace, err, s);
+}
+
+extern "C" int drb_mlp_adam (int order, float *params, const float *grad, float *m, float *v,
+                             float lr, float beta1, float beta2, float eps, int step, void *stream)
+{
+  if (!mlp_order_ok (order)) return DRB_ERR_INVALID_ARG;
   if (!params || !grad || !m || !v || step < 1)
   {
     set_last_error ("mlp_adam: bad arguments");
     return DRB_ERR_INVALID_ARG;
   }
+  const int np = drb_mlp_param_count (order);
   const float c1 = 1.f / (1.f - powf (beta1, (float)step));
   const float c2 = 1.f / (1.f - powf (beta2, (float)step));
-  adam_kernel<<<div_up (kParams, 256), 256, 0, (cudaStream_t)stream>>> (params, grad, m, v, kParams, lr,
-                                                                        beta1, beta2, eps, c1, c2);
+  adam_kernel<<<div_up (np, 256), 256, 0, (cudaStream_t)stream>>> (params, grad, m, v, np, lr, beta1,
+                                                                   beta2, eps, c1, c2);
   return check_launch ("adam_kernel");
 }
 
@@ -894,28 +1043,16 @@ extern "C" int drb_mlp_guess (const float *params, const void *wbf16, const drb_
                               const int *elem, const float *pts, const int *order, int n,
                               float *guess, int *err, void *stream)
 {
-  if (!params || !wbf16 || !mesh || !mesh->packed || mesh->dim != 3 || mesh->order != 2 ||
-      mesh->ncomp != 3 || mesh->shape != DRB_SHAPE_TENSOR || n < 0 ||
-      (n > 0 && (!elem || !pts || !guess)))
+  if (!mesh_ok (mesh, "mlp_guess")) return DRB_ERR_INVALID_ARG;
+  if (!params || !wbf16 || n < 0 || (n > 0 && (!elem || !pts || !guess)))
   {
-    set_last_error ("mlp_guess: needs a packed order-2 hex mesh");
+    set_last_error ("mlp_guess: bad arguments");
     return DRB_ERR_INVALID_ARG;
   }
   if (n == 0) return DRB_OK;
-  GuessArgs a;
-  a.params = params;
-  a.wb = (const __nv_bfloat16 *)wbf16;
-  a.packed = mesh->packed;
-  a.stride = packed_stride (27, 3);
-  a.elem = elem;
-  a.pts = pts;
-  a.order = order;
-  a.n = n;
-  a.guess = guess;
-  a.err = err;
-  cudaFuncSetAttribute (mlp_guess_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kGuessSmem);
-  const int tiles = div_up (n, 128);
-  const int grid = min (div_up (tiles, kGuessGroups), sm_count ());
-  mlp_guess_kernel<<<grid, kGuessThreads, kGuessSmem, (cudaStream_t)stream>>> (a);
-  return check_launch ("mlp_guess_kernel");
+  cudaStream_t s = (cudaStream_t)stream;
+  const int o = mesh->order;
+  return o == 1 ? guess_p<1> (params, wbf16, mesh, elem, pts, order, n, guess, err, s)
+         : o == 2 ? guess_p<2> (params, wbf16, mesh, elem, pts, order, n, guess, err, s)
+                  : guess_p<3> (params, wbf16, mesh, elem, pts, order, n, guess, err, s);
 }

@@ -558,7 +558,7 @@ DRB_D int locate_sample (const VolumeParams &vp, const float (&pt)[3], const flo
       if (leaf < 0) return -1;
       el = __ldg (vp.lp.leaf_nodes + leaf);
       bool given;
-      candidate_guess<S> (vp.lp, leaf, 0, false, x, given);
+      candidate_guess<S> (vp.lp, leaf, 0, false, pt, x, given);
     }
     int steps = 0;
     ++cands;
@@ -1154,6 +1154,8 @@ static int volume_common (const drb_mesh *mesh, const drb_mesh *field, const drb
   lp.max_steps = no.max_steps;
   lp.guess_mode = no.guess_mode;
   lp.guess = nullptr;
+  lp.leaf_maps = (mesh->shape == DRB_SHAPE_TENSOR && mesh->dim == 3)
+                 ? (const float4 *)bvh->leaf_maps : nullptr;
   vp.field_packed = field->packed;
   vp.field_idx = field->ctrl_idx;
   vp.field_vals = field->values;
@@ -1487,12 +1489,17 @@ extern "C" int drb_surface_mesh_lines (const void *rays, const void *hits, int n
 
 extern "C" int drb_sort_partials (const void *partials, int n, void *sorted, void *stream)
 {
-  if (n < 0 || (n > 0 && (!partials || !sorted)) || partials == sorted)
+  if (n < 0 || (n > 0 && (!partials || !sorted)))
   {
-    set_last_error ("sort_partials: bad arguments (the output may not alias the input)");
+    set_last_error ("sort_partials: bad arguments");
     return DRB_ERR_INVALID_ARG;
   }
   if (n == 0) return DRB_OK;
+  if (partials == sorted)
+  {
+    set_last_error ("sort_partials: the output may not alias the input");
+    return DRB_ERR_INVALID_ARG;
+  }
   cudaStream_t s = (cudaStream_t)stream;
   Scratch scr (s);
   unsigned *k0 = scr.alloc<unsigned> (n);

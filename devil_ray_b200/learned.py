@@ -1,8 +1,9 @@
 """Learned initial guess for the Newton inversion (no reference counterpart).
 
-A small MLP (81 control-point coordinates + 3 point coordinates, 84 -> 128
--> 128 -> 3, GELU, BF16 weights, FP32 accumulation) predicts the
-reference-space coordinates of a point in a candidate order-2 hex element.
+A small MLP (the candidate hex element's control-point coordinates + the 3
+point coordinates -> 128 -> 128 -> 3, GELU, BF16 weights, FP32
+accumulation; 84 inputs at order 2, 195 at order 3) predicts the
+reference-space coordinates of a point in the element.
 It is trained on Newton solutions the method itself produces, by the
 library's own tcgen05 forward/backward kernels (drb_mlp_train_step, Adam in
 drb_mlp_adam), and used only as the first guess of the first candidate
@@ -29,12 +30,30 @@ import torch
 from . import _lib as L
 from .api import BatchedLocator, UnstructuredMesh, _dev, _ptr, _stream
 
-N_IN, N_IN_PAD, N_HID, N_OUT = 84, 96, 128, 3
-W1, B1 = 0, N_HID * N_IN
-W2, B2 = B1 + N_HID, B1 + N_HID + N_HID * N_HID
-W3 = B2 + N_HID
-B3 = W3 + N_OUT * N_HID
-N_PARAMS = B3 + N_OUT
+N_HID, N_OUT = 128, 3
+
+
+class Layout:
+    """Offsets of the network's parameters in its fp32 vector for order-P
+    hex elements: W1 [128 x n_in], b1, W2 [128 x 128], b2, W3 [3 x 128], b3."""
+
+    def __init__(self, order: int):
+        self.order = order
+        self.n_in = 3 * (order + 1) ** 3 + 3
+        self.n_in_pad = (self.n_in + 15) // 16 * 16
+        self.W1 = 0
+        self.B1 = self.W1 + N_HID * self.n_in
+        self.W2 = self.B1 + N_HID
+        self.B2 = self.W2 + N_HID * N_HID
+        self.W3 = self.B2 + N_HID
+        self.B3 = self.W3 + N_OUT * N_HID
+        self.n_params = self.B3 + N_OUT
+
+
+# the order-2 network of the learned-guess workload
+_L2 = Layout(2)
+N_IN, N_IN_PAD = _L2.n_in, _L2.n_in_pad
+W1, B1, W2, B2, W3, B3, N_PARAMS = _L2.W1, _L2.B1, _L2.W2, _L2.B2, _L2.W3, _L2.B3, _L2.n_params
 
 _configured = False
 
@@ -45,14 +64,15 @@ def _lib():
     if not _configured:
         vp, ci, cf = C.c_void_p, C.c_int, C.c_float
         sig = {
-            "drb_mlp_param_count": (ci, []),
-            "drb_mlp_bf16_count": (ci, []),
-            "drb_mlp_workspace_bytes": (C.c_longlong, [ci]),
-            "drb_mlp_prepare": (ci, [vp, vp, vp]),
+            "drb_mlp_param_count": (ci, [ci]),
+            "drb_mlp_bf16_count": (ci, [ci]),
+            "drb_mlp_input_width": (ci, [ci]),
+            "drb_mlp_workspace_bytes": (C.c_longlong, [ci, ci]),
+            "drb_mlp_prepare": (ci, [ci, vp, vp, vp]),
             "drb_mlp_features": (ci, [C.POINTER(L.DrbMesh), vp, vp, ci, ci, vp, vp]),
-            "drb_mlp_forward": (ci, [vp, vp, vp, ci, ci, vp, vp, vp, vp]),
-            "drb_mlp_train_step": (ci, [vp, vp, vp, vp, vp, ci, ci, vp, vp, vp, vp, vp]),
-            "drb_mlp_adam": (ci, [vp, vp, vp, vp, cf, cf, cf, cf, ci, vp]),
+            "drb_mlp_forward": (ci, [ci, vp, vp, vp, ci, ci, vp, vp, vp, vp]),
+            "drb_mlp_train_step": (ci, [ci, vp, vp, vp, vp, vp, ci, ci, vp, vp, vp, vp, vp]),
+            "drb_mlp_adam": (ci, [ci, vp, vp, vp, vp, cf, cf, cf, cf, ci, vp]),
             "drb_mlp_guess": (ci, [vp, vp, C.POINTER(L.DrbMesh), vp, vp, vp, ci, vp, vp, vp]),
             "drb_map_points": (ci, [C.POINTER(L.DrbMesh), vp, vp, ci, vp, vp]),
             "drb_newton_pairs": (ci, [C.POINTER(L.DrbMesh), vp, vp, ci, cf, ci, vp, vp, vp, vp,
@@ -91,23 +111,27 @@ def newton_pairs(mesh: UnstructuredMesh, elem, pts, tol=1e-5, max_steps=20, gues
 class GuessMLP:
     """Parameters (fp32 masters on the device) and the library calls."""
 
-    def __init__(self, device="cuda", seed=0):
+    def __init__(self, device="cuda", seed=0, order: int = 2):
         lib = _lib()
-        assert lib.drb_mlp_param_count() == N_PARAMS
+        self.order = order
+        self.layout = lay = Layout(order)
+        assert lib.drb_mlp_param_count(order) == lay.n_params
+        assert lib.drb_mlp_input_width(order) == lay.n_in_pad
         self.device = torch.device(device)
         g = torch.Generator().manual_seed(seed)
-        p = torch.zeros(N_PARAMS, dtype=torch.float32)
+        p = torch.zeros(lay.n_params, dtype=torch.float32)
 
         def init(off, fan_out, fan_in):
             bound = math.sqrt(6.0 / (fan_in + fan_out))
             p[off:off + fan_out * fan_in] = (torch.rand(fan_out * fan_in, generator=g) * 2 - 1) * bound
 
-        init(W1, N_HID, N_IN)
-        init(W2, N_HID, N_HID)
-        init(W3, N_OUT, N_HID)
-        p[B3:B3 + 3] = 0.5  # centre of the reference element
+        init(lay.W1, N_HID, lay.n_in)
+        init(lay.W2, N_HID, N_HID)
+        init(lay.W3, N_OUT, N_HID)
+        p[lay.B3:lay.B3 + 3] = 0.5  # centre of the reference element
         self.params = p.to(self.device)
-        self.wbf16 = torch.empty(lib.drb_mlp_bf16_count(), dtype=torch.bfloat16, device=self.device)
+        self.wbf16 = torch.empty(lib.drb_mlp_bf16_count(order), dtype=torch.bfloat16,
+                                 device=self.device)
         self.m = torch.zeros_like(self.params)
         self.v = torch.zeros_like(self.params)
         self.step_count = 0
@@ -115,8 +139,8 @@ class GuessMLP:
         self.prepare()
 
     def prepare(self, stream=None):
-        L.check(_lib().drb_mlp_prepare(_ptr(self.params), _ptr(self.wbf16), _stream(stream)),
-                "drb_mlp_prepare")
+        L.check(_lib().drb_mlp_prepare(self.order, _ptr(self.params), _ptr(self.wbf16),
+                                       _stream(stream)), "drb_mlp_prepare")
 
     def check_err(self):
         if int(self.err.item()) != 0:
@@ -129,20 +153,23 @@ class GuessMLP:
     def features(self, mesh, elem, pts, n_pad=None, stream=None):
         n = elem.numel()
         n_pad = n_pad or self.pad(n)
-        X = torch.empty((n_pad, N_IN_PAD), dtype=torch.bfloat16, device=self.device)
+        if mesh.order != self.order:
+            raise ValueError(f"network of order {self.order}, mesh of order {mesh.order}")
+        X = torch.empty((n_pad, self.layout.n_in_pad), dtype=torch.bfloat16, device=self.device)
         L.check(_lib().drb_mlp_features(C.byref(mesh.desc()), _ptr(elem), _ptr(pts), n, n_pad,
                                         _ptr(X), _stream(stream)), "drb_mlp_features")
         return X
 
     def workspace(self, n_pad):
-        nb = _lib().drb_mlp_workspace_bytes(n_pad)
+        nb = _lib().drb_mlp_workspace_bytes(self.order, n_pad)
         return torch.empty(nb, dtype=torch.uint8, device=self.device)
 
     def forward(self, X, n, ws=None, stream=None):
         n_pad = X.shape[0]
         ws = ws if ws is not None else self.workspace(n_pad)
         y = torch.empty((max(n, 1), 3), dtype=torch.float32, device=self.device)
-        L.check(_lib().drb_mlp_forward(_ptr(self.params), _ptr(self.wbf16), _ptr(X), n, n_pad,
+        L.check(_lib().drb_mlp_forward(self.order, _ptr(self.params), _ptr(self.wbf16), _ptr(X), n,
+                                       n_pad,
                                        _ptr(y), _ptr(ws), _ptr(self.err), _stream(stream)),
                 "drb_mlp_forward")
         return y[:n]
@@ -152,7 +179,7 @@ class GuessMLP:
         ws = ws if ws is not None else self.workspace(n_pad)
         g = torch.empty_like(self.params)
         loss = torch.zeros(1, dtype=torch.float32, device=self.device)
-        L.check(_lib().drb_mlp_train_step(_ptr(self.params), _ptr(self.wbf16), _ptr(X),
+        L.check(_lib().drb_mlp_train_step(self.order, _ptr(self.params), _ptr(self.wbf16), _ptr(X),
                                           _ptr(target), _ptr(weight), n, n_pad, _ptr(g),
                                           _ptr(loss), _ptr(ws), _ptr(self.err), _stream(stream)),
                 "drb_mlp_train_step")
@@ -160,11 +187,14 @@ class GuessMLP:
 
     def adam(self, g, lr=1e-3, b1=0.9, b2=0.999, eps=1e-8, stream=None):
         self.step_count += 1
-        L.check(_lib().drb_mlp_adam(_ptr(self.params), _ptr(g), _ptr(self.m), _ptr(self.v), lr,
+        L.check(_lib().drb_mlp_adam(self.order, _ptr(self.params), _ptr(g), _ptr(self.m),
+                                    _ptr(self.v), lr,
                                     b1, b2, eps, self.step_count, _stream(stream)), "drb_mlp_adam")
         self.prepare(stream)
 
     def guess(self, mesh, elem, pts, order=None, stream=None):
+        if mesh.order != self.order:
+            raise ValueError(f"network of order {self.order}, mesh of order {mesh.order}")
         n = elem.numel()
         out = torch.empty((max(n, 1), 3), dtype=torch.float32, device=self.device)
         L.check(_lib().drb_mlp_guess(_ptr(self.params), _ptr(self.wbf16), C.byref(mesh.desc()),

@@ -43,9 +43,15 @@ enum drb_guess_mode
   /* centre of the candidate leaf's reference sub-box, the reference's
    * intended guess (device_mesh.hpp:161-162). */
   DRB_GUESS_SUBREF_CENTER = 2,
+  /* the element map linearised at the candidate leaf's reference sub-box
+   * centre c: x0 = c + J(c)^-1 (p - X(c)), from the per-leaf maps of
+   * drb_bvh_leaf_maps (hex meshes; without them, as DRB_GUESS_SUBREF_CENTER).
+   * No reference counterpart: the reference's guess is its sub-box centre. */
+  DRB_GUESS_SUBBOX_LINEAR = 4,
   /* caller-provided guess per point for its first candidate element (e.g.
    * the learned guess), element centre for later candidates and as the
-   * fallback when the guessed solve does not converge. */
+   * fallback when the guessed solve does not converge within max_steps (a
+   * guessed solve that converged outside the element is not retried). */
   DRB_GUESS_GIVEN = 3
 };
 
@@ -127,7 +133,17 @@ typedef struct drb_bvh
   float *wide_nodes;     /* device float[32 * n_wide]: 8 x float4 per node */
   int n_wide;
   int wide_depth;        /* wide levels (root = 1) */
+  /* Optional per-leaf linear maps for DRB_GUESS_SUBBOX_LINEAR
+   * (drb_bvh_leaf_maps); NULL: that guess falls back to the sub-box centre. */
+  float *leaf_maps;      /* device float[16 * n_leaf] */
 } drb_bvh;
+
+/* Per-leaf linearisation of a hex mesh's element maps for
+ * DRB_GUESS_SUBBOX_LINEAR: for sorted leaf k with element e and reference
+ * sub-box centre c, maps[16 k ..] = (c, X_e(c), J_e(c)^-1 row-major, 0),
+ * X in absolute coordinates.  A leaf whose Jacobian is singular gets a zero
+ * inverse (the guess is then c).  No reference counterpart. */
+int drb_bvh_leaf_maps (const drb_mesh *mesh, const drb_bvh *bvh, float *maps, void *stream);
 
 /* 4-wide traversal tree of a built BVH (no reference counterpart: the
  * reference traverses the binary nodes, device_mesh.hpp:262-318).  Every
@@ -243,13 +259,15 @@ typedef struct drb_locate_config
   int blocks_per_sm;     /* resident blocks per SM, 0 = as many as fit */
   int chunk;             /* queries a warp pops from the global queue at once */
   int sort_queries;      /* 0 = process the queries in input order; 1 =
-                            in Morton-cell order, the query records staged
-                            in that order (one coalesced read per warp) and
-                            the results written at each query's input
-                            index; 2 = as 1 with the results also staged
-                            contiguously and put back in input order by a
-                            separate pass (not with DRB_GUESS_GIVEN, which
-                            then runs as 1) */
+                            in Morton-cell order, each query read through
+                            that order and its result written at its input
+                            index (the fastest end to end); 2 = as 1 but
+                            the query records staged in that order first
+                            (a gather pass; one coalesced read per warp in
+                            the kernel); 3 = as 2 with the results also
+                            staged contiguously and put back in input order
+                            by a separate pass (not with DRB_GUESS_GIVEN,
+                            which then runs as 2) */
   int reg_elements;      /* where a candidate's control points are read from
                             during its Newton solve: 0 = through L1 on every
                             step; 1 = registers (orders <= 2; fewer loads,
@@ -522,30 +540,36 @@ int drb_scalar_buffer_write (const void *rays, const void *hits, const float *fr
 int drb_ray_max (void *rays, const void *hits, int n, void *stream);
 
 /* -------------------------------------------- learned initial guess --
- * No counterpart in the reference.  A small MLP (27 control points x 3 +
- * point x 3 = 84 inputs -> 128 -> 128 -> 3, GELU) predicts the reference
- * coordinates of a point in an order-2 hex candidate element.  Parameters:
- * one fp32 vector of drb_mlp_param_count() floats (W1 [128 x 84], b1,
- * W2 [128 x 128], b2, W3 [3 x 128], b3); bf16 tensor-core operands:
- * drb_mlp_bf16_count() values written by drb_mlp_prepare.  Tensor-core
- * kernels report a bounded-wait timeout through *err (device int32). */
-int drb_mlp_param_count (void);
-int drb_mlp_bf16_count (void);
-long long drb_mlp_workspace_bytes (int n_pad);
-int drb_mlp_prepare (const float *params, void *wbf16, void *stream);
-/* features of (element, point) pairs: X device bf16 [n_pad x 96] */
+ * No counterpart in the reference.  A small MLP (the (P+1)^3 control points
+ * x 3 + point x 3 inputs -> 128 -> 128 -> 3, GELU) predicts the reference
+ * coordinates of a point in an order-P hex candidate element: 84 inputs at
+ * order 2, 195 at order 3.  `order` selects the network; the mesh's order
+ * does where a mesh is passed.  Parameters: one fp32 vector of
+ * drb_mlp_param_count(order) floats (W1 [128 x inputs], b1, W2 [128 x
+ * 128], b2, W3 [3 x 128], b3); bf16 tensor-core operands:
+ * drb_mlp_bf16_count(order) values written by drb_mlp_prepare.  Feature
+ * rows are drb_mlp_input_width(order) wide (inputs padded to 16: 96 at
+ * order 2, 208 at order 3).  Tensor-core kernels report a bounded-wait
+ * timeout through *err (device int32).  Counts are -1 for an order outside
+ * 1..3. */
+int drb_mlp_param_count (int order);
+int drb_mlp_bf16_count (int order);
+int drb_mlp_input_width (int order);
+long long drb_mlp_workspace_bytes (int order, int n_pad);
+int drb_mlp_prepare (int order, const float *params, void *wbf16, void *stream);
+/* features of (element, point) pairs: X device bf16 [n_pad x input width] */
 int drb_mlp_features (const drb_mesh *mesh, const int *elem, const float *pts, int n, int n_pad,
                       void *X, void *stream);
 /* forward: y device float[3n]; n_pad multiple of 128 */
-int drb_mlp_forward (const float *params, const void *wbf16, const void *X, int n, int n_pad,
-                     float *y, void *workspace, int *err, void *stream);
+int drb_mlp_forward (int order, const float *params, const void *wbf16, const void *X, int n,
+                     int n_pad, float *y, void *workspace, int *err, void *stream);
 /* one training step: masked MSE against target (device float[3n], weight
  * optional device float[n]); grad (device float[param_count]) and *loss */
-int drb_mlp_train_step (const float *params, const void *wbf16, const void *X,
+int drb_mlp_train_step (int order, const float *params, const void *wbf16, const void *X,
                         const float *target, const float *weight, int n, int n_pad, float *grad,
                         float *loss, void *workspace, int *err, void *stream);
-int drb_mlp_adam (float *params, const float *grad, float *m, float *v, float lr, float beta1,
-                  float beta2, float eps, int step, void *stream);
+int drb_mlp_adam (int order, float *params, const float *grad, float *m, float *v, float lr,
+                  float beta1, float beta2, float eps, int step, void *stream);
 /* fused tensor-core inference: guess device float[3n] for the pairs
  * (elem[q], pts[q]); rows are visited in the order order[0..n) when given
  * (the Morton order of drb_query_order keeps a tile's elements together in

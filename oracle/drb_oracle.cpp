@@ -256,7 +256,10 @@ int locate_one (int p, const int *ctrl_idx, const float *xyz, const float *nodes
       int steps = 0;
       bool found = newton<T> (p, cp, tgt, x, T (tol), max_steps, steps, simplex);
       iters += steps;
-      if (!found && given)
+      // the centre retry only after a guessed solve that used its whole
+      // step budget (one that converged outside the element has shown the
+      // point is not in it)
+      if (!found && given && steps >= max_steps)
       {
         x[0] = x[1] = x[2] = centre;
         found = newton<T> (p, cp, tgt, x, T (tol), max_steps, steps, simplex);

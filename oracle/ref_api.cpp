@@ -699,8 +699,9 @@ int ref_volume_rays (void *h, int n_rays, const float *rays9, int samples, int u
 // Renderer::render (rendering/renderer.cpp:229-363) over a collection of
 // n_dom hex-mesh domains (arrays concatenated: orders, n_elem and n_ctrl per
 // domain; their control indices, coordinates and field "f" values one after
-// the other), with an optional boundary Surface (MeshBoundary of the
-// collection; mesh lines when draw_mesh), an optional Volume, and the camera
+// the other), with an optional boundary Surface (MeshBoundary of domains
+// surf_first .. surf_first + surf_count - 1; mesh lines when draw_mesh), an
+// optional Volume of the whole collection, and the camera
 // moved by reset_to_bounds(collection bounds, pads3) when pads3 is given,
 // then elevate and azimuth.  Colour bars off.  Writes the framebuffer's
 // colours and depths; with save_prefix set, also <prefix>.png and
@@ -708,7 +709,8 @@ int ref_volume_rays (void *h, int n_rays, const float *rays9, int samples, int u
 int ref_render_scene (int n_dom, const int *orders, const int *n_elems, const int *n_ctrls,
                       const int *ctrl_idx, const float *xyz, const float *field, int w, int h,
                       const float *cam9, float fov, const double *pads3, float elevate_deg,
-                      float azimuth_deg, int surface, int draw_mesh, float line_thickness,
+                      float azimuth_deg, int surface, int surf_first, int surf_count,
+                      int draw_mesh, float line_thickness,
                       int volume, int samples, int use_lighting, int tf_samples, int n_rgb,
                       const float *rgb_pts, int n_alpha, const float *alpha_pts, float *rgba,
                       float *depth, const char *save_prefix)
@@ -740,8 +742,10 @@ int ref_render_scene (int n_dom, const int *orders, const int *n_elems, const in
     Collection faces;
     if (surface)
     {
+      Collection part;
+      for (int d = surf_first; d < surf_first + surf_count; ++d) part.add_domain (col.domain (d));
       MeshBoundary boundary;
-      faces = boundary.execute (col);
+      faces = boundary.execute (part);
       std::shared_ptr<Surface> surf = std::make_shared<Surface> (faces);
       surf->field ("f");
       surf->color_map ().color_table (table);

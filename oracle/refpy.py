@@ -59,8 +59,8 @@ def lib():
                                       C.c_float, vp, vp]
         L.ref_render_scene.argtypes = [C.c_int, vp, vp, vp, vp, vp, vp, C.c_int, C.c_int, vp,
                                        C.c_float, vp, C.c_float, C.c_float, C.c_int, C.c_int,
-                                       C.c_float, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int,
-                                       vp, C.c_int, vp, vp, vp, C.c_char_p]
+                                       C.c_int, C.c_int, C.c_float, C.c_int, C.c_int, C.c_int,
+                                       C.c_int, C.c_int, vp, C.c_int, vp, vp, vp, C.c_char_p]
         L.ref_hex_set_bvh.argtypes = [vp, C.c_int, vp, C.c_int, vp, vp, vp, vp]
         L.ref_volume_rays.argtypes = [vp, C.c_int, vp, C.c_int, C.c_int, C.c_int, C.c_int, vp,
                                       C.c_int, vp, C.c_int, vp, vp, C.c_int]
@@ -313,11 +313,14 @@ def camera_move(w, h, cam9, fov, bounds6=None, pads=(0.0, 0.0, 0.0), elevate=0.0
 
 
 def render_scene(domains, w, h, cam9, fov, pads=None, elevate=0.0, azimuth=0.0, surface=True,
-                 draw_mesh=False, line_thickness=0.05, volume=True, samples=200,
+                 surface_domains=None, draw_mesh=False, line_thickness=0.05, volume=True, samples=200,
                  use_lighting=True, tf_samples=1024, rgb_pts=None, alpha_pts=None,
                  save_prefix=None):
     """The reference's Renderer::render over hex-mesh domains, each a tuple
-    (order, ctrl_idx, xyz, field): returns (rgba [h, w, 4], depth [h, w])."""
+    (order, ctrl_idx, xyz, field), the surface over the domain range
+    surface_domains = (first, count) (all by default): returns (rgba [h, w,
+    4], depth [h, w])."""
+    sd = surface_domains if surface_domains is not None else (0, len(domains))
     orders = np.array([d[0] for d in domains], np.int32)
     nds = (orders + 1) ** 3
     n_el = np.array([np.asarray(d[1]).size // nd for d, nd in zip(domains, nds)], np.int32)
@@ -335,7 +338,8 @@ def render_scene(domains, w, h, cam9, fov, pads=None, elevate=0.0, azimuth=0.0, 
     depth = np.zeros((h, w), np.float32)
     st = lib().ref_render_scene(len(domains), _p(orders), _p(n_el), _p(n_ctrl), _p(ci), _p(xyz),
                                 _p(fld), w, h, _p(cam), fov, None if p3 is None else _p(p3),
-                                elevate, azimuth, int(surface), int(draw_mesh), line_thickness,
+                                elevate, azimuth, int(surface), int(sd[0]), int(sd[1]),
+                                int(draw_mesh), line_thickness,
                                 int(volume), samples, int(use_lighting), tf_samples,
                                 rgb.size // 4, _p(rgb), alp.size // 2, _p(alp), _p(rgba),
                                 _p(depth),

@@ -161,8 +161,8 @@ def _scene_domains(name):
     return [(m.order, m.ctrl_idx, m.xyz, m.field)]
 
 
-def _write_scene(d, doms, w, cam9, fov, pads, elevate, azimuth, surface, draw_mesh, thickness,
-                 volume, samples, lighting, tf_samples, rgb, alpha):
+def _write_scene(d, doms, w, cam9, fov, pads, elevate, azimuth, surface, surf_domains, draw_mesh,
+                 thickness, volume, samples, lighting, tf_samples, rgb, alpha):
     with open(d / "scene.bin", "wb") as f:
         np.array([len(doms)], np.int32).tofile(f)
         for order, ci, xyz, fld in doms:
@@ -177,7 +177,7 @@ def _write_scene(d, doms, w, cam9, fov, pads, elevate, azimuth, surface, draw_me
         np.array([pads is not None], np.int32).tofile(f)
         np.asarray(pads if pads is not None else (0, 0, 0), np.float64).tofile(f)
         np.array([elevate, azimuth], np.float32).tofile(f)
-        np.array([surface, draw_mesh], np.int32).tofile(f)
+        np.array([surface, surf_domains[0], surf_domains[1], draw_mesh], np.int32).tofile(f)
         np.array([thickness], np.float32).tofile(f)
         np.array([volume, samples, lighting, tf_samples], np.int32).tofile(f)
         np.array([rgb.shape[0]], np.int32).tofile(f)
@@ -187,17 +187,24 @@ def _write_scene(d, doms, w, cam9, fov, pads, elevate, azimuth, surface, draw_me
 
 
 SCENES = {
-    # two domains, camera on the collection's padded bounds then turned;
-    # surfaces of both domains (their cut faces too) and the volume in front
+    # two domains, camera on the collection's padded bounds then turned; the
+    # far domain's boundary surface and, composited in front of it, the
+    # volume of both domains (a surface of the whole collection would hide
+    # the volume behind its near faces)
     "two_domain_surface_volume": dict(mesh="two_domains", pads=(0.1, 0.05, 0.2), elevate=15.0,
-                                      azimuth=30.0, surface=1, draw_mesh=0, volume=1,
-                                      lighting=1),
+                                      azimuth=30.0, surface=1, surf_domains=(0, 1), draw_mesh=0,
+                                      volume=1, lighting=1),
+    # two domains, both domains' boundary surfaces (their cut faces too)
+    "two_domain_surfaces": dict(mesh="two_domains", pads=(0.0, 0.1, 0.0), elevate=-20.0,
+                                azimuth=75.0, surface=1, surf_domains=(0, 2), draw_mesh=1,
+                                volume=0, lighting=1),
     # one domain, mesh lines over the shaded boundary, the volume in front
     "mesh_lines": dict(mesh="one_domain", pads=None, elevate=0.0, azimuth=-20.0, surface=1,
-                       draw_mesh=1, volume=1, lighting=1),
+                       surf_domains=(0, 1), draw_mesh=1, volume=1, lighting=1),
     # two domains, volume alone, unlit
     "two_domain_volume": dict(mesh="two_domains", pads=(0.0, 0.0, 0.0), elevate=-10.0,
-                              azimuth=0.0, surface=0, draw_mesh=0, volume=1, lighting=0),
+                              azimuth=0.0, surface=0, surf_domains=(0, 0), draw_mesh=0, volume=1,
+                              lighting=0),
 }
 
 
@@ -221,8 +228,8 @@ def test_cpp_renderer_matches_reference(cuda, ref, tmp_path, scene):
     rgb = np.array(meshgen.TF_RGB, np.float32)
     alpha = np.array(meshgen.TF_ALPHA, np.float32)
     _write_scene(tmp_path, doms, w, cam9, fov, sc["pads"], sc["elevate"], sc["azimuth"],
-                 sc["surface"], sc["draw_mesh"], thickness, sc["volume"], samples,
-                 sc["lighting"], tf_samples, rgb, alpha)
+                 sc["surface"], sc["surf_domains"], sc["draw_mesh"], thickness, sc["volume"],
+                 samples, sc["lighting"], tf_samples, rgb, alpha)
     out = subprocess.run([str(RENDER_EXE), str(tmp_path)], capture_output=True, text=True,
                          timeout=300)
     assert out.returncode == 0, out.stderr
@@ -244,6 +251,7 @@ def test_cpp_renderer_matches_reference(cuda, ref, tmp_path, scene):
     assert camf[6] == np.float32(want_fov)
     rimg, rdep = ref.render_scene(doms, w, w, cam9, fov, pads=sc["pads"], elevate=sc["elevate"],
                                   azimuth=sc["azimuth"], surface=bool(sc["surface"]),
+                                  surface_domains=sc["surf_domains"],
                                   draw_mesh=bool(sc["draw_mesh"]), line_thickness=thickness,
                                   volume=bool(sc["volume"]), samples=samples,
                                   use_lighting=bool(sc["lighting"]), tf_samples=tf_samples,

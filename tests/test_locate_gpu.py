@@ -253,10 +253,10 @@ def test_locate_graph_replay_matches_eager(cuda, shape):
 @pytest.mark.parametrize("name", ["volume_8", "p3_10", "p1_9"])
 @pytest.mark.parametrize("guess", ["centre", "subref"])
 def test_staged_equals_ordered_and_plain(cuda, name, guess):
-    """drb_locate_batched stages its queries in processing order and writes
-    its results contiguously; the answers equal the query-order path's
-    (drb_locate_ordered, which reads the queries where they lie) and the
-    plain one-thread-per-query kernel's bit for bit, statistics included."""
+    """Every placement of the queries and results (read through the Morton
+    order, staged records, staged results) and the caller-ordered path
+    (drb_locate_ordered) give the plain one-thread-per-query kernel's
+    answers bit for bit, statistics included."""
     import torch
     from devil_ray_b200 import _lib as L
     from devil_ray_b200 import api
@@ -267,15 +267,18 @@ def test_staged_equals_ordered_and_plain(cuda, name, guess):
     order = loc.order(q)
     c1, r1, i1, a1, n1 = loc.locate(q, order=order, stats=True)
     c2, r2 = g.locate(q, tol=1e-5, max_steps=20, guess_mode=mode)
-    # results staged as well and put back by a separate pass (sort_queries 2)
-    loc2 = api.BatchedLocator(g, tol=1e-5, max_steps=20, guess_mode=mode,
-                              config=L.DrbLocateConfig(128, 0, 64, 2, 0))
-    c3, r3, i3, a3, n3 = loc2.locate(q, stats=True)
+    # query records staged first (sort_queries 2), results staged as well
+    # and put back by a separate pass (3)
+    out = []
+    for mode_s in (2, 3):
+        loc_s = api.BatchedLocator(g, tol=1e-5, max_steps=20, guess_mode=mode,
+                                   config=L.DrbLocateConfig(128, 0, 64, mode_s, 0))
+        out.append(loc_s.locate(q, stats=True))
     torch.cuda.synchronize()
-    for c, r in ((c1, r1), (c2, r2), (c3, r3)):
+    for c, r in ((c1, r1), (c2, r2)) + tuple((o[0], o[1]) for o in out):
         assert torch.equal(c0, c)
         assert torch.equal(r0.view(torch.int32), r.view(torch.int32))
-    for i, a, nd in ((i1, a1, n1), (i3, a3, n3)):
+    for i, a, nd in ((i1, a1, n1),) + tuple((o[2], o[3], o[4]) for o in out):
         assert torch.equal(i0, i) and torch.equal(a0, a) and torch.equal(n0, nd)
 
 
@@ -319,3 +322,40 @@ def test_autotuner_config_is_valid_and_exact(cuda):
     torch.cuda.synchronize()
     assert torch.equal(c0, c1)
     assert torch.equal(r0.view(torch.int32), r1.view(torch.int32))
+
+
+@pytest.mark.parametrize("name", ["trilinear_12", "trilinear_12_d25", "p3_10", "p1_9"])
+def test_subbox_linear_guess(cuda, name):
+    """The first guess from each leaf's linearised element map
+    (GUESS_SUBBOX_LINEAR) converges to the same answers as the element-centre
+    guess (same cells except on shared faces, reference points within the
+    1e-5 tolerance, FP64 error below 1e-5), with fewer Newton steps than the
+    sub-box-centre guess; the plain and batched kernels agree bit for bit."""
+    import torch
+    from devil_ray_b200 import _lib as L
+    from devil_ray_b200 import api
+    from oracle import restate
+    m, q, g = _setup(cuda, name, 60000, 37)
+    lin = api.BatchedLocator(g, tol=1e-5, max_steps=20, guess_mode=L.GUESS_SUBBOX_LINEAR)
+    c4, r4, i4, a4, _ = lin.locate(q, stats=True)
+    assert g.get_bvh().leaf_maps is not None
+    cp, rp = g.locate(q, tol=1e-5, max_steps=20, guess_mode=L.GUESS_SUBBOX_LINEAR)
+    c1, r1, i1, *_ = api.BatchedLocator(g, 1e-5, 20, L.GUESS_ELEM_CENTER).locate(q, stats=True)
+    c2, r2, i2, *_ = api.BatchedLocator(g, 1e-5, 20, L.GUESS_SUBREF_CENTER).locate(q, stats=True)
+    torch.cuda.synchronize()
+    assert torch.equal(c4, cp) and torch.equal(r4.view(torch.int32), rp.view(torch.int32))
+    c4n, r4n, c1n, r1n = c4.cpu().numpy(), r4.cpu().numpy(), c1.cpu().numpy(), r1.cpu().numpy()
+    same = c4n == c1n
+    assert (~same).mean() < 2e-3
+    assert _shared_face_ok(m, c4n[~same], r4n[~same], c1n[~same], r1n[~same]).all()
+    hit = same & (c4n >= 0)
+    assert np.abs(r4n[hit] - r1n[hit]).max() < 1e-5
+    if restate.available():
+        f64, ok = restate.newton_fp64(m.order, m.ctrl_idx, m.xyz, c4n, q)
+        sel = (c4n >= 0) & ok
+        assert np.abs(f64[sel] - r4n[sel]).max() < 1e-5
+    loc = c4 >= 0
+    m4, m2, m1 = (float(i[loc].float().mean()) for i in (i4, i2, i1))
+    print(f"{name}: mean Newton steps: sub-box linear {m4:.3f}, sub-box centre {m2:.3f}, "
+          f"element centre {m1:.3f}")
+    assert m4 < m2

@@ -1,9 +1,10 @@
-"""The learned initial guess: tcgen05 BF16 GEMMs (FP32 accumulation) checked
-against a NumPy FP64 evaluation of the same quantised network, gradients
-checked against the CPU oracle's FP64 backward, the fused guess kernel
-against the layer-by-layer forward, the hinted locate against drb_locate
-with the same guesses, and a short training run showing the gain over the
-element-centre guess."""
+"""The learned initial guess, for the order-2 and order-3 networks: tcgen05
+BF16 GEMMs (FP32 accumulation) checked against a NumPy FP64 evaluation of
+the same quantised network, gradients checked against the FP64 backward,
+the fused guess kernel against the layer-by-layer forward, the hinted
+locate against drb_locate with the same guesses, and short training runs
+showing what the network gains over the element-centre guess (the method
+without it) and how it compares with the free sub-box-centre guess."""
 import numpy as np
 import pytest
 
@@ -28,23 +29,24 @@ def gelu_grad(x):
     return 0.5 * (1 + t) + 0.5 * x * (1 - t * t) * du
 
 
-def unpack(p):
+def unpack(p, order=2):
     from devil_ray_b200 import learned as LG
+    lay = LG.Layout(order)
     p = np.asarray(p, np.float64)
-    W1 = p[LG.W1:LG.B1].reshape(128, 84)
-    b1 = p[LG.B1:LG.W2]
-    W2 = p[LG.W2:LG.B2].reshape(128, 128)
-    b2 = p[LG.B2:LG.W3]
-    W3 = p[LG.W3:LG.B3].reshape(3, 128)
-    b3 = p[LG.B3:LG.N_PARAMS]
+    W1 = p[lay.W1:lay.B1].reshape(128, lay.n_in)
+    b1 = p[lay.B1:lay.W2]
+    W2 = p[lay.W2:lay.B2].reshape(128, 128)
+    b2 = p[lay.B2:lay.W3]
+    W3 = p[lay.W3:lay.B3].reshape(3, 128)
+    b3 = p[lay.B3:lay.n_params]
     return W1, b1, W2, b2, W3, b3
 
 
-def oracle_forward(p, X):
+def oracle_forward(p, X, order=2):
     """FP64 forward of the network as the kernels quantise it: bf16 inputs,
     W1, W2 and first-layer activations; fp32-exact head."""
-    W1, b1, W2, b2, W3, b3 = unpack(p)
-    Xq = bf16(X)[:, :84]
+    W1, b1, W2, b2, W3, b3 = unpack(p, order)
+    Xq = bf16(X)[:, :W1.shape[1]]
     Z1 = Xq @ bf16(W1).T + b1
     H1 = bf16(gelu(Z1))
     Z2 = H1 @ bf16(W2).T + b2
@@ -53,9 +55,9 @@ def oracle_forward(p, X):
     return Xq, Z1, H1, Z2, H2, y
 
 
-def oracle_grad(p, X, T, w, n):
-    W1, b1, W2, b2, W3, b3 = unpack(p)
-    Xq, Z1, H1, Z2, H2, y = oracle_forward(p, X)
+def oracle_grad(p, X, T, w, n, order=2):
+    W1, b1, W2, b2, W3, b3 = unpack(p, order)
+    Xq, Z1, H1, Z2, H2, y = oracle_forward(p, X, order)
     dY = 2 * w[:, None] * (y - T) / n
     g = {}
     g["W3"] = dY.T @ H2
@@ -70,14 +72,18 @@ def oracle_grad(p, X, T, w, n):
     return g, loss
 
 
-@pytest.fixture(scope="module")
-def setup(cuda):
+@pytest.fixture(scope="module", params=[2, 3])
+def setup(cuda, request):
     import torch
     from devil_ray_b200 import api, meshgen
     from devil_ray_b200 import learned as LG
-    m = meshgen.trilinear_distorted_mesh(12, 2, 0.15, seed=31)
+    order = request.param
+    if order == 2:
+        m = meshgen.trilinear_distorted_mesh(12, 2, 0.15, seed=31)
+    else:
+        m = meshgen.warped_mesh(8, 3, 0.05, gaussian_field_seed=4)
     mesh = api.UnstructuredMesh(m.ctrl_idx, m.xyz, m.order, device=cuda)
-    model = LG.GuessMLP(cuda, seed=7)
+    model = LG.GuessMLP(cuda, seed=7, order=order)
     # perturb the biases so every parameter block matters
     g = torch.Generator(device="cpu").manual_seed(3)
     model.params += (torch.rand(model.params.shape, generator=g) - 0.5).cuda() * 0.02
@@ -97,7 +103,7 @@ def test_tcgen05_forward_matches_fp64(setup):
     model.check_err()
     p = model.params.cpu().numpy()
     Xn = X.float().cpu().numpy()[:n]
-    *_, yo = oracle_forward(p, Xn)
+    *_, yo = oracle_forward(p, Xn, model.order)
     err = np.abs(y.cpu().numpy() - yo).max()
     scale = np.abs(yo).max()
     print(f"forward: max |y - y_fp64| {err:.3e} (|y| <= {scale:.2f})")
@@ -113,11 +119,12 @@ def test_tcgen05_gradients_match_fp64(setup):
     from devil_ray_b200 import learned as LG
     p = model.params.cpu().numpy()
     og, oloss = oracle_grad(p, X.float().cpu().numpy()[:n], label.cpu().numpy().astype(np.float64),
-                            w.cpu().numpy().astype(np.float64), n)
+                            w.cpu().numpy().astype(np.float64), n, model.order)
     gg = grad.cpu().numpy()
-    blocks = {"W1": gg[LG.W1:LG.B1].reshape(128, 84), "b1": gg[LG.B1:LG.W2],
-              "W2": gg[LG.W2:LG.B2].reshape(128, 128), "b2": gg[LG.B2:LG.W3],
-              "W3": gg[LG.W3:LG.B3].reshape(3, 128), "b3": gg[LG.B3:LG.N_PARAMS]}
+    lay = model.layout
+    blocks = {"W1": gg[lay.W1:lay.B1].reshape(128, lay.n_in), "b1": gg[lay.B1:lay.W2],
+              "W2": gg[lay.W2:lay.B2].reshape(128, 128), "b2": gg[lay.B2:lay.W3],
+              "W3": gg[lay.W3:lay.B3].reshape(3, 128), "b3": gg[lay.B3:lay.n_params]}
     for k, v in blocks.items():
         ref = og[k]
         rel = np.abs(v - ref).max() / max(np.abs(ref).max(), 1e-12)
@@ -171,14 +178,24 @@ def test_hinted_locate_equals_plain_given_guess(cuda, setup):
     assert torch.equal(it0, it1) and torch.equal(ca0, ca1)
 
 
-def test_training_reduces_newton_iterations(cuda):
+@pytest.mark.parametrize("order", [2, 3])
+def test_training_reduces_newton_iterations(cuda, order):
+    """Trained on the method's own solutions, the network's guess needs
+    fewer Newton steps than the element centre (the method without it) on
+    held-out in-element pairs and on located queries, with the same cells
+    and reference points.  Against the free sub-box-centre guess the mean
+    steps of the located queries are printed; the network is not asserted
+    to win there (at order 2 it does not)."""
     import torch
     from devil_ray_b200 import _lib as L
     from devil_ray_b200 import api, meshgen
     from devil_ray_b200 import learned as LG
-    m = meshgen.trilinear_distorted_mesh(16, 2, 0.15, seed=41)
+    if order == 2:
+        m = meshgen.trilinear_distorted_mesh(16, 2, 0.15, seed=41)
+    else:
+        m = meshgen.warped_mesh(12, 3, 0.05, gaussian_field_seed=4)
     mesh = api.UnstructuredMesh(m.ctrl_idx, m.xyz, m.order, device=cuda)
-    model = LG.GuessMLP(cuda, seed=1)
+    model = LG.GuessMLP(cuda, seed=1, order=order)
     losses = LG.train(model, mesh, samples=1 << 20, batch=16384, epochs=4, lr=3e-3)
     assert losses[-1] < 0.05 * losses[0], losses
     # guessed vs centre solves on held-out (element, point) pairs
@@ -188,22 +205,25 @@ def test_training_reduces_newton_iterations(cuda):
     rc, fc, ic = LG.newton_pairs(mesh, he, hp, 1e-5, 20)
     ok = fc
     err = (guess[ok] - rc[ok]).abs().max(dim=1).values
-    print(f"held-out guess error: median {err.median().item():.3e}, "
+    print(f"order {order} held-out guess error: median {err.median().item():.3e}, "
           f"p99 {err.quantile(0.99).item():.3e}; guessed solve converged "
           f"{fg[ok].float().mean().item():.5f}; iterations {ig[ok].float().mean().item():.3f} "
           f"vs centre {ic[ok].float().mean().item():.3f}")
     assert ig[ok].float().mean() < ic[ok].float().mean()
     q = torch.as_tensor(meshgen.uniform_queries(200000, 99), device=cuda)
     c0, r0, it0, *_ = api.BatchedLocator(mesh, 1e-5, 20).locate(q, stats=True)
+    cs, rs, its, *_ = api.BatchedLocator(mesh, 1e-5, 20, guess_mode=L.GUESS_SUBREF_CENTER
+                                         ).locate(q, stats=True)
     ll = LG.LearnedLocator(mesh, model, 1e-5, 20)
     c1, r1, it1, *_ = ll.locate(q, stats=True)
     torch.cuda.synchronize()
-    hit = (c0 >= 0) & (c1 >= 0)
+    hit = (c0 >= 0) & (c1 >= 0) & (cs >= 0)
     agree = (c0 == c1).float().mean().item()
     mi0 = it0[hit].float().mean().item()
     mi1 = it1[hit].float().mean().item()
-    print(f"learned guess: mean Newton iterations {mi1:.3f} vs centre {mi0:.3f}, "
-          f"cell agreement {agree:.5f}, final loss {losses[-1]:.2e}")
+    mis = its[hit].float().mean().item()
+    print(f"order {order} learned guess: mean Newton steps {mi1:.3f}, element centre {mi0:.3f}, "
+          f"sub-box centre {mis:.3f}; cell agreement {agree:.5f}, final loss {losses[-1]:.2e}")
     assert agree > 0.999
     assert (r0[hit] - r1[hit]).abs().max().item() < 1e-5
     assert mi1 < mi0

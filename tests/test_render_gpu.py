@@ -59,12 +59,17 @@ def _volume_case(cuda, ref, mesh_name, w, samples, lighting, coherent, guess):
 
 
 def _near_face_rays(cuda, ref, m, w, samples, pixels, band=2e-4):
-    """For each pixel, whether its ray has a sample point that the
-    reference's locate puts within `band` of a face of its element (a point
-    on a face shared by two elements, which either may own within the
-    Newton tolerance).  The sample points are the reference march's:
+    """For each pixel, whether its ray has a sample point on an element
+    face: one that the reference's locate or the GPU's puts within `band`
+    of a face of its element (a face shared by two elements, which either
+    may own within the Newton tolerance), or one just outside the mesh that
+    the reference misses while Newton accepts it within the tolerance in the
+    element of the ray's previous sample (the coherent march tries that
+    element first; a BVH locate never considers a point outside every
+    leaf box).  The sample points are the reference march's:
     near + k * dt with dt = |bounds diagonal| / samples, accumulated in
     float32 (rendering/volume.cpp:89-99,148-205)."""
+    import torch
     from devil_ray_b200 import api
     from devil_ray_b200.render import Camera, cull_rays
     g = api.UnstructuredMesh(m.ctrl_idx, m.xyz, m.order, device=cuda)
@@ -78,6 +83,7 @@ def _near_face_rays(cuda, ref, m, w, samples, pixels, band=2e-4):
     mag = np.sqrt(np.float32(e[0] * e[0] + e[1] * e[1] + e[2] * e[2]), dtype=np.float32)
     dt = np.float32(mag / np.float32(samples))
     rm = ref.RefHexMesh(m.order, m.ctrl_idx, m.xyz)
+    from devil_ray_b200 import _lib as L
     out = np.zeros(len(pixels), bool)
     for k, px in enumerate(pixels):
         sel = np.nonzero(pid == px)[0]
@@ -91,9 +97,22 @@ def _near_face_rays(cuda, ref, m, w, samples, pixels, band=2e-4):
             d = np.float32(d + dt)
         if not pts:
             continue
-        cell, rr = rm.locate(np.asarray(pts, np.float32))
-        ins = rr[cell >= 0]
+        pts = np.asarray(pts, np.float32)
+        cell, rr = rm.locate(pts)
+        gc, gr = g.locate(pts, tol=1e-4, max_steps=20, guess_mode=L.GUESS_ZERO)
+        gc, gr = gc.cpu().numpy(), gr.cpu().numpy()
+        ins = np.concatenate([rr[cell >= 0], gr[gc >= 0]])
         out[k] = bool(np.any((ins < band) | (ins > 1.0 - band)))
+        if not out[k]:
+            # exits: a missed sample after a located one, solved in that element
+            j = np.nonzero((cell[1:] < 0) & (cell[:-1] >= 0))[0] + 1
+            if j.size:
+                from devil_ray_b200.learned import newton_pairs
+                el = torch.as_tensor(cell[j - 1], dtype=torch.int32, device=cuda)
+                p = torch.as_tensor(pts[j], device=cuda)
+                x, _, _ = newton_pairs(g, el, p, 1e-5, 20)
+                x = x.cpu().numpy()
+                out[k] = bool(np.any(np.all((x > -band) & (x < 1.0 + band), axis=1)))
     return out
 
 
