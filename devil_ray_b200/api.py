@@ -272,7 +272,7 @@ class BatchedLocator:
     def _bvh(self, stream=None) -> BVH:
         b = self.bvh if self.bvh is not None else self.mesh.get_bvh(stream)
         if (self.guess_mode == L.GUESS_SUBBOX_LINEAR and b.leaf_maps is None
-                and self.mesh.shape == L.SHAPE_TENSOR and self.mesh.dim == 3):
+                and self.mesh.dim == 3):
             b.build_leaf_maps(self.mesh, stream)
         return b
 

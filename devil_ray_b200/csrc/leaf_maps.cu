@@ -7,24 +7,28 @@
 //   x0 = c + J(c)^-1 (p - X(c))
 // lands about one quadratic Newton step closer to the solution.  The map of
 // each leaf, (c, X(c), J(c)^-1), is evaluated once per BVH by this kernel
-// and read by the locate kernels as four float4 per candidate.  No
-// reference counterpart.
+// and read by the locate kernels as four float4 per candidate.  Hexes take
+// the centre of the leaf's reference box, tets the centroid of its
+// sub-simplex (subref_center, data_model/subref.hpp:39-48).  No reference
+// counterpart.
 #include "bernstein.cuh"
 #include "drb_common.cuh"
 #include "drb_internal.h"
 #include "newton.cuh"
+#include "simplex.cuh"
 
 namespace drb
 {
 namespace
 {
 
-template <int P, class CP>
+template <int P, bool TET, class CP>
 DRB_D void write_leaf_map (const CP &cp, const float (&origin)[3], const float (&c)[3],
                            float4 *__restrict__ out)
 {
   float X[3], Ju[3], Jv[3], Jw[3];
-  hex_eval_d<P, 3> (cp, c[0], c[1], c[2], X, Ju, Jv, Jw);
+  if (TET) tet_eval_d<P, 3> (cp, c[0], c[1], c[2], X, Ju, Jv, Jw);
+  else hex_eval_d<P, 3> (cp, c[0], c[1], c[2], X, Ju, Jv, Jw);
   // J: rows physical x, y, z; columns d/du, d/dv, d/dw.  Inverse by
   // cofactors in double (a once-per-leaf cost).
   const double a = Ju[0], b = Jv[0], cc = Jw[0];
@@ -55,19 +59,31 @@ DRB_D void write_leaf_map (const CP &cp, const float (&origin)[3], const float (
   out[3] = make_float4 (inv[6], inv[7], inv[8], 0.f);
 }
 
-template <int P>
+template <int P, bool TET>
 __global__ void leaf_maps_kernel (const float *__restrict__ packed, int stride,
                                   const int *__restrict__ ctrl_idx, const float *__restrict__ xyz,
                                   const int *__restrict__ leaf_nodes, const int *__restrict__ aabb_ids,
                                   const float *__restrict__ ref_boxes, int n_leaf,
                                   float4 *__restrict__ maps)
 {
-  constexpr int ND = (P + 1) * (P + 1) * (P + 1);
+  constexpr int ND = TET ? tet_dofs<P> () : (P + 1) * (P + 1) * (P + 1);
   const int k = blockIdx.x * blockDim.x + threadIdx.x;
   if (k >= n_leaf) return;
   const int el = __ldg (leaf_nodes + k);
-  const float *rb = ref_boxes + 6 * (size_t)__ldg (aabb_ids + k);
-  const float c[3] = { (rb[0] + rb[3]) * 0.5f, (rb[1] + rb[4]) * 0.5f, (rb[2] + rb[5]) * 0.5f };
+  float c[3];
+  if (TET)
+  {
+    // sub-simplex vertices: origin, then the u, v, w axis vertices
+    const float *rb = ref_boxes + 12 * (size_t)__ldg (aabb_ids + k);
+#pragma unroll
+    for (int d = 0; d < 3; ++d) c[d] = (rb[d] + rb[3 + d] + rb[6 + d] + rb[9 + d]) * 0.25f;
+  }
+  else
+  {
+    const float *rb = ref_boxes + 6 * (size_t)__ldg (aabb_ids + k);
+#pragma unroll
+    for (int d = 0; d < 3; ++d) c[d] = (rb[d] + rb[3 + d]) * 0.5f;
+  }
   if (packed)
   {
     // packed rows hold coordinates relative to the element's first control
@@ -75,12 +91,12 @@ __global__ void leaf_maps_kernel (const float *__restrict__ packed, int stride,
     const float *row = packed + (size_t)el * stride;
     const float origin[3] = { row[packed_origin (ND)], row[packed_origin (ND) + 1],
                               row[packed_origin (ND) + 2] };
-    write_leaf_map<P> (PackedCP{ row }, origin, c, maps + 4 * (size_t)k);
+    write_leaf_map<P, TET> (PackedCP{ row }, origin, c, maps + 4 * (size_t)k);
   }
   else
   {
     const float origin[3] = { 0.f, 0.f, 0.f };
-    write_leaf_map<P> (IndirectCP{ ctrl_idx + (size_t)el * ND, xyz, 3 }, origin, c,
+    write_leaf_map<P, TET> (IndirectCP{ ctrl_idx + (size_t)el * ND, xyz, 3 }, origin, c,
                        maps + 4 * (size_t)k);
   }
 }
@@ -98,10 +114,10 @@ extern "C" int drb_bvh_leaf_maps (const drb_mesh *mesh, const drb_bvh *bvh, floa
     set_last_error ("bvh_leaf_maps: bad arguments");
     return DRB_ERR_INVALID_ARG;
   }
-  if (mesh->shape != DRB_SHAPE_TENSOR || mesh->dim != 3 || mesh->ncomp != 3 || mesh->order < 1 ||
-      mesh->order > 3)
+  if ((mesh->shape != DRB_SHAPE_TENSOR && mesh->shape != DRB_SHAPE_SIMPLEX) || mesh->dim != 3 ||
+      mesh->ncomp != 3 || mesh->order < 1 || mesh->order > 3)
   {
-    set_last_error ("bvh_leaf_maps: needs a hex geometry mesh of order 1..3");
+    set_last_error ("bvh_leaf_maps: needs a hex or tet geometry mesh of order 1..3");
     return DRB_ERR_UNSUPPORTED;
   }
   if (reinterpret_cast<uintptr_t> (maps) % 16)
@@ -114,10 +130,14 @@ extern "C" int drb_bvh_leaf_maps (const drb_mesh *mesh, const drb_bvh *bvh, floa
   cudaStream_t s = (cudaStream_t)stream;
   const int stride = packed_stride (mesh_nd (mesh), 3);
   const int blocks = div_up (n, 128);
-#define DRB_LM(P) leaf_maps_kernel<P><<<blocks, 128, 0, s>>> (mesh->packed, stride, mesh->ctrl_idx, mesh->values, bvh->leaf_nodes, bvh->aabb_ids, bvh->ref_boxes, n, (float4 *)maps)
-  if (mesh->order == 1) DRB_LM (1);
-  else if (mesh->order == 2) DRB_LM (2);
-  else DRB_LM (3);
+  const bool tet = mesh->shape == DRB_SHAPE_SIMPLEX;
+#define DRB_LM(P, T) leaf_maps_kernel<P, T><<<blocks, 128, 0, s>>> (mesh->packed, stride, mesh->ctrl_idx, mesh->values, bvh->leaf_nodes, bvh->aabb_ids, bvh->ref_boxes, n, (float4 *)maps)
+  if (tet && mesh->order == 1) DRB_LM (1, true);
+  else if (tet && mesh->order == 2) DRB_LM (2, true);
+  else if (tet) DRB_LM (3, true);
+  else if (mesh->order == 1) DRB_LM (1, false);
+  else if (mesh->order == 2) DRB_LM (2, false);
+  else DRB_LM (3, false);
 #undef DRB_LM
   return check_launch ("leaf_maps_kernel");
 }

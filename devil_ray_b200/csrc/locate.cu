@@ -82,8 +82,7 @@ extern "C" int drb_locate (const drb_mesh *mesh, const drb_bvh *bvh, const float
   lp.max_steps = opts->max_steps;
   lp.guess_mode = opts->guess_mode;
   lp.guess = opts->guess;
-  lp.leaf_maps = (mesh->shape == DRB_SHAPE_TENSOR && mesh->dim == 3)
-                 ? (const float4 *)bvh->leaf_maps : nullptr;
+  lp.leaf_maps = mesh->dim == 3 ? (const float4 *)bvh->leaf_maps : nullptr;
   cudaStream_t s = (cudaStream_t)stream;
   const int blocks = div_up (n, 128);
 #define DRB_LK(P, S) locate_kernel<P, S><<<blocks, 128, 0, s>>> (lp, pts, n, cell, ref, stats.iters, stats.candidates, stats.nodes)

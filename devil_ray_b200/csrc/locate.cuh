@@ -320,9 +320,11 @@ DRB_D void candidate_guess (const LocateParams &lp, int leaf, long long qi, bool
   {
     x[0] = x[1] = x[2] = 0.f;
   }
-  else if (lp.guess_mode == DRB_GUESS_SUBBOX_LINEAR && S == kTensor && lp.leaf_maps)
+  else if (lp.guess_mode == DRB_GUESS_SUBBOX_LINEAR && (S == kTensor || S == kSimplex) &&
+           lp.leaf_maps)
   {
-    // the element map linearised at the leaf's sub-box centre c:
+    // the element map linearised at the leaf's sub-box centre (a tet's:
+    // its sub-simplex centroid) c:
     // x = c + J(c)^-1 (p - X(c)); record (c, X(c), J^-1 row-major, 0)
     const float4 *m = lp.leaf_maps + 4 * (size_t)leaf;
     const float4 a = __ldg (m), b = __ldg (m + 1), c = __ldg (m + 2), d = __ldg (m + 3);

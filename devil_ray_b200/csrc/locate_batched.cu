@@ -533,8 +533,7 @@ LocateParams make_params (const drb_mesh *mesh, const drb_bvh *bvh, const drb_ne
   lp.guess = opts->guess;
   lp.hull = (mesh->shape == DRB_SHAPE_SIMPLEX && mesh->dim == 3) ? (const float4 *)mesh->hull_planes
                                                                    : nullptr;
-  lp.leaf_maps = (mesh->shape == DRB_SHAPE_TENSOR && mesh->dim == 3) ? (const float4 *)bvh->leaf_maps
-                                                                     : nullptr;
+  lp.leaf_maps = mesh->dim == 3 ? (const float4 *)bvh->leaf_maps : nullptr;
   return lp;
 }
 

@@ -330,6 +330,7 @@ struct VolumeParams
   int n_lights;
   int use_lighting;
   int coherent;
+  int quadratic_predictor;    // coherent mode 2: r_{k-1} + 2 J^-1 dx
   float sample_dist;
   int cull;
   CullBox box;
@@ -524,8 +525,9 @@ DRB_D int step_across (const VolumeParams &vp, int el, int f, float (&x)[3])
 // prediction outside the previous element goes straight to the BVH.
 template <int P, bool WIDE, int S = kTensor>
 DRB_D int locate_sample (const VolumeParams &vp, const float (&pt)[3], const float (&step)[3],
-                         int prev_el, const float (&prev_ref)[3], LU3 &lu, float (&ref)[3],
-                         int &iters, int &cands, int &nodes)
+                         int prev_el, const float (&prev_ref)[3], bool prev2_ok,
+                         const float (&prev2_ref)[3], LU3 &lu, float (&ref)[3], int &iters,
+                         int &cands, int &nodes)
 {
   int todo[TraversalStack<WIDE>::kDepth];
   int sp = 0, cur = 0;
@@ -535,11 +537,24 @@ DRB_D int locate_sample (const VolumeParams &vp, const float (&pt)[3], const flo
   float x[3];
   if (vp.coherent && prev_el >= 0)
   {
+    // predictor along the ray: r + J^-1 dx from the previous sample's
+    // factorised Jacobian, or, when the two previous samples lie in the same
+    // element, r_{k-1} + 2 J_k^-1 dx, which is exact where the reference
+    // point moves quadratically in the ray parameter
     float dr[3];
     lu.solve (step, dr);
-    x[0] = prev_ref[0] + dr[0];
-    x[1] = prev_ref[1] + dr[1];
-    x[2] = prev_ref[2] + dr[2];
+    if (prev2_ok)
+    {
+      x[0] = prev2_ref[0] + 2.f * dr[0];
+      x[1] = prev2_ref[1] + 2.f * dr[1];
+      x[2] = prev2_ref[2] + 2.f * dr[2];
+    }
+    else
+    {
+      x[0] = prev_ref[0] + dr[0];
+      x[1] = prev_ref[1] + dr[1];
+      x[2] = prev_ref[2] + dr[2];
+    }
     if (S == kSimplex ? is_inside_simplex (x, kCoherentMargin) : is_inside_ref (x, kCoherentMargin))
     {
       el = prev_el;
@@ -605,6 +620,8 @@ struct RayMarch
   float first_depth;
   int prev_el;
   float prev_ref[3];
+  bool prev2_ok;      // the sample before prev was in prev_el too
+  float prev2_ref[3];
   int n_samples, iters, cands, nodes;
 };
 
@@ -726,6 +743,8 @@ volume_kernel (VolumeParams vp, const Ray *__restrict__ rays, int n_rays, int *_
         s.seg_depth = 0.f;
         s.prev_el = -1;
         s.prev_ref[0] = s.prev_ref[1] = s.prev_ref[2] = 0.5f;
+        s.prev2_ok = false;
+        s.prev2_ref[0] = s.prev2_ref[1] = s.prev2_ref[2] = 0.5f;
         s.n_samples = s.iters = s.cands = s.nodes = 0;
         step[0] = s.ray.dir.x * vp.sample_dist;
         step[1] = s.ray.dir.y * vp.sample_dist;
@@ -744,8 +763,8 @@ volume_kernel (VolumeParams vp, const Ray *__restrict__ rays, int n_rays, int *_
                           s.ray.orig.y + s.distance * s.ray.dir.y,
                           s.ray.orig.z + s.distance * s.ray.dir.z };
     float ref[3];
-    const int el = locate_sample<P, WIDE, S> (vp, pt, step, s.prev_el, s.prev_ref, lu, ref, s.iters,
-                                              s.cands, s.nodes);
+    const int el = locate_sample<P, WIDE, S> (vp, pt, step, s.prev_el, s.prev_ref, s.prev2_ok,
+                                              s.prev2_ref, lu, ref, s.iters, s.cands, s.nodes);
     bool done = false;
     if (el >= 0)
     {
@@ -758,6 +777,10 @@ volume_kernel (VolumeParams vp, const Ray *__restrict__ rays, int n_rays, int *_
       ++s.n_samples;
       const float4 sc = shade_sample<P, S> (vp, el, ref, s.ray, lu, pt);
       blend (s.color, sc);
+      s.prev2_ok = vp.quadratic_predictor && el == s.prev_el;
+      s.prev2_ref[0] = s.prev_ref[0];
+      s.prev2_ref[1] = s.prev_ref[1];
+      s.prev2_ref[2] = s.prev_ref[2];
       s.prev_el = el;
       s.prev_ref[0] = ref[0];
       s.prev_ref[1] = ref[1];
@@ -773,6 +796,7 @@ volume_kernel (VolumeParams vp, const Ray *__restrict__ rays, int n_rays, int *_
     else
     {
       s.prev_el = -1;
+      s.prev2_ok = false;
       if (s.in_seg)
       {
         end_segment (s, partials);
@@ -1154,8 +1178,7 @@ static int volume_common (const drb_mesh *mesh, const drb_mesh *field, const drb
   lp.max_steps = no.max_steps;
   lp.guess_mode = no.guess_mode;
   lp.guess = nullptr;
-  lp.leaf_maps = (mesh->shape == DRB_SHAPE_TENSOR && mesh->dim == 3)
-                 ? (const float4 *)bvh->leaf_maps : nullptr;
+  lp.leaf_maps = mesh->dim == 3 ? (const float4 *)bvh->leaf_maps : nullptr;
   vp.field_packed = field->packed;
   vp.field_idx = field->ctrl_idx;
   vp.field_vals = field->values;
@@ -1174,7 +1197,8 @@ static int volume_common (const drb_mesh *mesh, const drb_mesh *field, const drb
   vp.lights = (const PointLight *)lights;
   vp.n_lights = n_lights;
   vp.use_lighting = o->use_lighting;
-  vp.coherent = o->coherent;
+  vp.coherent = o->coherent != 0;
+  vp.quadratic_predictor = o->coherent == 2;
   vp.cull = o->cull;
   vp.box = cull_box (bvh->bounds);
   // sample distance: |bounds diagonal| / samples (volume.cpp:89-91)

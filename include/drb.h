@@ -44,8 +44,9 @@ enum drb_guess_mode
    * intended guess (device_mesh.hpp:161-162). */
   DRB_GUESS_SUBREF_CENTER = 2,
   /* the element map linearised at the candidate leaf's reference sub-box
-   * centre c: x0 = c + J(c)^-1 (p - X(c)), from the per-leaf maps of
-   * drb_bvh_leaf_maps (hex meshes; without them, as DRB_GUESS_SUBREF_CENTER).
+   * centre c (a tet's: its sub-simplex centroid): x0 = c + J(c)^-1 (p - X(c)),
+   * from the per-leaf maps of drb_bvh_leaf_maps (3D meshes; without them,
+   * and on 2D meshes, as DRB_GUESS_SUBREF_CENTER).
    * No reference counterpart: the reference's guess is its sub-box centre. */
   DRB_GUESS_SUBBOX_LINEAR = 4,
   /* caller-provided guess per point for its first candidate element (e.g.
@@ -138,9 +139,10 @@ typedef struct drb_bvh
   float *leaf_maps;      /* device float[16 * n_leaf] */
 } drb_bvh;
 
-/* Per-leaf linearisation of a hex mesh's element maps for
+/* Per-leaf linearisation of a hex or tet mesh's element maps for
  * DRB_GUESS_SUBBOX_LINEAR: for sorted leaf k with element e and reference
- * sub-box centre c, maps[16 k ..] = (c, X_e(c), J_e(c)^-1 row-major, 0),
+ * sub-box centre c (tets: the mean of the sub-simplex's four vertices),
+ * maps[16 k ..] = (c, X_e(c), J_e(c)^-1 row-major, 0),
  * X in absolute coordinates.  A leaf whose Jacobian is singular gets a zero
  * inverse (the guess is then c).  No reference counterpart. */
 int drb_bvh_leaf_maps (const drb_mesh *mesh, const drb_bvh *bvh, float *maps, void *stream);
@@ -395,7 +397,11 @@ typedef struct drb_volume_opts
   float tol;              /* Newton tolerance (reference: 1e-4) */
   int max_steps;          /* Newton steps (reference: 20) */
   int guess_mode;         /* drb_guess_mode for full locates */
-  int coherent;           /* 1: try the previous sample's element first */
+  int coherent;           /* 1: try the previous sample's element first,
+                             from r + J^-1 dx (the previous sample's point
+                             and factorised Jacobian); 2: as 1, from
+                             r_{k-1} + 2 J^-1 dx when the two previous
+                             samples lie in the same element */
   float bounds[6];        /* Collection::bounds of the data (sample distance) */
   int cull;               /* 1: rays are raw camera rays; the march applies the
                              slab test of remove_missed_rays itself (no

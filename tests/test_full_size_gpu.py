@@ -132,23 +132,26 @@ def test_c4_volume_full_size_properties(cuda):
     vol.color_map().samples(1024)
     vol.tol = 1e-5
     imgs, samples = [], []
-    for coherent in (True, False):
+    # coherent with the first-order and the quadratic predictor, then plain
+    for coherent in (1, 2, 0):
         vol.coherent = coherent
         vol.guess_mode = L.GUESS_ELEM_CENTER
         fb, st = vol.render(cam, [light], stats=True)
         torch.cuda.synchronize()
         imgs.append(fb.colors.cpu().numpy())      # before the background composite
         samples.append(int(st[0].long().sum()))
-    a, pl = imgs
-    assert np.all((a >= 0) & (a <= 1))
-    d = np.abs(a - pl)
-    bad = np.any(d > 1.0 / 255.0, axis=-1)
-    print(f"C4: coherent vs plain march, {bad.sum()} of {w * w} pixels differ by > 1/255, "
-          f"max {d.max():.2e}; samples {samples[0]} vs {samples[1]}")
-    assert bad.mean() < 0.005
-    # the blobs cover part of the view; both marches take the same samples
-    assert (a[:, 3] > 0.01).mean() > 0.05
-    assert abs(samples[0] - samples[1]) < 1e-5 * samples[1]
+    pl = imgs[-1]
+    for k, a in enumerate(imgs[:2]):
+        assert np.all((a >= 0) & (a <= 1))
+        d = np.abs(a - pl)
+        bad = np.any(d > 1.0 / 255.0, axis=-1)
+        print(f"C4: coherent (predictor {k + 1}) vs plain march, {bad.sum()} of {w * w} "
+              f"pixels differ by > 1/255, max {d.max():.2e}; samples {samples[k]} vs "
+              f"{samples[-1]}")
+        assert bad.mean() < 0.005
+        # the blobs cover part of the view; both marches take the same samples
+        assert (a[:, 3] > 0.01).mean() > 0.05
+        assert abs(samples[k] - samples[-1]) < 1e-5 * samples[-1]
 
 
 def test_c3_second_mesh_d25(cuda, ref):

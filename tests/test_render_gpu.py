@@ -116,7 +116,7 @@ def _near_face_rays(cuda, ref, m, w, samples, pixels, band=2e-4):
     return out
 
 
-@pytest.mark.parametrize("coherent", [False, True])
+@pytest.mark.parametrize("coherent", [0, 1, 2])
 @pytest.mark.parametrize("lighting", [True, False])
 def test_volume_image_matches_reference(cuda, ref, coherent, lighting):
     """Images within 1/255 per channel, except pixels whose ray samples a
