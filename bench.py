@@ -87,18 +87,40 @@ def dist_info():
 
 
 class ClockSampler:
-    """nvidia-smi clock/throttle samples while the timed region runs."""
+    """SM clock and throttle-reason samples while the timed region runs:
+    NVML polled every 5 ms from a thread (the first sample is taken before
+    start() returns), else nvidia-smi at its 100 ms period."""
 
     QUERY = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+    # NVML clocks-event reasons reported, by pynvml constant name
+    REASONS = {"sw_power_cap": "nvmlClocksEventReasonSwPowerCap",
+               "hw_slowdown": "nvmlClocksEventReasonHwSlowdown",
+               "sw_thermal_slowdown": "nvmlClocksEventReasonSwThermalSlowdown",
+               "hw_thermal_slowdown": "nvmlClocksEventReasonHwThermalSlowdown"}
 
     def __init__(self, gpu_index: int):
         self.idx = gpu_index
         self.proc = None
         self.lines = []
+        self.nvml = None
+        self.samples = []
+        self._stop = threading.Event()
 
     def start(self):
+        try:
+            import pynvml as N
+            N.nvmlInit()
+            h = N.nvmlDeviceGetHandleByIndex(self.idx)
+            self.max_mhz = float(N.nvmlDeviceGetMaxClockInfo(h, N.NVML_CLOCK_SM))
+            self.nvml = (N, h)
+            self._poll_once()
+            self._t = threading.Thread(target=self._poll, daemon=True)
+            self._t.start()
+            return
+        except Exception:
+            self.nvml = None
         try:
             self.proc = subprocess.Popen(
                 ["nvidia-smi", f"--id={self.idx}", f"--query-gpu={self.QUERY}",
@@ -109,11 +131,40 @@ class ClockSampler:
         except FileNotFoundError:
             self.proc = None
 
+    def _poll_once(self):
+        N, h = self.nvml
+        sm = float(N.nvmlDeviceGetClockInfo(h, N.NVML_CLOCK_SM))
+        try:
+            bits = int(N.nvmlDeviceGetCurrentClocksEventReasons(h))
+        except AttributeError:
+            bits = int(N.nvmlDeviceGetCurrentClocksThrottleReasons(h))
+        self.samples.append((sm, bits))
+
+    def _poll(self):
+        while not self._stop.wait(0.005):
+            try:
+                self._poll_once()
+            except Exception:
+                return
+
     def _read(self):
         for line in self.proc.stdout:
             self.lines.append(line.strip())
 
     def stop(self):
+        if self.nvml is not None:
+            self._stop.set()
+            self._t.join(timeout=1)
+            try:
+                self._poll_once()
+            except Exception:
+                pass
+            sm = [x for x, _ in self.samples]
+            N = self.nvml[0]
+            reasons = sorted(name for name, const in self.REASONS.items()
+                             if any(b & getattr(N, const) for _, b in self.samples))
+            return {"sm_mhz": float(np.median(sm)), "sm_max_mhz": self.max_mhz,
+                    "reasons": reasons, "samples": len(sm), "source": "NVML, 5 ms period"}
         if self.proc is None:
             return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
         self.proc.terminate()
@@ -136,7 +187,7 @@ class ClockSampler:
                 if v.lower().startswith("active"):
                     reasons.add(name)
         return {"sm_mhz": float(np.median(sm)) if sm else None, "sm_max_mhz": mx,
-                "reasons": sorted(reasons), "samples": len(sm)}
+                "reasons": sorted(reasons), "samples": len(sm), "source": "nvidia-smi, 100 ms"}
 
 
 WORKLOAD_DESC = ("locate_64: 64^3 hex order 2, trilinear distortion 15%, 16M uniform queries "
@@ -984,7 +1035,8 @@ def profile_volume(dev, args):
     print(json.dumps({"profile_volume": args.profile_volume, "coherent": args.coherent,
                       "ms_per_frame": ms,
                       "samples": samples, "samples_per_s": samples / (ms * 1e-3),
-                      "mean_iters_per_sample": float(st[1].long().sum()) / max(samples, 1)}))
+                      "mean_iters_per_sample": float(st[1].long().sum()) / max(samples, 1),
+                      "mean_solves_per_sample": float(st[2].long().sum()) / max(samples, 1)}))
     return 0
 
 

@@ -281,8 +281,8 @@ class BatchedLocator:
         best = L.DrbLocateConfig()
         ms = C.c_float()
         opts = L.DrbNewtonOpts(self.tol, self.max_steps, self.guess_mode, None)
+        bd = self._bvh(stream).desc()  # first: it may add the mesh's hull planes
         d = self.mesh.desc()
-        bd = self._bvh(stream).desc()
         L.check(L.lib().drb_locate_tune(C.byref(d), C.byref(bd), _ptr(pts), pts.shape[0],
                                         C.byref(opts), C.byref(best), C.byref(ms),
                                         _stream(stream)), "drb_locate_tune")
@@ -316,8 +316,8 @@ class BatchedLocator:
         dev = self.mesh.device
         opts = L.DrbNewtonOpts(self.tol, self.max_steps, self.guess_mode, None)
         cfg = None if self.config is None else C.byref(self.config)
+        bd = self._bvh(stream).desc()  # first: it may add the mesh's hull planes
         d = self.mesh.desc()
-        bd = self._bvh(stream).desc()
         if records:
             res = torch.empty((n, 4), dtype=torch.float32, device=dev) if out is None else out
             cell = ref = None
@@ -344,8 +344,8 @@ class BatchedLocator:
         opts = L.DrbNewtonOpts(self.tol, self.max_steps, mode,
                                None if guess is None else guess.data_ptr())
         cfg = None if self.config is None else C.byref(self.config)
+        bd = self._bvh(stream).desc()  # first: it may add the mesh's hull planes
         d = self.mesh.desc()
-        bd = self._bvh(stream).desc()
         if order is None:
             L.check(L.lib().drb_locate_batched(C.byref(d), C.byref(bd), _ptr(pts), n,
                                                C.byref(opts), cfg, _ptr(cell), _ptr(ref), qs,
@@ -376,8 +376,8 @@ class BatchedLocator:
         n = host_points.shape[0]
         opts = L.DrbNewtonOpts(self.tol, self.max_steps, self.guess_mode, None)
         cfg = None if self.config is None else C.byref(self.config)
+        bd = self._bvh(stream).desc()  # first: it may add the mesh's hull planes
         d = self.mesh.desc()
-        bd = self._bvh(stream).desc()
         L.check(L.lib().drb_locate_host(C.byref(d), C.byref(bd), _ptr(host_points), n,
                                         C.byref(opts), cfg, chunk, _ptr(cell), _ptr(ref),
                                         _stream(stream)), "drb_locate_host")

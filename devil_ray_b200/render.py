@@ -285,9 +285,10 @@ class Volume:
         rng = self._range()
         np_ = C.c_int()
         st, rs = self._stats(n, stats)
+        bd = self.mesh.get_bvh().desc()  # first: it may add the mesh's hull planes
         L.check(L.lib().drb_volume_integrate(
             C.byref(self.mesh.desc()), C.byref(self.field_.desc()),
-            C.byref(self.mesh.get_bvh().desc()), _ptr(active), n, C.byref(o), _ptr(tf),
+            C.byref(bd), _ptr(active), n, C.byref(o), _ptr(tf),
             tf.shape[0], rng.ctypes.data_as(C.c_void_p), _ptr(lt), len(lights), _ptr(parts),
             C.byref(np_), rs, _stream(stream)), "drb_volume_integrate")
         out = parts[: np_.value]
@@ -317,9 +318,10 @@ class Volume:
         tf = self._tf()
         rng = self._range()
         st, rs = self._stats(n, stats)
+        bd = self.mesh.get_bvh().desc()  # first: it may add the mesh's hull planes
         L.check(L.lib().drb_volume_render(
             C.byref(self.mesh.desc()), C.byref(self.field_.desc()),
-            C.byref(self.mesh.get_bvh().desc()), _ptr(active), n, C.byref(o), _ptr(tf),
+            C.byref(bd), _ptr(active), n, C.byref(o), _ptr(tf),
             tf.shape[0], rng.ctypes.data_as(C.c_void_p), _ptr(lt), len(lights),
             _ptr(fb.colors), _ptr(fb.depths), rs, _stream(stream)), "drb_volume_render")
         return (fb, st) if stats else fb

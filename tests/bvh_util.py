@@ -116,3 +116,30 @@ def widen(inner: np.ndarray):
                     codes[w, k] = g if g < 0 else wid[g // 4]
                     k += 1
     return boxes, codes.astype(np.int32)
+
+
+def leaf_maps_fp64(shape: str, p: int, ctrl_idx, xyz, bvh, leaves):
+    """FP64 restatement of drb_bvh_leaf_maps for the given sorted leaves:
+    (c, X(c), J(c)^-1 row-major) with c the sub-box centre (hex) or the mean
+    of the sub-simplex's four vertices (tet), in the float32 arithmetic of
+    the kernel."""
+    from oracle import restate
+    nd = (p + 1) ** 3 if shape == "hex" else (p + 1) * (p + 2) * (p + 3) // 6
+    ci = np.asarray(ctrl_idx).reshape(-1, nd)
+    els = bvh.leaf_nodes.cpu().numpy()[leaves]
+    ids = bvh.aabb_ids.cpu().numpy()[leaves]
+    rb = bvh.ref_boxes.cpu().numpy()
+    out = np.zeros((len(leaves), 15))
+    for k, (e, a) in enumerate(zip(els, ids)):
+        if shape == "hex":
+            b = rb.reshape(-1, 6)[a]
+            c = ((b[:3] + b[3:]) * np.float32(0.5)).astype(np.float32)
+            X, J = restate.hex_eval_d(p, xyz[ci[e]], c)
+        else:
+            b = rb.reshape(-1, 12)[a].reshape(4, 3)
+            c = ((b[0] + b[1] + b[2] + b[3]) * np.float32(0.25)).astype(np.float32)
+            X, J = restate.tet_eval_d(p, xyz[ci[e]], c)
+        out[k, :3] = c
+        out[k, 3:6] = X[0]
+        out[k, 6:] = np.linalg.inv(J[0].T).ravel()
+    return out

@@ -324,6 +324,27 @@ def test_autotuner_config_is_valid_and_exact(cuda):
     assert torch.equal(r0.view(torch.int32), r1.view(torch.int32))
 
 
+@pytest.mark.parametrize("name", ["trilinear_12", "p3_10", "p1_9"])
+def test_leaf_maps_match_fp64(cuda, name):
+    """drb_bvh_leaf_maps on a hex mesh: each sampled leaf's record holds its
+    sub-box centre, the element map there and the inverse Jacobian, against
+    an FP64 evaluation of the same element at the same point."""
+    import torch
+    from tests.bvh_util import leaf_maps_fp64
+    m, _, g = _setup(cuda, name, 16, 1)
+    b = g.get_bvh()
+    b.build_leaf_maps(g)
+    torch.cuda.synchronize()
+    maps = b.leaf_maps.cpu().numpy()
+    leaves = np.random.default_rng(6).choice(b.n_leaf, 3000, replace=False)
+    want = leaf_maps_fp64("hex", m.order, m.ctrl_idx, m.xyz, b, leaves)
+    got = maps[leaves, :15]
+    assert np.array_equal(got[:, :3], want[:, :3].astype(np.float32))
+    assert np.abs(got[:, 3:6] - want[:, 3:6]).max() < 1e-5
+    scale = np.abs(want[:, 6:]).max(axis=1, keepdims=True)
+    assert (np.abs(got[:, 6:] - want[:, 6:]) / scale).max() < 1e-4
+
+
 @pytest.mark.parametrize("name", ["trilinear_12", "trilinear_12_d25", "p3_10", "p1_9"])
 def test_subbox_linear_guess(cuda, name):
     """The first guess from each leaf's linearised element map

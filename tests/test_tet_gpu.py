@@ -161,6 +161,28 @@ def test_tet_batched_identical_to_plain(cuda, p, row_mode):
 
 
 @pytest.mark.parametrize("p", ORDERS)
+def test_tet_leaf_maps_match_fp64(cuda, p):
+    """drb_bvh_leaf_maps on a tet mesh: each sampled leaf's record holds its
+    sub-simplex centroid, the element map there and the inverse Jacobian,
+    against an FP64 evaluation of the same element at the same point."""
+    import torch
+    from tests.bvh_util import leaf_maps_fp64
+    m = _mesh(p)
+    g = _gpu(m, cuda)
+    b = g.get_bvh()
+    b.build_leaf_maps(g)
+    torch.cuda.synchronize()
+    maps = b.leaf_maps.cpu().numpy()
+    leaves = np.random.default_rng(5).choice(b.n_leaf, 3000, replace=False)
+    want = leaf_maps_fp64("tet", p, m.ctrl_idx, m.xyz, b, leaves)
+    got = maps[leaves, :15]
+    assert np.array_equal(got[:, :3], want[:, :3].astype(np.float32))
+    assert np.abs(got[:, 3:6] - want[:, 3:6]).max() < 1e-5
+    scale = np.abs(want[:, 6:]).max(axis=1, keepdims=True)
+    assert (np.abs(got[:, 6:] - want[:, 6:]) / scale).max() < 1e-4
+
+
+@pytest.mark.parametrize("p", ORDERS)
 def test_tet_subbox_linear_guess(cuda, p):
     """The first guess from each leaf's element map linearised at its
     sub-simplex centroid (GUESS_SUBBOX_LINEAR on a tet mesh) finds the same
