@@ -469,17 +469,13 @@ DRB_D void blend (float4 &front, const float4 &back)
   front.w = alpha + front.w;
 }
 
-// A predicted reference point this far outside [0,1]^3 means the sample
-// has left the previous element: go straight to the BVH.
+// A predicted reference point outside the previous element means the sample
+// has left it.  Hexes with a face table step across the exit face at once
+// (margin 0: the face walk comes back if the prediction was off); without
+// one, and for tets (whose next stop is the BVH), a prediction within this
+// margin is solved in the previous element first.
 constexpr float kCoherentMargin = 0.1f;
 
-// Locate one sample.  Coherent mode first tries the previous sample's
-// element, starting from a predictor step r_prev + J^-1 (pt - pt_prev) with
-// the previous solve's Jacobian (lu), so that the solve usually converges in
-// two steps; then, or in plain mode, the BVH candidates in the reference's
-// order (same acceptance rule either way).  All candidates go through one
-// Newton call site, which keeps the kernel's code small.  On success lu
-// holds the located solve's Jacobian.
 // Face by which a reference point outside [0,1]^3 leaves the element (the
 // axis with the largest excursion; faces u0, u1, v0, v1, w0, w1), -1 inside.
 DRB_D int exit_face (const float (&x)[3])
@@ -517,12 +513,15 @@ DRB_D int step_across (const VolumeParams &vp, int el, int f, float (&x)[3])
 // element, starting from a predictor step r_prev + J^-1 (pt - pt_prev) with
 // the previous solve's Jacobian (lu), so that the solve usually converges in
 // two steps.  When the prediction (or that solve) leaves the element, the
-// element across the exit face is tried once (face-neighbour table).  Then,
+// element across the exit face is tried (face-neighbour table), and from its
+// solve the next one, up to kFaceSteps elements (a ray passing near an edge
+// or a corner crosses two or three faces between samples).  Then,
 // or in plain mode, the BVH candidates in the reference's order; the same
 // acceptance rule throughout.  All candidates go through one Newton call
 // site, which keeps the kernel's code small.  On success lu holds the
 // located solve's Jacobian.  Tets (S = kSimplex) have no face table: a
 // prediction outside the previous element goes straight to the BVH.
+constexpr int kFaceSteps = 3;
 template <int P, bool WIDE, int S = kTensor>
 DRB_D int locate_sample (const VolumeParams &vp, const float (&pt)[3], const float (&step)[3],
                          int prev_el, const float (&prev_ref)[3], bool prev2_ok,
@@ -533,7 +532,7 @@ DRB_D int locate_sample (const VolumeParams &vp, const float (&pt)[3], const flo
   int sp = 0, cur = 0;
   todo[0] = kBarrier;
   int el = -1, leaf = -1;
-  bool crossed = false; // the one face step of this sample is used
+  int crossed = 0; // face steps taken by this sample
   float x[3];
   if (vp.coherent && prev_el >= 0)
   {
@@ -555,14 +554,15 @@ DRB_D int locate_sample (const VolumeParams &vp, const float (&pt)[3], const flo
       x[1] = prev_ref[1] + dr[1];
       x[2] = prev_ref[2] + dr[2];
     }
-    if (S == kSimplex ? is_inside_simplex (x, kCoherentMargin) : is_inside_ref (x, kCoherentMargin))
+    const float margin = (S == kTensor && vp.nbr) ? 0.f : kCoherentMargin;
+    if (S == kSimplex ? is_inside_simplex (x, margin) : is_inside_ref (x, margin))
     {
       el = prev_el;
     }
     else
     {
       el = S == kSimplex ? -1 : step_across (vp, prev_el, exit_face (x), x);
-      crossed = true;
+      crossed = 1;
     }
   }
   while (true)
@@ -588,10 +588,10 @@ DRB_D int locate_sample (const VolumeParams &vp, const float (&pt)[3], const flo
       ref[2] = x[2];
       return el;
     }
-    if (S == kTensor && leaf < 0 && !crossed)
+    if (S == kTensor && leaf < 0 && crossed < kFaceSteps)
     {
-      // the previous element's solve ended outside it: step across
-      crossed = true;
+      // the solve ended outside its element: step across its exit face
+      ++crossed;
       el = step_across (vp, el, exit_face (x), x);
       if (el >= 0) continue;
     }
