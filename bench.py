@@ -41,6 +41,8 @@ sys.path.insert(0, str(ROOT))
 WORKLOAD = "locate_64"
 N_QUERIES = 16_777_216
 TOL = 1e-5
+# grid cells of the locate workload: half the mean leaf extent per axis
+GRID_CELL_SCALE = 0.5
 MAX_STEPS = 20
 METRIC = "located pts/s (Newton-resolved, tol 1e-5)"
 
@@ -75,6 +77,9 @@ def parse():
                          "resident), chunk, row mode, query order mode (default 1)")
     ap.add_argument("--guess", default="centre", choices=["centre", "subref", "linear"],
                     help="first guess of --profile")
+    ap.add_argument("--grid", type=float, default=0.0, metavar="SCALE",
+                    help="--profile over grid candidate lists with cells of SCALE times the "
+                         "mean leaf extent (0: the 4-wide tree)")
     ap.add_argument("--coherent", type=int, default=1, choices=[1, 2],
                     help="predictor of --profile-volume's coherent march: 1 first-order, "
                          "2 quadratic")
@@ -443,6 +448,22 @@ def surface_c1(dev, with_cpu):
                                     "cores": refpy.num_threads(), "kind": "reference",
                                     "sample": "the whole 1024^2 frame"}
     return out
+
+
+def grid_touched_entries(gbvh, pts) -> int:
+    """Entries of the grid cells that hold at least one of the points (the
+    cell of a point: clamp(floor((x - origin) * inv), 0, dims - 1) per axis
+    in float32, as the kernels compute it)."""
+    import torch
+    dims, origin, inv = gbvh.grid_geom
+    c = []
+    for d in range(3):
+        v = (pts[:, d] - torch.tensor(origin[d], dtype=torch.float32, device=pts.device)) \
+            * torch.tensor(inv[d], dtype=torch.float32, device=pts.device)
+        c.append(v.clamp(0.0, float(dims[d] - 1)).floor().long())
+    cells = torch.unique((c[2] * dims[1] + c[1]) * dims[0] + c[0])
+    st = gbvh.grid_start.long()
+    return int((st[cells + 1] - st[cells]).sum().item())
 
 
 def tet_locate(dev, args, with_cpu):
@@ -1083,6 +1104,8 @@ def main():
             loc.guess_mode = L.GUESS_SUBREF_CENTER
         elif args.guess == "linear":
             loc.guess_mode = L.GUESS_SUBBOX_LINEAR
+        if args.grid > 0:
+            loc.bvh = bvh.without_grid().build_grid(args.grid)
     else:
         best_cfg, tune_ms = loc.tune(pts[: min(n, 1 << 21)])
     cell = torch.empty(n, dtype=torch.int32, device=dev)
@@ -1138,6 +1161,7 @@ def main():
                               "located": int((cell >= 0).sum().item()),
                               "launches_per_step": launches / args.steps,
                               "kernel_ms": kern_ms, "launch": args.launch, "guess": args.guess,
+                              "grid": args.grid,
                               "gpm_dram_gbs": dr[0] if dr else None,
                               "gpm_dram_bytes_per_launch":
                                   dr[0] * 1e9 * dr[1] / args.steps if dr else None}))
@@ -1238,6 +1262,36 @@ def main():
                            "element map linearised at its sub-box centre"}
     del it_l, ca_l, nd_l
 
+    # the linear-guess locate over uniform-grid candidate lists (the same
+    # candidates in the same order as the tree walk, bit-identical results)
+    gbvh = bvh.without_grid()
+    ev0.record()
+    gbvh.build_grid(GRID_CELL_SCALE)
+    ev1.record()
+    torch.cuda.synchronize()
+    grid_build_ms = ev0.elapsed_time(ev1)
+    loc_grid = api.BatchedLocator(mesh, tol=TOL, max_steps=MAX_STEPS,
+                                  guess_mode=L.GUESS_SUBBOX_LINEAR, bvh=gbvh)
+    grid_cfg, _ = loc_grid.tune(pts[: min(n, 1 << 21)])
+    for _ in range(2):
+        loc_grid.locate(pts, out=(cell, ref))
+    grid_ms = timed(lambda: loc_grid.locate(pts, out=(cell, ref)), args.steps) / args.steps
+    grid_located = int((cell >= 0).sum().item())
+    _, _, it_g, ca_g, nd_g = loc_grid.locate(pts, stats=True)
+    grid_stats = (float(it_g.float().mean()), float(ca_g.float().mean()),
+                  float(nd_g.float().mean()))
+    grid_value = job_located(grid_located) / (grid_ms * 1e-3)
+    batched_grid = {"value": grid_value, "ms_per_step": grid_ms,
+                    "mean_newton_iters": grid_stats[0], "mean_entries_tested": grid_stats[2],
+                    "grid_build_ms": grid_build_ms, "cell_scale": GRID_CELL_SCALE,
+                    "grid_dims": list(gbvh.grid_geom[0]),
+                    "grid_entries": int(gbvh.grid_entries.shape[0]),
+                    "grid_bytes": int(gbvh.grid_entries.numel() * 4 + gbvh.grid_start.numel() * 4),
+                    "launch_config": grid_cfg.as_dict(),
+                    "note": "sub-box linear guess; candidates from the query's grid cell list "
+                            "instead of the tree walk (same candidates, same order)"}
+    del it_g, ca_g, nd_g
+
     head_name, head_locate, head_loc, head_value = ("batched (element-centre guess)", loc.locate,
                                                     loc, batched_value)
     if sub_value > head_value:
@@ -1246,11 +1300,15 @@ def main():
     if lin_value > head_value:
         head_name, head_locate, head_loc, head_value = ("batched (sub-box linear guess)",
                                                         loc_lin.locate, loc_lin, lin_value)
+    if grid_value > head_value:
+        head_name, head_locate, head_loc, head_value = ("batched (sub-box linear guess, "
+                                                        "grid candidate lists)",
+                                                        loc_grid.locate, loc_grid, grid_value)
     # the kernel of the faster batched path alone (roofline): its queries
     # already in Morton-cell order (drb_locate_ordered), the same launch shape
     roof_loc = head_loc
     roof_stats = sub_stats if roof_loc is loc_sub else lin_stats if roof_loc is loc_lin else \
-        (mean_it, mean_ca, mean_nd)
+        grid_stats if roof_loc is loc_grid else (mean_it, mean_ca, mean_nd)
     qorder = roof_loc.order(pts)
     for _ in range(2):
         roof_loc.locate(pts, order=qorder, out=(cell, ref))
@@ -1303,10 +1361,14 @@ def main():
     # packed element rows, and for the sub-box-centre guess the leaf sub-box
     # ids and reference boxes.  Repeated visits are served by the caches, so
     # these bytes are the floor of the launch's DRAM traffic.
+    # With the grid lists, the entries of the cells that hold queries replace
+    # the tree (32 B each).
     stride = L.lib().drb_packed_stride(3, m.order, 3)
     sub_guess = roof_loc is loc_sub
-    lin_guess = roof_loc is loc_lin
-    compulsory = (n * (16 + 16) + bvh.n_wide * 128 + bvh.n_leaf * 4 + m.n_elem * stride * 4
+    grid_path = roof_loc is loc_grid
+    lin_guess = roof_loc is loc_lin or grid_path
+    tree_bytes = grid_touched_entries(gbvh, pts) * 32 if grid_path else bvh.n_wide * 128
+    compulsory = (n * (16 + 16) + tree_bytes + bvh.n_leaf * 4 + m.n_elem * stride * 4
                   + (bvh.n_leaf * (4 + 24) if sub_guess else 0)
                   + (bvh.n_leaf * 64 if lin_guess else 0))
     achieved_gbs = compulsory / (kern_ms * 1e-3) / 1e9
@@ -1318,8 +1380,9 @@ def main():
     bytes_q = 12 + 16 + nd_dofs * 16 + 24 + 64 * mean_nd_binary
     r_it, r_ca, r_nd = roof_stats
     # FP32 work of the same launch: Newton steps, inside tests (6 compares
-    # per candidate) and box tests (24 compares per 4-wide node visited)
-    flops_q = r_it * newton_step_flops(m.order) + 6 * r_ca + 24 * r_nd
+    # per candidate) and box tests (24 compares per 4-wide node visited, or 6
+    # per grid entry tested)
+    flops_q = r_it * newton_step_flops(m.order) + 6 * r_ca + (6 if grid_path else 24) * r_nd
     achieved_tflops = n * flops_q / (kern_ms * 1e-3) / 1e12
     peaks = {}
     try:
@@ -1400,16 +1463,22 @@ def main():
             "dtype": "f32", "data": "synthetic",
             "config": {"workload": WORKLOAD_DESC,
                        "queries_per_gpu": n, "elements": m.n_elem, "bvh_leaves": bvh.n_leaf,
-                       "path": head_name, "launch_config": best_cfg.as_dict(),
-                       "l2": "inputs larger than L2 (201 MB queries, 553 MB BVH nodes)",
+                       "path": head_name,
+                       "launch_config": (grid_cfg if head_loc is loc_grid else best_cfg).as_dict(),
+                       "l2": "inputs larger than L2 (201 MB queries, 553 MB BVH nodes"
+                             + (f", {batched_grid['grid_bytes'] / 1e9:.1f} GB grid lists)"
+                                if grid_path else ")"),
                        "parallelism": f"replicas x{world}, queries sharded, no collective"},
             "roofline": {"bound": "hbm", "achieved": achieved_gbs, "peak": peak, "unit": "GB/s",
                          "frac": achieved_gbs / peak,
                          "traffic": traffic,
                          "achieved_bytes": "compulsory DRAM bytes per launch: 4 B order "
                                            "entry + 12 B point in and 16 B result (cell + "
-                                           "reference point) out per query, the 4-wide "
-                                           "tree, leaf ids and packed rows once"
+                                           "reference point) out per query, "
+                                           + ("the 32-byte grid entries of every cell that "
+                                              "holds a query" if grid_path else
+                                              "the 4-wide tree")
+                                           + ", leaf ids and packed rows once"
                                            + (", leaf sub-box ids and reference boxes once"
                                               if sub_guess else "")
                                            + (", the 64-byte leaf maps once" if lin_guess
@@ -1428,6 +1497,8 @@ def main():
                          "kernel_ms": kern_ms, "kernel_guess": "sub-box centre" if sub_guess
                          else "sub-box linear" if lin_guess else "element centre",
                          "launch_config": roof_loc.config.as_dict(),
+                         "kernel_traversal": "grid candidate lists" if grid_path
+                         else "4-wide tree",
                          "cache_inclusive_bytes_per_query": bytes_q,
                          "cache_inclusive_gbs": n * bytes_q / (kern_ms * 1e-3) / 1e9,
                          "fp32": {"flops_per_query": flops_q, "achieved_tflops": achieved_tflops,
@@ -1451,6 +1522,7 @@ def main():
                               "element-centre guess"},
             "batched_subref": batched_sub,
             "batched_linear": batched_lin,
+            "batched_grid": batched_grid,
             "batched": {"value": batched_value, "ms_per_step": batched_ms,
                         "note": "Morton-ordered persistent kernel, element-centre guess"},
             "graph_small_batches": graph_small,

@@ -41,7 +41,10 @@ class DrbBvh(C.Structure):
                 ("inner_nodes", C.c_void_p), ("leaf_nodes", C.c_void_p),
                 ("aabb_ids", C.c_void_p), ("ref_boxes", C.c_void_p),
                 ("bounds", C.c_float * 6), ("wide_nodes", C.c_void_p), ("n_wide", C.c_int),
-                ("wide_depth", C.c_int), ("leaf_maps", C.c_void_p)]
+                ("wide_depth", C.c_int), ("leaf_maps", C.c_void_p),
+                ("grid_start", C.c_void_p), ("grid_entries", C.c_void_p),
+                ("grid_dims", C.c_int * 3), ("grid_origin", C.c_float * 3),
+                ("grid_inv", C.c_float * 3)]
 
 
 class DrbNewtonOpts(C.Structure):
@@ -135,6 +138,9 @@ _SIGS = {
                                   C.c_void_p]),
     "drb_bvh_leaf_maps": (C.c_int, [C.POINTER(DrbMesh), C.POINTER(DrbBvh), C.c_void_p,
                                     C.c_void_p]),
+    "drb_bvh_grid_size": (C.c_int, [C.POINTER(DrbBvh), C.c_float, C.POINTER(C.c_longlong),
+                                    C.c_void_p]),
+    "drb_bvh_grid_build": (C.c_int, [C.POINTER(DrbBvh), C.c_void_p]),
     "drb_query_stage": (C.c_int, [C.POINTER(DrbBvh), C.c_void_p, C.c_int, C.c_void_p,
                                   C.c_void_p]),
     "drb_locate_staged": (C.c_int, [C.POINTER(DrbMesh), C.POINTER(DrbBvh), C.c_void_p, C.c_int,

@@ -70,6 +70,10 @@ class BVH:
         self.wide_depth = 0
         # optional per-leaf linear maps (drb_bvh_leaf_maps)
         self.leaf_maps = None
+        # optional uniform-grid candidate lists (drb_bvh_grid_build)
+        self.grid_start = None
+        self.grid_entries = None
+        self.grid_geom = None  # (dims, origin, inv)
 
     def desc(self) -> L.DrbBvh:
         d = L.DrbBvh()
@@ -85,7 +89,34 @@ class BVH:
             d.n_wide, d.wide_depth = self.n_wide, self.wide_depth
         if self.leaf_maps is not None:
             d.leaf_maps = self.leaf_maps.data_ptr()
+        if self.grid_start is not None:
+            d.grid_start = self.grid_start.data_ptr()
+            d.grid_entries = self.grid_entries.data_ptr()
+            dims, origin, inv = self.grid_geom
+            for q in range(3):
+                d.grid_dims[q], d.grid_origin[q], d.grid_inv[q] = dims[q], origin[q], inv[q]
         return d
+
+    def build_grid(self, cell_scale: float = 1.0, stream=None):
+        """Uniform-grid candidate lists of the leaves (drb_bvh_grid_size +
+        drb_bvh_grid_build): the batched locates then scan the point's cell
+        instead of walking the tree, with identical candidates and results.
+        Cells are about cell_scale times the mean leaf extent per axis."""
+        self.grid_start = self.grid_entries = self.grid_geom = None
+        d = self.desc()
+        m = C.c_longlong()
+        L.check(L.lib().drb_bvh_grid_size(C.byref(d), float(cell_scale), C.byref(m),
+                                          _stream(stream)), "drb_bvh_grid_size")
+        dims = tuple(d.grid_dims)
+        dev = self.inner_nodes.device
+        self.grid_start = torch.empty(dims[0] * dims[1] * dims[2] + 1, dtype=torch.int32,
+                                      device=dev)
+        self.grid_entries = torch.empty((m.value, 8), dtype=torch.float32, device=dev)
+        self.grid_geom = (dims, tuple(d.grid_origin), tuple(d.grid_inv))
+        d = self.desc()
+        L.check(L.lib().drb_bvh_grid_build(C.byref(d), _stream(stream)), "drb_bvh_grid_build")
+        return self
+
 
     def build_leaf_maps(self, mesh: "UnstructuredMesh", stream=None):
         """Per-leaf linear maps of the element maps at the reference
@@ -114,6 +145,14 @@ class BVH:
         b = BVH.__new__(BVH)
         b.__dict__.update(self.__dict__)
         b.wide_nodes, b.n_wide, b.wide_depth = None, 0, 0
+        b.grid_start = b.grid_entries = b.grid_geom = None
+        return b
+
+    def without_grid(self) -> "BVH":
+        """A view of the same BVH without its grid lists (tree traversal)."""
+        b = BVH.__new__(BVH)
+        b.__dict__.update(self.__dict__)
+        b.grid_start = b.grid_entries = b.grid_geom = None
         return b
 
 

@@ -139,6 +139,60 @@ struct LocateParams
   const float4 *leaf_maps = nullptr; // per-leaf linear maps (drb_bvh_leaf_maps) or NULL
 };
 
+// Uniform-grid candidate lists of a BVH (drb_bvh_grid_build); a separate
+// kernel argument, so the tree-walking kernels carry none of it.
+struct GridLists
+{
+  const int *start = nullptr;
+  const float4 *entries = nullptr;
+  int dims[3] = { 1, 1, 1 };
+  float origin[3] = { 0.f, 0.f, 0.f };
+  float inv[3] = { 0.f, 0.f, 0.f };
+};
+
+// Cell coordinate of x along one grid axis: floor((x - o) * inv) clamped to
+// [0, g - 1].  Monotone in x, so every point of a box [lo, hi] falls in a
+// cell between those of lo and hi; the grid build files each leaf under
+// that range with this same function.  NaN maps to 0.
+DRB_D int grid_axis (float x, float o, float inv, int g)
+{
+  float v = __fmul_rn (__fsub_rn (x, o), inv);
+  v = fminf (fmaxf (v, 0.f), (float)(g - 1));
+  return __float2int_rd (v);
+}
+
+DRB_D int grid_cell (const int (&dims)[3], const float (&o)[3], const float (&inv)[3],
+                     const float (&p)[3])
+{
+  const int cx = grid_axis (p[0], o[0], inv[0], dims[0]);
+  const int cy = grid_axis (p[1], o[1], inv[1], dims[1]);
+  const int cz = grid_axis (p[2], o[2], inv[2], dims[2]);
+  return (cz * dims[1] + cy) * dims[0] + cx;
+}
+
+// Next candidate leaf of a point from its grid cell's list: the entries
+// hold every leaf whose box overlaps the cell, in leaf order, each with its
+// box (the same floats as in its parent's node) and element.  A leaf is
+// reached by the left-first traversal exactly when its own box holds the
+// point (refit makes every ancestor's box contain it), and that traversal
+// meets leaves in index order (each Karras node covers a contiguous range,
+// left before right), so this scan yields the traversal's candidates in
+// the traversal's order.  cur and end index the entries; -1 when done.
+DRB_D int next_grid_leaf (const GridLists &gl, const float (&p)[3], int &cur, int end,
+                          int &visited)
+{
+  while (cur < end)
+  {
+    const float4 a = __ldg (gl.entries + 2 * (size_t)cur);
+    const float4 b = __ldg (gl.entries + 2 * (size_t)cur + 1);
+    ++cur;
+    ++visited;
+    if (!(p[0] < a.x || p[1] < a.y || p[2] < a.z || p[0] > b.x || p[1] > b.y || p[2] > b.z))
+      return __float_as_int (a.w);
+  }
+  return -1;
+}
+
 // Candidate filter of the batched locate (drb_tet_hull_planes): true when
 // the query lies more than kHullMargin * tol * D outside one of the tet's
 // hull planes, where no Newton solve can be accepted.

@@ -225,13 +225,15 @@ template <int P> constexpr size_t smem_rows_bytes_per_warp ()
 // writes, which the kernel's latency-bound loop absorbs); with res set they
 // go to res[pos] as (cell as int bits, reference point), contiguous, for a
 // separate pass to put back.  Statistics always go to the input index.
-template <int P, int MODE, bool WIDE, int S = kTensor>
+// TRAV: 0 binary tree, 1 4-wide tree, 2 grid candidate lists.
+template <int P, int MODE, int TRAV, int S = kTensor>
 __global__ void locate_persistent_kernel (LocateParams lp, const float *__restrict__ pts,
                                           const int *__restrict__ order, int n, int chunk,
                                           int *__restrict__ queue_head, int *__restrict__ cell,
                                           float *__restrict__ ref, int *__restrict__ it_out,
                                           int *__restrict__ ca_out, int *__restrict__ nd_out,
-                                          const float4 *__restrict__ staged, float4 *__restrict__ res)
+                                          const float4 *__restrict__ staged, float4 *__restrict__ res,
+                                          GridLists gl)
 {
   const unsigned FULL = 0xffffffffu;
   const int lane = threadIdx.x & 31;
@@ -242,7 +244,8 @@ __global__ void locate_persistent_kernel (LocateParams lp, const float *__restri
   bool exhausted = false;          // warp-uniform
   int qi = -1;
   float pt[3] = { 0.f, 0.f, 0.f };
-  int todo[TraversalStack<WIDE>::kDepth];
+  constexpr bool WIDE = TRAV == 1, GRID = TRAV == 2;
+  int todo[GRID ? 1 : TraversalStack<WIDE>::kDepth];
   int sp = 0, cur = kBarrier;
   int iters = 0, cands = 0, nodes = 0;
   bool first = true;
@@ -302,6 +305,13 @@ __global__ void locate_persistent_kernel (LocateParams lp, const float *__restri
         sp = 0;
         todo[0] = kBarrier;
         cur = 0;
+        if constexpr (GRID)
+        {
+          // grid lists: cur walks the cell's entries up to sp
+          const int c = grid_cell (gl.dims, gl.origin, gl.inv, pt);
+          cur = __ldg (gl.start + c);
+          sp = __ldg (gl.start + c + 1);
+        }
         iters = cands = nodes = 0;
         first = true;
         failed0 = failed1 = failed2 = -1;
@@ -313,7 +323,11 @@ __global__ void locate_persistent_kernel (LocateParams lp, const float *__restri
 
     // ---- traversal phase: advance to the next candidate leaf ----
     int leaf = -1;
-    if (qi >= 0) leaf = next_leaf<WIDE> (lp.nodes, lp.wide, pt, todo, sp, cur, nodes);
+    if (qi >= 0)
+    {
+      if constexpr (GRID) leaf = next_grid_leaf (gl, pt, cur, sp, nodes);
+      else leaf = next_leaf<WIDE> (lp.nodes, lp.wide, pt, todo, sp, cur, nodes);
+    }
 
     // ---- candidate phase: converged Newton solves ----
     int el = -1;
@@ -380,8 +394,11 @@ __global__ void locate_persistent_kernel (LocateParams lp, const float *__restri
             failed1 = failed0;
             failed0 = el;
           }
-          cur = todo[sp];
-          --sp;
+          if constexpr (!GRID)
+          {
+            cur = todo[sp];
+            --sp;
+          }
         }
       }
       else
@@ -414,26 +431,32 @@ __global__ void locate_persistent_kernel (LocateParams lp, const float *__restri
 }
 
 // Tets run the L1 and register row modes (shared rows are tensor-only).
-template <int P, bool W, int S> const void *persistent_fn_pw (int mode)
+template <int P, int W, int S> const void *persistent_fn_pw (int mode)
 {
   if (S == kTensor && mode == kRowsShared) return (const void *)locate_persistent_kernel<P, kRowsShared, W>;
   if (mode == kRowsReg && P <= 2) return (const void *)locate_persistent_kernel<P, kRowsReg, W, S>;
   return (const void *)locate_persistent_kernel<P, kRowsL1, W, S>;
 }
 
-template <int S> const void *persistent_fn_s (int order, int mode, bool wide)
+template <int P, int S> const void *persistent_fn_p (int mode, int trav)
 {
-  if (order == 1) return wide ? persistent_fn_pw<1, true, S> (mode) : persistent_fn_pw<1, false, S> (mode);
-  if (order == 2) return wide ? persistent_fn_pw<2, true, S> (mode) : persistent_fn_pw<2, false, S> (mode);
-  return wide ? persistent_fn_pw<3, true, S> (mode) : persistent_fn_pw<3, false, S> (mode);
+  return trav == 2 ? persistent_fn_pw<P, 2, S> (mode) : trav == 1 ? persistent_fn_pw<P, 1, S> (mode)
+                                                      : persistent_fn_pw<P, 0, S> (mode);
 }
 
-const void *persistent_fn (const drb_mesh *mesh, int mode, bool wide)
+template <int S> const void *persistent_fn_s (int order, int mode, int trav)
 {
-  if (mesh->shape == DRB_SHAPE_SIMPLEX && mesh->dim == 2) return persistent_fn_s<kTri2D> (mesh->order, mode, wide);
-  if (mesh->shape == DRB_SHAPE_SIMPLEX) return persistent_fn_s<kSimplex> (mesh->order, mode, wide);
-  if (mesh->dim == 2) return persistent_fn_s<kQuad2D> (mesh->order, mode, wide);
-  return persistent_fn_s<kTensor> (mesh->order, mode, wide);
+  if (order == 1) return persistent_fn_p<1, S> (mode, trav);
+  if (order == 2) return persistent_fn_p<2, S> (mode, trav);
+  return persistent_fn_p<3, S> (mode, trav);
+}
+
+const void *persistent_fn (const drb_mesh *mesh, int mode, int trav)
+{
+  if (mesh->shape == DRB_SHAPE_SIMPLEX && mesh->dim == 2) return persistent_fn_s<kTri2D> (mesh->order, mode, trav);
+  if (mesh->shape == DRB_SHAPE_SIMPLEX) return persistent_fn_s<kSimplex> (mesh->order, mode, trav);
+  if (mesh->dim == 2) return persistent_fn_s<kQuad2D> (mesh->order, mode, trav);
+  return persistent_fn_s<kTensor> (mesh->order, mode, trav);
 }
 
 // Row mode actually used: registers only for orders 1-2, shared rows only
@@ -461,12 +484,12 @@ struct Staging
   float4 *res = nullptr;
 };
 
-template <int P, bool W, int S>
+template <int P, int W, int S>
 void launch_pw (int mode, dim3 grid, int block, size_t smem, cudaStream_t s, const LocateParams &lp,
-                const float *pts, const int *ord, int n, int chunk, int *head, int *cell, float *ref,
+                const GridLists &gl, const float *pts, const int *ord, int n, int chunk, int *head, int *cell, float *ref,
                 drb_query_stats st, Staging sg)
 {
-#define DRB_LP(M, SS) locate_persistent_kernel<P, M, W, SS><<<grid, block, smem, s>>> (lp, pts, ord, n, chunk, head, cell, ref, st.iters, st.candidates, st.nodes, sg.staged, sg.res)
+#define DRB_LP(M, SS) locate_persistent_kernel<P, M, W, SS><<<grid, block, smem, s>>> (lp, pts, ord, n, chunk, head, cell, ref, st.iters, st.candidates, st.nodes, sg.staged, sg.res, gl)
   if (S == kTensor && mode == kRowsShared) DRB_LP (kRowsShared, kTensor);
   else if (mode == kRowsReg && P <= 2) DRB_LP (P <= 2 ? kRowsReg : kRowsL1, S);
   else DRB_LP (kRowsL1, S);
@@ -474,40 +497,68 @@ void launch_pw (int mode, dim3 grid, int block, size_t smem, cudaStream_t s, con
 }
 
 template <int S>
-void launch_s (int order, bool wide, int mode, dim3 grid, int block, size_t smem, cudaStream_t s,
-               const LocateParams &lp, const float *pts, const int *ord, int n, int chunk, int *head,
-               int *cell, float *ref, drb_query_stats st, Staging sg)
+void launch_s (int order, int trav, int mode, dim3 grid, int block, size_t smem, cudaStream_t s,
+               const LocateParams &lp, const GridLists &gl, const float *pts, const int *ord, int n,
+               int chunk, int *head, int *cell, float *ref, drb_query_stats st, Staging sg)
 {
-  if (order == 1) { if (wide) launch_pw<1, true, S> (mode, grid, block, smem, s, lp, pts, ord, n, chunk, head, cell, ref, st, sg); else launch_pw<1, false, S> (mode, grid, block, smem, s, lp, pts, ord, n, chunk, head, cell, ref, st, sg); }
-  else if (order == 2) { if (wide) launch_pw<2, true, S> (mode, grid, block, smem, s, lp, pts, ord, n, chunk, head, cell, ref, st, sg); else launch_pw<2, false, S> (mode, grid, block, smem, s, lp, pts, ord, n, chunk, head, cell, ref, st, sg); }
-  else { if (wide) launch_pw<3, true, S> (mode, grid, block, smem, s, lp, pts, ord, n, chunk, head, cell, ref, st, sg); else launch_pw<3, false, S> (mode, grid, block, smem, s, lp, pts, ord, n, chunk, head, cell, ref, st, sg); }
+#define DRB_LT(P, T) launch_pw<P, T, S> (mode, grid, block, smem, s, lp, gl, pts, ord, n, chunk, head, cell, ref, st, sg)
+#define DRB_LO(P) { if (trav == 2) DRB_LT (P, 2); else if (trav == 1) DRB_LT (P, 1); else DRB_LT (P, 0); }
+  if (order == 1) DRB_LO (1)
+  else if (order == 2) DRB_LO (2)
+  else DRB_LO (3)
+#undef DRB_LO
+#undef DRB_LT
+}
+
+// Traversal of the batched kernels: grid lists, else the 4-wide tree, else
+// the binary tree.
+int traversal_kind (const LocateParams &lp, const GridLists &gl)
+{
+  return (gl.start && gl.entries) ? 2 : lp.wide ? 1 : 0;
+}
+
+GridLists grid_lists (const drb_bvh *bvh)
+{
+  GridLists gl;
+  if (bvh->grid_start && bvh->grid_entries)
+  {
+    gl.start = bvh->grid_start;
+    gl.entries = (const float4 *)bvh->grid_entries;
+    for (int d = 0; d < 3; ++d)
+    {
+      gl.dims[d] = bvh->grid_dims[d];
+      gl.origin[d] = bvh->grid_origin[d];
+      gl.inv[d] = bvh->grid_inv[d];
+    }
+  }
+  return gl;
 }
 
 int launch_persistent (const drb_mesh *mesh, int mode, dim3 grid, int block, cudaStream_t s,
-                       const LocateParams &lp, const float *pts, const int *ord, int n, int chunk,
+                       const LocateParams &lp, const GridLists &gl, const float *pts, const int *ord, int n, int chunk,
                        int *head, int *cell, float *ref, drb_query_stats st, Staging sg = Staging ())
 {
   const int order = mesh->order;
   const size_t smem = dynamic_smem (order, mode, block);
-  const bool wide = lp.wide != nullptr;
+  const int trav = traversal_kind (lp, gl);
   if (smem > 48 * 1024)
-    cudaFuncSetAttribute (persistent_fn (mesh, mode, wide), cudaFuncAttributeMaxDynamicSharedMemorySize,
+    cudaFuncSetAttribute (persistent_fn (mesh, mode, trav), cudaFuncAttributeMaxDynamicSharedMemorySize,
                           (int)smem);
   if (mesh->shape == DRB_SHAPE_SIMPLEX && mesh->dim == 2)
-    launch_s<kTri2D> (order, wide, mode, grid, block, smem, s, lp, pts, ord, n, chunk, head, cell, ref, st, sg);
+    launch_s<kTri2D> (order, trav, mode, grid, block, smem, s, lp, gl, pts, ord, n, chunk, head, cell, ref, st, sg);
   else if (mesh->shape == DRB_SHAPE_SIMPLEX)
-    launch_s<kSimplex> (order, wide, mode, grid, block, smem, s, lp, pts, ord, n, chunk, head, cell, ref, st, sg);
+    launch_s<kSimplex> (order, trav, mode, grid, block, smem, s, lp, gl, pts, ord, n, chunk, head, cell, ref, st, sg);
   else if (mesh->dim == 2)
-    launch_s<kQuad2D> (order, wide, mode, grid, block, smem, s, lp, pts, ord, n, chunk, head, cell, ref, st, sg);
+    launch_s<kQuad2D> (order, trav, mode, grid, block, smem, s, lp, gl, pts, ord, n, chunk, head, cell, ref, st, sg);
   else
-    launch_s<kTensor> (order, wide, mode, grid, block, smem, s, lp, pts, ord, n, chunk, head, cell, ref, st, sg);
+    launch_s<kTensor> (order, trav, mode, grid, block, smem, s, lp, gl, pts, ord, n, chunk, head, cell, ref, st, sg);
   return check_launch ("locate_persistent_kernel");
 }
 
-int resident_blocks (const drb_mesh *mesh, int mode, bool wide, int block)
+int resident_blocks (const drb_mesh *mesh, int mode, int trav, int block)
 {
   const size_t smem = dynamic_smem (mesh->order, mode, block);
-  const void *fn = persistent_fn (mesh, mode, wide);
+  const void *fn = persistent_fn (mesh, mode, trav);
   if (smem > 48 * 1024)
     cudaFuncSetAttribute (fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
   int nb = 0;
@@ -608,7 +659,8 @@ int check_config (const drb_locate_config &cfg)
 int persistent_blocks (const drb_mesh *mesh, const drb_bvh *bvh, const drb_locate_config &cfg,
                        int mode, int n)
 {
-  const int per_sm = resident_blocks (mesh, mode, bvh->wide_nodes != nullptr, cfg.block);
+  const int per_sm = resident_blocks (mesh, mode, bvh->grid_start && bvh->grid_entries ? 2
+                                                 : bvh->wide_nodes ? 1 : 0, cfg.block);
   const int bps = (cfg.blocks_per_sm > 0) ? min (cfg.blocks_per_sm, per_sm) : per_sm;
   const long long warps_needed = ((long long)n + 31) / 32;
   long long blocks = (long long)bps * sm_count ();
@@ -634,8 +686,8 @@ int locate_staged_launch (const drb_mesh *mesh, const drb_bvh *bvh, const float4
   Staging sg;
   sg.staged = staged;
   sg.res = res;
-  return launch_persistent (mesh, mode, dim3 ((unsigned)blocks), cfg.block, s, lp, nullptr,
-                            nullptr, n, cfg.chunk, head, cell, ref, stats, sg);
+  return launch_persistent (mesh, mode, dim3 ((unsigned)blocks), cfg.block, s, lp, grid_lists (bvh),
+                            nullptr, nullptr, n, cfg.chunk, head, cell, ref, stats, sg);
 }
 
 // Sorted, staged batch over caller buffers: stage the queries in Morton-cell
@@ -705,7 +757,8 @@ int locate_batched_impl (const drb_mesh *mesh, const drb_bvh *bvh, const float *
   const int mode = effective_mode (mesh, cfg.reg_elements);
   const int blocks = persistent_blocks (mesh, bvh, cfg, mode, n);
   const LocateParams lp = make_params (mesh, bvh, opts);
-  return launch_persistent (mesh, mode, dim3 ((unsigned)blocks), cfg.block, s, lp, pts, ord, n,
+  return launch_persistent (mesh, mode, dim3 ((unsigned)blocks), cfg.block, s, lp, grid_lists (bvh),
+                            pts, ord, n,
                             cfg.chunk, head, cell, ref, stats);
 }
 
@@ -733,7 +786,8 @@ int locate_batched_ws (const drb_mesh *mesh, const drb_bvh *bvh, const float *pt
   const int mode = effective_mode (mesh, cfg.reg_elements);
   const int blocks = persistent_blocks (mesh, bvh, cfg, mode, n);
   const LocateParams lp = make_params (mesh, bvh, opts);
-  return launch_persistent (mesh, mode, dim3 ((unsigned)blocks), cfg.block, s, lp, pts, ord, n,
+  return launch_persistent (mesh, mode, dim3 ((unsigned)blocks), cfg.block, s, lp, grid_lists (bvh),
+                            pts, ord, n,
                             cfg.chunk, ws.head, cell, ref, stats);
 }
 

@@ -137,7 +137,40 @@ typedef struct drb_bvh
   /* Optional per-leaf linear maps for DRB_GUESS_SUBBOX_LINEAR
    * (drb_bvh_leaf_maps); NULL: that guess falls back to the sub-box centre. */
   float *leaf_maps;      /* device float[16 * n_leaf] */
+  /* Optional uniform-grid candidate lists for the batched kernels
+   * (drb_bvh_grid_size + drb_bvh_grid_build); NULL: they traverse the tree.
+   * Cell (cx, cy, cz) is (cz * dims[1] + cy) * dims[0] + cx, with
+   * c = clamp(floor((x - origin) * inv), 0, dims - 1) per axis. */
+  int *grid_start;       /* device int32[n_cells + 1]: list of cell c = entries
+                            [grid_start[c], grid_start[c + 1]) */
+  float *grid_entries;   /* device float[8 * n_entries]: per entry the leaf's box
+                            low corner, its leaf index (int bits), its high
+                            corner, its element id (int bits) */
+  int grid_dims[3];
+  float grid_origin[3];
+  float grid_inv[3];     /* cells per unit length (0 on a flat axis) */
 } drb_bvh;
+
+/* Uniform-grid candidate lists over a built BVH's leaves (no reference
+ * counterpart; the reference traverses its binary nodes,
+ * device_mesh.hpp:262-318).  Each cell lists every leaf whose box overlaps
+ * it, in leaf order, with the box and element inline.  A leaf is a
+ * traversal candidate exactly when its box holds the point, and the
+ * left-first traversal meets candidates in leaf order, so a batched locate
+ * that scans the point's cell visits the same candidates in the same order
+ * as the traversal: results are identical (the statistics' node count then
+ * counts entries tested).  Points with a NaN coordinate scan cell 0.
+ *
+ * drb_bvh_grid_size picks the grid (cells about cell_scale times the mean
+ * leaf extent on each axis, at most 2^28 cells), writes grid_dims,
+ * grid_origin and grid_inv into *bvh and returns the number of entries in
+ * *n_entries; it synchronises the stream.  The caller allocates
+ * int32[n_cells + 1] and float[8 * n_entries], sets grid_start and
+ * grid_entries, and calls drb_bvh_grid_build (stream-ordered scratch of
+ * about 24 bytes per entry and leaf).  Needs at least two leaves and fewer
+ * than 2^31 entries. */
+int drb_bvh_grid_size (drb_bvh *bvh, float cell_scale, long long *n_entries, void *stream);
+int drb_bvh_grid_build (const drb_bvh *bvh, void *stream);
 
 /* Per-leaf linearisation of a hex or tet mesh's element maps for
  * DRB_GUESS_SUBBOX_LINEAR: for sorted leaf k with element e and reference

@@ -52,6 +52,17 @@ def test_invalid_arguments_rejected_without_gpu():
                           L.DrbQueryStats(), None) == L.DRB_ERR_INVALID_ARG
 
 
+def test_grid_rejects_missing_bvh():
+    """drb_bvh_grid_size / drb_bvh_grid_build need a built BVH (no GPU use)."""
+    import ctypes as C
+    from devil_ray_b200 import _lib as L
+    d = L.DrbBvh()
+    m = C.c_longlong()
+    assert L.lib().drb_bvh_grid_size(C.byref(d), 1.0, C.byref(m), None) == L.DRB_ERR_INVALID_ARG
+    assert L.lib().drb_bvh_grid_build(C.byref(d), None) == L.DRB_ERR_INVALID_ARG
+    assert L.lib().drb_bvh_grid_size(None, 1.0, C.byref(m), None) == L.DRB_ERR_INVALID_ARG
+
+
 def test_widen_rejects_missing_bvh():
     from devil_ray_b200 import _lib as L
     lib = L.lib()
