@@ -1001,7 +1001,8 @@ def volume_bench(dev, args, timed, with_cpu=False):
 
 def profile_tet(dev, args):
     """One batched locate of N queries in the tet workload's mesh (196,608
-    order-2 tets), block 256, all resident blocks, chunk 32, register rows."""
+    order-2 tets), block 256, all resident blocks, chunk 32, register rows,
+    timed over --steps locates after --warmup."""
     import torch
     from devil_ray_b200 import _lib as L
     from devil_ray_b200 import api, meshgen
@@ -1011,10 +1012,21 @@ def profile_tet(dev, args):
     q = torch.as_tensor(meshgen.uniform_queries(args.profile_tet, 77), device=dev)
     loc = api.BatchedLocator(mesh, tol=TOL, max_steps=MAX_STEPS,
                              config=L.DrbLocateConfig(256, 0, 32, 1, 1))
-    cell, _ = loc.locate(q)
+    cell, ref = loc.locate(q)
+    for _ in range(max(args.warmup, 1)):
+        loc.locate(q, out=(cell, ref))
     torch.cuda.synchronize()
-    print(json.dumps({"profile_tet": args.profile_tet,
-                      "located_fraction": float((cell >= 0).float().mean())}))
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    for _ in range(args.steps):
+        loc.locate(q, out=(cell, ref))
+    e1.record()
+    torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1) / args.steps
+    located = int((cell >= 0).sum())
+    print(json.dumps({"profile_tet": args.profile_tet, "ms_per_step": ms,
+                      "located_fraction": located / q.shape[0],
+                      "located_pts_per_s": located / (ms * 1e-3)}))
     return 0
 
 

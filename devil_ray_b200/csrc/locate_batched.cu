@@ -322,11 +322,34 @@ __global__ void locate_persistent_kernel (LocateParams lp, const float *__restri
     if (__ballot_sync (FULL, qi >= 0) == 0u) break;
 
     // ---- traversal phase: advance to the next candidate leaf ----
+    // Simplex kinds: a candidate that the repeat or hull filter rejects
+    // needs no solve, so the lane moves straight on to the next candidate
+    // here instead of sitting out the warp's solves of this iteration.
     int leaf = -1;
     if (qi >= 0)
     {
-      if constexpr (GRID) leaf = next_grid_leaf (gl, pt, cur, sp, nodes);
-      else leaf = next_leaf<WIDE> (lp.nodes, lp.wide, pt, todo, sp, cur, nodes);
+      while (true)
+      {
+        if constexpr (GRID) leaf = next_grid_leaf (gl, pt, cur, sp, nodes);
+        else leaf = next_leaf<WIDE> (lp.nodes, lp.wide, pt, todo, sp, cur, nodes);
+        if (!kSkipRepeats || leaf < 0) break;
+        const int e = __ldg (lp.leaf_nodes + leaf);
+        const bool repeat = leaf_free_guess && (e == failed0 || e == failed1 || e == failed2);
+        if (!repeat && !(S == kSimplex && lp.hull && hull_rejects (lp, e, pt))) break;
+        ++cands;
+        first = false;
+        if (!repeat)
+        {
+          failed2 = failed1;
+          failed1 = failed0;
+          failed0 = e;
+        }
+        if constexpr (!GRID)
+        {
+          cur = todo[sp];
+          --sp;
+        }
+      }
     }
 
     // ---- candidate phase: converged Newton solves ----
@@ -374,10 +397,8 @@ __global__ void locate_persistent_kernel (LocateParams lp, const float *__restri
       if (leaf >= 0)
       {
         ++cands;
-        const bool repeat = leaf_free_guess && (el == failed0 || el == failed1 || el == failed2);
-        const bool found = (repeat || (S == kSimplex && lp.hull && hull_rejects (lp, el, pt)))
-                           ? false
-                           : (MODE == kRowsShared)
+        // (the simplex filters ran in the traversal phase)
+        const bool found = (MODE == kRowsShared)
                            ? solve_candidate_smem<P> (lp, leaf, my_row, qi, first, pt, x, iters)
                            : solve_candidate<P, MODE == kRowsReg, S> (lp, leaf, el, qi, first, pt, x, iters);
         first = false;
@@ -388,7 +409,7 @@ __global__ void locate_persistent_kernel (LocateParams lp, const float *__restri
         }
         else
         {
-          if (kSkipRepeats && !repeat)
+          if (kSkipRepeats)
           {
             failed2 = failed1;
             failed1 = failed0;
