@@ -226,14 +226,14 @@ template <int P> constexpr size_t smem_rows_bytes_per_warp ()
 // go to res[pos] as (cell as int bits, reference point), contiguous, for a
 // separate pass to put back.  Statistics always go to the input index.
 // TRAV: 0 binary tree, 1 4-wide tree, 2 grid candidate lists.
-template <int P, int MODE, int TRAV, int S = kTensor>
-__global__ void locate_persistent_kernel (LocateParams lp, const float *__restrict__ pts,
-                                          const int *__restrict__ order, int n, int chunk,
-                                          int *__restrict__ queue_head, int *__restrict__ cell,
-                                          float *__restrict__ ref, int *__restrict__ it_out,
-                                          int *__restrict__ ca_out, int *__restrict__ nd_out,
-                                          const float4 *__restrict__ staged, float4 *__restrict__ res,
-                                          GridLists gl)
+template <int P, int MODE, int TRAV, int S>
+DRB_D void persistent_body (const LocateParams &lp, const float *__restrict__ pts,
+                                            const int *__restrict__ order, int n, int chunk,
+                                            int *__restrict__ queue_head, int *__restrict__ cell,
+                                            float *__restrict__ ref, int *__restrict__ it_out,
+                                            int *__restrict__ ca_out, int *__restrict__ nd_out,
+                                            const float4 *__restrict__ staged,
+                                            float4 *__restrict__ res, const GridLists &gl)
 {
   const unsigned FULL = 0xffffffffu;
   const int lane = threadIdx.x & 31;
@@ -451,12 +451,42 @@ __global__ void locate_persistent_kernel (LocateParams lp, const float *__restri
   }
 }
 
+#define DRB_PERSISTENT_ARGS                                                                   \
+  LocateParams lp, const float *__restrict__ pts, const int *__restrict__ order, int n, int chunk, \
+      int *__restrict__ queue_head, int *__restrict__ cell, float *__restrict__ ref,              \
+      int *__restrict__ it_out, int *__restrict__ ca_out, int *__restrict__ nd_out,               \
+      const float4 *__restrict__ staged, float4 *__restrict__ res, GridLists gl
+template <int P, int MODE, int TRAV, int S = kTensor>
+__global__ void locate_persistent_kernel (DRB_PERSISTENT_ARGS)
+{
+  persistent_body<P, MODE, TRAV, S> (lp, pts, order, n, chunk, queue_head, cell, ref, it_out, ca_out,
+                                     nd_out, staged, res, gl);
+}
+// The grid scan with L1 rows at orders 1-2, held to 80 registers (the
+// compiler's choice of 89 at order 2 costs a quarter of the resident warps;
+// measured 9 % faster at 80, slower at 72, where it spills).
+template <int P, int MODE, int TRAV, int S = kTensor>
+__global__ void __maxnreg__ (80) locate_persistent_kernel_r80 (DRB_PERSISTENT_ARGS)
+{
+  persistent_body<P, MODE, TRAV, S> (lp, pts, order, n, chunk, queue_head, cell, ref, it_out, ca_out,
+                                     nd_out, staged, res, gl);
+}
+#undef DRB_PERSISTENT_ARGS
+
+template <int P, int MODE, int TRAV> constexpr bool capped_kernel ()
+{
+  return TRAV == 2 && MODE == kRowsL1 && P <= 2;
+}
+
 // Tets run the L1 and register row modes (shared rows are tensor-only).
 template <int P, int W, int S> const void *persistent_fn_pw (int mode)
 {
   if (S == kTensor && mode == kRowsShared) return (const void *)locate_persistent_kernel<P, kRowsShared, W>;
   if (mode == kRowsReg && P <= 2) return (const void *)locate_persistent_kernel<P, kRowsReg, W, S>;
-  return (const void *)locate_persistent_kernel<P, kRowsL1, W, S>;
+  if constexpr (capped_kernel<P, kRowsL1, W> ())
+    return (const void *)locate_persistent_kernel_r80<P, kRowsL1, W, S>;
+  else
+    return (const void *)locate_persistent_kernel<P, kRowsL1, W, S>;
 }
 
 template <int P, int S> const void *persistent_fn_p (int mode, int trav)
@@ -510,10 +540,11 @@ void launch_pw (int mode, dim3 grid, int block, size_t smem, cudaStream_t s, con
                 const GridLists &gl, const float *pts, const int *ord, int n, int chunk, int *head, int *cell, float *ref,
                 drb_query_stats st, Staging sg)
 {
-#define DRB_LP(M, SS) locate_persistent_kernel<P, M, W, SS><<<grid, block, smem, s>>> (lp, pts, ord, n, chunk, head, cell, ref, st.iters, st.candidates, st.nodes, sg.staged, sg.res, gl)
-  if (S == kTensor && mode == kRowsShared) DRB_LP (kRowsShared, kTensor);
-  else if (mode == kRowsReg && P <= 2) DRB_LP (P <= 2 ? kRowsReg : kRowsL1, S);
-  else DRB_LP (kRowsL1, S);
+#define DRB_LP(K, M, SS) K<P, M, W, SS><<<grid, block, smem, s>>> (lp, pts, ord, n, chunk, head, cell, ref, st.iters, st.candidates, st.nodes, sg.staged, sg.res, gl)
+  if (S == kTensor && mode == kRowsShared) DRB_LP (locate_persistent_kernel, kRowsShared, kTensor);
+  else if (mode == kRowsReg && P <= 2) DRB_LP (locate_persistent_kernel, P <= 2 ? kRowsReg : kRowsL1, S);
+  else if constexpr (capped_kernel<P, kRowsL1, W> ()) DRB_LP (locate_persistent_kernel_r80, kRowsL1, S);
+  else DRB_LP (locate_persistent_kernel, kRowsL1, S);
 #undef DRB_LP
 }
 
