@@ -41,8 +41,8 @@ sys.path.insert(0, str(ROOT))
 WORKLOAD = "locate_64"
 N_QUERIES = 16_777_216
 TOL = 1e-5
-# grid cells of the locate workload: half the mean leaf extent per axis
-GRID_CELL_SCALE = 0.5
+# grid cells of the locate workload: 0.75 of the mean leaf extent per axis
+GRID_CELL_SCALE = 0.75
 MAX_STEPS = 20
 METRIC = "located pts/s (Newton-resolved, tol 1e-5)"
 
@@ -1298,7 +1298,8 @@ def main():
                     "grid_build_ms": grid_build_ms, "cell_scale": GRID_CELL_SCALE,
                     "grid_dims": list(gbvh.grid_geom[0]),
                     "grid_entries": int(gbvh.grid_entries.shape[0]),
-                    "grid_bytes": int(gbvh.grid_entries.numel() * 4 + gbvh.grid_start.numel() * 4),
+                    "grid_bytes": int(gbvh.grid_entries.numel() * 4 + gbvh.grid_start.numel() * 4
+                                      + gbvh.grid_boxes.numel() * 4),
                     "launch_config": grid_cfg.as_dict(),
                     "note": "sub-box linear guess; candidates from the query's grid cell list "
                             "instead of the tree walk (same candidates, same order)"}

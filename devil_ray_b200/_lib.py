@@ -43,6 +43,7 @@ class DrbBvh(C.Structure):
                 ("bounds", C.c_float * 6), ("wide_nodes", C.c_void_p), ("n_wide", C.c_int),
                 ("wide_depth", C.c_int), ("leaf_maps", C.c_void_p),
                 ("grid_start", C.c_void_p), ("grid_entries", C.c_void_p),
+                ("grid_boxes", C.c_void_p),
                 ("grid_dims", C.c_int * 3), ("grid_origin", C.c_float * 3),
                 ("grid_inv", C.c_float * 3)]
 

@@ -73,6 +73,7 @@ class BVH:
         # optional uniform-grid candidate lists (drb_bvh_grid_build)
         self.grid_start = None
         self.grid_entries = None
+        self.grid_boxes = None
         self.grid_geom = None  # (dims, origin, inv)
 
     def desc(self) -> L.DrbBvh:
@@ -92,6 +93,7 @@ class BVH:
         if self.grid_start is not None:
             d.grid_start = self.grid_start.data_ptr()
             d.grid_entries = self.grid_entries.data_ptr()
+            d.grid_boxes = self.grid_boxes.data_ptr()
             dims, origin, inv = self.grid_geom
             for q in range(3):
                 d.grid_dims[q], d.grid_origin[q], d.grid_inv[q] = dims[q], origin[q], inv[q]
@@ -102,7 +104,7 @@ class BVH:
         drb_bvh_grid_build): the batched locates then scan the point's cell
         instead of walking the tree, with identical candidates and results.
         Cells are about cell_scale times the mean leaf extent per axis."""
-        self.grid_start = self.grid_entries = self.grid_geom = None
+        self.grid_start = self.grid_entries = self.grid_boxes = self.grid_geom = None
         d = self.desc()
         m = C.c_longlong()
         L.check(L.lib().drb_bvh_grid_size(C.byref(d), float(cell_scale), C.byref(m),
@@ -111,7 +113,8 @@ class BVH:
         dev = self.inner_nodes.device
         self.grid_start = torch.empty(dims[0] * dims[1] * dims[2] + 1, dtype=torch.int32,
                                       device=dev)
-        self.grid_entries = torch.empty((m.value, 8), dtype=torch.float32, device=dev)
+        self.grid_entries = torch.empty(m.value, dtype=torch.int32, device=dev)
+        self.grid_boxes = torch.empty((self.n_leaf, 8), dtype=torch.float32, device=dev)
         self.grid_geom = (dims, tuple(d.grid_origin), tuple(d.grid_inv))
         d = self.desc()
         L.check(L.lib().drb_bvh_grid_build(C.byref(d), _stream(stream)), "drb_bvh_grid_build")
@@ -145,14 +148,14 @@ class BVH:
         b = BVH.__new__(BVH)
         b.__dict__.update(self.__dict__)
         b.wide_nodes, b.n_wide, b.wide_depth = None, 0, 0
-        b.grid_start = b.grid_entries = b.grid_geom = None
+        b.grid_start = b.grid_entries = b.grid_boxes = b.grid_geom = None
         return b
 
     def without_grid(self) -> "BVH":
         """A view of the same BVH without its grid lists (tree traversal)."""
         b = BVH.__new__(BVH)
         b.__dict__.update(self.__dict__)
-        b.grid_start = b.grid_entries = b.grid_geom = None
+        b.grid_start = b.grid_entries = b.grid_boxes = b.grid_geom = None
         return b
 
 

@@ -6,16 +6,17 @@
 // box holds the point, and the left-first traversal meets leaves in index
 // order, a list per grid cell of the leaves whose boxes overlap the cell,
 // sorted by leaf index, yields the same candidates in the same order: the
-// point's cell gives a short contiguous run of (box, leaf, element) entries
-// to test instead of a chain of dependent node loads.  No reference
-// counterpart (the reference traverses its binary nodes,
-// data_model/device_mesh.hpp:262-318).
+// point's cell gives a short contiguous run of leaf indices whose boxes
+// (a 32-byte record per leaf) are tested instead of a chain of dependent
+// node loads.  No reference counterpart (the reference traverses its binary
+// nodes, data_model/device_mesh.hpp:262-318).
 //
 // Build: the leaf boxes are read back out of their parents' node records
 // (the same floats the traversal tests), each leaf is filed under every
 // cell its box overlaps (grid_axis of its corners), the (cell, leaf) pairs
-// are sorted stably by cell, and the entries and per-cell starts are
-// written from the sorted pairs.
+// are sorted stably by cell (the sorted leaf indices are the entries), the
+// per-cell starts are found by binary search, and the box table is written
+// once per leaf.
 #include "drb_common.cuh"
 #include "drb_internal.h"
 #include "locate.cuh"
@@ -137,16 +138,15 @@ __global__ void pair_emit_kernel (GridGeom g, const float *__restrict__ boxes, i
       }
 }
 
-// Entries from the sorted pairs: box, leaf and element of each.
-__global__ void entry_fill_kernel (const int *__restrict__ vals, int m, const float *__restrict__ boxes,
-                                   const int *__restrict__ leaf_nodes, float4 *__restrict__ entries)
+// Box table: per leaf its box and element (32 bytes, float4 aligned).
+__global__ void box_table_kernel (const float *__restrict__ boxes, int n,
+                                  const int *__restrict__ leaf_nodes, float4 *__restrict__ table)
 {
-  const int i = blockIdx.x * blockDim.x + threadIdx.x;
-  if (i >= m) return;
-  const int k = vals[i];
+  const int k = blockIdx.x * blockDim.x + threadIdx.x;
+  if (k >= n) return;
   const float *b = boxes + 6 * (size_t)k;
-  entries[2 * (size_t)i] = make_float4 (b[0], b[1], b[2], __int_as_float (k));
-  entries[2 * (size_t)i + 1] = make_float4 (b[3], b[4], b[5], __int_as_float (__ldg (leaf_nodes + k)));
+  table[2 * (size_t)k] = make_float4 (b[0], b[1], b[2], __int_as_float (__ldg (leaf_nodes + k)));
+  table[2 * (size_t)k + 1] = make_float4 (b[3], b[4], b[5], 0.f);
 }
 
 // start[c] = first sorted pair whose cell is >= c (lower bound), and
@@ -261,9 +261,9 @@ extern "C" int drb_bvh_grid_size (drb_bvh *bvh, float cell_scale, long long *n_e
 extern "C" int drb_bvh_grid_build (const drb_bvh *bvh, void *stream)
 {
   if (int st = check_bvh (bvh, "bvh_grid_build: needs a built BVH with at least two leaves")) return st;
-  if (!bvh->grid_start || !bvh->grid_entries)
+  if (!bvh->grid_start || !bvh->grid_entries || !bvh->grid_boxes)
   {
-    set_last_error ("bvh_grid_build: grid_start and grid_entries must be set");
+    set_last_error ("bvh_grid_build: grid_start, grid_entries and grid_boxes must be set");
     return DRB_ERR_INVALID_ARG;
   }
   const GridGeom g = geom_of (bvh);
@@ -302,16 +302,16 @@ extern "C" int drb_bvh_grid_build (const drb_bvh *bvh, void *stream)
   unsigned *keys = scr.alloc<unsigned> (m);
   int *vals = scr.alloc<int> (m);
   unsigned *keys_s = scr.alloc<unsigned> (m);
-  int *vals_s = scr.alloc<int> (m);
-  if (!keys || !vals || !keys_s || !vals_s) return status_from (scr.err);
+  if (!keys || !vals || !keys_s) return status_from (scr.err);
   pair_emit_kernel<<<div_up (n, 256), 256, 0, s>>> (g, boxes, n, offsets, keys, vals);
   if (int st = check_launch ("pair_emit_kernel")) return st;
   int bits = 1;
   while ((1ll << bits) < n_cells) ++bits;
-  if (int st = radix_sort_pairs (keys, vals, keys_s, vals_s, m, bits, s)) return st;
-  entry_fill_kernel<<<div_up (m, 256), 256, 0, s>>> (vals_s, m, boxes, bvh->leaf_nodes,
-                                                     (float4 *)bvh->grid_entries);
-  if (int st = check_launch ("entry_fill_kernel")) return st;
+  // the sorted leaf indices are the entries
+  if (int st = radix_sort_pairs (keys, vals, keys_s, bvh->grid_entries, m, bits, s)) return st;
+  box_table_kernel<<<div_up (n, 256), 256, 0, s>>> (boxes, n, bvh->leaf_nodes,
+                                                    (float4 *)bvh->grid_boxes);
+  if (int st = check_launch ("box_table_kernel")) return st;
   cell_start_kernel<<<div_up (n_cells + 1, 256), 256, 0, s>>> (keys_s, m, n_cells, bvh->grid_start);
   return check_launch ("cell_start_kernel");
 }

@@ -144,7 +144,8 @@ struct LocateParams
 struct GridLists
 {
   const int *start = nullptr;
-  const float4 *entries = nullptr;
+  const int *entries = nullptr;  // leaf indices, cell by cell
+  const float4 *boxes = nullptr; // per leaf: lo.xyz + element bits, hi.xyz + 0
   int dims[3] = { 1, 1, 1 };
   float origin[3] = { 0.f, 0.f, 0.f };
   float inv[3] = { 0.f, 0.f, 0.f };
@@ -171,8 +172,8 @@ DRB_D int grid_cell (const int (&dims)[3], const float (&o)[3], const float (&in
 }
 
 // Next candidate leaf of a point from its grid cell's list: the entries
-// hold every leaf whose box overlaps the cell, in leaf order, each with its
-// box (the same floats as in its parent's node) and element.  A leaf is
+// hold every leaf whose box overlaps the cell, in leaf order; each leaf's
+// box (the same floats as in its parent's node) is in gl.boxes.  A leaf is
 // reached by the left-first traversal exactly when its own box holds the
 // point (refit makes every ancestor's box contain it), and that traversal
 // meets leaves in index order (each Karras node covers a contiguous range,
@@ -183,12 +184,13 @@ DRB_D int next_grid_leaf (const GridLists &gl, const float (&p)[3], int &cur, in
 {
   while (cur < end)
   {
-    const float4 a = __ldg (gl.entries + 2 * (size_t)cur);
-    const float4 b = __ldg (gl.entries + 2 * (size_t)cur + 1);
+    const int k = __ldg (gl.entries + cur);
+    const float4 a = __ldg (gl.boxes + 2 * (size_t)k);
+    const float4 b = __ldg (gl.boxes + 2 * (size_t)k + 1);
     ++cur;
     ++visited;
     if (!(p[0] < a.x || p[1] < a.y || p[2] < a.z || p[0] > b.x || p[1] > b.y || p[2] > b.z))
-      return __float_as_int (a.w);
+      return k;
   }
   return -1;
 }

@@ -566,16 +566,17 @@ void launch_s (int order, int trav, int mode, dim3 grid, int block, size_t smem,
 // the binary tree.
 int traversal_kind (const LocateParams &lp, const GridLists &gl)
 {
-  return (gl.start && gl.entries) ? 2 : lp.wide ? 1 : 0;
+  return gl.start ? 2 : lp.wide ? 1 : 0;
 }
 
 GridLists grid_lists (const drb_bvh *bvh)
 {
   GridLists gl;
-  if (bvh->grid_start && bvh->grid_entries)
+  if (bvh->grid_start && bvh->grid_entries && bvh->grid_boxes)
   {
     gl.start = bvh->grid_start;
-    gl.entries = (const float4 *)bvh->grid_entries;
+    gl.entries = bvh->grid_entries;
+    gl.boxes = (const float4 *)bvh->grid_boxes;
     for (int d = 0; d < 3; ++d)
     {
       gl.dims[d] = bvh->grid_dims[d];
@@ -711,7 +712,7 @@ int check_config (const drb_locate_config &cfg)
 int persistent_blocks (const drb_mesh *mesh, const drb_bvh *bvh, const drb_locate_config &cfg,
                        int mode, int n)
 {
-  const int per_sm = resident_blocks (mesh, mode, bvh->grid_start && bvh->grid_entries ? 2
+  const int per_sm = resident_blocks (mesh, mode, grid_lists (bvh).start ? 2
                                                  : bvh->wide_nodes ? 1 : 0, cfg.block);
   const int bps = (cfg.blocks_per_sm > 0) ? min (cfg.blocks_per_sm, per_sm) : per_sm;
   const long long warps_needed = ((long long)n + 31) / 32;

@@ -143,9 +143,10 @@ typedef struct drb_bvh
    * c = clamp(floor((x - origin) * inv), 0, dims - 1) per axis. */
   int *grid_start;       /* device int32[n_cells + 1]: list of cell c = entries
                             [grid_start[c], grid_start[c + 1]) */
-  float *grid_entries;   /* device float[8 * n_entries]: per entry the leaf's box
-                            low corner, its leaf index (int bits), its high
-                            corner, its element id (int bits) */
+  int *grid_entries;     /* device int32[n_entries]: sorted leaf indices */
+  float *grid_boxes;     /* device float[8 * n_leaf]: per sorted leaf its box low
+                            corner, its element id (int bits), its high corner,
+                            0 (the floats of its parent's node record) */
   int grid_dims[3];
   float grid_origin[3];
   float grid_inv[3];     /* cells per unit length (0 on a flat axis) */
@@ -154,7 +155,7 @@ typedef struct drb_bvh
 /* Uniform-grid candidate lists over a built BVH's leaves (no reference
  * counterpart; the reference traverses its binary nodes,
  * device_mesh.hpp:262-318).  Each cell lists every leaf whose box overlaps
- * it, in leaf order, with the box and element inline.  A leaf is a
+ * it, in leaf order; the leaves' boxes sit in a table beside.  A leaf is a
  * traversal candidate exactly when its box holds the point, and the
  * left-first traversal meets candidates in leaf order, so a batched locate
  * that scans the point's cell visits the same candidates in the same order
@@ -165,10 +166,10 @@ typedef struct drb_bvh
  * leaf extent on each axis, at most 2^28 cells), writes grid_dims,
  * grid_origin and grid_inv into *bvh and returns the number of entries in
  * *n_entries; it synchronises the stream.  The caller allocates
- * int32[n_cells + 1] and float[8 * n_entries], sets grid_start and
- * grid_entries, and calls drb_bvh_grid_build (stream-ordered scratch of
- * about 24 bytes per entry and leaf).  Needs at least two leaves and fewer
- * than 2^31 entries. */
+ * int32[n_cells + 1], int32[n_entries] and float[8 * n_leaf], sets
+ * grid_start, grid_entries and grid_boxes, and calls drb_bvh_grid_build
+ * (stream-ordered scratch of about 12 bytes per entry and 32 per leaf).
+ * Needs at least two leaves and fewer than 2^31 entries. */
 int drb_bvh_grid_size (drb_bvh *bvh, float cell_scale, long long *n_entries, void *stream);
 int drb_bvh_grid_build (const drb_bvh *bvh, void *stream);
 
