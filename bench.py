@@ -450,10 +450,10 @@ def surface_c1(dev, with_cpu):
     return out
 
 
-def grid_touched_entries(gbvh, pts) -> int:
-    """Entries of the grid cells that hold at least one of the points (the
-    cell of a point: clamp(floor((x - origin) * inv), 0, dims - 1) per axis
-    in float32, as the kernels compute it)."""
+def grid_touched_entries(gbvh, pts):
+    """(cells, entries) of the grid cells that hold at least one of the
+    points (the cell of a point: clamp(floor((x - origin) * inv), 0,
+    dims - 1) per axis in float32, as the kernels compute it)."""
     import torch
     dims, origin, inv = gbvh.grid_geom
     c = []
@@ -463,7 +463,7 @@ def grid_touched_entries(gbvh, pts) -> int:
         c.append(v.clamp(0.0, float(dims[d] - 1)).floor().long())
     cells = torch.unique((c[2] * dims[1] + c[1]) * dims[0] + c[0])
     st = gbvh.grid_start.long()
-    return int((st[cells + 1] - st[cells]).sum().item())
+    return int(cells.numel()), int((st[cells + 1] - st[cells]).sum().item())
 
 
 def tet_locate(dev, args, with_cpu):
@@ -1284,7 +1284,17 @@ def main():
     grid_build_ms = ev0.elapsed_time(ev1)
     loc_grid = api.BatchedLocator(mesh, tol=TOL, max_steps=MAX_STEPS,
                                   guess_mode=L.GUESS_SUBBOX_LINEAR, bvh=gbvh)
-    grid_cfg, _ = loc_grid.tune(pts[: min(n, 1 << 21)])
+    # the tuner's sample is sparser than the full batch: keep the faster of
+    # its pick and the tree leg's shape on the full batch
+    tuned_cfg, _ = loc_grid.tune(pts[: min(n, 1 << 21)])
+    shape_ms = {}
+    for c in (tuned_cfg, best_cfg):
+        loc_grid.config = c
+        for _ in range(2):
+            loc_grid.locate(pts, out=(cell, ref))
+        shape_ms[tuple(c.as_dict().values())] = timed(lambda: loc_grid.locate(pts, out=(cell, ref)), 3)
+    grid_cfg = min((tuned_cfg, best_cfg), key=lambda c: shape_ms[tuple(c.as_dict().values())])
+    loc_grid.config = grid_cfg
     for _ in range(2):
         loc_grid.locate(pts, out=(cell, ref))
     grid_ms = timed(lambda: loc_grid.locate(pts, out=(cell, ref)), args.steps) / args.steps
@@ -1374,13 +1384,18 @@ def main():
     # packed element rows, and for the sub-box-centre guess the leaf sub-box
     # ids and reference boxes.  Repeated visits are served by the caches, so
     # these bytes are the floor of the launch's DRAM traffic.
-    # With the grid lists, the entries of the cells that hold queries replace
-    # the tree (32 B each).
+    # With the grid lists, the tree is replaced by the cell starts and the
+    # entries (4 B each) of the cells that hold queries, and the 32-byte box
+    # records of the leaves.
     stride = L.lib().drb_packed_stride(3, m.order, 3)
     sub_guess = roof_loc is loc_sub
     grid_path = roof_loc is loc_grid
     lin_guess = roof_loc is loc_lin or grid_path
-    tree_bytes = grid_touched_entries(gbvh, pts) * 32 if grid_path else bvh.n_wide * 128
+    if grid_path:
+        touched_cells, touched_entries = grid_touched_entries(gbvh, pts)
+        tree_bytes = touched_cells * 8 + touched_entries * 4 + bvh.n_leaf * 32
+    else:
+        tree_bytes = bvh.n_wide * 128
     compulsory = (n * (16 + 16) + tree_bytes + bvh.n_leaf * 4 + m.n_elem * stride * 4
                   + (bvh.n_leaf * (4 + 24) if sub_guess else 0)
                   + (bvh.n_leaf * 64 if lin_guess else 0))
@@ -1488,9 +1503,9 @@ def main():
                          "achieved_bytes": "compulsory DRAM bytes per launch: 4 B order "
                                            "entry + 12 B point in and 16 B result (cell + "
                                            "reference point) out per query, "
-                                           + ("the 32-byte grid entries of every cell that "
-                                              "holds a query" if grid_path else
-                                              "the 4-wide tree")
+                                           + ("the start and 4-byte entries of every grid "
+                                              "cell that holds a query, the 32-byte box "
+                                              "records" if grid_path else "the 4-wide tree")
                                            + ", leaf ids and packed rows once"
                                            + (", leaf sub-box ids and reference boxes once"
                                               if sub_guess else "")
