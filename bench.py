@@ -78,8 +78,8 @@ def parse():
     ap.add_argument("--guess", default="centre", choices=["centre", "subref", "linear"],
                     help="first guess of --profile")
     ap.add_argument("--grid", type=float, default=0.0, metavar="SCALE",
-                    help="--profile over grid candidate lists with cells of SCALE times the "
-                         "mean leaf extent (0: the 4-wide tree)")
+                    help="--profile / --profile-tet over grid candidate lists with cells of "
+                         "SCALE times the mean leaf extent (0: the 4-wide tree)")
     ap.add_argument("--coherent", type=int, default=1, choices=[1, 2],
                     help="predictor of --profile-volume's coherent march: 1 first-order, "
                          "2 quadratic")
@@ -1012,6 +1012,8 @@ def profile_tet(dev, args):
     q = torch.as_tensor(meshgen.uniform_queries(args.profile_tet, 77), device=dev)
     loc = api.BatchedLocator(mesh, tol=TOL, max_steps=MAX_STEPS,
                              config=L.DrbLocateConfig(256, 0, 32, 1, 1))
+    if args.grid > 0:
+        loc.bvh = mesh.get_bvh().without_grid().build_grid(args.grid)
     cell, ref = loc.locate(q)
     for _ in range(max(args.warmup, 1)):
         loc.locate(q, out=(cell, ref))
@@ -1024,7 +1026,7 @@ def profile_tet(dev, args):
     torch.cuda.synchronize()
     ms = e0.elapsed_time(e1) / args.steps
     located = int((cell >= 0).sum())
-    print(json.dumps({"profile_tet": args.profile_tet, "ms_per_step": ms,
+    print(json.dumps({"profile_tet": args.profile_tet, "grid": args.grid, "ms_per_step": ms,
                       "located_fraction": located / q.shape[0],
                       "located_pts_per_s": located / (ms * 1e-3)}))
     return 0
@@ -1284,16 +1286,23 @@ def main():
     grid_build_ms = ev0.elapsed_time(ev1)
     loc_grid = api.BatchedLocator(mesh, tol=TOL, max_steps=MAX_STEPS,
                                   guess_mode=L.GUESS_SUBBOX_LINEAR, bvh=gbvh)
-    # the tuner's sample is sparser than the full batch: keep the faster of
-    # its pick and the tree leg's shape on the full batch
+    # the tuner's sample is sparser than the full batch: keep the fastest of
+    # its pick and the tree leg's shape on the full batch, each with the
+    # queries read through the order (1) or staged as records first (2)
     tuned_cfg, _ = loc_grid.tune(pts[: min(n, 1 << 21)])
-    shape_ms = {}
+    cands = []
     for c in (tuned_cfg, best_cfg):
+        for sq in (1, 2):
+            d = c.as_dict()
+            cands.append(L.DrbLocateConfig(d["block"], d["blocks_per_sm"], d["chunk"], sq,
+                                           d["reg_elements"]))
+    shape_ms = []
+    for c in cands:
         loc_grid.config = c
         for _ in range(2):
             loc_grid.locate(pts, out=(cell, ref))
-        shape_ms[tuple(c.as_dict().values())] = timed(lambda: loc_grid.locate(pts, out=(cell, ref)), 3)
-    grid_cfg = min((tuned_cfg, best_cfg), key=lambda c: shape_ms[tuple(c.as_dict().values())])
+        shape_ms.append(timed(lambda: loc_grid.locate(pts, out=(cell, ref)), 3))
+    grid_cfg = cands[min(range(len(cands)), key=lambda i: shape_ms[i])]
     loc_grid.config = grid_cfg
     for _ in range(2):
         loc_grid.locate(pts, out=(cell, ref))
@@ -1332,15 +1341,19 @@ def main():
     roof_loc = head_loc
     roof_stats = sub_stats if roof_loc is loc_sub else lin_stats if roof_loc is loc_lin else \
         grid_stats if roof_loc is loc_grid else (mean_it, mean_ca, mean_nd)
-    qorder = roof_loc.order(pts)
+    if roof_loc.config is not None and roof_loc.config.sort_queries >= 2:
+        qstaged = roof_loc.stage(pts)
+        roof_kern = lambda: roof_loc.locate_staged(qstaged, out=(cell, ref))
+    else:
+        qstaged = roof_loc.order(pts)
+        roof_kern = lambda: roof_loc.locate(pts, order=qstaged, out=(cell, ref))
     for _ in range(2):
-        roof_loc.locate(pts, order=qorder, out=(cell, ref))
+        roof_kern()
     dram = DramMeter(local)
     dram.start()
-    kern_ms = timed(lambda: roof_loc.locate(pts, order=qorder, out=(cell, ref)),
-                    args.steps) / args.steps
+    kern_ms = timed(roof_kern, args.steps) / args.steps
     dram_read = dram.stop()
-    del qorder
+    del qstaged, roof_kern
     learned = None
     if not args.no_learned and m.order == 2:
         try:
