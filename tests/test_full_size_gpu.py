@@ -60,6 +60,44 @@ def test_c2_locate_full_size(cuda, ref):
     assert sel[outside].float().mean().item() < 1e-5
 
 
+def test_c2_headline_path_full_size(cuda):
+    """The bench's headline path at full size (sub-box linear guess, grid
+    candidate lists at cells of 0.75 mean leaf extents, staged query
+    records): the same cells and reference points, bit for bit, as the
+    plain kernel with the same guess walking the binary tree, and the same
+    cells as the element-centre guess except on shared faces, reference
+    points within the 1e-5 tolerance."""
+    import torch
+    from devil_ray_b200 import _lib as L
+    from devil_ray_b200 import api, meshgen
+    m = meshgen.workload_mesh("locate_64")
+    q = meshgen.uniform_queries(1 << 24, 1001)
+    g = api.UnstructuredMesh(m.ctrl_idx, m.xyz, m.order, device=cuda)
+    pts = torch.as_tensor(q, device=cuda)
+    gb = g.get_bvh().without_grid().build_grid(0.75)
+    cfg = L.DrbLocateConfig(64, 0, 64, 2, 0)
+    head = api.BatchedLocator(g, tol=1e-5, max_steps=20, guess_mode=L.GUESS_SUBBOX_LINEAR,
+                              config=cfg, bvh=gb)
+    c1, r1 = head.locate(pts)
+    g.get_bvh().leaf_maps = gb.leaf_maps
+    c0, r0 = g.locate(pts, tol=1e-5, max_steps=20, guess_mode=L.GUESS_SUBBOX_LINEAR)
+    torch.cuda.synchronize()
+    assert torch.equal(c0, c1)
+    assert torch.equal(r0.view(torch.int32), r1.view(torch.int32))
+    ce, re = api.BatchedLocator(g, tol=1e-5, max_steps=20).locate(pts)
+    torch.cuda.synchronize()
+    same = c1 == ce
+    print(f"headline path: {int((~same).sum())} of {q.shape[0]} cells differ from the "
+          f"element-centre guess")
+    assert same.float().mean().item() > 0.9999
+    hit = same & (c1 >= 0)
+    assert (r1[hit] - re[hit]).abs().max().item() < 1e-5
+    diff = ~same
+    if bool(diff.any()):
+        rr = torch.cat([r1[diff & (c1 >= 0)], re[diff & (ce >= 0)]])
+        assert bool(((rr < 2e-3) | (rr > 1 - 2e-3)).any(dim=1).all())
+
+
 def test_c1_surface_full_size(cuda, ref):
     import torch
     from devil_ray_b200 import api, meshgen
