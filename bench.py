@@ -1521,6 +1521,9 @@ def main():
                        "parallelism": f"replicas x{world}, queries sharded, no collective"},
             "roofline": {"bound": "hbm", "achieved": achieved_gbs, "peak": peak, "unit": "GB/s",
                          "frac": achieved_gbs / peak,
+                         # compulsory bytes cannot move faster than a copy:
+                         # a fraction above 1.2 means a byte-count error
+                         "frac_plausible": achieved_gbs / peak <= 1.2,
                          "traffic": traffic,
                          "achieved_bytes": "compulsory DRAM bytes per launch: 4 B order "
                                            "entry + 12 B point in and 16 B result (cell + "
