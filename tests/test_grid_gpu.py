@@ -112,3 +112,28 @@ def test_grid_rejects_bad_calls(cuda):
     assert L.lib().drb_bvh_grid_size(C.byref(bd), 0.0, C.byref(m), None) == L.DRB_ERR_INVALID_ARG
     # no lists set: build refuses
     assert L.lib().drb_bvh_grid_build(C.byref(bd), None) == L.DRB_ERR_INVALID_ARG
+
+
+def test_grid_locate_edge_cases(cuda):
+    """Empty batches, points far outside, on the bounds, at infinity and with
+    a NaN coordinate: the grid path returns what the tree walk returns."""
+    import torch
+    from devil_ray_b200 import _lib as L
+    from devil_ray_b200 import api
+    _, g = _gpu(cuda, "trilinear_12")
+    bvh = g.get_bvh()
+    grid = bvh.without_grid().build_grid(0.75)
+    tree = api.BatchedLocator(g, tol=1e-5, max_steps=20, bvh=bvh.without_grid())
+    fast = api.BatchedLocator(g, tol=1e-5, max_steps=20, bvh=grid)
+    c, r = fast.locate(np.zeros((0, 3), np.float32))
+    assert c.numel() == 0
+    pts = np.array([[5, 5, 5], [-1, 0.5, 0.5], [np.nan, 0.5, 0.5], [0.5, np.inf, 0.5],
+                    [-np.inf, 0.2, 0.2], [0, 0, 0], [1, 1, 1], [0.5, 0.5, 0.5],
+                    [1e30, -1e30, 0.5]], np.float32)
+    c0, r0 = tree.locate(pts)
+    c1, r1 = fast.locate(pts)
+    torch.cuda.synchronize()
+    assert torch.equal(c0, c1)
+    assert torch.equal(r0.view(torch.int32), r1.view(torch.int32))
+    c1 = c1.cpu().numpy()
+    assert (c1[:5] == -1).all() and c1[8] == -1 and c1[7] >= 0
