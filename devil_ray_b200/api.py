@@ -205,11 +205,12 @@ class UnstructuredMesh:
         return m
 
     def face_neighbors(self, stream=None):
-        """Element across each of the six faces of every element (-1 on the
-        boundary), built once (drb_mesh_face_neighbors); the volume march
-        follows rays across faces with it."""
+        """Element across each face of every element (six per hex, four per
+        tet; -1 on the boundary), built once (drb_mesh_face_neighbors); the
+        volume march follows rays across faces with it."""
         if getattr(self, "_neighbors", None) is None:
-            nb = torch.empty((max(self.n_elem, 1), 6), dtype=torch.int32, device=self.device)
+            fpe = 4 if self.shape == L.SHAPE_SIMPLEX else 6
+            nb = torch.empty((max(self.n_elem, 1), fpe), dtype=torch.int32, device=self.device)
             d = self.desc()
             L.check(L.lib().drb_mesh_face_neighbors(C.byref(d), _ptr(nb), _stream(stream)),
                     "drb_mesh_face_neighbors")

@@ -134,10 +134,10 @@ const drb_bvh *ElementMesh::device_bvh ()
       drb_check (drb_tet_hull_planes (&g.mesh, g.hull.p, nullptr), "drb_tet_hull_planes");
       g.mesh.hull_planes = g.hull.p;
     }
-    if (m_dim == 3 && m_etype == Tensor)
+    if (m_dim == 3)
     {
       // face neighbours: the volume march steps across faces with them
-      g.nbr.alloc ((size_t)6 * cells ());
+      g.nbr.alloc ((size_t)(m_etype == Simplex ? 4 : 6) * std::max (cells (), 1));
       drb_check (drb_mesh_face_neighbors (&g.mesh, g.nbr.p, nullptr), "drb_mesh_face_neighbors");
       g.mesh.face_neighbors = g.nbr.p;
     }

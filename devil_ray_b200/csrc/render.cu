@@ -470,16 +470,36 @@ DRB_D void blend (float4 &front, const float4 &back)
 }
 
 // A predicted reference point outside the previous element means the sample
-// has left it.  Hexes with a face table step across the exit face at once
-// (margin 0: the face walk comes back if the prediction was off); without
-// one, and for tets (whose next stop is the BVH), a prediction within this
-// margin is solved in the previous element first.
+// has left it.  With a face table the march steps across the exit face at
+// once (margin 0: the face walk comes back if the prediction was off);
+// without one, whose next stop is the BVH, a prediction within this margin
+// is solved in the previous element first.
 constexpr float kCoherentMargin = 0.1f;
 
 // Face by which a reference point outside [0,1]^3 leaves the element (the
 // axis with the largest excursion; faces u0, u1, v0, v1, w0, w1), -1 inside.
+// Tets: the most negative of u, v, w and 1 - u - v - w (faces u=0, v=0,
+// w=0, u+v+w=1).
+template <int S = kTensor>
 DRB_D int exit_face (const float (&x)[3])
 {
+  if (S == kSimplex)
+  {
+    int f = -1;
+    float worst = 0.f;
+    const float t = 1.f - (x[0] + x[1] + x[2]);
+#pragma unroll
+    for (int d = 0; d < 3; ++d)
+    {
+      if (-x[d] > worst)
+      {
+        worst = -x[d];
+        f = d;
+      }
+    }
+    if (-t > worst) f = 3;
+    return f;
+  }
   int f = -1;
   float worst = 0.f;
 #pragma unroll
@@ -500,10 +520,18 @@ DRB_D int exit_face (const float (&x)[3])
 }
 
 // The element across face f, and the guess carried over into its frame
-// (the structured-lattice case: the same axes, shifted by one).
+// (hexes: the structured-lattice case, the same axes shifted by one; tets,
+// whose neighbours' frames are unrelated: the neighbour's centroid).
+template <int S = kTensor>
 DRB_D int step_across (const VolumeParams &vp, int el, int f, float (&x)[3])
 {
   if (f < 0 || !vp.nbr) return -1;
+  if (S == kSimplex)
+  {
+    const int nb = __ldg (vp.nbr + 4 * (size_t)el + f);
+    if (nb >= 0) x[0] = x[1] = x[2] = 0.25f;
+    return nb;
+  }
   const int nb = __ldg (vp.nbr + 6 * (size_t)el + f);
   if (nb >= 0) x[f >> 1] += (f & 1) ? -1.f : 1.f;
   return nb;
@@ -514,14 +542,14 @@ DRB_D int step_across (const VolumeParams &vp, int el, int f, float (&x)[3])
 // the previous solve's Jacobian (lu), so that the solve usually converges in
 // two steps.  When the prediction (or that solve) leaves the element, the
 // element across the exit face is tried (face-neighbour table), and from its
-// solve the next one, up to kFaceSteps elements (a ray passing near an edge
-// or a corner crosses two or three faces between samples).  Then,
-// or in plain mode, the BVH candidates in the reference's order; the same
-// acceptance rule throughout.  All candidates go through one Newton call
-// site, which keeps the kernel's code small.  On success lu holds the
-// located solve's Jacobian.  Tets (S = kSimplex) have no face table: a
-// prediction outside the previous element goes straight to the BVH.
-constexpr int kFaceSteps = 3;
+// solve the next one, up to face_steps<S>() elements (a ray passing near an
+// edge or a corner of a hex crosses two or three faces between samples; the
+// six tets of a cube are thinner).  Tets take the neighbour's centroid as
+// the first guess.  Then, or in plain mode, the BVH candidates in the
+// reference's order; the same acceptance rule throughout.  All candidates
+// go through one Newton call site, which keeps the kernel's code small.  On
+// success lu holds the located solve's Jacobian.
+template <int S> constexpr int face_steps () { return S == kSimplex ? 6 : 3; }
 template <int P, bool WIDE, int S = kTensor>
 DRB_D int locate_sample (const VolumeParams &vp, const float (&pt)[3], const float (&step)[3],
                          int prev_el, const float (&prev_ref)[3], bool prev2_ok,
@@ -554,14 +582,14 @@ DRB_D int locate_sample (const VolumeParams &vp, const float (&pt)[3], const flo
       x[1] = prev_ref[1] + dr[1];
       x[2] = prev_ref[2] + dr[2];
     }
-    const float margin = (S == kTensor && vp.nbr) ? 0.f : kCoherentMargin;
+    const float margin = vp.nbr ? 0.f : kCoherentMargin;
     if (S == kSimplex ? is_inside_simplex (x, margin) : is_inside_ref (x, margin))
     {
       el = prev_el;
     }
     else
     {
-      el = S == kSimplex ? -1 : step_across (vp, prev_el, exit_face (x), x);
+      el = step_across<S> (vp, prev_el, exit_face<S> (x), x);
       crossed = 1;
     }
   }
@@ -588,11 +616,11 @@ DRB_D int locate_sample (const VolumeParams &vp, const float (&pt)[3], const flo
       ref[2] = x[2];
       return el;
     }
-    if (S == kTensor && leaf < 0 && crossed < kFaceSteps)
+    if (leaf < 0 && crossed < face_steps<S> ())
     {
       // the solve ended outside its element: step across its exit face
       ++crossed;
-      el = step_across (vp, el, exit_face (x), x);
+      el = step_across<S> (vp, el, exit_face<S> (x), x);
       if (el >= 0) continue;
     }
     el = -1;
@@ -1183,7 +1211,7 @@ static int volume_common (const drb_mesh *mesh, const drb_mesh *field, const drb
   vp.field_idx = field->ctrl_idx;
   vp.field_vals = field->values;
   vp.fstride = packed_stride (nd, 1);
-  vp.nbr = mesh->shape == DRB_SHAPE_TENSOR ? mesh->face_neighbors : nullptr;
+  vp.nbr = mesh->face_neighbors;
   vp.tf = (const float4 *)tf;
   vp.tf_size = tf_size;
   // DeviceColorMap: range of the field's control values, rcp_safe(length)

@@ -223,8 +223,8 @@ class Volume:
 
     def __init__(self, mesh: UnstructuredMesh, field: UnstructuredField):
         self.mesh, self.field_ = mesh, field
-        if mesh.dim == 3 and mesh.shape == L.SHAPE_TENSOR:
-            mesh.face_neighbors()  # the march steps across hex faces with them
+        if mesh.dim == 3:
+            mesh.face_neighbors()  # the march steps across element faces with them
         self.n_samples = 100
         self.lighting = True
         self.cmap = ColorMap()

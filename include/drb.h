@@ -90,8 +90,9 @@ typedef struct drb_mesh
   const float *values;   /* device float[n_ctrl * ncomp] */
   const float *packed;   /* optional device float[n_elem * drb_packed_stride_shape()]:
                             element-major copy made by drb_pack_elements(), or NULL */
-  const int *face_neighbors; /* optional device int32[6 * n_elem] of a hex geometry
-                            mesh (drb_mesh_face_neighbors), or NULL */
+  const int *face_neighbors; /* optional device int32[6 * n_elem] of a hex or
+                            int32[4 * n_elem] of a tet geometry mesh
+                            (drb_mesh_face_neighbors), or NULL */
   int shape;             /* drb_shape; 0 (tensor) when zero-initialised */
   const float *hull_planes; /* optional device float[20 * n_elem] of a tet geometry
                             mesh (drb_tet_hull_planes), or NULL */
@@ -108,10 +109,11 @@ typedef struct drb_mesh
  * unfiltered solve. */
 int drb_tet_hull_planes (const drb_mesh *mesh, float *planes, void *stream);
 
-/* Face neighbours of a hex mesh (no reference counterpart; faces are
- * matched by their four corner control points, as MeshBoundary matches
- * them, mesh_utils.cpp:98-398): neighbors[6 e + f] is the element across
- * face f of element e (f = u0, u1, v0, v1, w0, w1), -1 on the boundary.
+/* Face neighbours of a hex or tet mesh (no reference counterpart; faces
+ * are matched by their corner control points, as MeshBoundary matches them,
+ * mesh_utils.cpp:98-398): for a hex, neighbors[6 e + f] is the element
+ * across face f of element e (f = u0, u1, v0, v1, w0, w1); for a tet,
+ * neighbors[4 e + f] with f = u=0, v=0, w=0, u+v+w=1; -1 on the boundary.
  * The volume march uses it (through drb_mesh.face_neighbors) to step into
  * the next element across the face a ray leaves by before searching the
  * BVH. */

@@ -160,6 +160,41 @@ def test_tet_batched_identical_to_plain(cuda, p, row_mode):
     assert torch.equal(ref0.view(torch.int32), ref1.view(torch.int32))
 
 
+@pytest.mark.parametrize("p", [1, 2])
+def test_tet_face_neighbors(cuda, p):
+    """Tet face-neighbour table against a NumPy restatement: face f of
+    element e (u=0, v=0, w=0, u+v+w=1, by its three corner control points)
+    and the other element with the same three corners; 2 (6 n^2) boundary
+    faces on the n^3 x 6 Kuhn mesh."""
+    import torch
+    from devil_ray_b200 import meshgen
+    n = 6
+    m = _mesh(p, n)
+    g = _gpu(m, cuda)
+    nb = g.face_neighbors().cpu().numpy()
+    torch.cuda.synchronize()
+    nd = meshgen.tet_dofs(p)
+    conn = np.asarray(m.ctrl_idx).reshape(-1, nd)
+    # corner dofs of the (i, j, k) layout: u vertex (p,0,0), v vertex
+    # (0,p,0), w vertex (0,0,p), origin (0,0,0)
+    iv = sum(p + 1 - q for q in range(p))
+    U, V, W, O = conn[:, p], conn[:, iv], conn[:, nd - 1], conn[:, 0]
+    faces = [(V, W, O), (U, W, O), (U, V, O), (U, V, W)]
+    owner = {}
+    for f, cs in enumerate(faces):
+        for e, key in enumerate(zip(*(np.sort(np.stack(cs, 1), axis=1).T))):
+            owner.setdefault(key, []).append((e, f))
+    want = np.full((conn.shape[0], 4), -1, np.int64)
+    for key, lst in owner.items():
+        assert len(lst) <= 2
+        if len(lst) == 2:
+            (a, fa), (b, fb) = lst
+            want[a, fa], want[b, fb] = b, a
+    assert nb.shape == (conn.shape[0], 4)
+    assert np.array_equal(nb, want)
+    assert (nb < 0).sum() == 2 * 6 * n * n
+
+
 @pytest.mark.parametrize("p", ORDERS)
 def test_tet_leaf_maps_match_fp64(cuda, p):
     """drb_bvh_leaf_maps on a tet mesh: each sampled leaf's record holds its
@@ -249,16 +284,22 @@ def test_tet_point_location_field_values(cuda, ref, p):
             assert np.abs(vals[sel] - rv).max() < 1e-4
 
 
-def test_tet_unsupported_entry_points_fail_loudly(cuda):
+def test_face_neighbors_reject_2d_meshes(cuda):
+    """Face tables are for hex and tet meshes: a 2D descriptor is rejected
+    before anything is written."""
     import ctypes as C
+    import torch
     from devil_ray_b200 import _lib as L
     m = _mesh(1, n=2)
     g = _gpu(m, cuda)
     d = g.desc()
-    nb = C.c_void_p(g.packed.data_ptr())
-    st = L.lib().drb_mesh_face_neighbors(C.byref(d), nb, None)
+    d.dim = 2
+    buf = torch.full((4 * g.n_elem,), 7, dtype=torch.int32, device=cuda)
+    st = L.lib().drb_mesh_face_neighbors(C.byref(d), C.c_void_p(buf.data_ptr()), None)
     assert st != 0
-    assert "hex" in L.lib().drb_last_error().decode()
+    assert "hex or tet" in L.lib().drb_last_error().decode()
+    torch.cuda.synchronize()
+    assert bool((buf == 7).all())
 
 
 @pytest.mark.parametrize("p", [1, 2, 3])
