@@ -137,3 +137,33 @@ def test_grid_locate_edge_cases(cuda):
     assert torch.equal(r0.view(torch.int32), r1.view(torch.int32))
     c1 = c1.cpu().numpy()
     assert (c1[:5] == -1).all() and c1[8] == -1 and c1[7] >= 0
+
+
+@pytest.mark.parametrize("kind", ["quad", "tri"])
+def test_grid_locate_equals_tree_2d(cuda, kind):
+    """2D quad and triangle meshes (their boxes are flat in z, so the grid
+    has one cell across z): grid and tree give the same answers bit for
+    bit, with queries on and off the mesh plane."""
+    import torch
+    from devil_ray_b200 import _lib as L
+    from devil_ray_b200 import api, meshgen
+    if kind == "quad":
+        m = meshgen.quad_warped_mesh(24, 2, 0.04, jitter=0.004, seed=9)
+        g = api.UnstructuredMesh(m.ctrl_idx, m.xyz, 2, dim=2, device=cuda)
+    else:
+        m = meshgen.tri_warped_mesh(16, 2, 0.04, jitter=0.004, seed=9)
+        g = api.UnstructuredMesh(m.ctrl_idx, m.xyz, 2, dim=2, device=cuda, shape=L.SHAPE_SIMPLEX)
+    rng = np.random.default_rng(3)
+    xy = rng.uniform(-0.05, 1.05, size=(50000, 2))
+    z = np.where(rng.random(50000) < 0.9, 0.0, 0.01)
+    q = np.concatenate([xy, z[:, None]], 1).astype(np.float32)
+    bvh = g.get_bvh()
+    tree = api.BatchedLocator(g, tol=1e-5, max_steps=20, bvh=bvh.without_grid())
+    grid = api.BatchedLocator(g, tol=1e-5, max_steps=20, bvh=bvh.without_grid().build_grid(1.0))
+    c0, r0, i0, a0, _ = tree.locate(q, stats=True)
+    c1, r1, i1, a1, _ = grid.locate(q, stats=True)
+    torch.cuda.synchronize()
+    assert grid.bvh.grid_geom[0][2] == 1
+    assert torch.equal(c0, c1) and torch.equal(r0.view(torch.int32), r1.view(torch.int32))
+    assert torch.equal(i0, i1) and torch.equal(a0, a1)
+    assert (c1 >= 0).float().mean() > 0.5
