@@ -1449,7 +1449,7 @@ def main():
         # drb_locate_host: chunked copies in and out overlapped with the
         # locate; the chunk size that pipelines best on this batch
         chunk_ms = {}
-        for ch in (1 << 20, 1 << 21):
+        for ch in (1 << 19, 1 << 20, 1 << 21):
             head_loc.locate_host(host_pts, out=(host_cell, host_ref), chunk=ch)
             chunk_ms[ch] = timed(lambda: head_loc.locate_host(host_pts, out=(host_cell, host_ref),
                                                                chunk=ch), 3)
@@ -1466,6 +1466,26 @@ def main():
 
     e2e_step()
     e2e_ms = timed(e2e_step, args.steps) / args.steps
+    # the copies alone, both directions at once on two streams: the floor
+    # of the end-to-end time
+    s_in, s_out = torch.cuda.Stream(), torch.cuda.Stream()
+    host_back = torch.empty((n, 4), dtype=torch.float32).pin_memory()
+    dev_out = torch.empty((n, 4), dtype=torch.float32, device=dev)
+
+    def copies_only():
+        cur = torch.cuda.current_stream()
+        s_in.wait_stream(cur)
+        s_out.wait_stream(cur)
+        with torch.cuda.stream(s_in):
+            dpts.copy_(host_pts, non_blocking=True)
+        with torch.cuda.stream(s_out):
+            host_back.copy_(dev_out, non_blocking=True)
+        cur.wait_stream(s_in)
+        cur.wait_stream(s_out)
+
+    copies_only()
+    copy_ms = timed(copies_only, 3) / 3
+    del host_back, dev_out
     e2e_located = int((host_cell >= 0).sum())
     e2e_value = job_located(e2e_located) / (e2e_ms * 1e-3)
 
@@ -1561,6 +1581,7 @@ def main():
             "e2e": {"value": e2e_value, "unit": "points/s",
                     "h2d_bytes_per_step": int(n * 12), "d2h_bytes_per_step": int(n * 16),
                     "ms_per_step": e2e_ms, "chunk": e2e_chunk,
+                    "copies_only_ms": copy_ms,
                     "api": "drb_locate_host (pinned host buffers, copies overlapped)"
                            if head_loc is not None else
                            "copy in, locate, copy out on one stream"},
