@@ -1287,15 +1287,18 @@ def main():
     loc_grid = api.BatchedLocator(mesh, tol=TOL, max_steps=MAX_STEPS,
                                   guess_mode=L.GUESS_SUBBOX_LINEAR, bvh=gbvh)
     # the tuner's sample is sparser than the full batch: keep the fastest of
-    # its pick and the tree leg's shape on the full batch, each with the
-    # queries read through the order (1) or staged as records first (2)
+    # its pick, the tree leg's shape and two fixed shapes on the full batch,
+    # each with the queries read through the order (1) or staged as records
+    # first (2)
     tuned_cfg, _ = loc_grid.tune(pts[: min(n, 1 << 21)])
-    cands = []
-    for c in (tuned_cfg, best_cfg):
+    cands, seen = [], set()
+    shapes = [tuple(c.as_dict()[k] for k in ("block", "blocks_per_sm", "chunk", "reg_elements"))
+              for c in (tuned_cfg, best_cfg)] + [(64, 0, 64, 0), (128, 0, 64, 0)]
+    for b_, bps_, ch_, rows_ in shapes:
         for sq in (1, 2):
-            d = c.as_dict()
-            cands.append(L.DrbLocateConfig(d["block"], d["blocks_per_sm"], d["chunk"], sq,
-                                           d["reg_elements"]))
+            if (b_, bps_, ch_, rows_, sq) not in seen:
+                seen.add((b_, bps_, ch_, rows_, sq))
+                cands.append(L.DrbLocateConfig(b_, bps_, ch_, sq, rows_))
     shape_ms = []
     for c in cands:
         loc_grid.config = c
