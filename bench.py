@@ -1291,14 +1291,13 @@ def main():
     # each with the queries read through the order (1) or staged as records
     # first (2)
     tuned_cfg, _ = loc_grid.tune(pts[: min(n, 1 << 21)])
-    cands, seen = [], set()
+    # (a fixed count on every rank: each trial is a collective timing)
+    cands = []
     shapes = [tuple(c.as_dict()[k] for k in ("block", "blocks_per_sm", "chunk", "reg_elements"))
               for c in (tuned_cfg, best_cfg)] + [(64, 0, 64, 0), (128, 0, 64, 0)]
     for b_, bps_, ch_, rows_ in shapes:
         for sq in (1, 2):
-            if (b_, bps_, ch_, rows_, sq) not in seen:
-                seen.add((b_, bps_, ch_, rows_, sq))
-                cands.append(L.DrbLocateConfig(b_, bps_, ch_, sq, rows_))
+            cands.append(L.DrbLocateConfig(b_, bps_, ch_, sq, rows_))
     shape_ms = []
     for c in cands:
         loc_grid.config = c
