@@ -76,7 +76,7 @@ def parse():
                     help="launch shape of --profile: block, blocks per SM (0 = all "
                          "resident), chunk, row mode, query order mode (default 1)")
     ap.add_argument("--guess", default="centre", choices=["centre", "subref", "linear"],
-                    help="first guess of --profile")
+                    help="first guess of --profile and --profile-tet")
     ap.add_argument("--grid", type=float, default=0.0, metavar="SCALE",
                     help="--profile / --profile-tet over grid candidate lists with cells of "
                          "SCALE times the mean leaf extent (0: the 4-wide tree)")
@@ -1010,7 +1010,9 @@ def profile_tet(dev, args):
     mesh = api.UnstructuredMesh(m.ctrl_idx, m.xyz, m.order, device=dev, shape=L.SHAPE_SIMPLEX)
     mesh.get_bvh()
     q = torch.as_tensor(meshgen.uniform_queries(args.profile_tet, 77), device=dev)
-    loc = api.BatchedLocator(mesh, tol=TOL, max_steps=MAX_STEPS,
+    guess = {"centre": L.GUESS_ELEM_CENTER, "subref": L.GUESS_SUBREF_CENTER,
+             "linear": L.GUESS_SUBBOX_LINEAR}[args.guess]
+    loc = api.BatchedLocator(mesh, tol=TOL, max_steps=MAX_STEPS, guess_mode=guess,
                              config=L.DrbLocateConfig(256, 0, 32, 1, 1))
     if args.grid > 0:
         loc.bvh = mesh.get_bvh().without_grid().build_grid(args.grid)
@@ -1026,7 +1028,11 @@ def profile_tet(dev, args):
     torch.cuda.synchronize()
     ms = e0.elapsed_time(e1) / args.steps
     located = int((cell >= 0).sum())
-    print(json.dumps({"profile_tet": args.profile_tet, "grid": args.grid, "ms_per_step": ms,
+    _, _, its, cas, _ = loc.locate(q, stats=True)
+    loc_ok = cell >= 0
+    print(json.dumps({"profile_tet": args.profile_tet, "grid": args.grid, "guess": args.guess,
+                      "mean_newton_iters": float(its[loc_ok].float().mean()),
+                      "mean_candidates": float(cas[loc_ok].float().mean()), "ms_per_step": ms,
                       "located_fraction": located / q.shape[0],
                       "located_pts_per_s": located / (ms * 1e-3)}))
     return 0
