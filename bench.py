@@ -584,8 +584,9 @@ def learned_leg(dev, args, mesh, pts, cfg, timed, job_located, baselines, plain_
 def second_mesh_leg(dev, args, pts, cfg, timed, job_located):
     """The learned-guess config's second mesh (64^3 order 2, 25 % trilinear
     distortion): the same held-out queries located by the plain kernel, the
-    batched kernel with the sub-box-centre guess, and the learned path
-    trained on this mesh."""
+    batched kernel with the sub-box-centre and linear guesses (over the tree
+    and over grid candidate lists), and the learned path trained on this
+    mesh."""
     import torch
     from devil_ray_b200 import _lib as L
     from devil_ray_b200 import api, meshgen
@@ -616,6 +617,16 @@ def second_mesh_leg(dev, args, pts, cfg, timed, job_located):
     lin_ms = timed(lambda: lin.locate(pts, out=(cell, ref)), args.steps) / args.steps
     _, _, it_l, _, _ = lin.locate(pts, stats=True)
     lin_value = job_located(located) / (lin_ms * 1e-3)
+    # the linear guess over grid candidate lists (the headline path's form)
+    gbvh = mesh.get_bvh().without_grid().build_grid(GRID_CELL_SCALE)
+    gcfg = L.DrbLocateConfig(64, 0, 64, 2, 0)
+    grid = api.BatchedLocator(mesh, tol=TOL, max_steps=MAX_STEPS,
+                              guess_mode=L.GUESS_SUBBOX_LINEAR, config=gcfg, bvh=gbvh)
+    for _ in range(2):
+        grid.locate(pts, out=(cell, ref))
+    grid_ms = timed(lambda: grid.locate(pts, out=(cell, ref)), args.steps) / args.steps
+    grid_value = job_located(located) / (grid_ms * 1e-3)
+    del grid, gbvh
     centre = api.BatchedLocator(mesh, tol=TOL, max_steps=MAX_STEPS,
                                 guess_mode=L.GUESS_ELEM_CENTER, config=cfg)
     _, _, it_c, _, _ = centre.locate(pts, stats=True)
@@ -631,6 +642,10 @@ def second_mesh_leg(dev, args, pts, cfg, timed, job_located):
                                "mean_newton_iters": float(it_s.float().mean())},
             "batched_linear": {"value": lin_value, "ms_per_step": lin_ms,
                                "mean_newton_iters": float(it_l.float().mean())},
+            "batched_grid": {"value": grid_value, "ms_per_step": grid_ms,
+                             "launch_config": gcfg.as_dict(),
+                             "note": "sub-box linear guess over grid candidate lists, "
+                                     "staged query records"},
             "learned": lg}
 
 
