@@ -631,7 +631,8 @@ def second_mesh_leg(dev, args, pts, cfg, timed, job_located):
                                 guess_mode=L.GUESS_ELEM_CENTER, config=cfg)
     _, _, it_c, _, _ = centre.locate(pts, stats=True)
     lg = learned_leg(dev, args, mesh, pts, cfg, timed, job_located,
-                     {"batched_subref": sub_value, "batched_linear": lin_value}, plain_value,
+                     {"batched_subref": sub_value, "batched_linear": lin_value,
+                      "batched_grid": grid_value}, plain_value,
                      float(it_c.float().mean()))
     lg.pop("_locate", None)
     return {"workload": "locate_64_d25: 64^3 hex order 2, trilinear distortion 25%, the same "
@@ -1382,7 +1383,7 @@ def main():
         try:
             learned = learned_leg(dev, args, mesh, pts, best_cfg, timed, job_located,
                                   {"batched_subref": sub_value, "batched_centre": batched_value,
-                                   "batched_linear": lin_value},
+                                   "batched_linear": lin_value, "batched_grid": grid_value},
                                   plain_value, mean_it)
         except Exception as exc:
             learned = {"error": repr(exc)}
