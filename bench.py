@@ -535,12 +535,15 @@ def tet_locate(dev, args, with_cpu):
 
 
 def learned_leg(dev, args, mesh, pts, cfg, timed, job_located, baselines, plain_value,
-                mean_it_centre):
+                mean_it_centre, grid=None):
     """Train the guess network on the mesh (4M Newton solutions of the
     method itself, the library's tcgen05 kernels) and time the learned-guess
     path on the held-out queries: located pts/s, its iteration histogram,
     the fallback rate of the guessed solves on held-out in-element pairs, and
-    its ratio to the plain kernel and to the batched paths without it."""
+    its ratio to the plain kernel and to the batched paths without it.
+    grid = (BVH with grid lists, launch config): the learned path over the
+    grid lists is timed too, and the faster of the two forms is the leg's
+    value."""
     import torch
     from devil_ray_b200 import learned as LG
     n = pts.shape[0]
@@ -557,6 +560,19 @@ def learned_leg(dev, args, mesh, pts, cfg, timed, job_located, baselines, plain_
         ll.locate(pts, out=(cell_l, ref_l))
     ms_l = timed(lambda: ll.locate(pts, out=(cell_l, ref_l)), args.steps) / args.steps
     located_l = int((cell_l >= 0).sum().item())
+    forms = {"tree": {"ms_per_step": ms_l}}
+    if grid is not None:
+        llg = LG.LearnedLocator(mesh, model, TOL, MAX_STEPS, config=grid[1], bvh=grid[0])
+        for _ in range(3):
+            llg.locate(pts, out=(cell_l, ref_l))
+        ms_g = timed(lambda: llg.locate(pts, out=(cell_l, ref_l)), args.steps) / args.steps
+        forms["grid_lists"] = {"ms_per_step": ms_g}
+        if int((cell_l >= 0).sum().item()) != located_l:
+            raise RuntimeError("learned path over grid lists located a different count")
+        if ms_g < ms_l:
+            ll, ms_l = llg, ms_g
+    for f in forms.values():
+        f["value"] = job_located(located_l) / (f["ms_per_step"] * 1e-3)
     _, _, it_l, _, _ = ll.locate(pts, stats=True)
     hist_l = torch.bincount(it_l.long().clamp(max=40), minlength=41).cpu().numpy().tolist()
     he, hp, hl, hw = LG.training_set(mesh, 1 << 20, seed=12345)
@@ -566,6 +582,7 @@ def learned_leg(dev, args, mesh, pts, cfg, timed, job_located, baselines, plain_
     ok = fc
     value = job_located(located_l) / (ms_l * 1e-3)
     out = {"value": value, "ms_per_step": ms_l, "located": located_l,
+           "form": "grid_lists" if ll.bvh is not None else "tree", "forms": forms,
            "mean_newton_iters": float(it_l.float().mean()),
            "mean_newton_iters_centre": mean_it_centre,
            "iteration_histogram": hist_l,
@@ -626,15 +643,16 @@ def second_mesh_leg(dev, args, pts, cfg, timed, job_located):
         grid.locate(pts, out=(cell, ref))
     grid_ms = timed(lambda: grid.locate(pts, out=(cell, ref)), args.steps) / args.steps
     grid_value = job_located(located) / (grid_ms * 1e-3)
-    del grid, gbvh
+    del grid
     centre = api.BatchedLocator(mesh, tol=TOL, max_steps=MAX_STEPS,
                                 guess_mode=L.GUESS_ELEM_CENTER, config=cfg)
     _, _, it_c, _, _ = centre.locate(pts, stats=True)
     lg = learned_leg(dev, args, mesh, pts, cfg, timed, job_located,
                      {"batched_subref": sub_value, "batched_linear": lin_value,
                       "batched_grid": grid_value}, plain_value,
-                     float(it_c.float().mean()))
+                     float(it_c.float().mean()), grid=(gbvh, cfg))
     lg.pop("_locate", None)
+    del gbvh
     return {"workload": "locate_64_d25: 64^3 hex order 2, trilinear distortion 25%, the same "
                         f"{n} held-out queries, tol 1e-5, 20 steps",
             "located_fraction": located / n,
@@ -1384,7 +1402,7 @@ def main():
             learned = learned_leg(dev, args, mesh, pts, best_cfg, timed, job_located,
                                   {"batched_subref": sub_value, "batched_centre": batched_value,
                                    "batched_linear": lin_value, "batched_grid": grid_value},
-                                  plain_value, mean_it)
+                                  plain_value, mean_it, grid=(gbvh, grid_cfg))
         except Exception as exc:
             learned = {"error": repr(exc)}
         if learned.get("value", 0.0) > head_value:

@@ -151,6 +151,25 @@ struct GridLists
   float inv[3] = { 0.f, 0.f, 0.f };
 };
 
+// Grid lists of a BVH, or empty ones (start null) when it has none.
+inline GridLists grid_lists (const drb_bvh *bvh)
+{
+  GridLists gl;
+  if (bvh->grid_start && bvh->grid_entries && bvh->grid_boxes)
+  {
+    gl.start = bvh->grid_start;
+    gl.entries = bvh->grid_entries;
+    gl.boxes = (const float4 *)bvh->grid_boxes;
+    for (int d = 0; d < 3; ++d)
+    {
+      gl.dims[d] = bvh->grid_dims[d];
+      gl.origin[d] = bvh->grid_origin[d];
+      gl.inv[d] = bvh->grid_inv[d];
+    }
+  }
+  return gl;
+}
+
 // Cell coordinate of x along one grid axis: floor((x - o) * inv) clamped to
 // [0, g - 1].  Monotone in x, so every point of a box [lo, hi] falls in a
 // cell between those of lo and hi; the grid build files each leaf under

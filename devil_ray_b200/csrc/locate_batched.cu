@@ -569,24 +569,6 @@ int traversal_kind (const LocateParams &lp, const GridLists &gl)
   return gl.start ? 2 : lp.wide ? 1 : 0;
 }
 
-GridLists grid_lists (const drb_bvh *bvh)
-{
-  GridLists gl;
-  if (bvh->grid_start && bvh->grid_entries && bvh->grid_boxes)
-  {
-    gl.start = bvh->grid_start;
-    gl.entries = bvh->grid_entries;
-    gl.boxes = (const float4 *)bvh->grid_boxes;
-    for (int d = 0; d < 3; ++d)
-    {
-      gl.dims[d] = bvh->grid_dims[d];
-      gl.origin[d] = bvh->grid_origin[d];
-      gl.inv[d] = bvh->grid_inv[d];
-    }
-  }
-  return gl;
-}
-
 int launch_persistent (const drb_mesh *mesh, int mode, dim3 grid, int block, cudaStream_t s,
                        const LocateParams &lp, const GridLists &gl, const float *pts, const int *ord, int n, int chunk,
                        int *head, int *cell, float *ref, drb_query_stats st, Staging sg = Staging ())

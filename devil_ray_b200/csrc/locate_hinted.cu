@@ -3,7 +3,9 @@
 //   first_candidate_kernel  traverse each query (in Morton order) to its first
 //                           candidate leaf in the reference's traversal order
 //                           (device_mesh.hpp:248-318) without solving; the
-//                           (query, element) pairs feed the guess network
+//                           (query, element) pairs feed the guess network.
+//                           With grid lists the first leaf comes from the
+//                           query's cell (first_grid_candidate_kernel).
 //   locate_hinted_kernel    persistent warps as in drb_locate_batched; a query
 //                           first solves in its first candidate from the given
 //                           guess (element-centre fallback), and only if that
@@ -34,6 +36,25 @@ __global__ void first_candidate_kernel (const float4 *__restrict__ nodes, const 
   int sp = 0, cur = 0, visited = 0;
   todo[0] = kBarrier;
   const int leaf = next_leaf<WIDE> (nodes, wide, pt, todo, sp, cur, visited);
+  first_leaf[qi] = leaf;
+  if (first_elem) first_elem[qi] = leaf >= 0 ? __ldg (leaf_nodes + leaf) : -1;
+}
+
+// First candidate from the point's grid cell: the first listed leaf whose
+// box holds the point, which is the traversal's first leaf (the lists hold
+// the traversal's candidates in its order).
+__global__ void first_grid_candidate_kernel (GridLists gl, const int *__restrict__ leaf_nodes,
+                                             const float *__restrict__ pts,
+                                             const int *__restrict__ order, int n,
+                                             int *__restrict__ first_leaf, int *__restrict__ first_elem)
+{
+  const int pos = blockIdx.x * blockDim.x + threadIdx.x;
+  if (pos >= n) return;
+  const int qi = order ? order[pos] : pos;
+  const float pt[3] = { pts[3 * (size_t)qi], pts[3 * (size_t)qi + 1], pts[3 * (size_t)qi + 2] };
+  const int c = grid_cell (gl.dims, gl.origin, gl.inv, pt);
+  int cur = __ldg (gl.start + c), visited = 0;
+  const int leaf = next_grid_leaf (gl, pt, cur, __ldg (gl.start + c + 1), visited);
   first_leaf[qi] = leaf;
   if (first_elem) first_elem[qi] = leaf >= 0 ? __ldg (leaf_nodes + leaf) : -1;
 }
@@ -177,7 +198,11 @@ extern "C" int drb_first_candidates (const drb_bvh *bvh, const float *pts, int n
     return DRB_ERR_INVALID_ARG;
   }
   if (n == 0) return DRB_OK;
-  if (bvh->wide_nodes)
+  const GridLists gl = grid_lists (bvh);
+  if (gl.start)
+    first_grid_candidate_kernel<<<div_up (n, 128), 128, 0, (cudaStream_t)stream>>> (
+    gl, bvh->leaf_nodes, pts, order, n, first_leaf, first_elem);
+  else if (bvh->wide_nodes)
     first_candidate_kernel<true><<<div_up (n, 128), 128, 0, (cudaStream_t)stream>>> (
     (const float4 *)bvh->inner_nodes, (const float4 *)bvh->wide_nodes, bvh->leaf_nodes, pts, order,
     n, first_leaf, first_elem);

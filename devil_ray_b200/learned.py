@@ -256,20 +256,27 @@ def train(model: GuessMLP, mesh: UnstructuredMesh, samples=1 << 22, batch=16384,
 
 
 class LearnedLocator:
-    """Batched point location with the learned first guess."""
+    """Batched point location with the learned first guess.
+
+    bvh: None for the mesh's own BVH.  A BVH with grid lists
+    (BVH.build_grid) takes the first candidates from the query's cell and
+    solves through drb_locate_batched with the given guesses; otherwise the
+    hinted locate resumes the tree walk after the first candidate.  Both
+    equal drb_locate with DRB_GUESS_GIVEN."""
 
     def __init__(self, mesh: UnstructuredMesh, model: GuessMLP, tol=1e-5, max_steps=20,
-                 config: L.DrbLocateConfig | None = None):
+                 config: L.DrbLocateConfig | None = None, bvh=None):
         self.mesh, self.model = mesh, model
         self.tol, self.max_steps = tol, max_steps
         self.config = config
+        self.bvh = bvh
         self._order = BatchedLocator(mesh, tol, max_steps)
 
     def locate(self, points, order=None, stats=False, out=None, stream=None):
         pts = _dev(points, torch.float32, self.mesh.device).reshape(-1, 3)
         n = pts.shape[0]
         dev = self.mesh.device
-        bvh = self.mesh.get_bvh()
+        bvh = self.bvh if self.bvh is not None else self.mesh.get_bvh()
         if order is None:
             order = self._order.order(pts, stream)
         # Work on a Morton-ordered copy of the points: the first-candidate
@@ -294,11 +301,22 @@ class LearnedLocator:
         st = [torch.empty(n, dtype=torch.int32, device=dev) for _ in range(3)] if stats else None
         qs = L.DrbQueryStats(*(t.data_ptr() for t in st)) if stats else L.DrbQueryStats()
         opts = L.DrbNewtonOpts(self.tol, self.max_steps, L.GUESS_GIVEN, guess.data_ptr())
-        cfg = None if self.config is None else C.byref(self.config)
-        L.check(_lib().drb_locate_hinted(C.byref(self.mesh.desc()), C.byref(bvh.desc()),
-                                         _ptr(pts_s), n, None, _ptr(first_leaf),
-                                         C.byref(opts), cfg, _ptr(cell_s), _ptr(ref_s), qs,
-                                         _stream(stream)), "drb_locate_hinted")
+        if bvh.grid_start is not None:
+            # the points are in Morton order already: solve them in index order
+            cfg = L.DrbLocateConfig(128, 0, 64, 1, 0) if self.config is None else \
+                L.DrbLocateConfig(*(getattr(self.config, f) for f, _ in L.DrbLocateConfig._fields_))
+            cfg.sort_queries = 0
+            bd = bvh.desc()
+            L.check(_lib().drb_locate_batched(C.byref(self.mesh.desc()), C.byref(bd), _ptr(pts_s),
+                                              n, C.byref(opts), C.byref(cfg), _ptr(cell_s),
+                                              _ptr(ref_s), qs, _stream(stream)),
+                    "drb_locate_batched")
+        else:
+            cfg = None if self.config is None else C.byref(self.config)
+            L.check(_lib().drb_locate_hinted(C.byref(self.mesh.desc()), C.byref(bvh.desc()),
+                                             _ptr(pts_s), n, None, _ptr(first_leaf),
+                                             C.byref(opts), cfg, _ptr(cell_s), _ptr(ref_s), qs,
+                                             _stream(stream)), "drb_locate_hinted")
         cell.index_copy_(0, ol, cell_s)
         ref.index_copy_(0, ol, ref_s)
         if stats:

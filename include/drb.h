@@ -642,7 +642,9 @@ int drb_newton_pairs (const drb_mesh *mesh, const int *elem, const float *pts, i
                       int max_steps, const float *guess, float *ref, int *found, int *iters,
                       void *stream);
 /* First candidate leaf (and element) of each query in the traversal order of
- * DeviceMesh::locate (device_mesh.hpp:248-318); -1 when there is none. */
+ * DeviceMesh::locate (device_mesh.hpp:248-318); -1 when there is none.  With
+ * grid lists (drb_bvh_grid_build) the leaf comes from the query's cell: the
+ * same leaf. */
 int drb_first_candidates (const drb_bvh *bvh, const float *pts, int n, const int *order,
                           int *first_leaf, int *first_elem, void *stream);
 /* Persistent locate that starts at each query's first candidate (guess from

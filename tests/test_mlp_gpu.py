@@ -178,6 +178,44 @@ def test_hinted_locate_equals_plain_given_guess(cuda, setup):
     assert torch.equal(it0, it1) and torch.equal(ca0, ca1)
 
 
+def test_learned_locate_over_grid_equals_plain_given_guess(cuda, setup):
+    """Over a BVH with grid lists the first candidates come from the query's
+    cell and the solve runs through drb_locate_batched: the same first
+    leaves as the tree walk, and the same cells, reference points,
+    iterations and candidates as drb_locate with those guesses."""
+    import ctypes as C
+    import torch
+    from devil_ray_b200 import _lib as L
+    from devil_ray_b200 import learned as LG
+    from devil_ray_b200 import meshgen
+    mesh, model, *_ = setup
+    q = torch.as_tensor(meshgen.uniform_queries(50000, 23), device=cuda)
+    tree = mesh.get_bvh()
+    grid = tree.without_grid().build_grid(0.75)
+    ll = LG.LearnedLocator(mesh, model, tol=1e-5, max_steps=20, bvh=grid)
+    order = ll._order.order(q)
+    firsts = []
+    for b in (tree, grid):
+        fl = torch.empty(q.shape[0], dtype=torch.int32, device=cuda)
+        fe = torch.empty_like(fl)
+        L.check(LG._lib().drb_first_candidates(C.byref(b.desc()), C.c_void_p(q.data_ptr()),
+                                               q.shape[0], C.c_void_p(order.data_ptr()),
+                                               C.c_void_p(fl.data_ptr()),
+                                               C.c_void_p(fe.data_ptr()), None), "first")
+        firsts.append((fl, fe))
+    torch.cuda.synchronize()
+    assert torch.equal(firsts[0][0], firsts[1][0]) and torch.equal(firsts[0][1], firsts[1][1])
+    guess = model.guess(mesh, firsts[1][1], q)
+    c0, r0, it0, ca0, _ = mesh.locate(q, tol=1e-5, max_steps=20, guess_mode=L.GUESS_GIVEN,
+                                      guess=guess, stats=True)
+    c1, r1, it1, ca1, _ = ll.locate(q, order=order, stats=True)
+    torch.cuda.synchronize()
+    assert torch.equal(c0, c1)
+    assert torch.equal(r0, r1)
+    assert torch.equal(it0, it1) and torch.equal(ca0, ca1)
+    assert (c1 >= 0).float().mean() > 0.5
+
+
 @pytest.mark.parametrize("order", [2, 3])
 def test_training_reduces_newton_iterations(cuda, order):
     """Trained on the method's own solutions, the network's guess needs
