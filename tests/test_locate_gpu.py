@@ -282,13 +282,15 @@ def test_staged_equals_ordered_and_plain(cuda, name, guess):
         assert torch.equal(i0, i) and torch.equal(a0, a) and torch.equal(n0, nd)
 
 
-def test_stage_records_and_staged_kernel(cuda):
+@pytest.mark.parametrize("n", [1000, 80000, 2500000])
+def test_stage_records_and_staged_kernel(cuda, n):
     """drb_query_stage lists every query once, cell by cell along the Morton
     curve, with its input index in w; drb_locate_staged on those records
-    gives each query the answer drb_locate_batched gives it."""
+    gives each query the answer drb_locate_batched gives it.  The sizes
+    take the staging with no fine bits (one pass), one and three."""
     import torch
     from devil_ray_b200 import api
-    m, q, g = _setup(cuda, "trilinear_12", 80000, 29)
+    m, q, g = _setup(cuda, "trilinear_12", n, 29)
     loc = api.BatchedLocator(g, tol=1e-5, max_steps=20)
     rec = loc.stage(q)
     res = loc.locate_staged(rec, records=True)
@@ -303,6 +305,27 @@ def test_stage_records_and_staged_kernel(cuda):
     cell_of = res[:, 0].contiguous().view(torch.int32)
     assert torch.equal(cell_of, c0[idx])
     assert torch.equal(res[:, 1:].contiguous().view(torch.int32), r0[idx].view(torch.int32))
+    code = _morton_cells(rec[:, :3].cpu().numpy(), g.get_bvh().bounds)
+    assert np.all(np.diff(code) >= 0)
+
+
+def _morton_cells(p, bounds):
+    """Morton code (x lowest) of each point's query-order cell over the BVH
+    bounds, 3..7 bits per axis so that a cell holds about eight queries."""
+    n = p.shape[0]
+    bits = 3
+    while bits < 7 and (8 << (3 * bits)) < n:
+        bits += 1
+    code = np.zeros(n, np.int64)
+    for k in range(3):
+        lo, hi = np.float32(bounds[2 * k]), np.float32(bounds[2 * k + 1])
+        sc = np.float32(1.0) / np.float32(hi - lo)
+        t = ((p[:, k].astype(np.float32) - lo) * sc).astype(np.float32) * np.float32(1 << bits)
+        t = np.minimum(np.maximum(t, np.float32(0)), np.float32((1 << bits) - 1))
+        x = np.where(np.isnan(t), 0, t).astype(np.int64)
+        for b in range(bits):
+            code |= ((x >> b) & 1) << (3 * b + k)
+    return code
 
 
 def test_autotuner_config_is_valid_and_exact(cuda):
