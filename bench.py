@@ -1328,15 +1328,15 @@ def main():
                                   guess_mode=L.GUESS_SUBBOX_LINEAR, bvh=gbvh)
     # the tuner's sample is sparser than the full batch: keep the fastest of
     # its pick, the tree leg's shape and two fixed shapes on the full batch,
-    # each with the queries read through the order (1) or staged as records
-    # first (2)
+    # each with the queries read through the order (1), staged as records
+    # first (2), or with the results staged too and put back by a gather (3)
     tuned_cfg, _ = loc_grid.tune(pts[: min(n, 1 << 21)])
     # (a fixed count on every rank: each trial is a collective timing)
     cands = []
     shapes = [tuple(c.as_dict()[k] for k in ("block", "blocks_per_sm", "chunk", "reg_elements"))
               for c in (tuned_cfg, best_cfg)] + [(64, 0, 64, 0), (128, 0, 64, 0)]
     for b_, bps_, ch_, rows_ in shapes:
-        for sq in (1, 2):
+        for sq in (1, 2, 3):
             cands.append(L.DrbLocateConfig(b_, bps_, ch_, sq, rows_))
     shape_ms = []
     for c in cands:
@@ -1383,7 +1383,11 @@ def main():
     roof_loc = head_loc
     roof_stats = sub_stats if roof_loc is loc_sub else lin_stats if roof_loc is loc_lin else \
         grid_stats if roof_loc is loc_grid else (mean_it, mean_ca, mean_nd)
-    if roof_loc.config is not None and roof_loc.config.sort_queries >= 2:
+    if roof_loc.config is not None and roof_loc.config.sort_queries == 3:
+        qstaged = roof_loc.stage(pts)
+        res_rec = torch.empty((n, 4), dtype=torch.float32, device=dev)
+        roof_kern = lambda: roof_loc.locate_staged(qstaged, out=res_rec, records=True)
+    elif roof_loc.config is not None and roof_loc.config.sort_queries == 2:
         qstaged = roof_loc.stage(pts)
         roof_kern = lambda: roof_loc.locate_staged(qstaged, out=(cell, ref))
     else:

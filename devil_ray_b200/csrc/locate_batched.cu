@@ -92,12 +92,17 @@ __global__ void cell_count_kernel (const float *__restrict__ pts, int n, float x
   rank[i] = atomicAdd (hist + c, 1);
 }
 
+// order[pos] = i and, when pos_of is set, pos_of[i] = pos (written in input
+// order, so the inverse permutation costs a coalesced store).
 __global__ void cell_scatter_kernel (const unsigned *__restrict__ cell_of, const int *__restrict__ rank,
-                                     const int *__restrict__ offset, int n, int *__restrict__ order)
+                                     const int *__restrict__ offset, int n, int *__restrict__ order,
+                                     int *__restrict__ pos_of)
 {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= n) return;
-  order[__ldg (offset + cell_of[i]) + rank[i]] = i;
+  const int pos = __ldg (offset + cell_of[i]) + rank[i];
+  order[pos] = i;
+  if (pos_of) pos_of[i] = pos;
 }
 
 // ------------------------------------------------------- staged queries --
@@ -109,7 +114,7 @@ __global__ void cell_scatter_kernel (const unsigned *__restrict__ cell_of, const
 // scattering the records themselves would write 16 bytes at random into an
 // array larger than L2, a DRAM read-modify-write per record.
 __global__ void stage_gather_kernel (const float *__restrict__ pts, const int *__restrict__ order,
-                                     int n, float4 *__restrict__ staged, int *__restrict__ pos_of)
+                                     int n, float4 *__restrict__ staged)
 {
   const int k = blockIdx.x * blockDim.x + threadIdx.x;
   if (k >= n) return;
@@ -117,7 +122,6 @@ __global__ void stage_gather_kernel (const float *__restrict__ pts, const int *_
   const float x = __ldg (pts + 3 * (size_t)i), y = __ldg (pts + 3 * (size_t)i + 1),
               z = __ldg (pts + 3 * (size_t)i + 2);
   staged[k] = make_float4 (x, y, z, __int_as_float (i));
-  if (pos_of) pos_of[i] = k;
 }
 
 // Results back to input order: query i's record (cell as int bits, then the
@@ -172,11 +176,11 @@ int cell_positions (const drb_bvh *bvh, const float *pts, int n, unsigned *cell_
 
 // order[0..n) over caller buffers (as cell_positions).
 int cell_order (const drb_bvh *bvh, const float *pts, int n, int *order, unsigned *cell_of,
-                int *rank, int *hist, int *scan_tmp, cudaStream_t s)
+                int *rank, int *hist, int *scan_tmp, cudaStream_t s, int *pos_of = nullptr)
 {
   int st = cell_positions (bvh, pts, n, cell_of, rank, hist, scan_tmp, s);
   if (st) return st;
-  cell_scatter_kernel<<<div_up (n, 256), 256, 0, s>>> (cell_of, rank, hist, n, order);
+  cell_scatter_kernel<<<div_up (n, 256), 256, 0, s>>> (cell_of, rank, hist, n, order, pos_of);
   return check_launch ("cell_scatter_kernel");
 }
 
@@ -187,9 +191,9 @@ int cell_order (const drb_bvh *bvh, const float *pts, int n, int *order, unsigne
 int cell_stage (const drb_bvh *bvh, const float *pts, int n, float4 *staged, int *order,
                 unsigned *cell_of, int *rank, int *hist, int *scan_tmp, int *pos_of, cudaStream_t s)
 {
-  int st = cell_order (bvh, pts, n, order, cell_of, rank, hist, scan_tmp, s);
+  int st = cell_order (bvh, pts, n, order, cell_of, rank, hist, scan_tmp, s, pos_of);
   if (st) return st;
-  stage_gather_kernel<<<div_up (n, 256), 256, 0, s>>> (pts, order, n, staged, pos_of);
+  stage_gather_kernel<<<div_up (n, 256), 256, 0, s>>> (pts, order, n, staged);
   return check_launch ("stage_gather_kernel");
 }
 
