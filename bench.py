@@ -1491,11 +1491,11 @@ def main():
     dpts = torch.empty_like(pts)
 
     e2e_chunk = None
+    chunk_ms = {}
     if head_loc is not None:
         # drb_locate_host: chunked copies in and out overlapped with the
         # locate; the chunk size that pipelines best on this batch
-        chunk_ms = {}
-        for ch in (1 << 19, 1 << 20, 1 << 21):
+        for ch in (1 << 19, 1 << 20, 1 << 21, 1 << 22):
             head_loc.locate_host(host_pts, out=(host_cell, host_ref), chunk=ch)
             chunk_ms[ch] = timed(lambda: head_loc.locate_host(host_pts, out=(host_cell, host_ref),
                                                                chunk=ch), 3)
@@ -1627,6 +1627,7 @@ def main():
             "e2e": {"value": e2e_value, "unit": "points/s",
                     "h2d_bytes_per_step": int(n * 12), "d2h_bytes_per_step": int(n * 16),
                     "ms_per_step": e2e_ms, "chunk": e2e_chunk,
+                    "ms_by_chunk": {str(k): v / 3 for k, v in chunk_ms.items()},
                     "copies_only_ms": copy_ms,
                     "api": "drb_locate_host (pinned host buffers, copies overlapped)"
                            if head_loc is not None else
