@@ -1,4 +1,4 @@
-// Per-(element, point) kernels used to generate and judge the learned guess:
+// Per-(element, point) kernels used to generate and check the learned guess:
 //   map_points_kernel    physical point X_e(r) of reference points r
 //                        (Element::eval, pos_tensor_element.tcc:99-232)
 //   newton_pairs_kernel  Newton inversion of each point in a given element

@@ -1,7 +1,7 @@
 """Point-location parity on the GPU (drb_locate through the C-ABI) against
 the reference's Mesh::locate (oracle/_ref) and the restated oracle.
 
-Bar (from the north star): located element ids identical except for points
+Bar: located element ids identical except for points
 on shared faces/edges (counted and checked to be within the is_inside band
 of both elements); reference coordinates within 1e-5; the FP64 Newton error
 of every GPU result is stated and bounded.
