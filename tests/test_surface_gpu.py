@@ -80,4 +80,6 @@ def test_surface_render_matches_reference(cuda, ref, name):
     bad = np.any(d > 1.0 / 255.0, axis=-1)
     print(f"{name}: hits {np.mean(gidx >= 0):.3f}, mismatched hits {(~same).sum()}, "
           f"pixels > 1/255: {bad.sum()}, max diff {d.max():.2e}")
-    assert bad.mean() < 0.005
+    # the few rays on shared edges hit the neighbouring face, whose shading
+    # there is the same within 1/255: every pixel is within 1/255
+    assert not bad.any()
