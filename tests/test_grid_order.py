@@ -10,7 +10,8 @@ point's grid cell (every leaf whose box overlaps the cell, in leaf order)
 yields the same candidates in the same order.  Both halves are checked here
 with the walk restated from that file: on random points, on points placed
 exactly on leaf box faces and corners (where the <= / >= comparisons
-decide), and outside the mesh.  Points with a NaN coordinate are left out:
+decide), and outside the mesh; on the BVHs of hex (orders 2 and 3), tet,
+quad and triangle meshes.  Points with a NaN coordinate are left out:
 every box comparison with NaN is false, so the walk reaches every leaf
 while the grid maps the point to its first cell; no solve converges for
 such a point, so both give no cell."""
@@ -75,14 +76,25 @@ def _grid(lb: np.ndarray, o, inv, g):
     return cells
 
 
-@pytest.mark.parametrize("name", ["trilinear_6", "warped_p3_4"])
+@pytest.mark.parametrize("name", ["trilinear_6", "warped_p3_4", "tet_p2", "quad_p2", "tri_p2"])
 def test_walk_order_is_leaf_order_and_grid_scan_matches(ref, name):
     from devil_ray_b200 import meshgen
+    flat = name in ("quad_p2", "tri_p2")
     if name == "trilinear_6":
         m = meshgen.trilinear_distorted_mesh(6, 2, 0.15, seed=11)
-    else:
+        b = ref.RefHexMesh(m.order, m.ctrl_idx, m.xyz).bvh()
+    elif name == "warped_p3_4":
         m = meshgen.warped_mesh(4, 3, 0.08, jitter=0.01, seed=5)
-    b = ref.RefHexMesh(m.order, m.ctrl_idx, m.xyz).bvh()
+        b = ref.RefHexMesh(m.order, m.ctrl_idx, m.xyz).bvh()
+    elif name == "tet_p2":
+        m = meshgen.tet_warped_mesh(3, 2, 0.05, jitter=0.01, seed=5)
+        b = ref.RefTetMesh(m.order, m.ctrl_idx, m.xyz).bvh()
+    elif name == "quad_p2":
+        m = meshgen.quad_warped_mesh(8, 2, 0.04, jitter=0.004, seed=9)
+        b = ref.RefQuadMesh(m.order, m.ctrl_idx, m.xyz).bvh()
+    else:
+        m = meshgen.tri_warped_mesh(6, 2, 0.04, jitter=0.004, seed=9)
+        b = ref.RefTriMesh(m.order, m.ctrl_idx, m.xyz).bvh()
     inner = b["inner"]
     n_leaf = b["leaf_nodes"].shape[0]
     inner4 = inner.reshape(-1, 4)
@@ -93,6 +105,10 @@ def test_walk_order_is_leaf_order_and_grid_scan_matches(ref, name):
 
     rng = np.random.default_rng(7)
     pts = [rng.uniform(-0.05, 1.05, 3).astype(np.float32) for _ in range(1500)]
+    if flat:
+        # 2D meshes lie in z = 0: most queries on the plane, some off it
+        for q in pts[:1300]:
+            q[2] = 0.0
     # on leaf box faces and corners: coordinates taken from the boxes
     for k in rng.choice(n_leaf, 300, replace=False):
         q = rng.uniform(lb[k, 0::2], lb[k, 1::2]).astype(np.float32)
@@ -108,8 +124,10 @@ def test_walk_order_is_leaf_order_and_grid_scan_matches(ref, name):
     bounds = b["bounds"]
     o = bounds[0::2].astype(np.float32)
     ext = (lb[:, 1::2] - lb[:, 0::2]).mean(axis=0)
-    g = [max(1, int(np.ceil((bounds[2 * d + 1] - bounds[2 * d]) / ext[d]))) for d in range(3)]
-    inv = [np.float32(g[d] / (bounds[2 * d + 1] - bounds[2 * d])) for d in range(3)]
+    span = [float(bounds[2 * d + 1] - bounds[2 * d]) for d in range(3)]
+    g = [max(1, int(np.ceil(span[d] / ext[d]))) if ext[d] > 0 and span[d] > 0 else 1
+         for d in range(3)]
+    inv = [np.float32(g[d] / span[d]) if span[d] > 0 else np.float32(0) for d in range(3)]
     cells = _grid(lb, o, inv, g)
 
     reached = 0
